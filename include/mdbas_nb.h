@@ -1,0 +1,414 @@
+/*
+ * mdbas_nb.h -- C ABI of libmdbas_nb.so, the B200 (sm_100a) implementation of
+ * MDBas's real-space nonbonded hot path.
+ *
+ * Three groups of entry points:
+ *
+ *  1. Drop-in replacements with MDBas's own prototypes.  A MDBas build links
+ *     libmdbas_nb.so in place of obj/energy.o and obj/list.o; everything else
+ *     (integrators, bonded terms, k-space, I/O) stays MDBas's own code, which
+ *     these routines reach through weak references.  Errors go through
+ *     my_error-style reporting (message on stderr/outFile, exit) exactly as in
+ *     MDBas; the *_status API below returns codes instead.
+ *
+ *  2. A UserEnergyPtr plugin (include/user.h:29-33 of MDBas) plus the init call
+ *     the plugin ABI lacks (charges, LJ parameters, exclusions) and a getter for
+ *     the energy/virial the plugin ABI cannot return.
+ *
+ *  3. A device-resident engine (mdbas_nb_engine_*) that keeps positions,
+ *     topology, the cluster-pair list and the fixed-point accumulators in HBM
+ *     between calls; it is what the drop-in's mixed-precision mode and the
+ *     benchmarks drive.  Every engine call returns an mdbas_nb_status.
+ *
+ * Units are MDBas internal units throughout: lengths in Angstrom, energies in
+ * 10 J/mol (kcal/mol x 418.4), charges in e.
+ */
+#ifndef MDBAS_NB_H
+#define MDBAS_NB_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* MDBas data model.  Field order and types match MDBas include/global.h    */
+/* (enums :79-153, PBC :175-184, CTRL :195-217, PARAM :219-238, BOND         */
+/* :247-252, ANGLE :254-259, DIHE :261-267, NEIGH :269-276, ENERGY :282-290, */
+/* CONSTRAINT :296-300, EWALD :311-316) so that the same struct pointers can */
+/* be passed across the ABI.  When MDBas's global.h is already included its  */
+/* definitions are used instead.                                              */
+/* ------------------------------------------------------------------------ */
+#ifndef GLOBALH_INCLUDED
+#ifndef MDBAS_NB_MIRROR_TYPES
+#define MDBAS_NB_MIRROR_TYPES
+
+enum ELEC_TYPE { NOELEC = 0, FULL = 1, SHIFT1 = 2, SHIFT2 = 3, SWITCH = 4 };
+enum VDW_TYPE { NOVDW = 0, VFULL = 1, VSWITCH = 2 };
+enum BOX_TYPE { NOBOX = 0, CUBIC = 1, ORBIC = 2, TCLIN = 3 };
+enum INTEGRATOR_TYPE { LEAPFROG = 0, VELOCITY = 1 };
+enum ENSEMBLE_TYPE { NVE = 0, NVT_B = 1, NPT_B = 2, NVT_H = 3, NPT_H = 4 };
+enum BOND_TYPE { BHARM = 0, BMORSE = 1 };
+enum ANGLE_TYPE { AHARM = 0 };
+enum DIHE_TYPE { DCOS = 1, DHARM = 2 };
+
+typedef struct {
+  enum BOX_TYPE type;
+  double a, a1, a2, a3, b, b1, b2, b3, c, c1, c2, c3;
+  double u, u1, u2, u3, v, v1, v2, v3, w, w1, w2, w3;
+  double pa, pb, pc, det, vol, vol0;
+  double stress1, stress2, stress3;
+  double stress4, stress5, stress6;
+  double stress7, stress8, stress9;
+} PBC;
+
+typedef struct {
+  int newjob;
+  int keyRand, keyTraj, keyProp, keyForF, keyRest;
+  int printOut, printProp, printTraj, printRest;
+  int keyMd, mdType;
+  int seed;
+  int keyMinim;
+  int keyLink, noLink;
+  int keyConstH;
+  int keyNb14, keyNumForce;
+  int keyEwald, keyAlpha, keyMmax;
+  enum ELEC_TYPE elecType;
+  enum VDW_TYPE vdwType;
+  enum INTEGRATOR_TYPE integrator;
+  enum ENSEMBLE_TYPE ens;
+} CTRL;
+
+typedef struct {
+  int step, nSteps;
+  double timeStep, rTimeStep;
+  int nAtom, nDegFree, nFrozen;
+  int nBond, nAngle, nDihedral, nImproper, nUb;
+  int nConst, maxCycle;
+  double tolShake;
+  double chargeConst, delr, scal14;
+  double cutOff, rcutOff, cutOff2, rcutOff2;
+  double cutOn, cutOn2, switch2;
+  double temp0, press0, kinTemp0;
+  double tolMinim, maxminsiz, maxminst;
+} PARAM;
+
+typedef struct {
+  enum BOND_TYPE type;
+  int a, b;
+  double k, r0, beta;
+} BOND;
+
+typedef struct {
+  enum ANGLE_TYPE type;
+  int a, b, c;
+  double k, theta0;
+} ANGLE;
+
+typedef struct {
+  enum DIHE_TYPE type;
+  int order;
+  int a, b, c, d;
+  double k, phi0, mult;
+} DIHE;
+
+typedef struct {
+  int update;
+  int linkRatio;
+  int nCells;
+  int sizeList;
+  int nPair14;
+} NEIGH;
+
+typedef struct {
+  double tot, pot, kin;
+  double elec, vdw;
+  double bond, ang, ub, dihe, impr;
+  double conint, consv;
+  double virelec, virvdw, virbond, virub;
+  double virshake, virpot, virtot;
+} ENERGY;
+
+typedef struct {
+  int a, b;
+  double rc2;
+} CONSTRAINT;
+
+typedef struct {
+  int nbsp;
+  int mmax, m1max, m2max, m3max;
+  double prec, tol, tol1, alpha;
+} EWALD;
+
+#endif /* MDBAS_NB_MIRROR_TYPES */
+#endif /* GLOBALH_INCLUDED */
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+typedef enum {
+  MDBAS_NB_OK = 0,
+  MDBAS_NB_ERR_ARG = 1,          /* invalid argument (null pointer, bad size)   */
+  MDBAS_NB_ERR_CUDA = 2,         /* a CUDA runtime call failed                  */
+  MDBAS_NB_ERR_NO_DEVICE = 3,    /* no usable sm_100 device                     */
+  MDBAS_NB_ERR_ALLOC = 4,        /* device or host allocation failed            */
+  MDBAS_NB_ERR_CAPACITY = 5,     /* a device list outgrew its capacity; the
+                                    engine grows it and rebuilds, callers see
+                                    this only when growing failed               */
+  MDBAS_NB_ERR_BOX = 6,          /* box too small or unsupported for the path  */
+  MDBAS_NB_ERR_LINKCELL = 7,     /* fewer than 2*linkRatio+1 cells per side
+                                    (MDBas LNKCELL_NCELLS_ERROR)                */
+  MDBAS_NB_ERR_EXCL = 8,         /* exclusion topology invalid (MDBas
+                                    EXCLLIST_LASTATOM_ERROR / DIHE_NONPARAM)    */
+  MDBAS_NB_ERR_UNSUPPORTED = 9,  /* option not implemented on this path        */
+  MDBAS_NB_ERR_OVERFLOW = 10,    /* a fixed-point accumulator would overflow   */
+  MDBAS_NB_ERR_NONFINITE = 11,   /* NaN/Inf coordinates                         */
+  MDBAS_NB_ERR_MISSING = 12,     /* a MDBas routine this call delegates to
+                                    (bonded terms, k-space) is not linked       */
+  MDBAS_NB_ERR_STATE = 13        /* call out of order (e.g. compute before
+                                    positions were set)                         */
+} mdbas_nb_status;
+
+const char *mdbas_nb_status_string(int status);
+/* Last status recorded by any call in this process (drop-in routines record
+ * their status here before reporting it the MDBas way). */
+int mdbas_nb_last_status(void);
+/* Text of the last CUDA or validation failure (empty when none). */
+const char *mdbas_nb_last_message(void);
+/* Library version and the compute capability it was built for (1000 = sm_100a). */
+int mdbas_nb_version(void);
+int mdbas_nb_build_arch(void);
+
+/* Drop-in precision mode, read by energy()/ewald_energy()/nonbond_energy().
+ *   0 (default): plain FP64 GPU form over the caller's Verlet list, the same
+ *                pair set and operation order as MDBas's CPU loop.
+ *   1          : FP32 pair arithmetic + 64-bit fixed-point accumulation over
+ *                the library's own cluster-pair list (built on the device from
+ *                the same coordinates; equal to MDBas's pair set whenever the
+ *                caller's list is current, i.e. no atom moved more than half
+ *                the skin since it was built).
+ * The environment variable MDBAS_NB_MODE=fp64|mixed sets the initial value. */
+int mdbas_nb_set_mode(int mode);
+int mdbas_nb_get_mode(void);
+
+/* ------------------------------------------------------------------------ */
+/* 1. Drop-in replacements (MDBas include/energy.h, include/list.h)          */
+/* ------------------------------------------------------------------------ */
+
+/* Replaces init_energy_ptrs (energy.c:35-92): records ctrl->elecType and
+ * ctrl->vdwType; unknown values report UNKNOWN_ELEC/VDW errors like MDBas. */
+void init_energy_ptrs(CTRL *ctrl);
+
+/* Replaces energy() (include/energy.h:30-37, src/energy.c:103-205): zeroes
+ * forces, energies and the stress tensor, evaluates the nonbonded terms on the
+ * GPU, then MDBas's own bonded routines and freeze_atoms (weak references). */
+void energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, NEIGH *neigh,
+            BOND bond[], BOND ub[], ANGLE angle[], DIHE dihe[], DIHE impr[],
+            const double x[], const double y[], const double z[],
+            double vx[], double vy[], double vz[], double fx[], double fy[],
+            double fz[], const double q[], const double eps[], const double sig[],
+            const double eps14[], const double sig14[], const int frozen[],
+            const int neighList[], const int neighPair[], const int neighOrder[],
+            const int neighList14[], int **exclList, const int exclPair[]);
+
+/* Replaces nonbond_energy (include/energy.h:39-42, src/energy.c:216-345):
+ * cut-off Coulomb (shift1/shift2/switch per init_energy_ptrs) + switched LJ
+ * over the caller's list; accumulates into fx/fy/fz and ener. */
+void nonbond_energy(PARAM *param, ENERGY *ener, PBC *box,
+                    const double x[], const double y[], const double z[], double fx[], double fy[],
+                    double fz[], const double q[], const double eps[], const double sig[],
+                    const int neighList[], const int neighPair[], const int neighOrder[]);
+
+/* Replaces nonbond14_energy (include/energy.h:44-47, src/energy.c:356-439). */
+void nonbond14_energy(PARAM *param, ENERGY *ener, PBC *box, NEIGH *neigh,
+                      const double x[], const double y[], const double z[], double fx[], double fy[],
+                      double fz[], const double q[], const double eps[], const double sig[],
+                      const int neighList14[]);
+
+/* Replaces ewald_energy (include/energy.h:49-53, src/energy.c:450-643):
+ * real-space Ewald direct term + switched LJ over the caller's list and the
+ * erf exclusion correction on the GPU; keyEwald==1/2 k-space goes to MDBas's
+ * own ewald_rec/spme_energy (weak references). */
+void ewald_energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, const double x[],
+                  const double y[], const double z[], double fx[], double fy[],
+                  double fz[], const double q[], const double eps[], const double sig[],
+                  const int neighList[], const int neighPair[], const int neighOrder[],
+                  int **exclList, const int exclPair[]);
+
+/* Replaces ewald14_energy (include/energy.h:55-58, src/energy.c:654-742). */
+void ewald14_energy(PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, NEIGH *neigh,
+                    const double x[], const double y[], const double z[], double fx[], double fy[],
+                    double fz[], const double q[], const double eps[], const double sig[],
+                    const int neighList14[]);
+
+/* Replaces makelist (include/list.h:28-31, src/list.c:29-106). */
+void makelist(CTRL *ctrl, PARAM *param, PBC *box, NEIGH *neigh, CONSTRAINT constList[],
+              BOND bond[], ANGLE angle[], DIHE dihe[], DIHE impr[], double x[], double y[],
+              double z[], int frozen[], int **neighList, int **neighPair, int **neighOrder,
+              int **neighList14, int ***exclList, int **exclPair);
+
+/* Replaces exclude_list (include/list.h:33-35, src/list.c:108-894): half
+ * (j>i) exclusion rows, 1-4 pair list; host code (one-off topology walk). */
+void exclude_list(CTRL *ctrl, PARAM *param, NEIGH *neigh, CONSTRAINT constList[],
+                  BOND bond[], ANGLE angle[], DIHE dihe[], DIHE impr[],
+                  int **neighList14, int ***exclList, int **exclPair);
+
+/* Replaces verlet_list (include/list.h:37-39, src/list.c:896-1040): O(N^2)
+ * half list built on the GPU, same entries in the same order as MDBas. */
+void verlet_list(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[], double z[],
+                 int frozen[], int **neighList, int **neighPair, int **neighOrder,
+                 int **exclList, int exclPair[]);
+
+/* Replaces verlet_list_update (include/list.h:41-43, src/list.c:1042-1123). */
+void verlet_list_update(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[], double z[],
+                        int frozen[], int **neighList, int neighPair[], int **exclList,
+                        int exclPair[]);
+
+/* Replaces link_cell_exclude_list (include/list.h:45-47, src/list.c:1125-1791):
+ * symmetric exclusion rows; host code. */
+void link_cell_exclude_list(CTRL *ctrl, PARAM *param, NEIGH *neigh, CONSTRAINT constList[],
+                            BOND bond[], ANGLE angle[], DIHE dihe[], DIHE impr[],
+                            int **neighList14, int ***exclList, int **exclPair);
+
+/* Replaces link_cell_verlet_list (include/list.h:49-51, src/list.c:1793-2274):
+ * wraps x/y/z in place (image_update), bins into link cells and builds the
+ * half list on the GPU, same entries in the same order as MDBas. */
+void link_cell_verlet_list(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[], double z[],
+                           int frozen[], int **neighList, int **neighPair, int **neighOrder,
+                           int **exclList, int exclPair[]);
+
+/* Replaces link_cell_verlet_list_update (include/list.h:53-55,
+ * src/list.c:2276-2619): no wrap, list storage reused and grown by 1% steps. */
+void link_cell_verlet_list_update(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[],
+                                  double z[], int frozen[], int **neighList, int neighPair[],
+                                  int neighOrder[], int **exclList, int exclPair[]);
+
+/* ------------------------------------------------------------------------ */
+/* Status-returning forms of the drop-in list and energy routines.           */
+/* They take the same arguments and never exit the process.                  */
+/* ------------------------------------------------------------------------ */
+int mdbas_nb_verlet_list_status(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[],
+                                double z[], int frozen[], int **neighList, int **neighPair,
+                                int **neighOrder, int **exclList, int exclPair[], int update);
+int mdbas_nb_link_cell_list_status(PARAM *param, PBC *box, NEIGH *neigh, double x[], double y[],
+                                   double z[], int frozen[], int **neighList, int **neighPair,
+                                   int **neighOrder, int **exclList, int exclPair[], int update);
+int mdbas_nb_ewald_energy_status(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box,
+                                 const double x[], const double y[], const double z[], double fx[],
+                                 double fy[], double fz[], const double q[], const double eps[],
+                                 const double sig[], const int neighList[], const int neighPair[],
+                                 const int neighOrder[], int **exclList, const int exclPair[]);
+
+/* ------------------------------------------------------------------------ */
+/* 2. UserEnergyPtr plugin (MDBas include/user.h:29-33, plugins/custom_nb.c) */
+/* ------------------------------------------------------------------------ */
+
+/* The plugin ABI carries neither charges, LJ parameters nor exclusions:
+ * register them once.  eps/sig are MDBas per-atom values (eps_i =
+ * sqrt(eps*418.4), sig_i = FORF sigma).  exclPair/exclList use MDBas's
+ * layout (rows may be half or symmetric; only j>i entries are used).
+ * alpha is the Ewald splitting parameter; vdwSwitch selects vdw_switch (1)
+ * or no LJ (0). */
+int mdbas_nb_plugin_init(int nAtom, const double q[], const double eps[], const double sig[],
+                         const int exclPair[], int **exclList, double alpha, int vdwSwitch);
+
+/* UserEnergyPtr-compatible entry: real-space Ewald + switched LJ over the
+ * given half list, exclusion correction included; ADDS forces into fx/fy/fz
+ * and returns elec+vdw (internal units).  neighList14 is unused (water-style
+ * systems have no 1-4 pairs; ewald14_energy covers them in the drop-in). */
+double mdbas_nb_user_energy(const PARAM *param, const PBC *box,
+                            const double x[], const double y[], const double z[],
+                            double fx[], double fy[], double fz[],
+                            const int neighList[], const int neighPair[], const int neighOrder[],
+                            const int neighList14[]);
+
+/* Energy and virial terms of the last mdbas_nb_user_energy call:
+ * out[0..3] = elec, vdw, virelec, virvdw. */
+int mdbas_nb_plugin_last_energy(double out[4]);
+void mdbas_nb_plugin_release(void);
+
+/* ------------------------------------------------------------------------ */
+/* 3. Device-resident engine                                                 */
+/* ------------------------------------------------------------------------ */
+typedef struct mdbas_nb_engine mdbas_nb_engine;
+
+typedef struct {
+  int nAtom;
+  int device;             /* CUDA device ordinal                             */
+  double cutOff;          /* rc (A)                                          */
+  double cutOn;           /* LJ switch start (A)                             */
+  double delr;            /* Verlet skin (A)                                 */
+  double alpha;           /* Ewald splitting parameter (1/A)                 */
+  double chargeConst;     /* Coulomb constant in internal units              */
+  int vdwSwitch;          /* 1: vdw_switch, 0: no LJ                         */
+  int precision;          /* 0: plain FP64 pair kernel, 1: FP32 + fixed point */
+  int linkRatio;          /* precision 0: MDBas link ratio (1..5)            */
+  int noLink;             /* precision 0: force the all-pairs builder        */
+} mdbas_nb_engine_config;
+
+/* Energy/virial terms (internal units) filled by mdbas_nb_engine_energies. */
+typedef struct {
+  double elec_direct;     /* sum qel*erfc(a r)/r over in-cut-off pairs       */
+  double elec_corr;       /* -sum qel*erf(a r)/r over excluded pairs         */
+  double elec_self;       /* -C a/sqrt(pi) sum q^2                           */
+  double vdw;             /* switched LJ                                     */
+  double vir_direct;      /* sum r dE/dr, MDBas's virial convention          */
+  double vir_corr;
+  double vir_vdw;
+  double n_pairs;         /* in-cut-off pair interactions evaluated          */
+} mdbas_nb_energies;
+
+int mdbas_nb_engine_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *cfg,
+                           const PBC *box);
+int mdbas_nb_engine_destroy(mdbas_nb_engine *e);
+/* Work on this CUDA stream (cudaStream_t passed as void*; NULL = default). */
+int mdbas_nb_engine_set_stream(mdbas_nb_engine *e, void *stream);
+int mdbas_nb_engine_set_box(mdbas_nb_engine *e, const PBC *box);
+/* Per-atom topology.  eps/sig as MDBas per-atom values; frozen may be NULL;
+ * exclusions in MDBas row layout flattened: exclPair[i] entries of exclFlat
+ * per atom in order (half or symmetric rows; duplicates are harmless). */
+int mdbas_nb_engine_set_topology(mdbas_nb_engine *e, const double *q, const double *eps,
+                                 const double *sig, const int *frozen, const int *exclPair,
+                                 const int *exclFlat);
+/* Positions: host pointers (copied H2D on the engine stream) or device
+ * pointers (device != 0), FP64, original atom order. */
+int mdbas_nb_engine_set_positions(mdbas_nb_engine *e, const double *x, const double *y,
+                                  const double *z, int device_ptrs);
+/* Sort atoms into cells/clusters and build the cluster-pair list (precision 1)
+ * or the MDBas-format half list (precision 0). */
+int mdbas_nb_engine_build(mdbas_nb_engine *e);
+/* Refresh the per-atom float4 layout from the current FP64 positions without
+ * rebuilding the list (between rebuilds during dynamics). */
+int mdbas_nb_engine_refresh(mdbas_nb_engine *e);
+/* Evaluate forces, energies and virial into the device accumulators. */
+int mdbas_nb_engine_compute(mdbas_nb_engine *e);
+/* Forces in original atom order, FP64; host or device destination. */
+int mdbas_nb_engine_get_forces(mdbas_nb_engine *e, double *fx, double *fy, double *fz,
+                               int device_ptrs);
+int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out);
+/* Statistics of the current list: out[0] = clusters (or atoms), out[1] =
+ * list entries (cluster pairs or atom pairs), out[2] = candidate atom pairs
+ * evaluated per compute, out[3] = list capacity. */
+int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]);
+/* Export the atom-pair set the current list evaluates within distance
+ * sqrt(r2max) (original indices, i<j), for parity checks.  *count receives
+ * the number of pairs; pairs (2*capacity ints) may be NULL to query it. */
+int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, long long capacity,
+                                 long long *count);
+/* Kernels this engine launched since creation. */
+long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e);
+/* Average duration (ms) of the pair kernel over the launches recorded since
+ * the last call with reset != 0, measured with CUDA events on the engine
+ * stream when timing is enabled. */
+int mdbas_nb_engine_set_timing(mdbas_nb_engine *e, int enable);
+int mdbas_nb_engine_kernel_time(mdbas_nb_engine *e, int which, double *avg_ms, long long *count,
+                                int reset);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MDBAS_NB_H */

@@ -1,0 +1,526 @@
+// cluster.cu -- cell-sorted cluster layout and the cluster-pair list.
+//
+// Layout.  The box is cut into an x-y grid of cells ("columns") whose width
+// makes 8 atoms at the system's density fill a roughly cubic volume.  Cells
+// are numbered in Morton (Z-curve) order of their (cx, cy) indices, atoms are
+// counting-sorted into cells and sorted by z inside each cell, and every run
+// of 8 consecutive atoms of a cell is one cluster (a cell's last cluster is
+// padded).  Each cluster keeps an FP64 origin (its bounding-box centre) and
+// FP32 half extents; each atom slot keeps float4 (x,y,z relative to the
+// cluster origin, q*sqrt(C)) and float2 (2*eps_i, sig_i).  Relative FP32
+// coordinates keep ~1e-6 A resolution in any box size; the large part of
+// every displacement (origin to origin, periodic shift included) is formed
+// in FP64 once per cluster pair.
+//
+// Cluster-pair search ("cell sweep").  One warp per i cluster walks the
+// cells within reach in x-y (periodic images as explicit shifts), lanes test
+// 32 candidate j clusters at a time against the i bounding box for each
+// z image, and a ballot + prefix count compacts the survivors into a
+// per-warp buffer.  Newton's third law: each unordered cluster pair is kept
+// once (j > i, or j == i with a positive or zero shift, the latter with only
+// the upper triangle of atom pairs).  Buffers are flushed as work items of
+// 32 entries; at flush the warp builds each entry's 64-bit interaction mask
+// (padding, exclusions, frozen pairs, self-pair triangle) with two ballots.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "cluster.cuh"
+
+namespace mdbas {
+
+namespace {
+
+constexpr int kSearchThreads = 128;
+constexpr int kBufCap = 64;
+
+__device__ __forceinline__ double wrap_pos(double v, double L, double invL) {
+  return v - L * floor(v * invL + 0.5);
+}
+
+__global__ void k_col_bin(int n, ClusterGeom g, const int *__restrict__ colRank,
+                          const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, int *__restrict__ atomCol,
+                          double *__restrict__ atomZ, int *__restrict__ colCount,
+                          long long *__restrict__ counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double sx = x[i] / g.Lx + 0.5, sy = y[i] / g.Ly + 0.5, sz = z[i] / g.Lz + 0.5;
+  if (!(isfinite(sx) && isfinite(sy) && isfinite(sz))) {
+    atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), 2ull);
+    sx = sy = sz = 0.5;
+  }
+  sx -= floor(sx);
+  sy -= floor(sy);
+  sz -= floor(sz);
+  const int cx = min((int)(sx * g.ncx), g.ncx - 1);
+  const int cy = min((int)(sy * g.ncy), g.ncy - 1);
+  const int col = colRank[cy * g.ncx + cx];
+  atomCol[i] = col;
+  atomZ[i] = sz;
+  atomicAdd(colCount + col, 1);
+}
+
+__global__ void k_col_pad(int nCols, const int *__restrict__ colCount, int *__restrict__ colPad) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < nCols) colPad[c] = (colCount[c] + kClusterSize - 1) & ~(kClusterSize - 1);
+}
+
+__global__ void k_col_clstart(int nCols, const int *__restrict__ colPadStart,
+                              int *__restrict__ colClStart) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= nCols) colClStart[c] = colPadStart[c] / kClusterSize;
+}
+
+__global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
+                              const int *__restrict__ colStart, int *__restrict__ colFill,
+                              int *__restrict__ tmpIdx) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = atomCol[i];
+  tmpIdx[colStart[c] + atomicAdd(colFill + c, 1)] = i;
+}
+
+// Sort a cell's atoms by (z, index): rank = members ordered before this one.
+__global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
+                           const int *__restrict__ colPadStart, const int *__restrict__ tmpIdx,
+                           const double *__restrict__ atomZ, int *__restrict__ slotAtom) {
+  __shared__ double sz[512];
+  __shared__ int si[512];
+  const int c = blockIdx.x;
+  if (c >= nCols) return;
+  const int s = colStart[c], e = colStart[c + 1];
+  const int ps = colPadStart[c], pe = colPadStart[c + 1];
+  for (int base = s; base < e; base += blockDim.x) {
+    const int m = base + threadIdx.x;
+    const int mi = (m < e) ? tmpIdx[m] : 0;
+    const double mz = (m < e) ? atomZ[mi] : 0.0;
+    int rank = 0;
+    for (int cb = s; cb < e; cb += 512) {
+      const int cnt = min(512, e - cb);
+      __syncthreads();
+      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const int a = tmpIdx[cb + t];
+        si[t] = a;
+        sz[t] = atomZ[a];
+      }
+      __syncthreads();
+      if (m < e)
+        for (int t = 0; t < cnt; ++t)
+          rank += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+    }
+    if (m < e) slotAtom[ps + rank] = mi;
+  }
+  for (int p = ps + (e - s) + threadIdx.x; p < pe; p += blockDim.x) slotAtom[p] = -1;
+}
+
+// One thread per cluster: FP64 origin and half extents, slot data.
+__global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__ slotAtom,
+                           const int *__restrict__ atomCol, const int *__restrict__ colXY,
+                           const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, const double *__restrict__ q,
+                           const double *__restrict__ eps, const double *__restrict__ sig,
+                           double sqrtC, double4 *__restrict__ origin, float4 *__restrict__ half,
+                           float4 *__restrict__ xq, float2 *__restrict__ lj,
+                           int *__restrict__ slotOf, int *__restrict__ clusterXY) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nClusters) return;
+  const double ilx = 1.0 / g.Lx, ily = 1.0 / g.Ly, ilz = 1.0 / g.Lz;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  double px[kClusterSize], py[kClusterSize], pz[kClusterSize];
+  int atoms[kClusterSize];
+#pragma unroll
+  for (int k = 0; k < kClusterSize; ++k) {
+    const int a = slotAtom[c * kClusterSize + k];
+    atoms[k] = a;
+    if (a >= 0) {
+      px[k] = wrap_pos(x[a], g.Lx, ilx);
+      py[k] = wrap_pos(y[a], g.Ly, ily);
+      pz[k] = wrap_pos(z[a], g.Lz, ilz);
+      lo[0] = fmin(lo[0], px[k]); hi[0] = fmax(hi[0], px[k]);
+      lo[1] = fmin(lo[1], py[k]); hi[1] = fmax(hi[1], py[k]);
+      lo[2] = fmin(lo[2], pz[k]); hi[2] = fmax(hi[2], pz[k]);
+    }
+  }
+  const double ox = 0.5 * (lo[0] + hi[0]), oy = 0.5 * (lo[1] + hi[1]), oz = 0.5 * (lo[2] + hi[2]);
+  origin[c] = make_double4(ox, oy, oz, 0.0);
+  // Half extents rounded up so that the FP32 box always contains its atoms.
+  half[c] = make_float4(__double2float_ru(0.5 * (hi[0] - lo[0]) * (1.0 + 1e-6) + 1e-6),
+                        __double2float_ru(0.5 * (hi[1] - lo[1]) * (1.0 + 1e-6) + 1e-6),
+                        __double2float_ru(0.5 * (hi[2] - lo[2]) * (1.0 + 1e-6) + 1e-6), 0.f);
+  clusterXY[c] = colXY[atomCol[atoms[0]]];
+#pragma unroll
+  for (int k = 0; k < kClusterSize; ++k) {
+    const int s = c * kClusterSize + k;
+    const int a = atoms[k];
+    if (a >= 0) {
+      xq[s] = make_float4((float)(px[k] - ox), (float)(py[k] - oy), (float)(pz[k] - oz),
+                          (float)(q[a] * sqrtC));
+      lj[s] = make_float2((float)(2.0 * eps[a]), (float)sig[a]);
+      slotOf[a] = s;
+    } else {
+      xq[s] = make_float4(0.f, 0.f, 0.f, 0.f);
+      lj[s] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+__device__ __forceinline__ bool excl_has(int es, int ee, const int *__restrict__ exclFlat, int j) {
+  for (int k = es; k < ee; ++k)
+    if (__ldg(exclFlat + k) == j) return true;
+  return false;
+}
+
+struct SearchBuf {
+  int j[kBufCap];
+  int sidx[kBufCap];
+  float sx[kBufCap], sy[kBufCap], sz[kBufCap];
+  uint2 mask[kItemMax];
+};
+
+// Flush the first cnt (<= kItemMax) buffered entries as one work item.
+__device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, int ia, int fi, int es, int ee,
+                           const int *__restrict__ slotAtom, const int *__restrict__ frozen,
+                           const int *__restrict__ exclFlat, CPairEntry *__restrict__ entries,
+                           uint2 *__restrict__ masks, int4 *__restrict__ items,
+                           long long *__restrict__ counters, long long entryCap,
+                           long long itemCap) {
+  const int il = lane & 7, jl = lane >> 3;
+  for (int k = 0; k < cnt; ++k) {
+    const int cj = B.j[k];
+    const bool selfzero = (cj == ci) && (B.sidx[k] == 13);
+    const int ja = slotAtom[cj * kClusterSize + jl];
+    const int jb = slotAtom[cj * kClusterSize + jl + 4];
+    bool oka = (ia >= 0) && (ja >= 0);
+    bool okb = (ia >= 0) && (jb >= 0);
+    if (oka) {
+      if (frozen && fi * frozen[ja] != 0) oka = false;
+      else if (selfzero && jl <= il) oka = false;
+      else if (excl_has(es, ee, exclFlat, ja)) oka = false;
+    }
+    if (okb) {
+      if (frozen && fi * frozen[jb] != 0) okb = false;
+      else if (selfzero && jl + 4 <= il) okb = false;
+      else if (excl_has(es, ee, exclFlat, jb)) okb = false;
+    }
+    const unsigned mlo = __ballot_sync(0xffffffffu, oka);
+    const unsigned mhi = __ballot_sync(0xffffffffu, okb);
+    if (lane == 0) B.mask[k] = make_uint2(mlo, mhi);
+  }
+  long long e0 = 0, it = 0;
+  if (lane == 0) {
+    e0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 0),
+                              (unsigned long long)cnt);
+    it = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 1), 1ull);
+  }
+  __syncwarp();
+  e0 = __shfl_sync(0xffffffffu, e0, 0);
+  it = __shfl_sync(0xffffffffu, it, 0);
+  if (e0 + cnt > entryCap || it >= itemCap) {
+    if (lane == 0) atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), 1ull);
+    return;
+  }
+  for (int k = lane; k < cnt; k += 32) {
+    CPairEntry en;
+    en.j = B.j[k];
+    en.sx = B.sx[k];
+    en.sy = B.sy[k];
+    en.sz = B.sz[k];
+    entries[e0 + k] = en;
+    masks[e0 + k] = B.mask[k];
+  }
+  if (lane == 0) items[it] = make_int4(ci, (int)e0, cnt, 0);
+}
+
+__global__ void __launch_bounds__(kSearchThreads)
+k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
+         const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
+         const double4 *__restrict__ origin, const float4 *__restrict__ half,
+         const int *__restrict__ slotAtom, const int *__restrict__ frozen,
+         const int *__restrict__ exclStart, const int *__restrict__ exclFlat,
+         CPairEntry *__restrict__ entries, uint2 *__restrict__ masks, int4 *__restrict__ items,
+         long long *__restrict__ counters, long long entryCap, long long itemCap) {
+  __shared__ SearchBuf bufs[kSearchThreads / 32];
+  const int lane = threadIdx.x & 31;
+  const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (ci >= nClusters) return;
+  SearchBuf &B = bufs[threadIdx.x >> 5];
+
+  const double4 oi = origin[ci];
+  const float4 hi = half[ci];
+  const int xy = clusterXY[ci];
+  const int cx = xy & 0xffff, cy = xy >> 16;
+  const int ia = slotAtom[ci * kClusterSize + (lane & 7)];
+  const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
+  const int es = (ia >= 0) ? exclStart[ia] : 0;
+  const int ee = (ia >= 0) ? exclStart[ia + 1] : 0;
+  const float rl = sqrtf(g.rlist2);
+  int cnt = 0;
+  long long cand = 0;
+
+  for (int dy = -g.Dy; dy <= g.Dy; ++dy) {
+    int jy = cy + dy, sy = 0;
+    if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
+    // distance in y from the i box to the cell's y interval (this image)
+    {
+      const double ylo = -0.5 * g.Ly + jy * g.wy + sy * g.Ly, yhi = ylo + g.wy;
+      const double gy = fmax(fmax(ylo - (oi.y + hi.y), (oi.y - hi.y) - yhi), 0.0);
+      if (gy > rl) continue;
+    }
+    for (int dx = -g.Dx; dx <= g.Dx; ++dx) {
+      int jx = cx + dx, sx = 0;
+      if (jx < 0) { jx += g.ncx; sx = -1; } else if (jx >= g.ncx) { jx -= g.ncx; sx = 1; }
+      const double xlo = -0.5 * g.Lx + jx * g.wx + sx * g.Lx, xhi = xlo + g.wx;
+      const double gx = fmax(fmax(xlo - (oi.x + hi.x), (oi.x - hi.x) - xhi), 0.0);
+      if (gx > rl) continue;
+      const int col = colRank[jy * g.ncx + jx];
+      const int cs = colClStart[col], ce = colClStart[col + 1];
+      for (int base = cs; base < ce; base += 32) {
+        const int cj = base + lane;
+        const bool valid = cj < ce;
+        double4 oj = make_double4(0, 0, 0, 0);
+        float4 hj = make_float4(0, 0, 0, 0);
+        if (valid) {
+          oj = origin[cj];
+          hj = half[cj];
+        }
+        const double ddx = oj.x + sx * g.Lx - oi.x;
+        const double ddy = oj.y + sy * g.Ly - oi.y;
+        for (int sz = -1; sz <= 1; ++sz) {
+          const double ddz = oj.z + sz * g.Lz - oi.z;
+          const float fx = (float)ddx, fy = (float)ddy, fz = (float)ddz;
+          const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
+          const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
+          const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
+          const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+          const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
+          const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
+          const bool pass = valid && half_ok && (gxx * gxx + gyy * gyy + gzz * gzz <= g.rlist2);
+          cand += valid;
+          const unsigned m = __ballot_sync(0xffffffffu, pass);
+          const int add = __popc(m);
+          if (add == 0) continue;
+          if (cnt + add > kBufCap) {
+            // cannot happen with kBufCap >= 2*kItemMax, flushed below
+          }
+          if (pass) {
+            const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+            B.j[pos] = cj;
+            B.sidx[pos] = sidx;
+            B.sx[pos] = fx;
+            B.sy[pos] = fy;
+            B.sz[pos] = fz;
+          }
+          cnt += add;
+          __syncwarp();
+          if (cnt >= kItemMax) {
+            flush_item(B, kItemMax, ci, lane, ia, fi, es, ee, slotAtom, frozen, exclFlat, entries,
+                       masks, items, counters, entryCap, itemCap);
+            __syncwarp();
+            const int rem = cnt - kItemMax;
+            if (lane < rem) {
+              const int jv = B.j[kItemMax + lane], sv = B.sidx[kItemMax + lane];
+              const float a = B.sx[kItemMax + lane], b = B.sy[kItemMax + lane],
+                          c = B.sz[kItemMax + lane];
+              __syncwarp(__activemask());
+              B.j[lane] = jv;
+              B.sidx[lane] = sv;
+              B.sx[lane] = a;
+              B.sy[lane] = b;
+              B.sz[lane] = c;
+            }
+            cnt = rem;
+            __syncwarp();
+          }
+        }
+      }
+    }
+  }
+  if (cnt > 0) {
+    flush_item(B, cnt, ci, lane, ia, fi, es, ee, slotAtom, frozen, exclFlat, entries, masks,
+               items, counters, entryCap, itemCap);
+  }
+  // candidate statistics
+  cand = __shfl_sync(0xffffffffu, cand, 0) * 0 + cand;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
+  if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3),
+                           (unsigned long long)cand);
+}
+
+__global__ void k_refresh(int nSlots, ClusterGeom g, const int *__restrict__ slotAtom,
+                          const double4 *__restrict__ origin, const double *__restrict__ x,
+                          const double *__restrict__ y, const double *__restrict__ z,
+                          const double *__restrict__ q, double sqrtC, float4 *__restrict__ xq) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nSlots) return;
+  const int a = slotAtom[s];
+  if (a < 0) return;
+  const double4 o = origin[s / kClusterSize];
+  double dx = x[a] - o.x, dy = y[a] - o.y, dz = z[a] - o.z;
+  dx -= g.Lx * rint(dx / g.Lx);
+  dy -= g.Ly * rint(dy / g.Ly);
+  dz -= g.Lz * rint(dz / g.Lz);
+  xq[s] = make_float4((float)dx, (float)dy, (float)dz, (float)(q[a] * sqrtC));
+}
+
+unsigned morton2(unsigned x, unsigned y) {
+  auto spread = [](unsigned v) {
+    v &= 0xffff;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+  };
+  return spread(x) | (spread(y) << 1);
+}
+
+}  // namespace
+
+int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
+                  double sqrtC, const double *x, const double *y, const double *z,
+                  const double *q, const double *eps, const double *sig, const int *frozen,
+                  const int *exclStart, const int *exclFlat, cudaStream_t s) {
+  if (b.type != CUBIC && b.type != ORBIC) return MDBAS_NB_ERR_UNSUPPORTED;
+  if (n <= 0) return MDBAS_NB_ERR_ARG;
+  ClusterGeom g{};
+  g.Lx = b.a1;
+  g.Ly = (b.type == CUBIC) ? b.a1 : b.b2;
+  g.Lz = (b.type == CUBIC) ? b.a1 : b.c3;
+  const double rlist = cutOff + delr;
+  // The pair kernel relies on a unique image within the cut-off.
+  if (std::min(g.Lx, std::min(g.Ly, g.Lz)) <= 2.0 * cutOff) return MDBAS_NB_ERR_BOX;
+  const double vol = g.Lx * g.Ly * g.Lz;
+  const double w0 = std::cbrt((double)kClusterSize * vol / (double)n);
+  g.ncx = std::max(1, (int)std::lround(g.Lx / w0));
+  g.ncy = std::max(1, (int)std::lround(g.Ly / w0));
+  g.wx = g.Lx / g.ncx;
+  g.wy = g.Ly / g.ncy;
+  g.Dx = (int)std::floor(rlist / g.wx) + 1;
+  g.Dy = (int)std::floor(rlist / g.wy) + 1;
+  if (g.Dx >= g.ncx || g.Dy >= g.ncy) {
+    // Fewer cells than the search reaches: use one cell column fewer than
+    // the reach in that direction so shifts stay within one image.
+    if (rlist + g.wx >= g.Lx || rlist + g.wy >= g.Ly) return MDBAS_NB_ERR_BOX;
+    if (g.Dx >= g.ncx) g.Dx = g.ncx - 1;
+    if (g.Dy >= g.ncy) g.Dy = g.ncy - 1;
+  }
+  g.rlist2 = (float)(rlist * rlist * (1.0 + 1e-5));
+  const int nCols = g.ncx * g.ncy;
+
+  // Morton rank of each (cx, cy) cell; rebuilt when the grid changes.
+  if (nCols != w.nCols || g.ncx != w.geom.ncx || g.ncy != w.geom.ncy) {
+    std::vector<std::pair<unsigned, int>> keys(nCols);
+    for (int cy = 0; cy < g.ncy; ++cy)
+      for (int cx = 0; cx < g.ncx; ++cx)
+        keys[cy * g.ncx + cx] = {morton2(cx, cy), cy * g.ncx + cx};
+    std::sort(keys.begin(), keys.end());
+    std::vector<int> rank(nCols), xyOf(nCols);
+    for (int r = 0; r < nCols; ++r) {
+      const int cell = keys[r].second;
+      rank[cell] = r;
+      xyOf[r] = (cell % g.ncx) | ((cell / g.ncx) << 16);
+    }
+    MDB_TRY(w.colRank.ensure(sizeof(int) * nCols));
+    MDB_TRY(w.colXY.ensure(sizeof(int) * nCols));
+    MDB_CUDA(cudaMemcpyAsync(w.colRank.p, rank.data(), sizeof(int) * nCols,
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(w.colXY.p, xyOf.data(), sizeof(int) * nCols,
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+  }
+  w.geom = g;
+  w.nCols = nCols;
+
+  MDB_TRY(w.colCount.ensure(sizeof(int) * (nCols + 1)));
+  MDB_TRY(w.colFill.ensure(sizeof(int) * (nCols + 1)));
+  MDB_TRY(w.colStart.ensure(sizeof(int) * (nCols + 2)));
+  MDB_TRY(w.colPad.ensure(sizeof(int) * (nCols + 1)));
+  MDB_TRY(w.colPadStart.ensure(sizeof(int) * (nCols + 2)));
+  MDB_TRY(w.colClStart.ensure(sizeof(int) * (nCols + 2)));
+  MDB_TRY(w.atomCol.ensure(sizeof(int) * n));
+  MDB_TRY(w.atomZ.ensure(sizeof(double) * n));
+  MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
+  MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
+  MDB_TRY(w.scanTmp.ensure(scan_tmp_bytes(std::max(n, nCols) + 1)));
+  MDB_TRY(w.counters.ensure(sizeof(long long) * 4));
+  MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
+
+  MDB_CUDA(cudaMemsetAsync(w.colCount.p, 0, sizeof(int) * (nCols + 1), s));
+  MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
+  MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
+  MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, g, w.colRank.as<int>(), x, y, z,
+             w.atomCol.as<int>(), w.atomZ.as<double>(), w.colCount.as<int>(),
+             w.counters.as<long long>());
+  MDB_TRY(exclusive_scan32(w.colCount.as<int>(), w.colStart.as<int>(), nCols, w.scanTmp.p, s));
+  MDB_LAUNCH(k_col_pad, grid_for(nCols, 256), 256, 0, s, nCols, w.colCount.as<int>(),
+             w.colPad.as<int>());
+  MDB_TRY(exclusive_scan32(w.colPad.as<int>(), w.colPadStart.as<int>(), nCols, w.scanTmp.p, s));
+  int nSlots = 0;
+  long long flags[4];
+  MDB_CUDA(cudaMemcpyAsync(&nSlots, w.colPadStart.as<int>() + nCols, sizeof(int),
+                           cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaStreamSynchronize(s));
+  if (flags[2] & 2) return MDBAS_NB_ERR_NONFINITE;
+  w.nSlots = nSlots;
+  w.nClusters = nSlots / kClusterSize;
+  const int nCl = w.nClusters;
+
+  MDB_TRY(w.slotAtom.ensure(sizeof(int) * nSlots));
+  MDB_TRY(w.clusterXY.ensure(sizeof(int) * nCl));
+  MDB_TRY(w.origin.ensure(sizeof(double4) * nCl));
+  MDB_TRY(w.half.ensure(sizeof(float4) * nCl));
+  MDB_TRY(w.xq.ensure(sizeof(float4) * nSlots));
+  MDB_TRY(w.lj.ensure(sizeof(float2) * nSlots));
+  MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)nSlots));
+
+  MDB_LAUNCH(k_col_clstart, grid_for(nCols + 1, 256), 256, 0, s, nCols, w.colPadStart.as<int>(),
+             w.colClStart.as<int>());
+  MDB_LAUNCH(k_col_scatter, grid_for(n, 256), 256, 0, s, n, w.atomCol.as<int>(),
+             w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
+  MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
+             w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
+  MDB_LAUNCH(k_clusters, grid_for(nCl, 128), 128, 0, s, nCl, g, w.slotAtom.as<int>(),
+             w.atomCol.as<int>(), w.colXY.as<int>(), x, y, z, q, eps, sig, sqrtC,
+             w.origin.as<double4>(), w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(),
+             w.slotOf.as<int>(), w.clusterXY.as<int>());
+
+  // Cluster-pair search; grow the list and search again if it overflowed.
+  if (w.entryCap == 0) {
+    w.entryCap = (long long)nCl * 160 + 4096;
+    w.itemCap = w.entryCap / kItemMax + nCl + 1024;
+  }
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    MDB_TRY(w.entries.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
+    MDB_TRY(w.masks.ensure(sizeof(uint2) * (size_t)w.entryCap));
+    MDB_TRY(w.items.ensure(sizeof(int4) * (size_t)w.itemCap));
+    MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
+    MDB_LAUNCH(k_search, grid_for((long long)nCl * 32, kSearchThreads), kSearchThreads, 0, s, nCl,
+               g, w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
+               w.origin.as<double4>(), w.half.as<float4>(), w.slotAtom.as<int>(), frozen,
+               exclStart, exclFlat, w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+               w.items.as<int4>(), w.counters.as<long long>(), w.entryCap, w.itemCap);
+    MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+    w.nEntries = flags[0];
+    w.nItems = flags[1];
+    if (!(flags[2] & 1)) return MDBAS_NB_OK;
+    w.entryCap = (long long)(flags[0] * 1.25) + 4096;
+    w.itemCap = (long long)(flags[1] * 1.25) + 1024;
+  }
+  return MDBAS_NB_ERR_CAPACITY;
+}
+
+int cluster_refresh(ClusterWork &w, int n, const DevBox &b, const double *x, const double *y,
+                    const double *z, const double *q, double sqrtC, cudaStream_t s) {
+  (void)n;
+  (void)b;
+  if (w.nSlots <= 0) return MDBAS_NB_ERR_STATE;
+  MDB_LAUNCH(k_refresh, grid_for(w.nSlots, 256), 256, 0, s, w.nSlots, w.geom,
+             w.slotAtom.as<int>(), w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>());
+  return MDBAS_NB_OK;
+}
+
+}  // namespace mdbas

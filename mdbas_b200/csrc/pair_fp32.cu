@@ -1,0 +1,329 @@
+// pair_fp32.cu -- mixed-precision cluster-pair kernel (FP32 pair arithmetic,
+// 64-bit fixed-point accumulation) and its FP64 companions.
+//
+// Mapping.  One warp runs one work item: an i cluster (8 atoms) against up
+// to 32 j clusters.  Lane L owns i atom L%8 and j atoms L/8 and L/8+4 of each
+// j cluster, i.e. exactly bits L and 32+L of the entry's 64-bit interaction
+// mask.  Per j cluster the warp computes all 64 pairs with MDBas's formulas
+// (Ewald direct term, src/ewald.c:356-369; vdw_switch, src/vdw.c:144-184):
+//   - displacement: FP32 j-relative coordinates + the entry's FP32 shift
+//     (origin-to-origin vector formed in FP64) - FP32 i-relative coordinates;
+//   - erfc(x) = t P(t) exp(-x^2), t = 1/(1+px), P of degree 7 (own refit of
+//     the Abramowitz-Stegun 7.1.26 form, fit_erfc.py, max relative error
+//     2.4e-8 on [0, 6]); hardware rsqrt/rcp/ex2 (3 MUFU per pair);
+// the j forces are reduced across the 8 i lanes with a 3-step shuffle
+// reduce-scatter (6 shuffles for 6 values) and each j atom component is added
+// once per cluster pair (Newton's third law) as a 64-bit fixed-point
+// integer; i forces stay in registers for the whole item.  Energies and
+// virials are summed in FP32 per lane within an item and converted to fixed
+// point once per item.  Every quantity that reaches an accumulator is a
+// fixed-point integer computed from one cluster pair, one item or one
+// excluded pair, so the totals do not depend on the order in which warps or
+// blocks run, nor on the order in which the list builder emitted items.
+#include "cluster.cuh"
+#include "pair_fp32.cuh"
+
+namespace mdbas {
+
+namespace {
+
+// erfc fit constants (fit_erfc.py)
+constexpr float kErfcP = 3.225531683e-01f;
+constexpr float kErfcC0 = 1.826605733e-01f;
+constexpr float kErfcC1 = 1.717395874e-01f;
+constexpr float kErfcC2 = 2.389294945e-01f;
+constexpr float kErfcC3 = -8.776152576e-02f;
+constexpr float kErfcC4 = 6.608865734e-01f;
+constexpr float kErfcC5 = -6.320509922e-01f;
+constexpr float kErfcC6 = 6.305108379e-01f;
+constexpr float kErfcC7 = -1.649145727e-01f;
+
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// One pair.  d = x_j - x_i.  Returns whether it interacted; adds energy and
+// virial terms; f = (dE/dr)/r * d is the force on i (minus the force on j).
+template <bool VDW>
+__device__ __forceinline__ bool interact(const PairConstF &c, const float4 xj, const float2 lj,
+                                         const float sx, const float sy, const float sz,
+                                         const float qi, const float2 li, const bool bit,
+                                         float &fx, float &fy, float &fz, float &ec, float &ev,
+                                         float &vc, float &vv) {
+  const float dx = xj.x + sx, dy = xj.y + sy, dz = xj.z + sz;
+  const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+  const bool in = bit && (r2 <= c.rc2);
+  const float r2s = in ? r2 : 1.0f;
+  const float rinv = rsqrt_approx(r2s);
+  const float r = r2s * rinv;
+  const float qq = in ? qi * xj.w : 0.f;
+  const float t = rcp_approx(fmaf(c.p_alpha, r, 1.0f));
+  const float ex = ex2_approx(-c.c_ex * r2s);
+  float poly = fmaf(kErfcC7, t, kErfcC6);
+  poly = fmaf(poly, t, kErfcC5);
+  poly = fmaf(poly, t, kErfcC4);
+  poly = fmaf(poly, t, kErfcC3);
+  poly = fmaf(poly, t, kErfcC2);
+  poly = fmaf(poly, t, kErfcC1);
+  poly = fmaf(poly, t, kErfcC0);
+  const float qr = qq * rinv;
+  const float e_c = qr * (t * poly * ex);
+  const float de_c = -fmaf(qq * c.two_a_sqrtpi, ex, e_c) * rinv;
+  ec += e_c;
+  vc = fmaf(de_c, r, vc);
+  float F = de_c;
+  if (VDW) {
+    const float eps = in ? li.x * lj.x : 0.f;  // 4 eps_i eps_j
+    const float sg = (li.y + lj.y) * rinv;
+    const float s2 = sg * sg;
+    const float s6 = s2 * s2 * s2;
+    const float s12 = s6 * s6;
+    const float pv = eps * (s12 - s6);
+    const float dpv = eps * fmaf(-12.f, s12, 6.f * s6);  // r dE/dr
+    const bool sw = r2s > c.ron2;
+    const float s1 = c.rc2 - r2s;
+    const float S = sw ? s1 * s1 * fmaf(c.sw_a, r2s, c.sw_b) : 1.f;
+    const float dS = sw ? c.sw_c * r2s * s1 * (c.ron2 - r2s) : 0.f;
+    const float de_v = fmaf(pv, dS, dpv * S) * rinv;
+    ev = fmaf(pv, S, ev);
+    vv = fmaf(de_v, r, vv);
+    F += de_v;
+  }
+  F *= rinv;
+  fx = F * dx;
+  fy = F * dy;
+  fz = F * dz;
+  return in;
+}
+
+template <bool VDW>
+__global__ void __launch_bounds__(256)
+k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ items,
+            const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
+            const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
+            long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jh = lane >> 3;
+  const bool up = il & 4, mid = il & 2, lo = il & 1;
+  const int comp = mid ? (lo ? 3 : 2) : (lo ? 1 : 0);
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * nSlots;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;  // fixed point, summed per item
+  long long npair = 0;
+  bool overflow = false;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float ec = 0.f, ev = 0.f, vc = 0.f, vv = 0.f;
+    for (int e = e0; e < e0 + ne; ++e) {
+      const CPairEntry en = entries[e];
+      const uint2 mk = masks[e];
+      const float sx = en.sx - xi.x, sy = en.sy - xi.y, sz = en.sz - xi.z;
+      const int jb = en.j * kClusterSize + jh;
+      const float4 xa = xq[jb];
+      const float2 la = lj[jb];
+      const float4 xb = xq[jb + 4];
+      const float2 lb = lj[jb + 4];
+      float ax, ay, az, bx, by, bz;
+      const bool ina = interact<VDW>(c, xa, la, sx, sy, sz, xi.w, li, (mk.x >> lane) & 1u, ax,
+                                     ay, az, ec, ev, vc, vv);
+      const bool inb = interact<VDW>(c, xb, lb, sx, sy, sz, xi.w, li, (mk.y >> lane) & 1u, bx,
+                                     by, bz, ec, ev, vc, vv);
+      fix += ax + bx;
+      fiy += ay + by;
+      fiz += az + bz;
+      const unsigned ba = __ballot_sync(0xffffffffu, ina);
+      const unsigned bb = __ballot_sync(0xffffffffu, inb);
+      if ((ba | bb) == 0u) continue;
+      npair += __popc(ba) + __popc(bb);
+      // reduce-scatter of the two j atoms' forces over the 8 i lanes
+      float k0 = up ? bx : ax, k1 = up ? by : ay, k2 = up ? bz : az;
+      const float s0 = up ? ax : bx, s1 = up ? ay : by, s2 = up ? az : bz;
+      k0 += __shfl_xor_sync(0xffffffffu, s0, 4);
+      k1 += __shfl_xor_sync(0xffffffffu, s1, 4);
+      k2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+      const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
+      float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
+      u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
+      u1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+      const float w = lo ? u0 : u1;
+      float v = lo ? u1 : u0;
+      v += __shfl_xor_sync(0xffffffffu, w, 1);
+      if (comp < 3 && v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(fcomp + en.j * kClusterSize + (up ? jh + 4 : jh), fix_f(-v));
+      }
+    }
+    // i forces: sum over the four j lanes of each i atom
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jh < 3) {
+      const float v = (jh == 0) ? fix : (jh == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)jh * nSlots + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    // Each item's energy is converted to fixed point on its own, so totals
+    // do not depend on which warp ran which item.
+    Ec += fix_e(warp_sum_d((double)ec));
+    Ev += fix_e(warp_sum_d((double)ev));
+    Vc += fix_e(warp_sum_d((double)vc));
+    Vv += fix_e(warp_sum_d((double)vv));
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    red_add(acc + ACC_NPAIR, npair);
+  }
+}
+
+// Exclusion correction in FP64 (src/energy.c:567-621, ewald_corr
+// src/ewald.c:371-384) into the fixed-point accumulators.
+__global__ void __launch_bounds__(128)
+k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
+           const int *__restrict__ exclFlat, const double *__restrict__ x,
+           const double *__restrict__ y, const double *__restrict__ z,
+           const double *__restrict__ q, const int *__restrict__ slotOf,
+           long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  long long ecorr = 0, vcorr = 0;
+  if (i < n) {
+    const int e = exclStart[i + 1];
+    const int si = slotOf[i];
+    for (int k = exclStart[i]; k < e; ++k) {
+      const int j = exclFlat[k];
+      if (j <= i) continue;
+      double dx = x[j] - x[i], dy = y[j] - y[i], dz = z[j] - z[i];
+      const double r2 = dist_d(b, dx, dy, dz);
+      const double r = sqrt(r2);
+      const double rt = 1. / r;
+      const double qel = p.chargeConst * q[i] * q[j];
+      const double alphar = p.alpha * r;
+      const double eC = -qel * erf(alphar) * rt;
+      double dE = 2.0 * qel * p.alpha * exp(-(alphar * alphar)) / kSqrtPi;
+      dE = -(eC + dE) * rt;
+      // every pair term goes to fixed point on its own (order independence)
+      ecorr += fix_e(eC);
+      vcorr += fix_e(dE * r);
+      const long long fxj = fix_fd(dE * dx * rt), fyj = fix_fd(dE * dy * rt),
+                      fzj = fix_fd(dE * dz * rt);
+      const int sj = slotOf[j];
+      red_add(facc + si, fxj);
+      red_add(facc + (size_t)nSlots + si, fyj);
+      red_add(facc + 2 * (size_t)nSlots + si, fzj);
+      red_add(facc + sj, -fxj);
+      red_add(facc + (size_t)nSlots + sj, -fyj);
+      red_add(facc + 2 * (size_t)nSlots + sj, -fzj);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ecorr += __shfl_xor_sync(0xffffffffu, ecorr, o);
+    vcorr += __shfl_xor_sync(0xffffffffu, vcorr, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red_add(acc + ACC_E_CORR, ecorr);
+    red_add(acc + ACC_V_CORR, vcorr);
+  }
+}
+
+// Fixed-point forces (slot order) -> FP64 forces (atom order); accumulate
+// (+=) when add != 0, as MDBas's energy routines do.
+__global__ void k_forces_out(int n, const int *__restrict__ slotOf,
+                             const long long *__restrict__ facc, int nSlots, int add,
+                             double *__restrict__ fx, double *__restrict__ fy,
+                             double *__restrict__ fz) {
+  const int a = blockIdx.x * blockDim.x + threadIdx.x;
+  if (a >= n) return;
+  const int s = slotOf[a];
+  const double inv = 1.0 / kForceScale;
+  const double vx = (double)facc[s] * inv;
+  const double vy = (double)facc[(size_t)nSlots + s] * inv;
+  const double vz = (double)facc[2 * (size_t)nSlots + s] * inv;
+  if (add) {
+    fx[a] += vx;
+    fy[a] += vy;
+    fz[a] += vz;
+  } else {
+    fx[a] = vx;
+    fy[a] = vy;
+    fz[a] = vz;
+  }
+}
+
+}  // namespace
+
+PairConstF make_pair_const(const PairParams &p) {
+  PairConstF c;
+  c.rc2 = (float)p.cutOff2;
+  c.ron2 = (float)p.cutOn2;
+  c.p_alpha = (float)(kErfcP * p.alpha);
+  c.c_ex = (float)(p.alpha * p.alpha * 1.4426950408889634);
+  c.two_a_sqrtpi = (float)(2.0 * p.alpha / kSqrtPi);
+  c.sw_a = (float)(2.0 * p.switch2);
+  c.sw_b = (float)((p.cutOff2 - 3.0 * p.cutOn2) * p.switch2);
+  c.sw_c = (float)(12.0 * p.switch2);
+  c.vdw = p.vdwSwitch;
+  return c;
+}
+
+int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s) {
+  const PairConstF c = make_pair_const(p);
+  if (w.nItems <= 0) return MDBAS_NB_OK;
+  if (p.vdwSwitch)
+    MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),
+               w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+               w.acc.as<long long>());
+  else
+    MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, w.counters.as<long long>(),
+               w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+               w.acc.as<long long>());
+  return MDBAS_NB_OK;
+}
+
+int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
+                    const int *exclStart, const int *exclFlat, const double *x, const double *y,
+                    const double *z, const double *q, cudaStream_t s) {
+  if (n <= 0) return MDBAS_NB_OK;
+  MDB_LAUNCH(k_excl_fix, grid_for(n, 128), 128, 0, s, n, b, p, exclStart, exclFlat, x, y, z, q,
+             w.slotOf.as<int>(), w.facc.as<long long>(), w.nSlots, w.acc.as<long long>());
+  return MDBAS_NB_OK;
+}
+
+int forces_out_launch(ClusterWork &w, int n, int add, double *fx, double *fy, double *fz,
+                      cudaStream_t s) {
+  if (n <= 0) return MDBAS_NB_OK;
+  MDB_LAUNCH(k_forces_out, grid_for(n, 256), 256, 0, s, n, w.slotOf.as<int>(),
+             w.facc.as<long long>(), w.nSlots, add, fx, fy, fz);
+  return MDBAS_NB_OK;
+}
+
+}  // namespace mdbas

@@ -1,0 +1,28 @@
+// pair_fp32.cuh -- mixed-precision cluster-pair kernel interface.
+#pragma once
+
+#include "cluster.cuh"
+
+namespace mdbas {
+
+// FP32 constants of the pair kernel, folded from PairParams.
+struct PairConstF {
+  float rc2, ron2;
+  float p_alpha;       // erfc fit p * alpha
+  float c_ex;          // alpha^2 * log2(e), for exp(-(alpha r)^2) = 2^(-c_ex r^2)
+  float two_a_sqrtpi;  // 2 alpha / sqrt(pi)
+  float sw_a, sw_b, sw_c;  // switch: S = (rc2-r2)^2 (sw_a r2 + sw_b), dS = sw_c r2 (rc2-r2)(ron2-r2)
+  int vdw;
+};
+
+PairConstF make_pair_const(const PairParams &p);
+// The pair kernel over all work items (grid-stride, item count read on the
+// device, so the launch needs no host synchronisation).
+int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s);
+int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
+                    const int *exclStart, const int *exclFlat, const double *x, const double *y,
+                    const double *z, const double *q, cudaStream_t s);
+int forces_out_launch(ClusterWork &w, int n, int add, double *fx, double *fy, double *fz,
+                      cudaStream_t s);
+
+}  // namespace mdbas

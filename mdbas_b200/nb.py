@@ -1,0 +1,383 @@
+"""Python front of libmdbas_nb.so (ctypes over the C ABI of include/mdbas_nb.h).
+
+* ``lib()`` loads the in-tree library and fails loudly when it is missing:
+  there is no CPU fallback.
+* ``PBC``, ``PARAM``, ``CTRL``, ``NEIGH``, ``ENERGY``, ``EWALD``, ``BOND``,
+  ``ANGLE``, ``DIHE``, ``CONSTRAINT`` mirror MDBas's structs
+  (include/global.h:175-316) for calling the drop-in routines.
+* ``make_pbc`` fills a PBC the way MDBas's init_box does (src/init.c:840-908),
+  with the same FP64 operation order, so the reciprocal vectors are
+  bit-identical to MDBas's.
+* ``Engine`` drives the device-resident engine (mdbas_nb_engine_*).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libmdbas_nb.so")
+
+CUBIC, ORBIC, TCLIN = 1, 2, 3
+NOELEC, FULL, SHIFT1, SHIFT2, SWITCH = 0, 1, 2, 3, 4
+NOVDW, VFULL, VSWITCH = 0, 1, 2
+
+STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_ALLOC",
+          5: "ERR_CAPACITY", 6: "ERR_BOX", 7: "ERR_LINKCELL", 8: "ERR_EXCL",
+          9: "ERR_UNSUPPORTED", 10: "ERR_OVERFLOW", 11: "ERR_NONFINITE", 12: "ERR_MISSING",
+          13: "ERR_STATE"}
+
+
+class MdbasNbError(RuntimeError):
+    def __init__(self, status: int, where: str, msg: str = ""):
+        self.status = status
+        text = f"{where}: {STATUS.get(status, status)}"
+        if msg:
+            text += f" ({msg})"
+        super().__init__(text)
+
+
+# ---------------------------------------------------------------------------
+# MDBas structs (include/global.h)
+# ---------------------------------------------------------------------------
+_d = C.c_double
+_i = C.c_int
+
+
+class PBC(C.Structure):
+    _fields_ = [("type", _i)] + [(n, _d) for n in (
+        "a", "a1", "a2", "a3", "b", "b1", "b2", "b3", "c", "c1", "c2", "c3",
+        "u", "u1", "u2", "u3", "v", "v1", "v2", "v3", "w", "w1", "w2", "w3",
+        "pa", "pb", "pc", "det", "vol", "vol0",
+        "stress1", "stress2", "stress3", "stress4", "stress5", "stress6",
+        "stress7", "stress8", "stress9")]
+
+
+class CTRL(C.Structure):
+    _fields_ = [(n, _i) for n in (
+        "newjob", "keyRand", "keyTraj", "keyProp", "keyForF", "keyRest", "printOut", "printProp",
+        "printTraj", "printRest", "keyMd", "mdType", "seed", "keyMinim", "keyLink", "noLink",
+        "keyConstH", "keyNb14", "keyNumForce", "keyEwald", "keyAlpha", "keyMmax", "elecType",
+        "vdwType", "integrator", "ens")]
+
+
+class PARAM(C.Structure):
+    _fields_ = [("step", _i), ("nSteps", _i), ("timeStep", _d), ("rTimeStep", _d),
+                ("nAtom", _i), ("nDegFree", _i), ("nFrozen", _i), ("nBond", _i),
+                ("nAngle", _i), ("nDihedral", _i), ("nImproper", _i), ("nUb", _i),
+                ("nConst", _i), ("maxCycle", _i), ("tolShake", _d), ("chargeConst", _d),
+                ("delr", _d), ("scal14", _d), ("cutOff", _d), ("rcutOff", _d), ("cutOff2", _d),
+                ("rcutOff2", _d), ("cutOn", _d), ("cutOn2", _d), ("switch2", _d),
+                ("temp0", _d), ("press0", _d), ("kinTemp0", _d), ("tolMinim", _d),
+                ("maxminsiz", _d), ("maxminst", _d)]
+
+
+class BOND(C.Structure):
+    _fields_ = [("type", _i), ("a", _i), ("b", _i), ("k", _d), ("r0", _d), ("beta", _d)]
+
+
+class ANGLE(C.Structure):
+    _fields_ = [("type", _i), ("a", _i), ("b", _i), ("c", _i), ("k", _d), ("theta0", _d)]
+
+
+class DIHE(C.Structure):
+    _fields_ = [("type", _i), ("order", _i), ("a", _i), ("b", _i), ("c", _i), ("d", _i),
+                ("k", _d), ("phi0", _d), ("mult", _d)]
+
+
+class NEIGH(C.Structure):
+    _fields_ = [(n, _i) for n in ("update", "linkRatio", "nCells", "sizeList", "nPair14")]
+
+
+class ENERGY(C.Structure):
+    _fields_ = [(n, _d) for n in (
+        "tot", "pot", "kin", "elec", "vdw", "bond", "ang", "ub", "dihe", "impr", "conint",
+        "consv", "virelec", "virvdw", "virbond", "virub", "virshake", "virpot", "virtot")]
+
+
+class CONSTRAINT(C.Structure):
+    _fields_ = [("a", _i), ("b", _i), ("rc2", _d)]
+
+
+class EWALD(C.Structure):
+    _fields_ = [("nbsp", _i), ("mmax", _i), ("m1max", _i), ("m2max", _i), ("m3max", _i),
+                ("prec", _d), ("tol", _d), ("tol1", _d), ("alpha", _d)]
+
+
+class EngineConfig(C.Structure):
+    _fields_ = [("nAtom", _i), ("device", _i), ("cutOff", _d), ("cutOn", _d), ("delr", _d),
+                ("alpha", _d), ("chargeConst", _d), ("vdwSwitch", _i), ("precision", _i),
+                ("linkRatio", _i), ("noLink", _i)]
+
+
+class Energies(C.Structure):
+    _fields_ = [(n, _d) for n in ("elec_direct", "elec_corr", "elec_self", "vdw", "vir_direct",
+                                  "vir_corr", "vir_vdw", "n_pairs")]
+
+
+def make_pbc(cell, box_type: int = CUBIC) -> PBC:
+    """init_box (src/init.c:840-908) with MDBas's FP64 operation order."""
+    a1, a2, a3, b1, b2, b3, c1, c2, c3 = (float(v) for v in cell)
+    p = PBC()
+    p.type = box_type
+    p.a1, p.a2, p.a3, p.b1, p.b2, p.b3, p.c1, p.c2, p.c3 = a1, a2, a3, b1, b2, b3, c1, c2, c3
+    p.a = math.sqrt(a1 * a1 + a2 * a2 + a3 * a3)
+    p.b = math.sqrt(b1 * b1 + b2 * b2 + b3 * b3)
+    p.c = math.sqrt(c1 * c1 + c2 * c2 + c3 * c3)
+    u1 = b2 * c3 - c2 * b3
+    u2 = c1 * b3 - b1 * c3
+    u3 = b1 * c2 - c1 * b2
+    v1 = c2 * a3 - a2 * c3
+    v2 = a1 * c3 - c1 * a3
+    v3 = c1 * a2 - a1 * c2
+    w1 = a2 * b3 - b2 * a3
+    w2 = b1 * a3 - a1 * b3
+    w3 = a1 * b2 - b1 * a2
+    det = a1 * u1 + a2 * u2 + a3 * u3
+    p.det = det
+    p.vol = abs(det)
+    p.vol0 = p.vol
+    p.pa = p.vol / math.sqrt(u1 * u1 + u2 * u2 + u3 * u3)
+    p.pb = p.vol / math.sqrt(v1 * v1 + v2 * v2 + v3 * v3)
+    p.pc = p.vol / math.sqrt(w1 * w1 + w2 * w2 + w3 * w3)
+    p.u, p.v, p.w = 1.0 / p.pa, 1.0 / p.pb, 1.0 / p.pc
+    if abs(det) > 0.0:
+        u1, u2, u3 = u1 / det, u2 / det, u3 / det
+        v1, v2, v3 = v1 / det, v2 / det, v3 / det
+        w1, w2, w3 = w1 / det, w2 / det, w3 / det
+    else:
+        u1 = u2 = u3 = v1 = v2 = v3 = w1 = w2 = w3 = 0.0
+    p.u1, p.u2, p.u3, p.v1, p.v2, p.v3, p.w1, p.w2, p.w3 = u1, u2, u3, v1, v2, v3, w1, w2, w3
+    return p
+
+
+def make_param(n_atom: int, cutOff=12.0, cutOn=10.0, delr=2.0, chargeConst=None,
+               scal14=1.0) -> PARAM:
+    """PARAM with the derived cut-off terms of read_SIMU (src/io.c:714-723)."""
+    from .systems import CHARGE_CONST
+    p = PARAM()
+    p.nAtom = n_atom
+    p.cutOff, p.cutOn, p.delr = cutOff, cutOn, delr
+    p.chargeConst = CHARGE_CONST if chargeConst is None else chargeConst
+    p.scal14 = scal14
+    p.rcutOff = 1.0 / cutOff
+    p.cutOff2 = cutOff * cutOff
+    p.rcutOff2 = 1.0 / p.cutOff2
+    p.cutOn2 = cutOn * cutOn
+    d = p.cutOff2 - p.cutOn2
+    p.switch2 = 1.0 / (d * d * d)
+    return p
+
+
+# ---------------------------------------------------------------------------
+# Library loading
+# ---------------------------------------------------------------------------
+_LIB = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def lib():
+    """The CUDA library.  Raises when it is not built: no fallback exists."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing; run mdbas_b200.build.build() first")
+    L = C.CDLL(LIB_PATH)
+    L.mdbas_nb_status_string.restype = C.c_char_p
+    L.mdbas_nb_status_string.argtypes = [C.c_int]
+    L.mdbas_nb_last_message.restype = C.c_char_p
+    L.mdbas_nb_engine_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(EngineConfig),
+                                         C.POINTER(PBC)]
+    for name in ("destroy", "build", "refresh", "compute"):
+        getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p]
+    L.mdbas_nb_engine_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+    L.mdbas_nb_engine_set_box.argtypes = [C.c_void_p, C.POINTER(PBC)]
+    L.mdbas_nb_engine_set_topology.argtypes = [C.c_void_p, _dp, _dp, _dp, _ip, _ip, _ip]
+    L.mdbas_nb_engine_set_positions.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_int]
+    L.mdbas_nb_engine_get_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_int]
+    L.mdbas_nb_engine_energies.argtypes = [C.c_void_p, C.POINTER(Energies)]
+    L.mdbas_nb_engine_list_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    L.mdbas_nb_engine_export_pairs.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_longlong,
+                                               C.POINTER(C.c_longlong)]
+    L.mdbas_nb_engine_launch_count.restype = C.c_longlong
+    L.mdbas_nb_engine_launch_count.argtypes = [C.c_void_p]
+    L.mdbas_nb_engine_set_timing.argtypes = [C.c_void_p, C.c_int]
+    L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                              C.POINTER(C.c_longlong), C.c_int]
+    _LIB = L
+    return L
+
+
+def check(st: int, where: str) -> None:
+    if st != 0:
+        msg = lib().mdbas_nb_last_message()
+        raise MdbasNbError(st, where, msg.decode() if msg else "")
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class Engine:
+    """Device-resident nonbonded engine for one system.
+
+    precision 0: plain FP64 form over MDBas's half list (built on the GPU);
+    precision 1: FP32 pair arithmetic with 64-bit fixed-point accumulation
+    over the cluster-pair list.
+    """
+
+    def __init__(self, system, precision: int = 1, device: int = 0, cutOff=12.0, cutOn=10.0,
+                 delr=2.0, alpha=0.34, chargeConst=None, vdwSwitch=1, linkRatio=1, noLink=0,
+                 frozen=None, box_type: int = CUBIC, cell=None):
+        from .systems import CHARGE_CONST
+        L = lib()
+        self.n = system.n
+        self.precision = precision
+        cfg = EngineConfig(self.n, device, cutOff, cutOn, delr, alpha,
+                           CHARGE_CONST if chargeConst is None else chargeConst, vdwSwitch,
+                           precision, linkRatio, noLink)
+        self.pbc = make_pbc(system.cell() if cell is None else cell, box_type)
+        h = C.c_void_p()
+        check(L.mdbas_nb_engine_create(C.byref(h), C.byref(cfg), C.byref(self.pbc)),
+              "engine_create")
+        self.h = h
+        start, flat = system.exclusions(symmetric=True)
+        pair = np.diff(start).astype(np.int32)
+        self._topo = [np.ascontiguousarray(a, dtype=np.float64)
+                      for a in (system.q, system.eps, system.sig)]
+        fz = None if frozen is None else np.ascontiguousarray(frozen, dtype=np.int32)
+        flat = np.ascontiguousarray(flat if len(flat) else np.zeros(1, np.int32), dtype=np.int32)
+        check(L.mdbas_nb_engine_set_topology(
+            h, *(a.ctypes.data_as(_dp) for a in self._topo),
+            None if fz is None else fz.ctypes.data_as(_ip), pair.ctypes.data_as(_ip),
+            flat.ctypes.data_as(_ip)), "engine_set_topology")
+        self.set_positions(system.x, system.y, system.z)
+
+    def set_positions(self, x, y, z):
+        self._pos = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        check(lib().mdbas_nb_engine_set_positions(self.h, *(_ptr(a) for a in self._pos), 0),
+              "engine_set_positions")
+
+    def set_positions_device(self, xp: int, yp: int, zp: int):
+        check(lib().mdbas_nb_engine_set_positions(self.h, C.c_void_p(xp), C.c_void_p(yp),
+                                                  C.c_void_p(zp), 1), "engine_set_positions")
+
+    def build(self):
+        check(lib().mdbas_nb_engine_build(self.h), "engine_build")
+
+    def refresh(self):
+        check(lib().mdbas_nb_engine_refresh(self.h), "engine_refresh")
+
+    def compute(self):
+        check(lib().mdbas_nb_engine_compute(self.h), "engine_compute")
+
+    def forces(self):
+        f = [np.zeros(self.n) for _ in range(3)]
+        check(lib().mdbas_nb_engine_get_forces(self.h, *(_ptr(a) for a in f), 0),
+              "engine_get_forces")
+        return f
+
+    def forces_device(self, xp: int, yp: int, zp: int):
+        check(lib().mdbas_nb_engine_get_forces(self.h, C.c_void_p(xp), C.c_void_p(yp),
+                                               C.c_void_p(zp), 1), "engine_get_forces")
+
+    def energies(self) -> dict:
+        e = Energies()
+        check(lib().mdbas_nb_engine_energies(self.h, C.byref(e)), "engine_energies")
+        return {k: getattr(e, k) for k, _ in Energies._fields_}
+
+    def list_stats(self):
+        out = (C.c_longlong * 4)()
+        check(lib().mdbas_nb_engine_list_stats(self.h, out), "engine_list_stats")
+        return list(out)
+
+    def export_pairs(self, r2max: float) -> np.ndarray:
+        cnt = C.c_longlong(0)
+        check(lib().mdbas_nb_engine_export_pairs(self.h, r2max, None, 0, C.byref(cnt)),
+              "engine_export_pairs")
+        buf = np.zeros(2 * max(cnt.value, 1), np.int32)
+        check(lib().mdbas_nb_engine_export_pairs(self.h, r2max, _ptr(buf), cnt.value,
+                                                 C.byref(cnt)), "engine_export_pairs")
+        return buf[:2 * cnt.value].reshape(-1, 2)
+
+    def launches(self) -> int:
+        return int(lib().mdbas_nb_engine_launch_count(self.h))
+
+    def set_timing(self, on: bool):
+        check(lib().mdbas_nb_engine_set_timing(self.h, 1 if on else 0), "engine_set_timing")
+
+    def pair_kernel_ms(self, reset: bool = True):
+        ms, cnt = C.c_double(0), C.c_longlong(0)
+        check(lib().mdbas_nb_engine_kernel_time(self.h, 0, C.byref(ms), C.byref(cnt),
+                                                1 if reset else 0), "engine_kernel_time")
+        return ms.value, cnt.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().mdbas_nb_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# Drop-in routines (MDBas prototypes) for Python callers and tests.
+# ---------------------------------------------------------------------------
+_pp = C.POINTER(C.POINTER(C.c_int))
+_ppp = C.POINTER(C.POINTER(C.POINTER(C.c_int)))
+
+
+def bind_dropin():
+    """Declare ctypes prototypes of the drop-in routines on lib()."""
+    L = lib()
+    if getattr(L, "_dropin_bound", False):
+        return L
+    P = C.POINTER
+    L.init_energy_ptrs.argtypes = [P(CTRL)]
+    L.makelist.argtypes = [P(CTRL), P(PARAM), P(PBC), P(NEIGH), P(CONSTRAINT), P(BOND), P(ANGLE),
+                           P(DIHE), P(DIHE), _dp, _dp, _dp, _ip, _pp, _pp, _pp, _pp, _ppp, _pp]
+    for name in ("exclude_list", "link_cell_exclude_list"):
+        getattr(L, name).argtypes = [P(CTRL), P(PARAM), P(NEIGH), P(CONSTRAINT), P(BOND),
+                                     P(ANGLE), P(DIHE), P(DIHE), _pp, _ppp, _pp]
+    L.mdbas_nb_verlet_list_status.argtypes = [P(PARAM), P(PBC), P(NEIGH), _dp, _dp, _dp, _ip,
+                                              _pp, _pp, _pp, P(_ip), _ip, C.c_int]
+    L.mdbas_nb_link_cell_list_status.argtypes = L.mdbas_nb_verlet_list_status.argtypes
+    L.energy.argtypes = [P(CTRL), P(PARAM), P(ENERGY), P(EWALD), P(PBC), P(NEIGH), P(BOND),
+                         P(BOND), P(ANGLE), P(DIHE), P(DIHE), _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                         _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip, _ip, _ip, _ip, P(_ip), _ip]
+    L.mdbas_nb_ewald_energy_status.argtypes = [P(CTRL), P(PARAM), P(ENERGY), P(EWALD), P(PBC),
+                                               _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _dp, _ip,
+                                               _ip, _ip, P(_ip), _ip]
+    L.nonbond_energy.argtypes = [P(PARAM), P(ENERGY), P(PBC), _dp, _dp, _dp, _dp, _dp, _dp, _dp,
+                                 _dp, _dp, _ip, _ip, _ip]
+    L.ewald14_energy.argtypes = [P(PARAM), P(ENERGY), P(EWALD), P(PBC), P(NEIGH), _dp, _dp, _dp,
+                                 _dp, _dp, _dp, _dp, _dp, _dp, _ip]
+    L.nonbond14_energy.argtypes = [P(PARAM), P(ENERGY), P(PBC), P(NEIGH), _dp, _dp, _dp, _dp,
+                                   _dp, _dp, _dp, _dp, _dp, _ip]
+    L.mdbas_nb_plugin_init.argtypes = [C.c_int, _dp, _dp, _dp, _ip, P(_ip), C.c_double, C.c_int]
+    L.mdbas_nb_user_energy.restype = C.c_double
+    L.mdbas_nb_user_energy.argtypes = [P(PARAM), P(PBC), _dp, _dp, _dp, _dp, _dp, _dp, _ip, _ip,
+                                       _ip, _ip]
+    L.mdbas_nb_plugin_last_energy.argtypes = [_dp]
+    L.mdbas_nb_set_mode.argtypes = [C.c_int]
+    L._dropin_bound = True
+    return L
+
+
+def as_dp(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def as_ip(a: np.ndarray):
+    return a.ctypes.data_as(_ip)

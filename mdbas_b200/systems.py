@@ -1,0 +1,250 @@
+"""Seeded synthetic systems for the nonbonded hot path.
+
+There is no public benchmark suite for this path; every workload is
+generated here from a seed, in MDBas's conventions:
+
+* positions in Angstrom, box centred on the origin (MDBas's image_update
+  wraps into [-L/2, L/2), src/utils.c:162-218);
+* per-atom LJ parameters as read_FORF leaves them: ``eps_i = sqrt(eps *
+  418.4)`` (src/io.c:1174) and ``sig_i`` = half the LJ sigma (the CHARMM
+  Rmin/2 convention of tools/prepare.c:1999-2000), so that MDBas's
+  ``veps = eps_i*eps_j`` and ``vsig = sig_i+sig_j`` (src/energy.c:505-506)
+  are Lorentz-Berthelot combinations;
+* topology as FORF bonds and angles, from which MDBas's exclusion builders
+  (src/list.c:108, :1125) derive the excluded pairs.
+
+Water model (all water workloads): rigid 3-site water, O -0.834 e / H
++0.417 e, LJ on O only (eps 0.1521 kcal/mol, sigma 3.1507 A), O-H 0.9572 A,
+H-O-H 104.52 deg.  Molecules: oxygen on the sites of an n^3 lattice
+(n = ceil(cbrt(M)), spacing L/n, first M sites in i, j, k order), each
+jittered by a seeded uniform +-0.5 A per axis, with a seeded uniform random
+orientation.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KCAL_TO_IU = 418.4                 # include/global.h:41
+CHARGE_CONST = 332.0716 * KCAL_TO_IU  # CHARMM, src/init.c:102-103
+RBOLTZ_IU = 0.83144621             # include/global.h:49
+
+WATER_Q = (-0.834, 0.417, 0.417)
+WATER_EPS_KCAL = 0.1521
+WATER_SIGMA = 3.1507
+WATER_ROH = 0.9572
+WATER_THETA = math.radians(104.52)
+WATER_MASS = (15.9994, 1.008, 1.008)
+WATER_DENSITY = 0.0334             # molecules / A^3
+
+
+@dataclass
+class System:
+    """One periodic system in MDBas's per-atom layout (FP64, original order)."""
+
+    name: str
+    box: float                      # cubic edge (A)
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    q: np.ndarray
+    eps: np.ndarray                 # sqrt(eps_kcal * 418.4)
+    sig: np.ndarray                 # sigma / 2
+    mass: np.ndarray
+    bonds: np.ndarray               # (nb, 2) int32
+    angles: np.ndarray              # (na, 3) int32
+    vx: np.ndarray | None = None
+    vy: np.ndarray | None = None
+    vz: np.ndarray | None = None
+    types: np.ndarray | None = None
+    type_eps_kcal: np.ndarray | None = None
+    type_sigma: np.ndarray | None = None
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self) -> int:
+        return int(self.x.shape[0])
+
+    def cell(self) -> np.ndarray:
+        """The three box rows a, b, c as MDBas's CONF holds them."""
+        return np.array([self.box, 0, 0, 0, self.box, 0, 0, 0, self.box], dtype=np.float64)
+
+    def exclusions(self, symmetric: bool = True):
+        """Excluded pairs from bonds + angles as CSR (start[n+1], flat).
+
+        Symmetric rows are what link_cell_exclude_list builds; half rows (j>i)
+        what exclude_list builds.  Entries keep bond-then-angle order."""
+        n = self.n
+        rows = [[] for _ in range(n)]
+
+        def add(a, b):
+            if b not in rows[a]:
+                rows[a].append(b)
+
+        pairs = [tuple(b) for b in self.bonds.tolist()]
+        for a, b, c in self.angles.tolist():
+            pairs += [(a, b), (a, c), (b, c)]
+        for a, b in pairs:
+            if symmetric:
+                add(a, b)
+                add(b, a)
+            else:
+                add(min(a, b), max(a, b))
+        start = np.zeros(n + 1, dtype=np.int32)
+        start[1:] = np.cumsum([len(r) for r in rows])
+        flat = np.array([v for r in rows for v in r], dtype=np.int32)
+        return start, flat
+
+
+def _random_rotations(rng: np.random.Generator, m: int) -> np.ndarray:
+    """m uniform random rotation matrices from uniform unit quaternions."""
+    u1, u2, u3 = rng.random((3, m))
+    a = np.sqrt(1.0 - u1)
+    b = np.sqrt(u1)
+    qw = a * np.sin(2 * np.pi * u2)
+    qx = a * np.cos(2 * np.pi * u2)
+    qy = b * np.sin(2 * np.pi * u3)
+    qz = b * np.cos(2 * np.pi * u3)
+    r = np.empty((m, 3, 3))
+    r[:, 0, 0] = 1 - 2 * (qy * qy + qz * qz)
+    r[:, 0, 1] = 2 * (qx * qy - qz * qw)
+    r[:, 0, 2] = 2 * (qx * qz + qy * qw)
+    r[:, 1, 0] = 2 * (qx * qy + qz * qw)
+    r[:, 1, 1] = 1 - 2 * (qx * qx + qz * qz)
+    r[:, 1, 2] = 2 * (qy * qz - qx * qw)
+    r[:, 2, 0] = 2 * (qx * qz - qy * qw)
+    r[:, 2, 1] = 2 * (qy * qz + qx * qw)
+    r[:, 2, 2] = 1 - 2 * (qx * qx + qy * qy)
+    return r
+
+
+def _wrap(v: np.ndarray, box: float) -> np.ndarray:
+    return v - box * np.floor(v / box + 0.5)
+
+
+def water_box(n_molecules: int, box: float, seed: int = 1, jitter: float = 0.5,
+              temperature: float | None = None, name: str | None = None) -> System:
+    """Lattice-plus-jitter rigid water box (atoms O, H1, H2 per molecule)."""
+    rng = np.random.default_rng(seed)
+    m = int(n_molecules)
+    nl = int(math.ceil(round(m ** (1.0 / 3.0), 9)))
+    while nl ** 3 < m:
+        nl += 1
+    spacing = box / nl
+    idx = np.arange(m)
+    i = idx % nl
+    j = (idx // nl) % nl
+    k = idx // (nl * nl)
+    centres = np.stack([(i + 0.5) * spacing, (j + 0.5) * spacing, (k + 0.5) * spacing], 1)
+    centres -= 0.5 * box
+    centres += rng.uniform(-jitter, jitter, size=(m, 3))
+    # Body frame: O at origin, H in the xy plane symmetric about x.
+    half = 0.5 * WATER_THETA
+    body = np.array([[0.0, 0.0, 0.0],
+                     [WATER_ROH * math.cos(half), WATER_ROH * math.sin(half), 0.0],
+                     [WATER_ROH * math.cos(half), -WATER_ROH * math.sin(half), 0.0]])
+    rot = _random_rotations(rng, m)
+    pos = centres[:, None, :] + np.einsum('mij,aj->mai', rot, body)
+    pos = _wrap(pos.reshape(-1, 3), box)
+    n = 3 * m
+    q = np.tile(np.array(WATER_Q), m)
+    eps = np.tile(np.array([math.sqrt(WATER_EPS_KCAL * KCAL_TO_IU), 0.0, 0.0]), m)
+    sig = np.tile(np.array([0.5 * WATER_SIGMA, 0.0, 0.0]), m)
+    mass = np.tile(np.array(WATER_MASS), m)
+    base = 3 * np.arange(m, dtype=np.int32)
+    bonds = np.concatenate([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1)])
+    bonds = bonds.reshape(2, m, 2).transpose(1, 0, 2).reshape(-1, 2).astype(np.int32)
+    angles = np.stack([base + 1, base, base + 2], 1).astype(np.int32)
+    sysm = System(name or f"water{n}", float(box), pos[:, 0].copy(), pos[:, 1].copy(),
+                  pos[:, 2].copy(), q, eps, sig, mass, bonds, angles,
+                  meta={"molecules": m, "seed": seed})
+    if temperature is not None:
+        sd = np.sqrt(RBOLTZ_IU * temperature / mass)
+        v = rng.normal(size=(n, 3)) * sd[:, None]
+        sysm.vx, sysm.vy, sysm.vz = v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy()
+    return sysm
+
+
+def water_box_for_atoms(n_atoms: int, seed: int = 1, density: float = WATER_DENSITY,
+                        **kw) -> System:
+    """Water box holding n_atoms (a multiple of 3) at the given density."""
+    m = n_atoms // 3
+    box = (m / density) ** (1.0 / 3.0)
+    return water_box(m, box, seed=seed, **kw)
+
+
+def lj_fluid(n: int = 12000, box: float = 50.0, seed: int = 1, n_types: int = 4,
+             min_sep: float = 2.0, qmax: float = 0.8, max_iter: int = 2000) -> System:
+    """Charged LJ fluid: seeded uniform positions relaxed to a minimum
+    separation, per-atom charges U[-qmax, qmax] shifted to net zero, per-type
+    eps U[0.05, 0.3] kcal/mol and sigma U[2.8, 3.8] A, no exclusions.
+
+    12,000 spheres of diameter 2 A in a 50 A cube fill 40% of the volume,
+    above the ~38% jamming limit of random sequential addition, so rejection
+    sampling cannot reach that density.  Positions are therefore drawn
+    uniformly and then every pair closer than 1.04 * ``min_sep`` is pushed
+    apart along its axis (each atom by half the shortfall) until no pair is
+    closer than ``min_sep``."""
+    from scipy.spatial import cKDTree
+
+    rng = np.random.default_rng(seed)
+    pos = rng.uniform(0.0, box, size=(n, 3))
+    target = 1.04 * min_sep
+    for _ in range(max_iter):
+        tree = cKDTree(pos, boxsize=box)
+        pairs = tree.query_pairs(target, output_type='ndarray')
+        d = pos[pairs[:, 1]] - pos[pairs[:, 0]]
+        d -= box * np.round(d / box)
+        r = np.sqrt((d * d).sum(1))
+        if len(r) == 0 or r.min() >= min_sep:
+            break
+        r = np.maximum(r, 1e-6)
+        push = (0.5 * (target - r) / r)[:, None] * d
+        delta = np.zeros_like(pos)
+        np.add.at(delta, pairs[:, 0], -push)
+        np.add.at(delta, pairs[:, 1], push)
+        pos = np.mod(pos + delta, box)
+    else:
+        raise RuntimeError("lj_fluid: overlap removal did not converge")
+    pos -= 0.5 * box
+    types = rng.integers(0, n_types, size=n).astype(np.int32)
+    t_eps = rng.uniform(0.05, 0.3, size=n_types)
+    t_sig = rng.uniform(2.8, 3.8, size=n_types)
+    q = rng.uniform(-qmax, qmax, size=n)
+    q -= q.mean()
+    eps = np.sqrt(t_eps[types] * KCAL_TO_IU)
+    sig = 0.5 * t_sig[types]
+    empty2 = np.zeros((0, 2), dtype=np.int32)
+    empty3 = np.zeros((0, 3), dtype=np.int32)
+    return System(f"ljfluid{n}", float(box), pos[:, 0].copy(), pos[:, 1].copy(),
+                  pos[:, 2].copy(), q, eps, sig, np.full(n, 39.948), empty2, empty3,
+                  types=types, type_eps_kcal=t_eps, type_sigma=t_sig,
+                  meta={"seed": seed})
+
+
+def replica_sizes(count: int = 64, lo: int = 1500, hi: int = 30000, seed: int = 1) -> list[int]:
+    """Atom counts drawn log-uniform in [lo, hi], rounded to multiples of 3."""
+    rng = np.random.default_rng(seed)
+    v = np.exp(rng.uniform(math.log(lo), math.log(hi), size=count))
+    return [int(max(lo, min(hi, 3 * round(x / 3)))) for x in v]
+
+
+# Named workloads (sizes of the reference's headline configurations).
+def config_small(seed: int = 1) -> System:
+    """3,000-atom water (1,000 molecules) in a 31.0 A box."""
+    return water_box(1000, 31.0, seed=seed, name="water3000")
+
+
+def config_96k(seed: int = 1, temperature: float | None = 300.0) -> System:
+    """96,000-atom water (32,000 molecules) in a 98.6 A box, MB velocities."""
+    return water_box(32000, 98.6, seed=seed, temperature=temperature, name="water96000")
+
+
+def config_1m(seed: int = 1) -> System:
+    """999,999-atom water (333,333 molecules) in a 215 A box."""
+    return water_box(333333, 215.0, seed=seed, name="water999999")
+
+
+POTENTIAL = dict(cutOff=12.0, cutOn=10.0, delr=2.0, alpha=0.34, chargeConst=CHARGE_CONST)

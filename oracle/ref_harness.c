@@ -1,0 +1,297 @@
+/*
+ * ref_harness.c -- flat C entry points around the UNMODIFIED MDBas sources.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is compiled by oracle/Makefile together
+ * with MDBas's own src/*.c (read in place, never copied) into
+ * oracle/_ref/libmdbas_ref.so.  Only tests/, the smoke check and the CPU
+ * baseline leg of bench.py load that library, always as the checker.
+ *
+ * The harness replaces MDBas's driver (src/mdbas.c:51 main) for the hot path:
+ *   - it fills the CTRL/PARAM/PBC/NEIGH/EWALD structs the way read_SIMU
+ *     (src/io.c:47-111 defaults, src/io.c:714-723 derived cut-off terms) and
+ *     init_system (src/init.c:102-103 CHARMM charge constant, src/init.c:840
+ *     init_box) leave them, without reading SIMU/CONF/FORF files;
+ *   - it calls the reference's own makelist (src/list.c:29), which selects the
+ *     link-cell or O(N^2) builder and the matching exclusion builder;
+ *   - it calls the reference's own energy() (src/energy.c:103) with
+ *     keyEwald=3, so ewald_energy (src/energy.c:450) skips both k-space
+ *     branches (src/energy.c:469-472) and returns exactly the real-space direct
+ *     term, the exclusion correction and the switched LJ term.
+ * The FP64 Ewald self term lives inside ewald_rec (src/ewald.c:165-171), which
+ * keyEwald=3 skips; ref_self_energy restates that one formula.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <time.h>
+
+#include "global.h"
+#include "energy.h"
+#include "list.h"
+#include "utils.h"
+#include "init.h"
+#include "spme.h"
+
+/* MDBas's driver owns this global (src/mdbas.c:43). */
+FILE *outFile = NULL;
+
+/* src/spme.c needs FFTW3, which is absent here; energy.c references these
+ * three symbols but keyEwald=3 never reaches them. */
+void init_spme(CTRL *ctrl, PARAM *param, EWALD *ewald, PBC *box)
+{ (void)ctrl; (void)param; (void)ewald; (void)box; }
+void spme_free(PARAM *param) { (void)param; }
+double spme_energy(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
+                   const double z[], double fx[], double fy[], double fz[], const double q[],
+                   double stress[6], double *virEwaldRec)
+{
+  (void)param; (void)ewald; (void)box; (void)x; (void)y; (void)z; (void)fx; (void)fy;
+  (void)fz; (void)q; (void)stress; (void)virEwaldRec;
+  return 0.0;
+}
+
+typedef struct {
+  CTRL ctrl;
+  PARAM param;
+  PBC box;
+  NEIGH neigh;
+  EWALD ewald;
+  ENERGY ener;
+  BOND *bond;
+  ANGLE *angle;
+  CONSTRAINT *constList;
+  DIHE *dihe, *impr;
+  double *x, *y, *z, *q, *eps, *sig, *fx, *fy, *fz, *vx, *vy, *vz;
+  int *frozen;
+  int *neighList, *neighPair, *neighOrder, *neighList14, **exclList, *exclPair;
+  int listBuilt;
+} RefSys;
+
+static double *dup_d(const double *src, int n)
+{
+  double *p = (double *)calloc((size_t)(n > 0 ? n : 1), sizeof(double));
+  if (src) memcpy(p, src, (size_t)n * sizeof(double));
+  return p;
+}
+
+/*
+ * Create a system.  cell[9] holds the box rows a1 a2 a3 b1 b2 b3 c1 c2 c3
+ * (the CONF box lines); boxType follows enum BOX_TYPE (global.h:75-80).
+ * eps/sig are the per-atom FORF values after read_FORF's conversion
+ * (eps_i = sqrt(eps*418.4), src/io.c:1174; sig_i = FORF sigma, src/io.c:1175).
+ * bonds: 2*nBond atom indices; angles: 3*nAngle atom indices.
+ */
+RefSys *ref_create(int nAtom, int boxType, const double cell[9], double cutOff, double cutOn,
+                   double delr, int linkRatio, int noLink, double alpha,
+                   const double *x, const double *y, const double *z, const double *q,
+                   const double *eps, const double *sig, const int *frozen,
+                   int nBond, const int *bonds, int nAngle, const int *angles)
+{
+  RefSys *s = (RefSys *)calloc(1, sizeof(RefSys));
+  int i;
+  if (outFile == NULL) outFile = stderr;
+
+  s->ctrl.newjob = 1;
+  s->ctrl.mdType = 1;
+  s->ctrl.keyEwald = 3;
+  s->ctrl.noLink = noLink;
+  s->ctrl.elecType = FULL;
+  s->ctrl.vdwType = VSWITCH;
+
+  s->param.nAtom = nAtom;
+  s->param.nBond = nBond;
+  s->param.nAngle = nAngle;
+  s->param.cutOff = cutOff;
+  s->param.cutOn = cutOn;
+  s->param.delr = delr;
+  s->param.scal14 = 1.0;
+  s->param.chargeConst = chgcharmm * kcaltoiu;          /* src/init.c:102-103 */
+  s->param.rcutOff = 1. / s->param.cutOff;               /* src/io.c:714-721 */
+  s->param.cutOff2 = X2(s->param.cutOff);
+  s->param.rcutOff2 = 1. / s->param.cutOff2;
+  s->param.cutOn2 = X2(s->param.cutOn);
+  s->param.switch2 = 1. / X3(s->param.cutOff2 - s->param.cutOn2);
+
+  s->box.type = (enum BOX_TYPE)boxType;
+  s->box.a1 = cell[0]; s->box.a2 = cell[1]; s->box.a3 = cell[2];
+  s->box.b1 = cell[3]; s->box.b2 = cell[4]; s->box.b3 = cell[5];
+  s->box.c1 = cell[6]; s->box.c2 = cell[7]; s->box.c3 = cell[8];
+  init_box(&s->box);
+
+  s->neigh.update = 1;
+  s->neigh.linkRatio = linkRatio;
+
+  s->ewald.alpha = alpha;
+
+  s->x = dup_d(x, nAtom); s->y = dup_d(y, nAtom); s->z = dup_d(z, nAtom);
+  s->q = dup_d(q, nAtom); s->eps = dup_d(eps, nAtom); s->sig = dup_d(sig, nAtom);
+  s->fx = dup_d(NULL, nAtom); s->fy = dup_d(NULL, nAtom); s->fz = dup_d(NULL, nAtom);
+  s->vx = dup_d(NULL, nAtom); s->vy = dup_d(NULL, nAtom); s->vz = dup_d(NULL, nAtom);
+  s->frozen = (int *)calloc((size_t)nAtom, sizeof(int));
+  if (frozen) memcpy(s->frozen, frozen, (size_t)nAtom * sizeof(int));
+
+  s->bond = (BOND *)calloc((size_t)(nBond > 0 ? nBond : 1), sizeof(BOND));
+  for (i = 0; i < nBond; i++) { s->bond[i].a = bonds[2 * i]; s->bond[i].b = bonds[2 * i + 1]; }
+  s->angle = (ANGLE *)calloc((size_t)(nAngle > 0 ? nAngle : 1), sizeof(ANGLE));
+  for (i = 0; i < nAngle; i++) {
+    s->angle[i].a = angles[3 * i]; s->angle[i].b = angles[3 * i + 1]; s->angle[i].c = angles[3 * i + 2];
+  }
+  s->constList = (CONSTRAINT *)calloc(1, sizeof(CONSTRAINT));
+  s->dihe = (DIHE *)calloc(1, sizeof(DIHE));
+  s->impr = (DIHE *)calloc(1, sizeof(DIHE));
+  return s;
+}
+
+/* Box quantities after init_box, in PBC field order a..vol (for host checks). */
+void ref_box(const RefSys *s, double out[30])
+{
+  const PBC *b = &s->box;
+  double v[30] = {b->a, b->a1, b->a2, b->a3, b->b, b->b1, b->b2, b->b3, b->c, b->c1, b->c2, b->c3,
+                  b->u, b->u1, b->u2, b->u3, b->v, b->v1, b->v2, b->v3, b->w, b->w1, b->w2, b->w3,
+                  b->pa, b->pb, b->pc, b->det, b->vol, b->vol0};
+  memcpy(out, v, sizeof(v));
+}
+
+/* First list build through makelist(newjob=1) (src/list.c:36-85). */
+int ref_makelist(RefSys *s)
+{
+  s->ctrl.newjob = 1;
+  makelist(&s->ctrl, &s->param, &s->box, &s->neigh, s->constList, s->bond, s->angle, s->dihe,
+           s->impr, s->x, s->y, s->z, s->frozen, &s->neighList, &s->neighPair, &s->neighOrder,
+           &s->neighList14, &s->exclList, &s->exclPair);
+  s->listBuilt = 1;
+  return s->ctrl.keyLink;
+}
+
+/* Rebuild with new coordinates through makelist(newjob=0) (src/list.c:87-105). */
+void ref_update_list(RefSys *s, const double *x, const double *y, const double *z)
+{
+  if (x) memcpy(s->x, x, (size_t)s->param.nAtom * sizeof(double));
+  if (y) memcpy(s->y, y, (size_t)s->param.nAtom * sizeof(double));
+  if (z) memcpy(s->z, z, (size_t)s->param.nAtom * sizeof(double));
+  s->param.step = 0; /* step % update == 0 */
+  makelist(&s->ctrl, &s->param, &s->box, &s->neigh, s->constList, s->bond, s->angle, s->dihe,
+           s->impr, s->x, s->y, s->z, s->frozen, &s->neighList, &s->neighPair, &s->neighOrder,
+           &s->neighList14, &s->exclList, &s->exclPair);
+}
+
+int ref_key_link(const RefSys *s) { return s->ctrl.keyLink; }
+int ref_n_cells(const RefSys *s) { return s->neigh.nCells; }
+int ref_size_list(const RefSys *s) { return s->neigh.sizeList; }
+
+/* Number of list entries actually filled (sum of neighPair). */
+long ref_list_entries(const RefSys *s)
+{
+  long t = 0;
+  int i;
+  for (i = 0; i < s->param.nAtom; i++) t += s->neighPair[i];
+  return t;
+}
+
+void ref_get_list(const RefSys *s, int *neighList, int *neighPair, int *neighOrder)
+{
+  long t = ref_list_entries(s);
+  memcpy(neighList, s->neighList, (size_t)t * sizeof(int));
+  memcpy(neighPair, s->neighPair, (size_t)s->param.nAtom * sizeof(int));
+  memcpy(neighOrder, s->neighOrder, (size_t)s->param.nAtom * sizeof(int));
+}
+
+/* Exclusions as built by the reference: count per atom and flattened rows. */
+long ref_excl_entries(const RefSys *s)
+{
+  long t = 0;
+  int i;
+  for (i = 0; i < s->param.nAtom; i++) t += s->exclPair[i];
+  return t;
+}
+
+void ref_get_excl(const RefSys *s, int *exclPair, int *exclFlat)
+{
+  long o = 0;
+  int i, k;
+  memcpy(exclPair, s->exclPair, (size_t)s->param.nAtom * sizeof(int));
+  for (i = 0; i < s->param.nAtom; i++)
+    for (k = 0; k < s->exclPair[i]; k++) exclFlat[o++] = s->exclList[i][k];
+}
+
+/* Positions as the reference holds them (the link-cell build wraps them). */
+void ref_get_positions(const RefSys *s, double *x, double *y, double *z)
+{
+  memcpy(x, s->x, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(y, s->y, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(z, s->z, (size_t)s->param.nAtom * sizeof(double));
+}
+
+void ref_set_positions(RefSys *s, const double *x, const double *y, const double *z)
+{
+  memcpy(s->x, x, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(s->y, y, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(s->z, z, (size_t)s->param.nAtom * sizeof(double));
+}
+
+/*
+ * One energy() call (src/energy.c:103) on the current list.  Bonded terms are
+ * out of scope, so energy() sees nBond = nAngle = 0.
+ * out[0..5] = elec, vdw, virelec, virvdw, pot, virpot (internal units).
+ */
+void ref_energy(RefSys *s, double *fx, double *fy, double *fz, double out[6])
+{
+  PARAM p = s->param;
+  p.nBond = 0;
+  p.nAngle = 0;
+  p.nUb = 0;
+  p.nDihedral = 0;
+  p.nImproper = 0;
+  s->ctrl.keyEwald = 3;
+  init_energy_ptrs(&s->ctrl);
+  energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->bond, s->angle,
+         s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,
+         s->eps, s->sig, s->eps, s->sig, s->frozen, s->neighList, s->neighPair, s->neighOrder,
+         s->neighList14, s->exclList, s->exclPair);
+  if (fx) memcpy(fx, s->fx, (size_t)s->param.nAtom * sizeof(double));
+  if (fy) memcpy(fy, s->fy, (size_t)s->param.nAtom * sizeof(double));
+  if (fz) memcpy(fz, s->fz, (size_t)s->param.nAtom * sizeof(double));
+  out[0] = s->ener.elec;
+  out[1] = s->ener.vdw;
+  out[2] = s->ener.virelec;
+  out[3] = s->ener.virvdw;
+  out[4] = s->ener.pot;
+  out[5] = s->ener.virpot;
+}
+
+/* Ewald self energy, the formula of src/ewald.c:165-171 restated. */
+double ref_self_energy(const RefSys *s)
+{
+  double e = 0.;
+  int i;
+  for (i = 0; i < s->param.nAtom; i++) e += X2(s->q[i]);
+  return -s->param.chargeConst * s->ewald.alpha * e / SQRTPI;
+}
+
+/* Wall-clock seconds from CLOCK_MONOTONIC, for the CPU baseline. */
+double ref_now(void)
+{
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+void ref_destroy(RefSys *s)
+{
+  int i;
+  if (!s) return;
+  free(s->x); free(s->y); free(s->z); free(s->q); free(s->eps); free(s->sig);
+  free(s->fx); free(s->fy); free(s->fz); free(s->vx); free(s->vy); free(s->vz);
+  free(s->frozen); free(s->bond); free(s->angle); free(s->constList); free(s->dihe);
+  free(s->impr);
+  if (s->listBuilt) {
+    free(s->neighList); free(s->neighPair); free(s->neighOrder); free(s->neighList14);
+    if (s->exclList) {
+      int rows = s->ctrl.keyLink ? s->param.nAtom : s->param.nAtom - 1;
+      for (i = 0; i < rows; i++) free(s->exclList[i]);
+      free(s->exclList);
+    }
+    free(s->exclPair);
+  }
+  free(s);
+}

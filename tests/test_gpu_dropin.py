@@ -1,0 +1,102 @@
+"""The drop-in C ABI (MDBas prototypes) end to end on the GPU."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from mdbas_b200 import nb, systems
+from dropin_util import DropinSystem, force_rel_rms
+
+pytestmark = pytest.mark.gpu
+
+
+def _ref_energy(s, **kw):
+    if not oracle.Reference.available():
+        pytest.skip("MDBas reference library not built")
+    r = oracle.Reference(s, **kw)
+    r.makelist()
+    return r, r.energy()
+
+
+@pytest.mark.parametrize("which", ["small", "link"])
+def test_energy_dropin_fp64(gpu, which):
+    s = systems.config_small(1) if which == "small" else systems.water_box_for_atoms(18558, 3)
+    L = nb.bind_dropin()
+    L.mdbas_nb_set_mode(0)
+    d = DropinSystem(s)
+    d.makelist()
+    fx, fy, fz, e = d.energy()
+    r, (rfx, rfy, rfz, re) = _ref_energy(s)
+    assert force_rel_rms((fx, fy, fz), (rfx, rfy, rfz)) < 1e-12
+    for k in ("elec", "vdw", "virelec", "virvdw", "pot", "virpot"):
+        assert abs(e[k] - re[k]) <= 1e-12 * abs(re[k]), k
+    d.free()
+
+
+def test_energy_dropin_mixed(gpu):
+    s = systems.water_box_for_atoms(18558, 3)
+    L = nb.bind_dropin()
+    L.mdbas_nb_set_mode(1)
+    try:
+        d = DropinSystem(s)
+        d.makelist()
+        fx, fy, fz, e = d.energy()
+        # a second call reuses the cluster list (nothing moved)
+        fx2, fy2, fz2, e2 = d.energy()
+    finally:
+        L.mdbas_nb_set_mode(0)
+    r, (rfx, rfy, rfz, re) = _ref_energy(s)
+    assert force_rel_rms((fx, fy, fz), (rfx, rfy, rfz)) < 1e-5
+    assert abs(e["elec"] - re["elec"]) <= 1e-5 * abs(re["elec"])
+    assert np.array_equal(fx, fx2) and e == e2
+    d.free()
+
+
+def test_plugin_matches_ewald_energy(gpu):
+    s = systems.config_small(2)
+    L = nb.bind_dropin()
+    L.mdbas_nb_set_mode(0)
+    d = DropinSystem(s)
+    d.makelist()
+    fx, fy, fz, e = d.energy()
+    pair = np.ctypeslib.as_array(d.exclPair, (s.n,)).copy()
+    assert L.mdbas_nb_plugin_init(s.n, nb.as_dp(d.q), nb.as_dp(d.eps), nb.as_dp(d.sig),
+                                  nb.as_ip(pair), d.exclList, 0.34, 1) == 0
+    px, py, pz = np.zeros(s.n), np.zeros(s.n), np.zeros(s.n)
+    etot = L.mdbas_nb_user_energy(C.byref(d.param), C.byref(d.box), nb.as_dp(d.x),
+                                  nb.as_dp(d.y), nb.as_dp(d.z), nb.as_dp(px), nb.as_dp(py),
+                                  nb.as_dp(pz), d.neighList, d.neighPair, d.neighOrder,
+                                  d.neighList14)
+    assert force_rel_rms((px, py, pz), (fx, fy, fz)) < 1e-13
+    assert abs(etot - (e["elec"] + e["vdw"])) <= 1e-12 * abs(e["elec"])
+    out = np.zeros(4)
+    assert L.mdbas_nb_plugin_last_energy(nb.as_dp(out)) == 0
+    assert abs(out[2] - e["virelec"]) <= 1e-12 * abs(e["virelec"])
+    d.free()
+
+
+def test_status_forms_report_instead_of_exit(gpu):
+    # a 31 A box has 2 link cells per side: the link-cell builder must refuse
+    s = systems.config_small(1)
+    L = nb.bind_dropin()
+    d = DropinSystem(s)
+    lst = C.POINTER(C.c_int)()
+    pair = C.POINTER(C.c_int)()
+    order = C.POINTER(C.c_int)()
+    excl = (C.POINTER(C.c_int) * s.n)()
+    ep = np.zeros(s.n, np.int32)
+    st = L.mdbas_nb_link_cell_list_status(C.byref(d.param), C.byref(d.box), C.byref(d.neigh),
+                                          nb.as_dp(d.x), nb.as_dp(d.y), nb.as_dp(d.z),
+                                          nb.as_ip(d.frozen), C.byref(lst), C.byref(pair),
+                                          C.byref(order), excl, nb.as_ip(ep), 0)
+    assert st == 7  # MDBAS_NB_ERR_LINKCELL (MDBas LNKCELL_NCELLS_ERROR)
+    # non-finite coordinates are rejected by the engine, not computed
+    s2 = systems.config_small(1)
+    s2.x = s2.x.copy()
+    s2.x[5] = np.nan
+    eng = nb.Engine(s2, precision=1)
+    with pytest.raises(nb.MdbasNbError) as ei:
+        eng.build()
+    assert ei.value.status == 11
+    eng.close()

@@ -1,0 +1,170 @@
+"""GPU force/energy parity.
+
+* plain FP64 form: against MDBas's own energy() (relative 1e-12: only CUDA's
+  erfc/exp and the FP64 atomic order differ from the CPU build);
+* FP32 pair arithmetic + fixed-point accumulation: against the FP64
+  restatement, per-atom force RMS relative error <= 1e-5 and energy
+  relative error <= 1e-5; the evaluated pair set equals MDBas's.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from mdbas_b200 import nb, systems
+from dropin_util import force_rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+MIXED_FORCE_TOL = 1e-5
+MIXED_ENERGY_TOL = 1e-5
+
+
+def _oracle_fp64(s, link=None):
+    o = oracle.Oracle()
+    box = o.box(s.cell())
+    ok, _ = o.link_cell_counts(box)
+    if link is None:
+        link = ok
+    if link:
+        excl = s.exclusions(symmetric=True)
+        lst, pair, order = o.link_cell_list(box, s.x, s.y, s.z, excl)
+    else:
+        excl = s.exclusions(symmetric=False)
+        lst, pair, order = o.verlet_list(box, s.x, s.y, s.z, excl)
+    fx, fy, fz, e = o.ewald_energy(box, s, lst, pair, order, excl)
+    return (fx, fy, fz), e
+
+
+@pytest.mark.parametrize("which", ["small", "link"])
+def test_fp64_form_matches_reference(gpu, which):
+    if not oracle.Reference.available():
+        pytest.skip("MDBas reference library not built")
+    s = systems.config_small(1) if which == "small" else systems.water_box_for_atoms(18558, 3)
+    r = oracle.Reference(s)
+    r.makelist()
+    rx, ry, rz = r.positions()
+    rf = r.energy()
+    s.x, s.y, s.z = rx, ry, rz
+    eng = nb.Engine(s, precision=0)
+    eng.build()
+    eng.compute()
+    f = eng.forces()
+    e = eng.energies()
+    assert force_rel_rms(f, rf[:3]) < FP64_TOL
+    elec = e["elec_direct"] + e["elec_corr"]
+    assert abs(elec - rf[3]["elec"]) <= FP64_TOL * abs(rf[3]["elec"])
+    assert abs(e["vdw"] - rf[3]["vdw"]) <= FP64_TOL * abs(rf[3]["vdw"])
+    vir = e["vir_direct"] + e["vir_corr"]
+    assert abs(vir - rf[3]["virelec"]) <= FP64_TOL * abs(rf[3]["virelec"])
+    # MDBas sums q^2 sequentially in FP64 (its own rounding is ~1e-13 here)
+    assert abs(e["elec_self"] - r.self_energy()) <= 1e-12 * abs(r.self_energy())
+    eng.close()
+
+
+@pytest.mark.parametrize("which", ["small", "link", "ljfluid"])
+def test_mixed_form_accuracy(gpu, which):
+    if which == "small":
+        s = systems.config_small(1)
+    elif which == "link":
+        s = systems.water_box_for_atoms(18558, 3)
+    else:
+        s = systems.lj_fluid(12000, 50.0, seed=1)
+    rf, re = _oracle_fp64(s)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    eng.compute()
+    f = eng.forces()
+    e = eng.energies()
+    err = force_rel_rms(f, rf)
+    assert err < MIXED_FORCE_TOL, err
+    relec = re["e_dir"] + re["e_corr"]
+    elec = e["elec_direct"] + e["elec_corr"]
+    assert abs(elec - relec) <= MIXED_ENERGY_TOL * abs(relec)
+    assert abs(e["vdw"] - re["e_vdw"]) <= MIXED_ENERGY_TOL * max(abs(re["e_vdw"]), 1.0)
+    vir = e["vir_direct"] + e["vir_corr"] + e["vir_vdw"]
+    rvir = re["vir_dir"] + re["vir_corr"] + re["vir_vdw"]
+    assert abs(vir - rvir) <= MIXED_ENERGY_TOL * abs(rvir)
+    assert abs(e["n_pairs"] - re["n_pairs"]) <= 2
+    eng.close()
+
+
+def test_mixed_pair_set_equals_reference(gpu):
+    s = systems.water_box_for_atoms(18558, 3)
+    o = oracle.Oracle()
+    box = o.box(s.cell())
+    excl = s.exclusions(symmetric=True)
+    ref = o.pairs_within(box, s.x, s.y, s.z, excl, 144.0)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    got = eng.export_pairs(144.0)
+    a = set(map(tuple, ref.tolist()))
+    b = set(map(tuple, got.tolist()))
+    assert len(got) == len(b), "a pair was evaluated twice"
+    diff = a ^ b
+    # only pairs within FP32 rounding of the cut-off may differ
+    pos = np.stack([s.x, s.y, s.z], 1)
+    for i, j in diff:
+        d = pos[j] - pos[i]
+        d -= s.box * np.round(d / s.box)
+        assert abs(np.sqrt(d @ d) - 12.0) < 1e-4, (i, j)
+    eng.close()
+
+
+def test_mixed_deterministic_and_permutation_invariant(gpu):
+    s = systems.water_box_for_atoms(18558, 6)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    eng.compute()
+    f1 = eng.forces()
+    e1 = eng.energies()
+    eng.compute()
+    f2 = eng.forces()
+    eng.build()
+    eng.compute()
+    f3 = eng.forces()
+    e3 = eng.energies()
+    for a, b, c in zip(f1, f2, f3):
+        assert np.array_equal(a, b) and np.array_equal(a, c)
+    assert e1 == e3
+    eng.close()
+    # permute the atoms (exclusions follow): same forces bit for bit
+    perm = np.random.default_rng(11).permutation(s.n)
+    inv = np.empty_like(perm)
+    inv[perm] = np.arange(s.n)
+    sp = systems.System(s.name, s.box, s.x[perm], s.y[perm], s.z[perm], s.q[perm], s.eps[perm],
+                        s.sig[perm], s.mass[perm], inv[s.bonds].astype(np.int32),
+                        inv[s.angles].astype(np.int32))
+    engp = nb.Engine(sp, precision=1)
+    engp.build()
+    engp.compute()
+    fp = engp.forces()
+    ep = engp.energies()
+    for a, b in zip(f1, fp):
+        assert np.array_equal(a[perm], b)
+    assert ep == e1
+    engp.close()
+
+
+def test_refresh_between_builds(gpu):
+    # moving atoms by less than half the skin and refreshing must give the
+    # same forces as a full rebuild at the new positions
+    s = systems.water_box_for_atoms(18558, 8)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    rng = np.random.default_rng(2)
+    x = s.x + rng.uniform(-0.4, 0.4, s.n)
+    y = s.y + rng.uniform(-0.4, 0.4, s.n)
+    z = s.z + rng.uniform(-0.4, 0.4, s.n)
+    eng.set_positions(x, y, z)
+    eng.refresh()
+    eng.compute()
+    f_ref = eng.forces()
+    e_ref = eng.energies()
+    eng.build()
+    eng.compute()
+    f_new = eng.forces()
+    e_new = eng.energies()
+    assert force_rel_rms(f_ref, f_new) < 2 * MIXED_FORCE_TOL
+    assert e_ref["n_pairs"] == e_new["n_pairs"]
+    eng.close()
