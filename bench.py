@@ -1,0 +1,448 @@
+"""Benchmark of the real-space nonbonded hot path on B200.
+
+Workload: the 96,000-atom rigid-water box (32,000 molecules, 98.6 A cube,
+seeded lattice-plus-jitter generator), real-space Ewald (alpha 0.34 1/A)
++ CHARMM-switched LJ (10-12 A), Verlet skin 2 A.
+
+One step = one pass of the hot path from FP64 positions: cell sort and
+cluster-pair list build, then forces, energies and virial (FP32 pair kernel
+with 64-bit fixed-point accumulation, FP64 exclusion corrections).  Nothing
+is carried between steps but the topology; L2 is flushed (256 MiB write)
+before every timed step.  ``value`` = in-cut-off pair interactions (r <= 12 A,
+not excluded) per second of device time, summed over ranks; ``e2e`` is the
+same through the engine's C ABI with host buffers (pinned H2D of the
+positions and D2H of forces and energies inside the timed region).
+
+``--impl reference`` times MDBas itself (oracle/_ref, its list rebuild +
+energy() with real-space Ewald) on the host cores, one process per core
+slot, each process evaluating its own copy of the workload per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ns/day & pairs/s (96k-atom real-space NB), FP32+fixed-pt vs FP64 form, 1 B200"
+WORKLOAD = ("96,000-atom rigid water box (32,000 molecules, 98.6 A cube, 0.0334/A^3), "
+            "real-space Ewald alpha 0.34 + switched LJ 10-12 A, skin 2 A")
+# algorithmic FP32 flops per in-cut-off pair (FMA = 2): displacement 3, r^2 5,
+# r 1, q_i q_j 1, exp argument 3, erfc polynomial x exp 14, E_dir 2, dE_dir 4,
+# LJ core 14, switch 15, force scalar 2, force vector + i/j accumulation 9,
+# energy + virial 4
+FLOPS_PER_PAIR = 77
+# algorithmic HBM bytes per atom of one list rebuild (cell sort + cluster layout):
+# read FP64 xyz 24 + q/eps/sig 24, write cell keys 4 + permutation 8 + float4 16
+# + float2 8, sort passes 24
+LIST_BYTES_PER_ATOM = 108
+FS_PER_STEP = 1.0
+
+
+def _parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--seed", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--precision-seeds", type=int, default=10)
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="clocks", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: MDBas on the host cores
+# ---------------------------------------------------------------------------
+def _ref_worker(seed, steps, warmup, barrier, queue):
+    import oracle
+    from mdbas_b200 import systems
+    s = systems.config_96k(seed=seed, temperature=None)
+    r = oracle.Reference(s)
+    r.makelist()
+    x, y, z = r.positions()
+    times = []
+    for k in range(warmup + steps):
+        barrier.wait()
+        t0 = r.now()
+        r.update_list(x, y, z)
+        r.energy()
+        t1 = r.now()
+        if k >= warmup:
+            times.append(t1 - t0)
+    queue.put(times)
+
+
+def _count_pairs(seed):
+    import oracle
+    from mdbas_b200 import systems
+    s = systems.config_96k(seed=seed, temperature=None)
+    o = oracle.Oracle()
+    box = o.box(s.cell())
+    excl = s.exclusions(symmetric=True)
+    return len(o.pairs_within(box, s.x, s.y, s.z, excl, 144.0))
+
+
+def run_reference(args, rank, world):
+    import oracle
+    if rank != 0:
+        return
+    if not oracle.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/libmdbas_ref.so (MDBas built from its sources) is missing"}))
+        return
+    cores = os.cpu_count() or 1
+    try:
+        cores = len(os.sched_getaffinity(0))
+    except AttributeError:
+        pass
+    procs_n = max(1, min(cores, 32))
+    pairs = _count_pairs(args.seed)
+    ctx = mp.get_context("spawn")
+    barrier = ctx.Barrier(procs_n)
+    queue = ctx.Queue()
+    steps = max(1, args.steps)
+    warm = max(0, min(args.warmup, 3))
+    ps = [ctx.Process(target=_ref_worker, args=(args.seed + k, steps, warm, barrier, queue))
+          for k in range(procs_n)]
+    for p in ps:
+        p.start()
+    res = [queue.get() for _ in ps]
+    for p in ps:
+        p.join()
+    # each step: every process evaluates one copy; the step lasts as long as
+    # its slowest process
+    step_t = [max(r[k] for r in res) for k in range(steps)]
+    t = sum(step_t) / steps
+    value = procs_n * pairs / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "pairs/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": t * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator)",
+        "config": {"workload": WORKLOAD, "n_atoms": 96000, "in_cutoff_pairs": pairs,
+                   "step": "MDBas link_cell_verlet_list_update + energy() (keyEwald=3)",
+                   "processes": procs_n},
+        "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": procs_n, "kind": "reference",
+                         "sample": f"{procs_n} processes x {steps} steps, one 96k-atom list "
+                                   f"rebuild + energy() each"},
+        "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "ns_per_day": 86400.0 / t * FS_PER_STEP * 1e-6,
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline_sample(seed: int) -> dict:
+    """MDBas single-threaded on the host: list rebuild + energy(), ~3 steps."""
+    import oracle
+    from mdbas_b200 import systems
+    if not oracle.Reference.available():
+        return {"value": None, "unit": "pairs/s", "cores": 1, "kind": "reference",
+                "sample": "unavailable: oracle/_ref not built"}
+    s = systems.config_96k(seed=seed, temperature=None)
+    r = oracle.Reference(s)
+    r.makelist()
+    x, y, z = r.positions()
+    pairs = _count_pairs(seed)
+    ts = []
+    t_start = time.perf_counter()
+    while len(ts) < 3 or (time.perf_counter() - t_start < 10 and len(ts) < 6):
+        t0 = r.now()
+        r.update_list(x, y, z)
+        r.energy()
+        ts.append(r.now() - t0)
+    r.close()
+    t = statistics.median(ts)
+    return {"value": pairs / t, "unit": "pairs/s", "cores": 1, "kind": "reference",
+            "sample": f"{len(ts)} x (96k-atom link_cell_verlet_list_update + energy()), "
+                      f"median {t:.2f} s"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def _time_steps(torch, eng, stream, flush, steps, fn):
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    return [a.elapsed_time(b) for a, b in evs]
+
+
+def run_ours(args, rank, world):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from mdbas_b200 import nb, systems
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = local
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    s = systems.config_96k(seed=args.seed + rank, temperature=None)
+    eng = nb.Engine(s, precision=1, device=dev)
+    eng.set_stream(stream.cuda_stream)
+    eng64 = nb.Engine(s, precision=0, device=dev)
+    eng64.set_stream(stream.cuda_stream)
+
+    def step32():
+        eng.build()
+        eng.compute()
+
+    def step64():
+        eng64.build()
+        eng64.compute()
+
+    for _ in range(max(3, args.warmup)):
+        step32()
+    step64()
+    torch.cuda.synchronize()
+    e = eng.energies()
+    pairs = int(e["n_pairs"])
+    stats = eng.list_stats()
+
+    # ---- timed region (FP32 + fixed point) --------------------------------
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    launches0 = eng.launches()
+    ms = _time_steps(torch, eng, stream, flush, args.steps, step32)
+    launches = eng.launches() - launches0
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    t_step = sum(ms) / len(ms)
+    if world > 1:
+        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_step = float(tt.item())
+        pt = torch.tensor([float(pairs)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(pt, op=dist.ReduceOp.SUM)
+        total_pairs = float(pt.item())
+        dist.barrier()
+    else:
+        total_pairs = float(pairs)
+    value = total_pairs / (t_step * 1e-3)
+
+    # ---- pair kernel alone (CUDA events on the launching stream) ----------
+    eng.set_timing(True)
+    eng.pair_kernel_ms(reset=True)
+    for _ in range(args.steps):
+        flush.zero_()
+        eng.compute()
+    pair_ms, _ = eng.pair_kernel_ms(reset=True)
+    eng.set_timing(False)
+    # list build alone
+    ms_build = _time_steps(torch, eng, stream, flush, args.steps, eng.build)
+    t_build = sum(ms_build) / len(ms_build)
+
+    # ---- plain FP64 form, same step ---------------------------------------
+    ms64 = _time_steps(torch, eng64, stream, flush, args.steps, step64)
+    t64 = sum(ms64) / len(ms64)
+    eng64.set_timing(True)
+    eng64.pair_kernel_ms(reset=True)
+    for _ in range(max(3, args.steps // 2)):
+        flush.zero_()
+        eng64.compute()
+    pair64_ms, _ = eng64.pair_kernel_ms(reset=True)
+    eng64.set_timing(False)
+
+    # ---- e2e through the C ABI with pinned host buffers -------------------
+    n = s.n
+    hx = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hy = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hz = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    fx = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    fy = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    fz = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    hx[:], hy[:], hz[:] = s.x, s.y, s.z
+
+    def step_e2e():
+        eng.set_positions(hx, hy, hz)
+        eng.build()
+        eng.compute()
+        eng.forces_into(fx, fy, fz)
+        eng.energies()
+
+    for _ in range(2):
+        step_e2e()
+    ms_e2e = _time_steps(torch, eng, stream, flush, args.steps, step_e2e)
+    t_e2e = sum(ms_e2e) / len(ms_e2e)
+    if world > 1:
+        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_e2e = float(tt.item())
+    e2e_value = total_pairs / (t_e2e * 1e-3)
+
+    # ---- roofline of the pair kernel ---------------------------------------
+    peak = nb.fp32_peak_tflops(dev)
+    achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
+    traffic = None
+    prof = os.path.join(ROOT, "profiles", "pair_fp32_96k_traffic.json")
+    if os.path.exists(prof):
+        try:
+            traffic = json.load(open(prof)).get("dram_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    # ---- precision vs the FP64 form over seeds ------------------------------
+    prec = None
+    if rank == 0 and args.precision_seeds > 0:
+        errs, eerr = [], []
+        for sd in range(args.precision_seeds):
+            sp = systems.config_96k(seed=sd, temperature=None)
+            a = nb.Engine(sp, precision=1, device=dev)
+            b = nb.Engine(sp, precision=0, device=dev)
+            for x in (a, b):
+                x.build()
+                x.compute()
+            fa, fb = a.forces(), b.forces()
+            num = sum(((u - v) ** 2).sum() for u, v in zip(fa, fb))
+            den = sum((v ** 2).sum() for v in fb)
+            errs.append(math.sqrt(num / den))
+            ea, eb = a.energies(), b.energies()
+            tot_a = ea["elec_direct"] + ea["elec_corr"] + ea["vdw"]
+            tot_b = eb["elec_direct"] + eb["elec_corr"] + eb["vdw"]
+            eerr.append(abs(tot_a - tot_b) / abs(tot_b))
+            a.close()
+            b.close()
+        prec = {"force_rel_rms_max": max(errs), "force_rel_rms_mean": statistics.mean(errs),
+                "energy_rel_max": max(eerr), "seeds": args.precision_seeds,
+                "against": "plain FP64 GPU form (itself within 1e-12 of MDBas)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(args.seed)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": t_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair arithmetic, int64 fixed-point accumulation, fp64 positions",
+            "data": "synthetic (seeded lattice-plus-jitter water generator)",
+            "config": {"workload": WORKLOAD, "n_atoms": n, "in_cutoff_pairs": pairs,
+                       "clusters": stats[0], "cluster_pairs": stats[1],
+                       "pair_efficiency": pairs / max(1, stats[2]),
+                       "step": "cluster-pair list build + forces/energy/virial",
+                       "l2": "flushed before every timed step (256 MiB write)",
+                       "parallelism": f"replicas x{world}"},
+            "ns_per_day": 86400.0 / (t_step * 1e-3) * FS_PER_STEP * 1e-6,
+            "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
+            "list_build": {"ms": t_build,
+                           "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9},
+            "fp64_form": {"ms_per_step": t64, "pairs_per_s": pairs / (t64 * 1e-3),
+                          "pair_kernel_ms": pair64_ms,
+                          "pair_kernel_pairs_per_s": pairs / (pair64_ms * 1e-3)},
+            "speedup_vs_fp64_form": {"step": t64 / t_step, "pair_kernel": pair64_ms / pair_ms},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_source": "measured FFMA probe (mdbas_nb_fp32_peak)",
+                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32"},
+            "precision": prec,
+            "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": t_e2e,
+                    "h2d_bytes_per_step": 3 * 8 * n,
+                    "d2h_bytes_per_step": 3 * 8 * n + 8 * 8},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    eng.close()
+    eng64.close()
+
+
+def main():
+    args = _parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

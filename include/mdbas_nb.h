@@ -407,6 +407,11 @@ int mdbas_nb_engine_set_timing(mdbas_nb_engine *e, int enable);
 int mdbas_nb_engine_kernel_time(mdbas_nb_engine *e, int which, double *avg_ms, long long *count,
                                 int reset);
 
+/* Measured FP32 FFMA throughput of a device (TFLOP/s, 2 flops per FFMA), the
+ * peak the FP32 pair kernel's roofline fraction is quoted against; ms gets the
+ * probe kernel's duration. */
+int mdbas_nb_fp32_peak(int device, double *tflops, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

@@ -211,8 +211,16 @@ def lib():
     L.mdbas_nb_engine_set_timing.argtypes = [C.c_void_p, C.c_int]
     L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
+    L.mdbas_nb_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     _LIB = L
     return L
+
+
+def fp32_peak_tflops(device: int = 0) -> float:
+    """Measured FFMA throughput (TFLOP/s) of the device."""
+    tf, ms = C.c_double(0), C.c_double(0)
+    check(lib().mdbas_nb_fp32_peak(device, C.byref(tf), C.byref(ms)), "fp32_peak")
+    return tf.value
 
 
 def check(st: int, where: str) -> None:
@@ -283,6 +291,15 @@ class Engine:
         check(lib().mdbas_nb_engine_get_forces(self.h, *(_ptr(a) for a in f), 0),
               "engine_get_forces")
         return f
+
+    def forces_into(self, fx: np.ndarray, fy: np.ndarray, fz: np.ndarray):
+        """Copy the forces into caller-owned (e.g. pinned) FP64 arrays."""
+        check(lib().mdbas_nb_engine_get_forces(self.h, _ptr(fx), _ptr(fy), _ptr(fz), 0),
+              "engine_get_forces")
+
+    def set_stream(self, stream_handle: int):
+        check(lib().mdbas_nb_engine_set_stream(self.h, C.c_void_p(stream_handle)),
+              "engine_set_stream")
 
     def forces_device(self, xp: int, yp: int, zp: int):
         check(lib().mdbas_nb_engine_get_forces(self.h, C.c_void_p(xp), C.c_void_p(yp),
