@@ -233,6 +233,12 @@ class Reference:
             lib.ref_energy.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp]
             lib.ref_self_energy.restype = C.c_double
             lib.ref_self_energy.argtypes = [C.c_void_p]
+            lib.ref_set_torsions.argtypes = [C.c_void_p, C.c_int, _ip, C.c_int, _ip]
+            lib.ref_n_pair14.restype = C.c_int
+            lib.ref_n_pair14.argtypes = [C.c_void_p]
+            lib.ref_get_list14.argtypes = [C.c_void_p, _ip]
+            lib.ref_layout.restype = C.c_int
+            lib.ref_layout.argtypes = [C.c_char_p, C.c_int]
             lib.ref_now.restype = C.c_double
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
@@ -253,6 +259,28 @@ class Reference:
                                 _d(sysm.eps), _d(sysm.sig),
                                 None if fz is None else fz.ctypes.data,
                                 len(sysm.bonds), bonds, len(sysm.angles), angles)
+
+    def set_torsions(self, dihe=None, impr=None):
+        d = _i(np.asarray(dihe, dtype=np.int32).reshape(-1)) if dihe is not None and len(dihe) \
+            else np.zeros(4, np.int32)
+        m = _i(np.asarray(impr, dtype=np.int32).reshape(-1)) if impr is not None and len(impr) \
+            else np.zeros(4, np.int32)
+        nd = 0 if dihe is None else len(dihe)
+        ni = 0 if impr is None else len(impr)
+        self.lib().ref_set_torsions(self.h, nd, d, ni, m)
+
+    def list14(self):
+        n14 = self.lib().ref_n_pair14(self.h)
+        out = np.zeros(2 * max(n14, 1), np.int32)
+        if n14:
+            self.lib().ref_get_list14(self.h, out)
+        return out[:2 * n14]
+
+    @classmethod
+    def layout(cls) -> str:
+        buf = C.create_string_buffer(4096)
+        cls.lib().ref_layout(buf, 4096)
+        return buf.value.decode()
 
     def box(self) -> np.ndarray:
         out = np.zeros(30)

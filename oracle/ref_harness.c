@@ -25,6 +25,7 @@
 #include <string.h>
 #include <math.h>
 #include <time.h>
+#include <stddef.h>
 
 #include "global.h"
 #include "energy.h"
@@ -140,6 +141,65 @@ RefSys *ref_create(int nAtom, int boxType, const double cell[9], double cutOff, 
   s->dihe = (DIHE *)calloc(1, sizeof(DIHE));
   s->impr = (DIHE *)calloc(1, sizeof(DIHE));
   return s;
+}
+
+/* Dihedrals and impropers (4 atom indices each) for the exclusion builders;
+ * call before ref_makelist. */
+void ref_set_torsions(RefSys *s, int nDihedral, const int *dihe, int nImproper, const int *impr)
+{
+  int i;
+  free(s->dihe);
+  free(s->impr);
+  s->dihe = (DIHE *)calloc((size_t)(nDihedral > 0 ? nDihedral : 1), sizeof(DIHE));
+  s->impr = (DIHE *)calloc((size_t)(nImproper > 0 ? nImproper : 1), sizeof(DIHE));
+  for (i = 0; i < nDihedral; i++) {
+    s->dihe[i].a = dihe[4 * i]; s->dihe[i].b = dihe[4 * i + 1];
+    s->dihe[i].c = dihe[4 * i + 2]; s->dihe[i].d = dihe[4 * i + 3];
+  }
+  for (i = 0; i < nImproper; i++) {
+    s->impr[i].a = impr[4 * i]; s->impr[i].b = impr[4 * i + 1];
+    s->impr[i].c = impr[4 * i + 2]; s->impr[i].d = impr[4 * i + 3];
+  }
+  s->param.nDihedral = nDihedral;
+  s->param.nImproper = nImproper;
+}
+
+int ref_n_pair14(const RefSys *s) { return s->neigh.nPair14; }
+
+void ref_get_list14(const RefSys *s, int *out)
+{
+  memcpy(out, s->neighList14, (size_t)(2 * s->neigh.nPair14) * sizeof(int));
+}
+
+/* sizeof and field offsets of MDBas's structs, for the ABI layout check:
+ * "NAME size off0 off1 ...;" for each struct, written into buf. */
+#define OFF(T, f) (int)offsetof(T, f)
+int ref_layout(char *buf, int len)
+{
+  int n = 0;
+  n += snprintf(buf + n, len - n, "PBC %d %d %d %d %d %d %d;", (int)sizeof(PBC), OFF(PBC, type),
+                OFF(PBC, a1), OFF(PBC, u1), OFF(PBC, pa), OFF(PBC, vol0), OFF(PBC, stress9));
+  n += snprintf(buf + n, len - n, "CTRL %d %d %d %d %d %d;", (int)sizeof(CTRL), OFF(CTRL, newjob),
+                OFF(CTRL, keyLink), OFF(CTRL, keyEwald), OFF(CTRL, elecType), OFF(CTRL, ens));
+  n += snprintf(buf + n, len - n, "PARAM %d %d %d %d %d %d %d %d;", (int)sizeof(PARAM),
+                OFF(PARAM, timeStep), OFF(PARAM, nAtom), OFF(PARAM, tolShake),
+                OFF(PARAM, chargeConst), OFF(PARAM, cutOff2), OFF(PARAM, switch2),
+                OFF(PARAM, maxminst));
+  n += snprintf(buf + n, len - n, "BOND %d %d %d %d;", (int)sizeof(BOND), OFF(BOND, a),
+                OFF(BOND, k), OFF(BOND, beta));
+  n += snprintf(buf + n, len - n, "ANGLE %d %d %d %d;", (int)sizeof(ANGLE), OFF(ANGLE, a),
+                OFF(ANGLE, c), OFF(ANGLE, theta0));
+  n += snprintf(buf + n, len - n, "DIHE %d %d %d %d;", (int)sizeof(DIHE), OFF(DIHE, order),
+                OFF(DIHE, d), OFF(DIHE, mult));
+  n += snprintf(buf + n, len - n, "NEIGH %d %d %d;", (int)sizeof(NEIGH), OFF(NEIGH, linkRatio),
+                OFF(NEIGH, nPair14));
+  n += snprintf(buf + n, len - n, "ENERGY %d %d %d %d;", (int)sizeof(ENERGY), OFF(ENERGY, elec),
+                OFF(ENERGY, virelec), OFF(ENERGY, virtot));
+  n += snprintf(buf + n, len - n, "CONSTRAINT %d %d;", (int)sizeof(CONSTRAINT),
+                OFF(CONSTRAINT, rc2));
+  n += snprintf(buf + n, len - n, "EWALD %d %d %d;", (int)sizeof(EWALD), OFF(EWALD, m3max),
+                OFF(EWALD, alpha));
+  return n;
 }
 
 /* Box quantities after init_box, in PBC field order a..vol (for host checks). */
