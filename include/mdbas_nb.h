@@ -412,6 +412,40 @@ int mdbas_nb_engine_kernel_time(mdbas_nb_engine *e, int which, double *avg_ms, l
  * probe kernel's duration. */
 int mdbas_nb_fp32_peak(int device, double *tflops, double *ms);
 
+/* ------------------------------------------------------------------------ */
+/* Evaluation without device allocation (no counterpart in MDBas).           */
+/* ------------------------------------------------------------------------ */
+/* For callers that cannot let the library call cudaMalloc -- programs that
+ * own all device memory through their own allocator, or loops that must not
+ * hit the device-wide synchronisation cudaMalloc/cudaFree imply.  Same work
+ * as the plain FP64 form of ewald_energy (direct Ewald term + switched LJ
+ * over a MDBas half list, erf exclusion correction for every excluded pair
+ * j>i), but every array is a DEVICE pointer owned by the caller and the only
+ * scratch is a fixed area compiled into the library:
+ * MDBAS_NB_NOALLOC_SCRATCH_BYTES per GPU that loads it, held until exit,
+ * enough for MDBAS_NB_NOALLOC_MAX_ATOMS atoms; larger systems are rejected
+ * with MDBAS_NB_ERR_CAPACITY.  The function calls no cudaMalloc/cudaFree.
+ *   x..sig, neighList/neighPair/neighOrder (MDBas layout), exclStart
+ *   (nAtom+1 offsets) + exclFlat (rows as in MDBas's exclList): inputs;
+ *   fx/fy/fz: forces are ADDED into them; energies (host, 6 doubles):
+ *   eDir, eCorr, eVdw, virDir, virCorr, virVdw.
+ * The first call on each device resolves the scratch area's device address
+ * (cudaGetSymbolAddress) with that device current: make it before any stream
+ * capture.  All calls share the scratch area, so calls that overlap on the
+ * GPU (unordered streams) race; order them on one stream or serialise them.
+ * Runs on `stream` (cudaStream_t as void*, NULL = default) and returns after
+ * the energies are copied back. */
+#define MDBAS_NB_NOALLOC_MAX_ATOMS 131072
+#define MDBAS_NB_NOALLOC_SCRATCH_BYTES 1574656
+int mdbas_nb_ewald_fp64_noalloc(int nAtom, const PBC *box, double cutOff, double cutOn,
+                                double alpha, double chargeConst, int vdwSwitch,
+                                const double *x, const double *y, const double *z,
+                                const double *q, const double *eps, const double *sig,
+                                const int *neighList, const int *neighPair,
+                                const int *neighOrder, const int *exclStart,
+                                const int *exclFlat, double *fx, double *fy, double *fz,
+                                double energies[6], void *stream);
+
 #ifdef __cplusplus
 }
 #endif
