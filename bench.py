@@ -301,6 +301,13 @@ def run_ours(args, rank, world):
         flush.zero_()
         eng.compute()
     pair_ms, _ = eng.pair_kernel_ms(reset=True)
+    # the filtered/compacted variant of the same kernel, for comparison
+    eng.set_variant(1)
+    for _ in range(args.steps):
+        flush.zero_()
+        eng.compute()
+    compact_ms, _ = eng.pair_kernel_ms(reset=True)
+    eng.set_variant(0)
     eng.set_timing(False)
     # list build alone
     ms_build = _time_steps(torch, eng, stream, flush, args.steps, eng.build)
@@ -398,7 +405,8 @@ def run_ours(args, rank, world):
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
             "ns_per_day": 86400.0 / (t_step * 1e-3) * FS_PER_STEP * 1e-6,
-            "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
+            "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
+                            "variant": "dense 8x8", "compacted_variant_ms": compact_ms},
             "list_build": {"ms": t_build,
                            "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9},
             "fp64_form": {"ms_per_step": t64, "pairs_per_s": pairs / (t64 * 1e-3),

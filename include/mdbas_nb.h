@@ -398,6 +398,10 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]);
  * the number of pairs; pairs (2*capacity ints) may be NULL to query it. */
 int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, long long capacity,
                                  long long *count);
+/* Pair kernel variant of the mixed-precision path: 0 (default) computes every
+ * pair of each 8x8 cluster pair in one warp step per cluster pair; 1 filters
+ * the pairs first and computes only in-cut-off pairs from per-atom queues. */
+int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
 /* Kernels this engine launched since creation. */
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e);
 /* Average duration (ms) of the pair kernel over the launches recorded since

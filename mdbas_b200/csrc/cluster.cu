@@ -20,7 +20,9 @@
 // once (j > i, or j == i with a positive or zero shift, the latter with only
 // the upper triangle of atom pairs).  Buffers are flushed as work items of
 // 32 entries; at flush the warp builds each entry's 64-bit interaction mask
-// (padding, exclusions, frozen pairs, self-pair triangle) with two ballots.
+// (pairs within the list radius at build time, padding, exclusions, frozen
+// pairs, self-pair triangle) with two ballots and drops entries whose mask
+// is empty.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -120,9 +122,11 @@ __global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__
                            const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, const double *__restrict__ q,
                            const double *__restrict__ eps, const double *__restrict__ sig,
-                           double sqrtC, double4 *__restrict__ origin, float4 *__restrict__ half,
+                           double sqrtC, double4 *__restrict__ origin,
+                           float4 *__restrict__ originF, float4 *__restrict__ half,
                            float4 *__restrict__ xq, float2 *__restrict__ lj,
-                           int *__restrict__ slotOf, int *__restrict__ clusterXY) {
+                           int *__restrict__ slotOf, int *__restrict__ clusterXY,
+                           int *__restrict__ hmaxBits) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nClusters) return;
   const double ilx = 1.0 / g.Lx, ily = 1.0 / g.Ly, ilz = 1.0 / g.Lz;
@@ -143,11 +147,20 @@ __global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__
     }
   }
   const double ox = 0.5 * (lo[0] + hi[0]), oy = 0.5 * (lo[1] + hi[1]), oz = 0.5 * (lo[2] + hi[2]);
+  int nreal = 0;
+#pragma unroll
+  for (int k = 0; k < kClusterSize; ++k) nreal += atoms[k] >= 0;
   origin[c] = make_double4(ox, oy, oz, 0.0);
-  // Half extents rounded up so that the FP32 box always contains its atoms.
+  originF[c] = make_float4((float)ox, (float)oy, (float)oz, (float)nreal);
+  // Half extents rounded up so that the FP32 box always contains its atoms;
+  // w holds the number of real (non-padding) atoms.
   half[c] = make_float4(__double2float_ru(0.5 * (hi[0] - lo[0]) * (1.0 + 1e-6) + 1e-6),
                         __double2float_ru(0.5 * (hi[1] - lo[1]) * (1.0 + 1e-6) + 1e-6),
-                        __double2float_ru(0.5 * (hi[2] - lo[2]) * (1.0 + 1e-6) + 1e-6), 0.f);
+                        __double2float_ru(0.5 * (hi[2] - lo[2]) * (1.0 + 1e-6) + 1e-6),
+                        (float)nreal);
+  atomicMax(hmaxBits + 0, __float_as_int(half[c].x));
+  atomicMax(hmaxBits + 1, __float_as_int(half[c].y));
+  atomicMax(hmaxBits + 2, __float_as_int(half[c].z));
   clusterXY[c] = colXY[atomCol[atoms[0]]];
 #pragma unroll
   for (int k = 0; k < kClusterSize; ++k) {
@@ -165,81 +178,121 @@ __global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__
   }
 }
 
-__device__ __forceinline__ bool excl_has(int es, int ee, const int *__restrict__ exclFlat, int j) {
-  for (int k = es; k < ee; ++k)
-    if (__ldg(exclFlat + k) == j) return true;
-  return false;
-}
+constexpr int kExclRegs = 8;  // exclusion partners per atom kept in registers
 
 struct SearchBuf {
   int j[kBufCap];
   int sidx[kBufCap];
-  float sx[kBufCap], sy[kBufCap], sz[kBufCap];
+  int nreal[kBufCap];
   uint2 mask[kItemMax];
 };
 
-// Flush the first cnt (<= kItemMax) buffered entries as one work item.
-__device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, int ia, int fi, int es, int ee,
-                           const int *__restrict__ slotAtom, const int *__restrict__ frozen,
-                           const int *__restrict__ exclFlat, CPairEntry *__restrict__ entries,
-                           uint2 *__restrict__ masks, int4 *__restrict__ items,
-                           long long *__restrict__ counters, long long entryCap,
-                           long long itemCap) {
+// Flush the first cnt (<= kItemMax) buffered entries as one work item.  Each
+// entry's 64-bit interaction mask is built with two ballots: lane L decides
+// pairs (i = L%8, j = L/8) and (i = L%8, j = L/8 + 4).  Exclusions come from
+// the lane's partner slots (registers; a global-memory loop for atoms with
+// more than kExclRegs partners).
+__device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double4 oi,
+                           const float4 oif, const float4 xi, const float4 *__restrict__ xq,
+                           const float4 *__restrict__ originF,
+                           const ClusterGeom &g, int nreal_i, const int (&ps)[kExclRegs], int nps,
+                           int es, int ee, int fi, const int *__restrict__ exclFlat,
+                           const int *__restrict__ slotOf, const int *__restrict__ slotAtom,
+                           const int *__restrict__ frozen, const double4 *__restrict__ origin,
+                           CPairEntry *__restrict__ entries, uint2 *__restrict__ masks,
+                           int4 *__restrict__ items, long long *__restrict__ counters,
+                           long long entryCap, long long itemCap) {
   const int il = lane & 7, jl = lane >> 3;
   for (int k = 0; k < cnt; ++k) {
     const int cj = B.j[k];
-    const bool selfzero = (cj == ci) && (B.sidx[k] == 13);
-    const int ja = slotAtom[cj * kClusterSize + jl];
-    const int jb = slotAtom[cj * kClusterSize + jl + 4];
-    bool oka = (ia >= 0) && (ja >= 0);
-    bool okb = (ia >= 0) && (jb >= 0);
-    if (oka) {
-      if (frozen && fi * frozen[ja] != 0) oka = false;
-      else if (selfzero && jl <= il) oka = false;
-      else if (excl_has(es, ee, exclFlat, ja)) oka = false;
+    const int nrj = B.nreal[k];
+    const int sidx = B.sidx[k];
+    const bool selfzero = (cj == ci) && (sidx == 13);
+    // pair distances at build time: only pairs within the list radius are
+    // kept (FP32 shift from the FP32 origins; rlist2 carries a 1e-5 margin)
+    const float4 ojf = originF[cj];
+    const float shx = (ojf.x + (sidx % 3 - 1) * (float)g.Lx) - oif.x;
+    const float shy = (ojf.y + ((sidx / 3) % 3 - 1) * (float)g.Ly) - oif.y;
+    const float shz = (ojf.z + (sidx / 9 - 1) * (float)g.Lz) - oif.z;
+    const float4 xa = xq[cj * kClusterSize + jl], xb = xq[cj * kClusterSize + jl + 4];
+    const float ax = xa.x + shx - xi.x, ay = xa.y + shy - xi.y, az = xa.z + shz - xi.z;
+    const float bx = xb.x + shx - xi.x, by = xb.y + shy - xi.y, bz = xb.z + shz - xi.z;
+    bool oka = (il < nreal_i) && (jl < nrj) && (ax * ax + ay * ay + az * az <= g.rlist2);
+    bool okb = (il < nreal_i) && (jl + 4 < nrj) && (bx * bx + by * by + bz * bz <= g.rlist2);
+    if (selfzero) {
+      oka = oka && (jl > il);
+      okb = okb && (jl + 4 > il);
     }
-    if (okb) {
-      if (frozen && fi * frozen[jb] != 0) okb = false;
-      else if (selfzero && jl + 4 <= il) okb = false;
-      else if (excl_has(es, ee, exclFlat, jb)) okb = false;
+    const int sa = cj * kClusterSize + jl, sb = sa + 4;
+#pragma unroll
+    for (int r = 0; r < kExclRegs; ++r) {
+      if (r < nps) {
+        oka = oka && (ps[r] != sa);
+        okb = okb && (ps[r] != sb);
+      }
+    }
+    if (nps > kExclRegs) {
+      for (int e = es + kExclRegs; e < ee; ++e) {
+        const int p = slotOf[__ldg(exclFlat + e)];
+        oka = oka && (p != sa);
+        okb = okb && (p != sb);
+      }
+    }
+    if (frozen && fi) {
+      const int ja = slotAtom[sa], jb = slotAtom[sb];
+      if (oka && ja >= 0 && frozen[ja]) oka = false;
+      if (okb && jb >= 0 && frozen[jb]) okb = false;
     }
     const unsigned mlo = __ballot_sync(0xffffffffu, oka);
     const unsigned mhi = __ballot_sync(0xffffffffu, okb);
     if (lane == 0) B.mask[k] = make_uint2(mlo, mhi);
   }
+  __syncwarp();
+  // keep the entries with at least one pair within the list radius
+  const bool keep = lane < cnt && (B.mask[lane].x | B.mask[lane].y) != 0u;
+  const unsigned km = __ballot_sync(0xffffffffu, keep);
+  const int nkeep = __popc(km);
+  if (nkeep == 0) return;
   long long e0 = 0, it = 0;
   if (lane == 0) {
     e0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 0),
-                              (unsigned long long)cnt);
+                              (unsigned long long)nkeep);
     it = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 1), 1ull);
   }
-  __syncwarp();
   e0 = __shfl_sync(0xffffffffu, e0, 0);
   it = __shfl_sync(0xffffffffu, it, 0);
-  if (e0 + cnt > entryCap || it >= itemCap) {
+  if (e0 + nkeep > entryCap || it >= itemCap) {
     if (lane == 0) atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), 1ull);
     return;
   }
-  for (int k = lane; k < cnt; k += 32) {
+  if (keep) {
+    const int k = lane;
+    const int pos = __popc(km & ((1u << lane) - 1u));
+    const int cj = B.j[k], sidx = B.sidx[k];
+    const double4 oj = origin[cj];
+    const int sx = sidx % 3 - 1, sy = (sidx / 3) % 3 - 1, sz = sidx / 9 - 1;
     CPairEntry en;
-    en.j = B.j[k];
-    en.sx = B.sx[k];
-    en.sy = B.sy[k];
-    en.sz = B.sz[k];
-    entries[e0 + k] = en;
-    masks[e0 + k] = B.mask[k];
+    en.j = cj;
+    en.sx = (float)(oj.x + sx * g.Lx - oi.x);
+    en.sy = (float)(oj.y + sy * g.Ly - oi.y);
+    en.sz = (float)(oj.z + sz * g.Lz - oi.z);
+    entries[e0 + pos] = en;
+    masks[e0 + pos] = B.mask[k];
   }
-  if (lane == 0) items[it] = make_int4(ci, (int)e0, cnt, 0);
+  if (lane == 0) items[it] = make_int4(ci, (int)e0, nkeep, 0);
 }
 
 __global__ void __launch_bounds__(kSearchThreads)
 k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
          const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
-         const double4 *__restrict__ origin, const float4 *__restrict__ half,
-         const int *__restrict__ slotAtom, const int *__restrict__ frozen,
+         const double4 *__restrict__ origin, const float4 *__restrict__ originF,
+         const float4 *__restrict__ half, const int *__restrict__ slotAtom,
+         const int *__restrict__ slotOf, const int *__restrict__ frozen,
          const int *__restrict__ exclStart, const int *__restrict__ exclFlat,
-         CPairEntry *__restrict__ entries, uint2 *__restrict__ masks, int4 *__restrict__ items,
-         long long *__restrict__ counters, long long entryCap, long long itemCap) {
+         const int *__restrict__ hmaxBits, const float4 *__restrict__ xq,
+         CPairEntry *__restrict__ entries,
+         uint2 *__restrict__ masks, int4 *__restrict__ items, long long *__restrict__ counters,
+         long long entryCap, long long itemCap) {
   __shared__ SearchBuf bufs[kSearchThreads / 32];
   const int lane = threadIdx.x & 31;
   const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -247,87 +300,95 @@ k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
   SearchBuf &B = bufs[threadIdx.x >> 5];
 
   const double4 oi = origin[ci];
+  const float4 oif = originF[ci];
   const float4 hi = half[ci];
+  const int nreal_i = (int)hi.w;
   const int xy = clusterXY[ci];
   const int cx = xy & 0xffff, cy = xy >> 16;
+  // this lane's i atom, its exclusion partners as slots
   const int ia = slotAtom[ci * kClusterSize + (lane & 7)];
+  int es = 0, ee = 0;
+  if (ia >= 0) {
+    es = exclStart[ia];
+    ee = exclStart[ia + 1];
+  }
+  const int nps = ee - es;
+  int ps[kExclRegs];
+#pragma unroll
+  for (int r = 0; r < kExclRegs; ++r) ps[r] = (r < nps) ? slotOf[__ldg(exclFlat + es + r)] : -1;
   const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
-  const int es = (ia >= 0) ? exclStart[ia] : 0;
-  const int ee = (ia >= 0) ? exclStart[ia + 1] : 0;
+  const float4 xi = xq[ci * kClusterSize + (lane & 7)];
+
   const float rl = sqrtf(g.rlist2);
+  const float Lx = (float)g.Lx, Ly = (float)g.Ly, Lz = (float)g.Lz;
+  const float wx = (float)g.wx, wy = (float)g.wy;
+  // z images that can reach any cluster at all: cluster centres lie in
+  // [-Lz/2, Lz/2) and no cluster extends more than hmax[2] from its centre
+  const float hzmax = __int_as_float(hmaxBits[2]);
+  const float zlo = oif.z - hi.z - rl - hzmax, zhi = oif.z + hi.z + rl + hzmax;
+  const bool zm = zlo < -0.5f * Lz;  // the image below can be within reach
+  const bool zp = zhi > 0.5f * Lz;   // the image above can be within reach
   int cnt = 0;
   long long cand = 0;
 
   for (int dy = -g.Dy; dy <= g.Dy; ++dy) {
     int jy = cy + dy, sy = 0;
     if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
-    // distance in y from the i box to the cell's y interval (this image)
-    {
-      const double ylo = -0.5 * g.Ly + jy * g.wy + sy * g.Ly, yhi = ylo + g.wy;
-      const double gy = fmax(fmax(ylo - (oi.y + hi.y), (oi.y - hi.y) - yhi), 0.0);
-      if (gy > rl) continue;
-    }
+    const float ylo = -0.5f * Ly + jy * wy + sy * Ly, yhi = ylo + wy;
+    const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
+    if (gy > rl) continue;
     for (int dx = -g.Dx; dx <= g.Dx; ++dx) {
       int jx = cx + dx, sx = 0;
       if (jx < 0) { jx += g.ncx; sx = -1; } else if (jx >= g.ncx) { jx -= g.ncx; sx = 1; }
-      const double xlo = -0.5 * g.Lx + jx * g.wx + sx * g.Lx, xhi = xlo + g.wx;
-      const double gx = fmax(fmax(xlo - (oi.x + hi.x), (oi.x - hi.x) - xhi), 0.0);
-      if (gx > rl) continue;
+      const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
+      const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
+      if (gx * gx + gy * gy > g.rlist2) continue;
       const int col = colRank[jy * g.ncx + jx];
       const int cs = colClStart[col], ce = colClStart[col + 1];
       for (int base = cs; base < ce; base += 32) {
         const int cj = base + lane;
         const bool valid = cj < ce;
-        double4 oj = make_double4(0, 0, 0, 0);
-        float4 hj = make_float4(0, 0, 0, 0);
+        float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
+        float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
         if (valid) {
-          oj = origin[cj];
+          oj = originF[cj];
           hj = half[cj];
         }
-        const double ddx = oj.x + sx * g.Lx - oi.x;
-        const double ddy = oj.y + sy * g.Ly - oi.y;
+        const float fx = oj.x + sx * Lx - oif.x;
+        const float fy = oj.y + sy * Ly - oif.y;
+        const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
+        const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
+        const float dxy = gxx * gxx + gyy * gyy;
         for (int sz = -1; sz <= 1; ++sz) {
-          const double ddz = oj.z + sz * g.Lz - oi.z;
-          const float fx = (float)ddx, fy = (float)ddy, fz = (float)ddz;
-          const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
-          const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
+          if ((sz < 0 && !zm) || (sz > 0 && !zp)) continue;
+          const float fz = oj.z + sz * Lz - oif.z;
           const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
           const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
           const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
           const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
-          const bool pass = valid && half_ok && (gxx * gxx + gyy * gyy + gzz * gzz <= g.rlist2);
+          const bool pass = valid && half_ok && (dxy + gzz * gzz <= g.rlist2);
           cand += valid;
           const unsigned m = __ballot_sync(0xffffffffu, pass);
-          const int add = __popc(m);
-          if (add == 0) continue;
-          if (cnt + add > kBufCap) {
-            // cannot happen with kBufCap >= 2*kItemMax, flushed below
-          }
+          if (m == 0u) continue;
           if (pass) {
             const int pos = cnt + __popc(m & ((1u << lane) - 1u));
             B.j[pos] = cj;
             B.sidx[pos] = sidx;
-            B.sx[pos] = fx;
-            B.sy[pos] = fy;
-            B.sz[pos] = fz;
+            B.nreal[pos] = (int)hj.w;
           }
-          cnt += add;
+          cnt += __popc(m);
           __syncwarp();
           if (cnt >= kItemMax) {
-            flush_item(B, kItemMax, ci, lane, ia, fi, es, ee, slotAtom, frozen, exclFlat, entries,
-                       masks, items, counters, entryCap, itemCap);
+            flush_item(B, kItemMax, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, es,
+                       ee, fi, exclFlat,
+                       slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
+                       entryCap, itemCap);
             __syncwarp();
             const int rem = cnt - kItemMax;
             if (lane < rem) {
-              const int jv = B.j[kItemMax + lane], sv = B.sidx[kItemMax + lane];
-              const float a = B.sx[kItemMax + lane], b = B.sy[kItemMax + lane],
-                          c = B.sz[kItemMax + lane];
-              __syncwarp(__activemask());
-              B.j[lane] = jv;
-              B.sidx[lane] = sv;
-              B.sx[lane] = a;
-              B.sy[lane] = b;
-              B.sz[lane] = c;
+              B.j[lane] = B.j[kItemMax + lane];
+              B.sidx[lane] = B.sidx[kItemMax + lane];
+              B.nreal[lane] = B.nreal[kItemMax + lane];
             }
             cnt = rem;
             __syncwarp();
@@ -336,16 +397,14 @@ k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
       }
     }
   }
-  if (cnt > 0) {
-    flush_item(B, cnt, ci, lane, ia, fi, es, ee, slotAtom, frozen, exclFlat, entries, masks,
-               items, counters, entryCap, itemCap);
-  }
-  // candidate statistics
-  cand = __shfl_sync(0xffffffffu, cand, 0) * 0 + cand;
+  if (cnt > 0)
+    flush_item(B, cnt, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, es, ee, fi,
+               exclFlat, slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
+               entryCap, itemCap);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
-  if (lane == 0) atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3),
-                           (unsigned long long)cand);
+  if (lane == 0)
+    atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3), (unsigned long long)cand);
 }
 
 __global__ void k_refresh(int nSlots, ClusterGeom g, const int *__restrict__ slotAtom,
@@ -472,6 +531,9 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   MDB_TRY(w.clusterXY.ensure(sizeof(int) * nCl));
   MDB_TRY(w.origin.ensure(sizeof(double4) * nCl));
   MDB_TRY(w.half.ensure(sizeof(float4) * nCl));
+  MDB_TRY(w.originF.ensure(sizeof(float4) * nCl));
+  MDB_TRY(w.hmax.ensure(sizeof(int) * 4));
+  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4, s));
   MDB_TRY(w.xq.ensure(sizeof(float4) * nSlots));
   MDB_TRY(w.lj.ensure(sizeof(float2) * nSlots));
   MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)nSlots));
@@ -484,8 +546,9 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
              w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
   MDB_LAUNCH(k_clusters, grid_for(nCl, 128), 128, 0, s, nCl, g, w.slotAtom.as<int>(),
              w.atomCol.as<int>(), w.colXY.as<int>(), x, y, z, q, eps, sig, sqrtC,
-             w.origin.as<double4>(), w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(),
-             w.slotOf.as<int>(), w.clusterXY.as<int>());
+             w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
+             w.xq.as<float4>(), w.lj.as<float2>(),
+             w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
 
   // Cluster-pair search; grow the list and search again if it overflowed.
   if (w.entryCap == 0) {
@@ -499,8 +562,10 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
     MDB_LAUNCH(k_search, grid_for((long long)nCl * 32, kSearchThreads), kSearchThreads, 0, s, nCl,
                g, w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
-               w.origin.as<double4>(), w.half.as<float4>(), w.slotAtom.as<int>(), frozen,
-               exclStart, exclFlat, w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+               w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
+               w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
+               w.hmax.as<int>(), w.xq.as<float4>(), w.entries.as<CPairEntry>(),
+               w.masks.as<uint2>(),
                w.items.as<int4>(), w.counters.as<long long>(), w.entryCap, w.itemCap);
     MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaStreamSynchronize(s));

@@ -41,7 +41,9 @@ struct ClusterWork {
   DBuf clusterXY;     // cluster -> cx | cy << 16
   DBuf colClStart;    // column slot -> first cluster (nCols + 1)
   DBuf origin;        // double4 per cluster (FP64 origin)
-  DBuf half;          // float4 per cluster (bbox half extents)
+  DBuf originF;       // float4 per cluster (FP32 origin, w = real atoms)
+  DBuf hmax;          // int[4]: largest half extent per axis (float bits)
+  DBuf half;          // float4 per cluster (bbox half extents, w = real atoms)
   DBuf xq;            // float4 per slot: position - origin, q*sqrt(C)
   DBuf lj;            // float2 per slot: 2*eps_i, sig_i
   // pair list

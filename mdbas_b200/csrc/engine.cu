@@ -345,7 +345,7 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
       e->block = 256;
     }
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev0, s));
-    ENG_TRY(e, pair_fp32_launch(w, e->pp, e->grid, e->block, s));
+    ENG_TRY(e, pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev1, s));
     ENG_TRY(e, excl_fix_launch(w, n, e->box, e->pp, e->exclStart.as<int>(),
                                e->exclFlat.as<int>(), e->x.as<double>(), e->y.as<double>(),
@@ -477,6 +477,12 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs,
 }
 
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e) { return e ? e->launches : -1; }
+
+int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
+  if (!e || (variant != kPairDense && variant != kPairCompact)) return MDBAS_NB_ERR_ARG;
+  e->variant = variant;
+  return MDBAS_NB_OK;
+}
 
 int mdbas_nb_engine_set_timing(mdbas_nb_engine *e, int enable) {
   if (!e) return MDBAS_NB_ERR_ARG;

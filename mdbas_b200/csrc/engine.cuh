@@ -28,6 +28,7 @@ struct mdbas_nb_engine {
   mdbas::ClusterWork cl;
   mdbas::DBuf fout;
   int grid = 0, block = 0;
+  int variant = 0;  // pair kernel variant (kPairDense)
   // export scratch
   mdbas::DBuf exportBuf, exportCount;
   // bookkeeping

@@ -203,6 +203,228 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// Compacted variant.  Same work items, entries and results as k_pair_fp32,
+// but only in-cut-off pairs reach the expensive arithmetic:
+//   filter: per entry the warp tests its 64 pairs (r^2 <= rc^2 and the mask
+//     bit) and appends the survivors to per-i-atom queues in shared memory
+//     (ballot + prefix count inside each group of 4 lanes that share an i
+//     atom), LJ pairs (both eps != 0) before Coulomb-only pairs; the j
+//     clusters' slot data are staged in shared memory on the way;
+//   compute: lane L keeps i atom L%8 and walks that atom's queue with the
+//     three other lanes of its group, one pair per lane per round; rounds
+//     past every queue's LJ part skip the LJ code (water: H atoms carry no
+//     LJ site, so most rounds are Coulomb-only);
+//   accumulation: i forces stay in registers for the whole item; each pair
+//     stores its force in its own (j atom, i atom) slot in shared memory, and
+//     at the end of a chunk one lane per j atom sums its slots in i order and
+//     adds the sum to the global fixed-point accumulators -- no atomics on
+//     shared memory, and the order of every FP32 sum is fixed.
+// ---------------------------------------------------------------------------
+constexpr int kChunk = 8;    // entries per filter/compute chunk
+constexpr int kCWarps = 4;   // warps per block
+
+struct CompactWarp {
+  int ej[kChunk];
+  uint2 inm[kChunk];                                  // in-cut-off bits per entry
+  float4 es[kChunk];                                  // FP32 shift per entry
+  float4 xs[kChunk * kClusterSize];                   // staged j atoms
+  float2 ls[kChunk * kClusterSize];                   // staged j LJ parameters
+  unsigned char qlj[kClusterSize][kChunk * kClusterSize];  // per-i-atom queues
+  unsigned char qn[kClusterSize][kChunk * kClusterSize];
+  float4 fst[kChunk * kClusterSize][kClusterSize];    // force of pair (j key, i atom)
+};
+
+template <bool VDW>
+__global__ void __launch_bounds__(kCWarps * 32, 4)
+k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ items,
+             const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
+             const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
+             long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  CompactWarp &W = reinterpret_cast<CompactWarp *>(smem_raw)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, q = lane >> 3;
+  const unsigned gmask = 0x01010101u << il;
+  const unsigned lt = (1u << lane) - 1u;
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0, npair = 0;
+  bool overflow = false;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    const bool iHasLJ = li.x != 0.f;
+    float fix = 0.f, fiy = 0.f, fiz = 0.f;
+    float ec = 0.f, ev = 0.f, vc = 0.f, vv = 0.f;
+    for (int c0 = 0; c0 < ne; c0 += kChunk) {
+      const int nEnt = min(kChunk, ne - c0);
+      // ---- filter ---------------------------------------------------------
+      int nLJ = 0, nN = 0;
+      for (int e = 0; e < nEnt; ++e) {
+        const CPairEntry en = entries[e0 + c0 + e];
+        const uint2 mk = masks[e0 + c0 + e];
+        const int jb = en.j * kClusterSize + q;
+        const float4 xa = xq[jb];
+        const float2 la = lj[jb];
+        const float4 xb = xq[jb + 4];
+        const float2 lb = lj[jb + 4];
+        if (il == 0) {
+          W.xs[e * kClusterSize + q] = xa;
+          W.xs[e * kClusterSize + q + 4] = xb;
+          W.ls[e * kClusterSize + q] = la;
+          W.ls[e * kClusterSize + q + 4] = lb;
+        }
+        const float sx = en.sx - xi.x, sy = en.sy - xi.y, sz = en.sz - xi.z;
+        const float ax = xa.x + sx, ay = xa.y + sy, az = xa.z + sz;
+        const float bx = xb.x + sx, by = xb.y + sy, bz = xb.z + sz;
+        const bool ina = ((mk.x >> lane) & 1u) && (fmaf(ax, ax, fmaf(ay, ay, az * az)) <= c.rc2);
+        const bool inb = ((mk.y >> lane) & 1u) && (fmaf(bx, bx, fmaf(by, by, bz * bz)) <= c.rc2);
+        const unsigned ba = __ballot_sync(0xffffffffu, ina);
+        const unsigned bb = __ballot_sync(0xffffffffu, inb);
+        if (lane == 0) {
+          W.ej[e] = en.j;
+          W.es[e] = make_float4(en.sx, en.sy, en.sz, 0.f);
+          W.inm[e] = make_uint2(ba, bb);
+        }
+        const bool lja = VDW && iHasLJ && (la.x != 0.f);
+        const bool ljb = VDW && iHasLJ && (lb.x != 0.f);
+        const unsigned char ka = (unsigned char)(e * kClusterSize + q);
+        const unsigned char kb = (unsigned char)(e * kClusterSize + q + 4);
+        unsigned m = __ballot_sync(0xffffffffu, ina && lja) & gmask;
+        if (ina && lja) W.qlj[il][nLJ + __popc(m & lt)] = ka;
+        nLJ += __popc(m);
+        m = __ballot_sync(0xffffffffu, inb && ljb) & gmask;
+        if (inb && ljb) W.qlj[il][nLJ + __popc(m & lt)] = kb;
+        nLJ += __popc(m);
+        m = __ballot_sync(0xffffffffu, ina && !lja) & gmask;
+        if (ina && !lja) W.qn[il][nN + __popc(m & lt)] = ka;
+        nN += __popc(m);
+        m = __ballot_sync(0xffffffffu, inb && !ljb) & gmask;
+        if (inb && !ljb) W.qn[il][nN + __popc(m & lt)] = kb;
+        nN += __popc(m);
+      }
+      __syncwarp();
+      const int nTot = nLJ + nN;
+      if (q == 0) npair += nTot;
+      const int R = (int)__reduce_max_sync(0xffffffffu, (unsigned)((nTot + 3) >> 2));
+      const int RL = (int)__reduce_max_sync(0xffffffffu, (unsigned)((nLJ + 3) >> 2));
+      // ---- compute ----------------------------------------------------------
+      for (int r = 0; r < R; ++r) {
+        const int kq = 4 * r + q;
+        const bool active = kq < nTot;
+        int key = 0;
+        if (active) key = (kq < nLJ) ? W.qlj[il][kq] : W.qn[il][kq - nLJ];
+        const float4 sh = W.es[key >> 3];
+        const float4 xj = W.xs[key];
+        const float dx = xj.x + (sh.x - xi.x), dy = xj.y + (sh.y - xi.y),
+                    dz = xj.z + (sh.z - xi.z);
+        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+        const float r2s = active ? r2 : 1.0f;
+        const float rinv = rsqrt_approx(r2s);
+        const float rr = r2s * rinv;
+        const float qq = active ? xi.w * xj.w : 0.f;
+        const float t = rcp_approx(fmaf(c.p_alpha, rr, 1.0f));
+        const float ex = ex2_approx(-c.c_ex * r2s);
+        float poly = fmaf(kErfcC7, t, kErfcC6);
+        poly = fmaf(poly, t, kErfcC5);
+        poly = fmaf(poly, t, kErfcC4);
+        poly = fmaf(poly, t, kErfcC3);
+        poly = fmaf(poly, t, kErfcC2);
+        poly = fmaf(poly, t, kErfcC1);
+        poly = fmaf(poly, t, kErfcC0);
+        const float e_c = qq * rinv * (t * poly * ex);
+        const float de_c = -fmaf(qq * c.two_a_sqrtpi, ex, e_c) * rinv;
+        ec += e_c;
+        vc = fmaf(de_c, rr, vc);
+        float F = de_c;
+        if (VDW && r < RL) {
+          const float2 ljj = W.ls[key];
+          const float eps = active ? li.x * ljj.x : 0.f;
+          const float sg = (li.y + ljj.y) * rinv;
+          const float s2 = sg * sg;
+          const float s6 = s2 * s2 * s2;
+          const float s12 = s6 * s6;
+          const float pv = eps * (s12 - s6);
+          const float dpv = eps * fmaf(-12.f, s12, 6.f * s6);
+          const bool sw = r2s > c.ron2;
+          const float s1 = c.rc2 - r2s;
+          const float S = sw ? s1 * s1 * fmaf(c.sw_a, r2s, c.sw_b) : 1.f;
+          const float dS = sw ? c.sw_c * r2s * s1 * (c.ron2 - r2s) : 0.f;
+          const float de_v = fmaf(pv, dS, dpv * S) * rinv;
+          ev = fmaf(pv, S, ev);
+          vv = fmaf(de_v, rr, vv);
+          F += de_v;
+        }
+        F *= rinv;
+        const float fx = F * dx, fy = F * dy, fz = F * dz;
+        fix += fx;
+        fiy += fy;
+        fiz += fz;
+        if (active) W.fst[key][il] = make_float4(fx, fy, fz, 0.f);
+      }
+      __syncwarp();
+      // ---- j forces: sum the stored pair forces of each j atom in i order ----
+      for (int key = lane; key < nEnt * kClusterSize; key += 32) {
+        const int e = key >> 3, jl = key & 7;
+        const uint2 im = W.inm[e];
+        const unsigned row = ((jl < 4) ? (im.x >> (8 * jl)) : (im.y >> (8 * (jl - 4)))) & 0xffu;
+        if (row == 0u) continue;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+#pragma unroll
+        for (int ii = 0; ii < kClusterSize; ++ii) {
+          if ((row >> ii) & 1u) {
+            const float4 f = W.fst[key][ii];
+            sx += f.x;
+            sy += f.y;
+            sz += f.z;
+          }
+        }
+        overflow |= !(fabsf(sx) < kForceLimitF && fabsf(sy) < kForceLimitF &&
+                      fabsf(sz) < kForceLimitF);
+        const int slot = W.ej[e] * kClusterSize + jl;
+        red_add(facc + slot, fix_f(-sx));
+        red_add(facc + (size_t)nSlots + slot, fix_f(-sy));
+        red_add(facc + 2 * (size_t)nSlots + slot, fix_f(-sz));
+      }
+      __syncwarp();
+    }
+    // i forces: sum over the four lanes of each i atom
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (q < 3) {
+      const float v = (q == 0) ? fix : (q == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)q * nSlots + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    Ec += fix_e(warp_sum_d((double)ec));
+    Ev += fix_e(warp_sum_d((double)ev));
+    Vc += fix_e(warp_sum_d((double)vc));
+    Vv += fix_e(warp_sum_d((double)vv));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    red_add(acc + ACC_NPAIR, npair);
+  }
+}
+
 // Exclusion correction in FP64 (src/energy.c:567-621, ewald_corr
 // src/ewald.c:371-384) into the fixed-point accumulators.
 __global__ void __launch_bounds__(128)
@@ -293,16 +515,45 @@ PairConstF make_pair_const(const PairParams &p) {
   return c;
 }
 
-int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s) {
+int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
+                     int variant) {
   const PairConstF c = make_pair_const(p);
   if (w.nItems <= 0) return MDBAS_NB_OK;
+  if (variant == kPairDense) {
+    if (p.vdwSwitch)
+      MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),
+                 w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+                 w.acc.as<long long>());
+    else
+      MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, w.counters.as<long long>(),
+                 w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+                 w.acc.as<long long>());
+    return MDBAS_NB_OK;
+  }
+  // compacted variant: fixed block of kCWarps warps, dynamic shared memory
+  const size_t smem = sizeof(CompactWarp) * kCWarps;
+  static bool attr_set[64][2];
+  int dev = 0;
+  MDB_CUDA(cudaGetDevice(&dev));
+  if (dev >= 0 && dev < 64 && !attr_set[dev][p.vdwSwitch ? 1 : 0]) {
+    if (p.vdwSwitch)
+      MDB_CUDA(cudaFuncSetAttribute(k_pair_fp32c<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    else
+      MDB_CUDA(cudaFuncSetAttribute(k_pair_fp32c<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_set[dev][p.vdwSwitch ? 1 : 0] = true;
+  }
+  const int cgrid = grid * block / (kCWarps * 32);
   if (p.vdwSwitch)
-    MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),
+    MDB_LAUNCH(k_pair_fp32c<true>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
                w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
                w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
                w.acc.as<long long>());
   else
-    MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, w.counters.as<long long>(),
+    MDB_LAUNCH(k_pair_fp32c<false>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
                w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
                w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
                w.acc.as<long long>());

@@ -16,9 +16,15 @@ struct PairConstF {
 };
 
 PairConstF make_pair_const(const PairParams &p);
+// Pair kernel variants: dense (all 64 pairs of an entry per warp step) and
+// compacted (only in-cut-off pairs reach the interaction arithmetic).
+enum { kPairDense = 0, kPairCompact = 1 };
 // The pair kernel over all work items (grid-stride, item count read on the
-// device, so the launch needs no host synchronisation).
-int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s);
+// device, so the launch needs no host synchronisation).  grid*block is the
+// number of threads of the dense variant; the compacted one uses the same
+// number of warps.
+int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
+                     int variant = kPairDense);
 int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
                     const int *exclStart, const int *exclFlat, const double *x, const double *y,
                     const double *z, const double *q, cudaStream_t s);

@@ -209,6 +209,7 @@ def lib():
     L.mdbas_nb_engine_launch_count.restype = C.c_longlong
     L.mdbas_nb_engine_launch_count.argtypes = [C.c_void_p]
     L.mdbas_nb_engine_set_timing.argtypes = [C.c_void_p, C.c_int]
+    L.mdbas_nb_engine_set_variant.argtypes = [C.c_void_p, C.c_int]
     L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
     L.mdbas_nb_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -326,6 +327,10 @@ class Engine:
 
     def launches(self) -> int:
         return int(lib().mdbas_nb_engine_launch_count(self.h))
+
+    def set_variant(self, variant: int):
+        """Pair kernel: 0 = dense 8x8 (default), 1 = filtered and compacted."""
+        check(lib().mdbas_nb_engine_set_variant(self.h, variant), "engine_set_variant")
 
     def set_timing(self, on: bool):
         check(lib().mdbas_nb_engine_set_timing(self.h, 1 if on else 0), "engine_set_timing")

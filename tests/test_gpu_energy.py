@@ -168,3 +168,19 @@ def test_refresh_between_builds(gpu):
     assert force_rel_rms(f_ref, f_new) < 2 * MIXED_FORCE_TOL
     assert e_ref["n_pairs"] == e_new["n_pairs"]
     eng.close()
+
+
+def test_pair_kernel_variants_agree(gpu):
+    s = systems.water_box_for_atoms(18558, 3)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    out = {}
+    for v in (0, 1):
+        eng.set_variant(v)
+        eng.compute()
+        out[v] = (eng.forces(), eng.energies())
+    assert force_rel_rms(out[1][0], out[0][0]) < 2e-6
+    assert out[1][1]["n_pairs"] == out[0][1]["n_pairs"]
+    e0, e1 = out[0][1], out[1][1]
+    assert abs(e1["elec_direct"] - e0["elec_direct"]) <= 1e-6 * abs(e0["elec_direct"])
+    eng.close()
