@@ -207,6 +207,9 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
 // ---------------------------------------------------------------------------
 // Compacted variant.  Same work items, entries and results as k_pair_fp32,
 // but only in-cut-off pairs reach the expensive arithmetic:
+//   staging: a chunk of 8 entries and their 64 j atoms are loaded into shared
+//     memory in one batch, so all global loads of a chunk are in flight
+//     together;
 //   filter: per entry the warp tests its 64 pairs (r^2 <= rc^2 and the mask
 //     bit) and appends the survivors to per-i-atom queues in shared memory
 //     (ballot + prefix count inside each group of 4 lanes that share an i
@@ -227,6 +230,7 @@ constexpr int kCWarps = 4;   // warps per block
 
 struct CompactWarp {
   int ej[kChunk];
+  uint2 em[kChunk];                                   // list masks per entry
   uint2 inm[kChunk];                                  // in-cut-off bits per entry
   float4 es[kChunk];                                  // FP32 shift per entry
   float4 xs[kChunk * kClusterSize];                   // staged j atoms
@@ -237,7 +241,7 @@ struct CompactWarp {
 };
 
 template <bool VDW>
-__global__ void __launch_bounds__(kCWarps * 32, 4)
+__global__ void __launch_bounds__(kCWarps * 32, 5)
 k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ items,
              const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
              const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
@@ -264,36 +268,39 @@ k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ it
     float ec = 0.f, ev = 0.f, vc = 0.f, vv = 0.f;
     for (int c0 = 0; c0 < ne; c0 += kChunk) {
       const int nEnt = min(kChunk, ne - c0);
+      // ---- stage the chunk's entries and j atoms in shared memory ----------
+      if (lane < nEnt) {
+        const CPairEntry en = entries[e0 + c0 + lane];
+        W.ej[lane] = en.j;
+        W.es[lane] = make_float4(en.sx, en.sy, en.sz, 0.f);
+        W.em[lane] = masks[e0 + c0 + lane];
+      }
+      __syncwarp();
+      for (int a = lane; a < nEnt * kClusterSize; a += 32) {
+        const int slot = W.ej[a >> 3] * kClusterSize + (a & 7);
+        W.xs[a] = xq[slot];
+        W.ls[a] = lj[slot];
+      }
+      __syncwarp();
       // ---- filter ---------------------------------------------------------
       int nLJ = 0, nN = 0;
       for (int e = 0; e < nEnt; ++e) {
-        const CPairEntry en = entries[e0 + c0 + e];
-        const uint2 mk = masks[e0 + c0 + e];
-        const int jb = en.j * kClusterSize + q;
-        const float4 xa = xq[jb];
-        const float2 la = lj[jb];
-        const float4 xb = xq[jb + 4];
-        const float2 lb = lj[jb + 4];
-        if (il == 0) {
-          W.xs[e * kClusterSize + q] = xa;
-          W.xs[e * kClusterSize + q + 4] = xb;
-          W.ls[e * kClusterSize + q] = la;
-          W.ls[e * kClusterSize + q + 4] = lb;
-        }
-        const float sx = en.sx - xi.x, sy = en.sy - xi.y, sz = en.sz - xi.z;
+        const float4 esh = W.es[e];
+        const uint2 mk = W.em[e];
+        const float4 xa = W.xs[e * kClusterSize + q];
+        const float4 xb = W.xs[e * kClusterSize + q + 4];
+        const float la = W.ls[e * kClusterSize + q].x;
+        const float lb = W.ls[e * kClusterSize + q + 4].x;
+        const float sx = esh.x - xi.x, sy = esh.y - xi.y, sz = esh.z - xi.z;
         const float ax = xa.x + sx, ay = xa.y + sy, az = xa.z + sz;
         const float bx = xb.x + sx, by = xb.y + sy, bz = xb.z + sz;
         const bool ina = ((mk.x >> lane) & 1u) && (fmaf(ax, ax, fmaf(ay, ay, az * az)) <= c.rc2);
         const bool inb = ((mk.y >> lane) & 1u) && (fmaf(bx, bx, fmaf(by, by, bz * bz)) <= c.rc2);
         const unsigned ba = __ballot_sync(0xffffffffu, ina);
         const unsigned bb = __ballot_sync(0xffffffffu, inb);
-        if (lane == 0) {
-          W.ej[e] = en.j;
-          W.es[e] = make_float4(en.sx, en.sy, en.sz, 0.f);
-          W.inm[e] = make_uint2(ba, bb);
-        }
-        const bool lja = VDW && iHasLJ && (la.x != 0.f);
-        const bool ljb = VDW && iHasLJ && (lb.x != 0.f);
+        if (lane == 0) W.inm[e] = make_uint2(ba, bb);
+        const bool lja = VDW && iHasLJ && (la != 0.f);
+        const bool ljb = VDW && iHasLJ && (lb != 0.f);
         const unsigned char ka = (unsigned char)(e * kClusterSize + q);
         const unsigned char kb = (unsigned char)(e * kClusterSize + q + 4);
         unsigned m = __ballot_sync(0xffffffffu, ina && lja) & gmask;

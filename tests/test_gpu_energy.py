@@ -182,5 +182,7 @@ def test_pair_kernel_variants_agree(gpu):
     assert force_rel_rms(out[1][0], out[0][0]) < 2e-6
     assert out[1][1]["n_pairs"] == out[0][1]["n_pairs"]
     e0, e1 = out[0][1], out[1][1]
-    assert abs(e1["elec_direct"] - e0["elec_direct"]) <= 1e-6 * abs(e0["elec_direct"])
+    # the direct sum cancels heavily; compare on the scale of the total
+    scale = abs(e0["elec_direct"] + e0["elec_corr"])
+    assert abs(e1["elec_direct"] - e0["elec_direct"]) <= 1e-6 * scale
     eng.close()
