@@ -57,6 +57,10 @@ def _parse():
     p.add_argument("--seed", type=int, default=1)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--precision-seeds", type=int, default=10)
+    p.add_argument("--md-steps", type=int, default=1000,
+                   help="timed velocity-Verlet steps (1 fs, rigid water) for ns/day")
+    p.add_argument("--nve-steps", type=int, default=10000,
+                   help="NVE steps (1 fs) for the energy-drift report; 0 skips it")
     return p.parse_args()
 
 
@@ -235,6 +239,66 @@ def _time_steps(torch, eng, stream, flush, steps, fn):
     return [a.elapsed_time(b) for a, b in evs]
 
 
+def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_steps, world):
+    """Velocity-Verlet dynamics of the 96k water box (rigid SHAKE/RATTLE
+    water, list rebuilt on half-skin displacement).  The lattice-plus-jitter
+    start is relaxed first (2,000 Berendsen steps at 0.5 fs toward 300 K,
+    untimed); then `steps` 1 fs NVE steps are timed with CUDA events on the
+    engine stream, and `nve_steps` more give the energy drift."""
+    import numpy as np
+    s = systems.config_96k(seed=seed, temperature=300.0)
+    cons = s.water_constraints()
+    e = nb.Engine(s, precision=precision, device=dev)
+    e.set_stream(stream.cuda_stream)
+    e.md_init(s.mass, (s.vx, s.vy, s.vz), time_step=0.0005, list_update=0, constraints=cons)
+    e.md_run(2000, target_temp=300.0, tau_t=0.05)
+    pos, vel = e.positions(), e.velocities()
+    e.set_positions(*pos)
+    e.md_init(s.mass, vel, time_step=0.001, list_update=0, constraints=cons)
+    e.md_run(20)
+    st0 = e.md_stats()
+    launches0 = e.launches()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    e.md_run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    st1 = e.md_stats()
+    out = {"ms_per_step": ms, "ns_per_day": 86400.0 / (ms * 1e-3) * 1e-6,
+           "time_step_fs": 1.0, "steps_timed": steps,
+           "list_builds_per_step": (st1["rebuilds"] - st0["rebuilds"]) / steps,
+           "launches_per_step": (e.launches() - launches0) / steps,
+           "constraints": "rigid water, SHAKE/RATTLE tol 1e-8",
+           "start": "2,000 Berendsen steps (0.5 fs, tau 0.05 ps, 300 K) from the lattice start"}
+    if nve_steps > 0:
+        every = 100
+        rows = e.md_run(nve_steps, energy_every=every)
+        n = s.n
+        ndf = 3 * n - len(cons[1]) - 3
+        tot, kin = rows[:, 3], rows[:, 2]
+        kT = 2.0 * float(np.mean(kin)) / ndf
+        t_ns = nve_steps * 1e-6
+        slope = float(np.polyfit(rows[:, 0] * 1e-6, tot, 1)[0])  # per ns
+        out["nve"] = {
+            "steps": nve_steps, "time_step_fs": 1.0, "energy_every": every,
+            "temperature_K": kT / 0.83144621,
+            "drift_kT_per_dof_per_ns": slope / (ndf * kT),
+            "total_first_last_kcal_mol": [float(tot[0]) / 418.4, float(tot[-1]) / 418.4],
+            "max_dev_over_kin": float((tot.max() - tot.min()) / np.mean(kin)),
+            "rebuilds": e.md_stats()["rebuilds"] - st1["rebuilds"],
+            "simulated_ns": t_ns}
+    e.close()
+    return out
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -387,6 +451,14 @@ def run_ours(args, rank, world):
                 "energy_rel_max": max(eerr), "seeds": args.precision_seeds,
                 "against": "plain FP64 GPU form (itself within 1e-12 of MDBas)"}
 
+    # ---- velocity-Verlet dynamics: ns/day, mixed and FP64 forms -----------
+    md = md64 = None
+    if args.md_steps > 0:
+        md = md_measure(torch, nb, systems, dev, stream, args.seed + rank, 1, args.md_steps,
+                        args.nve_steps, world)
+        md64 = md_measure(torch, nb, systems, dev, stream, args.seed + rank, 0,
+                          max(50, args.md_steps // 5), 0, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args.seed)
@@ -404,7 +476,9 @@ def run_ours(args, rank, world):
                        "step": "cluster-pair list build + forces/energy/virial",
                        "l2": "flushed before every timed step (256 MiB write)",
                        "parallelism": f"replicas x{world}"},
-            "ns_per_day": 86400.0 / (t_step * 1e-3) * FS_PER_STEP * 1e-6,
+            "ns_per_day": md["ns_per_day"] if md else None,
+            "md": md,
+            "md_fp64_form": md64,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
                             "variant": "dense 8x8", "compacted_variant_ms": compact_ms},
             "list_build": {"ms": t_build,

@@ -411,6 +411,42 @@ int mdbas_nb_engine_set_timing(mdbas_nb_engine *e, int enable);
 int mdbas_nb_engine_kernel_time(mdbas_nb_engine *e, int which, double *avg_ms, long long *count,
                                 int reset);
 
+/* ------------------------------------------------------------------------ */
+/* 4. Device-resident velocity-Verlet dynamics                               */
+/*    (replaces the loop src/mdbas.c:244-300 over vv_integrate,               */
+/*    src/integrate.c:1518-1634 vv_nve / 1636-1750 vv_nvt_b, with SHAKE and   */
+/*    RATTLE of src/shake.c:209-456, makelist and energy)                    */
+/* ------------------------------------------------------------------------ */
+/* Start dynamics from the engine's current positions.  mass in MDBas units
+ * (amu); velocities in A/ps (NULL = zero); timeStep in ps.  listUpdate > 0
+ * rebuilds the list every listUpdate steps (MDBas's "list" keyword);
+ * listUpdate = 0 rebuilds when an atom has moved more than delr/2 since the
+ * last build.  Constraints: nConst pairs (constAtoms[2k], constAtoms[2k+1])
+ * at squared length constLen2[k] (A^2), solved per molecule with MDBas's
+ * SHAKE/RATTLE iteration (tolShake <= 0 -> 1e-8, maxCycle <= 0 -> 150);
+ * a constrained molecule holds at most 16 atoms and 32 constraints.
+ * Evaluates the forces at the start positions. */
+int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double *vx,
+                            const double *vy, const double *vz, double timeStep, int listUpdate,
+                            int nConst, const int *constAtoms, const double *constLen2,
+                            double tolShake, int maxCycle);
+/* Advance nSteps steps.  tauT > 0 applies MDBas's Berendsen scaling toward
+ * targetTemp (K) after the second half kick (vv_nvt_b); tauT <= 0 is NVE.
+ * Every energyEvery steps (if energies != NULL) a row {step, potential,
+ * kinetic, total} (internal units; potential = the nonbonded real-space
+ * terms plus the Ewald self term) is appended to energies.  Returns
+ * MDBAS_NB_ERR_UNSUPPORTED if SHAKE did not converge (CONVERG_SHAKE_ERROR). */
+int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, double targetTemp,
+                           double tauT, double *energies);
+/* out[0] steps taken, out[1] list builds, out[2] largest SHAKE iteration
+ * count of the last md_run, out[3] constrained molecules. */
+int mdbas_nb_engine_md_stats(mdbas_nb_engine *e, long long out[4]);
+/* Current positions / velocities (original atom order). */
+int mdbas_nb_engine_get_positions(mdbas_nb_engine *e, double *x, double *y, double *z,
+                                  int device_ptrs);
+int mdbas_nb_engine_get_velocities(mdbas_nb_engine *e, double *vx, double *vy, double *vz,
+                                   int device_ptrs);
+
 /* Measured FP32 FFMA throughput of a device (TFLOP/s, 2 flops per FFMA), the
  * peak the FP32 pair kernel's roofline fraction is quoted against; ms gets the
  * probe kernel's duration. */

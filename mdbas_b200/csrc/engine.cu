@@ -131,11 +131,6 @@ PairParams make_params(double cutOff, double cutOn, double alpha, double chargeC
     }                                                                          \
   } while (0)
 
-struct LaunchScope {
-  explicit LaunchScope(mdbas_nb_engine *e) { g_launch_counter = &e->launches; }
-  ~LaunchScope() { g_launch_counter = nullptr; }
-};
-
 static int set_dev(mdbas_nb_engine *e) {
   MDB_CUDA(cudaSetDevice(e->device));
   return MDBAS_NB_OK;

@@ -38,9 +38,25 @@ struct mdbas_nb_engine {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double pairMs = 0.0;
   long long pairCount = 0;
+  // velocity-Verlet state (md.cu)
+  mdbas::DBuf mdMass, mdRmass, mdV, mdF, mdXb, mdWord;
+  mdbas::DBuf mdCa, mdCb, mdRc2, mdMol, mdNAt, mdDd;
+  int mdNCons = 0, mdNMol = 0, mdListUpdate = 0, mdMaxCycle = 150, mdDegFree = 0;
+  double mdDt = 0.0, mdTol = 1e-8;
+  long long mdSteps = 0, mdRebuilds = 0, mdShakeIter = 0;
+  bool mdReady = false;
 };
 
 namespace mdbas {
+// Counts the library's kernel launches into an engine for the lifetime of
+// the scope; nested scopes restore the outer counter.
+struct LaunchScope {
+  long long *prev;
+  explicit LaunchScope(mdbas_nb_engine *e) : prev(g_launch_counter) {
+    g_launch_counter = &e->launches;
+  }
+  ~LaunchScope() { g_launch_counter = prev; }
+};
 int engine_check_device(int device);
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);

@@ -1,0 +1,638 @@
+// md.cu -- device-resident velocity-Verlet dynamics (mdbas_nb_engine_md_*).
+//
+// One step restates MDBas's VV-NVE step (vv_nve, src/integrate.c:1518-1634,
+// driven as in src/mdbas.c:244-300):
+//   stage 1: v += dt/2 f/m, x += dt v, then SHAKE on positions (vv_shake_r,
+//            src/shake.c:209-326) with the constraint vectors taken before
+//            the drift (image_array, src/integrate.c:1542-1553);
+//   list:    rebuilt every `listUpdate` steps (MDBas's fixed `list N` cadence,
+//            src/list.c:87-105) or, with listUpdate = 0, when some atom moved
+//            more than half the skin since the last build (the displacement
+//            criterion is new behaviour);
+//   forces:  the engine's nonbonded evaluation (either precision form);
+//   stage 2: v += dt/2 f/m, SHAKE on velocities (vv_shake_v,
+//            src/shake.c:328-456), kinetic energy (kinetic, src/utils.c:502),
+//            positions wrapped into the box (image_update).
+// Everything stays on the GPU; the host only reads one word per step (the
+// displacement test) and the energies when asked.
+//
+// Constraints are solved molecule by molecule (connected components of the
+// constraint graph, one thread each) with MDBas's iteration: every constraint
+// of the molecule contributes a correction, atoms take the average over the
+// constraints they belong to (nAtConst), until the largest relative bond
+// error is below tolShake.  MDBas iterates all molecules together until the
+// worst one converges; here each molecule stops when it has converged, which
+// changes the positions only within tolShake.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "engine.cuh"
+#include "list_ref.cuh"
+#include "pair_fp32.cuh"
+
+using namespace mdbas;
+
+namespace mdbas {
+namespace {
+
+constexpr int kMolMaxAtoms = 16;
+constexpr int kMolMaxCons = 32;
+
+// stage 1 of vv_nve: half kick then drift (src/integrate.c:1555-1580)
+__global__ void k_vv_stage1(int n, double dt, const double *__restrict__ fx,
+                            const double *__restrict__ fy, const double *__restrict__ fz,
+                            const double *__restrict__ rmass, double *__restrict__ vx,
+                            double *__restrict__ vy, double *__restrict__ vz,
+                            double *__restrict__ x, double *__restrict__ y,
+                            double *__restrict__ z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vx[i] += 0.5 * dt * fx[i] * rmass[i];
+  vy[i] += 0.5 * dt * fy[i] * rmass[i];
+  vz[i] += 0.5 * dt * fz[i] * rmass[i];
+  x[i] += dt * vx[i];
+  y[i] += dt * vy[i];
+  z[i] += dt * vz[i];
+}
+
+__global__ void k_vv_kick(int n, double dt, const double *__restrict__ fx,
+                          const double *__restrict__ fy, const double *__restrict__ fz,
+                          const double *__restrict__ rmass, double *__restrict__ vx,
+                          double *__restrict__ vy, double *__restrict__ vz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  vx[i] += 0.5 * dt * fx[i] * rmass[i];
+  vy[i] += 0.5 * dt * fy[i] * rmass[i];
+  vz[i] += 0.5 * dt * fz[i] * rmass[i];
+}
+
+// constraint vectors before the drift, minimum image (dist2, src/utils.c:82)
+__global__ void k_cons_vectors(int nc, DevBox b, const int *__restrict__ ca,
+                               const int *__restrict__ cb, const double *__restrict__ x,
+                               const double *__restrict__ y, const double *__restrict__ z,
+                               double *__restrict__ ddx, double *__restrict__ ddy,
+                               double *__restrict__ ddz) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nc) return;
+  double dx = x[cb[c]] - x[ca[c]], dy = y[cb[c]] - y[ca[c]], dz = z[cb[c]] - z[ca[c]];
+  dist_d(b, dx, dy, dz);
+  ddx[c] = dx;
+  ddy[c] = dy;
+  ddz[c] = dz;
+}
+
+// Per-molecule SHAKE on positions and velocities (vv_shake_r).
+__global__ void k_shake_positions(int nMol, DevBox b, double dt, double tol, int maxCycle,
+                                  const int *__restrict__ molCons, const int *__restrict__ ca,
+                                  const int *__restrict__ cb, const double *__restrict__ rc2,
+                                  const double *__restrict__ ddx, const double *__restrict__ ddy,
+                                  const double *__restrict__ ddz,
+                                  const double *__restrict__ rmass,
+                                  const int *__restrict__ nAtConst, double *__restrict__ x,
+                                  double *__restrict__ y, double *__restrict__ z,
+                                  double *__restrict__ vx, double *__restrict__ vy,
+                                  double *__restrict__ vz, int *__restrict__ status) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nMol) return;
+  const int c0 = molCons[m], c1 = molCons[m + 1];
+  const int ncons = c1 - c0;
+  if (ncons <= 0) return;
+  if (ncons > kMolMaxCons) {
+    atomicOr(status, 2);
+    return;
+  }
+  // local atom table of the molecule
+  int atoms[kMolMaxAtoms];
+  int na = 0;
+  int la[kMolMaxCons], lb[kMolMaxCons];
+  for (int k = 0; k < ncons; ++k) {
+    const int a = ca[c0 + k], bb = cb[c0 + k];
+    int ia = -1, ib = -1;
+    for (int t = 0; t < na; ++t) {
+      if (atoms[t] == a) ia = t;
+      if (atoms[t] == bb) ib = t;
+    }
+    if (ia < 0) {
+      if (na >= kMolMaxAtoms) { atomicOr(status, 2); return; }
+      ia = na;
+      atoms[na++] = a;
+    }
+    if (ib < 0) {
+      if (na >= kMolMaxAtoms) { atomicOr(status, 2); return; }
+      ib = na;
+      atoms[na++] = bb;
+    }
+    la[k] = ia;
+    lb[k] = ib;
+  }
+  double xt[kMolMaxAtoms], yt[kMolMaxAtoms], zt[kMolMaxAtoms];
+  double rt2[kMolMaxCons], tx[kMolMaxCons], ty[kMolMaxCons], tz[kMolMaxCons];
+  bool converged = false;
+  int icycle = 0;
+  do {
+    double maxdist = 0.;
+    for (int k = 0; k < ncons; ++k) {
+      const int a = atoms[la[k]], bb = atoms[lb[k]];
+      double dx = x[bb] - x[a], dy = y[bb] - y[a], dz = z[bb] - z[a];
+      rt2[k] = dist_d(b, dx, dy, dz);
+      tx[k] = dx;
+      ty[k] = dy;
+      tz[k] = dz;
+      const double dist = fabs(rt2[k] - rc2[c0 + k]) / sqrt(rc2[c0 + k]);
+      maxdist = fmax(maxdist, dist);
+    }
+    maxdist = 0.5 * maxdist;
+    if (maxdist < tol) converged = true;
+    if (!converged) {
+      for (int t = 0; t < na; ++t) xt[t] = yt[t] = zt[t] = 0.;
+      for (int k = 0; k < ncons; ++k) {
+        const int c = c0 + k;
+        const int a = atoms[la[k]], bb = atoms[lb[k]];
+        const double trmi = dt * rmass[a];
+        const double trmj = dt * rmass[bb];
+        const double lambda = -(rc2[c] - rt2[k]) /
+                              (dt * (trmi + trmj) * ((ddx[c] * tx[k]) + (ddy[c] * ty[k]) +
+                                                     (ddz[c] * tz[k])));
+        const double lambdai = 0.5 * lambda * trmi;
+        xt[la[k]] += ddx[c] * lambdai;
+        yt[la[k]] += ddy[c] * lambdai;
+        zt[la[k]] += ddz[c] * lambdai;
+        const double lambdaj = -0.5 * lambda * trmj;
+        xt[lb[k]] += ddx[c] * lambdaj;
+        yt[lb[k]] += ddy[c] * lambdaj;
+        zt[lb[k]] += ddz[c] * lambdaj;
+      }
+      for (int k = 0; k < ncons; ++k) {
+        const int a = atoms[la[k]], bb = atoms[lb[k]];
+        const double nia = 1.0 / (double)nAtConst[a];
+        const double nib = 1.0 / (double)nAtConst[bb];
+        x[a] += dt * xt[la[k]] * nia;
+        y[a] += dt * yt[la[k]] * nia;
+        z[a] += dt * zt[la[k]] * nia;
+        x[bb] += dt * xt[lb[k]] * nib;
+        y[bb] += dt * yt[lb[k]] * nib;
+        z[bb] += dt * zt[lb[k]] * nib;
+        vx[a] += xt[la[k]] * nia;
+        vy[a] += yt[la[k]] * nia;
+        vz[a] += zt[la[k]] * nia;
+        vx[bb] += xt[lb[k]] * nib;
+        vy[bb] += yt[lb[k]] * nib;
+        vz[bb] += zt[lb[k]] * nib;
+      }
+    }
+    ++icycle;
+  } while (!converged && icycle < maxCycle);
+  if (!converged) atomicOr(status, 1);  // CONVERG_SHAKE_ERROR
+  atomicMax(status + 1, icycle);
+}
+
+// Per-molecule SHAKE on velocities (vv_shake_v).
+__global__ void k_shake_velocities(int nMol, double dt, double tolvel, int maxCycle,
+                                   const int *__restrict__ molCons, const int *__restrict__ ca,
+                                   const int *__restrict__ cb, const double *__restrict__ ddx,
+                                   const double *__restrict__ ddy,
+                                   const double *__restrict__ ddz,
+                                   const double *__restrict__ rmass,
+                                   const int *__restrict__ nAtConst, double *__restrict__ vx,
+                                   double *__restrict__ vy, double *__restrict__ vz,
+                                   int *__restrict__ status) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nMol) return;
+  const int c0 = molCons[m], c1 = molCons[m + 1];
+  const int ncons = c1 - c0;
+  if (ncons <= 0 || ncons > kMolMaxCons) return;
+  int atoms[kMolMaxAtoms];
+  int na = 0;
+  int la[kMolMaxCons], lb[kMolMaxCons];
+  for (int k = 0; k < ncons; ++k) {
+    const int a = ca[c0 + k], bb = cb[c0 + k];
+    int ia = -1, ib = -1;
+    for (int t = 0; t < na; ++t) {
+      if (atoms[t] == a) ia = t;
+      if (atoms[t] == bb) ib = t;
+    }
+    if (ia < 0) {
+      if (na >= kMolMaxAtoms) return;
+      ia = na;
+      atoms[na++] = a;
+    }
+    if (ib < 0) {
+      if (na >= kMolMaxAtoms) return;
+      ib = na;
+      atoms[na++] = bb;
+    }
+    la[k] = ia;
+    lb[k] = ib;
+  }
+  double xt[kMolMaxAtoms], yt[kMolMaxAtoms], zt[kMolMaxAtoms];
+  bool converged = false;
+  int icycle = 0;
+  do {
+    for (int t = 0; t < na; ++t) xt[t] = yt[t] = zt[t] = 0.;
+    double maxdist = 0.;
+    for (int k = 0; k < ncons; ++k) {
+      const int c = c0 + k;
+      const int a = atoms[la[k]], bb = atoms[lb[k]];
+      const double trmi = 0.5 * dt * rmass[a];
+      const double trmj = 0.5 * dt * rmass[bb];
+      const double lambda =
+          (ddx[c] * (vx[bb] - vx[a]) + ddy[c] * (vy[bb] - vy[a]) + ddz[c] * (vz[bb] - vz[a])) /
+          ((trmi + trmj) * (ddx[c] * ddx[c] + ddy[c] * ddy[c] + ddz[c] * ddz[c]));
+      maxdist = fmax(maxdist, fabs(lambda));
+      const double lambdai = lambda * trmi;
+      xt[la[k]] += ddx[c] * lambdai;
+      yt[la[k]] += ddy[c] * lambdai;
+      zt[la[k]] += ddz[c] * lambdai;
+      const double lambdaj = -lambda * trmj;
+      xt[lb[k]] += ddx[c] * lambdaj;
+      yt[lb[k]] += ddy[c] * lambdaj;
+      zt[lb[k]] += ddz[c] * lambdaj;
+    }
+    if (maxdist < tolvel) converged = true;
+    if (!converged) {
+      for (int k = 0; k < ncons; ++k) {
+        const int a = atoms[la[k]], bb = atoms[lb[k]];
+        const double nia = 1.0 / (double)nAtConst[a];
+        const double nib = 1.0 / (double)nAtConst[bb];
+        vx[a] += xt[la[k]] * nia;
+        vy[a] += yt[la[k]] * nia;
+        vz[a] += zt[la[k]] * nia;
+        vx[bb] += xt[lb[k]] * nib;
+        vy[bb] += yt[lb[k]] * nib;
+        vz[bb] += zt[lb[k]] * nib;
+      }
+    }
+    ++icycle;
+  } while (!converged && icycle < maxCycle);
+  if (!converged) atomicOr(status, 1);
+}
+
+// kinetic energy (src/utils.c:502-515), sum in fixed point (2^-24 units)
+__global__ void k_kinetic(int n, const double *__restrict__ mass, const double *__restrict__ vx,
+                          const double *__restrict__ vy, const double *__restrict__ vz,
+                          long long *__restrict__ acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  long long v = 0;
+  if (i < n) v = fix_e(0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) red_add(acc, v);
+}
+
+// largest squared displacement since the last build (minimum image), as the
+// bit pattern of a non-negative double (which orders like the double)
+__global__ void k_max_disp(int n, DevBox b, const double *__restrict__ x,
+                           const double *__restrict__ y, const double *__restrict__ z,
+                           const double *__restrict__ xb, const double *__restrict__ yb,
+                           const double *__restrict__ zb, unsigned long long *__restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double r2 = 0.;
+  if (i < n) {
+    double dx = x[i] - xb[i], dy = y[i] - yb[i], dz = z[i] - zb[i];
+    r2 = dist_d(b, dx, dy, dz);
+    if (!(r2 == r2)) r2 = 1e300;  // NaN forces a rebuild (which reports it)
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(r2));
+}
+
+// frozen atoms keep zero force and velocity (freeze_atoms, src/utils.c:131-150)
+__global__ void k_freeze(int n, const int *__restrict__ frozen, double *__restrict__ f,
+                         double *__restrict__ v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !frozen[i]) return;
+  f[i] = f[n + i] = f[2 * (size_t)n + i] = 0.;
+  v[i] = v[n + i] = v[2 * (size_t)n + i] = 0.;
+}
+
+// Berendsen scaling of vv_nvt_b (src/integrate.c:1722-1733): every thread
+// derives lambda from the kinetic energy summed on the device.
+__global__ void k_berendsen(int n, double dtOverTau, double kinTemp0,
+                            const long long *__restrict__ kfix, double *__restrict__ vx,
+                            double *__restrict__ vy, double *__restrict__ vz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double kin = (double)(*kfix) / kEnergyScale;
+  if (!(kin > 0.)) return;
+  const double lambda = sqrt(1.0 + dtOverTau * (kinTemp0 / kin - 1.0));
+  vx[i] *= lambda;
+  vy[i] *= lambda;
+  vz[i] *= lambda;
+}
+
+}  // namespace
+}  // namespace mdbas
+
+#define MD_TRY(expr)                                                           \
+  do {                                                                         \
+    int s__ = (expr);                                                          \
+    if (s__ != MDBAS_NB_OK) {                                                  \
+      set_last_status(s__, nullptr);                                           \
+      return s__;                                                              \
+    }                                                                          \
+  } while (0)
+
+namespace {
+
+// FP64 forces of the last compute, caller order, into e->mdF (3n).
+int md_forces(mdbas_nb_engine *e) {
+  const int n = e->n;
+  if (e->cfg.precision == 0) {
+    MDB_CUDA(cudaMemcpyAsync(e->mdF.p, e->f64.p, sizeof(double) * 3 * (size_t)n,
+                             cudaMemcpyDeviceToDevice, e->stream));
+    if (e->hasFrozen)
+      MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, e->stream, n, e->frozen.as<int>(),
+                 e->mdF.as<double>(), e->mdV.as<double>());
+    return MDBAS_NB_OK;
+  }
+  double *f = e->mdF.as<double>();
+  MDB_TRY(forces_out_launch(e->cl, n, 0, f, f + n, f + 2 * (size_t)n, e->stream));
+  if (e->hasFrozen)
+    MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, e->stream, n, e->frozen.as<int>(), f,
+               e->mdV.as<double>());
+  return MDBAS_NB_OK;
+}
+
+int md_build(mdbas_nb_engine *e) {
+  MD_TRY(mdbas_nb_engine_build(e));
+  const size_t bytes = sizeof(double) * (size_t)e->n;
+  MDB_CUDA(cudaMemcpyAsync(e->mdXb.p, e->x.p, bytes, cudaMemcpyDeviceToDevice, e->stream));
+  MDB_CUDA(cudaMemcpyAsync(e->mdXb.as<double>() + e->n, e->y.p, bytes, cudaMemcpyDeviceToDevice,
+                           e->stream));
+  MDB_CUDA(cudaMemcpyAsync(e->mdXb.as<double>() + 2 * (size_t)e->n, e->z.p, bytes,
+                           cudaMemcpyDeviceToDevice, e->stream));
+  e->mdRebuilds += 1;
+  return MDBAS_NB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double *vx,
+                            const double *vy, const double *vz, double timeStep, int listUpdate,
+                            int nConst, const int *constAtoms, const double *constLen2,
+                            double tolShake, int maxCycle) {
+  if (!e || !mass || !(timeStep > 0.) || listUpdate < 0 || nConst < 0) return MDBAS_NB_ERR_ARG;
+  if (!e->topoSet || !e->posSet) return MDBAS_NB_ERR_STATE;
+  if (nConst > 0 && (!constAtoms || !constLen2)) return MDBAS_NB_ERR_ARG;
+  MDB_CUDA(cudaSetDevice(e->device));
+  const int n = e->n;
+  std::vector<double> rm(n);
+  for (int i = 0; i < n; ++i) {
+    if (!(mass[i] > 0.)) return MDBAS_NB_ERR_ARG;
+    rm[i] = 1.0 / mass[i];
+  }
+  MD_TRY(e->mdMass.ensure(sizeof(double) * n));
+  MD_TRY(e->mdRmass.ensure(sizeof(double) * n));
+  MD_TRY(e->mdV.ensure(sizeof(double) * 3 * (size_t)n));
+  MD_TRY(e->mdF.ensure(sizeof(double) * 3 * (size_t)n));
+  MD_TRY(e->mdXb.ensure(sizeof(double) * 3 * (size_t)n));
+  MD_TRY(e->mdWord.ensure(sizeof(long long) * 8));
+  cudaStream_t s = e->stream;
+  MDB_CUDA(cudaMemcpyAsync(e->mdMass.p, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(e->mdRmass.p, rm.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
+                           s));
+  double *v = e->mdV.as<double>();
+  if (vx && vy && vz) {
+    MDB_CUDA(cudaMemcpyAsync(v, vx, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(v + n, vy, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(v + 2 * (size_t)n, vz, sizeof(double) * n, cudaMemcpyHostToDevice,
+                             s));
+  } else {
+    MDB_CUDA(cudaMemsetAsync(v, 0, sizeof(double) * 3 * (size_t)n, s));
+  }
+  // constraints grouped by molecule (connected components)
+  e->mdNCons = nConst;
+  e->mdNMol = 0;
+  if (nConst > 0) {
+    std::vector<int> parent(n);
+    for (int i = 0; i < n; ++i) parent[i] = i;
+    auto find = [&](int a) {
+      while (parent[a] != a) a = parent[a] = parent[parent[a]];
+      return a;
+    };
+    std::vector<int> cnt(n, 0);
+    for (int k = 0; k < nConst; ++k) {
+      const int a = constAtoms[2 * k], b = constAtoms[2 * k + 1];
+      if (a < 0 || a >= n || b < 0 || b >= n || a == b || !(constLen2[k] > 0.))
+        return MDBAS_NB_ERR_ARG;
+      parent[find(a)] = find(b);
+      cnt[a]++;
+      cnt[b]++;
+    }
+    std::vector<int> molOf(n, -1), order(nConst);
+    std::vector<int> molKey(nConst);
+    int nMol = 0;
+    std::vector<int> rootMol(n, -1);
+    for (int k = 0; k < nConst; ++k) {
+      const int r = find(constAtoms[2 * k]);
+      if (rootMol[r] < 0) rootMol[r] = nMol++;
+      molKey[k] = rootMol[r];
+      order[k] = k;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return molKey[a] < molKey[b]; });
+    std::vector<int> ca(nConst), cb(nConst), molStart(nMol + 1, 0);
+    std::vector<double> r2(nConst);
+    for (int t = 0; t < nConst; ++t) {
+      const int k = order[t];
+      ca[t] = constAtoms[2 * k];
+      cb[t] = constAtoms[2 * k + 1];
+      r2[t] = constLen2[k];
+      molStart[molKey[k] + 1]++;
+    }
+    for (int m = 0; m < nMol; ++m) molStart[m + 1] += molStart[m];
+    e->mdNMol = nMol;
+    MD_TRY(e->mdCa.ensure(sizeof(int) * nConst));
+    MD_TRY(e->mdCb.ensure(sizeof(int) * nConst));
+    MD_TRY(e->mdRc2.ensure(sizeof(double) * nConst));
+    MD_TRY(e->mdMol.ensure(sizeof(int) * (nMol + 1)));
+    MD_TRY(e->mdNAt.ensure(sizeof(int) * n));
+    MD_TRY(e->mdDd.ensure(sizeof(double) * 3 * (size_t)nConst));
+    MDB_CUDA(cudaMemcpyAsync(e->mdCa.p, ca.data(), sizeof(int) * nConst, cudaMemcpyHostToDevice,
+                             s));
+    MDB_CUDA(cudaMemcpyAsync(e->mdCb.p, cb.data(), sizeof(int) * nConst, cudaMemcpyHostToDevice,
+                             s));
+    MDB_CUDA(cudaMemcpyAsync(e->mdRc2.p, r2.data(), sizeof(double) * nConst,
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(e->mdMol.p, molStart.data(), sizeof(int) * (nMol + 1),
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(e->mdNAt.p, cnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+  }
+  int nFrozen = 0;
+  if (e->hasFrozen) {
+    std::vector<int> fr(n);
+    MDB_CUDA(cudaMemcpyAsync(fr.data(), e->frozen.p, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+    for (int i = 0; i < n; ++i) nFrozen += fr[i] != 0;
+  }
+  // degrees of freedom (get_degfree, src/utils.c:569-581)
+  e->mdDegFree = 3 * (n - nFrozen) - 3 - nConst;
+  e->mdDt = timeStep;
+  e->mdListUpdate = listUpdate;
+  e->mdTol = tolShake > 0. ? tolShake : 1e-8;          // src/io.c:95
+  e->mdMaxCycle = maxCycle > 0 ? maxCycle : 150;       // src/io.c:96
+  e->mdSteps = 0;
+  e->mdRebuilds = 0;
+  // forces at the initial positions
+  LaunchScope ls(e);
+  MD_TRY(md_build(e));
+  MD_TRY(mdbas_nb_engine_compute(e));
+  MD_TRY(md_forces(e));
+  e->mdReady = true;
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, double targetTemp,
+                           double tauT, double *energies) {
+  if (!e || nSteps < 0) return MDBAS_NB_ERR_ARG;
+  if (!e->mdReady) return MDBAS_NB_ERR_STATE;
+  MDB_CUDA(cudaSetDevice(e->device));
+  LaunchScope ls(e);
+  const int n = e->n;
+  cudaStream_t s = e->stream;
+  const double dt = e->mdDt;
+  double *x = e->x.as<double>(), *y = e->y.as<double>(), *z = e->z.as<double>();
+  double *vx = e->mdV.as<double>(), *vy = vx + n, *vz = vy + n;
+  double *fx = e->mdF.as<double>(), *fy = fx + n, *fz = fy + n;
+  double *ddx = e->mdDd.as<double>(), *ddy = ddx + e->mdNCons, *ddz = ddy + e->mdNCons;
+  long long *word = e->mdWord.as<long long>();
+  const double half2 = 0.25 * e->cfg.delr * e->cfg.delr;
+  const int g = grid_for(n, 256);
+  // kinTemp0 of the Berendsen bath (src/utils.c:555-581)
+  const double kinTemp0 = 0.5 * targetTemp * (double)e->mdDegFree * 0.83144621;
+  if (e->mdNCons > 0) MDB_CUDA(cudaMemsetAsync(word + 4, 0, sizeof(int) * 2, s));
+  int outRow = 0;
+  for (int step = 0; step < nSteps; ++step) {
+    const long long gstep = e->mdSteps + 1;
+    if (e->mdNCons > 0)
+      MDB_LAUNCH(k_cons_vectors, grid_for(e->mdNCons, 256), 256, 0, s, e->mdNCons, e->box,
+                 e->mdCa.as<int>(), e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
+    MDB_LAUNCH(k_vv_stage1, g, 256, 0, s, n, dt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy, vz,
+               x, y, z);
+    if (e->mdNCons > 0) {
+      MDB_LAUNCH(k_shake_positions, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, dt,
+                 e->mdTol, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
+                 e->mdCb.as<int>(), e->mdRc2.as<double>(), ddx, ddy, ddz,
+                 e->mdRmass.as<double>(), e->mdNAt.as<int>(), x, y, z, vx, vy, vz,
+                 reinterpret_cast<int *>(word + 4));
+    }
+    // list: fixed cadence or half-skin displacement
+    bool rebuild;
+    if (e->mdListUpdate > 0) {
+      rebuild = (gstep % e->mdListUpdate) == 0;
+    } else {
+      MDB_CUDA(cudaMemsetAsync(word, 0, sizeof(long long), s));
+      MDB_LAUNCH(k_max_disp, g, 256, 0, s, n, e->box, x, y, z, e->mdXb.as<double>(),
+                 e->mdXb.as<double>() + n, e->mdXb.as<double>() + 2 * (size_t)n,
+                 reinterpret_cast<unsigned long long *>(word));
+      unsigned long long bits = 0;
+      MDB_CUDA(cudaMemcpyAsync(&bits, word, sizeof(bits), cudaMemcpyDeviceToHost, s));
+      MDB_CUDA(cudaStreamSynchronize(s));
+      double d2;
+      memcpy(&d2, &bits, sizeof(d2));
+      rebuild = d2 > half2;
+    }
+    if (rebuild) MD_TRY(md_build(e));
+    else MD_TRY(mdbas_nb_engine_refresh(e));
+    MD_TRY(mdbas_nb_engine_compute(e));
+    MD_TRY(md_forces(e));
+    MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, dt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy, vz);
+    if (e->mdNCons > 0) {
+      // stage 2 takes the constraint vectors at the new positions
+      MDB_LAUNCH(k_cons_vectors, grid_for(e->mdNCons, 256), 256, 0, s, e->mdNCons, e->box,
+                 e->mdCa.as<int>(), e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
+      MDB_LAUNCH(k_shake_velocities, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, dt,
+                 e->mdTol / dt, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
+                 e->mdCb.as<int>(), ddx, ddy, ddz, e->mdRmass.as<double>(), e->mdNAt.as<int>(),
+                 vx, vy, vz, reinterpret_cast<int *>(word + 4));
+    }
+    const bool wantE = energies && energyEvery > 0 && (gstep % energyEvery) == 0;
+    const bool thermo = tauT > 0.;
+    if (wantE || thermo) {
+      MDB_CUDA(cudaMemsetAsync(word + 2, 0, sizeof(long long), s));
+      MDB_LAUNCH(k_kinetic, g, 256, 0, s, n, e->mdMass.as<double>(), vx, vy, vz, word + 2);
+    }
+    if (thermo)
+      MDB_LAUNCH(k_berendsen, g, 256, 0, s, n, dt / tauT, kinTemp0, word + 2, vx, vy, vz);
+    if (wantE) {
+      long long kfix = 0;
+      MDB_CUDA(cudaMemcpyAsync(&kfix, word + 2, sizeof(kfix), cudaMemcpyDeviceToHost, s));
+      mdbas_nb_energies en;
+      MD_TRY(mdbas_nb_engine_energies(e, &en));  // synchronises the stream
+      double kin = (double)kfix / kEnergyScale;
+      if (thermo && kin > 0.) kin *= 1.0 + dt / tauT * (kinTemp0 / kin - 1.0);
+      const double pot = en.elec_direct + en.elec_corr + en.elec_self + en.vdw;
+      energies[4 * outRow + 0] = (double)gstep;
+      energies[4 * outRow + 1] = pot;
+      energies[4 * outRow + 2] = kin;
+      energies[4 * outRow + 3] = pot + kin;
+      ++outRow;
+    }
+    // positions back into the box (image_update, src/integrate.c:1626)
+    MD_TRY(image_update_device(n, e->box, x, y, z, s));
+    e->mdSteps = gstep;
+  }
+  // constraint status
+  if (e->mdNCons > 0) {
+    int st[2] = {0, 0};
+    MDB_CUDA(cudaMemcpyAsync(st, word + 4, sizeof(st), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+    e->mdShakeIter = st[1];
+    if (st[0] & 1) {
+      set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "SHAKE did not converge (CONVERG_SHAKE_ERROR)");
+      return MDBAS_NB_ERR_UNSUPPORTED;
+    }
+    if (st[0] & 2) {
+      set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "a constrained molecule exceeds 16 atoms");
+      return MDBAS_NB_ERR_UNSUPPORTED;
+    }
+  }
+  MDB_CUDA(cudaStreamSynchronize(s));
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_md_stats(mdbas_nb_engine *e, long long out[4]) {
+  if (!e || !out) return MDBAS_NB_ERR_ARG;
+  out[0] = e->mdSteps;
+  out[1] = e->mdRebuilds;
+  out[2] = e->mdShakeIter;
+  out[3] = e->mdNMol;
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_get_positions(mdbas_nb_engine *e, double *x, double *y, double *z,
+                                  int device_ptrs) {
+  if (!e || !x || !y || !z) return MDBAS_NB_ERR_ARG;
+  MDB_CUDA(cudaSetDevice(e->device));
+  const cudaMemcpyKind k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t bytes = sizeof(double) * (size_t)e->n;
+  MDB_CUDA(cudaMemcpyAsync(x, e->x.p, bytes, k, e->stream));
+  MDB_CUDA(cudaMemcpyAsync(y, e->y.p, bytes, k, e->stream));
+  MDB_CUDA(cudaMemcpyAsync(z, e->z.p, bytes, k, e->stream));
+  MDB_CUDA(cudaStreamSynchronize(e->stream));
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_get_velocities(mdbas_nb_engine *e, double *vx, double *vy, double *vz,
+                                   int device_ptrs) {
+  if (!e || !vx || !vy || !vz) return MDBAS_NB_ERR_ARG;
+  if (!e->mdReady) return MDBAS_NB_ERR_STATE;
+  MDB_CUDA(cudaSetDevice(e->device));
+  const cudaMemcpyKind k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  const size_t bytes = sizeof(double) * (size_t)e->n;
+  const double *v = e->mdV.as<double>();
+  MDB_CUDA(cudaMemcpyAsync(vx, v, bytes, k, e->stream));
+  MDB_CUDA(cudaMemcpyAsync(vy, v + e->n, bytes, k, e->stream));
+  MDB_CUDA(cudaMemcpyAsync(vz, v + 2 * (size_t)e->n, bytes, k, e->stream));
+  MDB_CUDA(cudaStreamSynchronize(e->stream));
+  return MDBAS_NB_OK;
+}
+
+}  // extern "C"

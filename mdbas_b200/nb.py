@@ -213,6 +213,14 @@ def lib():
     L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
     L.mdbas_nb_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.mdbas_nb_engine_md_init.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
+                                          C.c_int, _ip, _dp, C.c_double, C.c_int]
+    L.mdbas_nb_engine_md_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
+                                         _dp]
+    L.mdbas_nb_engine_md_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    for name in ("get_positions", "get_velocities"):
+        getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                          C.c_void_p, C.c_int]
     _LIB = L
     return L
 
@@ -340,6 +348,53 @@ class Engine:
         check(lib().mdbas_nb_engine_kernel_time(self.h, 0, C.byref(ms), C.byref(cnt),
                                                 1 if reset else 0), "engine_kernel_time")
         return ms.value, cnt.value
+
+    # -- velocity-Verlet dynamics (mdbas_nb_engine_md_*) ----------------------
+    def md_init(self, mass, velocities=None, time_step=0.001, list_update=0, constraints=None,
+                tol_shake=1e-8, max_cycle=150):
+        """Start dynamics.  constraints = (pairs (k, 2) int, squared lengths (k,))."""
+        self._mass = np.ascontiguousarray(mass, dtype=np.float64)
+        if velocities is None:
+            vp = [None, None, None]
+        else:
+            self._v0 = [np.ascontiguousarray(a, dtype=np.float64) for a in velocities]
+            vp = [a.ctypes.data_as(_dp) for a in self._v0]
+        nc, cp, cl = 0, None, None
+        if constraints is not None and len(constraints[1]):
+            self._cpairs = np.ascontiguousarray(constraints[0], dtype=np.int32).reshape(-1)
+            self._clen2 = np.ascontiguousarray(constraints[1], dtype=np.float64)
+            nc = len(self._clen2)
+            cp, cl = self._cpairs.ctypes.data_as(_ip), self._clen2.ctypes.data_as(_dp)
+        check(lib().mdbas_nb_engine_md_init(self.h, self._mass.ctypes.data_as(_dp), *vp,
+                                            time_step, list_update, nc, cp, cl, tol_shake,
+                                            max_cycle), "engine_md_init")
+
+    def md_run(self, n_steps: int, energy_every: int = 0, target_temp: float = 0.0,
+               tau_t: float = 0.0):
+        """Advance n_steps; returns rows (step, potential, kinetic, total)."""
+        rows = n_steps // energy_every if energy_every > 0 else 0
+        buf = np.zeros((max(rows, 1), 4))
+        check(lib().mdbas_nb_engine_md_run(self.h, n_steps, energy_every, target_temp, tau_t,
+                                           buf.ctypes.data_as(_dp) if rows else None),
+              "engine_md_run")
+        return buf[:rows]
+
+    def md_stats(self):
+        out = (C.c_longlong * 4)()
+        check(lib().mdbas_nb_engine_md_stats(self.h, out), "engine_md_stats")
+        return {"steps": out[0], "rebuilds": out[1], "shake_iter": out[2], "molecules": out[3]}
+
+    def positions(self):
+        p = [np.zeros(self.n) for _ in range(3)]
+        check(lib().mdbas_nb_engine_get_positions(self.h, *(_ptr(a) for a in p), 0),
+              "engine_get_positions")
+        return p
+
+    def velocities(self):
+        v = [np.zeros(self.n) for _ in range(3)]
+        check(lib().mdbas_nb_engine_get_velocities(self.h, *(_ptr(a) for a in v), 0),
+              "engine_get_velocities")
+        return v
 
     def close(self):
         if getattr(self, "h", None):

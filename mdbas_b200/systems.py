@@ -71,6 +71,17 @@ class System:
         """The three box rows a, b, c as MDBas's CONF holds them."""
         return np.array([self.box, 0, 0, 0, self.box, 0, 0, 0, self.box], dtype=np.float64)
 
+    def water_constraints(self):
+        """Rigid-water constraints (O-H1, O-H2, H1-H2) of every molecule:
+        (pairs (3M, 2) int32, squared lengths (3M,))."""
+        m = self.n // 3
+        base = 3 * np.arange(m, dtype=np.int32)
+        pairs = np.stack([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1),
+                          np.stack([base + 1, base + 2], 1)], 1).reshape(-1, 2)
+        rhh = 2.0 * WATER_ROH * math.sin(0.5 * WATER_THETA)
+        lens = np.tile(np.array([WATER_ROH ** 2, WATER_ROH ** 2, rhh ** 2]), m)
+        return pairs.astype(np.int32), lens
+
     def exclusions(self, symmetric: bool = True):
         """Excluded pairs from bonds + angles as CSR (start[n+1], flat).
 
@@ -222,6 +233,14 @@ def lj_fluid(n: int = 12000, box: float = 50.0, seed: int = 1, n_types: int = 4,
                   pos[:, 2].copy(), q, eps, sig, np.full(n, 39.948), empty2, empty3,
                   types=types, type_eps_kcal=t_eps, type_sigma=t_sig,
                   meta={"seed": seed})
+
+
+def thermal_velocities(mass: np.ndarray, temperature: float, seed: int = 1):
+    """Seeded Maxwell-Boltzmann velocities (A/ps) for masses in amu."""
+    rng = np.random.default_rng(seed)
+    sd = np.sqrt(RBOLTZ_IU * temperature / np.asarray(mass, dtype=np.float64))
+    v = rng.normal(size=(len(sd), 3)) * sd[:, None]
+    return v[:, 0].copy(), v[:, 1].copy(), v[:, 2].copy()
 
 
 def replica_sizes(count: int = 64, lo: int = 1500, hi: int = 30000, seed: int = 1) -> list[int]:

@@ -240,6 +240,12 @@ class Reference:
             lib.ref_layout.restype = C.c_int
             lib.ref_layout.argtypes = [C.c_char_p, C.c_int]
             lib.ref_now.restype = C.c_double
+            lib.ref_md_init.restype = C.c_int
+            lib.ref_md_init.argtypes = [C.c_void_p, _dp, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                        C.c_double, C.c_int, C.c_double, C.c_double]
+            lib.ref_md_run.argtypes = [C.c_void_p, C.c_int, _dp]
+            lib.ref_get_velocities.argtypes = [C.c_void_p, _dp, _dp, _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
         return cls._lib
@@ -343,6 +349,39 @@ class Reference:
 
     def self_energy(self) -> float:
         return self.lib().ref_self_energy(self.h)
+
+    def md_init(self, mass, velocities=None, time_step=0.001, list_update=1, constraints=None,
+                tol_shake=1e-8, max_cycle=150, temp0=0.0, tau_t=0.0) -> int:
+        """Start MDBas's own velocity-Verlet dynamics (after makelist).  Returns
+        the degrees of freedom MDBas counts."""
+        self._md_keep = [_d(mass)]
+        vp = [None, None, None]
+        if velocities is not None:
+            vs = [_d(a) for a in velocities]
+            self._md_keep += vs
+            vp = [a.ctypes.data for a in vs]
+        nc, cp, cl = 0, None, None
+        if constraints is not None and len(constraints[1]):
+            pairs = _i(np.asarray(constraints[0]).reshape(-1))
+            lens = _d(constraints[1])
+            self._md_keep += [pairs, lens]
+            nc, cp, cl = len(lens), pairs.ctypes.data, lens.ctypes.data
+        r = self.lib().ref_md_init(self.h, self._md_keep[0], *vp, time_step, list_update, nc, cp,
+                                   cl, tol_shake, max_cycle, temp0, tau_t)
+        if r < 0:
+            raise RuntimeError("ref_md_init: list not built or dynamics already started")
+        return r
+
+    def md_run(self, n_steps: int) -> np.ndarray:
+        """Rows (step, pot, kin, pot + kin) after each step."""
+        rows = np.zeros((max(n_steps, 1), 4))
+        self.lib().ref_md_run(self.h, n_steps, rows)
+        return rows[:n_steps]
+
+    def velocities(self):
+        vx, vy, vz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        self.lib().ref_get_velocities(self.h, vx, vy, vz)
+        return vx, vy, vz
 
     def now(self) -> float:
         return self.lib().ref_now()

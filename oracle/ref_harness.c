@@ -33,6 +33,8 @@
 #include "utils.h"
 #include "init.h"
 #include "spme.h"
+#include "integrate.h"
+#include "shake.h"
 
 /* MDBas's driver owns this global (src/mdbas.c:43). */
 FILE *outFile = NULL;
@@ -66,6 +68,11 @@ typedef struct {
   int *frozen;
   int *neighList, *neighPair, *neighOrder, *neighList14, **exclList, *exclPair;
   int listBuilt;
+  /* dynamics (ref_md_init) */
+  double *mass, *rmass;
+  int *nAtConst;
+  BATH bath;
+  int mdInit;
 } RefSys;
 
 static double *dup_d(const double *src, int n)
@@ -344,6 +351,11 @@ void ref_destroy(RefSys *s)
   free(s->fx); free(s->fy); free(s->fz); free(s->vx); free(s->vy); free(s->vz);
   free(s->frozen); free(s->bond); free(s->angle); free(s->constList); free(s->dihe);
   free(s->impr);
+  free(s->mass); free(s->rmass); free(s->nAtConst);
+  if (s->mdInit) {
+    integrators_free_arrays(&s->ctrl, &s->param);
+    if (s->param.nConst > 0) shake_free_arrays();
+  }
   if (s->listBuilt) {
     free(s->neighList); free(s->neighPair); free(s->neighOrder); free(s->neighList14);
     if (s->exclList) {
@@ -354,4 +366,105 @@ void ref_destroy(RefSys *s)
     free(s->exclPair);
   }
   free(s);
+}
+
+/*
+ * Velocity-Verlet dynamics through MDBas's own integrator, as the MD loop of
+ * src/mdbas.c:244-300 drives it: vv_integrate stage 1 (src/integrate.c:1479,
+ * vv_nve/vv_nvt_b with vv_shake_r), makelist on the neigh.update cadence,
+ * energy(), vv_integrate stage 2 (vv_shake_v, kinetic, image_update).
+ * Bonded terms stay off (nBond = nAngle = 0 in energy(), as in ref_energy);
+ * the bonds/angles given to ref_create only feed the exclusion builders.
+ * constAtoms holds 2*nConst atom indices, constLen2 the squared lengths.
+ * tauT > 0 selects NVT_B (Berendsen) toward temp0, else NVE.
+ * Requires ref_makelist first.  MDBas keeps its integrator and SHAKE work
+ * arrays in file-scope statics, so one RefSys at a time may run dynamics.
+ */
+int ref_md_init(RefSys *s, const double *mass, const double *vx, const double *vy,
+                const double *vz, double timeStep, int listUpdate, int nConst,
+                const int *constAtoms, const double *constLen2, double tolShake, int maxCycle,
+                double temp0, double tauT)
+{
+  int i, n = s->param.nAtom;
+  if (!s->listBuilt || s->mdInit) return -1;
+  s->mass = dup_d(mass, n);
+  s->rmass = dup_d(NULL, n);
+  for (i = 0; i < n; i++) s->rmass[i] = 1.0 / mass[i];
+  if (vx) memcpy(s->vx, vx, (size_t)n * sizeof(double));
+  if (vy) memcpy(s->vy, vy, (size_t)n * sizeof(double));
+  if (vz) memcpy(s->vz, vz, (size_t)n * sizeof(double));
+  free(s->constList);
+  s->constList = (CONSTRAINT *)calloc((size_t)(nConst > 0 ? nConst : 1), sizeof(CONSTRAINT));
+  s->nAtConst = (int *)calloc((size_t)n, sizeof(int));
+  for (i = 0; i < nConst; i++) {
+    s->constList[i].a = constAtoms[2 * i];
+    s->constList[i].b = constAtoms[2 * i + 1];
+    s->constList[i].rc2 = constLen2[i];
+    s->nAtConst[constAtoms[2 * i]]++;
+    s->nAtConst[constAtoms[2 * i + 1]]++;
+  }
+  s->param.nConst = nConst;
+  s->param.tolShake = tolShake;
+  s->param.maxCycle = maxCycle;
+  s->param.timeStep = timeStep;
+  s->param.rTimeStep = 1. / timeStep;
+  s->param.step = 0;
+  s->param.nFrozen = 0;
+  for (i = 0; i < n; i++) s->param.nFrozen += s->frozen[i] != 0;
+  get_degfree(&s->param, &s->box);
+  s->param.temp0 = temp0;
+  s->param.kinTemp0 = 0.5 * temp0 * (double)s->param.nDegFree * rboltzui;
+  s->bath.tauT = tauT;
+  s->ctrl.integrator = VELOCITY;
+  s->ctrl.ens = tauT > 0. ? NVT_B : NVE;
+  s->neigh.update = listUpdate > 0 ? listUpdate : 1;
+  integrators_allocate_arrays(&s->ctrl, &s->param);
+  if (nConst > 0) shake_allocate_arrays(&s->param);
+  s->mdInit = 1;
+  /* forces and energies at time 0 (src/mdbas.c:166-176) */
+  {
+    double out[6];
+    ref_energy(s, NULL, NULL, NULL, out);
+  }
+  s->ener.kin = kinetic(&s->param, s->vx, s->vy, s->vz, s->mass);
+  return s->param.nDegFree;
+}
+
+/* nSteps MD steps; rows[4*k] = {step, pot, kin, pot+kin} after each step
+ * (pot = energy()'s real-space elec + vdw, internal units). */
+void ref_md_run(RefSys *s, int nSteps, double *rows)
+{
+  int k;
+  PARAM p;
+  for (k = 0; k < nSteps; k++) {
+    s->param.step++;
+    vv_integrate(&s->ctrl, &s->param, &s->ener, &s->box, &s->bath, s->constList, s->x, s->y,
+                 s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->mass, s->rmass,
+                 s->nAtConst, 1);
+    makelist(&s->ctrl, &s->param, &s->box, &s->neigh, s->constList, s->bond, s->angle, s->dihe,
+             s->impr, s->x, s->y, s->z, s->frozen, &s->neighList, &s->neighPair,
+             &s->neighOrder, &s->neighList14, &s->exclList, &s->exclPair);
+    p = s->param;
+    p.nBond = p.nAngle = p.nUb = p.nDihedral = p.nImproper = 0;
+    energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->bond, s->angle,
+           s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,
+           s->eps, s->sig, s->eps, s->sig, s->frozen, s->neighList, s->neighPair, s->neighOrder,
+           s->neighList14, s->exclList, s->exclPair);
+    vv_integrate(&s->ctrl, &s->param, &s->ener, &s->box, &s->bath, s->constList, s->x, s->y,
+                 s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->mass, s->rmass,
+                 s->nAtConst, 2);
+    if (rows) {
+      rows[4 * k + 0] = (double)s->param.step;
+      rows[4 * k + 1] = s->ener.pot;
+      rows[4 * k + 2] = s->ener.kin;
+      rows[4 * k + 3] = s->ener.pot + s->ener.kin;
+    }
+  }
+}
+
+void ref_get_velocities(const RefSys *s, double *vx, double *vy, double *vz)
+{
+  memcpy(vx, s->vx, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(vy, s->vy, (size_t)s->param.nAtom * sizeof(double));
+  memcpy(vz, s->vz, (size_t)s->param.nAtom * sizeof(double));
 }
