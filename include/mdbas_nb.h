@@ -438,6 +438,13 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
  * MDBAS_NB_ERR_UNSUPPORTED if SHAKE did not converge (CONVERG_SHAKE_ERROR). */
 int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, double targetTemp,
                            double tauT, double *energies);
+/* Mixed precision (precision 1) runs whole steps as CUDA graphs of
+ * stepsPerLaunch steps (default 20): the rebuild test is made on the device
+ * and the list build is a conditional graph node, so the host synchronises
+ * once per launch.  A launch whose rebuild outgrows the pair list is redone
+ * from a snapshot with a larger list.  0 runs every step from the host.
+ * Both forms give bit-identical trajectories (fixed-point sums). */
+int mdbas_nb_engine_md_set_graph(mdbas_nb_engine *e, int stepsPerLaunch);
 /* out[0] steps taken, out[1] list builds, out[2] largest SHAKE iteration
  * count of the last md_run, out[3] constrained molecules. */
 int mdbas_nb_engine_md_stats(mdbas_nb_engine *e, long long out[4]);

@@ -49,7 +49,7 @@ __global__ void k_col_bin(int n, ClusterGeom g, const int *__restrict__ colRank,
   if (i >= n) return;
   double sx = x[i] / g.Lx + 0.5, sy = y[i] / g.Ly + 0.5, sz = z[i] / g.Lz + 0.5;
   if (!(isfinite(sx) && isfinite(sy) && isfinite(sz))) {
-    atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), 2ull);
+    atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), (unsigned long long)CL_NONFINITE);
     sx = sy = sz = 0.5;
   }
   sx -= floor(sx);
@@ -117,7 +117,8 @@ __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
 }
 
 // One thread per cluster: FP64 origin and half extents, slot data.
-__global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__ slotAtom,
+__global__ void k_clusters(const int *__restrict__ nSlotsDev, ClusterGeom g,
+                           const int *__restrict__ slotAtom,
                            const int *__restrict__ atomCol, const int *__restrict__ colXY,
                            const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, const double *__restrict__ q,
@@ -128,7 +129,7 @@ __global__ void k_clusters(int nClusters, ClusterGeom g, const int *__restrict__
                            int *__restrict__ slotOf, int *__restrict__ clusterXY,
                            int *__restrict__ hmaxBits) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nClusters) return;
+  if (c >= (*nSlotsDev >> 3)) return;
   const double ilx = 1.0 / g.Lx, ily = 1.0 / g.Ly, ilz = 1.0 / g.Lz;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   double px[kClusterSize], py[kClusterSize], pz[kClusterSize];
@@ -262,7 +263,9 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
   e0 = __shfl_sync(0xffffffffu, e0, 0);
   it = __shfl_sync(0xffffffffu, it, 0);
   if (e0 + nkeep > entryCap || it >= itemCap) {
-    if (lane == 0) atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), 1ull);
+    if (lane == 0)
+      atomicOr(reinterpret_cast<unsigned long long *>(counters + 2),
+               (unsigned long long)CL_OVERFLOW);
     return;
   }
   if (keep) {
@@ -283,7 +286,7 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
 }
 
 __global__ void __launch_bounds__(kSearchThreads)
-k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
+k_search(const int *__restrict__ nSlotsDev, ClusterGeom g, const int *__restrict__ colRank,
          const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
          const double4 *__restrict__ origin, const float4 *__restrict__ originF,
          const float4 *__restrict__ half, const int *__restrict__ slotAtom,
@@ -296,7 +299,7 @@ k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
   __shared__ SearchBuf bufs[kSearchThreads / 32];
   const int lane = threadIdx.x & 31;
   const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (ci >= nClusters) return;
+  if (ci >= (*nSlotsDev >> 3)) return;
   SearchBuf &B = bufs[threadIdx.x >> 5];
 
   const double4 oi = origin[ci];
@@ -407,12 +410,13 @@ k_search(int nClusters, ClusterGeom g, const int *__restrict__ colRank,
     atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3), (unsigned long long)cand);
 }
 
-__global__ void k_refresh(int nSlots, ClusterGeom g, const int *__restrict__ slotAtom,
-                          const double4 *__restrict__ origin, const double *__restrict__ x,
-                          const double *__restrict__ y, const double *__restrict__ z,
-                          const double *__restrict__ q, double sqrtC, float4 *__restrict__ xq) {
+__global__ void k_refresh(const int *__restrict__ nSlotsDev, ClusterGeom g,
+                          const int *__restrict__ slotAtom, const double4 *__restrict__ origin,
+                          const double *__restrict__ x, const double *__restrict__ y,
+                          const double *__restrict__ z, const double *__restrict__ q, double sqrtC,
+                          float4 *__restrict__ xq) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= nSlots) return;
+  if (s >= *nSlotsDev) return;
   const int a = slotAtom[s];
   if (a < 0) return;
   const double4 o = origin[s / kClusterSize];
@@ -421,6 +425,10 @@ __global__ void k_refresh(int nSlots, ClusterGeom g, const int *__restrict__ slo
   dy -= g.Ly * rint(dy / g.Ly);
   dz -= g.Lz * rint(dz / g.Lz);
   xq[s] = make_float4((float)dx, (float)dy, (float)dz, (float)(q[a] * sqrtC));
+}
+
+__global__ void k_latch(const long long *__restrict__ counters, long long *__restrict__ sticky) {
+  if (threadIdx.x == 0) sticky[0] |= counters[2];
 }
 
 unsigned morton2(unsigned x, unsigned y) {
@@ -440,7 +448,7 @@ unsigned morton2(unsigned x, unsigned y) {
 int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
                   double sqrtC, const double *x, const double *y, const double *z,
                   const double *q, const double *eps, const double *sig, const int *frozen,
-                  const int *exclStart, const int *exclFlat, cudaStream_t s) {
+                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync) {
   if (b.type != CUBIC && b.type != ORBIC) return MDBAS_NB_ERR_UNSUPPORTED;
   if (n <= 0) return MDBAS_NB_ERR_ARG;
   ClusterGeom g{};
@@ -467,9 +475,13 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   }
   g.rlist2 = (float)(rlist * rlist * (1.0 + 1e-5));
   const int nCols = g.ncx * g.ncy;
+  const int slotCap = (n + (kClusterSize - 1) * nCols + kClusterSize - 1) & ~(kClusterSize - 1);
+  const bool sameGrid = nCols == w.nCols && g.ncx == w.geom.ncx && g.ncy == w.geom.ncy;
+  // The captured form cannot upload tables or grow buffers.
+  if (!sync && (!sameGrid || slotCap > w.slotCap || w.entryCap == 0)) return MDBAS_NB_ERR_STATE;
 
   // Morton rank of each (cx, cy) cell; rebuilt when the grid changes.
-  if (nCols != w.nCols || g.ncx != w.geom.ncx || g.ncy != w.geom.ncy) {
+  if (!sameGrid) {
     std::vector<std::pair<unsigned, int>> keys(nCols);
     for (int cy = 0; cy < g.ncy; ++cy)
       for (int cx = 0; cx < g.ncx; ++cx)
@@ -492,23 +504,43 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   w.geom = g;
   w.nCols = nCols;
 
-  MDB_TRY(w.colCount.ensure(sizeof(int) * (nCols + 1)));
-  MDB_TRY(w.colFill.ensure(sizeof(int) * (nCols + 1)));
-  MDB_TRY(w.colStart.ensure(sizeof(int) * (nCols + 2)));
-  MDB_TRY(w.colPad.ensure(sizeof(int) * (nCols + 1)));
-  MDB_TRY(w.colPadStart.ensure(sizeof(int) * (nCols + 2)));
-  MDB_TRY(w.colClStart.ensure(sizeof(int) * (nCols + 2)));
-  MDB_TRY(w.atomCol.ensure(sizeof(int) * n));
-  MDB_TRY(w.atomZ.ensure(sizeof(double) * n));
-  MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
-  MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
-  MDB_TRY(w.scanTmp.ensure(scan_tmp_bytes(std::max(n, nCols) + 1)));
-  MDB_TRY(w.counters.ensure(sizeof(long long) * 4));
-  MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
+  if (sync) {
+    MDB_TRY(w.colCount.ensure(sizeof(int) * (nCols + 1)));
+    MDB_TRY(w.colFill.ensure(sizeof(int) * (nCols + 1)));
+    MDB_TRY(w.colStart.ensure(sizeof(int) * (nCols + 2)));
+    MDB_TRY(w.colPad.ensure(sizeof(int) * (nCols + 1)));
+    MDB_TRY(w.colPadStart.ensure(sizeof(int) * (nCols + 2)));
+    MDB_TRY(w.colClStart.ensure(sizeof(int) * (nCols + 2)));
+    MDB_TRY(w.atomCol.ensure(sizeof(int) * n));
+    MDB_TRY(w.atomZ.ensure(sizeof(double) * n));
+    MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
+    MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
+    MDB_TRY(w.scanTmp.ensure(scan_tmp_bytes(std::max(n, nCols) + 1)));
+    MDB_TRY(w.counters.ensure(sizeof(long long) * 4));
+    MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
+    if (!w.sticky.p) {
+      MDB_TRY(w.sticky.ensure(sizeof(long long)));
+      MDB_CUDA(cudaMemsetAsync(w.sticky.p, 0, sizeof(long long), s));
+    }
+    if (slotCap > w.slotCap) {
+      w.slotCap = slotCap;
+      w.clCap = slotCap / kClusterSize;
+    }
+    MDB_TRY(w.slotAtom.ensure(sizeof(int) * w.slotCap));
+    MDB_TRY(w.clusterXY.ensure(sizeof(int) * w.clCap));
+    MDB_TRY(w.origin.ensure(sizeof(double4) * w.clCap));
+    MDB_TRY(w.half.ensure(sizeof(float4) * w.clCap));
+    MDB_TRY(w.originF.ensure(sizeof(float4) * w.clCap));
+    MDB_TRY(w.hmax.ensure(sizeof(int) * 4));
+    MDB_TRY(w.xq.ensure(sizeof(float4) * w.slotCap));
+    MDB_TRY(w.lj.ensure(sizeof(float2) * w.slotCap));
+    MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)w.slotCap));
+  }
 
   MDB_CUDA(cudaMemsetAsync(w.colCount.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
+  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4, s));
   MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, g, w.colRank.as<int>(), x, y, z,
              w.atomCol.as<int>(), w.atomZ.as<double>(), w.colCount.as<int>(),
              w.counters.as<long long>());
@@ -516,74 +548,82 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   MDB_LAUNCH(k_col_pad, grid_for(nCols, 256), 256, 0, s, nCols, w.colCount.as<int>(),
              w.colPad.as<int>());
   MDB_TRY(exclusive_scan32(w.colPad.as<int>(), w.colPadStart.as<int>(), nCols, w.scanTmp.p, s));
-  int nSlots = 0;
-  long long flags[4];
-  MDB_CUDA(cudaMemcpyAsync(&nSlots, w.colPadStart.as<int>() + nCols, sizeof(int),
-                           cudaMemcpyDeviceToHost, s));
-  MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
-  MDB_CUDA(cudaStreamSynchronize(s));
-  if (flags[2] & 2) return MDBAS_NB_ERR_NONFINITE;
-  w.nSlots = nSlots;
-  w.nClusters = nSlots / kClusterSize;
-  const int nCl = w.nClusters;
-
-  MDB_TRY(w.slotAtom.ensure(sizeof(int) * nSlots));
-  MDB_TRY(w.clusterXY.ensure(sizeof(int) * nCl));
-  MDB_TRY(w.origin.ensure(sizeof(double4) * nCl));
-  MDB_TRY(w.half.ensure(sizeof(float4) * nCl));
-  MDB_TRY(w.originF.ensure(sizeof(float4) * nCl));
-  MDB_TRY(w.hmax.ensure(sizeof(int) * 4));
-  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4, s));
-  MDB_TRY(w.xq.ensure(sizeof(float4) * nSlots));
-  MDB_TRY(w.lj.ensure(sizeof(float2) * nSlots));
-  MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)nSlots));
-
   MDB_LAUNCH(k_col_clstart, grid_for(nCols + 1, 256), 256, 0, s, nCols, w.colPadStart.as<int>(),
              w.colClStart.as<int>());
   MDB_LAUNCH(k_col_scatter, grid_for(n, 256), 256, 0, s, n, w.atomCol.as<int>(),
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
   MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
              w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
-  MDB_LAUNCH(k_clusters, grid_for(nCl, 128), 128, 0, s, nCl, g, w.slotAtom.as<int>(),
-             w.atomCol.as<int>(), w.colXY.as<int>(), x, y, z, q, eps, sig, sqrtC,
-             w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
-             w.xq.as<float4>(), w.lj.as<float2>(),
-             w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
+  MDB_LAUNCH(k_clusters, grid_for(w.clCap, 128), 128, 0, s, w.nSlotsDev(), g,
+             w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x, y, z, q, eps, sig,
+             sqrtC, w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
+             w.xq.as<float4>(), w.lj.as<float2>(), w.slotOf.as<int>(), w.clusterXY.as<int>(),
+             w.hmax.as<int>());
 
-  // Cluster-pair search; grow the list and search again if it overflowed.
+  // Cluster-pair search; in the synchronising form grow the list and search
+  // again if it overflowed.
   if (w.entryCap == 0) {
-    w.entryCap = (long long)nCl * 160 + 4096;
-    w.itemCap = w.entryCap / kItemMax + nCl + 1024;
+    w.entryCap = (long long)w.clCap * 160 + 4096;
+    w.itemCap = w.entryCap / kItemMax + w.clCap + 1024;
   }
   for (int attempt = 0; attempt < 4; ++attempt) {
-    MDB_TRY(w.entries.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
-    MDB_TRY(w.masks.ensure(sizeof(uint2) * (size_t)w.entryCap));
-    MDB_TRY(w.items.ensure(sizeof(int4) * (size_t)w.itemCap));
-    MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
-    MDB_LAUNCH(k_search, grid_for((long long)nCl * 32, kSearchThreads), kSearchThreads, 0, s, nCl,
-               g, w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
-               w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
-               w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
-               w.hmax.as<int>(), w.xq.as<float4>(), w.entries.as<CPairEntry>(),
-               w.masks.as<uint2>(),
-               w.items.as<int4>(), w.counters.as<long long>(), w.entryCap, w.itemCap);
+    if (sync) {
+      MDB_TRY(w.entries.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
+      MDB_TRY(w.masks.ensure(sizeof(uint2) * (size_t)w.entryCap));
+      MDB_TRY(w.items.ensure(sizeof(int4) * (size_t)w.itemCap));
+    }
+    MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
+    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long), s));
+    MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
+               w.nSlotsDev(), g, w.colRank.as<int>(), w.colClStart.as<int>(),
+               w.clusterXY.as<int>(), w.origin.as<double4>(), w.originF.as<float4>(),
+               w.half.as<float4>(), w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart,
+               exclFlat, w.hmax.as<int>(), w.xq.as<float4>(), w.entries.as<CPairEntry>(),
+               w.masks.as<uint2>(), w.items.as<int4>(), w.counters.as<long long>(), w.entryCap,
+               w.itemCap);
+    if (!sync) {
+      MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.sticky.as<long long>());
+      return MDBAS_NB_OK;
+    }
+    long long flags[4];
+    int nSlots = 0;
     MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaMemcpyAsync(&nSlots, w.nSlotsDev(), sizeof(int), cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaStreamSynchronize(s));
+    if (flags[2] & CL_NONFINITE) return MDBAS_NB_ERR_NONFINITE;
+    w.nSlots = nSlots;
+    w.nClusters = nSlots / kClusterSize;
     w.nEntries = flags[0];
     w.nItems = flags[1];
-    if (!(flags[2] & 1)) return MDBAS_NB_OK;
+    if (!(flags[2] & CL_OVERFLOW)) return MDBAS_NB_OK;
+    // the search does not clear the overflow bit; the next attempt starts clean
+    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 2, 0, sizeof(long long), s));
     w.entryCap = (long long)(flags[0] * 1.25) + 4096;
     w.itemCap = (long long)(flags[1] * 1.25) + 1024;
   }
   return MDBAS_NB_ERR_CAPACITY;
 }
 
+int cluster_read_counts(ClusterWork &w, cudaStream_t s) {
+  if (!w.counters.p || w.nCols <= 0) return MDBAS_NB_ERR_STATE;
+  long long flags[4];
+  int nSlots = 0;
+  MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaMemcpyAsync(&nSlots, w.nSlotsDev(), sizeof(int), cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaStreamSynchronize(s));
+  w.nSlots = nSlots;
+  w.nClusters = nSlots / kClusterSize;
+  w.nEntries = flags[0];
+  w.nItems = flags[1];
+  return MDBAS_NB_OK;
+}
+
 int cluster_refresh(ClusterWork &w, int n, const DevBox &b, const double *x, const double *y,
                     const double *z, const double *q, double sqrtC, cudaStream_t s) {
   (void)n;
   (void)b;
-  if (w.nSlots <= 0) return MDBAS_NB_ERR_STATE;
-  MDB_LAUNCH(k_refresh, grid_for(w.nSlots, 256), 256, 0, s, w.nSlots, w.geom,
+  if (w.slotCap <= 0) return MDBAS_NB_ERR_STATE;
+  MDB_LAUNCH(k_refresh, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(), w.geom,
              w.slotAtom.as<int>(), w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>());
   return MDBAS_NB_OK;
 }

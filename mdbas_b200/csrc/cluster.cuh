@@ -34,7 +34,12 @@ struct ClusterWork {
   DBuf atomCol, tmpIdx;
   DBuf atomZ;         // wrapped fractional z (FP64)
   DBuf scanTmp;
-  // layout
+  // layout.  Slot-indexed buffers hold slotCap = n + 7 * nCols slots (rounded
+  // up to a whole cluster), the most that per-column padding can produce, so
+  // a rebuild never reallocates and kernels read the actual count on the
+  // device (colPadStart[nCols]).  nSlots/nClusters are host copies, valid
+  // after a synchronising build or cluster_read_counts.
+  int slotCap = 0, clCap = 0;
   int nSlots = 0, nClusters = 0;
   DBuf slotAtom;      // slot -> atom (-1 for padding)
   DBuf slotOf;        // atom -> slot
@@ -53,16 +58,28 @@ struct ClusterWork {
   DBuf counters;      // int64[4]: entries, items, overflow flag, candidates
   long long entryCap = 0, itemCap = 0;
   long long nEntries = 0, nItems = 0;
+  DBuf sticky;        // int64: OR of every build's error bits since last read
   // accumulators
-  DBuf facc;          // int64 fixed-point forces, SoA [3][nSlots]
+  DBuf facc;          // int64 fixed-point forces, SoA [3][slotCap]
   DBuf acc;           // int64[ACC_COUNT]
+  const int *nSlotsDev() const { return colPadStart.as<int>() + nCols; }
 };
 
+// Bits of ClusterWork::counters[2] and ::sticky.
+enum ClusterFlag { CL_OVERFLOW = 1, CL_NONFINITE = 2 };
+
 // Sort atoms into cells/clusters and build the cluster-pair list.
+// sync = true: the host reads the counts back, grows the pair-list capacity
+// and searches again when it overflowed.  sync = false: no host interaction
+// and no allocation (the form captured into CUDA graphs); the layout must
+// have been set up by an earlier synchronising build of the same geometry,
+// and an overflow only raises CL_OVERFLOW in `sticky`.
 int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
                   double sqrtC, const double *x, const double *y, const double *z,
                   const double *q, const double *eps, const double *sig, const int *frozen,
-                  const int *exclStart, const int *exclFlat, cudaStream_t s);
+                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync = true);
+// Host copies of the list counts (synchronises the stream).
+int cluster_read_counts(ClusterWork &w, cudaStream_t s);
 // Refresh xq from the current FP64 positions (list kept).
 int cluster_refresh(ClusterWork &w, int n, const DevBox &b, const double *x, const double *y,
                     const double *z, const double *q, double sqrtC, cudaStream_t s);

@@ -428,7 +428,7 @@ int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch,
                            g.q.as<double>(), sqrt(param->chargeConst), g.s));
   }
   ClusterWork &w = g.cl;
-  MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.nSlots, g.s));
+  MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, g.s));
   MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, g.s));
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);

@@ -171,6 +171,7 @@ int mdbas_nb_engine_destroy(mdbas_nb_engine *e) {
   if (!e) return MDBAS_NB_OK;
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
+  md_release(e);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->ownStream) cudaStreamDestroy(e->stream);
@@ -195,6 +196,7 @@ int mdbas_nb_engine_set_box(mdbas_nb_engine *e, const PBC *box) {
   e->hostBox = *box;
   e->box = make_devbox(box);
   e->built = false;
+  e->mdGraphStale = true;
   return MDBAS_NB_OK;
 }
 
@@ -252,6 +254,7 @@ int mdbas_nb_engine_set_topology(mdbas_nb_engine *e, const double *q, const doub
   e->selfE = -e->cfg.chargeConst * e->cfg.alpha * ((double)q2 / kQ2Scale) / kSqrtPi;
   e->topoSet = true;
   e->built = false;
+  e->mdGraphStale = true;
   return MDBAS_NB_OK;
 }
 
@@ -331,7 +334,7 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
                          e->q.as<double>(), fx, fy, fz, e->acc64.as<double>(), s));
   } else {
     ClusterWork &w = e->cl;
-    MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.nSlots, s));
+    MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
     MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
     if (e->grid <= 0) {
       int sms = 148;
@@ -428,6 +431,8 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
     out[2] = e->ref.entries;
     out[3] = (long long)(e->ref.list.bytes / sizeof(int));
   } else {
+    ENG_TRY(e, set_dev(e));
+    ENG_TRY(e, cluster_read_counts(e->cl, e->stream));
     out[0] = e->cl.nClusters;
     out[1] = e->cl.nEntries;
     out[2] = e->cl.nEntries * 64;
@@ -453,6 +458,7 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs,
                e->ref.list.as<int>(), e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                r2max, e->exportBuf.as<int>(), cap, e->exportCount.as<unsigned long long>());
   } else {
+    ENG_TRY(e, cluster_read_counts(e->cl, s));
     MDB_LAUNCH(k_export_cluster_pairs, grid_for(e->cl.nItems * 32, 128), 128, 0, s,
                e->cl.nEntries, e->cl.items.as<int4>(), e->cl.nItems,
                e->cl.entries.as<CPairEntry>(), e->cl.masks.as<uint2>(), e->cl.xq.as<float4>(),

@@ -45,6 +45,15 @@ struct mdbas_nb_engine {
   double mdDt = 0.0, mdTol = 1e-8;
   long long mdSteps = 0, mdRebuilds = 0, mdShakeIter = 0;
   bool mdReady = false;
+  // CUDA graph of mdGraphSteps whole steps (precision 1); rebuilt when stale
+  int mdGraphSteps = 20, mdGraphK = 0;
+  long long mdGraphMainK = 0, mdGraphBodyK = 0;  // kernels per step / per rebuild
+  bool mdGraphStale = true;
+  double mdGraphTau = 0.0, mdGraphTemp = 0.0;
+  cudaGraph_t mdGraph = nullptr;
+  cudaGraphExec_t mdExec = nullptr;
+  cudaStream_t mdCapStream = nullptr, mdSideStream = nullptr;
+  mdbas::DBuf mdRows, mdSnap;
 };
 
 namespace mdbas {
@@ -58,6 +67,8 @@ struct LaunchScope {
   ~LaunchScope() { g_launch_counter = prev; }
 };
 int engine_check_device(int device);
+// Releases the dynamics graph and its streams (md.cu).
+void md_release(mdbas_nb_engine *e);
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);
 }  // namespace mdbas

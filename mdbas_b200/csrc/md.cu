@@ -324,6 +324,43 @@ __global__ void k_berendsen(int n, double dtOverTau, double kinTemp0,
   vz[i] *= lambda;
 }
 
+// --- graph-only kernels: the rebuild decision and the per-step record -----
+// Sets the rebuild condition from the largest squared displacement and
+// advances the device step counter.
+__global__ void k_decide_disp(cudaGraphConditionalHandle h,
+                              const unsigned long long *__restrict__ bits, double half2,
+                              long long *__restrict__ stepDev) {
+  if (threadIdx.x != 0) return;
+  const double d2 = __longlong_as_double((long long)bits[0]);
+  stepDev[0] += 1;
+  cudaGraphSetConditional(h, d2 > half2 ? 1u : 0u);
+}
+
+// Same for the fixed cadence of MDBas's "list N" (rebuild when step % N == 0).
+__global__ void k_decide_cadence(cudaGraphConditionalHandle h, long long *__restrict__ stepDev,
+                                 int update) {
+  if (threadIdx.x != 0) return;
+  const long long st = stepDev[0] + 1;
+  stepDev[0] = st;
+  cudaGraphSetConditional(h, (st % update) == 0 ? 1u : 0u);
+}
+
+__global__ void k_count(long long *__restrict__ c) {
+  if (threadIdx.x == 0) c[0] += 1;
+}
+
+// Fixed-point energies of the step (elec direct, elec corr, vdw, kinetic) and
+// the accumulated error bits.
+__global__ void k_md_row(long long *__restrict__ row, const long long *__restrict__ acc,
+                         const long long *__restrict__ kin, long long *__restrict__ flags) {
+  if (threadIdx.x != 0) return;
+  row[0] = acc[ACC_E_DIR];
+  row[1] = acc[ACC_E_CORR];
+  row[2] = acc[ACC_E_VDW];
+  row[3] = kin[0];
+  flags[0] |= acc[ACC_FLAGS];
+}
+
 }  // namespace
 }  // namespace mdbas
 
@@ -338,38 +375,372 @@ __global__ void k_berendsen(int n, double dtOverTau, double kinTemp0,
 
 namespace {
 
+// Slots of the engine's MD word buffer (int64 each).
+enum MdWord {
+  W_DISP = 0,     // largest squared displacement since the last build (bits)
+  W_FLAGS = 1,    // OR of the fixed-point error bits of the recorded steps
+  W_KIN = 2,      // kinetic energy, fixed point (2^-24)
+  W_SHAKE = 4,    // two ints: SHAKE error bits, largest iteration count
+  W_STEP = 6,     // device step counter (graph form)
+  W_BUILDS = 7,   // list builds inside the graph since the last read
+  W_COUNT = 8
+};
+
 // FP64 forces of the last compute, caller order, into e->mdF (3n).
-int md_forces(mdbas_nb_engine *e) {
+int md_forces(mdbas_nb_engine *e, cudaStream_t s) {
   const int n = e->n;
-  if (e->cfg.precision == 0) {
-    MDB_CUDA(cudaMemcpyAsync(e->mdF.p, e->f64.p, sizeof(double) * 3 * (size_t)n,
-                             cudaMemcpyDeviceToDevice, e->stream));
-    if (e->hasFrozen)
-      MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, e->stream, n, e->frozen.as<int>(),
-                 e->mdF.as<double>(), e->mdV.as<double>());
-    return MDBAS_NB_OK;
-  }
   double *f = e->mdF.as<double>();
-  MDB_TRY(forces_out_launch(e->cl, n, 0, f, f + n, f + 2 * (size_t)n, e->stream));
+  if (e->cfg.precision == 0) {
+    MDB_CUDA(cudaMemcpyAsync(f, e->f64.p, sizeof(double) * 3 * (size_t)n,
+                             cudaMemcpyDeviceToDevice, s));
+  } else {
+    MDB_TRY(forces_out_launch(e->cl, n, 0, f, f + n, f + 2 * (size_t)n, s));
+  }
   if (e->hasFrozen)
-    MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, e->stream, n, e->frozen.as<int>(), f,
+    MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, s, n, e->frozen.as<int>(), f,
                e->mdV.as<double>());
   return MDBAS_NB_OK;
 }
 
+int md_save_build_positions(mdbas_nb_engine *e, cudaStream_t s) {
+  const size_t bytes = sizeof(double) * (size_t)e->n;
+  double *xb = e->mdXb.as<double>();
+  MDB_CUDA(cudaMemcpyAsync(xb, e->x.p, bytes, cudaMemcpyDeviceToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(xb + e->n, e->y.p, bytes, cudaMemcpyDeviceToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(xb + 2 * (size_t)e->n, e->z.p, bytes, cudaMemcpyDeviceToDevice, s));
+  return MDBAS_NB_OK;
+}
+
+// Synchronising list build (either precision) at the current positions.
 int md_build(mdbas_nb_engine *e) {
   MD_TRY(mdbas_nb_engine_build(e));
-  const size_t bytes = sizeof(double) * (size_t)e->n;
-  MDB_CUDA(cudaMemcpyAsync(e->mdXb.p, e->x.p, bytes, cudaMemcpyDeviceToDevice, e->stream));
-  MDB_CUDA(cudaMemcpyAsync(e->mdXb.as<double>() + e->n, e->y.p, bytes, cudaMemcpyDeviceToDevice,
-                           e->stream));
-  MDB_CUDA(cudaMemcpyAsync(e->mdXb.as<double>() + 2 * (size_t)e->n, e->z.p, bytes,
-                           cudaMemcpyDeviceToDevice, e->stream));
+  MD_TRY(md_save_build_positions(e, e->stream));
   e->mdRebuilds += 1;
   return MDBAS_NB_OK;
 }
 
+// stage 1 of vv_nve: constraint vectors, half kick + drift, SHAKE on positions
+int md_stage1(mdbas_nb_engine *e, cudaStream_t s) {
+  const int n = e->n, nc = e->mdNCons;
+  double *x = e->x.as<double>(), *y = e->y.as<double>(), *z = e->z.as<double>();
+  double *vx = e->mdV.as<double>(), *vy = vx + n, *vz = vy + n;
+  const double *fx = e->mdF.as<double>(), *fy = fx + n, *fz = fy + n;
+  double *ddx = e->mdDd.as<double>(), *ddy = ddx + nc, *ddz = ddy + nc;
+  if (nc > 0)
+    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
+               e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
+  MDB_LAUNCH(k_vv_stage1, grid_for(n, 256), 256, 0, s, n, e->mdDt, fx, fy, fz,
+             e->mdRmass.as<double>(), vx, vy, vz, x, y, z);
+  if (nc > 0)
+    MDB_LAUNCH(k_shake_positions, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box,
+               e->mdDt, e->mdTol, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
+               e->mdCb.as<int>(), e->mdRc2.as<double>(), ddx, ddy, ddz, e->mdRmass.as<double>(),
+               e->mdNAt.as<int>(), x, y, z, vx, vy, vz,
+               reinterpret_cast<int *>(e->mdWord.as<long long>() + W_SHAKE));
+  return MDBAS_NB_OK;
+}
+
+int md_max_disp(mdbas_nb_engine *e, cudaStream_t s) {
+  const int n = e->n;
+  long long *word = e->mdWord.as<long long>();
+  const double *xb = e->mdXb.as<double>();
+  MDB_CUDA(cudaMemsetAsync(word + W_DISP, 0, sizeof(long long), s));
+  MDB_LAUNCH(k_max_disp, grid_for(n, 256), 256, 0, s, n, e->box, e->x.as<double>(),
+             e->y.as<double>(), e->z.as<double>(), xb, xb + n, xb + 2 * (size_t)n,
+             reinterpret_cast<unsigned long long *>(word + W_DISP));
+  return MDBAS_NB_OK;
+}
+
+// Nonbonded forces of the cluster form with no host interaction: refresh the
+// float4 layout, evaluate, convert to caller order.
+int md_forces_cluster(mdbas_nb_engine *e, cudaStream_t s) {
+  ClusterWork &w = e->cl;
+  const int n = e->n;
+  MDB_TRY(cluster_refresh(w, n, e->box, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                          e->q.as<double>(), sqrt(e->cfg.chargeConst), s));
+  MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
+  MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
+  MDB_TRY(pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
+  MDB_TRY(excl_fix_launch(w, n, e->box, e->pp, e->exclStart.as<int>(), e->exclFlat.as<int>(),
+                          e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                          e->q.as<double>(), s));
+  return md_forces(e, s);
+}
+
+// stage 2: half kick, RATTLE on velocities, kinetic energy (+ Berendsen),
+// positions wrapped into the box
+int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double kinTemp0) {
+  const int n = e->n, nc = e->mdNCons;
+  double *x = e->x.as<double>(), *y = e->y.as<double>(), *z = e->z.as<double>();
+  double *vx = e->mdV.as<double>(), *vy = vx + n, *vz = vy + n;
+  const double *fx = e->mdF.as<double>(), *fy = fx + n, *fz = fy + n;
+  double *ddx = e->mdDd.as<double>(), *ddy = ddx + nc, *ddz = ddy + nc;
+  long long *word = e->mdWord.as<long long>();
+  const int g = grid_for(n, 256);
+  MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, e->mdDt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy,
+             vz);
+  if (nc > 0) {
+    // stage 2 takes the constraint vectors at the new positions
+    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
+               e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
+    MDB_LAUNCH(k_shake_velocities, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->mdDt,
+               e->mdTol / e->mdDt, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
+               e->mdCb.as<int>(), ddx, ddy, ddz, e->mdRmass.as<double>(), e->mdNAt.as<int>(), vx,
+               vy, vz, reinterpret_cast<int *>(word + W_SHAKE));
+  }
+  const bool thermo = tauT > 0.;
+  if (kin || thermo) {
+    MDB_CUDA(cudaMemsetAsync(word + W_KIN, 0, sizeof(long long), s));
+    MDB_LAUNCH(k_kinetic, g, 256, 0, s, n, e->mdMass.as<double>(), vx, vy, vz, word + W_KIN);
+  }
+  if (thermo)
+    MDB_LAUNCH(k_berendsen, g, 256, 0, s, n, e->mdDt / tauT, kinTemp0, word + W_KIN, vx, vy,
+               vz);
+  // positions back into the box (image_update, src/integrate.c:1626)
+  return image_update_device(n, e->box, x, y, z, s);
+}
+
+double md_kin_row(double kin, double dt, double tauT, double kinTemp0) {
+  if (tauT > 0. && kin > 0.) kin *= 1.0 + dt / tauT * (kinTemp0 / kin - 1.0);
+  return kin;
+}
+
+int md_check_shake(mdbas_nb_engine *e, const int st[2]) {
+  e->mdShakeIter = std::max<long long>(e->mdShakeIter, st[1]);
+  if (st[0] & 1) {
+    set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "SHAKE did not converge (CONVERG_SHAKE_ERROR)");
+    return MDBAS_NB_ERR_UNSUPPORTED;
+  }
+  if (st[0] & 2) {
+    set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "a constrained molecule exceeds 16 atoms");
+    return MDBAS_NB_ERR_UNSUPPORTED;
+  }
+  return MDBAS_NB_OK;
+}
+
+// --- the graph form ------------------------------------------------------------
+struct CaptureCount {
+  long long main = 0, body = 0;
+};
+
+void md_graph_free(mdbas_nb_engine *e) {
+  if (e->mdExec) cudaGraphExecDestroy(e->mdExec);
+  if (e->mdGraph) cudaGraphDestroy(e->mdGraph);
+  e->mdExec = nullptr;
+  e->mdGraph = nullptr;
+  e->mdGraphK = 0;
+  e->mdGraphStale = true;
+}
+
+// The rebuild body: synchronisation-free cluster build, build positions
+// saved, build counter advanced.
+int md_capture_rebuild_body(mdbas_nb_engine *e, cudaGraph_t body, long long *counter) {
+  cudaStream_t side = e->mdSideStream;
+  MDB_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed));
+  g_launch_counter = counter;
+  const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
+  int st = cluster_build(e->cl, e->n, e->box, e->cfg.cutOff, e->cfg.delr,
+                         sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
+                         e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),
+                         e->sig.as<double>(), frozen, e->exclStart.as<int>(),
+                         e->exclFlat.as<int>(), side, false);
+  if (st == MDBAS_NB_OK) st = md_save_build_positions(e, side);
+  if (st == MDBAS_NB_OK) {
+    k_count<<<1, 32, 0, side>>>(e->mdWord.as<long long>() + W_BUILDS);
+    ++(*counter);
+    if (cudaGetLastError() != cudaSuccess) st = MDBAS_NB_ERR_CUDA;
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(side, &out);
+  if (st != MDBAS_NB_OK) return st;
+  MDB_CUDA(ce);
+  return MDBAS_NB_OK;
+}
+
+int md_capture_steps(mdbas_nb_engine *e, int K, double tauT, double kinTemp0,
+                     CaptureCount &cc) {
+  cudaStream_t cs = e->mdCapStream;
+  long long *word = e->mdWord.as<long long>();
+  const double half2 = 0.25 * e->cfg.delr * e->cfg.delr;
+  for (int k = 0; k < K; ++k) {
+    g_launch_counter = &cc.main;
+    MDB_TRY(md_stage1(e, cs));
+    // the rebuild decision, on the device
+    cudaStreamCaptureStatus cst;
+    cudaGraph_t capG = nullptr;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, &deps, &nd));
+    cudaGraphConditionalHandle h;
+    MDB_CUDA(cudaGraphConditionalHandleCreate(&h, capG, 0, cudaGraphCondAssignDefault));
+    if (e->mdListUpdate > 0) {
+      MDB_LAUNCH(k_decide_cadence, 1, 32, 0, cs, h, word + W_STEP, e->mdListUpdate);
+    } else {
+      MDB_TRY(md_max_disp(e, cs));
+      MDB_LAUNCH(k_decide_disp, 1, 32, 0, cs, h,
+                 reinterpret_cast<const unsigned long long *>(word + W_DISP), half2,
+                 word + W_STEP);
+    }
+    MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, &deps, &nd));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    MDB_CUDA(cudaGraphAddNode(&cn, capG, deps, nd, &cp));
+    long long bodyCount = 0;
+    MDB_TRY(md_capture_rebuild_body(e, cp.conditional.phGraph_out[0], &bodyCount));
+    cc.body = bodyCount;
+    MDB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &cn, 1, cudaStreamSetCaptureDependencies));
+    g_launch_counter = &cc.main;
+    MDB_TRY(md_forces_cluster(e, cs));
+    MDB_TRY(md_stage2(e, cs, true, tauT, kinTemp0));
+    MDB_LAUNCH(k_md_row, 1, 32, 0, cs, e->mdRows.as<long long>() + 4 * (size_t)k,
+               e->cl.acc.as<long long>(), word + W_KIN, word + W_FLAGS);
+  }
+  return MDBAS_NB_OK;
+}
+
+int md_capture(mdbas_nb_engine *e, int K, double targetTemp, double tauT, double kinTemp0) {
+  md_graph_free(e);
+  if (!e->mdCapStream)
+    MDB_CUDA(cudaStreamCreateWithFlags(&e->mdCapStream, cudaStreamNonBlocking));
+  if (!e->mdSideStream)
+    MDB_CUDA(cudaStreamCreateWithFlags(&e->mdSideStream, cudaStreamNonBlocking));
+  MDB_TRY(e->mdRows.ensure(sizeof(long long) * 4 * (size_t)K));
+  // everything the capture reads from the host must be final: finish the
+  // engine stream's work first
+  MDB_CUDA(cudaStreamSynchronize(e->stream));
+  long long *const saved = g_launch_counter;
+  CaptureCount cc;
+  MDB_CUDA(cudaStreamBeginCapture(e->mdCapStream, cudaStreamCaptureModeThreadLocal));
+  const int st = md_capture_steps(e, K, tauT, kinTemp0, cc);
+  g_launch_counter = saved;
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(e->mdCapStream, &graph);
+  if (st != MDBAS_NB_OK || ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (st != MDBAS_NB_OK) return st;
+    return cuda_fail(ce, "cudaStreamEndCapture", __FILE__, __LINE__);
+  }
+  cudaGraphExec_t exec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+  if (ie != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return cuda_fail(ie, "cudaGraphInstantiate", __FILE__, __LINE__);
+  }
+  e->mdGraph = graph;
+  e->mdExec = exec;
+  e->mdGraphK = K;
+  e->mdGraphTau = tauT;
+  e->mdGraphTemp = targetTemp;
+  e->mdGraphStale = false;
+  e->mdGraphMainK = cc.main / K;
+  e->mdGraphBodyK = cc.body;
+  return MDBAS_NB_OK;
+}
+
+int md_snapshot(mdbas_nb_engine *e, bool restore) {
+  const size_t n = (size_t)e->n, b = sizeof(double) * n;
+  double *snap = e->mdSnap.as<double>();
+  double *parts[4] = {e->x.as<double>(), e->y.as<double>(), e->z.as<double>(), nullptr};
+  const cudaMemcpyKind k = cudaMemcpyDeviceToDevice;
+  cudaStream_t s = e->stream;
+  for (int i = 0; i < 3; ++i) {
+    if (restore) MDB_CUDA(cudaMemcpyAsync(parts[i], snap + i * n, b, k, s));
+    else MDB_CUDA(cudaMemcpyAsync(snap + i * n, parts[i], b, k, s));
+  }
+  double *packed[3] = {e->mdV.as<double>(), e->mdF.as<double>(), e->mdXb.as<double>()};
+  for (int i = 0; i < 3; ++i) {
+    if (restore) MDB_CUDA(cudaMemcpyAsync(packed[i], snap + (3 + 3 * i) * n, 3 * b, k, s));
+    else MDB_CUDA(cudaMemcpyAsync(snap + (3 + 3 * i) * n, packed[i], 3 * b, k, s));
+  }
+  return MDBAS_NB_OK;
+}
+
+void md_write_row(double *energies, int row, long long gstep, double pot, double kin) {
+  energies[4 * row + 0] = (double)gstep;
+  energies[4 * row + 1] = pot;
+  energies[4 * row + 2] = kin;
+  energies[4 * row + 3] = pot + kin;
+}
+
+// Steps [done, done + K*chunks) through the graph.  Returns the number of
+// rows written through *outRow.
+int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetTemp,
+                 double tauT, double kinTemp0, double *energies, int *outRow) {
+  const int K = e->mdGraphSteps;
+  cudaStream_t s = e->stream;
+  long long *word = e->mdWord.as<long long>();
+  if (e->mdGraphStale || e->mdGraphK != K || e->mdGraphTau != tauT ||
+      e->mdGraphTemp != targetTemp)
+    MD_TRY(md_capture(e, K, targetTemp, tauT, kinTemp0));
+  MD_TRY(e->mdSnap.ensure(sizeof(double) * 12 * (size_t)e->n));
+  std::vector<long long> rows(4 * (size_t)K);
+  int growths = 0;
+  for (int c = 0; c < chunks;) {
+    const long long step0 = e->mdSteps;
+    MDB_CUDA(cudaMemcpyAsync(word + W_STEP, &step0, sizeof(long long), cudaMemcpyHostToDevice,
+                             s));
+    MDB_CUDA(cudaMemsetAsync(word + W_BUILDS, 0, sizeof(long long), s));
+    MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), s));
+    MD_TRY(md_snapshot(e, false));
+    MDB_CUDA(cudaGraphLaunch(e->mdExec, s));
+    long long w[W_COUNT], sticky = 0;
+    MDB_CUDA(cudaMemcpyAsync(w, word, sizeof(w), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaMemcpyAsync(&sticky, e->cl.sticky.p, sizeof(sticky), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaMemcpyAsync(rows.data(), e->mdRows.p, sizeof(long long) * rows.size(),
+                             cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+    e->launches += e->mdGraphMainK * K + e->mdGraphBodyK * w[W_BUILDS];
+    if (sticky & CL_NONFINITE) {
+      set_last_status(MDBAS_NB_ERR_NONFINITE, "non-finite positions during dynamics");
+      return MDBAS_NB_ERR_NONFINITE;
+    }
+    if (sticky & CL_OVERFLOW) {
+      // a rebuild inside the chunk outgrew the pair list: go back to the
+      // chunk's start, enlarge the list and capture again
+      if (++growths > 3) return MDBAS_NB_ERR_CAPACITY;
+      MD_TRY(md_snapshot(e, true));
+      e->cl.entryCap = (long long)(e->cl.entryCap * 1.5) + 4096;
+      e->cl.itemCap = (long long)(e->cl.itemCap * 1.5) + 1024;
+      MD_TRY(md_build(e));
+      MD_TRY(md_capture(e, K, targetTemp, tauT, kinTemp0));
+      continue;
+    }
+    const int st2[2] = {(int)(w[W_SHAKE] & 0xffffffff), (int)(w[W_SHAKE] >> 32)};
+    MD_TRY(md_check_shake(e, st2));
+    if (w[W_FLAGS] & FLAG_OVERFLOW) {
+      set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
+      return MDBAS_NB_ERR_OVERFLOW;
+    }
+    e->mdRebuilds += w[W_BUILDS];
+    for (int k = 0; k < K; ++k) {
+      const long long gstep = step0 + k + 1;
+      if (energies && energyEvery > 0 && gstep % energyEvery == 0) {
+        const long long *r = &rows[4 * (size_t)k];
+        const double pot = (double)(r[0] + r[1] + r[2]) / kEnergyScale + e->selfE;
+        const double kin = md_kin_row((double)r[3] / kEnergyScale, e->mdDt, tauT, kinTemp0);
+        md_write_row(energies, (*outRow)++, gstep, pot, kin);
+      }
+    }
+    e->mdSteps = step0 + K;
+    ++c;
+  }
+  return MDBAS_NB_OK;
+}
+
 }  // namespace
+
+void mdbas::md_release(mdbas_nb_engine *e) {
+  md_graph_free(e);
+  if (e->mdCapStream) cudaStreamDestroy(e->mdCapStream);
+  if (e->mdSideStream) cudaStreamDestroy(e->mdSideStream);
+  e->mdCapStream = e->mdSideStream = nullptr;
+}
 
 extern "C" {
 
@@ -387,13 +758,15 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
     if (!(mass[i] > 0.)) return MDBAS_NB_ERR_ARG;
     rm[i] = 1.0 / mass[i];
   }
+  md_graph_free(e);
   MD_TRY(e->mdMass.ensure(sizeof(double) * n));
   MD_TRY(e->mdRmass.ensure(sizeof(double) * n));
   MD_TRY(e->mdV.ensure(sizeof(double) * 3 * (size_t)n));
   MD_TRY(e->mdF.ensure(sizeof(double) * 3 * (size_t)n));
   MD_TRY(e->mdXb.ensure(sizeof(double) * 3 * (size_t)n));
-  MD_TRY(e->mdWord.ensure(sizeof(long long) * 8));
+  MD_TRY(e->mdWord.ensure(sizeof(long long) * W_COUNT));
   cudaStream_t s = e->stream;
+  MDB_CUDA(cudaMemsetAsync(e->mdWord.p, 0, sizeof(long long) * W_COUNT, s));
   MDB_CUDA(cudaMemcpyAsync(e->mdMass.p, mass, sizeof(double) * n, cudaMemcpyHostToDevice, s));
   MDB_CUDA(cudaMemcpyAsync(e->mdRmass.p, rm.data(), sizeof(double) * n, cudaMemcpyHostToDevice,
                            s));
@@ -425,10 +798,8 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
       cnt[a]++;
       cnt[b]++;
     }
-    std::vector<int> molOf(n, -1), order(nConst);
-    std::vector<int> molKey(nConst);
+    std::vector<int> order(nConst), molKey(nConst), rootMol(n, -1);
     int nMol = 0;
-    std::vector<int> rootMol(n, -1);
     for (int k = 0; k < nConst; ++k) {
       const int r = find(constAtoms[2 * k]);
       if (rootMol[r] < 0) rootMol[r] = nMol++;
@@ -480,12 +851,30 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   e->mdMaxCycle = maxCycle > 0 ? maxCycle : 150;       // src/io.c:96
   e->mdSteps = 0;
   e->mdRebuilds = 0;
+  e->mdShakeIter = 0;
+  if (e->grid <= 0) {
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+    e->grid = sms * 8;
+    e->block = 256;
+  }
   // forces at the initial positions
   LaunchScope ls(e);
   MD_TRY(md_build(e));
+  if (e->cfg.precision == 1) MD_TRY(mdbas_nb_engine_refresh(e));
   MD_TRY(mdbas_nb_engine_compute(e));
-  MD_TRY(md_forces(e));
+  MD_TRY(md_forces(e, e->stream));
+  MDB_CUDA(cudaStreamSynchronize(s));
   e->mdReady = true;
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_md_set_graph(mdbas_nb_engine *e, int stepsPerLaunch) {
+  if (!e || stepsPerLaunch < 0 || stepsPerLaunch > 1000) return MDBAS_NB_ERR_ARG;
+  if (stepsPerLaunch != e->mdGraphSteps) {
+    e->mdGraphSteps = stepsPerLaunch;
+    e->mdGraphStale = true;
+  }
   return MDBAS_NB_OK;
 }
 
@@ -495,106 +884,62 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   if (!e->mdReady) return MDBAS_NB_ERR_STATE;
   MDB_CUDA(cudaSetDevice(e->device));
   LaunchScope ls(e);
-  const int n = e->n;
   cudaStream_t s = e->stream;
-  const double dt = e->mdDt;
-  double *x = e->x.as<double>(), *y = e->y.as<double>(), *z = e->z.as<double>();
-  double *vx = e->mdV.as<double>(), *vy = vx + n, *vz = vy + n;
-  double *fx = e->mdF.as<double>(), *fy = fx + n, *fz = fy + n;
-  double *ddx = e->mdDd.as<double>(), *ddy = ddx + e->mdNCons, *ddz = ddy + e->mdNCons;
   long long *word = e->mdWord.as<long long>();
   const double half2 = 0.25 * e->cfg.delr * e->cfg.delr;
-  const int g = grid_for(n, 256);
   // kinTemp0 of the Berendsen bath (src/utils.c:555-581)
   const double kinTemp0 = 0.5 * targetTemp * (double)e->mdDegFree * 0.83144621;
-  if (e->mdNCons > 0) MDB_CUDA(cudaMemsetAsync(word + 4, 0, sizeof(int) * 2, s));
+  MDB_CUDA(cudaMemsetAsync(word + W_SHAKE, 0, sizeof(long long), s));
+  MDB_CUDA(cudaMemsetAsync(word + W_FLAGS, 0, sizeof(long long), s));
   int outRow = 0;
-  for (int step = 0; step < nSteps; ++step) {
+  int done = 0;
+  // whole graph launches first (mixed precision only)
+  const int K = e->mdGraphSteps;
+  if (e->cfg.precision == 1 && K > 0 && nSteps >= K) {
+    const int chunks = nSteps / K;
+    MD_TRY(md_run_graph(e, chunks, energyEvery, targetTemp, tauT, kinTemp0, energies, &outRow));
+    done = chunks * K;
+  }
+  for (int step = done; step < nSteps; ++step) {
     const long long gstep = e->mdSteps + 1;
-    if (e->mdNCons > 0)
-      MDB_LAUNCH(k_cons_vectors, grid_for(e->mdNCons, 256), 256, 0, s, e->mdNCons, e->box,
-                 e->mdCa.as<int>(), e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
-    MDB_LAUNCH(k_vv_stage1, g, 256, 0, s, n, dt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy, vz,
-               x, y, z);
-    if (e->mdNCons > 0) {
-      MDB_LAUNCH(k_shake_positions, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, dt,
-                 e->mdTol, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
-                 e->mdCb.as<int>(), e->mdRc2.as<double>(), ddx, ddy, ddz,
-                 e->mdRmass.as<double>(), e->mdNAt.as<int>(), x, y, z, vx, vy, vz,
-                 reinterpret_cast<int *>(word + 4));
-    }
+    MD_TRY(md_stage1(e, s));
     // list: fixed cadence or half-skin displacement
     bool rebuild;
     if (e->mdListUpdate > 0) {
       rebuild = (gstep % e->mdListUpdate) == 0;
     } else {
-      MDB_CUDA(cudaMemsetAsync(word, 0, sizeof(long long), s));
-      MDB_LAUNCH(k_max_disp, g, 256, 0, s, n, e->box, x, y, z, e->mdXb.as<double>(),
-                 e->mdXb.as<double>() + n, e->mdXb.as<double>() + 2 * (size_t)n,
-                 reinterpret_cast<unsigned long long *>(word));
+      MD_TRY(md_max_disp(e, s));
       unsigned long long bits = 0;
-      MDB_CUDA(cudaMemcpyAsync(&bits, word, sizeof(bits), cudaMemcpyDeviceToHost, s));
+      MDB_CUDA(cudaMemcpyAsync(&bits, word + W_DISP, sizeof(bits), cudaMemcpyDeviceToHost, s));
       MDB_CUDA(cudaStreamSynchronize(s));
       double d2;
       memcpy(&d2, &bits, sizeof(d2));
       rebuild = d2 > half2;
     }
     if (rebuild) MD_TRY(md_build(e));
-    else MD_TRY(mdbas_nb_engine_refresh(e));
+    if (e->cfg.precision == 1) MD_TRY(mdbas_nb_engine_refresh(e));
     MD_TRY(mdbas_nb_engine_compute(e));
-    MD_TRY(md_forces(e));
-    MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, dt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy, vz);
-    if (e->mdNCons > 0) {
-      // stage 2 takes the constraint vectors at the new positions
-      MDB_LAUNCH(k_cons_vectors, grid_for(e->mdNCons, 256), 256, 0, s, e->mdNCons, e->box,
-                 e->mdCa.as<int>(), e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
-      MDB_LAUNCH(k_shake_velocities, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, dt,
-                 e->mdTol / dt, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
-                 e->mdCb.as<int>(), ddx, ddy, ddz, e->mdRmass.as<double>(), e->mdNAt.as<int>(),
-                 vx, vy, vz, reinterpret_cast<int *>(word + 4));
-    }
+    MD_TRY(md_forces(e, s));
     const bool wantE = energies && energyEvery > 0 && (gstep % energyEvery) == 0;
-    const bool thermo = tauT > 0.;
-    if (wantE || thermo) {
-      MDB_CUDA(cudaMemsetAsync(word + 2, 0, sizeof(long long), s));
-      MDB_LAUNCH(k_kinetic, g, 256, 0, s, n, e->mdMass.as<double>(), vx, vy, vz, word + 2);
-    }
-    if (thermo)
-      MDB_LAUNCH(k_berendsen, g, 256, 0, s, n, dt / tauT, kinTemp0, word + 2, vx, vy, vz);
+    MD_TRY(md_stage2(e, s, wantE, tauT, kinTemp0));
     if (wantE) {
       long long kfix = 0;
-      MDB_CUDA(cudaMemcpyAsync(&kfix, word + 2, sizeof(kfix), cudaMemcpyDeviceToHost, s));
+      MDB_CUDA(cudaMemcpyAsync(&kfix, word + W_KIN, sizeof(kfix), cudaMemcpyDeviceToHost, s));
       mdbas_nb_energies en;
       MD_TRY(mdbas_nb_engine_energies(e, &en));  // synchronises the stream
-      double kin = (double)kfix / kEnergyScale;
-      if (thermo && kin > 0.) kin *= 1.0 + dt / tauT * (kinTemp0 / kin - 1.0);
       const double pot = en.elec_direct + en.elec_corr + en.elec_self + en.vdw;
-      energies[4 * outRow + 0] = (double)gstep;
-      energies[4 * outRow + 1] = pot;
-      energies[4 * outRow + 2] = kin;
-      energies[4 * outRow + 3] = pot + kin;
-      ++outRow;
+      md_write_row(energies, outRow++, gstep,
+                   pot, md_kin_row((double)kfix / kEnergyScale, e->mdDt, tauT, kinTemp0));
     }
-    // positions back into the box (image_update, src/integrate.c:1626)
-    MD_TRY(image_update_device(n, e->box, x, y, z, s));
     e->mdSteps = gstep;
   }
   // constraint status
-  if (e->mdNCons > 0) {
-    int st[2] = {0, 0};
-    MDB_CUDA(cudaMemcpyAsync(st, word + 4, sizeof(st), cudaMemcpyDeviceToHost, s));
-    MDB_CUDA(cudaStreamSynchronize(s));
-    e->mdShakeIter = st[1];
-    if (st[0] & 1) {
-      set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "SHAKE did not converge (CONVERG_SHAKE_ERROR)");
-      return MDBAS_NB_ERR_UNSUPPORTED;
-    }
-    if (st[0] & 2) {
-      set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "a constrained molecule exceeds 16 atoms");
-      return MDBAS_NB_ERR_UNSUPPORTED;
-    }
-  }
+  long long w[W_COUNT];
+  MDB_CUDA(cudaMemcpyAsync(w, word, sizeof(w), cudaMemcpyDeviceToHost, s));
   MDB_CUDA(cudaStreamSynchronize(s));
+  const int st2[2] = {(int)(w[W_SHAKE] & 0xffffffff), (int)(w[W_SHAKE] >> 32)};
+  MD_TRY(md_check_shake(e, st2));
+  e->computed = true;
   return MDBAS_NB_OK;
 }
 

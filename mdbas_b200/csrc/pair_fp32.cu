@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(256)
 k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ items,
             const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
             const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
-            long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+            long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
   const int lane = threadIdx.x & 31;
   const int il = lane & 7, jh = lane >> 3;
   const bool up = il & 4, mid = il & 2, lo = il & 1;
@@ -121,7 +121,7 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
   const long long nItems = counters[1];
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * nSlots;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * fstride;
   long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;  // fixed point, summed per item
   long long npair = 0;
   bool overflow = false;
@@ -183,7 +183,7 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
       const float v = (jh == 0) ? fix : (jh == 1 ? fiy : fiz);
       if (v != 0.f) {
         overflow |= !(fabsf(v) < kForceLimitF);
-        red_add(facc + (size_t)jh * nSlots + ci * kClusterSize + il, fix_f(v));
+        red_add(facc + (size_t)jh * fstride + ci * kClusterSize + il, fix_f(v));
       }
     }
     // Each item's energy is converted to fixed point on its own, so totals
@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kCWarps * 32, 5)
 k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ items,
              const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
              const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
-             long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+             long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   CompactWarp &W = reinterpret_cast<CompactWarp *>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
@@ -396,8 +396,8 @@ k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ it
                       fabsf(sz) < kForceLimitF);
         const int slot = W.ej[e] * kClusterSize + jl;
         red_add(facc + slot, fix_f(-sx));
-        red_add(facc + (size_t)nSlots + slot, fix_f(-sy));
-        red_add(facc + 2 * (size_t)nSlots + slot, fix_f(-sz));
+        red_add(facc + (size_t)fstride + slot, fix_f(-sy));
+        red_add(facc + 2 * (size_t)fstride + slot, fix_f(-sz));
       }
       __syncwarp();
     }
@@ -412,7 +412,7 @@ k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ it
       const float v = (q == 0) ? fix : (q == 1 ? fiy : fiz);
       if (v != 0.f) {
         overflow |= !(fabsf(v) < kForceLimitF);
-        red_add(facc + (size_t)q * nSlots + ci * kClusterSize + il, fix_f(v));
+        red_add(facc + (size_t)q * fstride + ci * kClusterSize + il, fix_f(v));
       }
     }
     Ec += fix_e(warp_sum_d((double)ec));
@@ -439,7 +439,7 @@ k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
            const int *__restrict__ exclFlat, const double *__restrict__ x,
            const double *__restrict__ y, const double *__restrict__ z,
            const double *__restrict__ q, const int *__restrict__ slotOf,
-           long long *__restrict__ facc, int nSlots, long long *__restrict__ acc) {
+           long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   long long ecorr = 0, vcorr = 0;
   if (i < n) {
@@ -464,11 +464,11 @@ k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
                       fzj = fix_fd(dE * dz * rt);
       const int sj = slotOf[j];
       red_add(facc + si, fxj);
-      red_add(facc + (size_t)nSlots + si, fyj);
-      red_add(facc + 2 * (size_t)nSlots + si, fzj);
+      red_add(facc + (size_t)fstride + si, fyj);
+      red_add(facc + 2 * (size_t)fstride + si, fzj);
       red_add(facc + sj, -fxj);
-      red_add(facc + (size_t)nSlots + sj, -fyj);
-      red_add(facc + 2 * (size_t)nSlots + sj, -fzj);
+      red_add(facc + (size_t)fstride + sj, -fyj);
+      red_add(facc + 2 * (size_t)fstride + sj, -fzj);
     }
   }
 #pragma unroll
@@ -485,7 +485,7 @@ k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
 // Fixed-point forces (slot order) -> FP64 forces (atom order); accumulate
 // (+=) when add != 0, as MDBas's energy routines do.
 __global__ void k_forces_out(int n, const int *__restrict__ slotOf,
-                             const long long *__restrict__ facc, int nSlots, int add,
+                             const long long *__restrict__ facc, int fstride, int add,
                              double *__restrict__ fx, double *__restrict__ fy,
                              double *__restrict__ fz) {
   const int a = blockIdx.x * blockDim.x + threadIdx.x;
@@ -493,8 +493,8 @@ __global__ void k_forces_out(int n, const int *__restrict__ slotOf,
   const int s = slotOf[a];
   const double inv = 1.0 / kForceScale;
   const double vx = (double)facc[s] * inv;
-  const double vy = (double)facc[(size_t)nSlots + s] * inv;
-  const double vz = (double)facc[2 * (size_t)nSlots + s] * inv;
+  const double vy = (double)facc[(size_t)fstride + s] * inv;
+  const double vz = (double)facc[2 * (size_t)fstride + s] * inv;
   if (add) {
     fx[a] += vx;
     fy[a] += vy;
@@ -525,17 +525,16 @@ PairConstF make_pair_const(const PairParams &p) {
 int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
                      int variant) {
   const PairConstF c = make_pair_const(p);
-  if (w.nItems <= 0) return MDBAS_NB_OK;
   if (variant == kPairDense) {
     if (p.vdwSwitch)
       MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),
                  w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
-                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                  w.acc.as<long long>());
     else
       MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, w.counters.as<long long>(),
                  w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
-                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+                 w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                  w.acc.as<long long>());
     return MDBAS_NB_OK;
   }
@@ -557,12 +556,12 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   if (p.vdwSwitch)
     MDB_LAUNCH(k_pair_fp32c<true>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
                w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
-               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                w.acc.as<long long>());
   else
     MDB_LAUNCH(k_pair_fp32c<false>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
                w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
-               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.nSlots,
+               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                w.acc.as<long long>());
   return MDBAS_NB_OK;
 }
@@ -572,7 +571,7 @@ int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
                     const double *z, const double *q, cudaStream_t s) {
   if (n <= 0) return MDBAS_NB_OK;
   MDB_LAUNCH(k_excl_fix, grid_for(n, 128), 128, 0, s, n, b, p, exclStart, exclFlat, x, y, z, q,
-             w.slotOf.as<int>(), w.facc.as<long long>(), w.nSlots, w.acc.as<long long>());
+             w.slotOf.as<int>(), w.facc.as<long long>(), w.slotCap, w.acc.as<long long>());
   return MDBAS_NB_OK;
 }
 
@@ -580,7 +579,7 @@ int forces_out_launch(ClusterWork &w, int n, int add, double *fx, double *fy, do
                       cudaStream_t s) {
   if (n <= 0) return MDBAS_NB_OK;
   MDB_LAUNCH(k_forces_out, grid_for(n, 256), 256, 0, s, n, w.slotOf.as<int>(),
-             w.facc.as<long long>(), w.nSlots, add, fx, fy, fz);
+             w.facc.as<long long>(), w.slotCap, add, fx, fy, fz);
   return MDBAS_NB_OK;
 }
 

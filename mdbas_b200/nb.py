@@ -218,6 +218,7 @@ def lib():
     L.mdbas_nb_engine_md_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
                                          _dp]
     L.mdbas_nb_engine_md_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    L.mdbas_nb_engine_md_set_graph.argtypes = [C.c_void_p, C.c_int]
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
@@ -378,6 +379,10 @@ class Engine:
                                            buf.ctypes.data_as(_dp) if rows else None),
               "engine_md_run")
         return buf[:rows]
+
+    def md_set_graph(self, steps_per_launch: int):
+        """Steps per CUDA-graph launch of the mixed-precision dynamics (0 = off)."""
+        check(lib().mdbas_nb_engine_md_set_graph(self.h, steps_per_launch), "engine_md_set_graph")
 
     def md_stats(self):
         out = (C.c_longlong * 4)()

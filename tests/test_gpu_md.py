@@ -45,8 +45,10 @@ def _ref_md(sysm, vel, dt, steps, list_update, constraints=None, temp0=0.0, tau_
 
 
 def _gpu_md(sysm, vel, dt, steps, list_update, precision, constraints=None, temp0=0.0,
-            tau_t=0.0, frozen=None):
+            tau_t=0.0, frozen=None, graph=None):
     e = nb.Engine(sysm, precision=precision, frozen=frozen, **POT)
+    if graph is not None:
+        e.md_set_graph(graph)
     e.md_init(sysm.mass, vel, time_step=dt, list_update=list_update, constraints=constraints)
     rows = e.md_run(steps, energy_every=1, target_temp=temp0, tau_t=tau_t)
     out = e.positions(), e.velocities(), rows, e.md_stats(), e.launches()
@@ -182,3 +184,36 @@ def test_md_mixed_nve_conserves_energy(gpu):
           f"rebuilds {st['rebuilds']}")
     assert abs(drift) < 0.01
     assert spread < 0.02
+
+
+@pytest.mark.parametrize("list_update", [0, 7])
+def test_md_graph_matches_stepwise_bitwise(gpu, water, list_update):
+    """Whole steps captured as CUDA graphs (device-side rebuild decision,
+    conditional list build) give the trajectory of the host-driven loop bit
+    for bit, energies included; 70 steps = three 20-step launches + 10 more."""
+    vel = (water.vx, water.vy, water.vz)
+    cons = water.water_constraints()
+    ap, av, arows, ast, al = _gpu_md(water, vel, 0.002, 70, list_update, 1, cons, graph=20)
+    bp, bv, brows, bst, bl = _gpu_md(water, vel, 0.002, 70, list_update, 1, cons, graph=0)
+    print(f"graph rebuilds {ast['rebuilds']} launches {al}; stepwise {bst['rebuilds']} {bl}")
+    assert ast["rebuilds"] == bst["rebuilds"] > 1
+    for k in range(3):
+        assert np.array_equal(ap[k], bp[k])
+        assert np.array_equal(av[k], bv[k])
+    assert np.array_equal(arows, brows)
+    assert al > 70 * 10
+
+
+def test_md_graph_berendsen_and_frozen(gpu, water):
+    vel = (water.vx, water.vy, water.vz)
+    cons = water.water_constraints()
+    frozen = np.zeros(water.n, np.int32)
+    frozen[3:9] = 1
+    a = _gpu_md(water, vel, 0.001, 40, 0, 1, cons, temp0=250.0, tau_t=0.05, frozen=frozen,
+                graph=20)
+    b = _gpu_md(water, vel, 0.001, 40, 0, 1, cons, temp0=250.0, tau_t=0.05, frozen=frozen,
+                graph=0)
+    for k in range(3):
+        assert np.array_equal(a[0][k], b[0][k])
+    assert np.array_equal(a[2], b[2])
+    assert all(np.all(a[1][k][3:9] == 0.0) for k in range(3))
