@@ -45,6 +45,10 @@ struct mdbas_nb_engine {
   double mdDt = 0.0, mdTol = 1e-8;
   long long mdSteps = 0, mdRebuilds = 0, mdShakeIter = 0;
   bool mdReady = false;
+  bool mdTri = false;   // every constrained molecule a rigid triangle (fused kernels)
+  int mdNTri = 0;       // atoms in those triangles
+  mdbas::DBuf mdTriAtoms, mdTriLen2;  // int4 / double4 per molecule
+  int mdMolClass = 0;  // SHAKE kernel class: 0 <= 3 atoms/3 constraints, 1 <= 4/6, 2 <= 16/32
   // CUDA graph of mdGraphSteps whole steps (precision 1); rebuilt when stale
   int mdGraphSteps = 20, mdGraphK = 0;
   long long mdGraphMainK = 0, mdGraphBodyK = 0;  // kernels per step / per rebuild

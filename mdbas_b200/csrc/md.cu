@@ -38,18 +38,21 @@ using namespace mdbas;
 namespace mdbas {
 namespace {
 
-constexpr int kMolMaxAtoms = 16;
-constexpr int kMolMaxCons = 32;
+// Molecule size classes of the SHAKE kernels: (atoms, constraints).
+constexpr int kMolTinyAtoms = 3, kMolTinyCons = 3;      // rigid water, X-H bonds
+constexpr int kMolSmallAtoms = 4, kMolSmallCons = 6;    // CH3, NH3+ ...
+constexpr int kMolMaxAtoms = 16, kMolMaxCons = 32;      // the largest accepted
 
 // stage 1 of vv_nve: half kick then drift (src/integrate.c:1555-1580)
+// (atoms with skip[i] != 0 are integrated by the fused rigid-triangle kernels)
 __global__ void k_vv_stage1(int n, double dt, const double *__restrict__ fx,
                             const double *__restrict__ fy, const double *__restrict__ fz,
                             const double *__restrict__ rmass, double *__restrict__ vx,
                             double *__restrict__ vy, double *__restrict__ vz,
                             double *__restrict__ x, double *__restrict__ y,
-                            double *__restrict__ z) {
+                            double *__restrict__ z, const int *__restrict__ skip) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || (skip && skip[i])) return;
   vx[i] += 0.5 * dt * fx[i] * rmass[i];
   vy[i] += 0.5 * dt * fy[i] * rmass[i];
   vz[i] += 0.5 * dt * fz[i] * rmass[i];
@@ -61,9 +64,10 @@ __global__ void k_vv_stage1(int n, double dt, const double *__restrict__ fx,
 __global__ void k_vv_kick(int n, double dt, const double *__restrict__ fx,
                           const double *__restrict__ fy, const double *__restrict__ fz,
                           const double *__restrict__ rmass, double *__restrict__ vx,
-                          double *__restrict__ vy, double *__restrict__ vz) {
+                          double *__restrict__ vy, double *__restrict__ vz,
+                          const int *__restrict__ skip) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  if (i >= n || (skip && skip[i])) return;
   vx[i] += 0.5 * dt * fx[i] * rmass[i];
   vy[i] += 0.5 * dt * fy[i] * rmass[i];
   vz[i] += 0.5 * dt * fz[i] * rmass[i];
@@ -84,190 +88,523 @@ __global__ void k_cons_vectors(int nc, DevBox b, const int *__restrict__ ca,
   ddz[c] = dz;
 }
 
-// Per-molecule SHAKE on positions and velocities (vv_shake_r).
-__global__ void k_shake_positions(int nMol, DevBox b, double dt, double tol, int maxCycle,
-                                  const int *__restrict__ molCons, const int *__restrict__ ca,
-                                  const int *__restrict__ cb, const double *__restrict__ rc2,
-                                  const double *__restrict__ ddx, const double *__restrict__ ddy,
-                                  const double *__restrict__ ddz,
-                                  const double *__restrict__ rmass,
-                                  const int *__restrict__ nAtConst, double *__restrict__ x,
-                                  double *__restrict__ y, double *__restrict__ z,
-                                  double *__restrict__ vx, double *__restrict__ vy,
-                                  double *__restrict__ vz, int *__restrict__ status) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nMol) return;
-  const int c0 = molCons[m], c1 = molCons[m + 1];
-  const int ncons = c1 - c0;
-  if (ncons <= 0) return;
-  if (ncons > kMolMaxCons) {
-    atomicOr(status, 2);
-    return;
+// --- per-molecule SHAKE / RATTLE ----------------------------------------------
+// One thread per molecule holds the molecule's atoms (at most MA) and
+// constraints (at most MC) in registers for the whole iteration: local atom
+// numbers are resolved once, and every access by a run-time local number is
+// a compile-time select over MA registers, so nothing goes to local memory.
+
+// (The large class indexes its arrays directly, from local memory.)
+template <int MA>
+__device__ __forceinline__ double pick(const double (&v)[MA], int i) {
+  if constexpr (MA > kMolSmallAtoms) {
+    return v[i];
+  } else {
+    double r = 0.;
+#pragma unroll
+    for (int t = 0; t < MA; ++t)
+      if (t == i) r = v[t];
+    return r;
   }
-  // local atom table of the molecule
-  int atoms[kMolMaxAtoms];
-  int na = 0;
-  int la[kMolMaxCons], lb[kMolMaxCons];
-  for (int k = 0; k < ncons; ++k) {
-    const int a = ca[c0 + k], bb = cb[c0 + k];
-    int ia = -1, ib = -1;
-    for (int t = 0; t < na; ++t) {
-      if (atoms[t] == a) ia = t;
-      if (atoms[t] == bb) ib = t;
-    }
-    if (ia < 0) {
-      if (na >= kMolMaxAtoms) { atomicOr(status, 2); return; }
-      ia = na;
-      atoms[na++] = a;
-    }
-    if (ib < 0) {
-      if (na >= kMolMaxAtoms) { atomicOr(status, 2); return; }
-      ib = na;
-      atoms[na++] = bb;
-    }
-    la[k] = ia;
-    lb[k] = ib;
-  }
-  double xt[kMolMaxAtoms], yt[kMolMaxAtoms], zt[kMolMaxAtoms];
-  double rt2[kMolMaxCons], tx[kMolMaxCons], ty[kMolMaxCons], tz[kMolMaxCons];
-  bool converged = false;
-  int icycle = 0;
-  do {
-    double maxdist = 0.;
-    for (int k = 0; k < ncons; ++k) {
-      const int a = atoms[la[k]], bb = atoms[lb[k]];
-      double dx = x[bb] - x[a], dy = y[bb] - y[a], dz = z[bb] - z[a];
-      rt2[k] = dist_d(b, dx, dy, dz);
-      tx[k] = dx;
-      ty[k] = dy;
-      tz[k] = dz;
-      const double dist = fabs(rt2[k] - rc2[c0 + k]) / sqrt(rc2[c0 + k]);
-      maxdist = fmax(maxdist, dist);
-    }
-    maxdist = 0.5 * maxdist;
-    if (maxdist < tol) converged = true;
-    if (!converged) {
-      for (int t = 0; t < na; ++t) xt[t] = yt[t] = zt[t] = 0.;
-      for (int k = 0; k < ncons; ++k) {
-        const int c = c0 + k;
-        const int a = atoms[la[k]], bb = atoms[lb[k]];
-        const double trmi = dt * rmass[a];
-        const double trmj = dt * rmass[bb];
-        const double lambda = -(rc2[c] - rt2[k]) /
-                              (dt * (trmi + trmj) * ((ddx[c] * tx[k]) + (ddy[c] * ty[k]) +
-                                                     (ddz[c] * tz[k])));
-        const double lambdai = 0.5 * lambda * trmi;
-        xt[la[k]] += ddx[c] * lambdai;
-        yt[la[k]] += ddy[c] * lambdai;
-        zt[la[k]] += ddz[c] * lambdai;
-        const double lambdaj = -0.5 * lambda * trmj;
-        xt[lb[k]] += ddx[c] * lambdaj;
-        yt[lb[k]] += ddy[c] * lambdaj;
-        zt[lb[k]] += ddz[c] * lambdaj;
-      }
-      for (int k = 0; k < ncons; ++k) {
-        const int a = atoms[la[k]], bb = atoms[lb[k]];
-        const double nia = 1.0 / (double)nAtConst[a];
-        const double nib = 1.0 / (double)nAtConst[bb];
-        x[a] += dt * xt[la[k]] * nia;
-        y[a] += dt * yt[la[k]] * nia;
-        z[a] += dt * zt[la[k]] * nia;
-        x[bb] += dt * xt[lb[k]] * nib;
-        y[bb] += dt * yt[lb[k]] * nib;
-        z[bb] += dt * zt[lb[k]] * nib;
-        vx[a] += xt[la[k]] * nia;
-        vy[a] += yt[la[k]] * nia;
-        vz[a] += zt[la[k]] * nia;
-        vx[bb] += xt[lb[k]] * nib;
-        vy[bb] += yt[lb[k]] * nib;
-        vz[bb] += zt[lb[k]] * nib;
-      }
-    }
-    ++icycle;
-  } while (!converged && icycle < maxCycle);
-  if (!converged) atomicOr(status, 1);  // CONVERG_SHAKE_ERROR
-  atomicMax(status + 1, icycle);
 }
 
-// Per-molecule SHAKE on velocities (vv_shake_v).
-__global__ void k_shake_velocities(int nMol, double dt, double tolvel, int maxCycle,
-                                   const int *__restrict__ molCons, const int *__restrict__ ca,
-                                   const int *__restrict__ cb, const double *__restrict__ ddx,
-                                   const double *__restrict__ ddy,
-                                   const double *__restrict__ ddz,
-                                   const double *__restrict__ rmass,
-                                   const int *__restrict__ nAtConst, double *__restrict__ vx,
-                                   double *__restrict__ vy, double *__restrict__ vz,
-                                   int *__restrict__ status) {
-  const int m = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m >= nMol) return;
-  const int c0 = molCons[m], c1 = molCons[m + 1];
-  const int ncons = c1 - c0;
-  if (ncons <= 0 || ncons > kMolMaxCons) return;
-  int atoms[kMolMaxAtoms];
-  int na = 0;
-  int la[kMolMaxCons], lb[kMolMaxCons];
-  for (int k = 0; k < ncons; ++k) {
-    const int a = ca[c0 + k], bb = cb[c0 + k];
-    int ia = -1, ib = -1;
-    for (int t = 0; t < na; ++t) {
-      if (atoms[t] == a) ia = t;
-      if (atoms[t] == bb) ib = t;
-    }
-    if (ia < 0) {
-      if (na >= kMolMaxAtoms) return;
-      ia = na;
-      atoms[na++] = a;
-    }
-    if (ib < 0) {
-      if (na >= kMolMaxAtoms) return;
-      ib = na;
-      atoms[na++] = bb;
-    }
-    la[k] = ia;
-    lb[k] = ib;
+template <int MA>
+__device__ __forceinline__ void add_to(double (&v)[MA], int i, double d) {
+  if constexpr (MA > kMolSmallAtoms) {
+    v[i] += d;
+  } else {
+#pragma unroll
+    for (int t = 0; t < MA; ++t)
+      if (t == i) v[t] += d;
   }
-  double xt[kMolMaxAtoms], yt[kMolMaxAtoms], zt[kMolMaxAtoms];
+}
+
+// Local numbering of the molecule's atoms in order of first appearance;
+// false when it has more than MA atoms.
+template <int MA, int MC>
+__device__ __forceinline__ bool mol_table(int c0, int ncons, const int *__restrict__ ca,
+                                          const int *__restrict__ cb, int (&atoms)[MA], int &na,
+                                          int (&la)[MC], int (&lb)[MC]) {
+  na = 0;
+#pragma unroll
+  for (int t = 0; t < MA; ++t) atoms[t] = -1;
+#pragma unroll
+  for (int k = 0; k < MC; ++k) {
+    la[k] = 0;
+    lb[k] = 0;
+    if (k < ncons) {
+      const int a = ca[c0 + k], b = cb[c0 + k];
+      int ia = -1, ib = -1;
+#pragma unroll
+      for (int t = 0; t < MA; ++t) {
+        if (atoms[t] == a) ia = t;
+        if (atoms[t] == b) ib = t;
+      }
+      if (ia < 0) {
+        if (na >= MA) return false;
+        ia = na;
+#pragma unroll
+        for (int t = 0; t < MA; ++t)
+          if (t == na) atoms[t] = a;
+        ++na;
+      }
+      if (ib < 0) {
+        if (na >= MA) return false;
+        ib = na;
+#pragma unroll
+        for (int t = 0; t < MA; ++t)
+          if (t == na) atoms[t] = b;
+        ++na;
+      }
+      la[k] = ia;
+      lb[k] = ib;
+    }
+  }
+  return true;
+}
+
+// Largest iteration count over the warp, one atomic per warp.
+__device__ __forceinline__ void report_cycles(int *status, int icycle) {
+  const int m = __reduce_max_sync(0xffffffffu, icycle);
+  if ((threadIdx.x & 31) == 0 && m > 0) atomicMax(status + 1, m);
+}
+
+// SHAKE on positions (vv_shake_r, src/shake.c:209-326): Jacobi corrections
+// of all constraints, averaged over each atom's constraint count, until the
+// largest relative bond error is below tol; positions and velocities move.
+template <int MA, int MC>
+__global__ void __launch_bounds__(128)
+k_shake_positions(int nMol, DevBox b, double dt, double tol, int maxCycle,
+                  const int *__restrict__ molCons, const int *__restrict__ ca,
+                  const int *__restrict__ cb, const double *__restrict__ rc2g,
+                  const double *__restrict__ ddxg, const double *__restrict__ ddyg,
+                  const double *__restrict__ ddzg, const double *__restrict__ rmass,
+                  const int *__restrict__ nAtConst, double *__restrict__ x,
+                  double *__restrict__ y, double *__restrict__ z, double *__restrict__ vx,
+                  double *__restrict__ vy, double *__restrict__ vz, int *__restrict__ status) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int c0 = 0, ncons = 0;
+  if (m < nMol) {
+    c0 = molCons[m];
+    ncons = molCons[m + 1] - c0;
+  }
+  int icycle = 0;
+  int atoms[MA], la[MC], lb[MC], na = 0;
+  bool active = ncons > 0;
+  if (active && (ncons > MC || !mol_table<MA, MC>(c0, ncons, ca, cb, atoms, na, la, lb))) {
+    atomicOr(status, 2);
+    active = false;
+  }
+  if (active) {
+    double px[MA], py[MA], pz[MA], qx[MA], qy[MA], qz[MA], rm[MA], inv[MA];
+#pragma unroll
+    for (int t = 0; t < MA; ++t) {
+      px[t] = py[t] = pz[t] = qx[t] = qy[t] = qz[t] = rm[t] = inv[t] = 0.;
+      if (t < na) {
+        const int a = atoms[t];
+        px[t] = x[a];
+        py[t] = y[a];
+        pz[t] = z[a];
+        qx[t] = vx[a];
+        qy[t] = vy[a];
+        qz[t] = vz[a];
+        rm[t] = rmass[a];
+        inv[t] = 1.0 / (double)nAtConst[a];
+      }
+    }
+    double dcx[MC], dcy[MC], dcz[MC], r2c[MC], irc[MC];
+#pragma unroll
+    for (int k = 0; k < MC; ++k) {
+      dcx[k] = dcy[k] = dcz[k] = 0.;
+      r2c[k] = irc[k] = 1.;
+      if (k < ncons) {
+        dcx[k] = ddxg[c0 + k];
+        dcy[k] = ddyg[c0 + k];
+        dcz[k] = ddzg[c0 + k];
+        r2c[k] = rc2g[c0 + k];
+        irc[k] = 1.0 / sqrt(r2c[k]);
+      }
+    }
+    bool converged = false;
+    do {
+      // current bond vectors (minimum image) and the largest relative error
+      double tx[MC], ty[MC], tz[MC], rt2[MC];
+      double maxdist = 0.;
+#pragma unroll
+      for (int k = 0; k < MC; ++k) {
+        tx[k] = ty[k] = tz[k] = rt2[k] = 0.;
+        if (k < ncons) {
+          tx[k] = pick(px, lb[k]) - pick(px, la[k]);
+          ty[k] = pick(py, lb[k]) - pick(py, la[k]);
+          tz[k] = pick(pz, lb[k]) - pick(pz, la[k]);
+          rt2[k] = dist_d(b, tx[k], ty[k], tz[k]);
+          maxdist = fmax(maxdist, fabs(rt2[k] - r2c[k]) * irc[k]);
+        }
+      }
+      maxdist = 0.5 * maxdist;
+      if (maxdist < tol) converged = true;
+      if (!converged) {
+        double xt[MA], yt[MA], zt[MA];
+#pragma unroll
+        for (int t = 0; t < MA; ++t) xt[t] = yt[t] = zt[t] = 0.;
+#pragma unroll
+        for (int k = 0; k < MC; ++k) {
+          if (k < ncons) {
+            const double dx = tx[k], dy = ty[k], dz = tz[k];
+            const double trmi = dt * pick(rm, la[k]);
+            const double trmj = dt * pick(rm, lb[k]);
+            const double lambda = -(r2c[k] - rt2[k]) /
+                                  (dt * (trmi + trmj) *
+                                   ((dcx[k] * dx) + (dcy[k] * dy) + (dcz[k] * dz)));
+            const double lambdai = 0.5 * lambda * trmi;
+            add_to(xt, la[k], dcx[k] * lambdai);
+            add_to(yt, la[k], dcy[k] * lambdai);
+            add_to(zt, la[k], dcz[k] * lambdai);
+            const double lambdaj = -0.5 * lambda * trmj;
+            add_to(xt, lb[k], dcx[k] * lambdaj);
+            add_to(yt, lb[k], dcy[k] * lambdaj);
+            add_to(zt, lb[k], dcz[k] * lambdaj);
+          }
+        }
+        // applied per constraint, each atom's share scaled by 1/nAtConst
+#pragma unroll
+        for (int k = 0; k < MC; ++k) {
+          if (k < ncons) {
+            const double nia = pick(inv, la[k]), nib = pick(inv, lb[k]);
+            const double xa = pick(xt, la[k]), ya = pick(yt, la[k]), za = pick(zt, la[k]);
+            const double xb = pick(xt, lb[k]), yb = pick(yt, lb[k]), zb = pick(zt, lb[k]);
+            add_to(px, la[k], dt * xa * nia);
+            add_to(py, la[k], dt * ya * nia);
+            add_to(pz, la[k], dt * za * nia);
+            add_to(px, lb[k], dt * xb * nib);
+            add_to(py, lb[k], dt * yb * nib);
+            add_to(pz, lb[k], dt * zb * nib);
+            add_to(qx, la[k], xa * nia);
+            add_to(qy, la[k], ya * nia);
+            add_to(qz, la[k], za * nia);
+            add_to(qx, lb[k], xb * nib);
+            add_to(qy, lb[k], yb * nib);
+            add_to(qz, lb[k], zb * nib);
+          }
+        }
+      }
+      ++icycle;
+    } while (!converged && icycle < maxCycle);
+    if (!converged) atomicOr(status, 1);  // CONVERG_SHAKE_ERROR
+#pragma unroll
+    for (int t = 0; t < MA; ++t) {
+      if (t < na) {
+        const int a = atoms[t];
+        x[a] = px[t];
+        y[a] = py[t];
+        z[a] = pz[t];
+        vx[a] = qx[t];
+        vy[a] = qy[t];
+        vz[a] = qz[t];
+      }
+    }
+  }
+  report_cycles(status, icycle);
+}
+
+// SHAKE on velocities (vv_shake_v, src/shake.c:328-456).
+template <int MA, int MC>
+__global__ void __launch_bounds__(128)
+k_shake_velocities(int nMol, double dt, double tolvel, int maxCycle,
+                   const int *__restrict__ molCons, const int *__restrict__ ca,
+                   const int *__restrict__ cb, const double *__restrict__ ddxg,
+                   const double *__restrict__ ddyg, const double *__restrict__ ddzg,
+                   const double *__restrict__ rmass, const int *__restrict__ nAtConst,
+                   double *__restrict__ vx, double *__restrict__ vy, double *__restrict__ vz,
+                   int *__restrict__ status) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int c0 = 0, ncons = 0;
+  if (m < nMol) {
+    c0 = molCons[m];
+    ncons = molCons[m + 1] - c0;
+  }
+  int atoms[MA], la[MC], lb[MC], na = 0;
+  const bool active =
+      ncons > 0 && ncons <= MC && mol_table<MA, MC>(c0, ncons, ca, cb, atoms, na, la, lb);
+  if (!active) return;
+  double qx[MA], qy[MA], qz[MA], rm[MA], inv[MA];
+#pragma unroll
+  for (int t = 0; t < MA; ++t) {
+    qx[t] = qy[t] = qz[t] = rm[t] = inv[t] = 0.;
+    if (t < na) {
+      const int a = atoms[t];
+      qx[t] = vx[a];
+      qy[t] = vy[a];
+      qz[t] = vz[a];
+      rm[t] = rmass[a];
+      inv[t] = 1.0 / (double)nAtConst[a];
+    }
+  }
+  double dcx[MC], dcy[MC], dcz[MC];
+#pragma unroll
+  for (int k = 0; k < MC; ++k) {
+    dcx[k] = dcy[k] = dcz[k] = 0.;
+    if (k < ncons) {
+      dcx[k] = ddxg[c0 + k];
+      dcy[k] = ddyg[c0 + k];
+      dcz[k] = ddzg[c0 + k];
+    }
+  }
   bool converged = false;
   int icycle = 0;
   do {
-    for (int t = 0; t < na; ++t) xt[t] = yt[t] = zt[t] = 0.;
+    double xt[MA], yt[MA], zt[MA];
+#pragma unroll
+    for (int t = 0; t < MA; ++t) xt[t] = yt[t] = zt[t] = 0.;
     double maxdist = 0.;
-    for (int k = 0; k < ncons; ++k) {
-      const int c = c0 + k;
-      const int a = atoms[la[k]], bb = atoms[lb[k]];
-      const double trmi = 0.5 * dt * rmass[a];
-      const double trmj = 0.5 * dt * rmass[bb];
-      const double lambda =
-          (ddx[c] * (vx[bb] - vx[a]) + ddy[c] * (vy[bb] - vy[a]) + ddz[c] * (vz[bb] - vz[a])) /
-          ((trmi + trmj) * (ddx[c] * ddx[c] + ddy[c] * ddy[c] + ddz[c] * ddz[c]));
-      maxdist = fmax(maxdist, fabs(lambda));
-      const double lambdai = lambda * trmi;
-      xt[la[k]] += ddx[c] * lambdai;
-      yt[la[k]] += ddy[c] * lambdai;
-      zt[la[k]] += ddz[c] * lambdai;
-      const double lambdaj = -lambda * trmj;
-      xt[lb[k]] += ddx[c] * lambdaj;
-      yt[lb[k]] += ddy[c] * lambdaj;
-      zt[lb[k]] += ddz[c] * lambdaj;
+#pragma unroll
+    for (int k = 0; k < MC; ++k) {
+      if (k < ncons) {
+        const double trmi = 0.5 * dt * pick(rm, la[k]);
+        const double trmj = 0.5 * dt * pick(rm, lb[k]);
+        const double lambda =
+            (dcx[k] * (pick(qx, lb[k]) - pick(qx, la[k])) +
+             dcy[k] * (pick(qy, lb[k]) - pick(qy, la[k])) +
+             dcz[k] * (pick(qz, lb[k]) - pick(qz, la[k]))) /
+            ((trmi + trmj) * (dcx[k] * dcx[k] + dcy[k] * dcy[k] + dcz[k] * dcz[k]));
+        maxdist = fmax(maxdist, fabs(lambda));
+        const double lambdai = lambda * trmi;
+        add_to(xt, la[k], dcx[k] * lambdai);
+        add_to(yt, la[k], dcy[k] * lambdai);
+        add_to(zt, la[k], dcz[k] * lambdai);
+        const double lambdaj = -lambda * trmj;
+        add_to(xt, lb[k], dcx[k] * lambdaj);
+        add_to(yt, lb[k], dcy[k] * lambdaj);
+        add_to(zt, lb[k], dcz[k] * lambdaj);
+      }
     }
     if (maxdist < tolvel) converged = true;
     if (!converged) {
-      for (int k = 0; k < ncons; ++k) {
-        const int a = atoms[la[k]], bb = atoms[lb[k]];
-        const double nia = 1.0 / (double)nAtConst[a];
-        const double nib = 1.0 / (double)nAtConst[bb];
-        vx[a] += xt[la[k]] * nia;
-        vy[a] += yt[la[k]] * nia;
-        vz[a] += zt[la[k]] * nia;
-        vx[bb] += xt[lb[k]] * nib;
-        vy[bb] += yt[lb[k]] * nib;
-        vz[bb] += zt[lb[k]] * nib;
+#pragma unroll
+      for (int k = 0; k < MC; ++k) {
+        if (k < ncons) {
+          const double nia = pick(inv, la[k]), nib = pick(inv, lb[k]);
+          add_to(qx, la[k], pick(xt, la[k]) * nia);
+          add_to(qy, la[k], pick(yt, la[k]) * nia);
+          add_to(qz, la[k], pick(zt, la[k]) * nia);
+          add_to(qx, lb[k], pick(xt, lb[k]) * nib);
+          add_to(qy, lb[k], pick(yt, lb[k]) * nib);
+          add_to(qz, lb[k], pick(zt, lb[k]) * nib);
+        }
       }
     }
     ++icycle;
   } while (!converged && icycle < maxCycle);
   if (!converged) atomicOr(status, 1);
+#pragma unroll
+  for (int t = 0; t < MA; ++t) {
+    if (t < na) {
+      const int a = atoms[t];
+      vx[a] = qx[t];
+      vy[a] = qy[t];
+      vz[a] = qz[t];
+    }
+  }
+}
+
+// --- rigid triangles (3 atoms, 3 constraints: rigid water) ---------------------
+// All of a molecule's stage-1 (or stage-2) work in one thread with the local
+// numbering fixed at compile time: constraint 0 = (a0, a1), 1 = (a0, a2),
+// 2 = (a1, a2); every atom belongs to two constraints (nAtConst = 2).  The
+// iteration is vv_shake_r / vv_shake_v's.
+__device__ __forceinline__ void tri_vectors(const DevBox &b, const double (&px)[3],
+                                            const double (&py)[3], const double (&pz)[3],
+                                            double (&dx)[3], double (&dy)[3], double (&dz)[3],
+                                            double (&r2)[3]) {
+  constexpr int LA[3] = {0, 0, 1}, LB[3] = {1, 2, 2};
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    dx[k] = px[LB[k]] - px[LA[k]];
+    dy[k] = py[LB[k]] - py[LA[k]];
+    dz[k] = pz[LB[k]] - pz[LA[k]];
+    r2[k] = dist_d(b, dx[k], dy[k], dz[k]);
+  }
+}
+
+__global__ void __launch_bounds__(128)
+k_tri_stage1(int nTri, DevBox b, double dt, double tol, int maxCycle,
+             const int4 *__restrict__ tri, const double4 *__restrict__ len2,
+             const double *__restrict__ fx, const double *__restrict__ fy,
+             const double *__restrict__ fz, const double *__restrict__ rmass,
+             double *__restrict__ x, double *__restrict__ y, double *__restrict__ z,
+             double *__restrict__ vx, double *__restrict__ vy, double *__restrict__ vz,
+             int *__restrict__ status) {
+  constexpr int LA[3] = {0, 0, 1}, LB[3] = {1, 2, 2};
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  int icycle = 0;
+  if (m < nTri) {
+    const int4 t = tri[m];
+    const int A[3] = {t.x, t.y, t.z};
+    const double4 l2 = len2[m];
+    const double r2c[3] = {l2.x, l2.y, l2.z};
+    double irc[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) irc[k] = 1.0 / sqrt(r2c[k]);
+    double px[3], py[3], pz[3], qx[3], qy[3], qz[3], rm[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      px[i] = x[A[i]];
+      py[i] = y[A[i]];
+      pz[i] = z[A[i]];
+      qx[i] = vx[A[i]];
+      qy[i] = vy[A[i]];
+      qz[i] = vz[A[i]];
+      rm[i] = rmass[A[i]];
+    }
+    // constraint vectors before the drift
+    double dcx[3], dcy[3], dcz[3], unused[3];
+    tri_vectors(b, px, py, pz, dcx, dcy, dcz, unused);
+    // half kick and drift
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      qx[i] += 0.5 * dt * fx[A[i]] * rm[i];
+      qy[i] += 0.5 * dt * fy[A[i]] * rm[i];
+      qz[i] += 0.5 * dt * fz[A[i]] * rm[i];
+      px[i] += dt * qx[i];
+      py[i] += dt * qy[i];
+      pz[i] += dt * qz[i];
+    }
+    bool converged = false;
+    do {
+      double tx[3], ty[3], tz[3], rt2[3];
+      tri_vectors(b, px, py, pz, tx, ty, tz, rt2);
+      double maxdist = 0.;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) maxdist = fmax(maxdist, fabs(rt2[k] - r2c[k]) * irc[k]);
+      maxdist = 0.5 * maxdist;
+      if (maxdist < tol) converged = true;
+      if (!converged) {
+        double xt[3] = {0., 0., 0.}, yt[3] = {0., 0., 0.}, zt[3] = {0., 0., 0.};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int ia = LA[k], ib = LB[k];
+          const double trmi = dt * rm[ia], trmj = dt * rm[ib];
+          const double lambda = -(r2c[k] - rt2[k]) /
+                                (dt * (trmi + trmj) *
+                                 ((dcx[k] * tx[k]) + (dcy[k] * ty[k]) + (dcz[k] * tz[k])));
+          const double lambdai = 0.5 * lambda * trmi;
+          xt[ia] += dcx[k] * lambdai;
+          yt[ia] += dcy[k] * lambdai;
+          zt[ia] += dcz[k] * lambdai;
+          const double lambdaj = -0.5 * lambda * trmj;
+          xt[ib] += dcx[k] * lambdaj;
+          yt[ib] += dcy[k] * lambdaj;
+          zt[ib] += dcz[k] * lambdaj;
+        }
+        // each atom takes half its correction from each of its two constraints
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const int ia = LA[k], ib = LB[k];
+          px[ia] += dt * xt[ia] * 0.5;
+          py[ia] += dt * yt[ia] * 0.5;
+          pz[ia] += dt * zt[ia] * 0.5;
+          px[ib] += dt * xt[ib] * 0.5;
+          py[ib] += dt * yt[ib] * 0.5;
+          pz[ib] += dt * zt[ib] * 0.5;
+          qx[ia] += xt[ia] * 0.5;
+          qy[ia] += yt[ia] * 0.5;
+          qz[ia] += zt[ia] * 0.5;
+          qx[ib] += xt[ib] * 0.5;
+          qy[ib] += yt[ib] * 0.5;
+          qz[ib] += zt[ib] * 0.5;
+        }
+      }
+      ++icycle;
+    } while (!converged && icycle < maxCycle);
+    if (!converged) atomicOr(status, 1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      x[A[i]] = px[i];
+      y[A[i]] = py[i];
+      z[A[i]] = pz[i];
+      vx[A[i]] = qx[i];
+      vy[A[i]] = qy[i];
+      vz[A[i]] = qz[i];
+    }
+  }
+  report_cycles(status, icycle);
+}
+
+__global__ void __launch_bounds__(128)
+k_tri_stage2(int nTri, DevBox b, double dt, double tolvel, int maxCycle,
+             const int4 *__restrict__ tri, const double *__restrict__ fx,
+             const double *__restrict__ fy, const double *__restrict__ fz,
+             const double *__restrict__ rmass, const double *__restrict__ x,
+             const double *__restrict__ y, const double *__restrict__ z,
+             double *__restrict__ vx, double *__restrict__ vy, double *__restrict__ vz,
+             int *__restrict__ status) {
+  constexpr int LA[3] = {0, 0, 1}, LB[3] = {1, 2, 2};
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nTri) return;
+  const int4 t = tri[m];
+  const int A[3] = {t.x, t.y, t.z};
+  double px[3], py[3], pz[3], qx[3], qy[3], qz[3], rm[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    px[i] = x[A[i]];
+    py[i] = y[A[i]];
+    pz[i] = z[A[i]];
+    rm[i] = rmass[A[i]];
+    qx[i] = vx[A[i]] + 0.5 * dt * fx[A[i]] * rm[i];
+    qy[i] = vy[A[i]] + 0.5 * dt * fy[A[i]] * rm[i];
+    qz[i] = vz[A[i]] + 0.5 * dt * fz[A[i]] * rm[i];
+  }
+  // constraint vectors at the new positions; the denominators are fixed
+  double dcx[3], dcy[3], dcz[3], dd2[3], trm[3][2], iden[3];
+  tri_vectors(b, px, py, pz, dcx, dcy, dcz, dd2);
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    trm[k][0] = 0.5 * dt * rm[LA[k]];
+    trm[k][1] = 0.5 * dt * rm[LB[k]];
+    iden[k] = 1.0 / ((trm[k][0] + trm[k][1]) * dd2[k]);
+  }
+  bool converged = false;
+  int icycle = 0;
+  do {
+    double xt[3] = {0., 0., 0.}, yt[3] = {0., 0., 0.}, zt[3] = {0., 0., 0.};
+    double maxdist = 0.;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const int ia = LA[k], ib = LB[k];
+      const double lambda = (dcx[k] * (qx[ib] - qx[ia]) + dcy[k] * (qy[ib] - qy[ia]) +
+                             dcz[k] * (qz[ib] - qz[ia])) * iden[k];
+      maxdist = fmax(maxdist, fabs(lambda));
+      const double lambdai = lambda * trm[k][0];
+      xt[ia] += dcx[k] * lambdai;
+      yt[ia] += dcy[k] * lambdai;
+      zt[ia] += dcz[k] * lambdai;
+      const double lambdaj = -lambda * trm[k][1];
+      xt[ib] += dcx[k] * lambdaj;
+      yt[ib] += dcy[k] * lambdaj;
+      zt[ib] += dcz[k] * lambdaj;
+    }
+    if (maxdist < tolvel) converged = true;
+    if (!converged) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        const int ia = LA[k], ib = LB[k];
+        qx[ia] += xt[ia] * 0.5;
+        qy[ia] += yt[ia] * 0.5;
+        qz[ia] += zt[ia] * 0.5;
+        qx[ib] += xt[ib] * 0.5;
+        qy[ib] += yt[ib] * 0.5;
+        qz[ib] += zt[ib] * 0.5;
+      }
+    }
+    ++icycle;
+  } while (!converged && icycle < maxCycle);
+  if (!converged) atomicOr(status, 1);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    vx[A[i]] = qx[i];
+    vy[A[i]] = qy[i];
+    vz[A[i]] = qz[i];
+  }
 }
 
 // kinetic energy (src/utils.c:502-515), sum in fixed point (2^-24 units)
@@ -426,17 +763,33 @@ int md_stage1(mdbas_nb_engine *e, cudaStream_t s) {
   double *vx = e->mdV.as<double>(), *vy = vx + n, *vz = vy + n;
   const double *fx = e->mdF.as<double>(), *fy = fx + n, *fz = fy + n;
   double *ddx = e->mdDd.as<double>(), *ddy = ddx + nc, *ddz = ddy + nc;
+  if (e->mdTri) {
+    // rigid triangles: vectors, kick, drift and SHAKE fused per molecule;
+    // the atom kernel integrates the unconstrained atoms only
+    if (e->mdNTri < n)
+      MDB_LAUNCH(k_vv_stage1, grid_for(n, 256), 256, 0, s, n, e->mdDt, fx, fy, fz,
+                 e->mdRmass.as<double>(), vx, vy, vz, x, y, z, e->mdNAt.as<int>());
+    MDB_LAUNCH(k_tri_stage1, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, e->mdDt,
+               e->mdTol, e->mdMaxCycle, e->mdTriAtoms.as<int4>(), e->mdTriLen2.as<double4>(),
+               fx, fy, fz, e->mdRmass.as<double>(), x, y, z, vx, vy, vz,
+               reinterpret_cast<int *>(e->mdWord.as<long long>() + W_SHAKE));
+    return MDBAS_NB_OK;
+  }
   if (nc > 0)
     MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
                e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
   MDB_LAUNCH(k_vv_stage1, grid_for(n, 256), 256, 0, s, n, e->mdDt, fx, fy, fz,
-             e->mdRmass.as<double>(), vx, vy, vz, x, y, z);
-  if (nc > 0)
-    MDB_LAUNCH(k_shake_positions, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box,
+             e->mdRmass.as<double>(), vx, vy, vz, x, y, z, nullptr);
+  if (nc > 0) {
+    auto shake = e->mdMolClass == 0   ? k_shake_positions<kMolTinyAtoms, kMolTinyCons>
+                 : e->mdMolClass == 1 ? k_shake_positions<kMolSmallAtoms, kMolSmallCons>
+                                      : k_shake_positions<kMolMaxAtoms, kMolMaxCons>;
+    MDB_LAUNCH(shake, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box,
                e->mdDt, e->mdTol, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
                e->mdCb.as<int>(), e->mdRc2.as<double>(), ddx, ddy, ddz, e->mdRmass.as<double>(),
                e->mdNAt.as<int>(), x, y, z, vx, vy, vz,
                reinterpret_cast<int *>(e->mdWord.as<long long>() + W_SHAKE));
+  }
   return MDBAS_NB_OK;
 }
 
@@ -477,13 +830,26 @@ int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double 
   double *ddx = e->mdDd.as<double>(), *ddy = ddx + nc, *ddz = ddy + nc;
   long long *word = e->mdWord.as<long long>();
   const int g = grid_for(n, 256);
-  MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, e->mdDt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy,
-             vz);
-  if (nc > 0) {
+  if (e->mdTri) {
+    if (e->mdNTri < n)
+      MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, e->mdDt, fx, fy, fz, e->mdRmass.as<double>(), vx,
+                 vy, vz, e->mdNAt.as<int>());
+    MDB_LAUNCH(k_tri_stage2, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, e->mdDt,
+               e->mdTol / e->mdDt, e->mdMaxCycle, e->mdTriAtoms.as<int4>(), fx, fy, fz,
+               e->mdRmass.as<double>(), x, y, z, vx, vy, vz,
+               reinterpret_cast<int *>(word + W_SHAKE));
+  } else {
+    MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, e->mdDt, fx, fy, fz, e->mdRmass.as<double>(), vx, vy,
+               vz, nullptr);
+  }
+  if (nc > 0 && !e->mdTri) {
     // stage 2 takes the constraint vectors at the new positions
     MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
                e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
-    MDB_LAUNCH(k_shake_velocities, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->mdDt,
+    auto rattle = e->mdMolClass == 0   ? k_shake_velocities<kMolTinyAtoms, kMolTinyCons>
+                  : e->mdMolClass == 1 ? k_shake_velocities<kMolSmallAtoms, kMolSmallCons>
+                                       : k_shake_velocities<kMolMaxAtoms, kMolMaxCons>;
+    MDB_LAUNCH(rattle, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->mdDt,
                e->mdTol / e->mdDt, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
                e->mdCb.as<int>(), ddx, ddy, ddz, e->mdRmass.as<double>(), e->mdNAt.as<int>(), vx,
                vy, vz, reinterpret_cast<int *>(word + W_SHAKE));
@@ -512,7 +878,7 @@ int md_check_shake(mdbas_nb_engine *e, const int st[2]) {
     return MDBAS_NB_ERR_UNSUPPORTED;
   }
   if (st[0] & 2) {
-    set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "a constrained molecule exceeds 16 atoms");
+    set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "a constrained molecule exceeds 16 atoms or 32 constraints");
     return MDBAS_NB_ERR_UNSUPPORTED;
   }
   return MDBAS_NB_OK;
@@ -782,6 +1148,8 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   // constraints grouped by molecule (connected components)
   e->mdNCons = nConst;
   e->mdNMol = 0;
+  e->mdTri = false;
+  e->mdNTri = 0;
   if (nConst > 0) {
     std::vector<int> parent(n);
     for (int i = 0; i < n; ++i) parent[i] = i;
@@ -818,6 +1186,70 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
       molStart[molKey[k] + 1]++;
     }
     for (int m = 0; m < nMol; ++m) molStart[m + 1] += molStart[m];
+    // molecule sizes: atoms and constraints of the largest molecule
+    std::vector<int> molAtoms(nMol, 0);
+    for (int i = 0; i < n; ++i)
+      if (cnt[i] > 0) molAtoms[rootMol[find(i)]]++;
+    int maxAtoms = 0, maxCons = 0;
+    for (int m = 0; m < nMol; ++m) {
+      maxAtoms = std::max(maxAtoms, molAtoms[m]);
+      maxCons = std::max(maxCons, molStart[m + 1] - molStart[m]);
+    }
+    if (maxAtoms > kMolMaxAtoms || maxCons > kMolMaxCons) {
+      set_last_status(MDBAS_NB_ERR_UNSUPPORTED,
+                      "a constrained molecule exceeds 16 atoms or 32 constraints");
+      return MDBAS_NB_ERR_UNSUPPORTED;
+    }
+    // every molecule a rigid triangle (3 atoms, the 3 pairs constrained)?
+    bool allTri = true;
+    std::vector<int> triAtoms;
+    std::vector<double> triLen2;
+    if (maxAtoms == 3 && maxCons == 3) {
+      triAtoms.resize(4 * (size_t)nMol);
+      triLen2.resize(4 * (size_t)nMol);
+      for (int m = 0; m < nMol && allTri; ++m) {
+        const int c0 = molStart[m];
+        if (molStart[m + 1] - c0 != 3) { allTri = false; break; }
+        // a0 = the first constraint's first atom, a1 its second, a2 the other
+        const int a0 = ca[c0], a1 = cb[c0];
+        int a2 = -1;
+        for (int k = 1; k < 3; ++k)
+          for (int v : {ca[c0 + k], cb[c0 + k]})
+            if (v != a0 && v != a1) a2 = v;
+        if (a2 < 0) { allTri = false; break; }
+        double l01 = -1, l02 = -1, l12 = -1;
+        for (int k = 0; k < 3; ++k) {
+          const int u = std::min(ca[c0 + k], cb[c0 + k]), v = std::max(ca[c0 + k], cb[c0 + k]);
+          if (u == std::min(a0, a1) && v == std::max(a0, a1)) l01 = r2[c0 + k];
+          else if (u == std::min(a0, a2) && v == std::max(a0, a2)) l02 = r2[c0 + k];
+          else if (u == std::min(a1, a2) && v == std::max(a1, a2)) l12 = r2[c0 + k];
+        }
+        if (l01 < 0 || l02 < 0 || l12 < 0) { allTri = false; break; }
+        triAtoms[4 * m + 0] = a0;
+        triAtoms[4 * m + 1] = a1;
+        triAtoms[4 * m + 2] = a2;
+        triAtoms[4 * m + 3] = 0;
+        triLen2[4 * m + 0] = l01;
+        triLen2[4 * m + 1] = l02;
+        triLen2[4 * m + 2] = l12;
+        triLen2[4 * m + 3] = 0.;
+      }
+    } else {
+      allTri = false;
+    }
+    e->mdTri = allTri;
+    e->mdNTri = allTri ? 3 * nMol : 0;
+    if (allTri) {
+      MD_TRY(e->mdTriAtoms.ensure(sizeof(int4) * (size_t)nMol));
+      MD_TRY(e->mdTriLen2.ensure(sizeof(double4) * (size_t)nMol));
+      MDB_CUDA(cudaMemcpyAsync(e->mdTriAtoms.p, triAtoms.data(), sizeof(int4) * (size_t)nMol,
+                               cudaMemcpyHostToDevice, s));
+      MDB_CUDA(cudaMemcpyAsync(e->mdTriLen2.p, triLen2.data(), sizeof(double4) * (size_t)nMol,
+                               cudaMemcpyHostToDevice, s));
+    }
+    e->mdMolClass = (maxAtoms <= kMolTinyAtoms && maxCons <= kMolTinyCons)     ? 0
+                    : (maxAtoms <= kMolSmallAtoms && maxCons <= kMolSmallCons) ? 1
+                                                                               : 2;
     e->mdNMol = nMol;
     MD_TRY(e->mdCa.ensure(sizeof(int) * nConst));
     MD_TRY(e->mdCb.ensure(sizeof(int) * nConst));

@@ -253,7 +253,7 @@ class Engine:
 
     def __init__(self, system, precision: int = 1, device: int = 0, cutOff=12.0, cutOn=10.0,
                  delr=2.0, alpha=0.34, chargeConst=None, vdwSwitch=1, linkRatio=1, noLink=0,
-                 frozen=None, box_type: int = CUBIC, cell=None):
+                 frozen=None, box_type: int = CUBIC, cell=None, exclusions=None):
         from .systems import CHARGE_CONST
         L = lib()
         self.n = system.n
@@ -266,7 +266,9 @@ class Engine:
         check(L.mdbas_nb_engine_create(C.byref(h), C.byref(cfg), C.byref(self.pbc)),
               "engine_create")
         self.h = h
-        start, flat = system.exclusions(symmetric=True)
+        # exclusions: (start[n+1], flat) rows, by default from the system's
+        # bonds and angles
+        start, flat = system.exclusions(symmetric=True) if exclusions is None else exclusions
         pair = np.diff(start).astype(np.int32)
         self._topo = [np.ascontiguousarray(a, dtype=np.float64)
                       for a in (system.q, system.eps, system.sig)]
