@@ -61,6 +61,8 @@ def _parse():
                    help="timed velocity-Verlet steps (1 fs, rigid water) for ns/day")
     p.add_argument("--nve-steps", type=int, default=10000,
                    help="NVE steps (1 fs) for the energy-drift report; 0 skips it")
+    p.add_argument("--large-steps", type=int, default=10,
+                   help="timed steps of the 999,999-atom box; 0 skips it")
     return p.parse_args()
 
 
@@ -299,6 +301,65 @@ def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_step
     return out
 
 
+def large_box_measure(torch, nb, systems, dev, stream, flush, seed, steps):
+    """The 999,999-atom water box (333,333 molecules, 215 A cube): the mixed
+    form's list build, pair kernel and whole step, and its forces against the
+    plain FP64 GPU form on every atom."""
+    import numpy as np
+    s = systems.config_1m(seed=seed)
+    n = s.n
+    eng = nb.Engine(s, precision=1, device=dev)
+    eng.set_stream(stream.cuda_stream)
+    for _ in range(3):
+        eng.build()
+        eng.compute()
+    torch.cuda.synchronize()
+    pairs = int(eng.energies()["n_pairs"])
+    stats = eng.list_stats()
+
+    def step():
+        eng.build()
+        eng.compute()
+
+    ms = _time_steps(torch, eng, stream, flush, steps, step)
+    ms_build = _time_steps(torch, eng, stream, flush, steps, eng.build)
+    eng.set_timing(True)
+    eng.pair_kernel_ms(reset=True)
+    for _ in range(steps):
+        flush.zero_()
+        eng.compute()
+    pair_ms, _ = eng.pair_kernel_ms(reset=True)
+    eng.set_timing(False)
+    fa = eng.forces()
+    ea = eng.energies()
+    eng.close()
+    e64 = nb.Engine(s, precision=0, device=dev)
+    e64.set_stream(stream.cuda_stream)
+    e64.build()
+    e64.compute()
+    fb = e64.forces()
+    eb = e64.energies()
+    e64.close()
+    num = sum(((u - v) ** 2).sum() for u, v in zip(fa, fb))
+    den = sum((v ** 2).sum() for v in fb)
+    tot_a = ea["elec_direct"] + ea["elec_corr"] + ea["vdw"]
+    tot_b = eb["elec_direct"] + eb["elec_corr"] + eb["vdw"]
+    t_step = sum(ms) / len(ms)
+    t_build = sum(ms_build) / len(ms_build)
+    return {
+        "workload": "999,999-atom rigid water box (333,333 molecules, 215 A cube)",
+        "n_atoms": n, "in_cutoff_pairs": pairs, "cluster_pairs": stats[1],
+        "ms_per_step": t_step, "pairs_per_s": pairs / (t_step * 1e-3),
+        "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
+        "list_build": {"ms": t_build,
+                       "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9,
+                       "bytes_per_atom": LIST_BYTES_PER_ATOM},
+        "force_rel_rms_vs_fp64_form": float(np.sqrt(num / den)),
+        "energy_rel_vs_fp64_form": abs(tot_a - tot_b) / abs(tot_b),
+        "fp64_form_pairs": int(eb["n_pairs"]),
+        "l2": "flushed before every timed step (256 MiB write)"}
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -459,6 +520,11 @@ def run_ours(args, rank, world):
         md64 = md_measure(torch, nb, systems, dev, stream, args.seed + rank, 0,
                           max(50, args.md_steps // 5), 0, world)
 
+    large = None
+    if args.large_steps > 0:
+        large = large_box_measure(torch, nb, systems, dev, stream, flush, args.seed + rank,
+                                  args.large_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args.seed)
@@ -479,6 +545,7 @@ def run_ours(args, rank, world):
             "ns_per_day": md["ns_per_day"] if md else None,
             "md": md,
             "md_fp64_form": md64,
+            "large_box": large,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
                             "variant": "dense 8x8", "compacted_variant_ms": compact_ms},
             "list_build": {"ms": t_build,
