@@ -402,6 +402,12 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, l
  * pair of each 8x8 cluster pair in one warp step per cluster pair; 1 filters
  * the pairs first and computes only in-cut-off pairs from per-atom queues. */
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
+/* Autotuner of the mixed-precision pair kernel: times each variant and
+ * launch shape (threads per block x blocks per SM) on the current list with
+ * CUDA events and keeps the fastest for later computes.  out = {variant,
+ * block, blocks per SM, candidates tried}.  Call after build; the
+ * accumulators are left dirty, so compute again before reading forces. */
+int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]);
 /* Kernels this engine launched since creation. */
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e);
 /* Average duration (ms) of the pair kernel over the launches recorded since
@@ -453,6 +459,23 @@ int mdbas_nb_engine_get_positions(mdbas_nb_engine *e, double *x, double *y, doub
                                   int device_ptrs);
 int mdbas_nb_engine_get_velocities(mdbas_nb_engine *e, double *vx, double *vy, double *vz,
                                    int device_ptrs);
+
+/* ------------------------------------------------------------------------ */
+/* 5. Batches of independent boxes (no counterpart in MDBas, which runs one   */
+/*    system per process)                                                    */
+/* ------------------------------------------------------------------------ */
+/* An engine over nRep independent periodic boxes (orthorhombic) whose atoms
+ * are concatenated: replica r owns repAtoms[r] consecutive atoms, in order.
+ * cfg->nAtom = sum of repAtoms; mixed precision only (cfg->precision = 1).
+ * Every engine call above then works on the concatenated arrays: topology
+ * with global atom indices in the exclusions, positions, forces, energies
+ * (summed over replicas) and dynamics.  The list build, the pair kernel, the
+ * exclusion correction and each integration stage run as one launch over
+ * all replicas, each pair with its own replica's box. */
+int mdbas_nb_batch_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *cfg, int nRep,
+                          const PBC *boxes, const int *repAtoms);
+/* Number of replicas of an engine (1 for a single system). */
+int mdbas_nb_batch_count(mdbas_nb_engine *e);
 
 /* Measured FP32 FFMA throughput of a device (TFLOP/s, 2 flops per FFMA), the
  * peak the FP32 pair kernel's roofline fraction is quoted against; ms gets the

@@ -40,13 +40,16 @@ __device__ __forceinline__ double wrap_pos(double v, double L, double invL) {
   return v - L * floor(v * invL + 0.5);
 }
 
-__global__ void k_col_bin(int n, ClusterGeom g, const int *__restrict__ colRank,
-                          const double *__restrict__ x, const double *__restrict__ y,
-                          const double *__restrict__ z, int *__restrict__ atomCol,
-                          double *__restrict__ atomZ, int *__restrict__ colCount,
-                          long long *__restrict__ counters) {
+__global__ void k_col_bin(int n, const ClusterGeom *__restrict__ geoms,
+                          const int *__restrict__ atomRep, const int *__restrict__ colOff,
+                          const int *__restrict__ colRank, const double *__restrict__ x,
+                          const double *__restrict__ y, const double *__restrict__ z,
+                          int *__restrict__ atomCol, double *__restrict__ atomZ,
+                          int *__restrict__ colCount, long long *__restrict__ counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const int rep = atomRep ? atomRep[i] : 0;
+  const ClusterGeom &g = geoms[rep];
   double sx = x[i] / g.Lx + 0.5, sy = y[i] / g.Ly + 0.5, sz = z[i] / g.Lz + 0.5;
   if (!(isfinite(sx) && isfinite(sy) && isfinite(sz))) {
     atomicOr(reinterpret_cast<unsigned long long *>(counters + 2), (unsigned long long)CL_NONFINITE);
@@ -57,7 +60,7 @@ __global__ void k_col_bin(int n, ClusterGeom g, const int *__restrict__ colRank,
   sz -= floor(sz);
   const int cx = min((int)(sx * g.ncx), g.ncx - 1);
   const int cy = min((int)(sy * g.ncy), g.ncy - 1);
-  const int col = colRank[cy * g.ncx + cx];
+  const int col = colRank[colOff[rep] + cy * g.ncx + cx];
   atomCol[i] = col;
   atomZ[i] = sz;
   atomicAdd(colCount + col, 1);
@@ -117,7 +120,9 @@ __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
 }
 
 // One thread per cluster: FP64 origin and half extents, slot data.
-__global__ void k_clusters(const int *__restrict__ nSlotsDev, ClusterGeom g,
+__global__ void k_clusters(const int *__restrict__ nSlotsDev,
+                           const ClusterGeom *__restrict__ geoms,
+                           const int *__restrict__ atomRep, int *__restrict__ clusterRep,
                            const int *__restrict__ slotAtom,
                            const int *__restrict__ atomCol, const int *__restrict__ colXY,
                            const double *__restrict__ x, const double *__restrict__ y,
@@ -130,6 +135,11 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev, ClusterGeom g,
                            int *__restrict__ hmaxBits) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= (*nSlotsDev >> 3)) return;
+  // a cluster's first slot always holds an atom (columns are padded at the end)
+  const int rep = atomRep ? atomRep[slotAtom[c * kClusterSize]] : 0;
+  if (clusterRep) clusterRep[c] = rep;
+  const ClusterGeom &g = geoms[rep];
+  hmaxBits += 4 * rep;
   const double ilx = 1.0 / g.Lx, ily = 1.0 / g.Ly, ilz = 1.0 / g.Lz;
   double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
   double px[kClusterSize], py[kClusterSize], pz[kClusterSize];
@@ -286,7 +296,9 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
 }
 
 __global__ void __launch_bounds__(kSearchThreads)
-k_search(const int *__restrict__ nSlotsDev, ClusterGeom g, const int *__restrict__ colRank,
+k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
+         const int *__restrict__ clusterRep, const int *__restrict__ colOff,
+         const int *__restrict__ colRank,
          const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
          const double4 *__restrict__ origin, const float4 *__restrict__ originF,
          const float4 *__restrict__ half, const int *__restrict__ slotAtom,
@@ -301,6 +313,10 @@ k_search(const int *__restrict__ nSlotsDev, ClusterGeom g, const int *__restrict
   const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ci >= (*nSlotsDev >> 3)) return;
   SearchBuf &B = bufs[threadIdx.x >> 5];
+  const int rep = clusterRep ? clusterRep[ci] : 0;
+  const ClusterGeom g = geoms[rep];
+  const int colBase = colOff[rep];
+  hmaxBits += 4 * rep;
 
   const double4 oi = origin[ci];
   const float4 oif = originF[ci];
@@ -346,7 +362,7 @@ k_search(const int *__restrict__ nSlotsDev, ClusterGeom g, const int *__restrict
       const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
       const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
       if (gx * gx + gy * gy > g.rlist2) continue;
-      const int col = colRank[jy * g.ncx + jx];
+      const int col = colRank[colBase + jy * g.ncx + jx];
       const int cs = colClStart[col], ce = colClStart[col + 1];
       for (int base = cs; base < ce; base += 32) {
         const int cj = base + lane;
@@ -410,7 +426,9 @@ k_search(const int *__restrict__ nSlotsDev, ClusterGeom g, const int *__restrict
     atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3), (unsigned long long)cand);
 }
 
-__global__ void k_refresh(const int *__restrict__ nSlotsDev, ClusterGeom g,
+__global__ void k_refresh(const int *__restrict__ nSlotsDev,
+                          const ClusterGeom *__restrict__ geoms,
+                          const int *__restrict__ clusterRep,
                           const int *__restrict__ slotAtom, const double4 *__restrict__ origin,
                           const double *__restrict__ x, const double *__restrict__ y,
                           const double *__restrict__ z, const double *__restrict__ q, double sqrtC,
@@ -419,6 +437,7 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev, ClusterGeom g,
   if (s >= *nSlotsDev) return;
   const int a = slotAtom[s];
   if (a < 0) return;
+  const ClusterGeom &g = geoms[clusterRep ? clusterRep[s / kClusterSize] : 0];
   const double4 o = origin[s / kClusterSize];
   double dx = x[a] - o.x, dy = y[a] - o.y, dz = z[a] - o.z;
   dx -= g.Lx * rint(dx / g.Lx);
@@ -445,13 +464,13 @@ unsigned morton2(unsigned x, unsigned y) {
 
 }  // namespace
 
-int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
-                  double sqrtC, const double *x, const double *y, const double *z,
-                  const double *q, const double *eps, const double *sig, const int *frozen,
-                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync) {
+namespace {
+
+// Column grid of one box (orthorhombic), or an error status.
+int make_geom(const DevBox &b, int n, double cutOff, double delr, ClusterGeom &g) {
   if (b.type != CUBIC && b.type != ORBIC) return MDBAS_NB_ERR_UNSUPPORTED;
   if (n <= 0) return MDBAS_NB_ERR_ARG;
-  ClusterGeom g{};
+  g = ClusterGeom{};
   g.Lx = b.a1;
   g.Ly = (b.type == CUBIC) ? b.a1 : b.b2;
   g.Lz = (b.type == CUBIC) ? b.a1 : b.c3;
@@ -474,34 +493,84 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
     if (g.Dy >= g.ncy) g.Dy = g.ncy - 1;
   }
   g.rlist2 = (float)(rlist * rlist * (1.0 + 1e-5));
-  const int nCols = g.ncx * g.ncy;
+  return MDBAS_NB_OK;
+}
+
+bool same_geom(const ClusterGeom &a, const ClusterGeom &b) {
+  return a.ncx == b.ncx && a.ncy == b.ncy && a.Dx == b.Dx && a.Dy == b.Dy && a.Lx == b.Lx &&
+         a.Ly == b.Ly && a.Lz == b.Lz && a.rlist2 == b.rlist2;
+}
+
+}  // namespace
+
+int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const int *atomOff,
+                  double cutOff, double delr, double sqrtC, const double *x, const double *y,
+                  const double *z, const double *q, const double *eps, const double *sig,
+                  const int *frozen, const int *exclStart, const int *exclFlat, cudaStream_t s,
+                  bool sync) {
+  if (nRep <= 0 || n <= 0 || atomOff[0] != 0 || atomOff[nRep] != n) return MDBAS_NB_ERR_ARG;
+  std::vector<ClusterGeom> geoms(nRep);
+  std::vector<int> colOff(nRep + 1, 0);
+  for (int r = 0; r < nRep; ++r) {
+    const int nr = atomOff[r + 1] - atomOff[r];
+    MDB_TRY(make_geom(boxes[r], nr, cutOff, delr, geoms[r]));
+    colOff[r + 1] = colOff[r] + geoms[r].ncx * geoms[r].ncy;
+  }
+  const int nCols = colOff[nRep];
   const int slotCap = (n + (kClusterSize - 1) * nCols + kClusterSize - 1) & ~(kClusterSize - 1);
-  const bool sameGrid = nCols == w.nCols && g.ncx == w.geom.ncx && g.ncy == w.geom.ncy;
+  bool sameGrid = nRep == w.nRep && w.atomOffH.size() == (size_t)nRep + 1;
+  for (int r = 0; sameGrid && r < nRep; ++r)
+    sameGrid = same_geom(geoms[r], w.geomH[r]) && atomOff[r + 1] == w.atomOffH[r + 1];
   // The captured form cannot upload tables or grow buffers.
   if (!sync && (!sameGrid || slotCap > w.slotCap || w.entryCap == 0)) return MDBAS_NB_ERR_STATE;
 
-  // Morton rank of each (cx, cy) cell; rebuilt when the grid changes.
+  // Per-replica tables, rebuilt when any grid changes: Morton rank of each
+  // (cx, cy) cell as a global column, and each column's (cx, cy).
   if (!sameGrid) {
-    std::vector<std::pair<unsigned, int>> keys(nCols);
-    for (int cy = 0; cy < g.ncy; ++cy)
-      for (int cx = 0; cx < g.ncx; ++cx)
-        keys[cy * g.ncx + cx] = {morton2(cx, cy), cy * g.ncx + cx};
-    std::sort(keys.begin(), keys.end());
     std::vector<int> rank(nCols), xyOf(nCols);
-    for (int r = 0; r < nCols; ++r) {
-      const int cell = keys[r].second;
-      rank[cell] = r;
-      xyOf[r] = (cell % g.ncx) | ((cell / g.ncx) << 16);
+    for (int r = 0; r < nRep; ++r) {
+      const ClusterGeom &g = geoms[r];
+      const int nc = g.ncx * g.ncy;
+      std::vector<std::pair<unsigned, int>> keys(nc);
+      for (int cy = 0; cy < g.ncy; ++cy)
+        for (int cx = 0; cx < g.ncx; ++cx)
+          keys[cy * g.ncx + cx] = {morton2(cx, cy), cy * g.ncx + cx};
+      std::sort(keys.begin(), keys.end());
+      for (int k = 0; k < nc; ++k) {
+        const int cell = keys[k].second;
+        rank[colOff[r] + cell] = colOff[r] + k;
+        xyOf[colOff[r] + k] = (cell % g.ncx) | ((cell / g.ncx) << 16);
+      }
     }
     MDB_TRY(w.colRank.ensure(sizeof(int) * nCols));
     MDB_TRY(w.colXY.ensure(sizeof(int) * nCols));
+    MDB_TRY(w.geoms.ensure(sizeof(ClusterGeom) * nRep));
+    MDB_TRY(w.colOff.ensure(sizeof(int) * (nRep + 1)));
+    MDB_TRY(w.boxes.ensure(sizeof(DevBox) * nRep));
     MDB_CUDA(cudaMemcpyAsync(w.colRank.p, rank.data(), sizeof(int) * nCols,
                              cudaMemcpyHostToDevice, s));
     MDB_CUDA(cudaMemcpyAsync(w.colXY.p, xyOf.data(), sizeof(int) * nCols,
                              cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(w.geoms.p, geoms.data(), sizeof(ClusterGeom) * nRep,
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(w.colOff.p, colOff.data(), sizeof(int) * (nRep + 1),
+                             cudaMemcpyHostToDevice, s));
+    MDB_CUDA(cudaMemcpyAsync(w.boxes.p, boxes, sizeof(DevBox) * nRep, cudaMemcpyHostToDevice, s));
+    if (nRep > 1) {
+      std::vector<int> rep(n);
+      for (int r = 0; r < nRep; ++r)
+        for (int i = atomOff[r]; i < atomOff[r + 1]; ++i) rep[i] = r;
+      MDB_TRY(w.atomRep.ensure(sizeof(int) * n));
+      MDB_CUDA(cudaMemcpyAsync(w.atomRep.p, rep.data(), sizeof(int) * n, cudaMemcpyHostToDevice,
+                               s));
+    }
     MDB_CUDA(cudaStreamSynchronize(s));
+    w.geomH = geoms;
+    w.colOffH = colOff;
+    w.atomOffH.assign(atomOff, atomOff + nRep + 1);
+    w.nRep = nRep;
   }
-  w.geom = g;
+  w.geom = geoms[0];
   w.nCols = nCols;
 
   if (sync) {
@@ -528,22 +597,24 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
     }
     MDB_TRY(w.slotAtom.ensure(sizeof(int) * w.slotCap));
     MDB_TRY(w.clusterXY.ensure(sizeof(int) * w.clCap));
+    if (nRep > 1) MDB_TRY(w.clusterRep.ensure(sizeof(int) * w.clCap));
     MDB_TRY(w.origin.ensure(sizeof(double4) * w.clCap));
     MDB_TRY(w.half.ensure(sizeof(float4) * w.clCap));
     MDB_TRY(w.originF.ensure(sizeof(float4) * w.clCap));
-    MDB_TRY(w.hmax.ensure(sizeof(int) * 4));
+    MDB_TRY(w.hmax.ensure(sizeof(int) * 4 * nRep));
     MDB_TRY(w.xq.ensure(sizeof(float4) * w.slotCap));
     MDB_TRY(w.lj.ensure(sizeof(float2) * w.slotCap));
     MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)w.slotCap));
   }
+  const ClusterGeom *gd = w.geoms.as<ClusterGeom>();
 
   MDB_CUDA(cudaMemsetAsync(w.colCount.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
-  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4, s));
-  MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, g, w.colRank.as<int>(), x, y, z,
-             w.atomCol.as<int>(), w.atomZ.as<double>(), w.colCount.as<int>(),
-             w.counters.as<long long>());
+  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4 * nRep, s));
+  MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, gd, w.atomRepDev(), w.colOff.as<int>(),
+             w.colRank.as<int>(), x, y, z, w.atomCol.as<int>(), w.atomZ.as<double>(),
+             w.colCount.as<int>(), w.counters.as<long long>());
   MDB_TRY(exclusive_scan32(w.colCount.as<int>(), w.colStart.as<int>(), nCols, w.scanTmp.p, s));
   MDB_LAUNCH(k_col_pad, grid_for(nCols, 256), 256, 0, s, nCols, w.colCount.as<int>(),
              w.colPad.as<int>());
@@ -554,11 +625,11 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
   MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
              w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
-  MDB_LAUNCH(k_clusters, grid_for(w.clCap, 128), 128, 0, s, w.nSlotsDev(), g,
-             w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x, y, z, q, eps, sig,
-             sqrtC, w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
-             w.xq.as<float4>(), w.lj.as<float2>(), w.slotOf.as<int>(), w.clusterXY.as<int>(),
-             w.hmax.as<int>());
+  MDB_LAUNCH(k_clusters, grid_for(w.clCap, 128), 128, 0, s, w.nSlotsDev(), gd, w.atomRepDev(),
+             nRep > 1 ? w.clusterRep.as<int>() : nullptr, w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x,
+             y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
+             w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.slotOf.as<int>(),
+             w.clusterXY.as<int>(), w.hmax.as<int>());
 
   // Cluster-pair search; in the synchronising form grow the list and search
   // again if it overflowed.
@@ -575,12 +646,12 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
     MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long), s));
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
-               w.nSlotsDev(), g, w.colRank.as<int>(), w.colClStart.as<int>(),
-               w.clusterXY.as<int>(), w.origin.as<double4>(), w.originF.as<float4>(),
-               w.half.as<float4>(), w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart,
-               exclFlat, w.hmax.as<int>(), w.xq.as<float4>(), w.entries.as<CPairEntry>(),
-               w.masks.as<uint2>(), w.items.as<int4>(), w.counters.as<long long>(), w.entryCap,
-               w.itemCap);
+               w.nSlotsDev(), gd, w.clusterRepDev(), w.colOff.as<int>(), w.colRank.as<int>(),
+               w.colClStart.as<int>(), w.clusterXY.as<int>(), w.origin.as<double4>(),
+               w.originF.as<float4>(), w.half.as<float4>(), w.slotAtom.as<int>(),
+               w.slotOf.as<int>(), frozen, exclStart, exclFlat, w.hmax.as<int>(),
+               w.xq.as<float4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+               w.items.as<int4>(), w.counters.as<long long>(), w.entryCap, w.itemCap);
     if (!sync) {
       MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.sticky.as<long long>());
       return MDBAS_NB_OK;
@@ -604,6 +675,15 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   return MDBAS_NB_ERR_CAPACITY;
 }
 
+int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
+                  double sqrtC, const double *x, const double *y, const double *z,
+                  const double *q, const double *eps, const double *sig, const int *frozen,
+                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync) {
+  const int off[2] = {0, n};
+  return cluster_build(w, n, 1, &b, off, cutOff, delr, sqrtC, x, y, z, q, eps, sig, frozen,
+                       exclStart, exclFlat, s, sync);
+}
+
 int cluster_read_counts(ClusterWork &w, cudaStream_t s) {
   if (!w.counters.p || w.nCols <= 0) return MDBAS_NB_ERR_STATE;
   long long flags[4];
@@ -618,13 +698,12 @@ int cluster_read_counts(ClusterWork &w, cudaStream_t s) {
   return MDBAS_NB_OK;
 }
 
-int cluster_refresh(ClusterWork &w, int n, const DevBox &b, const double *x, const double *y,
-                    const double *z, const double *q, double sqrtC, cudaStream_t s) {
-  (void)n;
-  (void)b;
+int cluster_refresh(ClusterWork &w, const double *x, const double *y, const double *z,
+                    const double *q, double sqrtC, cudaStream_t s) {
   if (w.slotCap <= 0) return MDBAS_NB_ERR_STATE;
-  MDB_LAUNCH(k_refresh, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(), w.geom,
-             w.slotAtom.as<int>(), w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>());
+  MDB_LAUNCH(k_refresh, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(),
+             w.geoms.as<ClusterGeom>(), w.clusterRepDev(), w.slotAtom.as<int>(),
+             w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>());
   return MDBAS_NB_OK;
 }
 

@@ -1,6 +1,8 @@
 // cluster.cuh -- cell-sorted 8-atom cluster layout and cluster-pair list.
 #pragma once
 
+#include <vector>
+
 #include "common.cuh"
 
 namespace mdbas {
@@ -24,12 +26,27 @@ struct CPairEntry {
   float sx, sy, sz;
 };
 
+// The layout holds a batch of independent boxes ("replicas"): replica r owns
+// atoms [atomOff[r], atomOff[r+1]) of the concatenated arrays and columns
+// [colOff[r], colOff[r+1]) of the global column numbering, hence a
+// contiguous run of slots and clusters; cluster-pair entries name global
+// clusters, so one pair-kernel launch serves every replica.  A single system
+// is a batch of one.
 struct ClusterWork {
   // grid
-  ClusterGeom geom{};
-  int nCols = 0;
-  DBuf colRank;       // (cy*ncx+cx) -> column slot in Morton order
-  DBuf colXY;         // column slot -> cx | cy << 16
+  int nRep = 0;
+  std::vector<ClusterGeom> geomH;  // per replica
+  std::vector<int> colOffH;        // nRep + 1
+  std::vector<int> atomOffH;       // nRep + 1
+  DBuf geoms;         // ClusterGeom[nRep]
+  DBuf colOff;        // int[nRep + 1]
+  DBuf boxes;         // DevBox[nRep]
+  DBuf atomRep;       // atom -> replica (nRep > 1 only)
+  DBuf clusterRep;    // cluster -> replica (nRep > 1 only)
+  ClusterGeom geom{}; // replica 0's grid (single-system callers)
+  int nCols = 0;      // columns of all replicas
+  DBuf colRank;       // colOff[r] + (cy*ncx+cx) -> global column, Morton order inside r
+  DBuf colXY;         // global column -> cx | cy << 16
   DBuf colCount, colFill, colStart, colPad, colPadStart;
   DBuf atomCol, tmpIdx;
   DBuf atomZ;         // wrapped fractional z (FP64)
@@ -47,7 +64,7 @@ struct ClusterWork {
   DBuf colClStart;    // column slot -> first cluster (nCols + 1)
   DBuf origin;        // double4 per cluster (FP64 origin)
   DBuf originF;       // float4 per cluster (FP32 origin, w = real atoms)
-  DBuf hmax;          // int[4]: largest half extent per axis (float bits)
+  DBuf hmax;          // int[4 * nRep]: largest half extent per axis (float bits)
   DBuf half;          // float4 per cluster (bbox half extents, w = real atoms)
   DBuf xq;            // float4 per slot: position - origin, q*sqrt(C)
   DBuf lj;            // float2 per slot: 2*eps_i, sig_i
@@ -63,6 +80,8 @@ struct ClusterWork {
   DBuf facc;          // int64 fixed-point forces, SoA [3][slotCap]
   DBuf acc;           // int64[ACC_COUNT]
   const int *nSlotsDev() const { return colPadStart.as<int>() + nCols; }
+  const int *atomRepDev() const { return nRep > 1 ? atomRep.as<int>() : nullptr; }
+  const int *clusterRepDev() const { return nRep > 1 ? clusterRep.as<int>() : nullptr; }
 };
 
 // Bits of ClusterWork::counters[2] and ::sticky.
@@ -74,6 +93,13 @@ enum ClusterFlag { CL_OVERFLOW = 1, CL_NONFINITE = 2 };
 // and no allocation (the form captured into CUDA graphs); the layout must
 // have been set up by an earlier synchronising build of the same geometry,
 // and an overflow only raises CL_OVERFLOW in `sticky`.
+// Batch form: nRep boxes, atomOff[nRep + 1] atom ranges (host arrays).
+int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const int *atomOff,
+                  double cutOff, double delr, double sqrtC, const double *x, const double *y,
+                  const double *z, const double *q, const double *eps, const double *sig,
+                  const int *frozen, const int *exclStart, const int *exclFlat, cudaStream_t s,
+                  bool sync = true);
+// Single box.
 int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
                   double sqrtC, const double *x, const double *y, const double *z,
                   const double *q, const double *eps, const double *sig, const int *frozen,
@@ -81,7 +107,7 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
 // Host copies of the list counts (synchronises the stream).
 int cluster_read_counts(ClusterWork &w, cudaStream_t s);
 // Refresh xq from the current FP64 positions (list kept).
-int cluster_refresh(ClusterWork &w, int n, const DevBox &b, const double *x, const double *y,
-                    const double *z, const double *q, double sqrtC, cudaStream_t s);
+int cluster_refresh(ClusterWork &w, const double *x, const double *y, const double *z,
+                    const double *q, double sqrtC, cudaStream_t s);
 
 }  // namespace mdbas

@@ -126,6 +126,29 @@ __device__ __forceinline__ double dist_d(const DevBox &b, double &dx, double &dy
   return dadd(dadd(dmul(dx, dx), dmul(dy, dy)), dmul(dz, dz));
 }
 
+// image_update (src/utils.c:162-218) of one position, in place.
+__device__ __forceinline__ void image_d(const DevBox &b, double &xi, double &yi, double &zi) {
+  if (b.type == CUBIC) {
+    xi = dsub(xi, dmul(b.a1, (double)nint_d(dmul(xi, b.u1))));
+    yi = dsub(yi, dmul(b.a1, (double)nint_d(dmul(yi, b.u1))));
+    zi = dsub(zi, dmul(b.a1, (double)nint_d(dmul(zi, b.u1))));
+  } else if (b.type == ORBIC) {
+    xi = dsub(xi, dmul(b.a1, (double)nint_d(dmul(xi, b.u1))));
+    yi = dsub(yi, dmul(b.b2, (double)nint_d(dmul(yi, b.v2))));
+    zi = dsub(zi, dmul(b.c3, (double)nint_d(dmul(zi, b.w3))));
+  } else if (b.type == TCLIN) {
+    double xt = dadd(dadd(dmul(xi, b.u1), dmul(yi, b.u2)), dmul(zi, b.u3));
+    double yt = dadd(dadd(dmul(xi, b.v1), dmul(yi, b.v2)), dmul(zi, b.v3));
+    double zt = dadd(dadd(dmul(xi, b.w1), dmul(yi, b.w2)), dmul(zi, b.w3));
+    xt = dsub(xt, (double)nint_d(xt));
+    yt = dsub(yt, (double)nint_d(yt));
+    zt = dsub(zt, (double)nint_d(zt));
+    xi = dadd(dadd(dmul(xt, b.a1), dmul(yt, b.b1)), dmul(zt, b.c1));
+    yi = dadd(dadd(dmul(xt, b.a2), dmul(yt, b.b2)), dmul(zt, b.c2));
+    zi = dadd(dadd(dmul(xt, b.a3), dmul(yt, b.b3)), dmul(zt, b.c3));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Fixed-point accumulation.  Forces are summed as int64 in units of 2^-32
 // internal units, energies and virials in units of 2^-24.  Integer addition

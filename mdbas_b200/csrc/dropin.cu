@@ -424,7 +424,7 @@ int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch,
     g.clBox = b;
     g.clValid = true;
   } else {
-    ST_TRY(cluster_refresh(g.cl, n, b, g.x.as<double>(), g.y.as<double>(), g.z.as<double>(),
+    ST_TRY(cluster_refresh(g.cl, g.x.as<double>(), g.y.as<double>(), g.z.as<double>(),
                            g.q.as<double>(), sqrt(param->chargeConst), g.s));
   }
   ClusterWork &w = g.cl;
@@ -433,7 +433,7 @@ int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch,
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
   ST_TRY(pair_fp32_launch(w, p, sms * 8, 256, g.s));
-  ST_TRY(excl_fix_launch(w, n, b, p, g.exclStart.as<int>(), g.exclFlat.as<int>(),
+  ST_TRY(excl_fix_launch(w, n, p, g.exclStart.as<int>(), g.exclFlat.as<int>(),
                          g.x.as<double>(), g.y.as<double>(), g.z.as<double>(), g.q.as<double>(),
                          g.s));
   double *fxd = g.f3.as<double>();

@@ -136,6 +136,14 @@ static int set_dev(mdbas_nb_engine *e) {
   return MDBAS_NB_OK;
 }
 
+// The replicas' boxes on the device, as the dynamics kernels read them.
+static int upload_boxes(mdbas_nb_engine *e) {
+  MDB_TRY(e->boxesDev.ensure(sizeof(DevBox) * e->repBoxes.size()));
+  MDB_CUDA(cudaMemcpy(e->boxesDev.p, e->repBoxes.data(), sizeof(DevBox) * e->repBoxes.size(),
+                      cudaMemcpyHostToDevice));
+  return MDBAS_NB_OK;
+}
+
 extern "C" {
 
 int mdbas_nb_engine_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *cfg,
@@ -153,6 +161,8 @@ int mdbas_nb_engine_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *
   e->device = cfg->device;
   e->hostBox = *box;
   e->box = make_devbox(box);
+  e->repBoxes.assign(1, e->box);
+  e->repOff = {0, e->n};
   e->pp = make_params(cfg->cutOff, cfg->cutOn, cfg->alpha, cfg->chargeConst, cfg->vdwSwitch,
                       FULL);
   if (set_dev(e) != MDBAS_NB_OK || cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) !=
@@ -163,9 +173,51 @@ int mdbas_nb_engine_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *
   e->ownStream = true;
   cudaEventCreate(&e->ev0);
   cudaEventCreate(&e->ev1);
+  if (upload_boxes(e) != MDBAS_NB_OK) {
+    mdbas_nb_engine_destroy(e);
+    return MDBAS_NB_ERR_CUDA;
+  }
   *out = e;
   return MDBAS_NB_OK;
 }
+
+int mdbas_nb_batch_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *cfg, int nRep,
+                          const PBC *boxes, const int *repAtoms) {
+  if (!out || !cfg || !boxes || !repAtoms || nRep <= 0) return MDBAS_NB_ERR_ARG;
+  if (cfg->precision != 1) return MDBAS_NB_ERR_UNSUPPORTED;
+  long long total = 0;
+  for (int r = 0; r < nRep; ++r) {
+    if (repAtoms[r] <= 0) return MDBAS_NB_ERR_ARG;
+    total += repAtoms[r];
+  }
+  if (total != cfg->nAtom || total > 0x7fffffffLL) return MDBAS_NB_ERR_ARG;
+  mdbas_nb_engine *e = nullptr;
+  int st = mdbas_nb_engine_create(&e, cfg, &boxes[0]);
+  if (st != MDBAS_NB_OK) return st;
+  e->nRep = nRep;
+  e->repBoxes.resize(nRep);
+  e->repOff.assign(nRep + 1, 0);
+  std::vector<int> rep(cfg->nAtom);
+  for (int r = 0; r < nRep; ++r) {
+    e->repBoxes[r] = make_devbox(&boxes[r]);
+    e->repOff[r + 1] = e->repOff[r] + repAtoms[r];
+    for (int i = e->repOff[r]; i < e->repOff[r + 1]; ++i) rep[i] = r;
+  }
+  st = upload_boxes(e);
+  if (st == MDBAS_NB_OK) st = e->atomRepDev.ensure(sizeof(int) * (size_t)cfg->nAtom);
+  if (st == MDBAS_NB_OK &&
+      cudaMemcpy(e->atomRepDev.p, rep.data(), sizeof(int) * (size_t)cfg->nAtom,
+                 cudaMemcpyHostToDevice) != cudaSuccess)
+    st = MDBAS_NB_ERR_CUDA;
+  if (st != MDBAS_NB_OK) {
+    mdbas_nb_engine_destroy(e);
+    return st;
+  }
+  *out = e;
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_batch_count(mdbas_nb_engine *e) { return e ? e->nRep : -1; }
 
 int mdbas_nb_engine_destroy(mdbas_nb_engine *e) {
   if (!e) return MDBAS_NB_OK;
@@ -193,8 +245,12 @@ int mdbas_nb_engine_set_stream(mdbas_nb_engine *e, void *stream) {
 
 int mdbas_nb_engine_set_box(mdbas_nb_engine *e, const PBC *box) {
   if (!e || !box) return MDBAS_NB_ERR_ARG;
+  if (e->nRep > 1) return MDBAS_NB_ERR_UNSUPPORTED;
+  ENG_TRY(e, set_dev(e));
   e->hostBox = *box;
   e->box = make_devbox(box);
+  e->repBoxes.assign(1, e->box);
+  ENG_TRY(e, upload_boxes(e));
   e->built = false;
   e->mdGraphStale = true;
   return MDBAS_NB_OK;
@@ -288,8 +344,8 @@ int mdbas_nb_engine_build(mdbas_nb_engine *e) {
                               lc, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                               frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream));
   } else {
-    ENG_TRY(e, cluster_build(e->cl, n, e->box, e->cfg.cutOff, e->cfg.delr,
-                             sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
+    ENG_TRY(e, cluster_build(e->cl, n, e->nRep, e->repBoxes.data(), e->repOff.data(),
+                             e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
                              e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),
                              e->sig.as<double>(), frozen, e->exclStart.as<int>(),
                              e->exclFlat.as<int>(), e->stream));
@@ -304,7 +360,7 @@ int mdbas_nb_engine_refresh(mdbas_nb_engine *e) {
   ENG_TRY(e, set_dev(e));
   LaunchScope ls(e);
   if (e->cfg.precision == 1)
-    ENG_TRY(e, cluster_refresh(e->cl, e->n, e->box, e->x.as<double>(), e->y.as<double>(),
+    ENG_TRY(e, cluster_refresh(e->cl, e->x.as<double>(), e->y.as<double>(),
                                e->z.as<double>(), e->q.as<double>(), sqrt(e->cfg.chargeConst),
                                e->stream));
   return MDBAS_NB_OK;
@@ -345,7 +401,7 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev0, s));
     ENG_TRY(e, pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev1, s));
-    ENG_TRY(e, excl_fix_launch(w, n, e->box, e->pp, e->exclStart.as<int>(),
+    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(),
                                e->exclFlat.as<int>(), e->x.as<double>(), e->y.as<double>(),
                                e->z.as<double>(), e->q.as<double>(), s));
   }
@@ -478,6 +534,55 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs,
 }
 
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e) { return e ? e->launches : -1; }
+
+int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
+  if (!e || !out) return MDBAS_NB_ERR_ARG;
+  if (e->cfg.precision != 1) return MDBAS_NB_ERR_UNSUPPORTED;
+  if (!e->built) return MDBAS_NB_ERR_STATE;
+  ENG_TRY(e, set_dev(e));
+  LaunchScope ls(e);
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);
+  struct Cand { int variant, block, bps; };
+  std::vector<Cand> cands;
+  // the dense kernel takes at most 256 threads per block (launch bounds)
+  for (int block : {64, 128, 256})
+    for (int bps : {2, 4, 8, 16, 32})
+      if (block * bps <= 2048 && bps <= 24) cands.push_back({kPairDense, block, bps});
+  for (int bps : {2, 4, 5}) cands.push_back({kPairCompact, 128, bps});
+  ClusterWork &w = e->cl;
+  cudaStream_t s = e->stream;
+  float best = 1e30f;
+  Cand pick = cands[0];
+  for (const Cand &c : cands) {
+    float tmin = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
+      MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
+      MDB_CUDA(cudaEventRecord(e->ev0, s));
+      ENG_TRY(e, pair_fp32_launch(w, e->pp, sms * c.bps, c.block, s, c.variant));
+      MDB_CUDA(cudaEventRecord(e->ev1, s));
+      MDB_CUDA(cudaEventSynchronize(e->ev1));
+      float ms = 0.f;
+      MDB_CUDA(cudaEventElapsedTime(&ms, e->ev0, e->ev1));
+      if (rep > 0) tmin = std::min(tmin, ms);  // the first run warms up
+    }
+    if (tmin < best) {
+      best = tmin;
+      pick = c;
+    }
+  }
+  e->variant = pick.variant;
+  e->grid = sms * pick.bps;
+  e->block = pick.block;
+  e->computed = false;
+  e->mdGraphStale = true;
+  out[0] = pick.variant;
+  out[1] = pick.block;
+  out[2] = pick.bps;
+  out[3] = (int)cands.size();
+  return MDBAS_NB_OK;
+}
 
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
   if (!e || (variant != kPairDense && variant != kPairCompact)) return MDBAS_NB_ERR_ARG;

@@ -1,6 +1,8 @@
 // engine.cuh -- the device-resident engine object behind mdbas_nb_engine_*.
 #pragma once
 
+#include <vector>
+
 #include "cluster.cuh"
 #include "list_ref.cuh"
 
@@ -9,7 +11,14 @@ struct mdbas_nb_engine {
   int n = 0;
   int device = 0;
   PBC hostBox{};
-  mdbas::DevBox box{};
+  mdbas::DevBox box{};          // replica 0's box
+  // batch of independent boxes (a single system is a batch of one)
+  int nRep = 1;
+  std::vector<mdbas::DevBox> repBoxes;  // nRep
+  std::vector<int> repOff;              // nRep + 1 atom offsets
+  mdbas::DBuf boxesDev;                 // DevBox[nRep]
+  mdbas::DBuf atomRepDev;               // atom -> replica (nRep > 1)
+  const int *atomRepPtr() const { return nRep > 1 ? atomRepDev.as<int>() : nullptr; }
   mdbas::PairParams pp{};
   cudaStream_t stream = nullptr;
   bool ownStream = false;

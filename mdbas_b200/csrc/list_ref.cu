@@ -43,25 +43,7 @@ __global__ void k_image_update(int n, DevBox b, double *x, double *y, double *z)
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double xi = x[i], yi = y[i], zi = z[i];
-  if (b.type == CUBIC) {
-    xi = dsub(xi, dmul(b.a1, (double)nint_d(dmul(xi, b.u1))));
-    yi = dsub(yi, dmul(b.a1, (double)nint_d(dmul(yi, b.u1))));
-    zi = dsub(zi, dmul(b.a1, (double)nint_d(dmul(zi, b.u1))));
-  } else if (b.type == ORBIC) {
-    xi = dsub(xi, dmul(b.a1, (double)nint_d(dmul(xi, b.u1))));
-    yi = dsub(yi, dmul(b.b2, (double)nint_d(dmul(yi, b.v2))));
-    zi = dsub(zi, dmul(b.c3, (double)nint_d(dmul(zi, b.w3))));
-  } else if (b.type == TCLIN) {
-    double xt = dadd(dadd(dmul(xi, b.u1), dmul(yi, b.u2)), dmul(zi, b.u3));
-    double yt = dadd(dadd(dmul(xi, b.v1), dmul(yi, b.v2)), dmul(zi, b.v3));
-    double zt = dadd(dadd(dmul(xi, b.w1), dmul(yi, b.w2)), dmul(zi, b.w3));
-    xt = dsub(xt, (double)nint_d(xt));
-    yt = dsub(yt, (double)nint_d(yt));
-    zt = dsub(zt, (double)nint_d(zt));
-    xi = dadd(dadd(dmul(xt, b.a1), dmul(yt, b.b1)), dmul(zt, b.c1));
-    yi = dadd(dadd(dmul(xt, b.a2), dmul(yt, b.b2)), dmul(zt, b.c2));
-    zi = dadd(dadd(dmul(xt, b.a3), dmul(yt, b.b3)), dmul(zt, b.c3));
-  }
+  image_d(b, xi, yi, zi);
   x[i] = xi;
   y[i] = yi;
   z[i] = zi;

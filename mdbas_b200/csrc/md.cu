@@ -74,13 +74,15 @@ __global__ void k_vv_kick(int n, double dt, const double *__restrict__ fx,
 }
 
 // constraint vectors before the drift, minimum image (dist2, src/utils.c:82)
-__global__ void k_cons_vectors(int nc, DevBox b, const int *__restrict__ ca,
+__global__ void k_cons_vectors(int nc, const DevBox *__restrict__ boxes,
+                               const int *__restrict__ atomRep, const int *__restrict__ ca,
                                const int *__restrict__ cb, const double *__restrict__ x,
                                const double *__restrict__ y, const double *__restrict__ z,
                                double *__restrict__ ddx, double *__restrict__ ddy,
                                double *__restrict__ ddz) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= nc) return;
+  const DevBox &b = boxes[atomRep ? atomRep[ca[c]] : 0];
   double dx = x[cb[c]] - x[ca[c]], dy = y[cb[c]] - y[ca[c]], dz = z[cb[c]] - z[ca[c]];
   dist_d(b, dx, dy, dz);
   ddx[c] = dx;
@@ -174,7 +176,8 @@ __device__ __forceinline__ void report_cycles(int *status, int icycle) {
 // largest relative bond error is below tol; positions and velocities move.
 template <int MA, int MC>
 __global__ void __launch_bounds__(128)
-k_shake_positions(int nMol, DevBox b, double dt, double tol, int maxCycle,
+k_shake_positions(int nMol, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
+                  double dt, double tol, int maxCycle,
                   const int *__restrict__ molCons, const int *__restrict__ ca,
                   const int *__restrict__ cb, const double *__restrict__ rc2g,
                   const double *__restrict__ ddxg, const double *__restrict__ ddyg,
@@ -196,6 +199,7 @@ k_shake_positions(int nMol, DevBox b, double dt, double tol, int maxCycle,
     active = false;
   }
   if (active) {
+    const DevBox &b = boxes[atomRep ? atomRep[atoms[0]] : 0];
     double px[MA], py[MA], pz[MA], qx[MA], qy[MA], qz[MA], rm[MA], inv[MA];
 #pragma unroll
     for (int t = 0; t < MA; ++t) {
@@ -427,7 +431,8 @@ __device__ __forceinline__ void tri_vectors(const DevBox &b, const double (&px)[
 }
 
 __global__ void __launch_bounds__(128)
-k_tri_stage1(int nTri, DevBox b, double dt, double tol, int maxCycle,
+k_tri_stage1(int nTri, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
+             double dt, double tol, int maxCycle,
              const int4 *__restrict__ tri, const double4 *__restrict__ len2,
              const double *__restrict__ fx, const double *__restrict__ fy,
              const double *__restrict__ fz, const double *__restrict__ rmass,
@@ -440,6 +445,7 @@ k_tri_stage1(int nTri, DevBox b, double dt, double tol, int maxCycle,
   if (m < nTri) {
     const int4 t = tri[m];
     const int A[3] = {t.x, t.y, t.z};
+    const DevBox &b = boxes[atomRep ? atomRep[t.x] : 0];
     const double4 l2 = len2[m];
     const double r2c[3] = {l2.x, l2.y, l2.z};
     double irc[3];
@@ -531,7 +537,8 @@ k_tri_stage1(int nTri, DevBox b, double dt, double tol, int maxCycle,
 }
 
 __global__ void __launch_bounds__(128)
-k_tri_stage2(int nTri, DevBox b, double dt, double tolvel, int maxCycle,
+k_tri_stage2(int nTri, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
+             double dt, double tolvel, int maxCycle,
              const int4 *__restrict__ tri, const double *__restrict__ fx,
              const double *__restrict__ fy, const double *__restrict__ fz,
              const double *__restrict__ rmass, const double *__restrict__ x,
@@ -543,6 +550,7 @@ k_tri_stage2(int nTri, DevBox b, double dt, double tolvel, int maxCycle,
   if (m >= nTri) return;
   const int4 t = tri[m];
   const int A[3] = {t.x, t.y, t.z};
+  const DevBox &b = boxes[atomRep ? atomRep[t.x] : 0];
   double px[3], py[3], pz[3], qx[3], qy[3], qz[3], rm[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
@@ -607,6 +615,18 @@ k_tri_stage2(int nTri, DevBox b, double dt, double tolvel, int maxCycle,
   }
 }
 
+// positions back into their box (image_update, src/utils.c:162-218)
+__global__ void k_wrap(int n, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
+                       double *__restrict__ x, double *__restrict__ y, double *__restrict__ z) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double xi = x[i], yi = y[i], zi = z[i];
+  image_d(boxes[atomRep ? atomRep[i] : 0], xi, yi, zi);
+  x[i] = xi;
+  y[i] = yi;
+  z[i] = zi;
+}
+
 // kinetic energy (src/utils.c:502-515), sum in fixed point (2^-24 units)
 __global__ void k_kinetic(int n, const double *__restrict__ mass, const double *__restrict__ vx,
                           const double *__restrict__ vy, const double *__restrict__ vz,
@@ -621,7 +641,8 @@ __global__ void k_kinetic(int n, const double *__restrict__ mass, const double *
 
 // largest squared displacement since the last build (minimum image), as the
 // bit pattern of a non-negative double (which orders like the double)
-__global__ void k_max_disp(int n, DevBox b, const double *__restrict__ x,
+__global__ void k_max_disp(int n, const DevBox *__restrict__ boxes,
+                           const int *__restrict__ atomRep, const double *__restrict__ x,
                            const double *__restrict__ y, const double *__restrict__ z,
                            const double *__restrict__ xb, const double *__restrict__ yb,
                            const double *__restrict__ zb, unsigned long long *__restrict__ out) {
@@ -629,7 +650,7 @@ __global__ void k_max_disp(int n, DevBox b, const double *__restrict__ x,
   double r2 = 0.;
   if (i < n) {
     double dx = x[i] - xb[i], dy = y[i] - yb[i], dz = z[i] - zb[i];
-    r2 = dist_d(b, dx, dy, dz);
+    r2 = dist_d(boxes[atomRep ? atomRep[i] : 0], dx, dy, dz);
     if (!(r2 == r2)) r2 = 1e300;  // NaN forces a rebuild (which reports it)
   }
 #pragma unroll
@@ -701,6 +722,9 @@ __global__ void k_md_row(long long *__restrict__ row, const long long *__restric
 }  // namespace
 }  // namespace mdbas
 
+// every replica's box and the atom -> replica map, as the MD kernels take them
+#define BOXES(e) (e)->boxesDev.as<DevBox>(), (e)->atomRepPtr()
+
 #define MD_TRY(expr)                                                           \
   do {                                                                         \
     int s__ = (expr);                                                          \
@@ -769,14 +793,14 @@ int md_stage1(mdbas_nb_engine *e, cudaStream_t s) {
     if (e->mdNTri < n)
       MDB_LAUNCH(k_vv_stage1, grid_for(n, 256), 256, 0, s, n, e->mdDt, fx, fy, fz,
                  e->mdRmass.as<double>(), vx, vy, vz, x, y, z, e->mdNAt.as<int>());
-    MDB_LAUNCH(k_tri_stage1, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, e->mdDt,
+    MDB_LAUNCH(k_tri_stage1, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, BOXES(e), e->mdDt,
                e->mdTol, e->mdMaxCycle, e->mdTriAtoms.as<int4>(), e->mdTriLen2.as<double4>(),
                fx, fy, fz, e->mdRmass.as<double>(), x, y, z, vx, vy, vz,
                reinterpret_cast<int *>(e->mdWord.as<long long>() + W_SHAKE));
     return MDBAS_NB_OK;
   }
   if (nc > 0)
-    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
+    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, BOXES(e), e->mdCa.as<int>(),
                e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
   MDB_LAUNCH(k_vv_stage1, grid_for(n, 256), 256, 0, s, n, e->mdDt, fx, fy, fz,
              e->mdRmass.as<double>(), vx, vy, vz, x, y, z, nullptr);
@@ -784,7 +808,7 @@ int md_stage1(mdbas_nb_engine *e, cudaStream_t s) {
     auto shake = e->mdMolClass == 0   ? k_shake_positions<kMolTinyAtoms, kMolTinyCons>
                  : e->mdMolClass == 1 ? k_shake_positions<kMolSmallAtoms, kMolSmallCons>
                                       : k_shake_positions<kMolMaxAtoms, kMolMaxCons>;
-    MDB_LAUNCH(shake, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box,
+    MDB_LAUNCH(shake, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, BOXES(e),
                e->mdDt, e->mdTol, e->mdMaxCycle, e->mdMol.as<int>(), e->mdCa.as<int>(),
                e->mdCb.as<int>(), e->mdRc2.as<double>(), ddx, ddy, ddz, e->mdRmass.as<double>(),
                e->mdNAt.as<int>(), x, y, z, vx, vy, vz,
@@ -798,7 +822,7 @@ int md_max_disp(mdbas_nb_engine *e, cudaStream_t s) {
   long long *word = e->mdWord.as<long long>();
   const double *xb = e->mdXb.as<double>();
   MDB_CUDA(cudaMemsetAsync(word + W_DISP, 0, sizeof(long long), s));
-  MDB_LAUNCH(k_max_disp, grid_for(n, 256), 256, 0, s, n, e->box, e->x.as<double>(),
+  MDB_LAUNCH(k_max_disp, grid_for(n, 256), 256, 0, s, n, BOXES(e), e->x.as<double>(),
              e->y.as<double>(), e->z.as<double>(), xb, xb + n, xb + 2 * (size_t)n,
              reinterpret_cast<unsigned long long *>(word + W_DISP));
   return MDBAS_NB_OK;
@@ -809,12 +833,12 @@ int md_max_disp(mdbas_nb_engine *e, cudaStream_t s) {
 int md_forces_cluster(mdbas_nb_engine *e, cudaStream_t s) {
   ClusterWork &w = e->cl;
   const int n = e->n;
-  MDB_TRY(cluster_refresh(w, n, e->box, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+  MDB_TRY(cluster_refresh(w, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                           e->q.as<double>(), sqrt(e->cfg.chargeConst), s));
   MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
   MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
   MDB_TRY(pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
-  MDB_TRY(excl_fix_launch(w, n, e->box, e->pp, e->exclStart.as<int>(), e->exclFlat.as<int>(),
+  MDB_TRY(excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(), e->exclFlat.as<int>(),
                           e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                           e->q.as<double>(), s));
   return md_forces(e, s);
@@ -834,7 +858,7 @@ int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double 
     if (e->mdNTri < n)
       MDB_LAUNCH(k_vv_kick, g, 256, 0, s, n, e->mdDt, fx, fy, fz, e->mdRmass.as<double>(), vx,
                  vy, vz, e->mdNAt.as<int>());
-    MDB_LAUNCH(k_tri_stage2, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, e->box, e->mdDt,
+    MDB_LAUNCH(k_tri_stage2, grid_for(e->mdNMol, 128), 128, 0, s, e->mdNMol, BOXES(e), e->mdDt,
                e->mdTol / e->mdDt, e->mdMaxCycle, e->mdTriAtoms.as<int4>(), fx, fy, fz,
                e->mdRmass.as<double>(), x, y, z, vx, vy, vz,
                reinterpret_cast<int *>(word + W_SHAKE));
@@ -844,7 +868,7 @@ int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double 
   }
   if (nc > 0 && !e->mdTri) {
     // stage 2 takes the constraint vectors at the new positions
-    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, e->box, e->mdCa.as<int>(),
+    MDB_LAUNCH(k_cons_vectors, grid_for(nc, 256), 256, 0, s, nc, BOXES(e), e->mdCa.as<int>(),
                e->mdCb.as<int>(), x, y, z, ddx, ddy, ddz);
     auto rattle = e->mdMolClass == 0   ? k_shake_velocities<kMolTinyAtoms, kMolTinyCons>
                   : e->mdMolClass == 1 ? k_shake_velocities<kMolSmallAtoms, kMolSmallCons>
@@ -863,7 +887,8 @@ int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double 
     MDB_LAUNCH(k_berendsen, g, 256, 0, s, n, e->mdDt / tauT, kinTemp0, word + W_KIN, vx, vy,
                vz);
   // positions back into the box (image_update, src/integrate.c:1626)
-  return image_update_device(n, e->box, x, y, z, s);
+  MDB_LAUNCH(k_wrap, g, 256, 0, s, n, BOXES(e), x, y, z);
+  return MDBAS_NB_OK;
 }
 
 double md_kin_row(double kin, double dt, double tauT, double kinTemp0) {
@@ -906,8 +931,9 @@ int md_capture_rebuild_body(mdbas_nb_engine *e, cudaGraph_t body, long long *cou
                                          cudaStreamCaptureModeRelaxed));
   g_launch_counter = counter;
   const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
-  int st = cluster_build(e->cl, e->n, e->box, e->cfg.cutOff, e->cfg.delr,
-                         sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
+  int st = cluster_build(e->cl, e->n, e->nRep, e->repBoxes.data(), e->repOff.data(),
+                         e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(),
+                         e->y.as<double>(),
                          e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),
                          e->sig.as<double>(), frozen, e->exclStart.as<int>(),
                          e->exclFlat.as<int>(), side, false);
@@ -1276,7 +1302,7 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
     for (int i = 0; i < n; ++i) nFrozen += fr[i] != 0;
   }
   // degrees of freedom (get_degfree, src/utils.c:569-581)
-  e->mdDegFree = 3 * (n - nFrozen) - 3 - nConst;
+  e->mdDegFree = 3 * (n - nFrozen) - 3 * e->nRep - nConst;  // centre of mass per replica
   e->mdDt = timeStep;
   e->mdListUpdate = listUpdate;
   e->mdTol = tolShake > 0. ? tolShake : 1e-8;          // src/io.c:95

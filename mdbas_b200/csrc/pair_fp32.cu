@@ -435,7 +435,8 @@ k_pair_fp32c(const long long *__restrict__ counters, const int4 *__restrict__ it
 // Exclusion correction in FP64 (src/energy.c:567-621, ewald_corr
 // src/ewald.c:371-384) into the fixed-point accumulators.
 __global__ void __launch_bounds__(128)
-k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
+k_excl_fix(int n, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
+           PairParams p, const int *__restrict__ exclStart,
            const int *__restrict__ exclFlat, const double *__restrict__ x,
            const double *__restrict__ y, const double *__restrict__ z,
            const double *__restrict__ q, const int *__restrict__ slotOf,
@@ -443,6 +444,7 @@ k_excl_fix(int n, DevBox b, PairParams p, const int *__restrict__ exclStart,
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   long long ecorr = 0, vcorr = 0;
   if (i < n) {
+    const DevBox &b = boxes[atomRep ? atomRep[i] : 0];
     const int e = exclStart[i + 1];
     const int si = slotOf[i];
     for (int k = exclStart[i]; k < e; ++k) {
@@ -566,11 +568,12 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   return MDBAS_NB_OK;
 }
 
-int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
-                    const int *exclStart, const int *exclFlat, const double *x, const double *y,
-                    const double *z, const double *q, cudaStream_t s) {
+int excl_fix_launch(ClusterWork &w, int n, const PairParams &p, const int *exclStart,
+                    const int *exclFlat, const double *x, const double *y, const double *z,
+                    const double *q, cudaStream_t s) {
   if (n <= 0) return MDBAS_NB_OK;
-  MDB_LAUNCH(k_excl_fix, grid_for(n, 128), 128, 0, s, n, b, p, exclStart, exclFlat, x, y, z, q,
+  MDB_LAUNCH(k_excl_fix, grid_for(n, 128), 128, 0, s, n, w.boxes.as<DevBox>(), w.atomRepDev(),
+             p, exclStart, exclFlat, x, y, z, q,
              w.slotOf.as<int>(), w.facc.as<long long>(), w.slotCap, w.acc.as<long long>());
   return MDBAS_NB_OK;
 }

@@ -25,9 +25,11 @@ enum { kPairDense = 0, kPairCompact = 1 };
 // number of warps.
 int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
                      int variant = kPairDense);
-int excl_fix_launch(ClusterWork &w, int n, const DevBox &b, const PairParams &p,
-                    const int *exclStart, const int *exclFlat, const double *x, const double *y,
-                    const double *z, const double *q, cudaStream_t s);
+// Ewald exclusion correction of every excluded pair (j > i), each replica's
+// pairs with its own box.
+int excl_fix_launch(ClusterWork &w, int n, const PairParams &p, const int *exclStart,
+                    const int *exclFlat, const double *x, const double *y, const double *z,
+                    const double *q, cudaStream_t s);
 int forces_out_launch(ClusterWork &w, int n, int add, double *fx, double *fy, double *fz,
                       cudaStream_t s);
 

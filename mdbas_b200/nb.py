@@ -219,6 +219,10 @@ def lib():
                                          _dp]
     L.mdbas_nb_engine_md_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     L.mdbas_nb_engine_md_set_graph.argtypes = [C.c_void_p, C.c_int]
+    L.mdbas_nb_batch_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(EngineConfig), C.c_int,
+                                        C.POINTER(PBC), _ip]
+    L.mdbas_nb_batch_count.argtypes = [C.c_void_p]
+    L.mdbas_nb_engine_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
@@ -261,10 +265,20 @@ class Engine:
         cfg = EngineConfig(self.n, device, cutOff, cutOn, delr, alpha,
                            CHARGE_CONST if chargeConst is None else chargeConst, vdwSwitch,
                            precision, linkRatio, noLink)
-        self.pbc = make_pbc(system.cell() if cell is None else cell, box_type)
         h = C.c_void_p()
-        check(L.mdbas_nb_engine_create(C.byref(h), C.byref(cfg), C.byref(self.pbc)),
-              "engine_create")
+        reps = system.meta.get("replicas") if system.meta else None
+        if reps:
+            # a batch of independent boxes (systems.concat)
+            self.pbc = (PBC * len(reps))(*[make_pbc(c, box_type) for c, _ in reps])
+            counts = np.array([k for _, k in reps], dtype=np.int32)
+            self.offsets = np.concatenate([[0], np.cumsum(counts)])
+            check(L.mdbas_nb_batch_create(C.byref(h), C.byref(cfg), len(reps), self.pbc,
+                                          counts.ctypes.data_as(_ip)), "batch_create")
+        else:
+            self.pbc = make_pbc(system.cell() if cell is None else cell, box_type)
+            self.offsets = np.array([0, self.n])
+            check(L.mdbas_nb_engine_create(C.byref(h), C.byref(cfg), C.byref(self.pbc)),
+                  "engine_create")
         self.h = h
         # exclusions: (start[n+1], flat) rows, by default from the system's
         # bonds and angles
@@ -381,6 +395,25 @@ class Engine:
                                            buf.ctypes.data_as(_dp) if rows else None),
               "engine_md_run")
         return buf[:rows]
+
+    def autotune(self) -> dict:
+        """Time the pair kernel's variants and launch shapes on the current list
+        and keep the fastest (call after build; recompute afterwards)."""
+        out = (C.c_int * 4)()
+        check(lib().mdbas_nb_engine_autotune(self.h, out), "engine_autotune")
+        return {"variant": out[0], "block": out[1], "blocks_per_sm": out[2],
+                "candidates": out[3]}
+
+    def split(self, arrays):
+        """Per-replica views of concatenated per-atom arrays."""
+        o = self.offsets
+        return [[a[o[r]:o[r + 1]] for a in arrays] for r in range(len(o) - 1)]
+
+    @staticmethod
+    def split_arrays(arrays, batch):
+        """Per-replica views of per-atom arrays of a systems.concat batch."""
+        o = batch.meta["offsets"]
+        return [[a[o[r]:o[r + 1]] for a in arrays] for r in range(len(o) - 1)]
 
     def md_set_graph(self, steps_per_launch: int):
         """Steps per CUDA-graph launch of the mixed-precision dynamics (0 = off)."""

@@ -250,6 +250,32 @@ def replica_sizes(count: int = 64, lo: int = 1500, hi: int = 30000, seed: int = 
     return [int(max(lo, min(hi, 3 * round(x / 3)))) for x in v]
 
 
+def concat(parts: list[System], name: str = "batch") -> System:
+    """Independent boxes as one batch: atoms concatenated in order, bonds and
+    angles renumbered, meta["replicas"] = [(cell rows, atom count), ...]."""
+    offs = np.cumsum([0] + [p.n for p in parts])
+    cat = lambda attr: np.concatenate([getattr(p, attr) for p in parts])
+    bonds = np.concatenate([p.bonds + o for p, o in zip(parts, offs)]).astype(np.int32)
+    angles = np.concatenate([p.angles + o for p, o in zip(parts, offs)]).astype(np.int32)
+    out = System(name, parts[0].box, cat("x"), cat("y"), cat("z"), cat("q"), cat("eps"),
+                 cat("sig"), cat("mass"), bonds.reshape(-1, 2), angles.reshape(-1, 3),
+                 meta={"replicas": [(p.cell(), p.n) for p in parts],
+                       "offsets": offs.tolist()})
+    if all(p.vx is not None for p in parts):
+        out.vx, out.vy, out.vz = cat("vx"), cat("vy"), cat("vz")
+    return out
+
+
+def config_replicas(count: int = 64, seed: int = 1, temperature: float | None = None) -> System:
+    """Batched replicas: `count` water boxes with seeded log-uniform atom
+    counts in [1,500, 30,000] (multiples of 3), each at 0.0334 molecules/A^3
+    from the lattice-plus-jitter generator (replica i uses seed + i)."""
+    sizes = replica_sizes(count, seed=seed)
+    parts = [water_box_for_atoms(n, seed=seed + i, temperature=temperature)
+             for i, n in enumerate(sizes)]
+    return concat(parts, name=f"replicas{count}")
+
+
 # Named workloads (sizes of the reference's headline configurations).
 def config_small(seed: int = 1) -> System:
     """3,000-atom water (1,000 molecules) in a 31.0 A box."""

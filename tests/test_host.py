@@ -100,3 +100,24 @@ def test_make_param_derived_terms():
     assert p.cutOff2 == 144.0 and p.cutOn2 == 100.0
     assert p.switch2 == 1.0 / (44.0 * 44.0 * 44.0)
     assert math.isclose(p.chargeConst, 332.0716 * 418.4)
+
+
+def test_concat_batch_layout():
+    from mdbas_b200 import systems
+    a = systems.water_box_for_atoms(1500, seed=1, temperature=300.0)
+    b = systems.water_box_for_atoms(2100, seed=2, temperature=300.0)
+    c = systems.concat([a, b])
+    assert c.n == a.n + b.n
+    assert c.meta["offsets"] == [0, a.n, a.n + b.n]
+    assert [n for _, n in c.meta["replicas"]] == [a.n, b.n]
+    assert np.array_equal(c.x[a.n:], b.x)
+    # bonds renumbered into the second replica's range
+    assert c.bonds.min() == 0 and c.bonds[len(a.bonds):].min() == a.n
+    start, flat = c.exclusions(symmetric=True)
+    sa, fa = a.exclusions(symmetric=True)
+    assert np.array_equal(start[:a.n + 1], sa)
+    assert np.array_equal(flat[:len(fa)], fa)
+    pairs, len2 = c.water_constraints()
+    assert len(pairs) == c.n and pairs.max() == c.n - 1
+    sizes = systems.replica_sizes(64, seed=1)
+    assert len(sizes) == 64 and all(s % 3 == 0 and 1500 <= s <= 30000 for s in sizes)
