@@ -63,6 +63,8 @@ def _parse():
                    help="NVE steps (1 fs) for the energy-drift report; 0 skips it")
     p.add_argument("--large-steps", type=int, default=10,
                    help="timed steps of the 999,999-atom box; 0 skips it")
+    p.add_argument("--replica-steps", type=int, default=100,
+                   help="timed dynamics steps of the 64-replica batch (one CUDA graph); 0 skips")
     return p.parse_args()
 
 
@@ -360,6 +362,95 @@ def large_box_measure(torch, nb, systems, dev, stream, flush, seed, steps):
         "l2": "flushed before every timed step (256 MiB write)"}
 
 
+def replicas_measure(torch, nb, systems, dev, stream, flush, seed, steps, world):
+    """64 independent water boxes (1,500-30,000 atoms, log-uniform) in one
+    engine: autotuned pair kernel, aggregate pairs/s of the build + force
+    step, a `steps`-step velocity-Verlet loop captured as one CUDA graph
+    (rigid water, rebuilds on half-skin displacement), and each replica's
+    force error against the plain FP64 form."""
+    import numpy as np
+    batch = systems.config_replicas(64, seed=seed, temperature=300.0)
+    parts_n = [k for _, k in batch.meta["replicas"]]
+    eng = nb.Engine(batch, precision=1, device=dev)
+    eng.set_stream(stream.cuda_stream)
+    eng.build()
+    tune = eng.autotune()
+    eng.compute()
+    torch.cuda.synchronize()
+    pairs = int(eng.energies()["n_pairs"])
+    fb = eng.forces()
+
+    def step():
+        eng.build()
+        eng.compute()
+
+    for _ in range(3):
+        step()
+    ms = _time_steps(torch, eng, stream, flush, 10, step)
+    eng.set_timing(True)
+    eng.pair_kernel_ms(reset=True)
+    for _ in range(10):
+        flush.zero_()
+        eng.compute()
+    pair_ms, _ = eng.pair_kernel_ms(reset=True)
+    eng.set_timing(False)
+    # per-replica error against the FP64 form
+    errs = []
+    for r, got in enumerate(nb.Engine.split_arrays(fb, batch)):
+        sub = systems.replica(batch, r)
+        ref = nb.Engine(sub, precision=0, device=dev)
+        ref.build()
+        ref.compute()
+        fr = ref.forces()
+        ref.close()
+        num = sum(((a - b) ** 2).sum() for a, b in zip(got, fr))
+        den = sum((b ** 2).sum() for b in fr)
+        errs.append(float(np.sqrt(num / den)))
+    # dynamics: relax, then `steps` NVE steps as one graph launch
+    cons = batch.water_constraints()
+    eng.md_set_graph(20)
+    eng.md_init(batch.mass, (batch.vx, batch.vy, batch.vz), time_step=0.0005, list_update=0,
+                constraints=cons)
+    eng.md_run(1000, target_temp=300.0, tau_t=0.05)
+    pos, vel = eng.positions(), eng.velocities()
+    eng.set_positions(*pos)
+    eng.md_set_graph(steps)
+    eng.md_init(batch.mass, vel, time_step=0.001, list_update=0, constraints=cons)
+    eng.md_run(steps)                       # captures the graph
+    st0 = eng.md_stats()
+    l0 = eng.launches()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.md_run(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    md_ms = e0.elapsed_time(e1) / steps
+    st1 = eng.md_stats()
+    launches = eng.launches() - l0
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([md_ms, sum(ms) / len(ms)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        md_ms, t_step = float(tt[0].item()), float(tt[1].item())
+    else:
+        t_step = sum(ms) / len(ms)
+    return {
+        "workload": "64 water boxes, 1,500-30,000 atoms (seeded log-uniform), one engine",
+        "n_atoms": int(batch.n), "replica_atoms_min_max": [min(parts_n), max(parts_n)],
+        "in_cutoff_pairs": pairs, "autotune": tune,
+        "ms_per_step": t_step, "pairs_per_s": pairs / (t_step * 1e-3),
+        "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
+        "force_rel_rms_vs_fp64_form": {"max": max(errs), "mean": float(np.mean(errs))},
+        "md": {"steps_per_graph_launch": steps, "ms_per_step": md_ms,
+               "pairs_per_s": pairs / (md_ms * 1e-3),
+               "aggregate_ns_per_day": 64 * 86400.0 / (md_ms * 1e-3) * 1e-6,
+               "list_builds": st1["rebuilds"] - st0["rebuilds"],
+               "kernel_launches_per_step": launches / steps}}
+
+
 def run_ours(args, rank, world):
     import numpy as np
     import torch
@@ -525,6 +616,11 @@ def run_ours(args, rank, world):
         large = large_box_measure(torch, nb, systems, dev, stream, flush, args.seed + rank,
                                   args.large_steps)
 
+    replicas = None
+    if args.replica_steps > 0:
+        replicas = replicas_measure(torch, nb, systems, dev, stream, flush, args.seed + rank,
+                                    args.replica_steps, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(args.seed)
@@ -546,6 +642,7 @@ def run_ours(args, rank, world):
             "md": md,
             "md_fp64_form": md64,
             "large_box": large,
+            "replicas": replicas,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
                             "variant": "dense 8x8", "compacted_variant_ms": compact_ms},
             "list_build": {"ms": t_build,

@@ -266,6 +266,22 @@ def concat(parts: list[System], name: str = "batch") -> System:
     return out
 
 
+def replica(batch: System, r: int) -> System:
+    """Replica r of a systems.concat batch as a System of its own."""
+    o = batch.meta["offsets"]
+    lo, hi = o[r], o[r + 1]
+    cell = batch.meta["replicas"][r][0]
+    sel = slice(lo, hi)
+    bsel = (batch.bonds[:, 0] >= lo) & (batch.bonds[:, 0] < hi)
+    asel = (batch.angles[:, 0] >= lo) & (batch.angles[:, 0] < hi)
+    out = System(f"{batch.name}[{r}]", float(cell[0]), batch.x[sel], batch.y[sel], batch.z[sel],
+                 batch.q[sel], batch.eps[sel], batch.sig[sel], batch.mass[sel],
+                 batch.bonds[bsel] - lo, batch.angles[asel] - lo)
+    if batch.vx is not None:
+        out.vx, out.vy, out.vz = batch.vx[sel], batch.vy[sel], batch.vz[sel]
+    return out
+
+
 def config_replicas(count: int = 64, seed: int = 1, temperature: float | None = None) -> System:
     """Batched replicas: `count` water boxes with seeded log-uniform atom
     counts in [1,500, 30,000] (multiples of 3), each at 0.0334 molecules/A^3
