@@ -13,6 +13,12 @@ not excluded) per second of device time, summed over ranks; ``e2e`` is the
 same through the engine's C ABI with host buffers (pinned H2D of the
 positions and D2H of forces and energies inside the timed region).
 
+Further keys: ``md`` (the device-resident velocity-Verlet step of the same box,
+rigid water, rebuilds on half-skin displacement, CUDA-graph launches of 20
+steps: ms per step and ns/day at 1 fs, and the NVE energy drift over
+``--nve-steps``), ``md_fp64_form`` (the same loop over the plain FP64 form),
+``large_box`` (999,999 atoms) and ``replicas`` (64 boxes in one engine).
+
 ``--impl reference`` times MDBas itself (oracle/_ref, its list rebuild +
 energy() with real-space Ewald) on the host cores, one process per core
 slot, each process evaluating its own copy of the workload per step.
