@@ -461,6 +461,22 @@ int mdbas_nb_engine_get_velocities(mdbas_nb_engine *e, double *vx, double *vy, d
                                    int device_ptrs);
 
 /* ------------------------------------------------------------------------ */
+/* 6. Adjoint of the real-space energy (no counterpart in MDBas, whose        */
+/*    numderiv.c gives only finite differences)                              */
+/* ------------------------------------------------------------------------ */
+/* On an FP64-form engine (precision 0) after build: gq/geps/gsig receive
+ * dE/d(q_i, eps_i, sig_i) per atom (eps_i, sig_i the per-atom MDBas values;
+ * E = real-space direct + exclusion correction + switched LJ + self term).
+ * With upstream weights v = (vx, vy, vz) on the forces F = -dE/dx, also
+ * hx/hy/hz = d(v.F)/dx (= -H v, a Hessian-vector product along positions)
+ * and pq/peps/psig = d(v.F)/d(q_i, eps_i, sig_i); pass vx = NULL to skip.
+ * Arrays of nAtom doubles, host (device_ptrs = 0) or device. */
+int mdbas_nb_engine_adjoint(mdbas_nb_engine *e, const double *vx, const double *vy,
+                            const double *vz, double *gq, double *geps, double *gsig,
+                            double *hx, double *hy, double *hz, double *pq, double *peps,
+                            double *psig, int device_ptrs);
+
+/* ------------------------------------------------------------------------ */
 /* 5. Batches of independent boxes (no counterpart in MDBas, which runs one   */
 /*    system per process)                                                    */
 /* ------------------------------------------------------------------------ */

@@ -40,6 +40,8 @@ struct mdbas_nb_engine {
   int variant = 0;  // pair kernel variant (kPairDense)
   // export scratch
   mdbas::DBuf exportBuf, exportCount;
+  // adjoint scratch (adjoint.cu)
+  mdbas::DBuf adjBuf;
   // bookkeeping
   bool built = false, computed = false;
   long long launches = 0;

@@ -223,6 +223,7 @@ def lib():
                                         C.POINTER(PBC), _ip]
     L.mdbas_nb_batch_count.argtypes = [C.c_void_p]
     L.mdbas_nb_engine_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
+    L.mdbas_nb_engine_adjoint.argtypes = [C.c_void_p] + [C.c_void_p] * 12 + [C.c_int]
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
@@ -288,11 +289,22 @@ class Engine:
                       for a in (system.q, system.eps, system.sig)]
         fz = None if frozen is None else np.ascontiguousarray(frozen, dtype=np.int32)
         flat = np.ascontiguousarray(flat if len(flat) else np.zeros(1, np.int32), dtype=np.int32)
+        self._frozen, self._excl_pair, self._excl_flat = fz, pair, flat
         check(L.mdbas_nb_engine_set_topology(
             h, *(a.ctypes.data_as(_dp) for a in self._topo),
             None if fz is None else fz.ctypes.data_as(_ip), pair.ctypes.data_as(_ip),
             flat.ctypes.data_as(_ip)), "engine_set_topology")
         self.set_positions(system.x, system.y, system.z)
+
+    def set_parameters(self, q, eps, sig):
+        """Replace the per-atom charges and LJ parameters (MDBas per-atom
+        values; exclusions and frozen atoms kept)."""
+        self._topo = [np.ascontiguousarray(a, dtype=np.float64) for a in (q, eps, sig)]
+        check(lib().mdbas_nb_engine_set_topology(
+            self.h, *(a.ctypes.data_as(_dp) for a in self._topo),
+            None if self._frozen is None else self._frozen.ctypes.data_as(_ip),
+            self._excl_pair.ctypes.data_as(_ip), self._excl_flat.ctypes.data_as(_ip)),
+            "engine_set_topology")
 
     def set_positions(self, x, y, z):
         self._pos = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
@@ -414,6 +426,20 @@ class Engine:
         """Per-replica views of per-atom arrays of a systems.concat batch."""
         o = batch.meta["offsets"]
         return [[a[o[r]:o[r + 1]] for a in arrays] for r in range(len(o) - 1)]
+
+    def adjoint(self, v=None) -> dict:
+        """dE/d(q, eps, sig) per atom and, with force weights v = (vx, vy, vz),
+        d(v.F)/dx and d(v.F)/d(q, eps, sig) (FP64 form engines, after build)."""
+        n = self.n
+        names = ["gq", "geps", "gsig", "hx", "hy", "hz", "pq", "peps", "psig"]
+        out = {k: np.zeros(n) for k in (names if v is not None else names[:3])}
+        vv = [None, None, None]
+        if v is not None:
+            self._adj_v = [np.ascontiguousarray(a, dtype=np.float64) for a in v]
+            vv = [_ptr(a) for a in self._adj_v]
+        ptrs = [_ptr(out[k]) if k in out else None for k in names]
+        check(lib().mdbas_nb_engine_adjoint(self.h, *vv, *ptrs, 0), "engine_adjoint")
+        return out
 
     def md_set_graph(self, steps_per_launch: int):
         """Steps per CUDA-graph launch of the mixed-precision dynamics (0 = off)."""
