@@ -523,13 +523,15 @@ def run_ours(args, rank, world):
         flush.zero_()
         eng.compute()
     pair_ms, _ = eng.pair_kernel_ms(reset=True)
-    # the filtered/compacted variant of the same kernel, for comparison
-    eng.set_variant(1)
-    for _ in range(args.steps):
-        flush.zero_()
-        eng.compute()
-    compact_ms, _ = eng.pair_kernel_ms(reset=True)
-    eng.set_variant(0)
+    # the other variants of the same kernel, for comparison
+    other_ms = {}
+    for v, name in ((0, "scalar_dense"), (1, "compacted")):
+        eng.set_variant(v)
+        for _ in range(args.steps):
+            flush.zero_()
+            eng.compute()
+        other_ms[name], _ = eng.pair_kernel_ms(reset=True)
+    eng.set_variant(2)
     eng.set_timing(False)
     # list build alone
     ms_build = _time_steps(torch, eng, stream, flush, args.steps, eng.build)
@@ -650,7 +652,8 @@ def run_ours(args, rank, world):
             "large_box": large,
             "replicas": replicas,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
-                            "variant": "dense 8x8", "compacted_variant_ms": compact_ms},
+                            "variant": "packed f32x2, 8x8 cluster pairs, staged",
+                            "other_variants_ms": other_ms},
             "list_build": {"ms": t_build,
                            "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9},
             "fp64_form": {"ms_per_step": t64, "pairs_per_s": pairs / (t64 * 1e-3),
@@ -660,7 +663,7 @@ def run_ours(args, rank, world):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured FFMA probe (mdbas_nb_fp32_peak)",
-                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32"},
+                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32x2"},
             "precision": prec,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 3 * 8 * n,

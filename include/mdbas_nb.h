@@ -398,9 +398,12 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]);
  * the number of pairs; pairs (2*capacity ints) may be NULL to query it. */
 int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, long long capacity,
                                  long long *count);
-/* Pair kernel variant of the mixed-precision path: 0 (default) computes every
- * pair of each 8x8 cluster pair in one warp step per cluster pair; 1 filters
- * the pairs first and computes only in-cut-off pairs from per-atom queues. */
+/* Pair kernel variant of the mixed-precision path: 2 (default) computes every
+ * pair of each 8x8 cluster pair in one warp step per cluster pair, a lane's
+ * two pairs in packed f32x2 arithmetic, with each chunk of 8 cluster pairs
+ * staged in shared memory; 0 is the same in scalar FP32 without staging;
+ * 1 filters the pairs first and computes only in-cut-off pairs from per-atom
+ * queues. */
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
 /* Autotuner of the mixed-precision pair kernel: times each variant and
  * launch shape (threads per block x blocks per SM) on the current list with

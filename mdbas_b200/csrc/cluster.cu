@@ -131,6 +131,7 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
                            double sqrtC, double4 *__restrict__ origin,
                            float4 *__restrict__ originF, float4 *__restrict__ half,
                            float4 *__restrict__ xq, float2 *__restrict__ lj,
+                           float *__restrict__ xp, float *__restrict__ ljp,
                            int *__restrict__ slotOf, int *__restrict__ clusterXY,
                            int *__restrict__ hmaxBits) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -177,15 +178,24 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
   for (int k = 0; k < kClusterSize; ++k) {
     const int s = c * kClusterSize + k;
     const int a = atoms[k];
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    float2 l = make_float2(0.f, 0.f);
     if (a >= 0) {
-      xq[s] = make_float4((float)(px[k] - ox), (float)(py[k] - oy), (float)(pz[k] - oz),
-                          (float)(q[a] * sqrtC));
-      lj[s] = make_float2((float)(2.0 * eps[a]), (float)sig[a]);
+      v = make_float4((float)(px[k] - ox), (float)(py[k] - oy), (float)(pz[k] - oz),
+                      (float)(q[a] * sqrtC));
+      l = make_float2((float)(2.0 * eps[a]), (float)sig[a]);
       slotOf[a] = s;
-    } else {
-      xq[s] = make_float4(0.f, 0.f, 0.f, 0.f);
-      lj[s] = make_float2(0.f, 0.f);
     }
+    xq[s] = v;
+    lj[s] = l;
+    float *p = xp + (size_t)(c * 4 + (k & 3)) * 8 + (k >> 2);
+    p[0] = v.x;
+    p[2] = v.y;
+    p[4] = v.z;
+    p[6] = v.w;
+    float *m = ljp + (size_t)(c * 4 + (k & 3)) * 4 + (k >> 2);
+    m[0] = l.x;
+    m[2] = l.y;
   }
 }
 
@@ -432,7 +442,7 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev,
                           const int *__restrict__ slotAtom, const double4 *__restrict__ origin,
                           const double *__restrict__ x, const double *__restrict__ y,
                           const double *__restrict__ z, const double *__restrict__ q, double sqrtC,
-                          float4 *__restrict__ xq) {
+                          float4 *__restrict__ xq, float *__restrict__ xp) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= *nSlotsDev) return;
   const int a = slotAtom[s];
@@ -443,7 +453,14 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev,
   dx -= g.Lx * rint(dx / g.Lx);
   dy -= g.Ly * rint(dy / g.Ly);
   dz -= g.Lz * rint(dz / g.Lz);
-  xq[s] = make_float4((float)dx, (float)dy, (float)dz, (float)(q[a] * sqrtC));
+  const float4 v = make_float4((float)dx, (float)dy, (float)dz, (float)(q[a] * sqrtC));
+  xq[s] = v;
+  const int k = s & (kClusterSize - 1);
+  float *p = xp + (size_t)((s / kClusterSize) * 4 + (k & 3)) * 8 + (k >> 2);
+  p[0] = v.x;
+  p[2] = v.y;
+  p[4] = v.z;
+  p[6] = v.w;
 }
 
 __global__ void k_latch(const long long *__restrict__ counters, long long *__restrict__ sticky) {
@@ -604,6 +621,8 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     MDB_TRY(w.hmax.ensure(sizeof(int) * 4 * nRep));
     MDB_TRY(w.xq.ensure(sizeof(float4) * w.slotCap));
     MDB_TRY(w.lj.ensure(sizeof(float2) * w.slotCap));
+    MDB_TRY(w.xp.ensure(sizeof(float4) * 8 * (size_t)w.clCap));
+    MDB_TRY(w.ljp.ensure(sizeof(float4) * 4 * (size_t)w.clCap));
     MDB_TRY(w.facc.ensure(sizeof(long long) * 3 * (size_t)w.slotCap));
   }
   const ClusterGeom *gd = w.geoms.as<ClusterGeom>();
@@ -628,8 +647,8 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
   MDB_LAUNCH(k_clusters, grid_for(w.clCap, 128), 128, 0, s, w.nSlotsDev(), gd, w.atomRepDev(),
              nRep > 1 ? w.clusterRep.as<int>() : nullptr, w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x,
              y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
-             w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.slotOf.as<int>(),
-             w.clusterXY.as<int>(), w.hmax.as<int>());
+             w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.xp.as<float>(),
+             w.ljp.as<float>(), w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
 
   // Cluster-pair search; in the synchronising form grow the list and search
   // again if it overflowed.
@@ -703,7 +722,7 @@ int cluster_refresh(ClusterWork &w, const double *x, const double *y, const doub
   if (w.slotCap <= 0) return MDBAS_NB_ERR_STATE;
   MDB_LAUNCH(k_refresh, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(),
              w.geoms.as<ClusterGeom>(), w.clusterRepDev(), w.slotAtom.as<int>(),
-             w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>());
+             w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>(), w.xp.as<float>());
   return MDBAS_NB_OK;
 }
 

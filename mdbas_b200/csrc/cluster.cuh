@@ -68,6 +68,13 @@ struct ClusterWork {
   DBuf half;          // float4 per cluster (bbox half extents, w = real atoms)
   DBuf xq;            // float4 per slot: position - origin, q*sqrt(C)
   DBuf lj;            // float2 per slot: 2*eps_i, sig_i
+  // The same slot data paired for packed (f32x2) arithmetic: for cluster c
+  // and h = 0..3 the atoms a = h and b = h + 4 sit side by side,
+  //   xp[2(4c+h)]   = (x_a, x_b, y_a, y_b), xp[2(4c+h)+1] = (z_a, z_b, q_a, q_b),
+  //   ljp[4c+h]     = (2eps_a, 2eps_b, sig_a, sig_b),
+  // so one lane's two j atoms load as float2 pairs.
+  DBuf xp;            // float4[8 per cluster]
+  DBuf ljp;           // float4[4 per cluster]
   // pair list
   DBuf entries;       // CPairEntry
   DBuf masks;         // uint2 (64 interaction bits)

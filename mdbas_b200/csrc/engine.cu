@@ -546,9 +546,10 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   struct Cand { int variant, block, bps; };
   std::vector<Cand> cands;
   // the dense kernel takes at most 256 threads per block (launch bounds)
-  for (int block : {64, 128, 256})
-    for (int bps : {2, 4, 8, 16, 32})
-      if (block * bps <= 2048 && bps <= 24) cands.push_back({kPairDense, block, bps});
+  for (int variant : {kPairPacked, kPairDense})
+    for (int block : {64, 128, 256})
+      for (int bps : {2, 4, 8, 16, 32})
+        if (block * bps <= 2048 && bps <= 24) cands.push_back({variant, block, bps});
   for (int bps : {2, 4, 5}) cands.push_back({kPairCompact, 128, bps});
   ClusterWork &w = e->cl;
   cudaStream_t s = e->stream;
@@ -585,7 +586,8 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
 }
 
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
-  if (!e || (variant != kPairDense && variant != kPairCompact)) return MDBAS_NB_ERR_ARG;
+  if (!e || (variant != kPairDense && variant != kPairCompact && variant != kPairPacked))
+    return MDBAS_NB_ERR_ARG;
   e->variant = variant;
   return MDBAS_NB_OK;
 }

@@ -37,7 +37,7 @@ struct mdbas_nb_engine {
   mdbas::ClusterWork cl;
   mdbas::DBuf fout;
   int grid = 0, block = 0;
-  int variant = 0;  // pair kernel variant (kPairDense)
+  int variant = 2;  // pair kernel variant (kPairPacked)
   // export scratch
   mdbas::DBuf exportBuf, exportCount;
   // adjoint scratch (adjoint.cu)

@@ -205,6 +205,214 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
 
 
 // ---------------------------------------------------------------------------
+// Packed variant (default).  The same mapping and results as k_pair_fp32, with
+// a lane's two pairs (j atoms h and h+4) evaluated together in f32x2
+// arithmetic (__ffma2_rn / __fmul2_rn / __fadd2_rn, one instruction for both
+// pairs on sm_100): the kernel is issue-bound, and this halves the issue
+// slots of its FP32 arithmetic.  The j data come from the pair-interleaved
+// copies xp/ljp, so each operand pair already sits in a register pair.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+
+template <bool VDW>
+__device__ __forceinline__ void interact2(const PairConstF &c, const float2 jx, const float2 jy,
+                                          const float2 jz, const float2 jq, const float2 jeps,
+                                          const float2 jsig, const float sx, const float sy,
+                                          const float sz, const float qi, const float2 li,
+                                          const bool bita, const bool bitb, bool &ina,
+                                          bool &inb, float2 &fx, float2 &fy, float2 &fz,
+                                          float2 &ec, float2 &ev, float2 &vc, float2 &vv) {
+  const float2 dx = __fadd2_rn(jx, f2(sx)), dy = __fadd2_rn(jy, f2(sy)),
+               dz = __fadd2_rn(jz, f2(sz));
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  ina = bita && (r2.x <= c.rc2);
+  inb = bitb && (r2.y <= c.rc2);
+  const float2 r2s = make_float2(ina ? r2.x : 1.0f, inb ? r2.y : 1.0f);
+  const float2 m = make_float2(ina ? 1.0f : 0.f, inb ? 1.0f : 0.f);
+  const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
+  const float2 nrinv = __fmul2_rn(rinv, f2(-1.0f));
+  const float2 r = __fmul2_rn(r2s, rinv);
+  const float2 qq = __fmul2_rn(__fmul2_rn(f2(qi), jq), m);
+  const float2 targ = __ffma2_rn(f2(c.p_alpha), r, f2(1.0f));
+  const float2 t = make_float2(rcp_approx(targ.x), rcp_approx(targ.y));
+  const float2 earg = __fmul2_rn(f2(-c.c_ex), r2s);
+  const float2 ex = make_float2(ex2_approx(earg.x), ex2_approx(earg.y));
+  float2 poly = __ffma2_rn(f2(kErfcC7), t, f2(kErfcC6));
+  poly = __ffma2_rn(poly, t, f2(kErfcC5));
+  poly = __ffma2_rn(poly, t, f2(kErfcC4));
+  poly = __ffma2_rn(poly, t, f2(kErfcC3));
+  poly = __ffma2_rn(poly, t, f2(kErfcC2));
+  poly = __ffma2_rn(poly, t, f2(kErfcC1));
+  poly = __ffma2_rn(poly, t, f2(kErfcC0));
+  const float2 qr = __fmul2_rn(qq, rinv);
+  const float2 e_c = __fmul2_rn(qr, __fmul2_rn(__fmul2_rn(t, poly), ex));
+  const float2 de_c =
+      __fmul2_rn(__ffma2_rn(__fmul2_rn(qq, f2(c.two_a_sqrtpi)), ex, e_c), nrinv);
+  ec = __fadd2_rn(ec, e_c);
+  vc = __ffma2_rn(de_c, r, vc);
+  float2 F = de_c;
+  if (VDW) {
+    const float2 eps = __fmul2_rn(__fmul2_rn(f2(li.x), jeps), m);  // 4 eps_i eps_j
+    const float2 sg = __fmul2_rn(__fadd2_rn(f2(li.y), jsig), rinv);
+    const float2 s2 = __fmul2_rn(sg, sg);
+    const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+    const float2 s12 = __fmul2_rn(s6, s6);
+    const float2 pv = __fmul2_rn(eps, __ffma2_rn(s6, f2(-1.0f), s12));
+    const float2 dpv = __fmul2_rn(eps, __ffma2_rn(f2(-12.f), s12, __fmul2_rn(f2(6.f), s6)));
+    const float2 s1 = __ffma2_rn(r2s, f2(-1.0f), f2(c.rc2));
+    const float2 Sv = __fmul2_rn(__fmul2_rn(s1, s1), __ffma2_rn(f2(c.sw_a), r2s, f2(c.sw_b)));
+    const float2 dSv = __fmul2_rn(__fmul2_rn(__fmul2_rn(f2(c.sw_c), r2s), s1),
+                                  __ffma2_rn(r2s, f2(-1.0f), f2(c.ron2)));
+    const bool swa = r2s.x > c.ron2, swb = r2s.y > c.ron2;
+    const float2 S = make_float2(swa ? Sv.x : 1.f, swb ? Sv.y : 1.f);
+    const float2 dS = make_float2(swa ? dSv.x : 0.f, swb ? dSv.y : 0.f);
+    const float2 de_v = __fmul2_rn(__ffma2_rn(pv, dS, __fmul2_rn(dpv, S)), rinv);
+    ev = __ffma2_rn(pv, S, ev);
+    vv = __ffma2_rn(de_v, r, vv);
+    F = __fadd2_rn(F, de_v);
+  }
+  F = __fmul2_rn(F, rinv);
+  fx = __fmul2_rn(F, dx);
+  fy = __fmul2_rn(F, dy);
+  fz = __fmul2_rn(F, dz);
+}
+
+// Per-warp staging area of the packed kernel: up to kStage entries of an item
+// with their j clusters' pair-interleaved data, loaded in one batch so that
+// all of a chunk's global loads are in flight together.
+constexpr int kStage = 8;
+struct StageWarp {
+  float4 en[kStage];            // j (as int bits), shift x, y, z
+  uint2 mk[kStage];             // interaction masks
+  float4 jd[kStage * 12];       // per entry and h: xp pair 0, xp pair 1, ljp
+};
+
+// (at most 80 registers: three blocks of 256 threads per SM)
+template <bool VDW>
+__global__ void __launch_bounds__(256, 3)
+k_pair_fp32x2(const long long *__restrict__ counters, const int4 *__restrict__ items,
+              const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
+              const float4 *__restrict__ xq, const float2 *__restrict__ lj,
+              const float4 *__restrict__ xp, const float4 *__restrict__ ljp, PairConstF c,
+              long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
+  __shared__ StageWarp stage[8];
+  StageWarp &S = stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jh = lane >> 3;
+  const bool up = il & 4, mid = il & 2, lo = il & 1;
+  const int comp = mid ? (lo ? 3 : 2) : (lo ? 1 : 0);
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * fstride;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;  // fixed point, summed per item
+  long long npair = 0;
+  bool overflow = false;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
+    float2 ec = f2(0.f), ev = f2(0.f), vc = f2(0.f), vv = f2(0.f);
+    for (int c0 = 0; c0 < ne; c0 += kStage) {
+      const int nc = min(kStage, ne - c0);
+      // stage: entries and masks (lanes 0..nc-1), then each lane three of
+      // the chunk's 12*nc float4 of j data
+      CPairEntry my{};
+      if (lane < nc) {
+        my = entries[e0 + c0 + lane];
+        S.en[lane] = make_float4(__int_as_float(my.j), my.sx, my.sy, my.sz);
+        S.mk[lane] = masks[e0 + c0 + lane];
+      }
+#pragma unroll
+      for (int r = 0; r < 3; ++r) {
+        const int idx = lane + 32 * r;             // < 96
+        const int k = idx / 12, q = idx - 12 * k;  // entry, (h, part)
+        const int jk = __shfl_sync(0xffffffffu, my.j, k & 7);
+        if (k < nc) {
+          const int h = q / 3, part = q - 3 * h;
+          const size_t jp = (size_t)jk * 4 + h;
+          S.jd[idx] = part < 2 ? xp[2 * jp + part] : ljp[jp];
+        }
+      }
+      __syncwarp();
+      for (int k = 0; k < nc; ++k) {
+        const float4 en = S.en[k];
+        const uint2 mk = S.mk[k];
+        const int j = __float_as_int(en.x);
+        const float sx = en.y - xi.x, sy = en.z - xi.y, sz = en.w - xi.z;
+        const float4 p0 = S.jd[k * 12 + jh * 3], p1 = S.jd[k * 12 + jh * 3 + 1],
+                     lp = S.jd[k * 12 + jh * 3 + 2];
+        float2 fx, fy, fz;
+        bool ina, inb;
+        interact2<VDW>(c, make_float2(p0.x, p0.y), make_float2(p0.z, p0.w),
+                       make_float2(p1.x, p1.y), make_float2(p1.z, p1.w),
+                       make_float2(lp.x, lp.y), make_float2(lp.z, lp.w), sx, sy, sz, xi.w, li,
+                       (mk.x >> lane) & 1u, (mk.y >> lane) & 1u, ina, inb, fx, fy, fz, ec, ev,
+                       vc, vv);
+        fi_x = __fadd2_rn(fi_x, fx);
+        fi_y = __fadd2_rn(fi_y, fy);
+        fi_z = __fadd2_rn(fi_z, fz);
+        const unsigned ba = __ballot_sync(0xffffffffu, ina);
+        const unsigned bb = __ballot_sync(0xffffffffu, inb);
+        if ((ba | bb) == 0u) continue;
+        npair += __popc(ba) + __popc(bb);
+        // reduce-scatter of the two j atoms' forces over the 8 i lanes
+        const float ax = fx.x, ay = fy.x, az = fz.x, bx = fx.y, by = fy.y, bz = fz.y;
+        float k0 = up ? bx : ax, k1 = up ? by : ay, k2 = up ? bz : az;
+        const float s0 = up ? ax : bx, s1 = up ? ay : by, s2 = up ? az : bz;
+        k0 += __shfl_xor_sync(0xffffffffu, s0, 4);
+        k1 += __shfl_xor_sync(0xffffffffu, s1, 4);
+        k2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+        const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
+        float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
+        u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
+        u1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+        const float w = lo ? u0 : u1;
+        float v = lo ? u1 : u0;
+        v += __shfl_xor_sync(0xffffffffu, w, 1);
+        if (comp < 3 && v != 0.f) {
+          overflow |= !(fabsf(v) < kForceLimitF);
+          red_add(fcomp + j * kClusterSize + (up ? jh + 4 : jh), fix_f(-v));
+        }
+      }
+      __syncwarp();
+    }
+    // i forces: the lane's two pairs, then the four j lanes of each i atom
+    float fix = fi_x.x + fi_x.y, fiy = fi_y.x + fi_y.y, fiz = fi_z.x + fi_z.y;
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jh < 3) {
+      const float v = (jh == 0) ? fix : (jh == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)jh * fstride + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    // Each item's energy is converted to fixed point on its own, so totals
+    // do not depend on which warp ran which item.
+    Ec += fix_e(warp_sum_d((double)ec.x + (double)ec.y));
+    Ev += fix_e(warp_sum_d((double)ev.x + (double)ev.y));
+    Vc += fix_e(warp_sum_d((double)vc.x + (double)vc.y));
+    Vv += fix_e(warp_sum_d((double)vv.x + (double)vv.y));
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    red_add(acc + ACC_NPAIR, npair);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Compacted variant.  Same work items, entries and results as k_pair_fp32,
 // but only in-cut-off pairs reach the expensive arithmetic:
 //   staging: a chunk of 8 entries and their 64 j atoms are loaded into shared
@@ -527,6 +735,14 @@ PairConstF make_pair_const(const PairParams &p) {
 int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
                      int variant) {
   const PairConstF c = make_pair_const(p);
+  if (variant == kPairPacked) {
+    auto kv = p.vdwSwitch ? k_pair_fp32x2<true> : k_pair_fp32x2<false>;
+    MDB_LAUNCH(kv, grid, block, 0, s, w.counters.as<long long>(), w.items.as<int4>(),
+               w.entries.as<CPairEntry>(), w.masks.as<uint2>(), w.xq.as<float4>(),
+               w.lj.as<float2>(), w.xp.as<float4>(), w.ljp.as<float4>(), c,
+               w.facc.as<long long>(), w.slotCap, w.acc.as<long long>());
+    return MDBAS_NB_OK;
+  }
   if (variant == kPairDense) {
     if (p.vdwSwitch)
       MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),

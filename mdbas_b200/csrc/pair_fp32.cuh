@@ -16,15 +16,16 @@ struct PairConstF {
 };
 
 PairConstF make_pair_const(const PairParams &p);
-// Pair kernel variants: dense (all 64 pairs of an entry per warp step) and
-// compacted (only in-cut-off pairs reach the interaction arithmetic).
-enum { kPairDense = 0, kPairCompact = 1 };
+// Pair kernel variants: dense (all 64 pairs of an entry per warp step, scalar
+// FP32), compacted (only in-cut-off pairs reach the interaction arithmetic)
+// and packed (the dense mapping in f32x2 arithmetic; the default).
+enum { kPairDense = 0, kPairCompact = 1, kPairPacked = 2 };
 // The pair kernel over all work items (grid-stride, item count read on the
 // device, so the launch needs no host synchronisation).  grid*block is the
 // number of threads of the dense variant; the compacted one uses the same
 // number of warps.
 int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
-                     int variant = kPairDense);
+                     int variant = kPairPacked);
 // Ewald exclusion correction of every excluded pair (j > i), each replica's
 // pairs with its own box.
 int excl_fix_launch(ClusterWork &w, int n, const PairParams &p, const int *exclStart,

@@ -366,7 +366,8 @@ class Engine:
         return int(lib().mdbas_nb_engine_launch_count(self.h))
 
     def set_variant(self, variant: int):
-        """Pair kernel: 0 = dense 8x8 (default), 1 = filtered and compacted."""
+        """Pair kernel: 2 = packed f32x2, staged (default), 0 = scalar dense 8x8,
+        1 = filtered and compacted."""
         check(lib().mdbas_nb_engine_set_variant(self.h, variant), "engine_set_variant")
 
     def set_timing(self, on: bool):
