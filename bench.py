@@ -71,6 +71,12 @@ def _parse():
                    help="timed steps of the 999,999-atom box; 0 skips it")
     p.add_argument("--replica-steps", type=int, default=100,
                    help="timed dynamics steps of the 64-replica batch (one CUDA graph); 0 skips")
+    p.add_argument("--case", choices=["pair", "md"], default=None,
+                   help="run one small case of the 96k box for a profiler and exit: 'pair' = "
+                        "list build + 4 force evaluations, 'md' = --md-steps dynamics steps "
+                        "driven from the host (a profiler sees no kernels inside graphs with "
+                        "conditional nodes)")
+    p.add_argument("--variant", type=int, default=2, help="pair kernel variant of --case pair")
     return p.parse_args()
 
 
@@ -579,7 +585,7 @@ def run_ours(args, rank, world):
     peak = nb.fp32_peak_tflops(dev)
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "pair_fp32_96k_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "pair_fp32x2_96k_traffic.json")
     if os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
@@ -677,8 +683,33 @@ def run_ours(args, rank, world):
     eng64.close()
 
 
+def run_case(args):
+    from mdbas_b200 import nb, systems
+    if args.case == "pair":
+        s = systems.config_96k(seed=args.seed, temperature=None)
+        e = nb.Engine(s, precision=1)
+        e.set_variant(args.variant)
+        e.build()
+        for _ in range(4):
+            e.compute()
+        print(json.dumps({"case": "pair", "variant": args.variant,
+                          "pairs": e.energies()["n_pairs"], "list": e.list_stats()}))
+    else:
+        s = systems.config_96k(seed=args.seed, temperature=300.0)
+        e = nb.Engine(s, precision=1)
+        e.md_set_graph(0)
+        e.md_init(s.mass, (s.vx, s.vy, s.vz), time_step=0.0005, list_update=0,
+                  constraints=s.water_constraints())
+        e.md_run(args.md_steps)
+        print(json.dumps({"case": "md", "steps": args.md_steps, "stats": e.md_stats()}))
+    e.close()
+
+
 def main():
     args = _parse()
+    if args.case:
+        run_case(args)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
