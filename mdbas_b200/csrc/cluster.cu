@@ -463,6 +463,68 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev,
   p[6] = v.w;
 }
 
+// One warp per item of the list: recompute each entry's mask at the inner
+// radius from the current layout (same lane/bit mapping as the pair kernel)
+// and append the entries that keep a pair to the inner list.
+__global__ void __launch_bounds__(128)
+k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
+        const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
+        const float4 *__restrict__ xq, float rin2, CPairEntry *__restrict__ entriesOut,
+        uint2 *__restrict__ masksOut, int4 *__restrict__ itemsOut,
+        long long *__restrict__ countersOut, long long entryCap, long long itemCap) {
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jl = lane >> 3;
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const float4 xi = xq[ci * kClusterSize + il];
+    uint2 mine = make_uint2(0u, 0u);
+    CPairEntry myEn{};
+    for (int k = 0; k < ne; ++k) {
+      const CPairEntry en = entries[e0 + k];
+      const uint2 mk = masks[e0 + k];
+      const float4 xa = xq[en.j * kClusterSize + jl], xb = xq[en.j * kClusterSize + jl + 4];
+      const float ax = xa.x + en.sx - xi.x, ay = xa.y + en.sy - xi.y, az = xa.z + en.sz - xi.z;
+      const float bx = xb.x + en.sx - xi.x, by = xb.y + en.sy - xi.y, bz = xb.z + en.sz - xi.z;
+      const bool ina = ((mk.x >> lane) & 1u) && (ax * ax + ay * ay + az * az <= rin2);
+      const bool inb = ((mk.y >> lane) & 1u) && (bx * bx + by * by + bz * bz <= rin2);
+      const unsigned lo = __ballot_sync(0xffffffffu, ina);
+      const unsigned hi = __ballot_sync(0xffffffffu, inb);
+      if (lane == k) {
+        mine = make_uint2(lo, hi);
+        myEn = en;
+      }
+    }
+    const bool keep = lane < ne && (mine.x | mine.y) != 0u;
+    const unsigned km = __ballot_sync(0xffffffffu, keep);
+    const int nkeep = __popc(km);
+    if (nkeep == 0) continue;
+    long long eo = 0, io = 0;
+    if (lane == 0) {
+      eo = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(countersOut + 0),
+                                (unsigned long long)nkeep);
+      io = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(countersOut + 1), 1ull);
+    }
+    eo = __shfl_sync(0xffffffffu, eo, 0);
+    io = __shfl_sync(0xffffffffu, io, 0);
+    if (eo + nkeep > entryCap || io >= itemCap) {
+      if (lane == 0)
+        atomicOr(reinterpret_cast<unsigned long long *>(countersOut + 2),
+                 (unsigned long long)CL_OVERFLOW);
+      continue;
+    }
+    if (keep) {
+      const int pos = __popc(km & ((1u << lane) - 1u));
+      entriesOut[eo + pos] = myEn;
+      masksOut[eo + pos] = mine;
+    }
+    if (lane == 0) itemsOut[io] = make_int4(ci, (int)eo, nkeep, 0);
+  }
+}
+
 __global__ void k_latch(const long long *__restrict__ counters, long long *__restrict__ sticky) {
   if (threadIdx.x == 0) sticky[0] |= counters[2];
 }
@@ -661,6 +723,10 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
       MDB_TRY(w.entries.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
       MDB_TRY(w.masks.ensure(sizeof(uint2) * (size_t)w.entryCap));
       MDB_TRY(w.items.ensure(sizeof(int4) * (size_t)w.itemCap));
+      MDB_TRY(w.entriesIn.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
+      MDB_TRY(w.masksIn.ensure(sizeof(uint2) * (size_t)w.entryCap));
+      MDB_TRY(w.itemsIn.ensure(sizeof(int4) * (size_t)w.itemCap));
+      MDB_TRY(w.countersIn.ensure(sizeof(long long) * 4));
     }
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
     MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long), s));
@@ -701,6 +767,20 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
   const int off[2] = {0, n};
   return cluster_build(w, n, 1, &b, off, cutOff, delr, sqrtC, x, y, z, q, eps, sig, frozen,
                        exclStart, exclFlat, s, sync);
+}
+
+int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s) {
+  if (w.entryCap <= 0 || !w.countersIn.p) return MDBAS_NB_ERR_STATE;
+  int dev = 0, sms = 148;
+  MDB_CUDA(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 4, s));
+  MDB_LAUNCH(k_prune, sms * 16, 128, 0, s, w.counters.as<long long>(), w.items.as<int4>(),
+             w.entries.as<CPairEntry>(), w.masks.as<uint2>(), w.xq.as<float4>(), rin2,
+             w.entriesIn.as<CPairEntry>(), w.masksIn.as<uint2>(), w.itemsIn.as<int4>(),
+             w.countersIn.as<long long>(), w.entryCap, w.itemCap);
+  MDB_LAUNCH(k_latch, 1, 32, 0, s, w.countersIn.as<long long>(), w.sticky.as<long long>());
+  return MDBAS_NB_OK;
 }
 
 int cluster_read_counts(ClusterWork &w, cudaStream_t s) {

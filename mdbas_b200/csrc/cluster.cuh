@@ -82,6 +82,11 @@ struct ClusterWork {
   DBuf counters;      // int64[4]: entries, items, overflow flag, candidates
   long long entryCap = 0, itemCap = 0;
   long long nEntries = 0, nItems = 0;
+  // Inner list for dynamics ("dynamic pruning"): the entries of the list
+  // above whose masks keep only the pairs found within an inner radius at the
+  // last prune; the pair kernel reads it instead while useInner is set.
+  DBuf entriesIn, masksIn, itemsIn, countersIn;
+  bool useInner = false;
   DBuf sticky;        // int64: OR of every build's error bits since last read
   // accumulators
   DBuf facc;          // int64 fixed-point forces, SoA [3][slotCap]
@@ -111,6 +116,10 @@ int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double 
                   double sqrtC, const double *x, const double *y, const double *z,
                   const double *q, const double *eps, const double *sig, const int *frozen,
                   const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync = true);
+// Prune the list into the inner list: keep the pairs within sqrt(rin2) at the
+// current layout (after cluster_refresh), drop entries left without pairs.
+// No host interaction (graph-capturable); requires a synchronising build.
+int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s);
 // Host copies of the list counts (synchronises the stream).
 int cluster_read_counts(ClusterWork &w, cudaStream_t s);
 // Refresh xq from the current FP64 positions (list kept).

@@ -344,6 +344,7 @@ int mdbas_nb_engine_build(mdbas_nb_engine *e) {
                               lc, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                               frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream));
   } else {
+    e->cl.useInner = false;  // a new list; dynamics prune it again
     ENG_TRY(e, cluster_build(e->cl, n, e->nRep, e->repBoxes.data(), e->repOff.data(),
                              e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
                              e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),

@@ -63,6 +63,10 @@ struct mdbas_nb_engine {
   // CUDA graph of mdGraphSteps whole steps (precision 1); rebuilt when stale
   int mdGraphSteps = 20, mdGraphK = 0;
   long long mdGraphMainK = 0, mdGraphBodyK = 0;  // kernels per step / per rebuild
+  long long mdGraphPruneK = 0;                   // kernels per prune
+  double mdPruneBuf = 0.0;  // inner-list buffer (A) of the mixed form; 0 = no pruning
+  mdbas::DBuf mdXp;         // positions at the last prune
+  long long mdPrunes = 0;
   bool mdGraphStale = true;
   double mdGraphTau = 0.0, mdGraphTemp = 0.0;
   cudaGraph_t mdGraph = nullptr;

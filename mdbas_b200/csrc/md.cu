@@ -639,23 +639,39 @@ __global__ void k_kinetic(int n, const double *__restrict__ mass, const double *
   if ((threadIdx.x & 31) == 0) red_add(acc, v);
 }
 
-// largest squared displacement since the last build (minimum image), as the
-// bit pattern of a non-negative double (which orders like the double)
+// largest squared displacement since the last build (minimum image) and,
+// when xp is given, since the last prune; each as the bit pattern of a
+// non-negative double (which orders like the double)
 __global__ void k_max_disp(int n, const DevBox *__restrict__ boxes,
                            const int *__restrict__ atomRep, const double *__restrict__ x,
                            const double *__restrict__ y, const double *__restrict__ z,
                            const double *__restrict__ xb, const double *__restrict__ yb,
-                           const double *__restrict__ zb, unsigned long long *__restrict__ out) {
+                           const double *__restrict__ zb, const double *__restrict__ xp,
+                           const double *__restrict__ yp, const double *__restrict__ zp,
+                           unsigned long long *__restrict__ outB,
+                           unsigned long long *__restrict__ outP) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double r2 = 0.;
+  double r2 = 0., p2 = 0.;
   if (i < n) {
+    const DevBox &b = boxes[atomRep ? atomRep[i] : 0];
     double dx = x[i] - xb[i], dy = y[i] - yb[i], dz = z[i] - zb[i];
-    r2 = dist_d(boxes[atomRep ? atomRep[i] : 0], dx, dy, dz);
+    r2 = dist_d(b, dx, dy, dz);
     if (!(r2 == r2)) r2 = 1e300;  // NaN forces a rebuild (which reports it)
+    if (xp) {
+      double ex = x[i] - xp[i], ey = y[i] - yp[i], ez = z[i] - zp[i];
+      p2 = dist_d(b, ex, ey, ez);
+      if (!(p2 == p2)) p2 = 1e300;
+    }
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(r2));
+  for (int o = 16; o > 0; o >>= 1) {
+    r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
+    p2 = fmax(p2, __shfl_xor_sync(0xffffffffu, p2, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(outB, (unsigned long long)__double_as_longlong(r2));
+    if (xp) atomicMax(outP, (unsigned long long)__double_as_longlong(p2));
+  }
 }
 
 // frozen atoms keep zero force and velocity (freeze_atoms, src/utils.c:131-150)
@@ -683,24 +699,24 @@ __global__ void k_berendsen(int n, double dtOverTau, double kinTemp0,
 }
 
 // --- graph-only kernels: the rebuild decision and the per-step record -----
-// Sets the rebuild condition from the largest squared displacement and
-// advances the device step counter.
-__global__ void k_decide_disp(cudaGraphConditionalHandle h,
-                              const unsigned long long *__restrict__ bits, double half2,
-                              long long *__restrict__ stepDev) {
-  if (threadIdx.x != 0) return;
-  const double d2 = __longlong_as_double((long long)bits[0]);
-  stepDev[0] += 1;
-  cudaGraphSetConditional(h, d2 > half2 ? 1u : 0u);
-}
-
-// Same for the fixed cadence of MDBas's "list N" (rebuild when step % N == 0).
-__global__ void k_decide_cadence(cudaGraphConditionalHandle h, long long *__restrict__ stepDev,
-                                 int update) {
+// Set the rebuild condition (hB) from the largest squared displacement since
+// the build, or from MDBas's fixed cadence "list N" (step % N == 0) when
+// update > 0, and the prune condition (hP: a rebuild, or the displacement
+// since the last prune past halfIn2; never when prune = 0); advance the
+// device step counter.
+__global__ void k_decide(cudaGraphConditionalHandle hB, cudaGraphConditionalHandle hP,
+                         const unsigned long long *__restrict__ bitsB,
+                         const unsigned long long *__restrict__ bitsP, double half2,
+                         double halfIn2, int update, int prune,
+                         long long *__restrict__ stepDev) {
   if (threadIdx.x != 0) return;
   const long long st = stepDev[0] + 1;
   stepDev[0] = st;
-  cudaGraphSetConditional(h, (st % update) == 0 ? 1u : 0u);
+  const bool rebuild = update > 0 ? (st % update) == 0
+                                  : __longlong_as_double((long long)bitsB[0]) > half2;
+  const bool pr = prune && (rebuild || __longlong_as_double((long long)bitsP[0]) > halfIn2);
+  cudaGraphSetConditional(hB, rebuild ? 1u : 0u);
+  if (prune) cudaGraphSetConditional(hP, pr ? 1u : 0u);
 }
 
 __global__ void k_count(long long *__restrict__ c) {
@@ -744,7 +760,9 @@ enum MdWord {
   W_SHAKE = 4,    // two ints: SHAKE error bits, largest iteration count
   W_STEP = 6,     // device step counter (graph form)
   W_BUILDS = 7,   // list builds inside the graph since the last read
-  W_COUNT = 8
+  W_DISP2 = 3,    // largest squared displacement since the last prune (bits)
+  W_PRUNES = 8,   // prunes inside the graph since the last read
+  W_COUNT = 10
 };
 
 // FP64 forces of the last compute, caller order, into e->mdF (3n).
@@ -817,24 +835,56 @@ int md_stage1(mdbas_nb_engine *e, cudaStream_t s) {
   return MDBAS_NB_OK;
 }
 
+bool md_prune_on(const mdbas_nb_engine *e) {
+  return e->cfg.precision == 1 && e->mdPruneBuf > 0.;
+}
+
 int md_max_disp(mdbas_nb_engine *e, cudaStream_t s) {
   const int n = e->n;
   long long *word = e->mdWord.as<long long>();
   const double *xb = e->mdXb.as<double>();
+  const double *xp = md_prune_on(e) ? e->mdXp.as<double>() : nullptr;
   MDB_CUDA(cudaMemsetAsync(word + W_DISP, 0, sizeof(long long), s));
+  MDB_CUDA(cudaMemsetAsync(word + W_DISP2, 0, sizeof(long long), s));
   MDB_LAUNCH(k_max_disp, grid_for(n, 256), 256, 0, s, n, BOXES(e), e->x.as<double>(),
-             e->y.as<double>(), e->z.as<double>(), xb, xb + n, xb + 2 * (size_t)n,
-             reinterpret_cast<unsigned long long *>(word + W_DISP));
+             e->y.as<double>(), e->z.as<double>(), xb, xb + n, xb + 2 * (size_t)n, xp,
+             xp ? xp + n : nullptr, xp ? xp + 2 * (size_t)n : nullptr,
+             reinterpret_cast<unsigned long long *>(word + W_DISP),
+             reinterpret_cast<unsigned long long *>(word + W_DISP2));
   return MDBAS_NB_OK;
 }
 
-// Nonbonded forces of the cluster form with no host interaction: refresh the
-// float4 layout, evaluate, convert to caller order.
+// Inner radius of the pruned list: the cut-off plus the prune buffer, with the
+// list radius's FP32 margin.
+float md_rin2(const mdbas_nb_engine *e) {
+  const double rin = e->cfg.cutOff + e->mdPruneBuf;
+  return (float)(rin * rin * (1.0 + 1e-5));
+}
+
+// Prune the list at the current (refreshed) layout and save the positions.
+int md_prune(mdbas_nb_engine *e, cudaStream_t s) {
+  MDB_TRY(cluster_prune(e->cl, md_rin2(e), s));
+  const size_t bytes = sizeof(double) * (size_t)e->n;
+  double *xp = e->mdXp.as<double>();
+  MDB_CUDA(cudaMemcpyAsync(xp, e->x.p, bytes, cudaMemcpyDeviceToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(xp + e->n, e->y.p, bytes, cudaMemcpyDeviceToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(xp + 2 * (size_t)e->n, e->z.p, bytes, cudaMemcpyDeviceToDevice, s));
+  return MDBAS_NB_OK;
+}
+
+// Host-driven prune (outside graphs): also switches the pair kernel over.
+int md_prune_sync(mdbas_nb_engine *e) {
+  MD_TRY(md_prune(e, e->stream));
+  e->cl.useInner = true;
+  e->mdPrunes += 1;
+  return MDBAS_NB_OK;
+}
+
+// Nonbonded forces of the cluster form with no host interaction, on the
+// current layout (refreshed by the caller): evaluate, convert to caller order.
 int md_forces_cluster(mdbas_nb_engine *e, cudaStream_t s) {
   ClusterWork &w = e->cl;
   const int n = e->n;
-  MDB_TRY(cluster_refresh(w, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
-                          e->q.as<double>(), sqrt(e->cfg.chargeConst), s));
   MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
   MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
   MDB_TRY(pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
@@ -842,6 +892,11 @@ int md_forces_cluster(mdbas_nb_engine *e, cudaStream_t s) {
                           e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                           e->q.as<double>(), s));
   return md_forces(e, s);
+}
+
+int md_refresh_cluster(mdbas_nb_engine *e, cudaStream_t s) {
+  return cluster_refresh(e->cl, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                         e->q.as<double>(), sqrt(e->cfg.chargeConst), s);
 }
 
 // stage 2: half kick, RATTLE on velocities, kinetic energy (+ Berendsen),
@@ -911,7 +966,7 @@ int md_check_shake(mdbas_nb_engine *e, const int st[2]) {
 
 // --- the graph form ------------------------------------------------------------
 struct CaptureCount {
-  long long main = 0, body = 0;
+  long long main = 0, body = 0, prune = 0;
 };
 
 void md_graph_free(mdbas_nb_engine *e) {
@@ -950,43 +1005,89 @@ int md_capture_rebuild_body(mdbas_nb_engine *e, cudaGraph_t body, long long *cou
   return MDBAS_NB_OK;
 }
 
+// Add an IF node on the capture stream's current dependencies and return its
+// body graph; the stream continues after the node.
+int md_add_if(cudaStream_t cs, cudaGraphConditionalHandle h, cudaGraph_t *body,
+              cudaGraphNode_t *node) {
+  cudaStreamCaptureStatus cst;
+  cudaGraph_t capG = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  MDB_CUDA(cudaGraphAddNode(node, capG, deps, nd, &cp));
+  *body = cp.conditional.phGraph_out[0];
+  return MDBAS_NB_OK;
+}
+
+// The prune body: prune at the refreshed layout, save the positions, count.
+int md_capture_prune_body(mdbas_nb_engine *e, cudaGraph_t body, long long *counter) {
+  cudaStream_t side = e->mdSideStream;
+  MDB_CUDA(cudaStreamBeginCaptureToGraph(side, body, nullptr, nullptr, 0,
+                                         cudaStreamCaptureModeRelaxed));
+  g_launch_counter = counter;
+  int st = md_prune(e, side);
+  if (st == MDBAS_NB_OK) {
+    k_count<<<1, 32, 0, side>>>(e->mdWord.as<long long>() + W_PRUNES);
+    ++(*counter);
+    if (cudaGetLastError() != cudaSuccess) st = MDBAS_NB_ERR_CUDA;
+  }
+  cudaGraph_t out = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(side, &out);
+  if (st != MDBAS_NB_OK) return st;
+  MDB_CUDA(ce);
+  return MDBAS_NB_OK;
+}
+
 int md_capture_steps(mdbas_nb_engine *e, int K, double tauT, double kinTemp0,
                      CaptureCount &cc) {
   cudaStream_t cs = e->mdCapStream;
   long long *word = e->mdWord.as<long long>();
   const double half2 = 0.25 * e->cfg.delr * e->cfg.delr;
+  const double halfIn2 = 0.25 * e->mdPruneBuf * e->mdPruneBuf;
+  const bool prune = md_prune_on(e);
   for (int k = 0; k < K; ++k) {
     g_launch_counter = &cc.main;
     MDB_TRY(md_stage1(e, cs));
-    // the rebuild decision, on the device
+    // the rebuild and prune decisions, on the device
     cudaStreamCaptureStatus cst;
     cudaGraph_t capG = nullptr;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t nd = 0;
-    MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, &deps, &nd));
-    cudaGraphConditionalHandle h;
-    MDB_CUDA(cudaGraphConditionalHandleCreate(&h, capG, 0, cudaGraphCondAssignDefault));
-    if (e->mdListUpdate > 0) {
-      MDB_LAUNCH(k_decide_cadence, 1, 32, 0, cs, h, word + W_STEP, e->mdListUpdate);
-    } else {
-      MDB_TRY(md_max_disp(e, cs));
-      MDB_LAUNCH(k_decide_disp, 1, 32, 0, cs, h,
-                 reinterpret_cast<const unsigned long long *>(word + W_DISP), half2,
-                 word + W_STEP);
-    }
-    MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, &deps, &nd));
-    cudaGraphNodeParams cp = {};
-    cp.type = cudaGraphNodeTypeConditional;
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeIf;
-    cp.conditional.size = 1;
-    cudaGraphNode_t cn;
-    MDB_CUDA(cudaGraphAddNode(&cn, capG, deps, nd, &cp));
+    MDB_CUDA(cudaStreamGetCaptureInfo(cs, &cst, nullptr, &capG, nullptr, nullptr));
+    // (a handle that no conditional node uses makes the graph invalid: the
+    // prune handle exists only with pruning on, else k_decide leaves it alone)
+    cudaGraphConditionalHandle hB, hP;
+    MDB_CUDA(cudaGraphConditionalHandleCreate(&hB, capG, 0, cudaGraphCondAssignDefault));
+    hP = hB;
+    if (prune)
+      MDB_CUDA(cudaGraphConditionalHandleCreate(&hP, capG, 0, cudaGraphCondAssignDefault));
+    if (e->mdListUpdate == 0 || prune) MDB_TRY(md_max_disp(e, cs));
+    MDB_LAUNCH(k_decide, 1, 32, 0, cs, hB, hP,
+               reinterpret_cast<const unsigned long long *>(word + W_DISP),
+               reinterpret_cast<const unsigned long long *>(word + W_DISP2), half2, halfIn2,
+               e->mdListUpdate, prune ? 1 : 0, word + W_STEP);
+    cudaGraph_t body;
+    cudaGraphNode_t node;
+    MDB_TRY(md_add_if(cs, hB, &body, &node));
     long long bodyCount = 0;
-    MDB_TRY(md_capture_rebuild_body(e, cp.conditional.phGraph_out[0], &bodyCount));
+    MDB_TRY(md_capture_rebuild_body(e, body, &bodyCount));
     cc.body = bodyCount;
-    MDB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &cn, 1, cudaStreamSetCaptureDependencies));
+    MDB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1,
+                                                 cudaStreamSetCaptureDependencies));
     g_launch_counter = &cc.main;
+    MDB_TRY(md_refresh_cluster(e, cs));
+    if (prune) {
+      MDB_TRY(md_add_if(cs, hP, &body, &node));
+      long long pruneCount = 0;
+      MDB_TRY(md_capture_prune_body(e, body, &pruneCount));
+      cc.prune = pruneCount;
+      MDB_CUDA(cudaStreamUpdateCaptureDependencies(cs, &node, 1,
+                                                   cudaStreamSetCaptureDependencies));
+      g_launch_counter = &cc.main;
+    }
     MDB_TRY(md_forces_cluster(e, cs));
     MDB_TRY(md_stage2(e, cs, true, tauT, kinTemp0));
     MDB_LAUNCH(k_md_row, 1, 32, 0, cs, e->mdRows.as<long long>() + 4 * (size_t)k,
@@ -1032,6 +1133,7 @@ int md_capture(mdbas_nb_engine *e, int K, double targetTemp, double tauT, double
   e->mdGraphStale = false;
   e->mdGraphMainK = cc.main / K;
   e->mdGraphBodyK = cc.body;
+  e->mdGraphPruneK = cc.prune;
   return MDBAS_NB_OK;
 }
 
@@ -1078,6 +1180,7 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
     MDB_CUDA(cudaMemcpyAsync(word + W_STEP, &step0, sizeof(long long), cudaMemcpyHostToDevice,
                              s));
     MDB_CUDA(cudaMemsetAsync(word + W_BUILDS, 0, sizeof(long long), s));
+    MDB_CUDA(cudaMemsetAsync(word + W_PRUNES, 0, sizeof(long long), s));
     MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), s));
     MD_TRY(md_snapshot(e, false));
     MDB_CUDA(cudaGraphLaunch(e->mdExec, s));
@@ -1087,7 +1190,8 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
     MDB_CUDA(cudaMemcpyAsync(rows.data(), e->mdRows.p, sizeof(long long) * rows.size(),
                              cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaStreamSynchronize(s));
-    e->launches += e->mdGraphMainK * K + e->mdGraphBodyK * w[W_BUILDS];
+    e->launches += e->mdGraphMainK * K + e->mdGraphBodyK * w[W_BUILDS] +
+                   e->mdGraphPruneK * w[W_PRUNES];
     if (sticky & CL_NONFINITE) {
       set_last_status(MDBAS_NB_ERR_NONFINITE, "non-finite positions during dynamics");
       return MDBAS_NB_ERR_NONFINITE;
@@ -1100,6 +1204,10 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
       e->cl.entryCap = (long long)(e->cl.entryCap * 1.5) + 4096;
       e->cl.itemCap = (long long)(e->cl.itemCap * 1.5) + 1024;
       MD_TRY(md_build(e));
+      if (md_prune_on(e)) {
+        MD_TRY(md_refresh_cluster(e, s));
+        MD_TRY(md_prune_sync(e));
+      }
       MD_TRY(md_capture(e, K, targetTemp, tauT, kinTemp0));
       continue;
     }
@@ -1110,6 +1218,7 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
       return MDBAS_NB_ERR_OVERFLOW;
     }
     e->mdRebuilds += w[W_BUILDS];
+    e->mdPrunes += w[W_PRUNES];
     for (int k = 0; k < K; ++k) {
       const long long gstep = step0 + k + 1;
       if (energies && energyEvery > 0 && gstep % energyEvery == 0) {
@@ -1318,8 +1427,11 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   }
   // forces at the initial positions
   LaunchScope ls(e);
+  e->mdPrunes = 0;
+  if (md_prune_on(e)) MD_TRY(e->mdXp.ensure(sizeof(double) * 3 * (size_t)n));
   MD_TRY(md_build(e));
   if (e->cfg.precision == 1) MD_TRY(mdbas_nb_engine_refresh(e));
+  if (md_prune_on(e)) MD_TRY(md_prune_sync(e));
   MD_TRY(mdbas_nb_engine_compute(e));
   MD_TRY(md_forces(e, e->stream));
   MDB_CUDA(cudaStreamSynchronize(s));
@@ -1345,6 +1457,7 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   cudaStream_t s = e->stream;
   long long *word = e->mdWord.as<long long>();
   const double half2 = 0.25 * e->cfg.delr * e->cfg.delr;
+  const double halfIn2 = 0.25 * e->mdPruneBuf * e->mdPruneBuf;
   // kinTemp0 of the Berendsen bath (src/utils.c:555-581)
   const double kinTemp0 = 0.5 * targetTemp * (double)e->mdDegFree * 0.83144621;
   MDB_CUDA(cudaMemsetAsync(word + W_SHAKE, 0, sizeof(long long), s));
@@ -1361,21 +1474,25 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   for (int step = done; step < nSteps; ++step) {
     const long long gstep = e->mdSteps + 1;
     MD_TRY(md_stage1(e, s));
-    // list: fixed cadence or half-skin displacement
-    bool rebuild;
-    if (e->mdListUpdate > 0) {
-      rebuild = (gstep % e->mdListUpdate) == 0;
-    } else {
+    // list: fixed cadence or half-skin displacement; inner list: a rebuild
+    // or half the prune buffer since the last prune (k_decide's rules)
+    const bool prune = md_prune_on(e);
+    double d2 = 0., p2 = 0.;
+    if (e->mdListUpdate == 0 || prune) {
       MD_TRY(md_max_disp(e, s));
-      unsigned long long bits = 0;
-      MDB_CUDA(cudaMemcpyAsync(&bits, word + W_DISP, sizeof(bits), cudaMemcpyDeviceToHost, s));
+      unsigned long long bits[2] = {0, 0};
+      MDB_CUDA(cudaMemcpyAsync(&bits[0], word + W_DISP, sizeof(bits[0]), cudaMemcpyDeviceToHost,
+                               s));
+      MDB_CUDA(cudaMemcpyAsync(&bits[1], word + W_DISP2, sizeof(bits[1]),
+                               cudaMemcpyDeviceToHost, s));
       MDB_CUDA(cudaStreamSynchronize(s));
-      double d2;
-      memcpy(&d2, &bits, sizeof(d2));
-      rebuild = d2 > half2;
+      memcpy(&d2, &bits[0], sizeof(d2));
+      memcpy(&p2, &bits[1], sizeof(p2));
     }
+    const bool rebuild = e->mdListUpdate > 0 ? (gstep % e->mdListUpdate) == 0 : d2 > half2;
     if (rebuild) MD_TRY(md_build(e));
     if (e->cfg.precision == 1) MD_TRY(mdbas_nb_engine_refresh(e));
+    if (prune && (rebuild || p2 > halfIn2)) MD_TRY(md_prune_sync(e));
     MD_TRY(mdbas_nb_engine_compute(e));
     MD_TRY(md_forces(e, s));
     const bool wantE = energies && energyEvery > 0 && (gstep % energyEvery) == 0;
@@ -1401,12 +1518,22 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   return MDBAS_NB_OK;
 }
 
-int mdbas_nb_engine_md_stats(mdbas_nb_engine *e, long long out[4]) {
+int mdbas_nb_engine_md_stats(mdbas_nb_engine *e, long long out[6]) {
   if (!e || !out) return MDBAS_NB_ERR_ARG;
   out[0] = e->mdSteps;
   out[1] = e->mdRebuilds;
   out[2] = e->mdShakeIter;
   out[3] = e->mdNMol;
+  out[4] = e->mdPrunes;
+  out[5] = e->cl.useInner ? 1 : 0;
+  return MDBAS_NB_OK;
+}
+
+int mdbas_nb_engine_md_set_prune(mdbas_nb_engine *e, double buffer) {
+  if (!e || buffer < 0. || buffer > e->cfg.delr) return MDBAS_NB_ERR_ARG;
+  e->mdPruneBuf = buffer;
+  e->mdGraphStale = true;
+  e->mdReady = false;  // md_init sets the lists up for the new setting
   return MDBAS_NB_OK;
 }
 

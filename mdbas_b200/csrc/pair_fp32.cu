@@ -735,23 +735,29 @@ PairConstF make_pair_const(const PairParams &p) {
 int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, cudaStream_t s,
                      int variant) {
   const PairConstF c = make_pair_const(p);
+  // the list the kernel walks: the built list or, during dynamics, its
+  // pruned inner copy
+  DBuf &counters = w.useInner ? w.countersIn : w.counters;
+  DBuf &items = w.useInner ? w.itemsIn : w.items;
+  DBuf &entries = w.useInner ? w.entriesIn : w.entries;
+  DBuf &masks = w.useInner ? w.masksIn : w.masks;
   if (variant == kPairPacked) {
     auto kv = p.vdwSwitch ? k_pair_fp32x2<true> : k_pair_fp32x2<false>;
-    MDB_LAUNCH(kv, grid, block, 0, s, w.counters.as<long long>(), w.items.as<int4>(),
-               w.entries.as<CPairEntry>(), w.masks.as<uint2>(), w.xq.as<float4>(),
+    MDB_LAUNCH(kv, grid, block, 0, s, counters.as<long long>(), items.as<int4>(),
+               entries.as<CPairEntry>(), masks.as<uint2>(), w.xq.as<float4>(),
                w.lj.as<float2>(), w.xp.as<float4>(), w.ljp.as<float4>(), c,
                w.facc.as<long long>(), w.slotCap, w.acc.as<long long>());
     return MDBAS_NB_OK;
   }
   if (variant == kPairDense) {
     if (p.vdwSwitch)
-      MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, w.counters.as<long long>(),
-                 w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+      MDB_LAUNCH(k_pair_fp32<true>, grid, block, 0, s, counters.as<long long>(),
+                 items.as<int4>(), entries.as<CPairEntry>(), masks.as<uint2>(),
                  w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                  w.acc.as<long long>());
     else
-      MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, w.counters.as<long long>(),
-                 w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+      MDB_LAUNCH(k_pair_fp32<false>, grid, block, 0, s, counters.as<long long>(),
+                 items.as<int4>(), entries.as<CPairEntry>(), masks.as<uint2>(),
                  w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                  w.acc.as<long long>());
     return MDBAS_NB_OK;
@@ -772,13 +778,13 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   }
   const int cgrid = grid * block / (kCWarps * 32);
   if (p.vdwSwitch)
-    MDB_LAUNCH(k_pair_fp32c<true>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
-               w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+    MDB_LAUNCH(k_pair_fp32c<true>, cgrid, kCWarps * 32, smem, s, counters.as<long long>(),
+               items.as<int4>(), entries.as<CPairEntry>(), masks.as<uint2>(),
                w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                w.acc.as<long long>());
   else
-    MDB_LAUNCH(k_pair_fp32c<false>, cgrid, kCWarps * 32, smem, s, w.counters.as<long long>(),
-               w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+    MDB_LAUNCH(k_pair_fp32c<false>, cgrid, kCWarps * 32, smem, s, counters.as<long long>(),
+               items.as<int4>(), entries.as<CPairEntry>(), masks.as<uint2>(),
                w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
                w.acc.as<long long>());
   return MDBAS_NB_OK;

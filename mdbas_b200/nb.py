@@ -219,6 +219,7 @@ def lib():
                                          _dp]
     L.mdbas_nb_engine_md_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     L.mdbas_nb_engine_md_set_graph.argtypes = [C.c_void_p, C.c_int]
+    L.mdbas_nb_engine_md_set_prune.argtypes = [C.c_void_p, C.c_double]
     L.mdbas_nb_batch_create.argtypes = [C.POINTER(C.c_void_p), C.POINTER(EngineConfig), C.c_int,
                                         C.POINTER(PBC), _ip]
     L.mdbas_nb_batch_count.argtypes = [C.c_void_p]
@@ -446,10 +447,15 @@ class Engine:
         """Steps per CUDA-graph launch of the mixed-precision dynamics (0 = off)."""
         check(lib().mdbas_nb_engine_md_set_graph(self.h, steps_per_launch), "engine_md_set_graph")
 
+    def md_set_prune(self, buffer: float):
+        """Inner-list buffer (A) of the mixed form's dynamics; 0 disables pruning."""
+        check(lib().mdbas_nb_engine_md_set_prune(self.h, buffer), "engine_md_set_prune")
+
     def md_stats(self):
-        out = (C.c_longlong * 4)()
+        out = (C.c_longlong * 6)()
         check(lib().mdbas_nb_engine_md_stats(self.h, out), "engine_md_stats")
-        return {"steps": out[0], "rebuilds": out[1], "shake_iter": out[2], "molecules": out[3]}
+        return {"steps": out[0], "rebuilds": out[1], "shake_iter": out[2], "molecules": out[3],
+                "prunes": out[4], "pruned_list": bool(out[5])}
 
     def positions(self):
         p = [np.zeros(self.n) for _ in range(3)]

@@ -48,10 +48,12 @@ def _ref_md(sysm, vel, dt, steps, list_update, constraints=None, temp0=0.0, tau_
 
 
 def _gpu_md(sysm, vel, dt, steps, list_update, precision, constraints=None, temp0=0.0,
-            tau_t=0.0, frozen=None, graph=None, exclusions=None):
+            tau_t=0.0, frozen=None, graph=None, exclusions=None, prune=None):
     e = nb.Engine(sysm, precision=precision, frozen=frozen, exclusions=exclusions, **POT)
     if graph is not None:
         e.md_set_graph(graph)
+    if prune is not None:
+        e.md_set_prune(prune)
     e.md_init(sysm.mass, vel, time_step=dt, list_update=list_update, constraints=constraints)
     rows = e.md_run(steps, energy_every=1, target_temp=temp0, tau_t=tau_t)
     out = e.positions(), e.velocities(), rows, e.md_stats(), e.launches()
@@ -281,3 +283,22 @@ def test_md_large_molecule_shake_matches_mdbas(gpu, ref_available):
     assert st["molecules"] == 64
     assert perr < 1e-6
     assert kin_err < 1e-6
+
+
+@pytest.mark.parametrize("graph", [0, 20])
+def test_md_pruned_list_bitwise_equal(gpu, water, graph):
+    """Dynamic pruning (inner list at rc + 0.5 A, re-pruned after half that
+    displacement) drops only cluster pairs whose every pair lies beyond the
+    cut-off, whose contributions are exact zeros: the trajectory equals the
+    unpruned one bit for bit."""
+    vel = (water.vx, water.vy, water.vz)
+    cons = water.water_constraints()
+    ap, av, arows, ast, _ = _gpu_md(water, vel, 0.002, 60, 0, 1, cons, graph=graph, prune=0.5)
+    bp, bv, brows, bst, _ = _gpu_md(water, vel, 0.002, 60, 0, 1, cons, graph=graph, prune=0.0)
+    print(f"pruned: {ast['prunes']} prunes, {ast['rebuilds']} rebuilds")
+    assert ast["pruned_list"] and not bst["pruned_list"]
+    assert ast["prunes"] > ast["rebuilds"]
+    for k in range(3):
+        assert np.array_equal(ap[k], bp[k])
+        assert np.array_equal(av[k], bv[k])
+    assert np.array_equal(arows, brows)
