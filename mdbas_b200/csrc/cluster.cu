@@ -208,6 +208,15 @@ struct SearchBuf {
   uint2 mask[kItemMax];
 };
 
+// Columns within reach of one i cluster, listed for the flat candidate scan.
+constexpr int kSearchCols = 192;
+struct SearchCols {
+  int start[kSearchCols];       // first cluster of the column
+  int count[kSearchCols];       // clusters in the column
+  int code[kSearchCols];        // (sx + 1) | (sy + 1) << 2
+  int prefix[kSearchCols + 1];  // cluster counts before the column
+};
+
 // Flush the first cnt (<= kItemMax) buffered entries as one work item.  Each
 // entry's 64-bit interaction mask is built with two ballots: lane L decides
 // pairs (i = L%8, j = L/8) and (i = L%8, j = L/8 + 4).  Exclusions come from
@@ -217,6 +226,7 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
                            const float4 oif, const float4 xi, const float4 *__restrict__ xq,
                            const float4 *__restrict__ originF,
                            const ClusterGeom &g, int nreal_i, const int (&ps)[kExclRegs], int nps,
+                           int pcLo, int pcHi,
                            int es, int ee, int fi, const int *__restrict__ exclFlat,
                            const int *__restrict__ slotOf, const int *__restrict__ slotAtom,
                            const int *__restrict__ frozen, const double4 *__restrict__ origin,
@@ -245,18 +255,22 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
       okb = okb && (jl + 4 > il);
     }
     const int sa = cj * kClusterSize + jl, sb = sa + 4;
+    // exclusion partners of the i cluster's atoms all lie in clusters
+    // [pcLo, pcHi] (warp-uniform test)
+    if (cj >= pcLo && cj <= pcHi) {
 #pragma unroll
-    for (int r = 0; r < kExclRegs; ++r) {
-      if (r < nps) {
-        oka = oka && (ps[r] != sa);
-        okb = okb && (ps[r] != sb);
+      for (int r = 0; r < kExclRegs; ++r) {
+        if (r < nps) {
+          oka = oka && (ps[r] != sa);
+          okb = okb && (ps[r] != sb);
+        }
       }
-    }
-    if (nps > kExclRegs) {
-      for (int e = es + kExclRegs; e < ee; ++e) {
-        const int p = slotOf[__ldg(exclFlat + e)];
-        oka = oka && (p != sa);
-        okb = okb && (p != sb);
+      if (nps > kExclRegs) {
+        for (int e = es + kExclRegs; e < ee; ++e) {
+          const int p = slotOf[__ldg(exclFlat + e)];
+          oka = oka && (p != sa);
+          okb = okb && (p != sb);
+        }
       }
     }
     if (frozen && fi) {
@@ -319,6 +333,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
          uint2 *__restrict__ masks, int4 *__restrict__ items, long long *__restrict__ counters,
          long long entryCap, long long itemCap) {
   __shared__ SearchBuf bufs[kSearchThreads / 32];
+  __shared__ SearchCols colbufs[kSearchThreads / 32];
   const int lane = threadIdx.x & 31;
   const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (ci >= (*nSlotsDev >> 3)) return;
@@ -345,6 +360,16 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   int ps[kExclRegs];
 #pragma unroll
   for (int r = 0; r < kExclRegs; ++r) ps[r] = (r < nps) ? slotOf[__ldg(exclFlat + es + r)] : -1;
+  // the clusters holding any exclusion partner of the i cluster's atoms
+  int pcLo = 0x7fffffff, pcHi = -1;
+  for (int e = es; e < ee; ++e) {
+    const int pc = (e - es < kExclRegs ? ps[min(e - es, kExclRegs - 1)]
+                                       : slotOf[__ldg(exclFlat + e)]) / kClusterSize;
+    pcLo = min(pcLo, pc);
+    pcHi = max(pcHi, pc);
+  }
+  pcLo = __reduce_min_sync(0xffffffffu, pcLo);
+  pcHi = __reduce_max_sync(0xffffffffu, pcHi);
   const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
   const float4 xi = xq[ci * kClusterSize + (lane & 7)];
 
@@ -357,77 +382,163 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   const float zlo = oif.z - hi.z - rl - hzmax, zhi = oif.z + hi.z + rl + hzmax;
   const bool zm = zlo < -0.5f * Lz;  // the image below can be within reach
   const bool zp = zhi > 0.5f * Lz;   // the image above can be within reach
+  // j origins within reach in z: |z_j + image - z_i| <= rl + h_i + hmax
+  const float zwlo = oif.z - hi.z - rl - hzmax, zwhi = oif.z + hi.z + rl + hzmax;
   int cnt = 0;
   long long cand = 0;
+  SearchCols &C = colbufs[threadIdx.x >> 5];
 
-  for (int dy = -g.Dy; dy <= g.Dy; ++dy) {
-    int jy = cy + dy, sy = 0;
-    if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
-    const float ylo = -0.5f * Ly + jy * wy + sy * Ly, yhi = ylo + wy;
-    const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
-    if (gy > rl) continue;
-    for (int dx = -g.Dx; dx <= g.Dx; ++dx) {
+  // Columns within reach are gathered 32 (dx, dy) offsets at a time into the
+  // warp's column list (first cluster, cluster count, periodic shift); once
+  // the list is nearly full or the offsets run out, the candidate clusters of
+  // all listed columns are tested as one flat index space, 32 per round, so
+  // every lane has work and all loads of a round are independent.
+  const int nx = 2 * g.Dx + 1, ny = 2 * g.Dy + 1, ncomb = nx * ny;
+  int ncol = 0;
+  for (int c0 = 0; c0 < ncomb; c0 += 32) {
+    const int cb = c0 + lane;
+    bool pass = false;
+    int cs = 0, cc = 0, code = 0;
+    if (cb < ncomb) {
+      const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
+      int jy = cy + dy, sy = 0;
+      if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
       int jx = cx + dx, sx = 0;
       if (jx < 0) { jx += g.ncx; sx = -1; } else if (jx >= g.ncx) { jx -= g.ncx; sx = 1; }
+      const float ylo = -0.5f * Ly + jy * wy + sy * Ly, yhi = ylo + wy;
+      const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
       const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
       const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
-      if (gx * gx + gy * gy > g.rlist2) continue;
-      const int col = colRank[colBase + jy * g.ncx + jx];
-      const int cs = colClStart[col], ce = colClStart[col + 1];
-      for (int base = cs; base < ce; base += 32) {
-        const int cj = base + lane;
-        const bool valid = cj < ce;
-        float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
-        float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) {
-          oj = originF[cj];
-          hj = half[cj];
+      if (gx * gx + gy * gy <= g.rlist2) {
+        const int col = colRank[colBase + jy * g.ncx + jx];
+        cs = colClStart[col];
+        cc = colClStart[col + 1];
+        code = (sx + 1) | ((sy + 1) << 2);
+        pass = cc > cs;
+      }
+    }
+    // Per z image within reach, the column's clusters (z-sorted) whose
+    // origin lies within the i box's reach: one listed range each.
+#pragma unroll
+    for (int sz = -1; sz <= 1; ++sz) {
+      int first = 0, n = 0;
+      if (pass && !((sz < 0 && !zm) || (sz > 0 && !zp))) {
+        const float lo = zwlo - sz * Lz, hiz = zwhi - sz * Lz;
+        int a = cs, b = cc;
+        while (a < b) {  // first origin z >= lo
+          const int mid = (a + b) >> 1;
+          if (__ldg(&originF[mid].z) < lo) a = mid + 1; else b = mid;
         }
-        const float fx = oj.x + sx * Lx - oif.x;
-        const float fy = oj.y + sy * Ly - oif.y;
-        const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
-        const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
-        const float dxy = gxx * gxx + gyy * gyy;
-        for (int sz = -1; sz <= 1; ++sz) {
-          if ((sz < 0 && !zm) || (sz > 0 && !zp)) continue;
-          const float fz = oj.z + sz * Lz - oif.z;
-          const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
-          const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
-          const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
-          const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
-          const bool pass = valid && half_ok && (dxy + gzz * gzz <= g.rlist2);
-          cand += valid;
-          const unsigned m = __ballot_sync(0xffffffffu, pass);
-          if (m == 0u) continue;
-          if (pass) {
-            const int pos = cnt + __popc(m & ((1u << lane) - 1u));
-            B.j[pos] = cj;
-            B.sidx[pos] = sidx;
-            B.nreal[pos] = (int)hj.w;
-          }
-          cnt += __popc(m);
+        first = a;
+        b = cc;
+        while (a < b) {  // first origin z > hiz
+          const int mid = (a + b) >> 1;
+          if (__ldg(&originF[mid].z) <= hiz) a = mid + 1; else b = mid;
+        }
+        n = a - first;
+      }
+      const bool has = n > 0;
+      const unsigned pm = __ballot_sync(0xffffffffu, has);
+      if (has) {
+        const int k = ncol + __popc(pm & ((1u << lane) - 1u));
+        C.start[k] = first;
+        C.count[k] = n;
+        C.code[k] = code | ((sz + 1) << 4);
+      }
+      ncol += __popc(pm);
+    }
+    if (ncol <= kSearchCols - 96 && c0 + 32 < ncomb) continue;
+    __syncwarp();
+    // prefix of the listed ranges' cluster counts (kPer ranges per lane)
+    constexpr int kPer = kSearchCols / 32;
+    int v[kPer], tot = 0;
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int k = kPer * lane + r;
+      v[r] = k < ncol ? C.count[k] : 0;
+      tot += v[r];
+    }
+    int incl = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    int run = incl - tot;
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < kPer; ++r) {
+      const int k = kPer * lane + r;
+      if (k <= ncol) C.prefix[k] = run;  // prefix[ncol] = total
+      run += v[r];
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    __syncwarp();
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int t = b0 + lane;
+      const bool valid = t < total;
+      int cj = 0, sx = 0, sy = 0, sz = 0;
+      float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
+      float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (valid) {
+        // the listed column holding flat index t
+        int lo = 0, hi2 = ncol - 1;
+        while (lo < hi2) {
+          const int mid = (lo + hi2 + 1) >> 1;
+          if (C.prefix[mid] <= t) lo = mid; else hi2 = mid - 1;
+        }
+        cj = C.start[lo] + (t - C.prefix[lo]);
+        const int code = C.code[lo];
+        sx = (code & 3) - 1;
+        sy = ((code >> 2) & 3) - 1;
+        sz = ((code >> 4) & 3) - 1;
+        oj = originF[cj];
+        hj = half[cj];
+      }
+      const float fx = oj.x + sx * Lx - oif.x;
+      const float fy = oj.y + sy * Ly - oif.y;
+      const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
+      const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
+      const float dxy = gxx * gxx + gyy * gyy;
+      cand += valid;
+      {
+        const float fz = oj.z + sz * Lz - oif.z;
+        const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
+        const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+        const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
+        const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
+        const bool pass = valid && half_ok && (dxy + gzz * gzz <= g.rlist2);
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        if (pass) {
+          const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+          B.j[pos] = cj;
+          B.sidx[pos] = sidx;
+          B.nreal[pos] = (int)hj.w;
+        }
+        cnt += __popc(m);
+        __syncwarp();
+        if (cnt >= kItemMax) {
+          flush_item(B, kItemMax, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps,
+                     pcLo, pcHi, es, ee, fi, exclFlat, slotOf, slotAtom, frozen, origin, entries,
+                     masks, items, counters, entryCap, itemCap);
           __syncwarp();
-          if (cnt >= kItemMax) {
-            flush_item(B, kItemMax, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, es,
-                       ee, fi, exclFlat,
-                       slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
-                       entryCap, itemCap);
-            __syncwarp();
-            const int rem = cnt - kItemMax;
-            if (lane < rem) {
-              B.j[lane] = B.j[kItemMax + lane];
-              B.sidx[lane] = B.sidx[kItemMax + lane];
-              B.nreal[lane] = B.nreal[kItemMax + lane];
-            }
-            cnt = rem;
-            __syncwarp();
+          const int rem = cnt - kItemMax;
+          if (lane < rem) {
+            B.j[lane] = B.j[kItemMax + lane];
+            B.sidx[lane] = B.sidx[kItemMax + lane];
+            B.nreal[lane] = B.nreal[kItemMax + lane];
           }
+          cnt = rem;
+          __syncwarp();
         }
       }
     }
+    ncol = 0;
+    __syncwarp();
   }
   if (cnt > 0)
-    flush_item(B, cnt, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, es, ee, fi,
+    flush_item(B, cnt, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, pcLo, pcHi, es,
+               ee, fi,
                exclFlat, slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
                entryCap, itemCap);
 #pragma unroll
