@@ -119,7 +119,19 @@ __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
   for (int p = ps + (e - s) + threadIdx.x; p < pe; p += blockDim.x) slotAtom[p] = -1;
 }
 
-// One thread per cluster: FP64 origin and half extents, slot data.
+// One thread per slot, 8 consecutive lanes per cluster: FP64 origin and half
+// extents (min/max over the cluster's lanes by shuffles), slot data.
+__device__ __forceinline__ double grp_min8(double v) {
+#pragma unroll
+  for (int o = 1; o < kClusterSize; o <<= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+__device__ __forceinline__ double grp_max8(double v) {
+#pragma unroll
+  for (int o = 1; o < kClusterSize; o <<= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
 __global__ void k_clusters(const int *__restrict__ nSlotsDev,
                            const ClusterGeom *__restrict__ geoms,
                            const int *__restrict__ atomRep, int *__restrict__ clusterRep,
@@ -134,69 +146,68 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
                            float *__restrict__ xp, float *__restrict__ ljp,
                            int *__restrict__ slotOf, int *__restrict__ clusterXY,
                            int *__restrict__ hmaxBits) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= (*nSlotsDev >> 3)) return;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;  // slot
+  const int c = t / kClusterSize, k = t % kClusterSize;
+  // every lane takes part in the shuffles; lanes past the last cluster only
+  // do that (8-lane groups are whole clusters: blockDim is a multiple of 32)
+  const bool active = c < (*nSlotsDev >> 3);
   // a cluster's first slot always holds an atom (columns are padded at the end)
-  const int rep = atomRep ? atomRep[slotAtom[c * kClusterSize]] : 0;
-  if (clusterRep) clusterRep[c] = rep;
+  const int a0 = active ? slotAtom[c * kClusterSize] : 0;
+  const int rep = (active && atomRep) ? atomRep[a0] : 0;
   const ClusterGeom &g = geoms[rep];
-  hmaxBits += 4 * rep;
-  const double ilx = 1.0 / g.Lx, ily = 1.0 / g.Ly, ilz = 1.0 / g.Lz;
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  double px[kClusterSize], py[kClusterSize], pz[kClusterSize];
-  int atoms[kClusterSize];
-#pragma unroll
-  for (int k = 0; k < kClusterSize; ++k) {
-    const int a = slotAtom[c * kClusterSize + k];
-    atoms[k] = a;
-    if (a >= 0) {
-      px[k] = wrap_pos(x[a], g.Lx, ilx);
-      py[k] = wrap_pos(y[a], g.Ly, ily);
-      pz[k] = wrap_pos(z[a], g.Lz, ilz);
-      lo[0] = fmin(lo[0], px[k]); hi[0] = fmax(hi[0], px[k]);
-      lo[1] = fmin(lo[1], py[k]); hi[1] = fmax(hi[1], py[k]);
-      lo[2] = fmin(lo[2], pz[k]); hi[2] = fmax(hi[2], pz[k]);
-    }
+  const int a = active ? slotAtom[t] : -1;
+  double px = 0., py = 0., pz = 0.;
+  double lx = 1e300, ly = 1e300, lz = 1e300, hx = -1e300, hy = -1e300, hz = -1e300;
+  if (a >= 0) {
+    px = wrap_pos(x[a], g.Lx, 1.0 / g.Lx);
+    py = wrap_pos(y[a], g.Ly, 1.0 / g.Ly);
+    pz = wrap_pos(z[a], g.Lz, 1.0 / g.Lz);
+    lx = hx = px;
+    ly = hy = py;
+    lz = hz = pz;
   }
-  const double ox = 0.5 * (lo[0] + hi[0]), oy = 0.5 * (lo[1] + hi[1]), oz = 0.5 * (lo[2] + hi[2]);
-  int nreal = 0;
-#pragma unroll
-  for (int k = 0; k < kClusterSize; ++k) nreal += atoms[k] >= 0;
-  origin[c] = make_double4(ox, oy, oz, 0.0);
-  originF[c] = make_float4((float)ox, (float)oy, (float)oz, (float)nreal);
-  // Half extents rounded up so that the FP32 box always contains its atoms;
-  // w holds the number of real (non-padding) atoms.
-  half[c] = make_float4(__double2float_ru(0.5 * (hi[0] - lo[0]) * (1.0 + 1e-6) + 1e-6),
-                        __double2float_ru(0.5 * (hi[1] - lo[1]) * (1.0 + 1e-6) + 1e-6),
-                        __double2float_ru(0.5 * (hi[2] - lo[2]) * (1.0 + 1e-6) + 1e-6),
-                        (float)nreal);
-  atomicMax(hmaxBits + 0, __float_as_int(half[c].x));
-  atomicMax(hmaxBits + 1, __float_as_int(half[c].y));
-  atomicMax(hmaxBits + 2, __float_as_int(half[c].z));
-  clusterXY[c] = colXY[atomCol[atoms[0]]];
-#pragma unroll
-  for (int k = 0; k < kClusterSize; ++k) {
-    const int s = c * kClusterSize + k;
-    const int a = atoms[k];
-    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    float2 l = make_float2(0.f, 0.f);
-    if (a >= 0) {
-      v = make_float4((float)(px[k] - ox), (float)(py[k] - oy), (float)(pz[k] - oz),
-                      (float)(q[a] * sqrtC));
-      l = make_float2((float)(2.0 * eps[a]), (float)sig[a]);
-      slotOf[a] = s;
-    }
-    xq[s] = v;
-    lj[s] = l;
-    float *p = xp + (size_t)(c * 4 + (k & 3)) * 8 + (k >> 2);
-    p[0] = v.x;
-    p[2] = v.y;
-    p[4] = v.z;
-    p[6] = v.w;
-    float *m = ljp + (size_t)(c * 4 + (k & 3)) * 4 + (k >> 2);
-    m[0] = l.x;
-    m[2] = l.y;
+  lx = grp_min8(lx);
+  ly = grp_min8(ly);
+  lz = grp_min8(lz);
+  hx = grp_max8(hx);
+  hy = grp_max8(hy);
+  hz = grp_max8(hz);
+  const int nreal = __popc(__ballot_sync(0xffffffffu, a >= 0) >> (threadIdx.x & 24) & 0xffu);
+  const double ox = 0.5 * (lx + hx), oy = 0.5 * (ly + hy), oz = 0.5 * (lz + hz);
+  if (!active) return;
+  if (k == 0) {
+    if (clusterRep) clusterRep[c] = rep;
+    origin[c] = make_double4(ox, oy, oz, 0.0);
+    originF[c] = make_float4((float)ox, (float)oy, (float)oz, (float)nreal);
+    // Half extents rounded up so that the FP32 box always contains its
+    // atoms; w holds the number of real (non-padding) atoms.
+    const float4 h = make_float4(__double2float_ru(0.5 * (hx - lx) * (1.0 + 1e-6) + 1e-6),
+                                 __double2float_ru(0.5 * (hy - ly) * (1.0 + 1e-6) + 1e-6),
+                                 __double2float_ru(0.5 * (hz - lz) * (1.0 + 1e-6) + 1e-6),
+                                 (float)nreal);
+    half[c] = h;
+    atomicMax(hmaxBits + 4 * rep + 0, __float_as_int(h.x));
+    atomicMax(hmaxBits + 4 * rep + 1, __float_as_int(h.y));
+    atomicMax(hmaxBits + 4 * rep + 2, __float_as_int(h.z));
+    clusterXY[c] = colXY[atomCol[a0]];
   }
+  float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+  float2 l = make_float2(0.f, 0.f);
+  if (a >= 0) {
+    v = make_float4((float)(px - ox), (float)(py - oy), (float)(pz - oz), (float)(q[a] * sqrtC));
+    l = make_float2((float)(2.0 * eps[a]), (float)sig[a]);
+    slotOf[a] = t;
+  }
+  xq[t] = v;
+  lj[t] = l;
+  float *p = xp + (size_t)(c * 4 + (k & 3)) * 8 + (k >> 2);
+  p[0] = v.x;
+  p[2] = v.y;
+  p[4] = v.z;
+  p[6] = v.w;
+  float *m = ljp + (size_t)(c * 4 + (k & 3)) * 4 + (k >> 2);
+  m[0] = l.x;
+  m[2] = l.y;
 }
 
 constexpr int kExclRegs = 8;  // exclusion partners per atom kept in registers
@@ -817,7 +828,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
   MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
              w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
-  MDB_LAUNCH(k_clusters, grid_for(w.clCap, 128), 128, 0, s, w.nSlotsDev(), gd, w.atomRepDev(),
+  MDB_LAUNCH(k_clusters, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(), gd, w.atomRepDev(),
              nRep > 1 ? w.clusterRep.as<int>() : nullptr, w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x,
              y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
              w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.xp.as<float>(),
