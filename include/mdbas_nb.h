@@ -474,6 +474,29 @@ int mdbas_nb_engine_get_velocities(mdbas_nb_engine *e, double *vx, double *vy, d
                                    int device_ptrs);
 
 /* ------------------------------------------------------------------------ */
+/* 7. Reciprocal space: smooth particle-mesh Ewald on the GPU                 */
+/*    (replaces src/spme.c, which needs FFTW3; include/spme.h:28-40)          */
+/* ------------------------------------------------------------------------ */
+/* MDBas prototypes: init_spme sets ewald->m1max..m3max, mmax (and alpha/tol
+ * as MDBas does); spme_energy adds the reciprocal forces to the caller's
+ * arrays, removes the mean force, fills stress[6] and the virial and returns
+ * the reciprocal energy plus the self and non-neutral terms; spme_free is a
+ * no-op (the device context is per process). */
+void init_spme(CTRL *ctrl, PARAM *param, EWALD *ewald, PBC *box);
+void spme_free(PARAM *param);
+double spme_energy(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
+                   const double z[], double fx[], double fy[], double fz[], const double q[],
+                   double stress[6], double *virEwaldRec);
+/* Status form on host or device arrays: grid m1 x m2 x m3, B-spline order
+ * nbsp (2..16).  Forces minus their mean are added to fx/fy/fz.  out[0] =
+ * energy (reciprocal + self + non-neutral), out[1] = virial, out[2..7] =
+ * stress.  stream: cudaStream_t (NULL = default). */
+int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, int m1, int m2,
+                  int m3, int nbsp, const double *x, const double *y, const double *z,
+                  const double *q, double *fx, double *fy, double *fz, double out[8],
+                  int device_ptrs, void *stream);
+
+/* ------------------------------------------------------------------------ */
 /* 6. Adjoint of the real-space energy (no counterpart in MDBas, whose        */
 /*    numderiv.c gives only finite differences)                              */
 /* ------------------------------------------------------------------------ */

@@ -76,7 +76,7 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         raise RuntimeError(f"nvcc failed:\n{msg}")
     if (not os.path.exists(LIB) or cmds
             or any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs)):
-        link = [cc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lcudart",
+        link = [cc, *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", LIB, *objs, "-lcudart", "-lcufft",
                 "-Xlinker", "-Bsymbolic"]
         if verbose:
             print(" ".join(link))

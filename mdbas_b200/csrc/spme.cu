@@ -1,0 +1,498 @@
+// spme.cu -- smooth particle-mesh Ewald on the GPU: MDBas's init_spme,
+// spme_energy and spme_free (include/spme.h:28-40; src/spme.c) and a
+// status-returning entry point.
+//
+// The algorithm is MDBas's (src/spme.c:357-700): per atom the cardinal
+// B-splines of order nbsp and their derivatives in each dimension
+// (bspgen's recursion), charges spread onto the m1 x m2 x m3 grid, an
+// unnormalised e^{+i} 3-D transform (FFTW_BACKWARD), the influence function
+// B(m) exp(-k^2 / 4 alpha^2) / k^2 inside the reciprocal cut-off with the
+// virial, an e^{-i} transform back (FFTW_FORWARD), force interpolation with
+// the mean force removed, and the energy sum(Q * (theta conv Q)) with the
+// self and non-neutral terms.  The transforms are cuFFT Z2Z plans in the
+// same row-major layout as fftw_plan_dft_3d(m1, m2, m3); spreading, the
+// influence function and the interpolation are the kernels below (FP64,
+// spreading by FP64 atomics).
+#include <cufft.h>
+#include <math.h>
+#include <string.h>
+
+#include <complex>
+#include <vector>
+
+#include "common.cuh"
+
+using namespace mdbas;
+
+namespace {
+
+constexpr int kMaxOrder = 16;  // B-spline orders 2..16
+
+struct SpmeBox {
+  double u1, u2, u3, v1, v2, v3, w1, w2, w3;  // reciprocal vectors
+  double u, v, w;                             // 1 / perpendicular widths
+  double vol;
+};
+
+// B-splines and derivatives of one atom in one dimension (bspgen,
+// src/spme.c:269-355): s is the scaled fractional coordinate.
+__device__ __forceinline__ void bspline(double s, int nbsp, double *bsp, double *bsd) {
+  const double fr = s - trunc(s);
+  for (int k = 0; k < nbsp; ++k) bsp[k] = bsd[k] = 0.;
+  bsd[0] = 1.0;
+  bsd[1] = -1.0;
+  bsp[0] = fr;
+  bsp[1] = 1.0 - fr;
+  for (int k = 2; k < nbsp; ++k) {
+    bsp[k] = 0.0;
+    for (int j = k; j > 0; --j) {
+      if (k == nbsp - 1) bsd[j] = bsp[j] - bsp[j - 1];
+      const double ts = s + (double)j - trunc(s);
+      bsp[j] = (ts * bsp[j] + ((double)(k + 1) - ts) * bsp[j - 1]) / (double)k;
+    }
+    if (k == nbsp - 1) bsd[0] = bsp[0];
+    bsp[0] = fr * bsp[0] / (double)k;
+  }
+}
+
+__device__ __forceinline__ int wrap_index(int i, int m) {
+  if (i >= m) i = 0;
+  if (i < 0) i += m;
+  return i;
+}
+
+// Per atom: grid coordinates, B-splines (bsp[3][nbsp], bsd[3][nbsp]) and the
+// integer grid cell.
+__global__ void k_spme_splines(int n, SpmeBox b, int m1, int m2, int m3, int nbsp,
+                               const double *__restrict__ x, const double *__restrict__ y,
+                               const double *__restrict__ z, double *__restrict__ spl,
+                               int *__restrict__ cell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double s[3] = {(double)m1 * (x[i] * b.u1 + y[i] * b.u2 + z[i] * b.u3 + 0.5),
+                       (double)m2 * (x[i] * b.v1 + y[i] * b.v2 + z[i] * b.v3 + 0.5),
+                       (double)m3 * (x[i] * b.w1 + y[i] * b.w2 + z[i] * b.w3 + 0.5)};
+  double *o = spl + (size_t)i * 6 * nbsp;
+  for (int d = 0; d < 3; ++d) {
+    double bp[kMaxOrder], bd[kMaxOrder];
+    bspline(s[d], nbsp, bp, bd);
+    for (int k = 0; k < nbsp; ++k) {
+      o[d * nbsp + k] = bp[k];
+      o[(3 + d) * nbsp + k] = bd[k];
+    }
+    cell[3 * i + d] = (int)s[d];
+  }
+}
+
+// Charge spreading: one thread per (atom, first-dimension offset).
+__global__ void k_spme_spread(int n, int m1, int m2, int m3, int nbsp,
+                              const double *__restrict__ q, const double *__restrict__ spl,
+                              const int *__restrict__ cell, double *__restrict__ qsp) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= (long long)n * nbsp) return;
+  const int l = (int)(t / nbsp), a = (int)(t % nbsp);
+  const double *o = spl + (size_t)l * 6 * nbsp;
+  const int ii = wrap_index(cell[3 * l] - a, m1);
+  const double qa = q[l] * o[a];
+  for (int bb = 0; bb < nbsp; ++bb) {
+    const int jj = wrap_index(cell[3 * l + 1] - bb, m2);
+    const double qab = qa * o[nbsp + bb];
+    const size_t base = (size_t)m3 * (jj + (size_t)m2 * ii);
+    for (int c = 0; c < nbsp; ++c) {
+      const int kk = wrap_index(cell[3 * l + 2] - c, m3);
+      atomicAdd(qsp + base + kk, qab * o[2 * nbsp + c]);
+    }
+  }
+}
+
+__global__ void k_spme_pack(long long mm, const double *__restrict__ qsp,
+                            cufftDoubleComplex *__restrict__ ft) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < mm) ft[t] = make_cuDoubleComplex(qsp[t], 0.0);
+}
+
+__device__ __forceinline__ void block_add(double v, double *out) {
+  __shared__ double red[32];
+  v = warp_sum_d(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+    v = warp_sum_d(v);
+    if (lane == 0) atomicAdd(out, v);
+  }
+  __syncthreads();
+}
+
+// Influence function and virial (src/spme.c:460-530); stress[6] += ...
+__global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralpha2, double rc2,
+                                 const double *__restrict__ bmod,  // m1 + m2 + m3
+                                 cufftDoubleComplex *__restrict__ ft, double *__restrict__ stress) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long mm = (long long)m1 * m2 * m3;
+  double s[6] = {0., 0., 0., 0., 0., 0.};
+  if (t < mm) {
+    const int k = (int)(t % m3), j = (int)((t / m3) % m2), i = (int)(t / ((long long)m3 * m2));
+    const int ii = i > m1 / 2 ? i - m1 : i, jj = j > m2 / 2 ? j - m2 : j,
+              kk = k > m3 / 2 ? k - m3 : k;
+    const double tw = 6.283185307179586;
+    const double ti = tw * (double)ii, tj = tw * (double)jj, tk = tw * (double)kk;
+    const double rmx = ti * b.u1 + tj * b.v1 + tk * b.w1;
+    const double rmy = ti * b.u2 + tj * b.v2 + tk * b.w2;
+    const double rmz = ti * b.u3 + tj * b.v3 + tk * b.w3;
+    const double rm = rmx * rmx + rmy * rmy + rmz * rmz;
+    const double bm = bmod[i] * bmod[m1 + j] * bmod[m1 + m2 + k];
+    cufftDoubleComplex f = ft[t];
+    if (rm > 2.220446049250313e-16 && rm <= rc2) {
+      const double rrm = 1.0 / rm;
+      const double a = bm * exp(ralpha2 * rm) * rrm;
+      const cufftDoubleComplex cam = make_cuDoubleComplex(a * f.x, a * f.y);
+      // creal(cam * conj(f)) = a |f|^2
+      const double vam = 2.0 * (rrm - ralpha2) * (cam.x * f.x + cam.y * f.y);
+      s[0] = -vam * rmx * rmx;
+      s[1] = -vam * rmx * rmy;
+      s[2] = -vam * rmx * rmz;
+      s[3] = -vam * rmy * rmy;
+      s[4] = -vam * rmy * rmz;
+      s[5] = -vam * rmz * rmz;
+      f = cam;
+    } else {
+      f = make_cuDoubleComplex(0.0, 0.0);
+    }
+    ft[t] = f;
+  }
+  for (int c = 0; c < 6; ++c) block_add(s[c], stress + c);
+}
+
+// Force interpolation (src/spme.c:532-575) into fr[3][n]; sums for the mean.
+__global__ void k_spme_forces(int n, int m1, int m2, int m3, int nbsp, SpmeBox b, double fact1,
+                              const double *__restrict__ q, const double *__restrict__ spl,
+                              const int *__restrict__ cell,
+                              const cufftDoubleComplex *__restrict__ ft, double *__restrict__ fr,
+                              double *__restrict__ fsum) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  double fx = 0., fy = 0., fz = 0.;
+  if (l < n) {
+    const double *o = spl + (size_t)l * 6 * nbsp;
+    const double *b1 = o, *b2 = o + nbsp, *b3 = o + 2 * nbsp;
+    const double *d1 = o + 3 * nbsp, *d2 = o + 4 * nbsp, *d3 = o + 5 * nbsp;
+    const double ql = q[l];
+    for (int a = 0; a < nbsp; ++a) {
+      const int ii = wrap_index(cell[3 * l] - a, m1);
+      for (int bb = 0; bb < nbsp; ++bb) {
+        const int jj = wrap_index(cell[3 * l + 1] - bb, m2);
+        const size_t base = (size_t)m3 * (jj + (size_t)m2 * ii);
+        for (int c = 0; c < nbsp; ++c) {
+          const int kk = wrap_index(cell[3 * l + 2] - c, m3);
+          const double qt = ft[base + kk].x;
+          const double fbx = qt * d1[a] * b2[bb] * b3[c] * (double)m1;
+          const double fby = qt * b1[a] * d2[bb] * b3[c] * (double)m2;
+          const double fbz = qt * b1[a] * b2[bb] * d3[c] * (double)m3;
+          fx += fact1 * ql * (fbx * b.u1 + fby * b.v1 + fbz * b.w1);
+          fy += fact1 * ql * (fbx * b.u2 + fby * b.v2 + fbz * b.w2);
+          fz += fact1 * ql * (fbx * b.u3 + fby * b.v3 + fbz * b.w3);
+        }
+      }
+    }
+    fr[l] = fx;
+    fr[n + l] = fy;
+    fr[2 * (size_t)n + l] = fz;
+  }
+  block_add(fx, fsum);
+  block_add(fy, fsum + 1);
+  block_add(fz, fsum + 2);
+}
+
+// sum over the grid of Re(theta conv Q) * Q
+__global__ void k_spme_energy(long long mm, const cufftDoubleComplex *__restrict__ ft,
+                              const double *__restrict__ qsp, double *__restrict__ out) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  block_add(t < mm ? ft[t].x * qsp[t] : 0.0, out);
+}
+
+// f += fr - mean (device arrays)
+__global__ void k_spme_add(int n, const double *__restrict__ fr, const double *__restrict__ fsum,
+                           double *__restrict__ fx, double *__restrict__ fy,
+                           double *__restrict__ fz) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= n) return;
+  const double inv = 1.0 / (double)n;
+  fx[l] += fr[l] - fsum[0] * inv;
+  fy[l] += fr[n + l] - fsum[1] * inv;
+  fz[l] += fr[2 * (size_t)n + l] - fsum[2] * inv;
+}
+
+// |bspc|^2 of one dimension (epl_cplx/bspcoef, src/spme.c:170-267).
+void bsp_moduli(int m, int nbsp, double *out) {
+  std::vector<double> bsp(nbsp, 0.0);
+  bsp[1] = 1.0;
+  for (int k = 2; k < nbsp; ++k) {
+    bsp[k] = 0.0;
+    for (int j = k; j > 0; --j) bsp[j] = ((double)j * bsp[j] + (double)(k + 1 - j) * bsp[j - 1]) / k;
+  }
+  std::vector<std::complex<double>> epl(m);
+  epl[0] = 1.0;
+  for (int i = 1; i <= m / 2; ++i) {
+    epl[i] = std::exp(std::complex<double>(0.0, 6.283185307179586 * (double)i / (double)m));
+    epl[m - i] = std::conj(epl[i]);
+  }
+  for (int i = 0; i < m; ++i) {
+    std::complex<double> coeff(0.0, 0.0);
+    for (int k = 0; k < nbsp - 1; ++k) coeff += bsp[k + 1] * epl[(size_t)((long long)i * k % m)];
+    const std::complex<double> c = epl[(size_t)((long long)i * (nbsp - 1) % m)] / coeff;
+    out[i] = std::real(c * std::conj(c));
+  }
+}
+
+struct SpmeCtx {
+  int device = -1;
+  int m1 = 0, m2 = 0, m3 = 0, nbsp = 0, n = 0;
+  cufftHandle plan = 0;
+  bool planValid = false;
+  DBuf qsp, ft, bmod, spl, cell, fr, sums, xyzq, fout;
+  ~SpmeCtx() {
+    if (planValid) cufftDestroy(plan);
+  }
+};
+
+SpmeCtx &spme_ctx() {
+  static SpmeCtx c;
+  return c;
+}
+
+SpmeBox make_spme_box(const PBC *p) {
+  SpmeBox b;
+  b.u1 = p->u1; b.u2 = p->u2; b.u3 = p->u3;
+  b.v1 = p->v1; b.v2 = p->v2; b.v3 = p->v3;
+  b.w1 = p->w1; b.w2 = p->w2; b.w3 = p->w3;
+  b.u = p->u; b.v = p->v; b.w = p->w;
+  b.vol = p->vol;
+  return b;
+}
+
+int cufft_check(cufftResult r, const char *what) {
+  if (r == CUFFT_SUCCESS) return MDBAS_NB_OK;
+  char buf[128];
+  snprintf(buf, sizeof(buf), "%s failed (cufftResult %d)", what, (int)r);
+  set_last_status(MDBAS_NB_ERR_CUDA, buf);
+  return MDBAS_NB_ERR_CUDA;
+}
+
+// Grid-size dependent state: plan, moduli, grid buffers.
+int spme_setup(SpmeCtx &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_t s) {
+  int dev = 0;
+  MDB_CUDA(cudaGetDevice(&dev));
+  const long long mm = (long long)m1 * m2 * m3;
+  if (!c.planValid || c.m1 != m1 || c.m2 != m2 || c.m3 != m3 || c.device != dev) {
+    if (c.planValid) cufftDestroy(c.plan);
+    c.planValid = false;
+    MDB_TRY(cufft_check(cufftPlan3d(&c.plan, m1, m2, m3, CUFFT_Z2Z), "cufftPlan3d"));
+    c.planValid = true;
+    c.m1 = m1;
+    c.m2 = m2;
+    c.m3 = m3;
+    c.device = dev;
+    c.nbsp = 0;
+  }
+  MDB_TRY(cufft_check(cufftSetStream(c.plan, s), "cufftSetStream"));
+  if (c.nbsp != nbsp) {
+    std::vector<double> bm(m1 + m2 + m3);
+    bsp_moduli(m1, nbsp, bm.data());
+    bsp_moduli(m2, nbsp, bm.data() + m1);
+    bsp_moduli(m3, nbsp, bm.data() + m1 + m2);
+    MDB_TRY(c.bmod.ensure(sizeof(double) * bm.size()));
+    MDB_CUDA(cudaMemcpy(c.bmod.p, bm.data(), sizeof(double) * bm.size(), cudaMemcpyHostToDevice));
+    c.nbsp = nbsp;
+  }
+  MDB_TRY(c.qsp.ensure(sizeof(double) * mm));
+  MDB_TRY(c.ft.ensure(sizeof(cufftDoubleComplex) * mm));
+  MDB_TRY(c.spl.ensure(sizeof(double) * 6 * (size_t)nbsp * n));
+  MDB_TRY(c.cell.ensure(sizeof(int) * 3 * (size_t)n));
+  MDB_TRY(c.fr.ensure(sizeof(double) * 3 * (size_t)n));
+  MDB_TRY(c.sums.ensure(sizeof(double) * 16));
+  c.n = n;
+  return MDBAS_NB_OK;
+}
+
+// The whole computation on device arrays; forces (minus their mean) are added
+// to fx/fy/fz; out[0] = reciprocal energy + self + non-neutral, out[1] =
+// virial, out[2..7] = stress (MDBas's 6-component layout).
+int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, int m2, int m3,
+             int nbsp, const double *x, const double *y, const double *z, const double *q,
+             double systq, double sumq2, double *fx, double *fy, double *fz, double out[8],
+             cudaStream_t s) {
+  SpmeCtx &c = spme_ctx();
+  MDB_TRY(spme_setup(c, n, m1, m2, m3, nbsp, s));
+  const SpmeBox b = make_spme_box(box);
+  const long long mm = (long long)m1 * m2 * m3;
+  double *sums = c.sums.as<double>();  // 0-5 stress, 6-8 force sums, 9 energy
+  MDB_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * 16, s));
+  MDB_CUDA(cudaMemsetAsync(c.qsp.p, 0, sizeof(double) * mm, s));
+  MDB_LAUNCH(k_spme_splines, grid_for(n, 128), 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z,
+             c.spl.as<double>(), c.cell.as<int>());
+  MDB_LAUNCH(k_spme_spread, grid_for((long long)n * nbsp, 128), 128, 0, s, n, m1, m2, m3, nbsp,
+             q, c.spl.as<double>(), c.cell.as<int>(), c.qsp.as<double>());
+  MDB_LAUNCH(k_spme_pack, grid_for(mm, 256), 256, 0, s, mm, c.qsp.as<double>(),
+             c.ft.as<cufftDoubleComplex>());
+  cufftDoubleComplex *ft = c.ft.as<cufftDoubleComplex>();
+  MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_INVERSE), "cufftExecZ2Z"));
+  const double rvol = 6.283185307179586 / b.vol;
+  const double ralpha2 = -0.25 / (alpha * alpha);
+  double rc = fmin((double)m1 * b.u, (double)m2 * b.v);
+  rc = fmin(rc, (double)m3 * b.w) * 1.05 * 6.283185307179586;
+  MDB_LAUNCH(k_spme_influence, grid_for(mm, 256), 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
+             c.bmod.as<double>(), ft, sums);
+  MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_FORWARD), "cufftExecZ2Z"));
+  MDB_LAUNCH(k_spme_forces, grid_for(n, 128), 128, 0, s, n, m1, m2, m3, nbsp, b,
+             -2.0 * rvol * chargeConst, q, c.spl.as<double>(), c.cell.as<int>(), ft,
+             c.fr.as<double>(), sums + 6);
+  MDB_LAUNCH(k_spme_energy, grid_for(mm, 256), 256, 0, s, mm, ft, c.qsp.as<double>(), sums + 9);
+  MDB_LAUNCH(k_spme_add, grid_for(n, 256), 256, 0, s, n, c.fr.as<double>(), sums + 6, fx, fy,
+             fz);
+  double h[16];
+  MDB_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaStreamSynchronize(s));
+  const double eself = -chargeConst * alpha * sumq2 / kSqrtPi;
+  const double enn = -(0.5 * 3.141592653589793 * chargeConst) *
+                     ((systq / alpha) * (systq / alpha) / b.vol);
+  const double fact1 = rvol * chargeConst;
+  const double erec = h[9];
+  double st[6];
+  st[0] = fact1 * (h[0] + erec) + enn;
+  st[1] = fact1 * h[1];
+  st[2] = fact1 * h[2];
+  st[3] = fact1 * (h[3] + erec) + enn;
+  st[4] = fact1 * h[4];
+  st[5] = fact1 * (h[5] + erec) + enn;
+  out[0] = fact1 * erec + eself + enn;
+  out[1] = -(st[0] + st[3] + st[5]);
+  for (int k = 0; k < 6; ++k) out[2 + k] = st[k];
+  return MDBAS_NB_OK;
+}
+
+int check_grid(int m1, int m2, int m3, int nbsp) {
+  if (m1 <= 0 || m2 <= 0 || m3 <= 0 || nbsp < 2 || nbsp > kMaxOrder) return MDBAS_NB_ERR_ARG;
+  if (nbsp > m1 || nbsp > m2 || nbsp > m3) return MDBAS_NB_ERR_ARG;
+  return MDBAS_NB_OK;
+}
+
+int nint_h(double x) { return (x >= 0.) ? (int)(x + 0.5) : (int)(x - 0.5); }
+
+}  // namespace
+
+extern "C" {
+
+int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, int m1, int m2,
+                  int m3, int nbsp, const double *x, const double *y, const double *z,
+                  const double *q, double *fx, double *fy, double *fz, double out[8],
+                  int device_ptrs, void *stream) {
+  if (nAtom <= 0 || !box || !x || !y || !z || !q || !fx || !fy || !fz || !out || !(alpha > 0.))
+    return MDBAS_NB_ERR_ARG;
+  MDB_TRY(check_grid(m1, m2, m3, nbsp));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  SpmeCtx &c = spme_ctx();
+  double systq = 0., sumq2 = 0.;
+  std::vector<double> hq;
+  const double *qh = q;
+  if (device_ptrs) {
+    hq.resize(nAtom);
+    MDB_CUDA(cudaMemcpy(hq.data(), q, sizeof(double) * nAtom, cudaMemcpyDeviceToHost));
+    qh = hq.data();
+  }
+  for (int i = 0; i < nAtom; ++i) {
+    systq += qh[i];
+    sumq2 += qh[i] * qh[i];
+  }
+  if (device_ptrs)
+    return spme_run(nAtom, box, alpha, chargeConst, m1, m2, m3, nbsp, x, y, z, q, systq, sumq2,
+                    fx, fy, fz, out, s);
+  // host arrays: stage through device buffers; forces are added to the
+  // caller's arrays
+  MDB_TRY(c.xyzq.ensure(sizeof(double) * 4 * (size_t)nAtom));
+  MDB_TRY(c.fout.ensure(sizeof(double) * 3 * (size_t)nAtom));
+  double *d = c.xyzq.as<double>(), *f = c.fout.as<double>();
+  const size_t bytes = sizeof(double) * nAtom;
+  MDB_CUDA(cudaMemcpyAsync(d, x, bytes, cudaMemcpyHostToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(d + nAtom, y, bytes, cudaMemcpyHostToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(d + 2 * (size_t)nAtom, z, bytes, cudaMemcpyHostToDevice, s));
+  MDB_CUDA(cudaMemcpyAsync(d + 3 * (size_t)nAtom, q, bytes, cudaMemcpyHostToDevice, s));
+  MDB_CUDA(cudaMemsetAsync(f, 0, 3 * bytes, s));
+  MDB_TRY(spme_run(nAtom, box, alpha, chargeConst, m1, m2, m3, nbsp, d, d + nAtom,
+                   d + 2 * (size_t)nAtom, d + 3 * (size_t)nAtom, systq, sumq2, f, f + nAtom,
+                   f + 2 * (size_t)nAtom, out, s));
+  std::vector<double> hf(3 * (size_t)nAtom);
+  MDB_CUDA(cudaMemcpy(hf.data(), f, 3 * bytes, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < nAtom; ++i) {
+    fx[i] += hf[i];
+    fy[i] += hf[nAtom + i];
+    fz[i] += hf[2 * (size_t)nAtom + i];
+  }
+  return MDBAS_NB_OK;
+}
+
+// MDBas's init_spme (src/spme.c:32-68): the grid of the reciprocal sum.
+void init_spme(CTRL *ctrl, PARAM *param, EWALD *ewald, PBC *box) {
+  ewald->prec = fmin(fabs(ewald->prec), 0.5);
+  ewald->tol = sqrt(fabs(log(ewald->prec * param->cutOff)));
+  if (!ctrl->keyAlpha)
+    ewald->alpha = sqrt(fabs(log(ewald->prec * param->cutOff * ewald->tol))) / param->cutOff;
+  ewald->tol1 = sqrt(-log(ewald->prec * param->cutOff *
+                          (2.0 * ewald->tol * ewald->alpha) * (2.0 * ewald->tol * ewald->alpha)));
+  if (!ctrl->keyMmax) {
+    ewald->m1max = nint_h(0.25 + box->pa * ewald->alpha * ewald->tol1 / 3.141592653589793);
+    ewald->m2max = nint_h(0.25 + box->pb * ewald->alpha * ewald->tol1 / 3.141592653589793);
+    ewald->m3max = nint_h(0.25 + box->pc * ewald->alpha * ewald->tol1 / 3.141592653589793);
+  }
+  int *m[3] = {&ewald->m1max, &ewald->m2max, &ewald->m3max};
+  for (int d = 0; d < 3; ++d) {
+    int p2 = 1;
+    while (*m[d] > p2 && p2 < 256) p2 *= 2;
+    *m[d] = 2 * p2;
+  }
+  ewald->mmax = ewald->m1max * ewald->m2max * ewald->m3max;
+}
+
+void spme_free(PARAM *param) { (void)param; }
+
+// MDBas's spme_energy (src/spme.c:357-700) on the GPU.  As in MDBas the
+// mean over the whole force arrays is removed after the reciprocal forces
+// are added (energy() calls it first, on zeroed arrays).
+double spme_energy(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
+                   const double z[], double fx[], double fy[], double fz[], const double q[],
+                   double stress[6], double *virEwaldRec) {
+  const int n = param->nAtom;
+  std::vector<double> rx(n, 0.), ry(n, 0.), rz(n, 0.);
+  double out[8];
+  const int st = mdbas_nb_spme(n, box, ewald->alpha, param->chargeConst, ewald->m1max,
+                               ewald->m2max, ewald->m3max, ewald->nbsp, x, y, z, q, rx.data(),
+                               ry.data(), rz.data(), out, 0, nullptr);
+  if (st != MDBAS_NB_OK) {
+    fprintf(stderr, "spme_energy (GPU): %s: %s\n", mdbas_nb_status_string(st),
+            mdbas_nb_last_message());
+    exit(1);
+  }
+  double mx = 0., my = 0., mz = 0.;
+  for (int i = 0; i < n; ++i) {
+    fx[i] += rx[i];
+    fy[i] += ry[i];
+    fz[i] += rz[i];
+    mx += fx[i];
+    my += fy[i];
+    mz += fz[i];
+  }
+  // rx had its own mean removed; MDBas removes the mean of the whole array
+  mx /= (double)n;
+  my /= (double)n;
+  mz /= (double)n;
+  for (int i = 0; i < n; ++i) {
+    fx[i] -= mx;
+    fy[i] -= my;
+    fz[i] -= mz;
+  }
+  for (int k = 0; k < 6; ++k) stress[k] = out[2 + k];
+  *virEwaldRec = out[1];
+  return out[0];
+}
+
+}  // extern "C"

@@ -225,6 +225,9 @@ def lib():
     L.mdbas_nb_batch_count.argtypes = [C.c_void_p]
     L.mdbas_nb_engine_autotune.argtypes = [C.c_void_p, C.POINTER(C.c_int)]
     L.mdbas_nb_engine_adjoint.argtypes = [C.c_void_p] + [C.c_void_p] * 12 + [C.c_int]
+    L.mdbas_nb_spme.argtypes = [C.c_int, C.POINTER(PBC), C.c_double, C.c_double, C.c_int,
+                                C.c_int, C.c_int, C.c_int] + [C.c_void_p] * 7 + [
+                                    C.POINTER(C.c_double), C.c_int, C.c_void_p]
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
@@ -247,6 +250,23 @@ def check(st: int, where: str) -> None:
 
 def _ptr(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def spme(system, alpha=0.34, grid=(32, 32, 32), nbsp=8, chargeConst=None, cell=None,
+         box_type: int = CUBIC):
+    """Reciprocal-space Ewald by SPME on the GPU (host arrays): (energy incl.
+    self and non-neutral terms, fx, fy, fz, virial)."""
+    from .systems import CHARGE_CONST
+    pbc = make_pbc(system.cell() if cell is None else cell, box_type)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (system.x, system.y, system.z,
+                                                               system.q)]
+    f = [np.zeros(system.n) for _ in range(3)]
+    out = (C.c_double * 8)()
+    check(lib().mdbas_nb_spme(system.n, C.byref(pbc), alpha,
+                              CHARGE_CONST if chargeConst is None else chargeConst, *grid, nbsp,
+                              *(_ptr(a) for a in arrs), *(_ptr(a) for a in f), out, 0, None),
+          "spme")
+    return out[0], f[0], f[1], f[2], out[1]
 
 
 class Engine:

@@ -246,6 +246,8 @@ class Reference:
                                         C.c_double, C.c_int, C.c_double, C.c_double]
             lib.ref_md_run.argtypes = [C.c_void_p, C.c_int, _dp]
             lib.ref_get_velocities.argtypes = [C.c_void_p, _dp, _dp, _dp]
+            lib.ref_ewald_rec.argtypes = [C.c_void_p, C.c_double, C.c_void_p, _dp, _dp, _dp,
+                                          _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
         return cls._lib
@@ -377,6 +379,19 @@ class Reference:
         rows = np.zeros((max(n_steps, 1), 4))
         self.lib().ref_md_run(self.h, n_steps, rows)
         return rows[:n_steps]
+
+    def ewald_rec(self, prec=1e-6, mmax=None):
+        """MDBas's explicit Ewald reciprocal sum (init_ewald + ewald_rec) with the
+        harness alpha: (energy incl. self and non-neutral terms, fx, fy, fz,
+        virial, (m1max, m2max, m3max), k vectors)."""
+        fx, fy, fz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)
+        out = np.zeros(6)
+        mm = None
+        if mmax is not None:
+            self._mm = _i(np.asarray(mmax, dtype=np.int32))
+            mm = self._mm.ctypes.data
+        self.lib().ref_ewald_rec(self.h, prec, mm, fx, fy, fz, out)
+        return (out[0], fx, fy, fz, out[1], tuple(int(v) for v in out[2:5]), int(out[5]))
 
     def velocities(self):
         vx, vy, vz = np.zeros(self.n), np.zeros(self.n), np.zeros(self.n)

@@ -33,6 +33,7 @@
 #include "utils.h"
 #include "init.h"
 #include "spme.h"
+#include "ewald.h"
 #include "integrate.h"
 #include "shake.h"
 
@@ -467,4 +468,40 @@ void ref_get_velocities(const RefSys *s, double *vx, double *vy, double *vz)
   memcpy(vx, s->vx, (size_t)s->param.nAtom * sizeof(double));
   memcpy(vy, s->vy, (size_t)s->param.nAtom * sizeof(double));
   memcpy(vz, s->vz, (size_t)s->param.nAtom * sizeof(double));
+}
+
+/*
+ * MDBas's explicit Ewald reciprocal sum: init_ewald (src/ewald.c:7-72) with
+ * the harness's alpha (keyAlpha) and, when mmax[0] > 0, the given k ranges
+ * (keyMmax), then ewald_rec (src/ewald.c:131-354) on zeroed force arrays
+ * (it rescales them), then ewald_free.  out[0] = energy (reciprocal + self +
+ * non-neutral terms), out[1] = virial, out[2..4] = m1max, m2max, m3max,
+ * out[5] = number of k vectors.
+ */
+void ref_ewald_rec(RefSys *s, double prec, const int mmax[3], double *fx, double *fy,
+                   double *fz, double out[6])
+{
+  double stress[6], vir = 0.;
+  int n = s->param.nAtom;
+  CTRL c = s->ctrl;
+  EWALD ew = s->ewald;
+  c.keyAlpha = 1;
+  c.keyMmax = mmax && mmax[0] > 0;
+  ew.prec = prec;
+  if (c.keyMmax) {
+    ew.m1max = mmax[0];
+    ew.m2max = mmax[1];
+    ew.m3max = mmax[2];
+  }
+  init_ewald(&c, &s->param, &ew, &s->box);
+  memset(fx, 0, (size_t)n * sizeof(double));
+  memset(fy, 0, (size_t)n * sizeof(double));
+  memset(fz, 0, (size_t)n * sizeof(double));
+  out[0] = ewald_rec(&s->param, &ew, &s->box, s->x, s->y, s->z, fx, fy, fz, s->q, stress, &vir);
+  out[1] = vir;
+  out[2] = ew.m1max;
+  out[3] = ew.m2max;
+  out[4] = ew.m3max;
+  out[5] = ew.mmax;
+  ewald_free(&ew);
 }
