@@ -204,7 +204,8 @@ void init_energy_ptrs(CTRL *ctrl);
 
 /* Replaces energy() (include/energy.h:30-37, src/energy.c:103-205): zeroes
  * forces, energies and the stress tensor, evaluates the nonbonded terms on the
- * GPU, then MDBas's own bonded routines and freeze_atoms (weak references). */
+ * GPU, then the bonded terms on the GPU (section 8) and MDBas's freeze_atoms
+ * (weak reference). */
 void energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, NEIGH *neigh,
             BOND bond[], BOND ub[], ANGLE angle[], DIHE dihe[], DIHE impr[],
             const double x[], const double y[], const double z[],
@@ -443,7 +444,8 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
  * targetTemp (K) after the second half kick (vv_nvt_b); tauT <= 0 is NVE.
  * Every energyEvery steps (if energies != NULL) a row {step, potential,
  * kinetic, total} (internal units; potential = the nonbonded real-space
- * terms plus the Ewald self term) is appended to energies.  Returns
+ * terms plus the Ewald self term plus the bonded terms of
+ * mdbas_nb_engine_set_bonded) is appended to energies.  Returns
  * MDBAS_NB_ERR_UNSUPPORTED if SHAKE did not converge (CONVERG_SHAKE_ERROR). */
 int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, double targetTemp,
                            double tauT, double *energies);
@@ -495,6 +497,55 @@ int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, i
                   int m3, int nbsp, const double *x, const double *y, const double *z,
                   const double *q, double *fx, double *fy, double *fz, double out[8],
                   int device_ptrs, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* 8. Bonded terms on the GPU (replace src/internal.c:21-620,                 */
+/*    include/internal.h:28-42)                                              */
+/* ------------------------------------------------------------------------ */
+/* MDBas prototypes: add the terms' forces to fx/fy/fz (host arrays) and their
+ * energies (and the bond / Urey-Bradley virials) to ener, as MDBas does:
+ * harmonic or Morse bonds (BHARM, BMORSE), harmonic Urey-Bradley terms,
+ * harmonic angles, cosine or harmonic dihedrals and impropers (DCOS, DHARM).
+ * FP64 with MDBas's operation order; each force component receives the
+ * terms' contributions in MDBas's order (harmonic bonds and Urey-Bradley
+ * terms are bit-identical; terms with exp, acos, atan2, cos or sin agree to
+ * the last place of those functions).  Errors terminate like MDBas. */
+void bond_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND bond[],
+                 const double *x, const double *y, const double *z, double *fx, double *fy,
+                 double *fz);
+void ub_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND ub[], const double *x,
+               const double *y, const double *z, double *fx, double *fy, double *fz);
+void angle_energy(const PARAM *param, ENERGY *ener, const PBC *box, const ANGLE angle[],
+                  const double *x, const double *y, const double *z, double *fx, double *fy,
+                  double *fz);
+void dihedral_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE dihe[],
+                     const double *x, const double *y, const double *z, double *fx, double *fy,
+                     double *fz);
+void improper_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE impr[],
+                     const double *x, const double *y, const double *z, double *fx, double *fy,
+                     double *fz);
+/* Status form of one routine: kind 0 bonds, 1 angles, 2 Urey-Bradley,
+ * 3 dihedrals, 4 impropers (the order of energy(), src/energy.c:167-190);
+ * terms points to nTerms MDBas structs (BOND, ANGLE, BOND, DIHE, DIHE).
+ * Host arrays; forces are added to fx/fy/fz; out[0] = energy, out[1] =
+ * virial (bonds and Urey-Bradley; 0 otherwise).  An atom index outside
+ * [0, nAtom) returns MDBAS_NB_ERR_ARG. */
+int mdbas_nb_bonded(int kind, int nAtom, const PBC *box, int nTerms, const void *terms,
+                    const double *x, const double *y, const double *z, double *fx, double *fy,
+                    double *fz, double out[2]);
+/* Bonded terms of an engine (atom indices in the engine's order; for a batch
+ * the concatenated indices, each term inside one replica).  Dynamics
+ * (section 4) then adds their forces after the nonbonded ones and their
+ * energy to the potential of the energy rows.  Counts of 0 clear a kind. */
+int mdbas_nb_engine_set_bonded(mdbas_nb_engine *e, int nBond, const BOND *bond, int nAngle,
+                               const ANGLE *angle, int nUb, const BOND *ub, int nDihedral,
+                               const DIHE *dihe, int nImproper, const DIHE *impr);
+/* Evaluate the engine's bonded terms at its current positions: forces are
+ * added to fx/fy/fz (host or device; NULL = energies only); out = {bond,
+ * angle, Urey-Bradley, dihedral, improper energies, bond virial, Urey-Bradley
+ * virial}. */
+int mdbas_nb_engine_bonded(mdbas_nb_engine *e, double *fx, double *fy, double *fz,
+                           int device_ptrs, double out[7]);
 
 /* ------------------------------------------------------------------------ */
 /* 6. Adjoint of the real-space energy (no counterpart in MDBas, whose        */

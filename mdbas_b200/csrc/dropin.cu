@@ -4,10 +4,11 @@
 // obj/list.o.  The prototypes are MDBas's (include/energy.h, include/list.h);
 // the caller owns every array, list builders allocate the list arrays with
 // malloc and grow them with realloc exactly as MDBas does, energy routines
-// accumulate into the caller's force arrays.  Routines MDBas keeps in other
-// objects (bonded terms in internal.o, k-space in ewald.o/spme.o,
-// freeze_atoms in utils.o, my_error in errors.o, the outFile global of
-// mdbas.o) are reached through weak references; when a routine the call
+// accumulate into the caller's force arrays.  The bonded terms of
+// internal.o (bond_energy ... improper_energy) are the library's own, on the
+// GPU (bonded.cu).  Routines MDBas keeps in other objects (explicit Ewald in
+// ewald.o, freeze_atoms in utils.o, my_error in errors.o, the outFile global
+// of mdbas.o) are reached through weak references; when a routine the call
 // needs is absent (e.g. the library is loaded into another program), the
 // call fails with MDBAS_NB_ERR_MISSING.
 //
@@ -46,21 +47,6 @@ double ewald_rec(PARAM *param, EWALD *ewald, PBC *box, const double x[], const d
 double spme_energy(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
                    const double z[], double fx[], double fy[], double fz[], const double q[],
                    double stress[6], double *virEwaldRec) __attribute__((weak));
-void bond_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND bond[],
-                 const double *x, const double *y, const double *z, double *fx, double *fy,
-                 double *fz) __attribute__((weak));
-void ub_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND ub[], const double *x,
-               const double *y, const double *z, double *fx, double *fy, double *fz)
-    __attribute__((weak));
-void angle_energy(const PARAM *param, ENERGY *ener, const PBC *box, const ANGLE angle[],
-                  const double *x, const double *y, const double *z, double *fx, double *fy,
-                  double *fz) __attribute__((weak));
-void dihedral_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE dihe[],
-                     const double *x, const double *y, const double *z, double *fx, double *fy,
-                     double *fz) __attribute__((weak));
-void improper_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE impr[],
-                     const double *x, const double *y, const double *z, double *fx, double *fy,
-                     double *fz) __attribute__((weak));
 void freeze_atoms(const PARAM *param, double *vx, double *vy, double *vz, double *fx, double *fy,
                   double *fz, const int *frozen) __attribute__((weak));
 }
@@ -901,23 +887,18 @@ void energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, NEIG
                        neighList14);
   }
   if (param->nBond > 0) {
-    if (!bond_energy) fail(MDBAS_NB_ERR_MISSING, "energy (bond_energy)");
     bond_energy(param, ener, box, bond, x, y, z, fx, fy, fz);
   }
   if (param->nAngle > 0) {
-    if (!angle_energy) fail(MDBAS_NB_ERR_MISSING, "energy (angle_energy)");
     angle_energy(param, ener, box, angle, x, y, z, fx, fy, fz);
   }
   if (param->nUb > 0) {
-    if (!ub_energy) fail(MDBAS_NB_ERR_MISSING, "energy (ub_energy)");
     ub_energy(param, ener, box, ub, x, y, z, fx, fy, fz);
   }
   if (param->nDihedral > 0) {
-    if (!dihedral_energy) fail(MDBAS_NB_ERR_MISSING, "energy (dihedral_energy)");
     dihedral_energy(param, ener, box, dihe, x, y, z, fx, fy, fz);
   }
   if (param->nImproper > 0) {
-    if (!improper_energy) fail(MDBAS_NB_ERR_MISSING, "energy (improper_energy)");
     improper_energy(param, ener, box, impr, x, y, z, fx, fy, fz);
   }
   ener->pot = ener->elec + ener->vdw + ener->bond + ener->ang + ener->ub + ener->dihe +
@@ -927,6 +908,56 @@ void energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, NEIG
     if (!freeze_atoms) fail(MDBAS_NB_ERR_MISSING, "energy (freeze_atoms)");
     freeze_atoms(param, vx, vy, vz, fx, fy, fz, frozen);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Bonded terms (src/internal.c:21-620), MDBas's prototypes (include/internal.h)
+// ---------------------------------------------------------------------------
+namespace {
+// kind as mdbas_nb_bonded numbers them; energies into *e, virial into *vir
+void bonded_dropin(int kind, const PARAM *param, const PBC *box, int nTerms, const void *terms,
+                   const double *x, const double *y, const double *z, double *fx, double *fy,
+                   double *fz, double *e, double *vir, const char *where) {
+  double out[2];
+  DROP_TRY(mdbas_nb_bonded(kind, param->nAtom, box, nTerms, terms, x, y, z, fx, fy, fz, out),
+           where);
+  *e += out[0];
+  if (vir) *vir += out[1];
+}
+}  // namespace
+
+void bond_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND bond[],
+                 const double *x, const double *y, const double *z, double *fx, double *fy,
+                 double *fz) {
+  bonded_dropin(0, param, box, param->nBond, bond, x, y, z, fx, fy, fz, &ener->bond,
+                &ener->virbond, "bond_energy");
+}
+
+void angle_energy(const PARAM *param, ENERGY *ener, const PBC *box, const ANGLE angle[],
+                  const double *x, const double *y, const double *z, double *fx, double *fy,
+                  double *fz) {
+  bonded_dropin(1, param, box, param->nAngle, angle, x, y, z, fx, fy, fz, &ener->ang, nullptr,
+                "angle_energy");
+}
+
+void ub_energy(const PARAM *param, ENERGY *ener, const PBC *box, const BOND ub[], const double *x,
+               const double *y, const double *z, double *fx, double *fy, double *fz) {
+  bonded_dropin(2, param, box, param->nUb, ub, x, y, z, fx, fy, fz, &ener->ub, &ener->virub,
+                "ub_energy");
+}
+
+void dihedral_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE dihe[],
+                     const double *x, const double *y, const double *z, double *fx, double *fy,
+                     double *fz) {
+  bonded_dropin(3, param, box, param->nDihedral, dihe, x, y, z, fx, fy, fz, &ener->dihe, nullptr,
+                "dihedral_energy");
+}
+
+void improper_energy(const PARAM *param, ENERGY *ener, const PBC *box, const DIHE impr[],
+                     const double *x, const double *y, const double *z, double *fx, double *fy,
+                     double *fz) {
+  bonded_dropin(4, param, box, param->nImproper, impr, x, y, z, fx, fy, fz, &ener->impr, nullptr,
+                "improper_energy");
 }
 
 // ---------------------------------------------------------------------------

@@ -3,6 +3,7 @@
 
 #include <vector>
 
+#include "bonded.cuh"
 #include "cluster.cuh"
 #include "list_ref.cuh"
 
@@ -42,6 +43,9 @@ struct mdbas_nb_engine {
   mdbas::DBuf exportBuf, exportCount;
   // adjoint scratch (adjoint.cu)
   mdbas::DBuf adjBuf;
+  // bonded terms (bonded.cu), added to the dynamics forces
+  mdbas::BondedTerms bonded;
+  mdbas::DBuf bondedF;
   // bookkeeping
   bool built = false, computed = false;
   long long launches = 0;

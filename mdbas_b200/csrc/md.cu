@@ -725,13 +725,16 @@ __global__ void k_count(long long *__restrict__ c) {
 
 // Fixed-point energies of the step (elec direct, elec corr, vdw, kinetic) and
 // the accumulated error bits.
+// row = {direct, correction, vdw, kinetic, bonded} in fixed point (2^-24)
 __global__ void k_md_row(long long *__restrict__ row, const long long *__restrict__ acc,
-                         const long long *__restrict__ kin, long long *__restrict__ flags) {
+                         const long long *__restrict__ kin, const long long *__restrict__ bonded,
+                         long long *__restrict__ flags) {
   if (threadIdx.x != 0) return;
   row[0] = acc[ACC_E_DIR];
   row[1] = acc[ACC_E_CORR];
   row[2] = acc[ACC_E_VDW];
   row[3] = kin[0];
+  row[4] = bonded ? bonded[0] : 0;
   flags[0] |= acc[ACC_FLAGS];
 }
 
@@ -765,7 +768,16 @@ enum MdWord {
   W_COUNT = 10
 };
 
-// FP64 forces of the last compute, caller order, into e->mdF (3n).
+constexpr int kRowWords = 5;  // k_md_row's row length
+
+// Fixed-point bonded energy of the last md_forces (null without bonded terms).
+const long long *md_bonded_fix(const mdbas_nb_engine *e) {
+  return e->bonded.nTerms() > 0 ? e->bonded.sums.as<long long>() + BS_FIX : nullptr;
+}
+
+// FP64 forces of the last compute, caller order, into e->mdF (3n); then the
+// bonded terms in MDBas's order (energy(), src/energy.c:167-190) and the
+// frozen atoms (freeze_atoms, src/energy.c:198-201).
 int md_forces(mdbas_nb_engine *e, cudaStream_t s) {
   const int n = e->n;
   double *f = e->mdF.as<double>();
@@ -775,6 +787,9 @@ int md_forces(mdbas_nb_engine *e, cudaStream_t s) {
   } else {
     MDB_TRY(forces_out_launch(e->cl, n, 0, f, f + n, f + 2 * (size_t)n, s));
   }
+  if (e->bonded.nTerms() > 0)
+    MDB_TRY(bonded_eval(e->bonded, BOXES(e), e->x.as<double>(), e->y.as<double>(),
+                        e->z.as<double>(), f, s));
   if (e->hasFrozen)
     MDB_LAUNCH(k_freeze, grid_for(n, 256), 256, 0, s, n, e->frozen.as<int>(), f,
                e->mdV.as<double>());
@@ -1090,8 +1105,8 @@ int md_capture_steps(mdbas_nb_engine *e, int K, double tauT, double kinTemp0,
     }
     MDB_TRY(md_forces_cluster(e, cs));
     MDB_TRY(md_stage2(e, cs, true, tauT, kinTemp0));
-    MDB_LAUNCH(k_md_row, 1, 32, 0, cs, e->mdRows.as<long long>() + 4 * (size_t)k,
-               e->cl.acc.as<long long>(), word + W_KIN, word + W_FLAGS);
+    MDB_LAUNCH(k_md_row, 1, 32, 0, cs, e->mdRows.as<long long>() + kRowWords * (size_t)k,
+               e->cl.acc.as<long long>(), word + W_KIN, md_bonded_fix(e), word + W_FLAGS);
   }
   return MDBAS_NB_OK;
 }
@@ -1102,7 +1117,7 @@ int md_capture(mdbas_nb_engine *e, int K, double targetTemp, double tauT, double
     MDB_CUDA(cudaStreamCreateWithFlags(&e->mdCapStream, cudaStreamNonBlocking));
   if (!e->mdSideStream)
     MDB_CUDA(cudaStreamCreateWithFlags(&e->mdSideStream, cudaStreamNonBlocking));
-  MDB_TRY(e->mdRows.ensure(sizeof(long long) * 4 * (size_t)K));
+  MDB_TRY(e->mdRows.ensure(sizeof(long long) * kRowWords * (size_t)K));
   // everything the capture reads from the host must be final: finish the
   // engine stream's work first
   MDB_CUDA(cudaStreamSynchronize(e->stream));
@@ -1173,7 +1188,7 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
       e->mdGraphTemp != targetTemp)
     MD_TRY(md_capture(e, K, targetTemp, tauT, kinTemp0));
   MD_TRY(e->mdSnap.ensure(sizeof(double) * 12 * (size_t)e->n));
-  std::vector<long long> rows(4 * (size_t)K);
+  std::vector<long long> rows(kRowWords * (size_t)K);
   int growths = 0;
   for (int c = 0; c < chunks;) {
     const long long step0 = e->mdSteps;
@@ -1222,8 +1237,8 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
     for (int k = 0; k < K; ++k) {
       const long long gstep = step0 + k + 1;
       if (energies && energyEvery > 0 && gstep % energyEvery == 0) {
-        const long long *r = &rows[4 * (size_t)k];
-        const double pot = (double)(r[0] + r[1] + r[2]) / kEnergyScale + e->selfE;
+        const long long *r = &rows[kRowWords * (size_t)k];
+        const double pot = (double)(r[0] + r[1] + r[2] + r[4]) / kEnergyScale + e->selfE;
         const double kin = md_kin_row((double)r[3] / kEnergyScale, e->mdDt, tauT, kinTemp0);
         md_write_row(energies, (*outRow)++, gstep, pot, kin);
       }
@@ -1500,9 +1515,13 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
     if (wantE) {
       long long kfix = 0;
       MDB_CUDA(cudaMemcpyAsync(&kfix, word + W_KIN, sizeof(kfix), cudaMemcpyDeviceToHost, s));
+      long long bfix = 0;
+      if (const long long *b = md_bonded_fix(e))
+        MDB_CUDA(cudaMemcpyAsync(&bfix, b, sizeof(bfix), cudaMemcpyDeviceToHost, s));
       mdbas_nb_energies en;
       MD_TRY(mdbas_nb_engine_energies(e, &en));  // synchronises the stream
-      const double pot = en.elec_direct + en.elec_corr + en.elec_self + en.vdw;
+      const double pot = en.elec_direct + en.elec_corr + en.elec_self + en.vdw +
+                         (double)bfix / kEnergyScale;
       md_write_row(energies, outRow++, gstep,
                    pot, md_kin_row((double)kfix / kEnergyScale, e->mdDt, tauT, kinTemp0));
     }

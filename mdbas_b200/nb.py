@@ -24,6 +24,8 @@ LIB_PATH = os.path.join(HERE, "libmdbas_nb.so")
 CUBIC, ORBIC, TCLIN = 1, 2, 3
 NOELEC, FULL, SHIFT1, SHIFT2, SWITCH = 0, 1, 2, 3, 4
 NOVDW, VFULL, VSWITCH = 0, 1, 2
+BHARM, BMORSE = 0, 1          # enum BOND_TYPE
+DCOS, DHARM = 1, 2            # enum DIHE_TYPE
 
 STATUS = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NO_DEVICE", 4: "ERR_ALLOC",
           5: "ERR_CAPACITY", 6: "ERR_BOX", 7: "ERR_LINKCELL", 8: "ERR_EXCL",
@@ -231,6 +233,11 @@ def lib():
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
+    L.mdbas_nb_bonded.argtypes = [C.c_int, C.c_int, C.POINTER(PBC), C.c_int, C.c_void_p] + [
+        C.c_void_p] * 6 + [C.POINTER(C.c_double)]
+    L.mdbas_nb_engine_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
+    L.mdbas_nb_engine_bonded.argtypes = [C.c_void_p] + [C.c_void_p] * 3 + [
+        C.c_int, C.POINTER(C.c_double)]
     _LIB = L
     return L
 
@@ -267,6 +274,59 @@ def spme(system, alpha=0.34, grid=(32, 32, 32), nbsp=8, chargeConst=None, cell=N
                               *(_ptr(a) for a in arrs), *(_ptr(a) for a in f), out, 0, None),
           "spme")
     return out[0], f[0], f[1], f[2], out[1]
+
+
+# Bonded kinds in the order of MDBas's energy() (src/energy.c:167-190).
+BONDED_KINDS = ("bonds", "angles", "ub", "dihedrals", "impropers")
+BONDED_ENERGIES = ("bond", "angle", "ub", "dihedral", "improper", "vir_bond", "vir_ub")
+
+
+def bonded_structs(spec: dict | None) -> list:
+    """MDBas struct arrays (BOND, ANGLE, BOND, DIHE, DIHE) of a bonded spec:
+    spec[kind] = {"atoms": (m, arity) ints, "k": ..., and per kind "type",
+    "r0", "beta" (bonds, ub), "theta0" (angles), "phi0", "mult" (torsions)}
+    with MDBas's units (k in internal units, angles in radians).  Missing
+    kinds give empty arrays."""
+    out = []
+    for kind, cls in zip(BONDED_KINDS, (BOND, ANGLE, BOND, DIHE, DIHE)):
+        t = (spec or {}).get(kind)
+        m = 0 if t is None else len(t["atoms"])
+        arr = (cls * max(1, m))()
+        for i in range(m):
+            at = [int(v) for v in t["atoms"][i]]
+            e = arr[i]
+            e.type = int(t["type"][i]) if "type" in t else (DCOS if cls is DIHE else 0)
+            e.k = float(t["k"][i])
+            if cls is BOND:
+                e.a, e.b = at
+                e.r0 = float(t["r0"][i])
+                e.beta = float(t["beta"][i]) if "beta" in t else 0.0
+            elif cls is ANGLE:
+                e.a, e.b, e.c = at
+                e.theta0 = float(t["theta0"][i])
+            else:
+                e.a, e.b, e.c, e.d = at
+                e.phi0 = float(t["phi0"][i])
+                e.mult = float(t["mult"][i]) if "mult" in t else 1.0
+        out.append((m, arr))
+    return out
+
+
+def bonded(kind: int, system, terms, forces=None, cell=None, box_type: int = CUBIC):
+    """One bonded routine on the GPU (mdbas_nb_bonded): kind 0..4 in
+    BONDED_KINDS order, terms a ctypes struct array (bonded_structs).
+    Returns (energy, virial, fx, fy, fz) with the forces added to `forces`
+    (copies) or to zeros."""
+    pbc = make_pbc(system.cell() if cell is None else cell, box_type)
+    n = system.n
+    pos = [np.ascontiguousarray(a, dtype=np.float64) for a in (system.x, system.y, system.z)]
+    f = ([np.zeros(n) for _ in range(3)] if forces is None
+         else [np.array(a, dtype=np.float64) for a in forces])
+    m = len(terms) if terms is not None else 0
+    out = (C.c_double * 2)()
+    check(lib().mdbas_nb_bonded(kind, n, C.byref(pbc), m, C.cast(terms, C.c_void_p),
+                                *(_ptr(a) for a in pos), *(_ptr(a) for a in f), out), "bonded")
+    return out[0], out[1], f[0], f[1], f[2]
 
 
 class Engine:
@@ -448,6 +508,23 @@ class Engine:
         """Per-replica views of per-atom arrays of a systems.concat batch."""
         o = batch.meta["offsets"]
         return [[a[o[r]:o[r + 1]] for a in arrays] for r in range(len(o) - 1)]
+
+    def set_bonded(self, spec: dict | None):
+        """Bonded terms of the dynamics (see bonded_structs; None clears)."""
+        self._bonded = bonded_structs(spec)
+        args = []
+        for m, arr in self._bonded:
+            args += [m, C.cast(arr, C.c_void_p)]
+        check(lib().mdbas_nb_engine_set_bonded(self.h, *args), "set_bonded")
+
+    def bonded(self, forces=None):
+        """Bonded energies at the current positions (dict of BONDED_ENERGIES)
+        and forces: added to copies of `forces` (3 arrays) or to zeros."""
+        f = ([np.zeros(self.n) for _ in range(3)] if forces is None
+             else [np.array(a, dtype=np.float64) for a in forces])
+        out = (C.c_double * 7)()
+        check(lib().mdbas_nb_engine_bonded(self.h, *(_ptr(a) for a in f), 0, out), "bonded")
+        return dict(zip(BONDED_ENERGIES, out)), f
 
     def adjoint(self, v=None) -> dict:
         """dE/d(q, eps, sig) per atom and, with force weights v = (vx, vy, vz),

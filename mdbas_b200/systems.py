@@ -292,6 +292,82 @@ def config_replicas(count: int = 64, seed: int = 1, temperature: float | None = 
     return concat(parts, name=f"replicas{count}")
 
 
+def flexible_chains(n_side: int = 4, box: float = 26.0, seed: int = 3, jitter: float = 0.05,
+                    temperature: float | None = None) -> System:
+    """n_side^3 flexible six-atom chains with every bonded kind of MDBas.
+
+    Chains are zig-zags (bond 1.53 A, angle 109.5 deg, planar trans) along
+    the box diagonal, centred on the sites of an n_side^3 lattice, each atom
+    jittered by a seeded uniform +-jitter A; charges alternate +-0.2 e, LJ
+    eps 0.1 kcal/mol, sigma 3.2 A, mass 14 amu.  meta["bonded"] holds the
+    bonded spec (mdbas_b200.nb.bonded_structs), in MDBas units (energies in
+    10 J/mol, angles in radians):
+
+    * bonds (k, k+1): harmonic k = 250 kcal/mol/A^2 (E = k/2 dr^2), r0 1.53,
+      except the middle bond (2, 3): Morse, depth 80 kcal/mol, beta 2 /A;
+    * angles (k, k+1, k+2): k = 60 kcal/mol/rad^2, theta0 109.5 deg;
+    * Urey-Bradley (k, k+2): k = 20 kcal/mol/A^2, r0 2.5 A;
+    * dihedrals (k..k+3): cosine, k = 1.5 kcal/mol, mult 3, phi0 0, except
+      the last (2..5): harmonic, k = 4 kcal/mol/rad^2, phi0 pi;
+    * impropers (k+1, k, k+2, k+3), k = 0..2 (planar, phi = 0, in the
+      unjittered chain): harmonic, k = 5 kcal/mol/rad^2, phi0 0.1 rad, except
+      the first: cosine, k = 2 kcal/mol, mult 2, phi0 0.5 rad.
+
+    meta["dihedrals"] lists the dihedral quadruples (for exclusion builders
+    that need them)."""
+    rng = np.random.default_rng(seed)
+    m = n_side ** 3
+    sp = box / n_side
+    idx = np.arange(m)
+    centres = np.stack([(idx % n_side + 0.5) * sp, (idx // n_side % n_side + 0.5) * sp,
+                        (idx // n_side ** 2 + 0.5) * sp], 1) - 0.5 * box
+    u = np.ones(3) / math.sqrt(3.0)
+    w = np.array([1.0, -1.0, 0.0]) / math.sqrt(2.0)
+    half = math.radians(109.5) / 2
+    step_u, step_w = 1.53 * math.sin(half), 1.53 * math.cos(half)
+    local = np.array([(k - 2.5) * step_u * u + (0.5 * step_w if k % 2 else -0.5 * step_w) * w
+                      for k in range(6)])
+    pos = centres[:, None, :] + local[None] + rng.uniform(-jitter, jitter, (m, 6, 3))
+    pos = _wrap(pos.reshape(-1, 3), box)
+    n = 6 * m
+    base = 6 * np.arange(m)
+
+    def terms(offsets):
+        return np.stack([np.stack([base + o for o in offs], 1) for offs in offsets],
+                        1).reshape(-1, len(offsets[0])).astype(np.int32)
+
+    kc = KCAL_TO_IU
+    bonds = terms([(k, k + 1) for k in range(5)])
+    btype = np.tile([0, 0, 1, 0, 0], m)
+    bk = np.where(btype == 1, 80.0 * kc, 250.0 * kc)
+    angles = terms([(k, k + 1, k + 2) for k in range(4)])
+    ub = terms([(k, k + 2) for k in range(4)])
+    dihe = terms([(k, k + 1, k + 2, k + 3) for k in range(3)])
+    dtype = np.tile([1, 1, 2], m)
+    impr = terms([(k + 1, k, k + 2, k + 3) for k in range(3)])
+    itype = np.tile([1, 2, 2], m)
+    spec = {
+        "bonds": dict(atoms=bonds, type=btype, k=bk, r0=np.full(len(bonds), 1.53),
+                      beta=np.where(btype == 1, 2.0, 0.0)),
+        "angles": dict(atoms=angles, k=np.full(len(angles), 60.0 * kc),
+                       theta0=np.full(len(angles), math.radians(109.5))),
+        "ub": dict(atoms=ub, k=np.full(len(ub), 20.0 * kc), r0=np.full(len(ub), 2.5)),
+        "dihedrals": dict(atoms=dihe, type=dtype, k=np.where(dtype == 1, 1.5 * kc, 4.0 * kc),
+                          phi0=np.where(dtype == 1, 0.0, math.pi),
+                          mult=np.where(dtype == 1, 3.0, 1.0)),
+        "impropers": dict(atoms=impr, type=itype, k=np.where(itype == 1, 2.0 * kc, 5.0 * kc),
+                          phi0=np.where(itype == 1, 0.5, 0.1),
+                          mult=np.where(itype == 1, 2.0, 1.0)),
+    }
+    q = np.tile([0.2, -0.2, 0.2, -0.2, 0.2, -0.2], m)
+    s = System("chains", box, pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), q,
+               np.full(n, math.sqrt(0.1 * KCAL_TO_IU)), np.full(n, 1.6), np.full(n, 14.0),
+               bonds, angles, meta={"bonded": spec, "dihedrals": dihe})
+    if temperature is not None:
+        s.vx, s.vy, s.vz = thermal_velocities(s.mass, temperature, seed=seed)
+    return s
+
+
 # Named workloads (sizes of the reference's headline configurations).
 def config_small(seed: int = 1) -> System:
     """3,000-atom water (1,000 molecules) in a 31.0 A box."""

@@ -248,6 +248,8 @@ class Reference:
             lib.ref_get_velocities.argtypes = [C.c_void_p, _dp, _dp, _dp]
             lib.ref_ewald_rec.argtypes = [C.c_void_p, C.c_double, C.c_void_p, _dp, _dp, _dp,
                                           _dp]
+            lib.ref_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
+            lib.ref_bonded_energies.argtypes = [C.c_void_p, _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
         return cls._lib
@@ -276,6 +278,22 @@ class Reference:
         nd = 0 if dihe is None else len(dihe)
         ni = 0 if impr is None else len(impr)
         self.lib().ref_set_torsions(self.h, nd, d, ni, m)
+
+    def set_bonded(self, structs):
+        """Bonded terms with parameters: five (count, ctypes array of MDBas
+        structs) in the order bonds, angles, Urey-Bradley, dihedrals,
+        impropers (ref_set_bonded copies them)."""
+        args = []
+        for m, arr in structs:
+            args += [int(m), C.cast(arr, C.c_void_p)]
+        self.lib().ref_set_bonded(self.h, *args)
+
+    def bonded_energies(self) -> dict:
+        """Bonded energies of the last energy() call."""
+        out = np.zeros(7)
+        self.lib().ref_bonded_energies(self.h, out)
+        return dict(zip(["bond", "angle", "ub", "dihedral", "improper", "vir_bond", "vir_ub"],
+                        out.tolist()))
 
     def list14(self):
         n14 = self.lib().ref_n_pair14(self.h)

@@ -61,8 +61,9 @@ typedef struct {
   NEIGH neigh;
   EWALD ewald;
   ENERGY ener;
-  BOND *bond;
+  BOND *bond, *ub;
   ANGLE *angle;
+  int bondedOn; /* ref_set_bonded: energy() evaluates the bonded terms */
   CONSTRAINT *constList;
   DIHE *dihe, *impr;
   double *x, *y, *z, *q, *eps, *sig, *fx, *fy, *fz, *vx, *vy, *vz;
@@ -170,6 +171,69 @@ void ref_set_torsions(RefSys *s, int nDihedral, const int *dihe, int nImproper, 
   }
   s->param.nDihedral = nDihedral;
   s->param.nImproper = nImproper;
+}
+
+/*
+ * Bonded terms with their parameters (MDBas structs, copied): bonds,
+ * angles, Urey-Bradley, dihedrals, impropers.  They replace the topology of
+ * ref_create / ref_set_torsions (so they also feed the exclusion builders)
+ * and from now on energy() evaluates them (src/energy.c:167-190).
+ */
+static void *dup_terms(const void *src, int n, size_t size)
+{
+  void *p = calloc((size_t)(n > 0 ? n : 1), size);
+  if (n > 0) memcpy(p, src, (size_t)n * size);
+  return p;
+}
+
+void ref_set_bonded(RefSys *s, int nBond, const BOND *bond, int nAngle, const ANGLE *angle,
+                    int nUb, const BOND *ub, int nDihedral, const DIHE *dihe, int nImproper,
+                    const DIHE *impr)
+{
+  free(s->bond);
+  free(s->angle);
+  free(s->ub);
+  free(s->dihe);
+  free(s->impr);
+  s->bond = (BOND *)dup_terms(bond, nBond, sizeof(BOND));
+  s->angle = (ANGLE *)dup_terms(angle, nAngle, sizeof(ANGLE));
+  s->ub = (BOND *)dup_terms(ub, nUb, sizeof(BOND));
+  s->dihe = (DIHE *)dup_terms(dihe, nDihedral, sizeof(DIHE));
+  s->impr = (DIHE *)dup_terms(impr, nImproper, sizeof(DIHE));
+  s->param.nBond = nBond;
+  s->param.nAngle = nAngle;
+  s->param.nUb = nUb;
+  s->param.nDihedral = nDihedral;
+  s->param.nImproper = nImproper;
+  s->bondedOn = 1;
+}
+
+/* Bonded energies of the last energy(): bond, angle, Urey-Bradley,
+ * dihedral, improper, bond virial, Urey-Bradley virial. */
+void ref_bonded_energies(const RefSys *s, double out[7])
+{
+  out[0] = s->ener.bond;
+  out[1] = s->ener.ang;
+  out[2] = s->ener.ub;
+  out[3] = s->ener.dihe;
+  out[4] = s->ener.impr;
+  out[5] = s->ener.virbond;
+  out[6] = s->ener.virub;
+}
+
+/* energy()'s parameters: the bonded counts only once ref_set_bonded gave
+ * the terms' parameters (before that the terms feed the exclusions only). */
+static PARAM energy_param(const RefSys *s)
+{
+  PARAM p = s->param;
+  if (!s->bondedOn) {
+    p.nBond = 0;
+    p.nAngle = 0;
+    p.nUb = 0;
+    p.nDihedral = 0;
+    p.nImproper = 0;
+  }
+  return p;
 }
 
 int ref_n_pair14(const RefSys *s) { return s->neigh.nPair14; }
@@ -298,21 +362,16 @@ void ref_set_positions(RefSys *s, const double *x, const double *y, const double
 }
 
 /*
- * One energy() call (src/energy.c:103) on the current list.  Bonded terms are
- * out of scope, so energy() sees nBond = nAngle = 0.
+ * One energy() call (src/energy.c:103) on the current list.  Bonded terms
+ * count only after ref_set_bonded (else energy() sees nBond = nAngle = 0).
  * out[0..5] = elec, vdw, virelec, virvdw, pot, virpot (internal units).
  */
 void ref_energy(RefSys *s, double *fx, double *fy, double *fz, double out[6])
 {
-  PARAM p = s->param;
-  p.nBond = 0;
-  p.nAngle = 0;
-  p.nUb = 0;
-  p.nDihedral = 0;
-  p.nImproper = 0;
+  PARAM p = energy_param(s);
   s->ctrl.keyEwald = 3;
   init_energy_ptrs(&s->ctrl);
-  energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->bond, s->angle,
+  energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->ub, s->angle,
          s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,
          s->eps, s->sig, s->eps, s->sig, s->frozen, s->neighList, s->neighPair, s->neighOrder,
          s->neighList14, s->exclList, s->exclPair);
@@ -350,7 +409,7 @@ void ref_destroy(RefSys *s)
   if (!s) return;
   free(s->x); free(s->y); free(s->z); free(s->q); free(s->eps); free(s->sig);
   free(s->fx); free(s->fy); free(s->fz); free(s->vx); free(s->vy); free(s->vz);
-  free(s->frozen); free(s->bond); free(s->angle); free(s->constList); free(s->dihe);
+  free(s->frozen); free(s->bond); free(s->ub); free(s->angle); free(s->constList); free(s->dihe);
   free(s->impr);
   free(s->mass); free(s->rmass); free(s->nAtConst);
   if (s->mdInit) {
@@ -374,8 +433,7 @@ void ref_destroy(RefSys *s)
  * src/mdbas.c:244-300 drives it: vv_integrate stage 1 (src/integrate.c:1479,
  * vv_nve/vv_nvt_b with vv_shake_r), makelist on the neigh.update cadence,
  * energy(), vv_integrate stage 2 (vv_shake_v, kinetic, image_update).
- * Bonded terms stay off (nBond = nAngle = 0 in energy(), as in ref_energy);
- * the bonds/angles given to ref_create only feed the exclusion builders.
+ * Bonded terms count as in ref_energy (only after ref_set_bonded).
  * constAtoms holds 2*nConst atom indices, constLen2 the squared lengths.
  * tauT > 0 selects NVT_B (Berendsen) toward temp0, else NVE.
  * Requires ref_makelist first.  MDBas keeps its integrator and SHAKE work
@@ -445,9 +503,8 @@ void ref_md_run(RefSys *s, int nSteps, double *rows)
     makelist(&s->ctrl, &s->param, &s->box, &s->neigh, s->constList, s->bond, s->angle, s->dihe,
              s->impr, s->x, s->y, s->z, s->frozen, &s->neighList, &s->neighPair,
              &s->neighOrder, &s->neighList14, &s->exclList, &s->exclPair);
-    p = s->param;
-    p.nBond = p.nAngle = p.nUb = p.nDihedral = p.nImproper = 0;
-    energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->bond, s->angle,
+    p = energy_param(s);
+    energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->ub, s->angle,
            s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,
            s->eps, s->sig, s->eps, s->sig, s->frozen, s->neighList, s->neighPair, s->neighOrder,
            s->neighList14, s->exclList, s->exclPair);
