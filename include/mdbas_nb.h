@@ -231,8 +231,8 @@ void nonbond14_energy(PARAM *param, ENERGY *ener, PBC *box, NEIGH *neigh,
 
 /* Replaces ewald_energy (include/energy.h:49-53, src/energy.c:450-643):
  * real-space Ewald direct term + switched LJ over the caller's list and the
- * erf exclusion correction on the GPU; keyEwald==1/2 k-space goes to MDBas's
- * own ewald_rec/spme_energy (weak references). */
+ * erf exclusion correction on the GPU; keyEwald==1/2 k-space by ewald_rec
+ * (section 9) / spme_energy (section 7), also on the GPU. */
 void ewald_energy(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *ewald, PBC *box, const double x[],
                   const double y[], const double z[], double fx[], double fy[],
                   double fz[], const double q[], const double eps[], const double sig[],
@@ -497,6 +497,32 @@ int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, i
                   int m3, int nbsp, const double *x, const double *y, const double *z,
                   const double *q, double *fx, double *fy, double *fz, double out[8],
                   int device_ptrs, void *stream);
+
+/* ------------------------------------------------------------------------ */
+/* 9. Explicit reciprocal-space Ewald sum on the GPU (replaces src/ewald.c:   */
+/*    10-354, include/ewald.h)                                               */
+/* ------------------------------------------------------------------------ */
+/* MDBas prototypes: init_ewald sets prec, tol, alpha (unless keyAlpha), tol1,
+ * m1max..m3max (unless keyMmax) and mmax = the number of k-vectors, as MDBas
+ * does (without MDBas's per-atom table allocation); ewald_free is a no-op;
+ * ewald_rec adds the reciprocal forces to fx/fy/fz and then multiplies the
+ * whole arrays by 4 pi C / V as MDBas does (energy() calls it on zeroed
+ * arrays), fills stress[6] and the virial and returns the reciprocal energy
+ * plus the self and non-neutral terms. */
+void init_ewald(CTRL *ctrl, PARAM *param, EWALD *ewald, PBC *box);
+void ewald_free(EWALD *ewald);
+double ewald_rec(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
+                 const double z[], double fx[], double fy[], double fz[], const double q[],
+                 double stress[6], double *virEwaldRec);
+/* Status form on host or device arrays: every k = 2 pi (m1 u + m2 v + m3 w)
+ * with |m_d| <= m{d}max inside MDBas's reciprocal cut-off.  The reciprocal
+ * forces are added to fx/fy/fz.  out[0] = energy (reciprocal + self +
+ * non-neutral), out[1] = virial, out[2..7] = stress.  stream: cudaStream_t
+ * (NULL = default). */
+int mdbas_nb_ewald_rec(int nAtom, const PBC *box, double alpha, double chargeConst, int m1max,
+                       int m2max, int m3max, const double *x, const double *y, const double *z,
+                       const double *q, double *fx, double *fy, double *fz, double out[8],
+                       int device_ptrs, void *stream);
 
 /* ------------------------------------------------------------------------ */
 /* 8. Bonded terms on the GPU (replace src/internal.c:21-620,                 */

@@ -3,8 +3,8 @@
 Every translation unit is compiled with
 ``-gencode arch=compute_100a,code=sm_100a -O3 -lineinfo`` into
 ``mdbas_b200/_build/`` and linked into ``mdbas_b200/libmdbas_nb.so``.
-pair_fp64.cu and bonded.cu are compiled with ``--fmad=false`` so that the
-plain FP64 forms keep MDBas's uncontracted operation order.  Objects are rebuilt when their
+pair_fp64.cu, bonded.cu and ewald_rec.cu are compiled with ``--fmad=false`` so
+that the plain FP64 forms keep MDBas's uncontracted operation order.  Objects are rebuilt when their
 source or any header under csrc/ or include/ is newer.
 """
 from __future__ import annotations
@@ -21,7 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmdbas_nb.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NO_FMAD = {"pair_fp64.cu", "bonded.cu"}
+NO_FMAD = {"pair_fp64.cu", "bonded.cu", "ewald_rec.cu"}
 
 
 def nvcc() -> str:

@@ -5,12 +5,13 @@
 // the caller owns every array, list builders allocate the list arrays with
 // malloc and grow them with realloc exactly as MDBas does, energy routines
 // accumulate into the caller's force arrays.  The bonded terms of
-// internal.o (bond_energy ... improper_energy) are the library's own, on the
-// GPU (bonded.cu).  Routines MDBas keeps in other objects (explicit Ewald in
-// ewald.o, freeze_atoms in utils.o, my_error in errors.o, the outFile global
-// of mdbas.o) are reached through weak references; when a routine the call
-// needs is absent (e.g. the library is loaded into another program), the
-// call fails with MDBAS_NB_ERR_MISSING.
+// internal.o (bond_energy ... improper_energy, bonded.cu) and the k-space
+// sums of ewald.o and spme.o (ewald_rec.cu, spme.cu) are the library's own,
+// on the GPU.  Routines MDBas keeps in other objects (freeze_atoms in
+// utils.o, my_error in errors.o, the outFile global of mdbas.o) are reached
+// through weak references; when a routine the call needs is absent (e.g. the
+// library is loaded into another program), the call fails with
+// MDBAS_NB_ERR_MISSING.
 //
 // Errors: the void drop-ins report like MDBas's my_error (src/errors.c:15)
 // -- through my_error itself when it is linked, with MDBas's error number
@@ -41,12 +42,6 @@ extern "C" {
 extern FILE *outFile __attribute__((weak));
 void my_error(int errorNumber, char file[], int line, int num_optional_args, ...)
     __attribute__((weak));
-double ewald_rec(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
-                 const double z[], double fx[], double fy[], double fz[], const double q[],
-                 double stress[6], double *virEwaldRec) __attribute__((weak));
-double spme_energy(PARAM *param, EWALD *ewald, PBC *box, const double x[], const double y[],
-                   const double z[], double fx[], double fy[], double fz[], const double q[],
-                   double stress[6], double *virEwaldRec) __attribute__((weak));
 void freeze_atoms(const PARAM *param, double *vx, double *vy, double *vz, double *fx, double *fy,
                   double *fz, const int *frozen) __attribute__((weak));
 }
@@ -722,13 +717,10 @@ int mdbas_nb_ewald_energy_status(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *
   if (!ctrl || !param || !ener || !ewald || !box || !x || !fx || !q) return MDBAS_NB_ERR_ARG;
   double eRec = 0., virRec = 0., stress1[6] = {0., 0., 0., 0., 0., 0.};
   // k-space first, as in MDBas: ewald_rec rescales the force arrays.
-  if (ctrl->keyEwald == 1) {
-    if (!ewald_rec) return MDBAS_NB_ERR_MISSING;
+  if (ctrl->keyEwald == 1)
     eRec = ewald_rec(param, ewald, box, x, y, z, fx, fy, fz, q, stress1, &virRec);
-  } else if (ctrl->keyEwald == 2) {
-    if (!spme_energy) return MDBAS_NB_ERR_MISSING;
+  else if (ctrl->keyEwald == 2)
     eRec = spme_energy(param, ewald, box, x, y, z, fx, fy, fz, q, stress1, &virRec);
-  }
   const int vdwSwitch = (g.ptrsSet ? g.vdwType : ctrl->vdwType) == VSWITCH;
   double e[6];
   ST_TRY(real_space(mdbas_nb_get_mode(), param->nAtom, param, ewald->alpha, vdwSwitch, box, x, y,

@@ -437,8 +437,8 @@ void init_spme(CTRL *ctrl, PARAM *param, EWALD *ewald, PBC *box) {
   ewald->tol = sqrt(fabs(log(ewald->prec * param->cutOff)));
   if (!ctrl->keyAlpha)
     ewald->alpha = sqrt(fabs(log(ewald->prec * param->cutOff * ewald->tol))) / param->cutOff;
-  ewald->tol1 = sqrt(-log(ewald->prec * param->cutOff *
-                          (2.0 * ewald->tol * ewald->alpha) * (2.0 * ewald->tol * ewald->alpha)));
+  const double ta = 2.0 * ewald->tol * ewald->alpha;
+  ewald->tol1 = sqrt(-log(ewald->prec * param->cutOff * (ta * ta)));
   if (!ctrl->keyMmax) {
     ewald->m1max = nint_h(0.25 + box->pa * ewald->alpha * ewald->tol1 / 3.141592653589793);
     ewald->m2max = nint_h(0.25 + box->pb * ewald->alpha * ewald->tol1 / 3.141592653589793);

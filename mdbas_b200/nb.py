@@ -233,6 +233,9 @@ def lib():
     for name in ("get_positions", "get_velocities"):
         getattr(L, f"mdbas_nb_engine_{name}").argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                           C.c_void_p, C.c_int]
+    L.mdbas_nb_ewald_rec.argtypes = [C.c_int, C.POINTER(PBC), C.c_double, C.c_double, C.c_int,
+                                     C.c_int, C.c_int] + [C.c_void_p] * 7 + [
+                                         C.POINTER(C.c_double), C.c_int, C.c_void_p]
     L.mdbas_nb_bonded.argtypes = [C.c_int, C.c_int, C.POINTER(PBC), C.c_int, C.c_void_p] + [
         C.c_void_p] * 6 + [C.POINTER(C.c_double)]
     L.mdbas_nb_engine_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
@@ -274,6 +277,25 @@ def spme(system, alpha=0.34, grid=(32, 32, 32), nbsp=8, chargeConst=None, cell=N
                               *(_ptr(a) for a in arrs), *(_ptr(a) for a in f), out, 0, None),
           "spme")
     return out[0], f[0], f[1], f[2], out[1]
+
+
+def ewald_rec(system, alpha=0.34, mmax=(8, 8, 8), chargeConst=None, cell=None,
+              box_type: int = CUBIC, forces=None):
+    """Explicit reciprocal-space Ewald sum on the GPU (host arrays): (energy
+    incl. self and non-neutral terms, fx, fy, fz, virial, stress[6]); the
+    forces are added to copies of `forces` (or to zeros)."""
+    from .systems import CHARGE_CONST
+    pbc = make_pbc(system.cell() if cell is None else cell, box_type)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (system.x, system.y, system.z,
+                                                               system.q)]
+    f = ([np.zeros(system.n) for _ in range(3)] if forces is None
+         else [np.array(a, dtype=np.float64) for a in forces])
+    out = (C.c_double * 8)()
+    check(lib().mdbas_nb_ewald_rec(system.n, C.byref(pbc), alpha,
+                                   CHARGE_CONST if chargeConst is None else chargeConst, *mmax,
+                                   *(_ptr(a) for a in arrs), *(_ptr(a) for a in f), out, 0,
+                                   None), "ewald_rec")
+    return out[0], f[0], f[1], f[2], out[1], list(out[2:8])
 
 
 # Bonded kinds in the order of MDBas's energy() (src/energy.c:167-190).
