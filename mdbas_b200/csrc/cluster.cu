@@ -216,7 +216,9 @@ struct SearchBuf {
   int j[kBufCap];
   int sidx[kBufCap];
   int nreal[kBufCap];
+  float4 sh[kBufCap];                  // FP32 shift: j origin + image - i origin
   uint2 mask[kItemMax];
+  float4 sj[kItemMax * kClusterSize];  // staged j atoms (xq) of the entries
 };
 
 // Columns within reach of one i cluster, listed for the flat candidate scan.
@@ -232,12 +234,14 @@ struct SearchCols {
 // entry's 64-bit interaction mask is built with two ballots: lane L decides
 // pairs (i = L%8, j = L/8) and (i = L%8, j = L/8 + 4).  Exclusions come from
 // the lane's partner slots (registers; a global-memory loop for atoms with
-// more than kExclRegs partners).
+// more than kExclRegs partners), checked only for entries whose j cluster
+// holds a partner of some lane's i atom (pc0/pc1: the clusters of a lane's
+// first two partners; atoms with more partners fall back to the warp's
+// partner-cluster range [pcLo, pcHi]).
 __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double4 oi,
-                           const float4 oif, const float4 xi, const float4 *__restrict__ xq,
-                           const float4 *__restrict__ originF,
+                           const float4 xi, const float4 *__restrict__ xq,
                            const ClusterGeom &g, int nreal_i, const int (&ps)[kExclRegs], int nps,
-                           int pcLo, int pcHi,
+                           int pc0, int pc1, int pcLo, int pcHi,
                            int es, int ee, int fi, const int *__restrict__ exclFlat,
                            const int *__restrict__ slotOf, const int *__restrict__ slotAtom,
                            const int *__restrict__ frozen, const double4 *__restrict__ origin,
@@ -245,6 +249,14 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
                            int4 *__restrict__ items, long long *__restrict__ counters,
                            long long entryCap, long long itemCap) {
   const int il = lane & 7, jl = lane >> 3;
+  // stage every entry's j cluster first: all loads of the flush in flight
+  // together
+#pragma unroll
+  for (int r = 0; r < kClusterSize; ++r) {
+    const int idx = lane + 32 * r, k = idx >> 3;
+    if (k < cnt) B.sj[idx] = xq[B.j[k] * kClusterSize + (idx & 7)];
+  }
+  __syncwarp();
   for (int k = 0; k < cnt; ++k) {
     const int cj = B.j[k];
     const int nrj = B.nreal[k];
@@ -252,13 +264,11 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
     const bool selfzero = (cj == ci) && (sidx == 13);
     // pair distances at build time: only pairs within the list radius are
     // kept (FP32 shift from the FP32 origins; rlist2 carries a 1e-5 margin)
-    const float4 ojf = originF[cj];
-    const float shx = (ojf.x + (sidx % 3 - 1) * (float)g.Lx) - oif.x;
-    const float shy = (ojf.y + ((sidx / 3) % 3 - 1) * (float)g.Ly) - oif.y;
-    const float shz = (ojf.z + (sidx / 9 - 1) * (float)g.Lz) - oif.z;
-    const float4 xa = xq[cj * kClusterSize + jl], xb = xq[cj * kClusterSize + jl + 4];
-    const float ax = xa.x + shx - xi.x, ay = xa.y + shy - xi.y, az = xa.z + shz - xi.z;
-    const float bx = xb.x + shx - xi.x, by = xb.y + shy - xi.y, bz = xb.z + shz - xi.z;
+    const float4 sh = B.sh[k];
+    const float tx = sh.x - xi.x, ty = sh.y - xi.y, tz = sh.z - xi.z;
+    const float4 xa = B.sj[k * kClusterSize + jl], xb = B.sj[k * kClusterSize + jl + 4];
+    const float ax = xa.x + tx, ay = xa.y + ty, az = xa.z + tz;
+    const float bx = xb.x + tx, by = xb.y + ty, bz = xb.z + tz;
     bool oka = (il < nreal_i) && (jl < nrj) && (ax * ax + ay * ay + az * az <= g.rlist2);
     bool okb = (il < nreal_i) && (jl + 4 < nrj) && (bx * bx + by * by + bz * bz <= g.rlist2);
     if (selfzero) {
@@ -266,9 +276,8 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
       okb = okb && (jl + 4 > il);
     }
     const int sa = cj * kClusterSize + jl, sb = sa + 4;
-    // exclusion partners of the i cluster's atoms all lie in clusters
-    // [pcLo, pcHi] (warp-uniform test)
-    if (cj >= pcLo && cj <= pcHi) {
+    const bool hit = cj == pc0 || cj == pc1 || (nps > 2 && cj >= pcLo && cj <= pcHi);
+    if (__any_sync(0xffffffffu, hit)) {
 #pragma unroll
       for (int r = 0; r < kExclRegs; ++r) {
         if (r < nps) {
@@ -330,7 +339,8 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
   if (lane == 0) items[it] = make_int4(ci, (int)e0, nkeep, 0);
 }
 
-__global__ void __launch_bounds__(kSearchThreads)
+// (at most 96 registers: five blocks of four warps per SM)
+__global__ void __launch_bounds__(kSearchThreads, 5)
 k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
          const int *__restrict__ clusterRep, const int *__restrict__ colOff,
          const int *__restrict__ colRank,
@@ -381,6 +391,8 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   }
   pcLo = __reduce_min_sync(0xffffffffu, pcLo);
   pcHi = __reduce_max_sync(0xffffffffu, pcHi);
+  const int pc0 = nps > 0 ? ps[0] / kClusterSize : -1;
+  const int pc1 = nps > 1 ? ps[1] / kClusterSize : -1;
   const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
   const float4 xi = xq[ci * kClusterSize + (lane & 7)];
 
@@ -447,6 +459,13 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
           if (__ldg(&originF[mid].z) <= hiz) a = mid + 1; else b = mid;
         }
         n = a - first;
+        // half list: a pair with cj < ci is listed from cj's side, so the
+        // range starts at ci at the earliest (cluster indices ascend within
+        // a column)
+        if (first < ci) {
+          n = max(0, first + n - ci);
+          first = ci;
+        }
       }
       const bool has = n > 0;
       const unsigned pm = __ballot_sync(0xffffffffu, has);
@@ -525,11 +544,12 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
           B.j[pos] = cj;
           B.sidx[pos] = sidx;
           B.nreal[pos] = (int)hj.w;
+          B.sh[pos] = make_float4(fx, fy, fz, 0.f);
         }
         cnt += __popc(m);
         __syncwarp();
         if (cnt >= kItemMax) {
-          flush_item(B, kItemMax, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps,
+          flush_item(B, kItemMax, ci, lane, oi, xi, xq, g, nreal_i, ps, nps, pc0, pc1,
                      pcLo, pcHi, es, ee, fi, exclFlat, slotOf, slotAtom, frozen, origin, entries,
                      masks, items, counters, entryCap, itemCap);
           __syncwarp();
@@ -538,6 +558,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
             B.j[lane] = B.j[kItemMax + lane];
             B.sidx[lane] = B.sidx[kItemMax + lane];
             B.nreal[lane] = B.nreal[kItemMax + lane];
+            B.sh[lane] = B.sh[kItemMax + lane];
           }
           cnt = rem;
           __syncwarp();
@@ -548,7 +569,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
     __syncwarp();
   }
   if (cnt > 0)
-    flush_item(B, cnt, ci, lane, oi, oif, xi, xq, originF, g, nreal_i, ps, nps, pcLo, pcHi, es,
+    flush_item(B, cnt, ci, lane, oi, xi, xq, g, nreal_i, ps, nps, pc0, pc1, pcLo, pcHi, es,
                ee, fi,
                exclFlat, slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
                entryCap, itemCap);
