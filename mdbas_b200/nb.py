@@ -328,6 +328,7 @@ def bonded_structs(spec: dict | None) -> list:
                 e.theta0 = float(t["theta0"][i])
             else:
                 e.a, e.b, e.c, e.d = at
+                e.order = int(t["order"][i]) if "order" in t else 0
                 e.phi0 = float(t["phi0"][i])
                 e.mult = float(t["mult"][i]) if "mult" in t else 1.0
         out.append((m, arr))

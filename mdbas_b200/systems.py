@@ -68,7 +68,10 @@ class System:
         return int(self.x.shape[0])
 
     def cell(self) -> np.ndarray:
-        """The three box rows a, b, c as MDBas's CONF holds them."""
+        """The three box rows a, b, c as MDBas's SIMU "pbc" block holds them
+        (meta["cell"] when the box is not a cube of edge `box`)."""
+        if self.meta and "cell" in self.meta:
+            return np.asarray(self.meta["cell"], dtype=np.float64)
         return np.array([self.box, 0, 0, 0, self.box, 0, 0, 0, self.box], dtype=np.float64)
 
     def water_constraints(self):
