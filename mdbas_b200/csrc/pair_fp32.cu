@@ -214,19 +214,30 @@ k_pair_fp32(const long long *__restrict__ counters, const int4 *__restrict__ ite
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
 
-template <bool VDW>
-__device__ __forceinline__ void interact2(const PairConstF &c, const float2 jx, const float2 jy,
-                                          const float2 jz, const float2 jq, const float2 jeps,
-                                          const float2 jsig, const float sx, const float sy,
-                                          const float sz, const float qi, const float2 li,
-                                          const bool bita, const bool bitb, bool &ina,
-                                          bool &inb, float2 &fx, float2 &fy, float2 &fz,
-                                          float2 &ec, float2 &ev, float2 &vc, float2 &vv) {
-  const float2 dx = __fadd2_rn(jx, f2(sx)), dy = __fadd2_rn(jy, f2(sy)),
-               dz = __fadd2_rn(jz, f2(sz));
-  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+// The lane's two displacements and squared distances; ina / inb: listed and
+// inside the cut-off.
+__device__ __forceinline__ void distance2(const PairConstF &c, const float2 jx, const float2 jy,
+                                          const float2 jz, const float sx, const float sy,
+                                          const float sz, const bool bita, const bool bitb,
+                                          float2 &dx, float2 &dy, float2 &dz, float2 &r2,
+                                          bool &ina, bool &inb) {
+  dx = __fadd2_rn(jx, f2(sx));
+  dy = __fadd2_rn(jy, f2(sy));
+  dz = __fadd2_rn(jz, f2(sz));
+  r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
   ina = bita && (r2.x <= c.rc2);
   inb = bitb && (r2.y <= c.rc2);
+}
+
+// Energies, virials and forces of the lane's two pairs (pairs outside the
+// cut-off or the list contribute exact zeros).
+template <bool VDW>
+__device__ __forceinline__ void interact2(const PairConstF &c, const float2 dx, const float2 dy,
+                                          const float2 dz, const float2 r2, const float2 jq,
+                                          const float2 jeps, const float2 jsig, const float qi,
+                                          const float2 li, const bool ina, const bool inb,
+                                          float2 &fx, float2 &fy, float2 &fz, float2 &ec,
+                                          float2 &ev, float2 &vc, float2 &vv) {
   const float2 r2s = make_float2(ina ? r2.x : 1.0f, inb ? r2.y : 1.0f);
   const float2 m = make_float2(ina ? 1.0f : 0.f, inb ? 1.0f : 0.f);
   const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
@@ -345,19 +356,22 @@ k_pair_fp32x2(const long long *__restrict__ counters, const int4 *__restrict__ i
         const float sx = en.y - xi.x, sy = en.z - xi.y, sz = en.w - xi.z;
         const float4 p0 = S.jd[k * 12 + jh * 3], p1 = S.jd[k * 12 + jh * 3 + 1],
                      lp = S.jd[k * 12 + jh * 3 + 2];
-        float2 fx, fy, fz;
+        float2 dx, dy, dz, r2;
         bool ina, inb;
-        interact2<VDW>(c, make_float2(p0.x, p0.y), make_float2(p0.z, p0.w),
-                       make_float2(p1.x, p1.y), make_float2(p1.z, p1.w),
-                       make_float2(lp.x, lp.y), make_float2(lp.z, lp.w), sx, sy, sz, xi.w, li,
-                       (mk.x >> lane) & 1u, (mk.y >> lane) & 1u, ina, inb, fx, fy, fz, ec, ev,
-                       vc, vv);
+        distance2(c, make_float2(p0.x, p0.y), make_float2(p0.z, p0.w), make_float2(p1.x, p1.y),
+                  sx, sy, sz, (mk.x >> lane) & 1u, (mk.y >> lane) & 1u, dx, dy, dz, r2, ina,
+                  inb);
+        const unsigned ba = __ballot_sync(0xffffffffu, ina);
+        const unsigned bb = __ballot_sync(0xffffffffu, inb);
+        // a cluster pair listed at the list radius with no pair inside the
+        // cut-off now contributes nothing: skip it (exact zeros otherwise)
+        if ((ba | bb) == 0u) continue;
+        float2 fx, fy, fz;
+        interact2<VDW>(c, dx, dy, dz, r2, make_float2(p1.z, p1.w), make_float2(lp.x, lp.y),
+                       make_float2(lp.z, lp.w), xi.w, li, ina, inb, fx, fy, fz, ec, ev, vc, vv);
         fi_x = __fadd2_rn(fi_x, fx);
         fi_y = __fadd2_rn(fi_y, fy);
         fi_z = __fadd2_rn(fi_z, fz);
-        const unsigned ba = __ballot_sync(0xffffffffu, ina);
-        const unsigned bb = __ballot_sync(0xffffffffu, inb);
-        if ((ba | bb) == 0u) continue;
         npair += __popc(ba) + __popc(bb);
         // reduce-scatter of the two j atoms' forces over the 8 i lanes
         const float ax = fx.x, ay = fy.x, az = fz.x, bx = fx.y, by = fy.y, bz = fz.y;
