@@ -281,12 +281,8 @@ def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_step
     e.md_run(steps)
     e1.record(stream)
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    from mdbas_b200 import ranks
+    ms = ranks.max_over_ranks([e0.elapsed_time(e1) / steps], "cuda" if world > 1 else "cpu")[0]
     st1 = e.md_stats()
     out = {"ms_per_step": ms, "ns_per_day": 86400.0 / (ms * 1e-3) * 1e-6,
            "time_step_fs": 1.0, "steps_timed": steps,
@@ -381,7 +377,12 @@ def replicas_measure(torch, nb, systems, dev, stream, flush, seed, steps, world)
     (rigid water, rebuilds on half-skin displacement), and each replica's
     force error against the plain FP64 form."""
     import numpy as np
-    batch = systems.config_replicas(64, seed=seed, temperature=300.0)
+
+    from mdbas_b200 import ranks
+    # with N ranks each takes a size-balanced share of the 64 boxes
+    rank = int(os.environ.get("RANK", "0"))
+    share = ranks.shard_sizes(systems.replica_sizes(64, seed=seed), world)[rank]
+    batch = systems.config_replicas(64, seed=seed, temperature=300.0, subset=share)
     parts_n = [k for _, k in batch.meta["replicas"]]
     eng = nb.Engine(batch, precision=1, device=dev)
     eng.set_stream(stream.cuda_stream)
@@ -442,22 +443,23 @@ def replicas_measure(torch, nb, systems, dev, stream, flush, seed, steps, world)
     st1 = eng.md_stats()
     launches = eng.launches() - l0
     eng.close()
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([md_ms, sum(ms) / len(ms)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        md_ms, t_step = float(tt[0].item()), float(tt[1].item())
-    else:
-        t_step = sum(ms) / len(ms)
+    dv = "cuda" if world > 1 else "cpu"
+    total_pairs, t_step, rate = ranks.job_rate(pairs, sum(ms) / len(ms), dv)
+    md_ms = ranks.max_over_ranks([md_ms], dv)[0]
+    pair_ms = ranks.max_over_ranks([pair_ms], dv)[0]
+    err_max = ranks.max_over_ranks([max(errs)], dv)[0]
+    n_atoms = int(ranks.sum_over_ranks([batch.n], dv)[0])
     return {
-        "workload": "64 water boxes, 1,500-30,000 atoms (seeded log-uniform), one engine",
-        "n_atoms": int(batch.n), "replica_atoms_min_max": [min(parts_n), max(parts_n)],
-        "in_cutoff_pairs": pairs, "autotune": tune,
-        "ms_per_step": t_step, "pairs_per_s": pairs / (t_step * 1e-3),
-        "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
-        "force_rel_rms_vs_fp64_form": {"max": max(errs), "mean": float(np.mean(errs))},
+        "workload": "64 water boxes, 1,500-30,000 atoms (seeded log-uniform), one engine per "
+                    "GPU holding its size-balanced share",
+        "n_atoms": n_atoms, "replicas_on_rank0": len(share),
+        "replica_atoms_min_max": [min(parts_n), max(parts_n)],
+        "in_cutoff_pairs": int(total_pairs), "autotune": tune,
+        "ms_per_step": t_step, "pairs_per_s": rate,
+        "pair_kernel": {"ms": pair_ms, "pairs_per_s": total_pairs / (pair_ms * 1e-3)},
+        "force_rel_rms_vs_fp64_form": {"max": err_max, "mean_rank0": float(np.mean(errs))},
         "md": {"steps_per_graph_launch": steps, "ms_per_step": md_ms,
-               "pairs_per_s": pairs / (md_ms * 1e-3),
+               "pairs_per_s": total_pairs / (md_ms * 1e-3),
                "aggregate_ns_per_day": 64 * 86400.0 / (md_ms * 1e-3) * 1e-6,
                "list_builds": st1["rebuilds"] - st0["rebuilds"],
                "kernel_launches_per_step": launches / steps}}
@@ -506,7 +508,7 @@ def run_ours(args, rank, world):
     import torch
     import torch.distributed as dist
 
-    from mdbas_b200 import nb, systems
+    from mdbas_b200 import nb, ranks, systems
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -514,7 +516,7 @@ def run_ours(args, rank, world):
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
-    s = systems.config_96k(seed=args.seed + rank, temperature=None)
+    s = systems.config_96k(seed=ranks.rank_seed(args.seed, rank), temperature=None)
     eng = nb.Engine(s, precision=1, device=dev)
     eng.set_stream(stream.cuda_stream)
     eng64 = nb.Engine(s, precision=0, device=dev)
@@ -547,17 +549,10 @@ def run_ours(args, rank, world):
     launches = eng.launches() - launches0
     clk = clocks.stop()
     torch.cuda.synchronize()
-    t_step = sum(ms) / len(ms)
+    dv = "cuda" if world > 1 else "cpu"
+    total_pairs, t_step, _ = ranks.job_rate(pairs, sum(ms) / len(ms), dv)
     if world > 1:
-        tt = torch.tensor([t_step], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_step = float(tt.item())
-        pt = torch.tensor([float(pairs)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(pt, op=dist.ReduceOp.SUM)
-        total_pairs = float(pt.item())
         dist.barrier()
-    else:
-        total_pairs = float(pairs)
     value = total_pairs / (t_step * 1e-3)
 
     # ---- pair kernel alone (CUDA events on the launching stream) ----------
@@ -612,11 +607,7 @@ def run_ours(args, rank, world):
     for _ in range(2):
         step_e2e()
     ms_e2e = _time_steps(torch, eng, stream, flush, args.steps, step_e2e)
-    t_e2e = sum(ms_e2e) / len(ms_e2e)
-    if world > 1:
-        tt = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_e2e = float(tt.item())
+    t_e2e = ranks.max_over_ranks([sum(ms_e2e) / len(ms_e2e)], dv)[0]
     e2e_value = total_pairs / (t_e2e * 1e-3)
 
     # ---- roofline of the pair kernel ---------------------------------------
@@ -672,7 +663,8 @@ def run_ours(args, rank, world):
 
     replicas = None
     if args.replica_steps > 0:
-        replicas = replicas_measure(torch, nb, systems, dev, stream, flush, args.seed + rank,
+        # one 64-box job shared by all ranks: the same seed everywhere
+        replicas = replicas_measure(torch, nb, systems, dev, stream, flush, args.seed,
                                     args.replica_steps, world)
 
     cpu = None

@@ -285,14 +285,17 @@ def replica(batch: System, r: int) -> System:
     return out
 
 
-def config_replicas(count: int = 64, seed: int = 1, temperature: float | None = None) -> System:
+def config_replicas(count: int = 64, seed: int = 1, temperature: float | None = None,
+                    subset=None) -> System:
     """Batched replicas: `count` water boxes with seeded log-uniform atom
     counts in [1,500, 30,000] (multiples of 3), each at 0.0334 molecules/A^3
-    from the lattice-plus-jitter generator (replica i uses seed + i)."""
+    from the lattice-plus-jitter generator (replica i uses seed + i).
+    `subset`: only these replica indices (one rank's share of the batch)."""
     sizes = replica_sizes(count, seed=seed)
-    parts = [water_box_for_atoms(n, seed=seed + i, temperature=temperature)
-             for i, n in enumerate(sizes)]
-    return concat(parts, name=f"replicas{count}")
+    idx = range(count) if subset is None else subset
+    parts = [water_box_for_atoms(sizes[i], seed=seed + i, temperature=temperature) for i in idx]
+    return concat(parts, name=f"replicas{count}" if subset is None else
+                  f"replicas{count}_part{len(parts)}")
 
 
 def flexible_chains(n_side: int = 4, box: float = 26.0, seed: int = 3, jitter: float = 0.05,
