@@ -61,27 +61,27 @@ __device__ __forceinline__ int wrap_index(int i, int m) {
   return i;
 }
 
-// Per atom: grid coordinates, B-splines (bsp[3][nbsp], bsd[3][nbsp]) and the
-// integer grid cell.
+// Per atom and dimension (one thread each): the grid coordinate, B-splines
+// (bsp[3][nbsp], bsd[3][nbsp] per atom) and the integer grid cell.
 __global__ void k_spme_splines(int n, SpmeBox b, int m1, int m2, int m3, int nbsp,
                                const double *__restrict__ x, const double *__restrict__ y,
                                const double *__restrict__ z, double *__restrict__ spl,
                                int *__restrict__ cell) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double s[3] = {(double)m1 * (x[i] * b.u1 + y[i] * b.u2 + z[i] * b.u3 + 0.5),
-                       (double)m2 * (x[i] * b.v1 + y[i] * b.v2 + z[i] * b.v3 + 0.5),
-                       (double)m3 * (x[i] * b.w1 + y[i] * b.w2 + z[i] * b.w3 + 0.5)};
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3LL * n) return;
+  const int i = (int)(t / 3), d = (int)(t % 3);
+  double s;
+  if (d == 0) s = (double)m1 * (x[i] * b.u1 + y[i] * b.u2 + z[i] * b.u3 + 0.5);
+  else if (d == 1) s = (double)m2 * (x[i] * b.v1 + y[i] * b.v2 + z[i] * b.v3 + 0.5);
+  else s = (double)m3 * (x[i] * b.w1 + y[i] * b.w2 + z[i] * b.w3 + 0.5);
   double *o = spl + (size_t)i * 6 * nbsp;
-  for (int d = 0; d < 3; ++d) {
-    double bp[kMaxOrder], bd[kMaxOrder];
-    bspline(s[d], nbsp, bp, bd);
-    for (int k = 0; k < nbsp; ++k) {
-      o[d * nbsp + k] = bp[k];
-      o[(3 + d) * nbsp + k] = bd[k];
-    }
-    cell[3 * i + d] = (int)s[d];
+  double bp[kMaxOrder], bd[kMaxOrder];
+  bspline(s, nbsp, bp, bd);
+  for (int k = 0; k < nbsp; ++k) {
+    o[d * nbsp + k] = bp[k];
+    o[(3 + d) * nbsp + k] = bd[k];
   }
+  cell[3 * i + d] = (int)s;
 }
 
 // Charge spreading: one thread per (atom, first-dimension offset).
@@ -166,35 +166,58 @@ __global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralph
 }
 
 // Force interpolation (src/spme.c:532-575) into fr[3][n]; sums for the mean.
-__global__ void k_spme_forces(int n, int m1, int m2, int m3, int nbsp, SpmeBox b, double fact1,
-                              const double *__restrict__ q, const double *__restrict__ spl,
-                              const int *__restrict__ cell,
+// MDBas's triple sum over the p^3 grid points of an atom factorises:
+//   sum_abc Q(a,b,c) d1_a b2_b b3_c = sum_a d1_a sum_b b2_b sum_c Q b3_c
+// (likewise for the y and z parts), so per (a, b) row only the two sums
+// over c of Q b3_c and Q d3_c are needed.  `group` lanes (the next power of
+// two >= p) share one atom, lane a taking the plane a; the group's three
+// partial forces are summed with shuffles.
+__global__ void k_spme_forces(int n, int m1, int m2, int m3, int nbsp, int group, SpmeBox b,
+                              double fact1, const double *__restrict__ q,
+                              const double *__restrict__ spl, const int *__restrict__ cell,
                               const cufftDoubleComplex *__restrict__ ft, double *__restrict__ fr,
                               double *__restrict__ fsum) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x;
-  double fx = 0., fy = 0., fz = 0.;
-  if (l < n) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int l = (int)(t / group), a = (int)(t % group);
+  double px = 0., py = 0., pz = 0.;
+  if (l < n && a < nbsp) {
     const double *o = spl + (size_t)l * 6 * nbsp;
-    const double *b1 = o, *b2 = o + nbsp, *b3 = o + 2 * nbsp;
-    const double *d1 = o + 3 * nbsp, *d2 = o + 4 * nbsp, *d3 = o + 5 * nbsp;
-    const double ql = q[l];
-    for (int a = 0; a < nbsp; ++a) {
-      const int ii = wrap_index(cell[3 * l] - a, m1);
-      for (int bb = 0; bb < nbsp; ++bb) {
-        const int jj = wrap_index(cell[3 * l + 1] - bb, m2);
-        const size_t base = (size_t)m3 * (jj + (size_t)m2 * ii);
-        for (int c = 0; c < nbsp; ++c) {
-          const int kk = wrap_index(cell[3 * l + 2] - c, m3);
-          const double qt = ft[base + kk].x;
-          const double fbx = qt * d1[a] * b2[bb] * b3[c] * (double)m1;
-          const double fby = qt * b1[a] * d2[bb] * b3[c] * (double)m2;
-          const double fbz = qt * b1[a] * b2[bb] * d3[c] * (double)m3;
-          fx += fact1 * ql * (fbx * b.u1 + fby * b.v1 + fbz * b.w1);
-          fy += fact1 * ql * (fbx * b.u2 + fby * b.v2 + fbz * b.w2);
-          fz += fact1 * ql * (fbx * b.u3 + fby * b.v3 + fbz * b.w3);
-        }
+    const double *b2 = o + nbsp, *b3 = o + 2 * nbsp;
+    const double *d2 = o + 4 * nbsp, *d3 = o + 5 * nbsp;
+    const int ii = wrap_index(cell[3 * l] - a, m1);
+    const int cy = cell[3 * l + 1], cz = cell[3 * l + 2];
+    double t1 = 0., t2 = 0., t3 = 0.;
+    for (int bb = 0; bb < nbsp; ++bb) {
+      const int jj = wrap_index(cy - bb, m2);
+      const size_t base = (size_t)m3 * (jj + (size_t)m2 * ii);
+      double sb = 0., sd = 0.;
+      for (int c = 0; c < nbsp; ++c) {
+        const double qt = ft[base + wrap_index(cz - c, m3)].x;
+        sb += qt * __ldg(b3 + c);
+        sd += qt * __ldg(d3 + c);
       }
+      const double wb = __ldg(b2 + bb);
+      t1 += wb * sb;
+      t2 += __ldg(d2 + bb) * sb;
+      t3 += wb * sd;
     }
+    px = __ldg(o + 3 * nbsp + a) * t1;  // d1_a
+    const double b1a = __ldg(o + a);
+    py = b1a * t2;
+    pz = b1a * t3;
+  }
+  for (int off = group >> 1; off > 0; off >>= 1) {
+    px += __shfl_xor_sync(0xffffffffu, px, off);
+    py += __shfl_xor_sync(0xffffffffu, py, off);
+    pz += __shfl_xor_sync(0xffffffffu, pz, off);
+  }
+  double fx = 0., fy = 0., fz = 0.;
+  if (l < n && a == 0) {
+    const double fbx = px * (double)m1, fby = py * (double)m2, fbz = pz * (double)m3;
+    const double fq = fact1 * q[l];
+    fx = fq * (fbx * b.u1 + fby * b.v1 + fbz * b.w1);
+    fy = fq * (fbx * b.u2 + fby * b.v2 + fbz * b.w2);
+    fz = fq * (fbx * b.u3 + fby * b.v3 + fbz * b.w3);
     fr[l] = fx;
     fr[n + l] = fy;
     fr[2 * (size_t)n + l] = fz;
@@ -329,7 +352,7 @@ int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, in
   double *sums = c.sums.as<double>();  // 0-5 stress, 6-8 force sums, 9 energy
   MDB_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * 16, s));
   MDB_CUDA(cudaMemsetAsync(c.qsp.p, 0, sizeof(double) * mm, s));
-  MDB_LAUNCH(k_spme_splines, grid_for(n, 128), 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z,
+  MDB_LAUNCH(k_spme_splines, grid_for(3LL * n, 128), 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z,
              c.spl.as<double>(), c.cell.as<int>());
   MDB_LAUNCH(k_spme_spread, grid_for((long long)n * nbsp, 128), 128, 0, s, n, m1, m2, m3, nbsp,
              q, c.spl.as<double>(), c.cell.as<int>(), c.qsp.as<double>());
@@ -344,7 +367,10 @@ int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, in
   MDB_LAUNCH(k_spme_influence, grid_for(mm, 256), 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
              c.bmod.as<double>(), ft, sums);
   MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_FORWARD), "cufftExecZ2Z"));
-  MDB_LAUNCH(k_spme_forces, grid_for(n, 128), 128, 0, s, n, m1, m2, m3, nbsp, b,
+  int group = 1;
+  while (group < nbsp) group <<= 1;
+  MDB_LAUNCH(k_spme_forces, grid_for((long long)n * group, 128), 128, 0, s, n, m1, m2, m3, nbsp,
+             group, b,
              -2.0 * rvol * chargeConst, q, c.spl.as<double>(), c.cell.as<int>(), ft,
              c.fr.as<double>(), sums + 6);
   MDB_LAUNCH(k_spme_energy, grid_for(mm, 256), 256, 0, s, mm, ft, c.qsp.as<double>(), sums + 9);
