@@ -573,6 +573,24 @@ int mdbas_nb_engine_set_bonded(mdbas_nb_engine *e, int nBond, const BOND *bond, 
 int mdbas_nb_engine_bonded(mdbas_nb_engine *e, double *fx, double *fy, double *fz,
                            int device_ptrs, double out[7]);
 
+/* Reciprocal space in the dynamics, as MDBas's energy() with keyEwald 1
+ * (ewald_rec) or 2 (spme_energy) adds it: kind 0 off (default: real space
+ * only, the benchmark's potential), 1 explicit Ewald sum over |m_d| <=
+ * m{d} (section 9), 2 SPME on an m1 x m2 x m3 grid with B-splines of order
+ * nbsp (section 7); the engine's alpha and charge constant.  Single boxes
+ * only (MDBAS_NB_ERR_UNSUPPORTED for a batch); call after the topology.
+ * Dynamics then add the reciprocal forces every step (inside the step's
+ * CUDA graph) and the energy rows' potential holds the reciprocal and
+ * non-neutral terms as well.  Explicit Ewald is deterministic; SPME spreads
+ * charges with FP64 atomics, so its trajectories agree run to run only to
+ * rounding. */
+int mdbas_nb_engine_set_kspace(mdbas_nb_engine *e, int kind, int m1, int m2, int m3, int nbsp);
+/* The engine's reciprocal term at its current positions: forces added to
+ * fx/fy/fz (host arrays, NULL = energy only); out[0] = energy (reciprocal +
+ * self + non-neutral, MDBas's ewald_rec / spme_energy value), out[1] =
+ * virial. */
+int mdbas_nb_engine_kspace(mdbas_nb_engine *e, double *fx, double *fy, double *fz, double out[2]);
+
 /* ------------------------------------------------------------------------ */
 /* 6. Adjoint of the real-space energy (no counterpart in MDBas, whose        */
 /*    numderiv.c gives only finite differences)                              */

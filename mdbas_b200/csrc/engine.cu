@@ -224,6 +224,7 @@ int mdbas_nb_engine_destroy(mdbas_nb_engine *e) {
   cudaSetDevice(e->device);
   cudaStreamSynchronize(e->stream);
   md_release(e);
+  kspace_release(e);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
   if (e->ownStream) cudaStreamDestroy(e->stream);

@@ -5,6 +5,7 @@
 
 #include "bonded.cuh"
 #include "cluster.cuh"
+#include "kspace.cuh"
 #include "list_ref.cuh"
 
 struct mdbas_nb_engine {
@@ -46,6 +47,15 @@ struct mdbas_nb_engine {
   // bonded terms (bonded.cu), added to the dynamics forces
   mdbas::BondedTerms bonded;
   mdbas::DBuf bondedF;
+  // reciprocal space of the dynamics (md_kspace.cu): 0 none, 1 explicit
+  // Ewald (m-range kspaceM), 2 SPME (grid kspaceM, order kspaceOrder)
+  int kspaceKind = 0;
+  int kspaceM[3] = {0, 0, 0};
+  int kspaceOrder = 0;
+  double kspaceSystq = 0.0, kspaceSumq2 = 0.0;
+  mdbas::EwaldWork *kEwald = nullptr;
+  mdbas::SpmeWork *kSpme = nullptr;
+  mdbas::DBuf kspaceFix, kspaceF;  // int64 energy word; scratch forces (3n)
   // bookkeeping
   bool built = false, computed = false;
   long long launches = 0;
@@ -92,6 +102,10 @@ struct LaunchScope {
 int engine_check_device(int device);
 // Releases the dynamics graph and its streams (md.cu).
 void md_release(mdbas_nb_engine *e);
+// Reciprocal forces added to f (3n, caller order) and the reciprocal plus
+// non-neutral energy into kspaceFix (md_kspace.cu); no-op when off.
+int md_kspace(mdbas_nb_engine *e, double *f, cudaStream_t s);
+void kspace_release(mdbas_nb_engine *e);
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);
 }  // namespace mdbas

@@ -25,7 +25,7 @@
 
 #include <vector>
 
-#include "common.cuh"
+#include "kspace.cuh"
 
 namespace mdbas {
 namespace {
@@ -248,28 +248,15 @@ __global__ void k_ewald_forces(int n, EwBox b, int M1, int M2, int M3, int nRows
   }
 }
 
-// k list of one box / alpha / m-range, built on the host with MDBas's
-// expressions (src/ewald.c:146-150, 255-300).
-struct KList {
-  bool valid = false;
-  double key[12] = {};
-  int M1 = 0, M2 = 0, M3 = 0;
-  int K = 0, nRows = 0;
-  DBuf km, kv, vam, rows, rowK;
-};
-
-struct EwaldCtx {
-  KList kl;
-  int device = -1;
-  DBuf part, S, bpart, sums, t12, xyzq, f;
-};
-
-EwaldCtx &ewald_ctx() {
-  static EwaldCtx c;
+// The standalone calls' state (the engine keeps its own).
+EwaldWork &ewald_ctx() {
+  static EwaldWork c;
   return c;
 }
 
-int build_klist(KList &kl, const PBC *box, double alpha, int M1, int M2, int M3) {
+// k list of one box / alpha / m-range, built on the host with MDBas's
+// expressions (src/ewald.c:146-150, 255-300).
+int build_klist(EwaldKList &kl, const PBC *box, double alpha, int M1, int M2, int M3) {
   const double key[12] = {box->u1, box->u2, box->u3, box->v1, box->v2, box->v3, box->w1,
                           box->w2, box->w3, alpha, box->u + box->v + box->w,
                           (double)M1 + 1000. * M2 + 1.e6 * M3};
@@ -361,13 +348,10 @@ EwBox make_ew_box(const PBC *p) {
   return b;
 }
 
-// Device arrays; out[0] = energy (reciprocal + self + non-neutral), out[1] =
-// virial, out[2..7] = stress; out[8] (if given) = number of k-vectors.
-int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, int M2, int M3,
-              const double *x, const double *y, const double *z, const double *q, double systq,
-              double sumq2, double *fx, double *fy, double *fz, int scaleInput, double out[8],
-              cudaStream_t s) {
-  EwaldCtx &c = ewald_ctx();
+int ewald_launch_impl(EwaldWork &c, int n, const PBC *box, double alpha, double chargeConst,
+                      int M1, int M2, int M3, const double *x, const double *y, const double *z,
+                      const double *q, double *fx, double *fy, double *fz, int scaleInput,
+                      cudaStream_t s) {
   int dev = 0;
   MDB_CUDA(cudaGetDevice(&dev));
   if (c.device != dev) {
@@ -375,7 +359,7 @@ int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, i
     c.device = dev;
   }
   MDB_TRY(build_klist(c.kl, box, alpha, M1, M2, M3));
-  const KList &kl = c.kl;
+  const EwaldKList &kl = c.kl;
   const EwBox b = make_ew_box(box);
   const int K = kl.K;
   // shared memory: the k-thread kernel's atom tile, the atom kernel's m3 table
@@ -391,10 +375,11 @@ int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, i
     set_last_status(MDBAS_NB_ERR_UNSUPPORTED, "reciprocal m-range too large for shared memory");
     return MDBAS_NB_ERR_UNSUPPORTED;
   }
-  double h[7] = {0., 0., 0., 0., 0., 0., 0.};
   const size_t smemF = sizeof(double) * 2 * (size_t)(M3 + 1) * fThreads;
   MDB_TRY(c.t12.ensure(sizeof(double) * 2 * (size_t)(M1 + M2 + 2) * n));
   MDB_TRY(c.S.ensure(sizeof(double2) * (size_t)(K > 0 ? K : 1)));
+  MDB_TRY(c.sums.ensure(sizeof(double) * 8));
+  if (K == 0) MDB_CUDA(cudaMemsetAsync(c.sums.p, 0, sizeof(double) * 8, s));
   if (K > 0) {
     const int kBlocks = (K + kSfThreads - 1) / kSfThreads;
     int sms = 148;
@@ -409,7 +394,6 @@ int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, i
     MDB_TRY(c.part.ensure(sizeof(double) * 2 * (size_t)P * K));
     const int kdBlocks = (K + 255) / 256;
     MDB_TRY(c.bpart.ensure(sizeof(double) * 7 * (size_t)kdBlocks));
-    MDB_TRY(c.sums.ensure(sizeof(double) * 8));
     MDB_LAUNCH(k_ewald_sf, dim3(kBlocks, P), kSfThreads, smemSf, s, n, K, perPart, tile, b, M1,
                M2, M3, kl.km.as<int4>(), x, y, z, q, c.part.as<double>());
     MDB_LAUNCH(k_ewald_kdata, kdBlocks, 256, 0, s, K, P, c.part.as<double>(),
@@ -426,8 +410,23 @@ int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, i
   MDB_LAUNCH(k_ewald_forces, grid_for(n, fThreads), fThreads, smemF, s, n, b, M1, M2, M3,
              kl.nRows, kl.rows.as<int4>(), kl.rowK.as<int>(), kl.kv.as<double4>(),
              c.S.as<double2>(), x, y, z, q, c.t12.as<double>(), fact0, scaleInput, fx, fy, fz);
-  if (K > 0) MDB_CUDA(cudaMemcpyAsync(h, c.sums.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  c.fact1 = fact1;
+  return MDBAS_NB_OK;
+}
+
+// Device arrays; out[0] = energy (reciprocal + self + non-neutral), out[1] =
+// virial, out[2..7] = stress.
+int ewald_run(int n, const PBC *box, double alpha, double chargeConst, int M1, int M2, int M3,
+              const double *x, const double *y, const double *z, const double *q, double systq,
+              double sumq2, double *fx, double *fy, double *fz, int scaleInput, double out[8],
+              cudaStream_t s) {
+  EwaldWork &c = ewald_ctx();
+  MDB_TRY(ewald_launch_impl(c, n, box, alpha, chargeConst, M1, M2, M3, x, y, z, q, fx, fy, fz,
+                            scaleInput, s));
+  double h[7];
+  MDB_CUDA(cudaMemcpyAsync(h, c.sums.p, sizeof(h), cudaMemcpyDeviceToHost, s));
   MDB_CUDA(cudaStreamSynchronize(s));
+  const double fact1 = c.fact1;
   // src/ewald.c:323-352
   const double eself = -chargeConst * alpha * sumq2 / kSqrtPi;
   const double enn = -(0.5 * kPi * chargeConst) * ((systq / alpha) * (systq / alpha) / box->vol);
@@ -451,7 +450,7 @@ int nint_h(double x) { return (x >= 0.) ? (int)(x + 0.5) : (int)(x - 0.5); }
 int ewald_host(int n, const PBC *box, double alpha, double chargeConst, int M1, int M2, int M3,
                const double *x, const double *y, const double *z, const double *q, double *fx,
                double *fy, double *fz, int scaleInput, double out[8]) {
-  EwaldCtx &c = ewald_ctx();
+  EwaldWork &c = ewald_ctx();
   double systq = 0., sumq2 = 0.;
   for (int i = 0; i < n; ++i) {  // src/ewald.c:166-172
     systq += q[i];
@@ -478,7 +477,27 @@ int ewald_host(int n, const PBC *box, double alpha, double chargeConst, int M1, 
   return MDBAS_NB_OK;
 }
 
+__global__ void k_kspace_fix(const double *__restrict__ src, double scale, double add,
+                             long long *__restrict__ dst) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) dst[0] = fix_e(scale * src[0] + add);
+}
+
 }  // namespace
+
+int ewald_launch(EwaldWork &c, int n, const PBC *box, double alpha, double chargeConst, int M1,
+                 int M2, int M3, const double *x, const double *y, const double *z,
+                 const double *q, double *fx, double *fy, double *fz, int scaleInput,
+                 cudaStream_t s) {
+  return ewald_launch_impl(c, n, box, alpha, chargeConst, M1, M2, M3, x, y, z, q, fx, fy, fz,
+                           scaleInput, s);
+}
+
+int kspace_fix_launch(const double *src, double scale, double add, long long *dst,
+                      cudaStream_t s) {
+  MDB_LAUNCH(k_kspace_fix, 1, 32, 0, s, src, scale, add, dst);
+  return MDBAS_NB_OK;
+}
+
 }  // namespace mdbas
 
 using namespace mdbas;

@@ -725,16 +725,18 @@ __global__ void k_count(long long *__restrict__ c) {
 
 // Fixed-point energies of the step (elec direct, elec corr, vdw, kinetic) and
 // the accumulated error bits.
-// row = {direct, correction, vdw, kinetic, bonded} in fixed point (2^-24)
+// row = {direct, correction, vdw, kinetic, bonded, reciprocal} in fixed
+// point (2^-24)
 __global__ void k_md_row(long long *__restrict__ row, const long long *__restrict__ acc,
                          const long long *__restrict__ kin, const long long *__restrict__ bonded,
-                         long long *__restrict__ flags) {
+                         const long long *__restrict__ kspace, long long *__restrict__ flags) {
   if (threadIdx.x != 0) return;
   row[0] = acc[ACC_E_DIR];
   row[1] = acc[ACC_E_CORR];
   row[2] = acc[ACC_E_VDW];
   row[3] = kin[0];
   row[4] = bonded ? bonded[0] : 0;
+  row[5] = kspace ? kspace[0] : 0;
   flags[0] |= acc[ACC_FLAGS];
 }
 
@@ -768,11 +770,17 @@ enum MdWord {
   W_COUNT = 10
 };
 
-constexpr int kRowWords = 5;  // k_md_row's row length
+constexpr int kRowWords = 6;  // k_md_row's row length
 
 // Fixed-point bonded energy of the last md_forces (null without bonded terms).
 const long long *md_bonded_fix(const mdbas_nb_engine *e) {
   return e->bonded.nTerms() > 0 ? e->bonded.sums.as<long long>() + BS_FIX : nullptr;
+}
+
+// Fixed-point reciprocal + non-neutral energy of the last md_forces (null
+// without k-space).
+const long long *md_kspace_fix(const mdbas_nb_engine *e) {
+  return e->kspaceKind != 0 ? e->kspaceFix.as<long long>() : nullptr;
 }
 
 // FP64 forces of the last compute, caller order, into e->mdF (3n); then the
@@ -787,6 +795,7 @@ int md_forces(mdbas_nb_engine *e, cudaStream_t s) {
   } else {
     MDB_TRY(forces_out_launch(e->cl, n, 0, f, f + n, f + 2 * (size_t)n, s));
   }
+  MDB_TRY(md_kspace(e, f, s));
   if (e->bonded.nTerms() > 0)
     MDB_TRY(bonded_eval(e->bonded, BOXES(e), e->x.as<double>(), e->y.as<double>(),
                         e->z.as<double>(), f, s));
@@ -1106,7 +1115,8 @@ int md_capture_steps(mdbas_nb_engine *e, int K, double tauT, double kinTemp0,
     MDB_TRY(md_forces_cluster(e, cs));
     MDB_TRY(md_stage2(e, cs, true, tauT, kinTemp0));
     MDB_LAUNCH(k_md_row, 1, 32, 0, cs, e->mdRows.as<long long>() + kRowWords * (size_t)k,
-               e->cl.acc.as<long long>(), word + W_KIN, md_bonded_fix(e), word + W_FLAGS);
+               e->cl.acc.as<long long>(), word + W_KIN, md_bonded_fix(e), md_kspace_fix(e),
+               word + W_FLAGS);
   }
   return MDBAS_NB_OK;
 }
@@ -1238,7 +1248,7 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
       const long long gstep = step0 + k + 1;
       if (energies && energyEvery > 0 && gstep % energyEvery == 0) {
         const long long *r = &rows[kRowWords * (size_t)k];
-        const double pot = (double)(r[0] + r[1] + r[2] + r[4]) / kEnergyScale + e->selfE;
+        const double pot = (double)(r[0] + r[1] + r[2] + r[4] + r[5]) / kEnergyScale + e->selfE;
         const double kin = md_kin_row((double)r[3] / kEnergyScale, e->mdDt, tauT, kinTemp0);
         md_write_row(energies, (*outRow)++, gstep, pot, kin);
       }
@@ -1515,13 +1525,15 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
     if (wantE) {
       long long kfix = 0;
       MDB_CUDA(cudaMemcpyAsync(&kfix, word + W_KIN, sizeof(kfix), cudaMemcpyDeviceToHost, s));
-      long long bfix = 0;
+      long long bfix = 0, kfixr = 0;
       if (const long long *b = md_bonded_fix(e))
         MDB_CUDA(cudaMemcpyAsync(&bfix, b, sizeof(bfix), cudaMemcpyDeviceToHost, s));
+      if (const long long *k = md_kspace_fix(e))
+        MDB_CUDA(cudaMemcpyAsync(&kfixr, k, sizeof(kfixr), cudaMemcpyDeviceToHost, s));
       mdbas_nb_energies en;
       MD_TRY(mdbas_nb_engine_energies(e, &en));  // synchronises the stream
       const double pot = en.elec_direct + en.elec_corr + en.elec_self + en.vdw +
-                         (double)bfix / kEnergyScale;
+                         (double)(bfix + kfixr) / kEnergyScale;
       md_write_row(energies, outRow++, gstep,
                    pot, md_kin_row((double)kfix / kEnergyScale, e->mdDt, tauT, kinTemp0));
     }

@@ -20,7 +20,7 @@
 #include <complex>
 #include <vector>
 
-#include "common.cuh"
+#include "kspace.cuh"
 
 using namespace mdbas;
 
@@ -268,19 +268,9 @@ void bsp_moduli(int m, int nbsp, double *out) {
   }
 }
 
-struct SpmeCtx {
-  int device = -1;
-  int m1 = 0, m2 = 0, m3 = 0, nbsp = 0, n = 0;
-  cufftHandle plan = 0;
-  bool planValid = false;
-  DBuf qsp, ft, bmod, spl, cell, fr, sums, xyzq, fout;
-  ~SpmeCtx() {
-    if (planValid) cufftDestroy(plan);
-  }
-};
-
-SpmeCtx &spme_ctx() {
-  static SpmeCtx c;
+// The standalone calls' state (the engine keeps its own).
+SpmeWork &spme_ctx() {
+  static SpmeWork c;
   return c;
 }
 
@@ -303,7 +293,7 @@ int cufft_check(cufftResult r, const char *what) {
 }
 
 // Grid-size dependent state: plan, moduli, grid buffers.
-int spme_setup(SpmeCtx &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_t s) {
+int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_t s) {
   int dev = 0;
   MDB_CUDA(cudaGetDevice(&dev));
   const long long mm = (long long)m1 * m2 * m3;
@@ -341,11 +331,10 @@ int spme_setup(SpmeCtx &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_t
 // The whole computation on device arrays; forces (minus their mean) are added
 // to fx/fy/fz; out[0] = reciprocal energy + self + non-neutral, out[1] =
 // virial, out[2..7] = stress (MDBas's 6-component layout).
-int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, int m2, int m3,
-             int nbsp, const double *x, const double *y, const double *z, const double *q,
-             double systq, double sumq2, double *fx, double *fy, double *fz, double out[8],
-             cudaStream_t s) {
-  SpmeCtx &c = spme_ctx();
+int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double chargeConst,
+                     int m1, int m2, int m3, int nbsp, const double *x, const double *y,
+                     const double *z, const double *q, double *fx, double *fy, double *fz,
+                     cudaStream_t s) {
   MDB_TRY(spme_setup(c, n, m1, m2, m3, nbsp, s));
   const SpmeBox b = make_spme_box(box);
   const long long mm = (long long)m1 * m2 * m3;
@@ -376,6 +365,20 @@ int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, in
   MDB_LAUNCH(k_spme_energy, grid_for(mm, 256), 256, 0, s, mm, ft, c.qsp.as<double>(), sums + 9);
   MDB_LAUNCH(k_spme_add, grid_for(n, 256), 256, 0, s, n, c.fr.as<double>(), sums + 6, fx, fy,
              fz);
+  c.f1 = rvol * chargeConst;
+  return MDBAS_NB_OK;
+}
+
+int spme_run(int n, const PBC *box, double alpha, double chargeConst, int m1, int m2, int m3,
+             int nbsp, const double *x, const double *y, const double *z, const double *q,
+             double systq, double sumq2, double *fx, double *fy, double *fz, double out[8],
+             cudaStream_t s) {
+  SpmeWork &c = spme_ctx();
+  MDB_TRY(spme_launch_impl(c, n, box, alpha, chargeConst, m1, m2, m3, nbsp, x, y, z, q, fx, fy,
+                           fz, s));
+  const SpmeBox b = make_spme_box(box);
+  const double rvol = 6.283185307179586 / b.vol;
+  double *sums = c.sums.as<double>();
   double h[16];
   MDB_CUDA(cudaMemcpyAsync(h, sums, sizeof(h), cudaMemcpyDeviceToHost, s));
   MDB_CUDA(cudaStreamSynchronize(s));
@@ -407,6 +410,14 @@ int nint_h(double x) { return (x >= 0.) ? (int)(x + 0.5) : (int)(x - 0.5); }
 
 }  // namespace
 
+int mdbas::spme_launch(SpmeWork &c, int n, const PBC *box, double alpha, double chargeConst,
+                       int m1, int m2, int m3, int nbsp, const double *x, const double *y,
+                       const double *z, const double *q, double *fx, double *fy, double *fz,
+                       cudaStream_t s) {
+  return spme_launch_impl(c, n, box, alpha, chargeConst, m1, m2, m3, nbsp, x, y, z, q, fx, fy, fz,
+                          s);
+}
+
 extern "C" {
 
 int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, int m1, int m2,
@@ -417,7 +428,7 @@ int mdbas_nb_spme(int nAtom, const PBC *box, double alpha, double chargeConst, i
     return MDBAS_NB_ERR_ARG;
   MDB_TRY(check_grid(m1, m2, m3, nbsp));
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  SpmeCtx &c = spme_ctx();
+  SpmeWork &c = spme_ctx();
   double systq = 0., sumq2 = 0.;
   std::vector<double> hq;
   const double *qh = q;

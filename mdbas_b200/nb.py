@@ -236,6 +236,9 @@ def lib():
     L.mdbas_nb_ewald_rec.argtypes = [C.c_int, C.POINTER(PBC), C.c_double, C.c_double, C.c_int,
                                      C.c_int, C.c_int] + [C.c_void_p] * 7 + [
                                          C.POINTER(C.c_double), C.c_int, C.c_void_p]
+    L.mdbas_nb_engine_set_kspace.argtypes = [C.c_void_p] + [C.c_int] * 5
+    L.mdbas_nb_engine_kspace.argtypes = [C.c_void_p] + [C.c_void_p] * 3 + [
+        C.POINTER(C.c_double)]
     L.mdbas_nb_bonded.argtypes = [C.c_int, C.c_int, C.POINTER(PBC), C.c_int, C.c_void_p] + [
         C.c_void_p] * 6 + [C.POINTER(C.c_double)]
     L.mdbas_nb_engine_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
@@ -539,6 +542,22 @@ class Engine:
         for m, arr in self._bonded:
             args += [m, C.cast(arr, C.c_void_p)]
         check(lib().mdbas_nb_engine_set_bonded(self.h, *args), "set_bonded")
+
+    def set_kspace(self, kind: int, m=(0, 0, 0), order: int = 0):
+        """Reciprocal space of the dynamics: 0 off, 1 explicit Ewald with the
+        m-range m, 2 SPME on the grid m with B-spline order `order`."""
+        check(lib().mdbas_nb_engine_set_kspace(self.h, int(kind), *[int(v) for v in m],
+                                               int(order)), "set_kspace")
+
+    def kspace(self, forces=None):
+        """(energy incl. self and non-neutral terms, virial, [fx, fy, fz]) of
+        the reciprocal term at the current positions; forces added to copies
+        of `forces` (or to zeros)."""
+        f = ([np.zeros(self.n) for _ in range(3)] if forces is None
+             else [np.array(a, dtype=np.float64) for a in forces])
+        out = (C.c_double * 2)()
+        check(lib().mdbas_nb_engine_kspace(self.h, *(_ptr(a) for a in f), out), "kspace")
+        return out[0], out[1], f
 
     def bonded(self, forces=None):
         """Bonded energies at the current positions (dict of BONDED_ENERGIES)

@@ -249,6 +249,8 @@ class Reference:
             lib.ref_ewald_rec.argtypes = [C.c_void_p, C.c_double, C.c_void_p, _dp, _dp, _dp,
                                           _dp]
             lib.ref_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
+            lib.ref_set_kspace.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
+            lib.ref_set_kspace.restype = C.c_int
             lib.ref_bonded_energies.argtypes = [C.c_void_p, _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
@@ -287,6 +289,12 @@ class Reference:
         for m, arr in structs:
             args += [int(m), C.cast(arr, C.c_void_p)]
         self.lib().ref_set_bonded(self.h, *args)
+
+    def set_kspace(self, mmax, prec=1e-6) -> int:
+        """Explicit Ewald k-space (MDBas's init_ewald + ewald_rec) in every
+        later energy() call, with the harness alpha and this m-range;
+        returns the k-vector count."""
+        return self.lib().ref_set_kspace(self.h, prec, *[int(v) for v in mmax])
 
     def bonded_energies(self) -> dict:
         """Bonded energies of the last energy() call."""

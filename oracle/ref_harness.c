@@ -64,6 +64,7 @@ typedef struct {
   BOND *bond, *ub;
   ANGLE *angle;
   int bondedOn; /* ref_set_bonded: energy() evaluates the bonded terms */
+  int kspaceKey; /* ref_set_kspace: energy()'s keyEwald (0: real space only, 3) */
   CONSTRAINT *constList;
   DIHE *dihe, *impr;
   double *x, *y, *z, *q, *eps, *sig, *fx, *fy, *fz, *vx, *vy, *vz;
@@ -236,6 +237,27 @@ static PARAM energy_param(const RefSys *s)
   return p;
 }
 
+/*
+ * Explicit Ewald k-space in energy() (keyEwald = 1, src/energy.c:469-470)
+ * with the harness alpha and the m-range m1..m3: MDBas's init_ewald sets the
+ * k count and allocates its tables (kept until ref_destroy).  Energies then
+ * include the reciprocal, self and non-neutral terms.  Returns mmax.
+ */
+int ref_set_kspace(RefSys *s, double prec, int m1, int m2, int m3)
+{
+  CTRL c = s->ctrl;
+  if (s->kspaceKey == 1) return -1;
+  c.keyAlpha = 1;
+  c.keyMmax = 1;
+  s->ewald.prec = prec;
+  s->ewald.m1max = m1;
+  s->ewald.m2max = m2;
+  s->ewald.m3max = m3;
+  init_ewald(&c, &s->param, &s->ewald, &s->box);
+  s->kspaceKey = 1;
+  return s->ewald.mmax;
+}
+
 int ref_n_pair14(const RefSys *s) { return s->neigh.nPair14; }
 
 void ref_get_list14(const RefSys *s, int *out)
@@ -369,7 +391,7 @@ void ref_set_positions(RefSys *s, const double *x, const double *y, const double
 void ref_energy(RefSys *s, double *fx, double *fy, double *fz, double out[6])
 {
   PARAM p = energy_param(s);
-  s->ctrl.keyEwald = 3;
+  s->ctrl.keyEwald = s->kspaceKey ? s->kspaceKey : 3;
   init_energy_ptrs(&s->ctrl);
   energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->ub, s->angle,
          s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,
@@ -407,6 +429,7 @@ void ref_destroy(RefSys *s)
 {
   int i;
   if (!s) return;
+  if (s->kspaceKey == 1) ewald_free(&s->ewald);
   free(s->x); free(s->y); free(s->z); free(s->q); free(s->eps); free(s->sig);
   free(s->fx); free(s->fy); free(s->fz); free(s->vx); free(s->vy); free(s->vz);
   free(s->frozen); free(s->bond); free(s->ub); free(s->angle); free(s->constList); free(s->dihe);
