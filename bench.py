@@ -67,6 +67,8 @@ def _parse():
                    help="timed velocity-Verlet steps (1 fs, rigid water) for ns/day")
     p.add_argument("--nve-steps", type=int, default=10000,
                    help="NVE steps (1 fs) for the energy-drift report; 0 skips it")
+    p.add_argument("--pme-steps", type=int, default=200,
+                   help="timed steps of the 96k dynamics with SPME in every step")
     p.add_argument("--large-steps", type=int, default=10,
                    help="timed steps of the 999,999-atom box; 0 skips it")
     p.add_argument("--replica-steps", type=int, default=100,
@@ -255,17 +257,21 @@ def _time_steps(torch, eng, stream, flush, steps, fn):
     return [a.elapsed_time(b) for a, b in evs]
 
 
-def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_steps, world):
+def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_steps, world,
+               kspace=None):
     """Velocity-Verlet dynamics of the 96k water box (rigid SHAKE/RATTLE
     water, list rebuilt on half-skin displacement).  The lattice-plus-jitter
     start is relaxed first (2,000 Berendsen steps at 0.5 fs toward 300 K,
     untimed); then `steps` 1 fs NVE steps are timed with CUDA events on the
-    engine stream, and `nve_steps` more give the energy drift."""
+    engine stream, and `nve_steps` more give the energy drift.  kspace =
+    (kind, grid, order) adds reciprocal space to every step."""
     import numpy as np
     s = systems.config_96k(seed=seed, temperature=300.0)
     cons = s.water_constraints()
     e = nb.Engine(s, precision=precision, device=dev)
     e.set_stream(stream.cuda_stream)
+    if kspace is not None:
+        e.set_kspace(*kspace)
     e.md_init(s.mass, (s.vx, s.vy, s.vz), time_step=0.0005, list_update=0, constraints=cons)
     e.md_run(2000, target_temp=300.0, tau_t=0.05)
     pos, vel = e.positions(), e.velocities()
@@ -653,6 +659,13 @@ def run_ours(args, rank, world):
                         args.nve_steps, world)
         md64 = md_measure(torch, nb, systems, dev, stream, args.seed + rank, 0,
                           max(50, args.md_steps // 5), 0, world)
+    # full electrostatics: SPME (MDBas's grid rule at prec 1e-6: 128^3, order
+    # 8) in every step of the same dynamics
+    md_pme = None
+    if args.pme_steps > 0:
+        md_pme = md_measure(torch, nb, systems, dev, stream, args.seed + rank, 1, args.pme_steps,
+                            0, world, kspace=(2, (128, 128, 128), 8))
+        md_pme["kspace"] = "SPME 128^3, B-spline order 8, every step, inside the step graph"
 
     spme = spme_measure(torch, nb, systems, dev, stream, args.seed + rank, 5)
 
@@ -687,6 +700,7 @@ def run_ours(args, rank, world):
             "ns_per_day": md["ns_per_day"] if md else None,
             "md": md,
             "md_fp64_form": md64,
+            "md_pme": md_pme,
             "large_box": large,
             "spme": spme,
             "replicas": replicas,
