@@ -404,7 +404,9 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, l
  * two pairs in packed f32x2 arithmetic, with each chunk of 8 cluster pairs
  * staged in shared memory; 0 is the same in scalar FP32 without staging;
  * 1 filters the pairs first and computes only in-cut-off pairs from per-atom
- * queues. */
+ * queues; 3 is variant 2 with each chunk's j data brought into shared memory
+ * by asynchronous bulk copies (cp.async.bulk with an mbarrier, double
+ * buffered) instead of per-lane loads -- the same results bit for bit. */
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
 /* Autotuner of the mixed-precision pair kernel: times each variant and
  * launch shape (threads per block x blocks per SM) on the current list with

@@ -178,7 +178,8 @@ enum AccSlot {
 };
 // Bits of the device error word (ACC_FLAGS slot).
 enum DevFlag {
-  FLAG_OVERFLOW = 1, FLAG_CAPACITY = 2, FLAG_NONFINITE = 4, FLAG_OUTSIDE = 8, FLAG_CELL = 16
+  FLAG_OVERFLOW = 1, FLAG_CAPACITY = 2, FLAG_NONFINITE = 4, FLAG_OUTSIDE = 8, FLAG_CELL = 16,
+  FLAG_STAGE = 32  // a bulk copy into shared memory did not complete in time
 };
 
 __device__ __forceinline__ void raise_flag(long long *acc, int bit) {

@@ -477,6 +477,10 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
     set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
     return MDBAS_NB_ERR_OVERFLOW;
   }
+  if (a[ACC_FLAGS] & FLAG_STAGE) {
+    set_last_status(MDBAS_NB_ERR_CUDA, "a bulk copy into shared memory timed out");
+    return MDBAS_NB_ERR_CUDA;
+  }
   return MDBAS_NB_OK;
 }
 
@@ -548,7 +552,7 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   struct Cand { int variant, block, bps; };
   std::vector<Cand> cands;
   // the dense kernel takes at most 256 threads per block (launch bounds)
-  for (int variant : {kPairPacked, kPairDense})
+  for (int variant : {kPairPacked, kPairBulk, kPairDense})
     for (int block : {64, 128, 256})
       for (int bps : {2, 4, 8, 16, 32})
         if (block * bps <= 2048 && bps <= 24) cands.push_back({variant, block, bps});
@@ -588,7 +592,8 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
 }
 
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
-  if (!e || (variant != kPairDense && variant != kPairCompact && variant != kPairPacked))
+  if (!e || (variant != kPairDense && variant != kPairCompact && variant != kPairPacked &&
+             variant != kPairBulk))
     return MDBAS_NB_ERR_ARG;
   e->variant = variant;
   return MDBAS_NB_OK;

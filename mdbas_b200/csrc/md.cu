@@ -1242,6 +1242,10 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
       set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
       return MDBAS_NB_ERR_OVERFLOW;
     }
+    if (w[W_FLAGS] & FLAG_STAGE) {
+      set_last_status(MDBAS_NB_ERR_CUDA, "a bulk copy into shared memory timed out");
+      return MDBAS_NB_ERR_CUDA;
+    }
     e->mdRebuilds += w[W_BUILDS];
     e->mdPrunes += w[W_PRUNES];
     for (int k = 0; k < K; ++k) {

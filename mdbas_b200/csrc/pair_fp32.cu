@@ -427,6 +427,245 @@ k_pair_fp32x2(const long long *__restrict__ counters, const int4 *__restrict__ i
 }
 
 // ---------------------------------------------------------------------------
+// Bulk-staged variant (kPairBulk).  The packed kernel's arithmetic and
+// results, with each chunk's j data brought into shared memory by
+// asynchronous bulk copies (cp.async.bulk, completion counted by an mbarrier)
+// instead of per-lane loads: a j cluster's pair-interleaved copies are two
+// contiguous blocks (xp: 128 B, ljp: 64 B), one copy each.  Two buffers per
+// warp: while a chunk is computed the next chunk's copies are in flight and
+// the entries of the one after are being loaded.  Waits are bounded: a copy
+// that does not complete sets FLAG_STAGE and the warp stops.
+// ---------------------------------------------------------------------------
+struct BulkBuf {
+  float4 en[kStage];       // j (as int bits), shift x, y, z
+  uint2 mk[kStage];        // interaction masks
+  float4 jd[kStage * 12];  // per entry: xp (8 float4: h, pair part) then ljp (4 float4: h)
+};
+struct BulkWarp {
+  BulkBuf buf[2];
+  unsigned long long bar[2];
+};
+constexpr unsigned kBulkBytes = 12 * 16;     // bytes copied per entry
+constexpr int kBulkWaitLimit = 1 << 20;      // try_wait rounds before giving up
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long *bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  unsigned long long state;
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 %0, [%1], %2;"
+               : "=l"(state)
+               : "r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("" ::"l"(state));
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bulk_to_smem(void *dst, const void *src, unsigned bytes,
+                                             unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Every lane waits for the buffer's phase (bounded, so each lane's later
+// reads see the copied data); true when all lanes saw it complete.
+__device__ __forceinline__ bool bulk_wait(unsigned long long *bar, unsigned parity) {
+  bool ok = false;
+  for (int r = 0; r < kBulkWaitLimit && !ok; ++r) ok = mbar_try_wait(bar, parity);
+  return __all_sync(0xffffffffu, ok);
+}
+
+// Stage one chunk: entries and masks by the lanes that hold them, then the
+// copies of the j data (the buffer's previous contents were read two chunks
+// ago, before a __syncwarp).
+__device__ __forceinline__ void bulk_issue(BulkBuf &B, unsigned long long *bar, int nc, int lane,
+                                           const CPairEntry &en, const uint2 &mk,
+                                           const float4 *__restrict__ xp,
+                                           const float4 *__restrict__ ljp) {
+  fence_proxy_async_smem();
+  if (lane < nc) {
+    B.en[lane] = make_float4(__int_as_float(en.j), en.sx, en.sy, en.sz);
+    B.mk[lane] = mk;
+  }
+  if (lane == 0) mbar_expect_tx(bar, (unsigned)nc * kBulkBytes);
+  __syncwarp();
+  if (lane < nc) {
+    bulk_to_smem(&B.jd[lane * 12], xp + (size_t)en.j * 8, 128, bar);
+    bulk_to_smem(&B.jd[lane * 12 + 8], ljp + (size_t)en.j * 4, 64, bar);
+  }
+}
+
+template <bool VDW>
+__global__ void __launch_bounds__(256, 3)
+k_pair_fp32x2_bulk(const long long *__restrict__ counters, const int4 *__restrict__ items,
+                   const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
+                   const float4 *__restrict__ xq, const float2 *__restrict__ lj,
+                   const float4 *__restrict__ xp, const float4 *__restrict__ ljp, PairConstF c,
+                   long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
+  __shared__ __align__(16) BulkWarp bw[8];
+  BulkWarp &W = bw[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jh = lane >> 3;
+  const bool up = il & 4, mid = il & 2, lo = il & 1;
+  const int comp = mid ? (lo ? 3 : 2) : (lo ? 1 : 0);
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * fstride;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;
+  long long npair = 0;
+  bool overflow = false;
+  if (lane == 0) {
+    mbar_init(&W.bar[0]);
+    mbar_init(&W.bar[1]);
+    fence_mbar_init();
+    fence_proxy_async_smem();
+  }
+  __syncwarp();
+  unsigned ph0 = 0, ph1 = 0;  // parity of each buffer's next phase
+  int b = 0;                  // buffer of the chunk being computed
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
+    float2 ec = f2(0.f), ev = f2(0.f), vc = f2(0.f), vv = f2(0.f);
+    const int nch = (ne + kStage - 1) / kStage;
+    // chunk 0 now; the entries of chunk 1 into registers
+    CPairEntry nen{};
+    uint2 nmk = make_uint2(0u, 0u);
+    {
+      const int nc = min(kStage, ne);
+      if (lane < nc) {
+        nen = entries[e0 + lane];
+        nmk = masks[e0 + lane];
+      }
+      bulk_issue(W.buf[b], &W.bar[b], nc, lane, nen, nmk, xp, ljp);
+    }
+    if (nch > 1) {
+      const int nc = min(kStage, ne - kStage);
+      if (lane < nc) {
+        nen = entries[e0 + kStage + lane];
+        nmk = masks[e0 + kStage + lane];
+      }
+    }
+    for (int ch = 0; ch < nch; ++ch) {
+      if (ch + 1 < nch) {
+        const int nc1 = min(kStage, ne - (ch + 1) * kStage);
+        bulk_issue(W.buf[b ^ 1], &W.bar[b ^ 1], nc1, lane, nen, nmk, xp, ljp);
+        if (ch + 2 < nch) {
+          const int nc2 = min(kStage, ne - (ch + 2) * kStage);
+          if (lane < nc2) {
+            nen = entries[e0 + (ch + 2) * kStage + lane];
+            nmk = masks[e0 + (ch + 2) * kStage + lane];
+          }
+        }
+      }
+      const unsigned par = b ? ph1 : ph0;
+      if (!bulk_wait(&W.bar[b], par)) {
+        // a copy did not complete: report, give the other buffer's copies
+        // (if any) a bounded time, and stop this warp
+        if (lane == 0) raise_flag(acc, FLAG_STAGE);
+        if (ch + 1 < nch) bulk_wait(&W.bar[b ^ 1], b ? ph0 : ph1);
+        return;
+      }
+      if (b) ph1 ^= 1u; else ph0 ^= 1u;
+      const BulkBuf &S = W.buf[b];
+      const int nc = min(kStage, ne - ch * kStage);
+      for (int k = 0; k < nc; ++k) {
+        const float4 en = S.en[k];
+        const uint2 mk = S.mk[k];
+        const int j = __float_as_int(en.x);
+        const float sx = en.y - xi.x, sy = en.z - xi.y, sz = en.w - xi.z;
+        const float4 p0 = S.jd[k * 12 + jh * 2], p1 = S.jd[k * 12 + jh * 2 + 1],
+                     lp = S.jd[k * 12 + 8 + jh];
+        float2 dx, dy, dz, r2;
+        bool ina, inb;
+        distance2(c, make_float2(p0.x, p0.y), make_float2(p0.z, p0.w), make_float2(p1.x, p1.y),
+                  sx, sy, sz, (mk.x >> lane) & 1u, (mk.y >> lane) & 1u, dx, dy, dz, r2, ina,
+                  inb);
+        const unsigned ba = __ballot_sync(0xffffffffu, ina);
+        const unsigned bb = __ballot_sync(0xffffffffu, inb);
+        if ((ba | bb) == 0u) continue;
+        float2 fx, fy, fz;
+        interact2<VDW>(c, dx, dy, dz, r2, make_float2(p1.z, p1.w), make_float2(lp.x, lp.y),
+                       make_float2(lp.z, lp.w), xi.w, li, ina, inb, fx, fy, fz, ec, ev, vc, vv);
+        fi_x = __fadd2_rn(fi_x, fx);
+        fi_y = __fadd2_rn(fi_y, fy);
+        fi_z = __fadd2_rn(fi_z, fz);
+        npair += __popc(ba) + __popc(bb);
+        const float ax = fx.x, ay = fy.x, az = fz.x, bx = fx.y, by = fy.y, bz = fz.y;
+        float k0 = up ? bx : ax, k1 = up ? by : ay, k2 = up ? bz : az;
+        const float s0 = up ? ax : bx, s1 = up ? ay : by, s2 = up ? az : bz;
+        k0 += __shfl_xor_sync(0xffffffffu, s0, 4);
+        k1 += __shfl_xor_sync(0xffffffffu, s1, 4);
+        k2 += __shfl_xor_sync(0xffffffffu, s2, 4);
+        const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
+        float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
+        u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
+        u1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+        const float w = lo ? u0 : u1;
+        float v = lo ? u1 : u0;
+        v += __shfl_xor_sync(0xffffffffu, w, 1);
+        if (comp < 3 && v != 0.f) {
+          overflow |= !(fabsf(v) < kForceLimitF);
+          red_add(fcomp + j * kClusterSize + (up ? jh + 4 : jh), fix_f(-v));
+        }
+      }
+      __syncwarp();
+      b ^= 1;
+    }
+    float fix = fi_x.x + fi_x.y, fiy = fi_y.x + fi_y.y, fiz = fi_z.x + fi_z.y;
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jh < 3) {
+      const float v = (jh == 0) ? fix : (jh == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)jh * fstride + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    Ec += fix_e(warp_sum_d((double)ec.x + (double)ec.y));
+    Ev += fix_e(warp_sum_d((double)ev.x + (double)ev.y));
+    Vc += fix_e(warp_sum_d((double)vc.x + (double)vc.y));
+    Vv += fix_e(warp_sum_d((double)vv.x + (double)vv.y));
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    red_add(acc + ACC_NPAIR, npair);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Compacted variant.  Same work items, entries and results as k_pair_fp32,
 // but only in-cut-off pairs reach the expensive arithmetic:
 //   staging: a chunk of 8 entries and their 64 j atoms are loaded into shared
@@ -757,6 +996,14 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   DBuf &masks = w.useInner ? w.masksIn : w.masks;
   if (variant == kPairPacked) {
     auto kv = p.vdwSwitch ? k_pair_fp32x2<true> : k_pair_fp32x2<false>;
+    MDB_LAUNCH(kv, grid, block, 0, s, counters.as<long long>(), items.as<int4>(),
+               entries.as<CPairEntry>(), masks.as<uint2>(), w.xq.as<float4>(),
+               w.lj.as<float2>(), w.xp.as<float4>(), w.ljp.as<float4>(), c,
+               w.facc.as<long long>(), w.slotCap, w.acc.as<long long>());
+    return MDBAS_NB_OK;
+  }
+  if (variant == kPairBulk) {
+    auto kv = p.vdwSwitch ? k_pair_fp32x2_bulk<true> : k_pair_fp32x2_bulk<false>;
     MDB_LAUNCH(kv, grid, block, 0, s, counters.as<long long>(), items.as<int4>(),
                entries.as<CPairEntry>(), masks.as<uint2>(), w.xq.as<float4>(),
                w.lj.as<float2>(), w.xp.as<float4>(), w.ljp.as<float4>(), c,

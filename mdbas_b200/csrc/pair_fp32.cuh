@@ -19,7 +19,7 @@ PairConstF make_pair_const(const PairParams &p);
 // Pair kernel variants: dense (all 64 pairs of an entry per warp step, scalar
 // FP32), compacted (only in-cut-off pairs reach the interaction arithmetic)
 // and packed (the dense mapping in f32x2 arithmetic; the default).
-enum { kPairDense = 0, kPairCompact = 1, kPairPacked = 2 };
+enum { kPairDense = 0, kPairCompact = 1, kPairPacked = 2, kPairBulk = 3 };
 // The pair kernel over all work items (grid-stride, item count read on the
 // device, so the launch needs no host synchronisation).  grid*block is the
 // number of threads of the dense variant; the compacted one uses the same

@@ -175,10 +175,16 @@ def test_pair_kernel_variants_agree(gpu):
     eng = nb.Engine(s, precision=1)
     eng.build()
     out = {}
-    for v in (0, 1):
+    for v in (0, 1, 2, 3):
         eng.set_variant(v)
         eng.compute()
         out[v] = (eng.forces(), eng.energies())
+    # packed f32x2 with per-lane loads (2) and with bulk-copy staging (3): the
+    # same arithmetic, bit for bit
+    for k in range(3):
+        assert np.array_equal(out[2][0][k], out[3][0][k])
+    assert out[2][1] == out[3][1]
+    assert force_rel_rms(out[2][0], out[0][0]) < 2e-6
     assert force_rel_rms(out[1][0], out[0][0]) < 2e-6
     assert out[1][1]["n_pairs"] == out[0][1]["n_pairs"]
     e0, e1 = out[0][1], out[1][1]
