@@ -583,9 +583,9 @@ int mdbas_nb_engine_bonded(mdbas_nb_engine *e, double *fx, double *fy, double *f
  * only (MDBAS_NB_ERR_UNSUPPORTED for a batch); call after the topology.
  * Dynamics then add the reciprocal forces every step (inside the step's
  * CUDA graph) and the energy rows' potential holds the reciprocal and
- * non-neutral terms as well.  Explicit Ewald is deterministic; SPME spreads
- * charges with FP64 atomics, so its trajectories agree run to run only to
- * rounding. */
+ * non-neutral terms as well.  Explicit Ewald is deterministic, and so is
+ * SPME when every grid dimension is a multiple of 8 (other grids spread
+ * charges with FP64 atomics and agree run to run only to rounding). */
 int mdbas_nb_engine_set_kspace(mdbas_nb_engine *e, int kind, int m1, int m2, int m3, int nbsp);
 /* The engine's reciprocal term at its current positions: forces added to
  * fx/fy/fz (host arrays, NULL = energy only); out[0] = energy (reciprocal +

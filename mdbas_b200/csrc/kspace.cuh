@@ -30,6 +30,12 @@ struct SpmeWork {
   cufftHandle plan = 0;
   bool planValid = false;
   DBuf qsp, ft, bmod, spl, cell, fr, sums, xyzq, fout;
+  // deterministic spreading: atoms binned by the 8^3 grid tile of their
+  // base cell, each tile's atoms in ascending index order
+  DBuf tileOf, tileCount, tileStart, tileFill, tileList, tileSorted, scanTmp;
+  DBuf halo;         // per tile: the (8 + p - 1)^3 halo box of its atoms' stencils
+  int haloSmem = 0;  // dynamic shared memory the halo kernel is allowed
+  DBuf part;         // per-block partial sums (fixed-order reductions)
   double f1 = 0.;  // (2 pi / V) C of the last launch
   ~SpmeWork() {
     if (planValid) cufftDestroy(plan);

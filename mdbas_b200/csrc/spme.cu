@@ -11,12 +11,15 @@
 // the mean force removed, and the energy sum(Q * (theta conv Q)) with the
 // self and non-neutral terms.  The transforms are cuFFT Z2Z plans in the
 // same row-major layout as fftw_plan_dft_3d(m1, m2, m3); spreading, the
-// influence function and the interpolation are the kernels below (FP64,
-// spreading by FP64 atomics).
+// influence function and the interpolation are the kernels below (FP64).
+// Spreading is deterministic when every grid dimension is a multiple of 8
+// (atoms binned by 8^3 grid tile, one block per tile, no atomics); other
+// grids spread with FP64 atomics.
 #include <cufft.h>
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <complex>
 #include <vector>
 
@@ -55,10 +58,19 @@ __device__ __forceinline__ void bspline(double s, int nbsp, double *bsp, double 
   }
 }
 
-__device__ __forceinline__ int wrap_index(int i, int m) {
-  if (i >= m) i = 0;
-  if (i < 0) i += m;
-  return i;
+// grid index of the stencil point base cell - offset; base cells are stored
+// in [0, m), so one wrap brings it into [0, m) as MDBas's does for atoms in
+// the box (src/spme.c:453-481)
+__device__ __forceinline__ int wrap_index(int i, int m) { return i < 0 ? i + m : i; }
+
+// base cell in [0, m).  MDBas's (int)s lies in [0, m] for atoms in the box
+// (image_update wraps them there before every energy call) and its indices
+// (int)s - a wrap to the same grid points; for atoms further out the
+// periodic image is used, which keeps every grid access in bounds (MDBas
+// folds indices >= m onto plane 0 and leaves the array below -(m - p + 1)).
+__device__ __forceinline__ int cell_mod(int c, int m) {
+  c %= m;
+  return c < 0 ? c + m : c;
 }
 
 // Per atom and dimension (one thread each): the grid coordinate, B-splines
@@ -81,7 +93,7 @@ __global__ void k_spme_splines(int n, SpmeBox b, int m1, int m2, int m3, int nbs
     o[d * nbsp + k] = bp[k];
     o[(3 + d) * nbsp + k] = bd[k];
   }
-  cell[3 * i + d] = (int)s;
+  cell[3 * i + d] = cell_mod((int)s, d == 0 ? m1 : (d == 1 ? m2 : m3));
 }
 
 // Charge spreading: one thread per (atom, first-dimension offset).
@@ -105,13 +117,153 @@ __global__ void k_spme_spread(int n, int m1, int m2, int m3, int nbsp,
   }
 }
 
+// Deterministic spreading.  The grid is cut into 8^3 tiles (every grid
+// dimension a multiple of 8); atoms are binned by the tile of their base
+// cell and each bin is put in ascending atom order.  Phase one, one block per
+// tile: the bin's atoms, one after the other, scatter their p^3 stencils
+// into a shared-memory copy of the tile plus its halo ((8 + p - 1)^3 points:
+// a stencil reaches p - 1 cells below its base cell), one thread per stencil
+// point; the halo boxes go to global memory.  Phase two, one thread per grid
+// point: the sum over the halo boxes that cover the point (its own tile and
+// the next ones upward, as far as the order reaches) in a fixed order.  No
+// atomics: the same sums in the same order on every run.
+constexpr int kSpTile = 8;
+constexpr int kSpBatch = 32;
+constexpr int kSpPts = (kMaxOrder * kMaxOrder * kMaxOrder + 511) / 512;  // per thread
+
+__global__ void k_spme_tile_count(int n, int m1, int m2, int m3, int nt2, int nt3,
+                                  const int *__restrict__ cell, int *__restrict__ tileOf,
+                                  int *__restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int t = ((cell[3 * i] / kSpTile) * nt2 + cell[3 * i + 1] / kSpTile) * nt3 +
+                cell[3 * i + 2] / kSpTile;
+  tileOf[i] = t;
+  atomicAdd(count + t, 1);
+}
+
+__global__ void k_spme_tile_fill(int n, const int *__restrict__ tileOf,
+                                 const int *__restrict__ start, int *__restrict__ fill,
+                                 int *__restrict__ list) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int t = tileOf[i];
+  list[start[t] + atomicAdd(fill + t, 1)] = i;
+}
+
+// one block per bin: its atoms in ascending index order (rank sort)
+__global__ void k_spme_tile_sort(const int *__restrict__ start, const int *__restrict__ list,
+                                 int *__restrict__ sorted) {
+  const int s0 = start[blockIdx.x], s1 = start[blockIdx.x + 1];
+  for (int u = s0 + threadIdx.x; u < s1; u += blockDim.x) {
+    const int a = list[u];
+    int rank = 0;
+    for (int v = s0; v < s1; ++v) rank += list[v] < a;
+    sorted[s0 + rank] = a;
+  }
+}
+
+template <int PTS>  // stencil points per thread: 1 when p^3 <= 512
+__global__ void __launch_bounds__(512, PTS == 1 ? 3 : 2)
+    k_spme_spread_halo(int nbsp, int nt2, int nt3, const double *__restrict__ q,
+                       const double *__restrict__ spl, const int *__restrict__ cell,
+                       const int *__restrict__ start, const int *__restrict__ sorted,
+                       double *__restrict__ halo) {
+  extern __shared__ double hb[];  // (8 + p - 1)^3 halo box
+  __shared__ double sq[kSpBatch];
+  __shared__ int sc[kSpBatch];
+  __shared__ double sb[kSpBatch][3 * kMaxOrder];
+  const int tile = blockIdx.x;
+  const int t3 = tile % nt3, t2 = (tile / nt3) % nt2, t1 = tile / (nt2 * nt3);
+  const int H = kSpTile + nbsp - 1, H3 = H * H * H, p3 = nbsp * nbsp * nbsp;
+  const int th = threadIdx.x;
+  // this thread's stencil points (a, b, c), at most PTS of them
+  int abc[PTS];
+#pragma unroll
+  for (int k = 0; k < PTS; ++k) {
+    const int idx = th + k * 512;
+    abc[k] = idx / (nbsp * nbsp) | ((idx / nbsp) % nbsp) << 8 | (idx % nbsp) << 16;
+  }
+  for (int u = th; u < H3; u += blockDim.x) hb[u] = 0.;
+  const int s0 = start[tile], s1 = start[tile + 1];
+  for (int base = s0; base < s1; base += kSpBatch) {
+    const int cnt = min(kSpBatch, s1 - base);
+    __syncthreads();
+    if (th < cnt) {
+      const int a = sorted[base + th];
+      sq[th] = q[a];
+      // the stencil's top corner in the halo box: base cell - tile origin + p - 1
+      sc[th] = ((cell[3 * a] - kSpTile * t1 + nbsp - 1) * H +
+                (cell[3 * a + 1] - kSpTile * t2 + nbsp - 1)) * H +
+               (cell[3 * a + 2] - kSpTile * t3 + nbsp - 1);
+    }
+    for (int idx = th; idx < cnt * 3 * nbsp; idx += blockDim.x) {
+      const int u = idx / (3 * nbsp), r = idx - u * 3 * nbsp;
+      sb[u][r] = spl[(size_t)sorted[base + u] * 6 * nbsp + r];
+    }
+    __syncthreads();
+    for (int u = 0; u < cnt; ++u) {
+      const double qu = sq[u];
+      const int su = sc[u];
+#pragma unroll
+      for (int k = 0; k < PTS; ++k)
+        if (th + k * 512 < p3) {
+          const int a = abc[k] & 0xff, bb = (abc[k] >> 8) & 0xff, c = abc[k] >> 16;
+          hb[su - (a * H + bb) * H - c] +=
+              ((qu * sb[u][a]) * sb[u][nbsp + bb]) * sb[u][2 * nbsp + c];
+        }
+      __syncthreads();  // the next atom may hit the same points
+    }
+  }
+  __syncthreads();
+  double *out = halo + (size_t)tile * H3;
+  for (int u = th; u < H3; u += blockDim.x) out[u] = hb[u];
+}
+
+// Phase two: grid point g takes, per dimension, the halo boxes of tiles
+// tg + d (d = 0 .. reach - 1, modulo the tile count) at the local coordinate
+// g - 8 (tg + d) + p - 1 when that is >= 0.  Writes the real grid and its
+// complex copy for the FFT.
+__global__ void k_spme_halo_gather(int m1, int m2, int m3, int nbsp, int reach, int nt1,
+                                   int nt2, int nt3, const double *__restrict__ halo,
+                                   double *__restrict__ qsp, cufftDoubleComplex *__restrict__ ft) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long mm = (long long)m1 * m2 * m3;
+  if (t >= mm) return;
+  const int k = (int)(t % m3), j = (int)((t / m3) % m2), i = (int)(t / ((long long)m3 * m2));
+  const int H = kSpTile + nbsp - 1, H3 = H * H * H;
+  const int ti = i / kSpTile, tj = j / kSpTile, tk = k / kSpTile;
+  double acc = 0.;
+  for (int d1 = 0; d1 < reach; ++d1) {
+    const int l1 = i - kSpTile * (ti + d1) + nbsp - 1;
+    if (l1 < 0) break;
+    const int s1 = (ti + d1) % nt1;
+    for (int d2 = 0; d2 < reach; ++d2) {
+      const int l2 = j - kSpTile * (tj + d2) + nbsp - 1;
+      if (l2 < 0) break;
+      const int s2 = (tj + d2) % nt2;
+      for (int d3 = 0; d3 < reach; ++d3) {
+        const int l3 = k - kSpTile * (tk + d3) + nbsp - 1;
+        if (l3 < 0) break;
+        const int s3 = (tk + d3) % nt3;
+        const size_t src = ((size_t)s1 * nt2 + s2) * nt3 + s3;
+        acc += halo[src * H3 + ((size_t)l1 * H + l2) * H + l3];
+      }
+    }
+  }
+  qsp[t] = acc;
+  ft[t] = make_cuDoubleComplex(acc, 0.0);
+}
+
 __global__ void k_spme_pack(long long mm, const double *__restrict__ qsp,
                             cufftDoubleComplex *__restrict__ ft) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < mm) ft[t] = make_cuDoubleComplex(qsp[t], 0.0);
 }
 
-__device__ __forceinline__ void block_add(double v, double *out) {
+// The block's sum of v into part[blockIdx.x] (fixed reduction order);
+// k_spme_sum adds the blocks' partials in block order: run-to-run identical.
+__device__ __forceinline__ void block_add(double v, double *part) {
   __shared__ double red[32];
   v = warp_sum_d(v);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -120,15 +272,34 @@ __device__ __forceinline__ void block_add(double v, double *out) {
   if (w == 0) {
     v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
     v = warp_sum_d(v);
-    if (lane == 0) atomicAdd(out, v);
+    if (lane == 0) part[blockIdx.x] = v;
   }
   __syncthreads();
+}
+
+// dst[q] = sum over b of part[q * nb + b], one block per q: thread t adds
+// the partials t, t + blockDim, ... in order, then a fixed tree.
+__global__ void __launch_bounds__(1024) k_spme_sum(const double *__restrict__ part, int nb,
+                                                   double *__restrict__ dst) {
+  __shared__ double red[32];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const double *p = part + (size_t)blockIdx.x * nb;
+  double v = 0.;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) v += p[b];
+  v = warp_sum_d(v);
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  if (w == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
+    v = warp_sum_d(v);
+    if (lane == 0) dst[blockIdx.x] = v;
+  }
 }
 
 // Influence function and virial (src/spme.c:460-530); stress[6] += ...
 __global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralpha2, double rc2,
                                  const double *__restrict__ bmod,  // m1 + m2 + m3
-                                 cufftDoubleComplex *__restrict__ ft, double *__restrict__ stress) {
+                                 cufftDoubleComplex *__restrict__ ft, double *__restrict__ part) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long mm = (long long)m1 * m2 * m3;
   double s[6] = {0., 0., 0., 0., 0., 0.};
@@ -162,7 +333,7 @@ __global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralph
     }
     ft[t] = f;
   }
-  for (int c = 0; c < 6; ++c) block_add(s[c], stress + c);
+  for (int c = 0; c < 6; ++c) block_add(s[c], part + (size_t)c * gridDim.x);
 }
 
 // Force interpolation (src/spme.c:532-575) into fr[3][n]; sums for the mean.
@@ -223,8 +394,8 @@ __global__ void k_spme_forces(int n, int m1, int m2, int m3, int nbsp, int group
     fr[2 * (size_t)n + l] = fz;
   }
   block_add(fx, fsum);
-  block_add(fy, fsum + 1);
-  block_add(fz, fsum + 2);
+  block_add(fy, fsum + gridDim.x);
+  block_add(fz, fsum + 2 * (size_t)gridDim.x);
 }
 
 // sum over the grid of Re(theta conv Q) * Q
@@ -235,6 +406,93 @@ __global__ void k_spme_energy(long long mm, const cufftDoubleComplex *__restrict
 }
 
 // f += fr - mean (device arrays)
+// Force interpolation per grid tile (same arithmetic per atom as
+// k_spme_forces): the block loads the tile's halo box of the convolved grid
+// (real part; local l is grid point 8 t - (p - 1) + l modulo m) into shared
+// memory, one warp per row, then takes the bin's atoms, `group` lanes per
+// atom.  fsum gets one partial per tile, accumulated in atom order.
+__global__ void __launch_bounds__(256)
+    k_spme_forces_tiled(int n, int m1, int m2, int m3, int nbsp, int group, int nt2, int nt3,
+                        SpmeBox b, double fact1, const double *__restrict__ q,
+                        const double *__restrict__ spl, const int *__restrict__ cell,
+                        const int *__restrict__ start, const int *__restrict__ sorted,
+                        const cufftDoubleComplex *__restrict__ ft, double *__restrict__ fr,
+                        double *__restrict__ fsum) {
+  extern __shared__ double hb[];
+  const int tile = blockIdx.x;
+  const int t3 = tile % nt3, t2 = (tile / nt3) % nt2, t1 = tile / (nt2 * nt3);
+  const int H = kSpTile + nbsp - 1;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int r = w; r < H * H; r += nw) {
+    const int l1 = r / H, l2 = r - l1 * H;
+    int g1 = kSpTile * t1 - (nbsp - 1) + l1, g2 = kSpTile * t2 - (nbsp - 1) + l2;
+    if (g1 < 0) g1 += m1;
+    if (g2 < 0) g2 += m2;
+    const cufftDoubleComplex *row = ft + ((size_t)g1 * m2 + g2) * m3;
+    if (lane < H) {
+      int g3 = kSpTile * t3 - (nbsp - 1) + lane;
+      if (g3 < 0) g3 += m3;
+      hb[r * H + lane] = row[g3].x;
+    }
+  }
+  __syncthreads();
+  const int s0 = start[tile], s1 = start[tile + 1];
+  const int per = blockDim.x / group, a = threadIdx.x % group;
+  double sx = 0., sy = 0., sz = 0.;
+  for (int base = s0; base < s1; base += per) {  // same trip count in the whole block
+    const int u = base + (int)threadIdx.x / group;
+    const int l = u < s1 ? sorted[u] : -1;
+    double px = 0., py = 0., pz = 0.;
+    if (l >= 0 && a < nbsp) {
+      const double *o = spl + (size_t)l * 6 * nbsp;
+      const double *b2 = o + nbsp, *b3 = o + 2 * nbsp;
+      const double *d2 = o + 4 * nbsp, *d3 = o + 5 * nbsp;
+      const int c1 = cell[3 * l] - kSpTile * t1 + nbsp - 1 - a;  // plane a, local
+      const int cy = cell[3 * l + 1] - kSpTile * t2 + nbsp - 1;
+      const int cz = cell[3 * l + 2] - kSpTile * t3 + nbsp - 1;
+      double t1s = 0., t2s = 0., t3s = 0.;
+      for (int bb = 0; bb < nbsp; ++bb) {
+        const double *row = hb + (c1 * H + cy - bb) * H + cz;
+        double sb = 0., sd = 0.;
+        for (int c = 0; c < nbsp; ++c) {
+          const double qt = row[-c];
+          sb += qt * __ldg(b3 + c);
+          sd += qt * __ldg(d3 + c);
+        }
+        const double wb = __ldg(b2 + bb);
+        t1s += wb * sb;
+        t2s += __ldg(d2 + bb) * sb;
+        t3s += wb * sd;
+      }
+      px = __ldg(o + 3 * nbsp + a) * t1s;  // d1_a
+      const double b1a = __ldg(o + a);
+      py = b1a * t2s;
+      pz = b1a * t3s;
+    }
+    for (int o = group >> 1; o > 0; o >>= 1) {
+      px += __shfl_xor_sync(0xffffffffu, px, o);
+      py += __shfl_xor_sync(0xffffffffu, py, o);
+      pz += __shfl_xor_sync(0xffffffffu, pz, o);
+    }
+    if (l >= 0 && a == 0) {
+      const double fbx = px * (double)m1, fby = py * (double)m2, fbz = pz * (double)m3;
+      const double fq = fact1 * q[l];
+      const double fx = fq * (fbx * b.u1 + fby * b.v1 + fbz * b.w1);
+      const double fy = fq * (fbx * b.u2 + fby * b.v2 + fbz * b.w2);
+      const double fz = fq * (fbx * b.u3 + fby * b.v3 + fbz * b.w3);
+      fr[l] = fx;
+      fr[n + l] = fy;
+      fr[2 * (size_t)n + l] = fz;
+      sx += fx;
+      sy += fy;
+      sz += fz;
+    }
+  }
+  block_add(sx, fsum);
+  block_add(sy, fsum + gridDim.x);
+  block_add(sz, fsum + 2 * (size_t)gridDim.x);
+}
+
 __global__ void k_spme_add(int n, const double *__restrict__ fr, const double *__restrict__ fsum,
                            double *__restrict__ fx, double *__restrict__ fy,
                            double *__restrict__ fz) {
@@ -307,6 +565,7 @@ int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_
     c.m3 = m3;
     c.device = dev;
     c.nbsp = 0;
+    c.haloSmem = 0;  // a function attribute is per device
   }
   MDB_TRY(cufft_check(cufftSetStream(c.plan, s), "cufftSetStream"));
   if (c.nbsp != nbsp) {
@@ -324,6 +583,37 @@ int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_
   MDB_TRY(c.cell.ensure(sizeof(int) * 3 * (size_t)n));
   MDB_TRY(c.fr.ensure(sizeof(double) * 3 * (size_t)n));
   MDB_TRY(c.sums.ensure(sizeof(double) * 16));
+  {
+    // per-block partial sums: influence (6 x blocks), forces (3 x blocks),
+    // energy (1 x blocks)
+    const long long gI = (mm + 255) / 256, gF = ((long long)n * 16 + 127) / 128;
+    const long long nt = (long long)(m1 / 8) * (m2 / 8) * (m3 / 8);
+    MDB_TRY(c.part.ensure(sizeof(double) * (size_t)std::max(6 * gI, 3 * std::max(gF, nt))));
+  }
+  {
+    const int nt = (m1 / 8) * (m2 / 8) * (m3 / 8);
+    MDB_TRY(c.tileOf.ensure(sizeof(int) * (size_t)n));
+    MDB_TRY(c.tileList.ensure(sizeof(int) * (size_t)n));
+    MDB_TRY(c.tileSorted.ensure(sizeof(int) * (size_t)n));
+    MDB_TRY(c.tileCount.ensure(sizeof(int) * (size_t)(nt + 1)));
+    MDB_TRY(c.tileStart.ensure(sizeof(int) * (size_t)(nt + 1)));
+    MDB_TRY(c.tileFill.ensure(sizeof(int) * (size_t)(nt + 1)));
+    MDB_TRY(c.scanTmp.ensure(scan_tmp_bytes(nt > 0 ? nt : 1)));
+    if (nt > 0) {
+      const int H = kSpTile + nbsp - 1;
+      const int smem = (int)sizeof(double) * H * H * H;
+      MDB_TRY(c.halo.ensure(sizeof(double) * (size_t)nt * H * H * H));
+      if (smem > c.haloSmem) {  // set once, before any capture of these launches
+        MDB_CUDA(cudaFuncSetAttribute(k_spme_spread_halo<1>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        MDB_CUDA(cudaFuncSetAttribute(k_spme_spread_halo<kSpPts>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        MDB_CUDA(cudaFuncSetAttribute(k_spme_forces_tiled,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        c.haloSmem = smem;
+      }
+    }
+  }
   c.n = n;
   return MDBAS_NB_OK;
 }
@@ -340,29 +630,74 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
   const long long mm = (long long)m1 * m2 * m3;
   double *sums = c.sums.as<double>();  // 0-5 stress, 6-8 force sums, 9 energy
   MDB_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * 16, s));
-  MDB_CUDA(cudaMemsetAsync(c.qsp.p, 0, sizeof(double) * mm, s));
   MDB_LAUNCH(k_spme_splines, grid_for(3LL * n, 128), 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z,
              c.spl.as<double>(), c.cell.as<int>());
-  MDB_LAUNCH(k_spme_spread, grid_for((long long)n * nbsp, 128), 128, 0, s, n, m1, m2, m3, nbsp,
-             q, c.spl.as<double>(), c.cell.as<int>(), c.qsp.as<double>());
-  MDB_LAUNCH(k_spme_pack, grid_for(mm, 256), 256, 0, s, mm, c.qsp.as<double>(),
-             c.ft.as<cufftDoubleComplex>());
+  const bool tiled = m1 % kSpTile == 0 && m2 % kSpTile == 0 && m3 % kSpTile == 0;
+  const int nt1 = m1 / kSpTile, nt2 = m2 / kSpTile, nt3 = m3 / kSpTile;
+  const int nt = nt1 * nt2 * nt3;
+  if (tiled) {
+    // deterministic: bins of atoms per 8^3 tile, one block per tile
+    const int reach = 1 + (nbsp + kSpTile - 2) / kSpTile;  // halo boxes covering a point, per dim
+    int *cnt = c.tileCount.as<int>();
+    MDB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * (size_t)(nt + 1), s));
+    MDB_CUDA(cudaMemsetAsync(c.tileFill.p, 0, sizeof(int) * (size_t)nt, s));
+    MDB_LAUNCH(k_spme_tile_count, grid_for(n, 256), 256, 0, s, n, m1, m2, m3, nt2, nt3,
+               c.cell.as<int>(),
+               c.tileOf.as<int>(), cnt);
+    MDB_TRY(exclusive_scan32(cnt, c.tileStart.as<int>(), nt, c.scanTmp.p, s));
+    MDB_LAUNCH(k_spme_tile_fill, grid_for(n, 256), 256, 0, s, n, c.tileOf.as<int>(),
+               c.tileStart.as<int>(), c.tileFill.as<int>(), c.tileList.as<int>());
+    MDB_LAUNCH(k_spme_tile_sort, nt, 64, 0, s, c.tileStart.as<int>(), c.tileList.as<int>(),
+               c.tileSorted.as<int>());
+    const int H = kSpTile + nbsp - 1;
+    if (nbsp <= 8)
+      MDB_LAUNCH(k_spme_spread_halo<1>, nt, 512, sizeof(double) * H * H * H, s, nbsp, nt2, nt3,
+                 q, c.spl.as<double>(), c.cell.as<int>(), c.tileStart.as<int>(),
+                 c.tileSorted.as<int>(), c.halo.as<double>());
+    else
+      MDB_LAUNCH(k_spme_spread_halo<kSpPts>, nt, 512, sizeof(double) * H * H * H, s, nbsp, nt2,
+                 nt3, q, c.spl.as<double>(), c.cell.as<int>(), c.tileStart.as<int>(),
+                 c.tileSorted.as<int>(), c.halo.as<double>());
+    MDB_LAUNCH(k_spme_halo_gather, grid_for(mm, 256), 256, 0, s, m1, m2, m3, nbsp, reach, nt1,
+               nt2, nt3, c.halo.as<double>(), c.qsp.as<double>(),
+               c.ft.as<cufftDoubleComplex>());
+  } else {
+    MDB_CUDA(cudaMemsetAsync(c.qsp.p, 0, sizeof(double) * mm, s));
+    MDB_LAUNCH(k_spme_spread, grid_for((long long)n * nbsp, 128), 128, 0, s, n, m1, m2, m3,
+               nbsp, q, c.spl.as<double>(), c.cell.as<int>(), c.qsp.as<double>());
+    MDB_LAUNCH(k_spme_pack, grid_for(mm, 256), 256, 0, s, mm, c.qsp.as<double>(),
+               c.ft.as<cufftDoubleComplex>());
+  }
   cufftDoubleComplex *ft = c.ft.as<cufftDoubleComplex>();
   MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_INVERSE), "cufftExecZ2Z"));
   const double rvol = 6.283185307179586 / b.vol;
   const double ralpha2 = -0.25 / (alpha * alpha);
   double rc = fmin((double)m1 * b.u, (double)m2 * b.v);
   rc = fmin(rc, (double)m3 * b.w) * 1.05 * 6.283185307179586;
-  MDB_LAUNCH(k_spme_influence, grid_for(mm, 256), 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
-             c.bmod.as<double>(), ft, sums);
+  const int gI = grid_for(mm, 256);
+  double *part = c.part.as<double>();
+  MDB_LAUNCH(k_spme_influence, gI, 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
+             c.bmod.as<double>(), ft, part);
+  MDB_LAUNCH(k_spme_sum, 6, 1024, 0, s, part, gI, sums);
   MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_FORWARD), "cufftExecZ2Z"));
   int group = 1;
   while (group < nbsp) group <<= 1;
-  MDB_LAUNCH(k_spme_forces, grid_for((long long)n * group, 128), 128, 0, s, n, m1, m2, m3, nbsp,
-             group, b,
-             -2.0 * rvol * chargeConst, q, c.spl.as<double>(), c.cell.as<int>(), ft,
-             c.fr.as<double>(), sums + 6);
-  MDB_LAUNCH(k_spme_energy, grid_for(mm, 256), 256, 0, s, mm, ft, c.qsp.as<double>(), sums + 9);
+  if (tiled) {
+    const int H = kSpTile + nbsp - 1;
+    MDB_LAUNCH(k_spme_forces_tiled, nt, 256, sizeof(double) * H * H * H, s, n, m1, m2, m3,
+               nbsp, group, nt2, nt3, b, -2.0 * rvol * chargeConst, q, c.spl.as<double>(),
+               c.cell.as<int>(), c.tileStart.as<int>(), c.tileSorted.as<int>(), ft,
+               c.fr.as<double>(), part);
+    MDB_LAUNCH(k_spme_sum, 3, 1024, 0, s, part, nt, sums + 6);
+  } else {
+    const int gF = grid_for((long long)n * group, 128);
+    MDB_LAUNCH(k_spme_forces, gF, 128, 0, s, n, m1, m2, m3, nbsp, group, b,
+               -2.0 * rvol * chargeConst, q, c.spl.as<double>(), c.cell.as<int>(), ft,
+               c.fr.as<double>(), part);
+    MDB_LAUNCH(k_spme_sum, 3, 1024, 0, s, part, gF, sums + 6);
+  }
+  MDB_LAUNCH(k_spme_energy, gI, 256, 0, s, mm, ft, c.qsp.as<double>(), part);
+  MDB_LAUNCH(k_spme_sum, 1, 1024, 0, s, part, gI, sums + 9);
   MDB_LAUNCH(k_spme_add, grid_for(n, 256), 256, 0, s, n, c.fr.as<double>(), sums + 6, fx, fy,
              fz);
   c.f1 = rvol * chargeConst;

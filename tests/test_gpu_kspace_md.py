@@ -67,15 +67,16 @@ def test_md_explicit_ewald_matches_mdbas(gpu, ref_available, water):
     assert pot < 1e-6 and tot < 1e-6
 
 
-def test_md_kspace_graph_equals_host_driven(gpu, water):
-    """Explicit Ewald (deterministic) inside the mixed form's 20-step graphs:
-    the trajectory equals the host-driven one bit for bit."""
+@pytest.mark.parametrize("kind,m,order", [(1, M, 0), (2, (32, 32, 32), 6)])
+def test_md_kspace_graph_equals_host_driven(gpu, water, kind, m, order):
+    """Explicit Ewald or SPME (both deterministic) inside the mixed form's
+    20-step graphs: the trajectory equals the host-driven one bit for bit."""
     vel = (water.vx, water.vy, water.vz)
     cons = water.water_constraints()
     out = []
     for graph in (20, 0):
         e = nb.Engine(water, precision=1, **POT)
-        e.set_kspace(1, M)
+        e.set_kspace(kind, m, order)
         e.md_set_graph(graph)
         e.md_init(water.mass, vel, time_step=0.001, list_update=0, constraints=cons)
         rows = e.md_run(40, energy_every=1)

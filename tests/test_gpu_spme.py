@@ -13,8 +13,12 @@ from dropin_util import DropinSystem, force_rel_rms
 pytestmark = pytest.mark.gpu
 
 
+# grids that are multiples of 8 take the binned (deterministic) spreading,
+# the others the atomic one; order 12 reaches three 8^3 tiles per dimension
 @pytest.mark.parametrize("grid,nbsp", [((32, 32, 32), 8), ((64, 64, 64), 8),
-                                       ((32, 32, 32), 4), ((16, 32, 64), 6)])
+                                       ((32, 32, 32), 4), ((16, 32, 64), 6),
+                                       ((20, 24, 36), 8), ((32, 32, 32), 12),
+                                       ((8, 16, 8), 6)])
 def test_spme_matches_restatement(gpu, oracle_lib, grid, nbsp):
     from oracle import spme_oracle as so
     s = systems.water_box(1000, 31.0, seed=3)
@@ -27,6 +31,34 @@ def test_spme_matches_restatement(gpu, oracle_lib, grid, nbsp):
     assert abs(e - er) <= 1e-11 * abs(er)
     assert abs(vir - rvir) <= 1e-10 * abs(rvir)
     assert rel < 1e-10
+
+
+def test_spme_deterministic(gpu):
+    """Binned spreading: two calls give the same bits."""
+    s = systems.water_box(1000, 31.0, seed=5)
+    a = nb.spme(s, alpha=0.34, grid=(32, 32, 32), nbsp=8)
+    b = nb.spme(s, alpha=0.34, grid=(32, 32, 32), nbsp=8)
+    assert a[0] == b[0] and a[4] == b[4]
+    for k in (1, 2, 3):
+        assert np.array_equal(a[k], b[k])
+
+
+def test_spme_atoms_outside_the_box(gpu, oracle_lib):
+    """Atoms whole box lengths beyond the upper faces spread like their
+    images, and every grid access stays in bounds.  (MDBas only sees atoms in
+    the box -- image_update wraps them before each energy call -- and would
+    fold such stencils onto plane 0.)"""
+    s = systems.water_box(1000, 31.0, seed=6)
+    rng = np.random.default_rng(2)
+    shift = 31.0 * rng.integers(0, 3, size=(s.n, 3))
+    moved = systems.System(**{**s.__dict__})
+    moved.x, moved.y, moved.z = s.x + shift[:, 0], s.y + shift[:, 1], s.z + shift[:, 2]
+    for grid in ((32, 32, 32), (20, 24, 36)):   # binned and atomic spreading
+        e0, *f0, v0 = nb.spme(s, alpha=0.34, grid=grid, nbsp=8)
+        e1, *f1, v1 = nb.spme(moved, alpha=0.34, grid=grid, nbsp=8)
+        assert abs(e1 - e0) <= 1e-10 * abs(e0)
+        assert abs(v1 - v0) <= 1e-10 * abs(v0)
+        assert force_rel_rms(f1, f0) < 1e-10
 
 
 def test_spme_orthorhombic_charged(gpu, oracle_lib):
