@@ -39,15 +39,20 @@ struct SpmeBox {
 
 // B-splines and derivatives of one atom in one dimension (bspgen,
 // src/spme.c:269-355): s is the scaled fractional coordinate.
-__device__ __forceinline__ void bspline(double s, int nbsp, double *bsp, double *bsd) {
+template <int P>  // the order, or 0: nbspRun
+__device__ __forceinline__ void bspline(double s, int nbspRun, double *bsp, double *bsd) {
+  const int nbsp = P > 0 ? P : nbspRun;
   const double fr = s - trunc(s);
+#pragma unroll
   for (int k = 0; k < nbsp; ++k) bsp[k] = bsd[k] = 0.;
   bsd[0] = 1.0;
   bsd[1] = -1.0;
   bsp[0] = fr;
   bsp[1] = 1.0 - fr;
+#pragma unroll
   for (int k = 2; k < nbsp; ++k) {
     bsp[k] = 0.0;
+#pragma unroll
     for (int j = k; j > 0; --j) {
       if (k == nbsp - 1) bsd[j] = bsp[j] - bsp[j - 1];
       const double ts = s + (double)j - trunc(s);
@@ -75,21 +80,24 @@ __device__ __forceinline__ int cell_mod(int c, int m) {
 
 // Per atom and dimension (one thread each): the grid coordinate, B-splines
 // (bsp[3][nbsp], bsd[3][nbsp] per atom) and the integer grid cell.
-__global__ void k_spme_splines(int n, SpmeBox b, int m1, int m2, int m3, int nbsp,
+template <int P>  // the order, or 0: nbspRun
+__global__ void k_spme_splines(int n, SpmeBox b, int m1, int m2, int m3, int nbspRun,
                                const double *__restrict__ x, const double *__restrict__ y,
                                const double *__restrict__ z, double *__restrict__ spl,
                                int *__restrict__ cell) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= 3LL * n) return;
-  const int i = (int)(t / 3), d = (int)(t % 3);
+  const int nbsp = P > 0 ? P : nbspRun;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 3 * n) return;
+  const int i = t / 3, d = t - 3 * (t / 3);
   double s;
   if (d == 0) s = (double)m1 * (x[i] * b.u1 + y[i] * b.u2 + z[i] * b.u3 + 0.5);
   else if (d == 1) s = (double)m2 * (x[i] * b.v1 + y[i] * b.v2 + z[i] * b.v3 + 0.5);
   else s = (double)m3 * (x[i] * b.w1 + y[i] * b.w2 + z[i] * b.w3 + 0.5);
   double *o = spl + (size_t)i * 6 * nbsp;
-  double bp[kMaxOrder], bd[kMaxOrder];
-  bspline(s, nbsp, bp, bd);
-  for (int k = 0; k < nbsp; ++k) {
+  double bp[P > 0 ? P : kMaxOrder], bd[P > 0 ? P : kMaxOrder];
+  bspline<P>(s, nbsp, bp, bd);
+#pragma unroll
+  for (int k = 0; k < (P > 0 ? P : nbsp); ++k) {
     o[d * nbsp + k] = bp[k];
     o[(3 + d) * nbsp + k] = bd[k];
   }
@@ -220,17 +228,80 @@ __global__ void __launch_bounds__(512, PTS == 1 ? 3 : 2)
   for (int u = th; u < H3; u += blockDim.x) out[u] = hb[u];
 }
 
+// Phase one for a B-spline order P known at compile time (P <= 9, so the
+// (8 + P - 1)^2 rows of the halo box fit one block): each thread owns one
+// row (l1, l2) of the box, kept in shared memory; an atom covers the row
+// when its stencil planes reach l1 and l2, and then adds ((q b1_a) b2_b) b3_c
+// to the row's points -- the same products, summed over the bin's atoms in
+// the same ascending order, as k_spme_spread_halo, but no thread ever
+// touches another's row: no barrier per atom.
+template <int P>
+__global__ void __launch_bounds__(256)
+    k_spme_spread_rows(int nt2, int nt3, const double *__restrict__ q,
+                       const double *__restrict__ spl, const int *__restrict__ cell,
+                       const int *__restrict__ start, const int *__restrict__ sorted,
+                       double *__restrict__ halo) {
+  constexpr int H = kSpTile + P - 1, H3 = H * H * H;
+  static_assert(H * H <= 256, "one row per thread");
+  __shared__ double hb[H3];
+  __shared__ double sq[kSpBatch];
+  __shared__ int sx[kSpBatch], sy[kSpBatch], sz[kSpBatch];
+  __shared__ double sb[kSpBatch][3 * P];
+  const int tile = blockIdx.x;
+  const int t3 = tile % nt3, t2 = (tile / nt3) % nt2, t1 = tile / (nt2 * nt3);
+  const int th = threadIdx.x;
+  const bool mine = th < H * H;
+  const int l1 = th / H, l2 = th - (th / H) * H;
+  if (mine) {
+#pragma unroll
+    for (int k = 0; k < H; ++k) hb[th * H + k] = 0.;
+  }
+  const int s0 = start[tile], s1 = start[tile + 1];
+  for (int base = s0; base < s1; base += kSpBatch) {
+    const int cnt = min(kSpBatch, s1 - base);
+    __syncthreads();
+    if (th < cnt) {
+      const int a = sorted[base + th];
+      sq[th] = q[a];
+      // the stencil's top corner in the halo box: base cell - tile origin + P - 1
+      sx[th] = cell[3 * a] - kSpTile * t1 + P - 1;
+      sy[th] = cell[3 * a + 1] - kSpTile * t2 + P - 1;
+      sz[th] = cell[3 * a + 2] - kSpTile * t3 + P - 1;
+    }
+    for (int idx = th; idx < cnt * 3 * P; idx += blockDim.x) {
+      const int u = idx / (3 * P), r = idx - u * 3 * P;
+      sb[u][r] = spl[(size_t)sorted[base + u] * 6 * P + r];
+    }
+    __syncthreads();
+    if (mine)
+      for (int u = 0; u < cnt; ++u) {
+        const int a = sx[u] - l1, bb = sy[u] - l2;
+        if ((unsigned)a < (unsigned)P && (unsigned)bb < (unsigned)P) {
+          const double w = (sq[u] * sb[u][a]) * sb[u][P + bb];
+          double *row = hb + th * H + sz[u];  // row[-c], c < P, stays in the row
+#pragma unroll
+          for (int c = 0; c < P; ++c) row[-c] += w * sb[u][2 * P + c];
+        }
+      }
+  }
+  __syncthreads();
+  double *out = halo + (size_t)tile * H3;
+  for (int u = th; u < H3; u += blockDim.x) out[u] = hb[u];
+}
+
 // Phase two: grid point g takes, per dimension, the halo boxes of tiles
 // tg + d (d = 0 .. reach - 1, modulo the tile count) at the local coordinate
 // g - 8 (tg + d) + p - 1 when that is >= 0.  Writes the real grid and its
-// complex copy for the FFT.
+// complex copy for the FFT.  Grid (ceil(m2 m3 / blockDim), m1), plane i =
+// blockIdx.y.
 __global__ void k_spme_halo_gather(int m1, int m2, int m3, int nbsp, int reach, int nt1,
                                    int nt2, int nt3, const double *__restrict__ halo,
                                    double *__restrict__ qsp, cufftDoubleComplex *__restrict__ ft) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long mm = (long long)m1 * m2 * m3;
-  if (t >= mm) return;
-  const int k = (int)(t % m3), j = (int)((t / m3) % m2), i = (int)(t / ((long long)m3 * m2));
+  const int i = blockIdx.y;
+  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t2 >= m2 * m3) return;
+  const long long t = (long long)i * m2 * m3 + t2;
+  const int j = t2 / m3, k = t2 - j * m3;
   const int H = kSpTile + nbsp - 1, H3 = H * H * H;
   const int ti = i / kSpTile, tj = j / kSpTile, tk = k / kSpTile;
   double acc = 0.;
@@ -255,15 +326,58 @@ __global__ void k_spme_halo_gather(int m1, int m2, int m3, int nbsp, int reach, 
   ft[t] = make_cuDoubleComplex(acc, 0.0);
 }
 
+// The same for orders P <= 9 (two halo boxes per dimension at most), fully
+// unrolled: same terms, same order.
+template <int P>
+__global__ void k_spme_halo_gather2(int m2, int m3, int nt1, int nt2, int nt3,
+                                    const double *__restrict__ halo, double *__restrict__ qsp,
+                                    cufftDoubleComplex *__restrict__ ft) {
+  constexpr int H = kSpTile + P - 1, H3 = H * H * H;
+  static_assert(P <= 9, "two halo boxes per dimension");
+  const int i = blockIdx.y;
+  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t2 >= m2 * m3) return;
+  const long long t = (long long)i * m2 * m3 + t2;
+  const int j = t2 / m3, k = t2 - j * m3;
+  const int ti = i / kSpTile, tj = j / kSpTile, tk = k / kSpTile;
+  // local coordinates in the own tile's box (d = 0) and the next one (d = 1)
+  const int l1 = i - kSpTile * ti + P - 1, l2 = j - kSpTile * tj + P - 1,
+            l3 = k - kSpTile * tk + P - 1;
+  const int u1 = ti + 1 == nt1 ? 0 : ti + 1, u2 = tj + 1 == nt2 ? 0 : tj + 1,
+            u3 = tk + 1 == nt3 ? 0 : tk + 1;
+  const bool n1 = l1 >= kSpTile, n2 = l2 >= kSpTile, n3 = l3 >= kSpTile;
+  double acc = 0.;
+#pragma unroll
+  for (int d1 = 0; d1 < 2; ++d1) {
+    if (d1 == 1 && !n1) break;
+    const int s1 = d1 ? u1 : ti, m1l = l1 - kSpTile * d1;
+#pragma unroll
+    for (int d2 = 0; d2 < 2; ++d2) {
+      if (d2 == 1 && !n2) break;
+      const int s2 = d2 ? u2 : tj, m2l = l2 - kSpTile * d2;
+#pragma unroll
+      for (int d3 = 0; d3 < 2; ++d3) {
+        if (d3 == 1 && !n3) break;
+        const int s3 = d3 ? u3 : tk, m3l = l3 - kSpTile * d3;
+        const size_t src = ((size_t)s1 * nt2 + s2) * nt3 + s3;
+        acc += halo[src * H3 + (m1l * H + m2l) * H + m3l];
+      }
+    }
+  }
+  qsp[t] = acc;
+  ft[t] = make_cuDoubleComplex(acc, 0.0);
+}
+
 __global__ void k_spme_pack(long long mm, const double *__restrict__ qsp,
                             cufftDoubleComplex *__restrict__ ft) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (t < mm) ft[t] = make_cuDoubleComplex(qsp[t], 0.0);
 }
 
-// The block's sum of v into part[blockIdx.x] (fixed reduction order);
-// k_spme_sum adds the blocks' partials in block order: run-to-run identical.
-__device__ __forceinline__ void block_add(double v, double *part) {
+// The block's sum of v into part[id] (id: the block's linear index; fixed
+// reduction order); k_spme_sum adds the blocks' partials in block order:
+// run-to-run identical.
+__device__ __forceinline__ void block_add(double v, double *part, int id) {
   __shared__ double red[32];
   v = warp_sum_d(v);
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -272,7 +386,7 @@ __device__ __forceinline__ void block_add(double v, double *part) {
   if (w == 0) {
     v = lane < (int)(blockDim.x >> 5) ? red[lane] : 0.0;
     v = warp_sum_d(v);
-    if (lane == 0) part[blockIdx.x] = v;
+    if (lane == 0) part[id] = v;
   }
   __syncthreads();
 }
@@ -297,14 +411,16 @@ __global__ void __launch_bounds__(1024) k_spme_sum(const double *__restrict__ pa
 }
 
 // Influence function and virial (src/spme.c:460-530); stress[6] += ...
+// Grid (ceil(m2 m3 / blockDim), m1): plane i = blockIdx.y, no 64-bit division.
 __global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralpha2, double rc2,
                                  const double *__restrict__ bmod,  // m1 + m2 + m3
                                  cufftDoubleComplex *__restrict__ ft, double *__restrict__ part) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long mm = (long long)m1 * m2 * m3;
+  const int i = blockIdx.y;
+  const int t2 = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)i * m2 * m3 + t2;
   double s[6] = {0., 0., 0., 0., 0., 0.};
-  if (t < mm) {
-    const int k = (int)(t % m3), j = (int)((t / m3) % m2), i = (int)(t / ((long long)m3 * m2));
+  if (t2 < m2 * m3) {
+    const int j = t2 / m3, k = t2 - j * m3;
     const int ii = i > m1 / 2 ? i - m1 : i, jj = j > m2 / 2 ? j - m2 : j,
               kk = k > m3 / 2 ? k - m3 : k;
     const double tw = 6.283185307179586;
@@ -333,7 +449,8 @@ __global__ void k_spme_influence(int m1, int m2, int m3, SpmeBox b, double ralph
     }
     ft[t] = f;
   }
-  for (int c = 0; c < 6; ++c) block_add(s[c], part + (size_t)c * gridDim.x);
+  const int nb = gridDim.x * gridDim.y, id = blockIdx.y * gridDim.x + blockIdx.x;
+  for (int c = 0; c < 6; ++c) block_add(s[c], part + (size_t)c * nb, id);
 }
 
 // Force interpolation (src/spme.c:532-575) into fr[3][n]; sums for the mean.
@@ -393,46 +510,58 @@ __global__ void k_spme_forces(int n, int m1, int m2, int m3, int nbsp, int group
     fr[n + l] = fy;
     fr[2 * (size_t)n + l] = fz;
   }
-  block_add(fx, fsum);
-  block_add(fy, fsum + gridDim.x);
-  block_add(fz, fsum + 2 * (size_t)gridDim.x);
+  block_add(fx, fsum, blockIdx.x);
+  block_add(fy, fsum + gridDim.x, blockIdx.x);
+  block_add(fz, fsum + 2 * (size_t)gridDim.x, blockIdx.x);
 }
 
 // sum over the grid of Re(theta conv Q) * Q
 __global__ void k_spme_energy(long long mm, const cufftDoubleComplex *__restrict__ ft,
                               const double *__restrict__ qsp, double *__restrict__ out) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  block_add(t < mm ? ft[t].x * qsp[t] : 0.0, out);
+  block_add(t < mm ? ft[t].x * qsp[t] : 0.0, out, blockIdx.x);
 }
 
-// f += fr - mean (device arrays)
 // Force interpolation per grid tile (same arithmetic per atom as
 // k_spme_forces): the block loads the tile's halo box of the convolved grid
 // (real part; local l is grid point 8 t - (p - 1) + l modulo m) into shared
 // memory, one warp per row, then takes the bin's atoms, `group` lanes per
 // atom.  fsum gets one partial per tile, accumulated in atom order.
+template <int P>  // the B-spline order, or 0: given at run time
 __global__ void __launch_bounds__(256)
-    k_spme_forces_tiled(int n, int m1, int m2, int m3, int nbsp, int group, int nt2, int nt3,
+    k_spme_forces_tiled(int n, int m1, int m2, int m3, int nbspRun, int group, int nt2, int nt3,
                         SpmeBox b, double fact1, const double *__restrict__ q,
                         const double *__restrict__ spl, const int *__restrict__ cell,
                         const int *__restrict__ start, const int *__restrict__ sorted,
                         const cufftDoubleComplex *__restrict__ ft, double *__restrict__ fr,
                         double *__restrict__ fsum) {
   extern __shared__ double hb[];
+  const int nbsp = P > 0 ? P : nbspRun;
   const int tile = blockIdx.x;
   const int t3 = tile % nt3, t2 = (tile / nt3) % nt2, t1 = tile / (nt2 * nt3);
   const int H = kSpTile + nbsp - 1;
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-  for (int r = w; r < H * H; r += nw) {
-    const int l1 = r / H, l2 = r - l1 * H;
-    int g1 = kSpTile * t1 - (nbsp - 1) + l1, g2 = kSpTile * t2 - (nbsp - 1) + l2;
-    if (g1 < 0) g1 += m1;
-    if (g2 < 0) g2 += m2;
-    const cufftDoubleComplex *row = ft + ((size_t)g1 * m2 + g2) * m3;
-    if (lane < H) {
-      int g3 = kSpTile * t3 - (nbsp - 1) + lane;
-      if (g3 < 0) g3 += m3;
-      hb[r * H + lane] = row[g3].x;
+  int g3 = kSpTile * t3 - (nbsp - 1) + lane;
+  if (g3 < 0) g3 += m3;
+  // four rows per warp in flight
+  for (int r0 = w; r0 < H * H; r0 += 4 * nw) {
+    double v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = r0 + k * nw;
+      v[k] = 0.;
+      if (r < H * H && lane < H) {
+        const int l1 = r / H, l2 = r - l1 * H;
+        int g1 = kSpTile * t1 - (nbsp - 1) + l1, g2 = kSpTile * t2 - (nbsp - 1) + l2;
+        if (g1 < 0) g1 += m1;
+        if (g2 < 0) g2 += m2;
+        v[k] = ft[((size_t)g1 * m2 + g2) * m3 + g3].x;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int r = r0 + k * nw;
+      if (r < H * H && lane < H) hb[r * H + lane] = v[k];
     }
   }
   __syncthreads();
@@ -451,18 +580,42 @@ __global__ void __launch_bounds__(256)
       const int cy = cell[3 * l + 1] - kSpTile * t2 + nbsp - 1;
       const int cz = cell[3 * l + 2] - kSpTile * t3 + nbsp - 1;
       double t1s = 0., t2s = 0., t3s = 0.;
-      for (int bb = 0; bb < nbsp; ++bb) {
-        const double *row = hb + (c1 * H + cy - bb) * H + cz;
-        double sb = 0., sd = 0.;
-        for (int c = 0; c < nbsp; ++c) {
-          const double qt = row[-c];
-          sb += qt * __ldg(b3 + c);
-          sd += qt * __ldg(d3 + c);
+      if constexpr (P > 0) {
+        double rb3[P], rd3[P];
+#pragma unroll
+        for (int c = 0; c < P; ++c) {
+          rb3[c] = __ldg(b3 + c);
+          rd3[c] = __ldg(d3 + c);
         }
-        const double wb = __ldg(b2 + bb);
-        t1s += wb * sb;
-        t2s += __ldg(d2 + bb) * sb;
-        t3s += wb * sd;
+#pragma unroll
+        for (int bb = 0; bb < P; ++bb) {
+          const double *row = hb + (c1 * H + cy - bb) * H + cz;
+          double sb = 0., sd = 0.;
+#pragma unroll
+          for (int c = 0; c < P; ++c) {
+            const double qt = row[-c];
+            sb += qt * rb3[c];
+            sd += qt * rd3[c];
+          }
+          const double wb = __ldg(b2 + bb);
+          t1s += wb * sb;
+          t2s += __ldg(d2 + bb) * sb;
+          t3s += wb * sd;
+        }
+      } else {
+        for (int bb = 0; bb < nbsp; ++bb) {
+          const double *row = hb + (c1 * H + cy - bb) * H + cz;
+          double sb = 0., sd = 0.;
+          for (int c = 0; c < nbsp; ++c) {
+            const double qt = row[-c];
+            sb += qt * __ldg(b3 + c);
+            sd += qt * __ldg(d3 + c);
+          }
+          const double wb = __ldg(b2 + bb);
+          t1s += wb * sb;
+          t2s += __ldg(d2 + bb) * sb;
+          t3s += wb * sd;
+        }
       }
       px = __ldg(o + 3 * nbsp + a) * t1s;  // d1_a
       const double b1a = __ldg(o + a);
@@ -488,11 +641,12 @@ __global__ void __launch_bounds__(256)
       sz += fz;
     }
   }
-  block_add(sx, fsum);
-  block_add(sy, fsum + gridDim.x);
-  block_add(sz, fsum + 2 * (size_t)gridDim.x);
+  block_add(sx, fsum, blockIdx.x);
+  block_add(sy, fsum + gridDim.x, blockIdx.x);
+  block_add(sz, fsum + 2 * (size_t)gridDim.x, blockIdx.x);
 }
 
+// f += fr - mean (device arrays)
 __global__ void k_spme_add(int n, const double *__restrict__ fr, const double *__restrict__ fsum,
                            double *__restrict__ fx, double *__restrict__ fy,
                            double *__restrict__ fz) {
@@ -552,6 +706,8 @@ int cufft_check(cufftResult r, const char *what) {
 
 // Grid-size dependent state: plan, moduli, grid buffers.
 int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_t s) {
+  // planes on the y grid dimension, 32-bit plane and atom indices
+  if (m1 > 65535 || (long long)m2 * m3 > (1LL << 30) || n > (1 << 28)) return MDBAS_NB_ERR_ARG;
   int dev = 0;
   MDB_CUDA(cudaGetDevice(&dev));
   const long long mm = (long long)m1 * m2 * m3;
@@ -586,7 +742,7 @@ int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_
   {
     // per-block partial sums: influence (6 x blocks), forces (3 x blocks),
     // energy (1 x blocks)
-    const long long gI = (mm + 255) / 256, gF = ((long long)n * 16 + 127) / 128;
+    const long long gI = ((long long)m2 * m3 + 255) / 256 * m1, gF = ((long long)n * 16 + 127) / 128;
     const long long nt = (long long)(m1 / 8) * (m2 / 8) * (m3 / 8);
     MDB_TRY(c.part.ensure(sizeof(double) * (size_t)std::max(6 * gI, 3 * std::max(gF, nt))));
   }
@@ -608,7 +764,7 @@ int spme_setup(SpmeWork &c, int n, int m1, int m2, int m3, int nbsp, cudaStream_
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         MDB_CUDA(cudaFuncSetAttribute(k_spme_spread_halo<kSpPts>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-        MDB_CUDA(cudaFuncSetAttribute(k_spme_forces_tiled,
+        MDB_CUDA(cudaFuncSetAttribute(k_spme_forces_tiled<0>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         c.haloSmem = smem;
       }
@@ -630,8 +786,19 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
   const long long mm = (long long)m1 * m2 * m3;
   double *sums = c.sums.as<double>();  // 0-5 stress, 6-8 force sums, 9 energy
   MDB_CUDA(cudaMemsetAsync(sums, 0, sizeof(double) * 16, s));
-  MDB_LAUNCH(k_spme_splines, grid_for(3LL * n, 128), 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z,
-             c.spl.as<double>(), c.cell.as<int>());
+  {
+    const int g = grid_for(3LL * n, 128);
+    double *spl = c.spl.as<double>();
+    int *cel = c.cell.as<int>();
+    if (nbsp == 8)
+      MDB_LAUNCH(k_spme_splines<8>, g, 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z, spl, cel);
+    else if (nbsp == 6)
+      MDB_LAUNCH(k_spme_splines<6>, g, 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z, spl, cel);
+    else if (nbsp == 4)
+      MDB_LAUNCH(k_spme_splines<4>, g, 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z, spl, cel);
+    else
+      MDB_LAUNCH(k_spme_splines<0>, g, 128, 0, s, n, b, m1, m2, m3, nbsp, x, y, z, spl, cel);
+  }
   const bool tiled = m1 % kSpTile == 0 && m2 % kSpTile == 0 && m3 % kSpTile == 0;
   const int nt1 = m1 / kSpTile, nt2 = m2 / kSpTile, nt3 = m3 / kSpTile;
   const int nt = nt1 * nt2 * nt3;
@@ -650,7 +817,17 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
     MDB_LAUNCH(k_spme_tile_sort, nt, 64, 0, s, c.tileStart.as<int>(), c.tileList.as<int>(),
                c.tileSorted.as<int>());
     const int H = kSpTile + nbsp - 1;
-    if (nbsp <= 8)
+    const int *tst = c.tileStart.as<int>(), *tso = c.tileSorted.as<int>();
+    const double *spl = c.spl.as<double>();
+    const int *cel = c.cell.as<int>();
+    double *hal = c.halo.as<double>();
+    if (nbsp == 8)
+      MDB_LAUNCH(k_spme_spread_rows<8>, nt, 256, 0, s, nt2, nt3, q, spl, cel, tst, tso, hal);
+    else if (nbsp == 6)
+      MDB_LAUNCH(k_spme_spread_rows<6>, nt, 256, 0, s, nt2, nt3, q, spl, cel, tst, tso, hal);
+    else if (nbsp == 4)
+      MDB_LAUNCH(k_spme_spread_rows<4>, nt, 256, 0, s, nt2, nt3, q, spl, cel, tst, tso, hal);
+    else if (nbsp <= 8)
       MDB_LAUNCH(k_spme_spread_halo<1>, nt, 512, sizeof(double) * H * H * H, s, nbsp, nt2, nt3,
                  q, c.spl.as<double>(), c.cell.as<int>(), c.tileStart.as<int>(),
                  c.tileSorted.as<int>(), c.halo.as<double>());
@@ -658,9 +835,18 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
       MDB_LAUNCH(k_spme_spread_halo<kSpPts>, nt, 512, sizeof(double) * H * H * H, s, nbsp, nt2,
                  nt3, q, c.spl.as<double>(), c.cell.as<int>(), c.tileStart.as<int>(),
                  c.tileSorted.as<int>(), c.halo.as<double>());
-    MDB_LAUNCH(k_spme_halo_gather, grid_for(mm, 256), 256, 0, s, m1, m2, m3, nbsp, reach, nt1,
-               nt2, nt3, c.halo.as<double>(), c.qsp.as<double>(),
-               c.ft.as<cufftDoubleComplex>());
+    const dim3 gg(grid_for((long long)m2 * m3, 256), m1);
+    double *qs = c.qsp.as<double>();
+    cufftDoubleComplex *fc = c.ft.as<cufftDoubleComplex>();
+    if (nbsp == 8)
+      MDB_LAUNCH(k_spme_halo_gather2<8>, gg, 256, 0, s, m2, m3, nt1, nt2, nt3, hal, qs, fc);
+    else if (nbsp == 6)
+      MDB_LAUNCH(k_spme_halo_gather2<6>, gg, 256, 0, s, m2, m3, nt1, nt2, nt3, hal, qs, fc);
+    else if (nbsp == 4)
+      MDB_LAUNCH(k_spme_halo_gather2<4>, gg, 256, 0, s, m2, m3, nt1, nt2, nt3, hal, qs, fc);
+    else
+      MDB_LAUNCH(k_spme_halo_gather, gg, 256, 0, s, m1, m2, m3, nbsp, reach, nt1, nt2, nt3, hal,
+                 qs, fc);
   } else {
     MDB_CUDA(cudaMemsetAsync(c.qsp.p, 0, sizeof(double) * mm, s));
     MDB_LAUNCH(k_spme_spread, grid_for((long long)n * nbsp, 128), 128, 0, s, n, m1, m2, m3,
@@ -674,9 +860,9 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
   const double ralpha2 = -0.25 / (alpha * alpha);
   double rc = fmin((double)m1 * b.u, (double)m2 * b.v);
   rc = fmin(rc, (double)m3 * b.w) * 1.05 * 6.283185307179586;
-  const int gI = grid_for(mm, 256);
+  const int gx = grid_for((long long)m2 * m3, 256), gI = gx * m1, gE = grid_for(mm, 256);
   double *part = c.part.as<double>();
-  MDB_LAUNCH(k_spme_influence, gI, 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
+  MDB_LAUNCH(k_spme_influence, dim3(gx, m1), 256, 0, s, m1, m2, m3, b, ralpha2, rc * rc,
              c.bmod.as<double>(), ft, part);
   MDB_LAUNCH(k_spme_sum, 6, 1024, 0, s, part, gI, sums);
   MDB_TRY(cufft_check(cufftExecZ2Z(c.plan, ft, ft, CUFFT_FORWARD), "cufftExecZ2Z"));
@@ -684,10 +870,24 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
   while (group < nbsp) group <<= 1;
   if (tiled) {
     const int H = kSpTile + nbsp - 1;
-    MDB_LAUNCH(k_spme_forces_tiled, nt, 256, sizeof(double) * H * H * H, s, n, m1, m2, m3,
-               nbsp, group, nt2, nt3, b, -2.0 * rvol * chargeConst, q, c.spl.as<double>(),
-               c.cell.as<int>(), c.tileStart.as<int>(), c.tileSorted.as<int>(), ft,
-               c.fr.as<double>(), part);
+    const size_t smem = sizeof(double) * H * H * H;
+    const double f2 = -2.0 * rvol * chargeConst;
+    const int *tst = c.tileStart.as<int>(), *tso = c.tileSorted.as<int>();
+    const double *spl = c.spl.as<double>();
+    const int *cel = c.cell.as<int>();
+    double *frr = c.fr.as<double>();
+    if (nbsp == 8)
+      MDB_LAUNCH(k_spme_forces_tiled<8>, nt, 256, smem, s, n, m1, m2, m3, nbsp, group, nt2, nt3,
+                 b, f2, q, spl, cel, tst, tso, ft, frr, part);
+    else if (nbsp == 6)
+      MDB_LAUNCH(k_spme_forces_tiled<6>, nt, 256, smem, s, n, m1, m2, m3, nbsp, group, nt2, nt3,
+                 b, f2, q, spl, cel, tst, tso, ft, frr, part);
+    else if (nbsp == 4)
+      MDB_LAUNCH(k_spme_forces_tiled<4>, nt, 256, smem, s, n, m1, m2, m3, nbsp, group, nt2, nt3,
+                 b, f2, q, spl, cel, tst, tso, ft, frr, part);
+    else
+      MDB_LAUNCH(k_spme_forces_tiled<0>, nt, 256, smem, s, n, m1, m2, m3, nbsp, group, nt2, nt3,
+                 b, f2, q, spl, cel, tst, tso, ft, frr, part);
     MDB_LAUNCH(k_spme_sum, 3, 1024, 0, s, part, nt, sums + 6);
   } else {
     const int gF = grid_for((long long)n * group, 128);
@@ -696,8 +896,8 @@ int spme_launch_impl(SpmeWork &c, int n, const PBC *box, double alpha, double ch
                c.fr.as<double>(), part);
     MDB_LAUNCH(k_spme_sum, 3, 1024, 0, s, part, gF, sums + 6);
   }
-  MDB_LAUNCH(k_spme_energy, gI, 256, 0, s, mm, ft, c.qsp.as<double>(), part);
-  MDB_LAUNCH(k_spme_sum, 1, 1024, 0, s, part, gI, sums + 9);
+  MDB_LAUNCH(k_spme_energy, gE, 256, 0, s, mm, ft, c.qsp.as<double>(), part);
+  MDB_LAUNCH(k_spme_sum, 1, 1024, 0, s, part, gE, sums + 9);
   MDB_LAUNCH(k_spme_add, grid_for(n, 256), 256, 0, s, n, c.fr.as<double>(), sums + 6, fx, fy,
              fz);
   c.f1 = rvol * chargeConst;
