@@ -218,7 +218,10 @@ struct SearchBuf {
   int nreal[kBufCap];
   float4 sh[kBufCap];                  // FP32 shift: j origin + image - i origin
   uint2 mask[kItemMax];
-  float4 sj[kItemMax * kClusterSize];  // staged j atoms (xq) of the entries
+  float4 sj[kClusterSize * kItemMax];  // staged j atoms (xq), sj[j * kItemMax + entry]
+  float4 si[kClusterSize];             // the i cluster's atoms (xq)
+  int ps[kClusterSize][kExclRegs];     // per i atom: its first exclusion partners' slots
+  int es[kClusterSize], ee[kClusterSize];  // per i atom: its range of exclFlat
 };
 
 // Columns within reach of one i cluster, listed for the flat candidate scan.
@@ -230,77 +233,88 @@ struct SearchCols {
   int prefix[kSearchCols + 1];  // cluster counts before the column
 };
 
-// Flush the first cnt (<= kItemMax) buffered entries as one work item.  Each
-// entry's 64-bit interaction mask is built with two ballots: lane L decides
-// pairs (i = L%8, j = L/8) and (i = L%8, j = L/8 + 4).  Exclusions come from
-// the lane's partner slots (registers; a global-memory loop for atoms with
-// more than kExclRegs partners), checked only for entries whose j cluster
-// holds a partner of some lane's i atom (pc0/pc1: the clusters of a lane's
-// first two partners; atoms with more partners fall back to the warp's
-// partner-cluster range [pcLo, pcHi]).
+// Flush the first cnt (<= kItemMax) buffered entries as one work item.  Lane
+// k builds entry k's 64-bit interaction mask on its own: bit i + 8 j (j < 4
+// in .x, j >= 4 in .y at i + 8 (j - 4)) for the pair (i atom i, j atom j)
+// within the list radius, both slots real, j > i on the cluster's own entry,
+// not an exclusion (checked only when the j cluster lies in the range of
+// clusters holding a partner of the i cluster's atoms: [pcLo, pcHi]) and not
+// both frozen.  The j clusters are staged transposed so that the 32 lanes
+// read 32 different entries without bank conflicts.
 __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double4 oi,
-                           const float4 xi, const float4 *__restrict__ xq,
-                           const ClusterGeom &g, int nreal_i, const int (&ps)[kExclRegs], int nps,
-                           int pc0, int pc1, int pcLo, int pcHi,
-                           int es, int ee, int fi, const int *__restrict__ exclFlat,
-                           const int *__restrict__ slotOf, const int *__restrict__ slotAtom,
-                           const int *__restrict__ frozen, const double4 *__restrict__ origin,
+                           const float4 *__restrict__ xq, const ClusterGeom &g, int nreal_i,
+                           int pcLo, int pcHi, unsigned fimask,
+                           const int *__restrict__ exclFlat, const int *__restrict__ slotOf,
+                           const int *__restrict__ slotAtom, const int *__restrict__ frozen,
+                           const double4 *__restrict__ origin,
                            CPairEntry *__restrict__ entries, uint2 *__restrict__ masks,
                            int4 *__restrict__ items, long long *__restrict__ counters,
                            long long entryCap, long long itemCap) {
-  const int il = lane & 7, jl = lane >> 3;
-  // stage every entry's j cluster first: all loads of the flush in flight
-  // together
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
-    const int idx = lane + 32 * r, k = idx >> 3;
-    if (k < cnt) B.sj[idx] = xq[B.j[k] * kClusterSize + (idx & 7)];
+    const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
+    if (k < cnt) B.sj[j * kItemMax + k] = xq[B.j[k] * kClusterSize + j];
   }
   __syncwarp();
-  for (int k = 0; k < cnt; ++k) {
-    const int cj = B.j[k];
-    const int nrj = B.nreal[k];
-    const int sidx = B.sidx[k];
-    const bool selfzero = (cj == ci) && (sidx == 13);
-    // pair distances at build time: only pairs within the list radius are
-    // kept (FP32 shift from the FP32 origins; rlist2 carries a 1e-5 margin)
+  if (lane < cnt) {
+    const int k = lane;
+    const int cj = B.j[k], nrj = B.nreal[k];
     const float4 sh = B.sh[k];
-    const float tx = sh.x - xi.x, ty = sh.y - xi.y, tz = sh.z - xi.z;
-    const float4 xa = B.sj[k * kClusterSize + jl], xb = B.sj[k * kClusterSize + jl + 4];
-    const float ax = xa.x + tx, ay = xa.y + ty, az = xa.z + tz;
-    const float bx = xb.x + tx, by = xb.y + ty, bz = xb.z + tz;
-    bool oka = (il < nreal_i) && (jl < nrj) && (ax * ax + ay * ay + az * az <= g.rlist2);
-    bool okb = (il < nreal_i) && (jl + 4 < nrj) && (bx * bx + by * by + bz * bz <= g.rlist2);
-    if (selfzero) {
-      oka = oka && (jl > il);
-      okb = okb && (jl + 4 > il);
-    }
-    const int sa = cj * kClusterSize + jl, sb = sa + 4;
-    const bool hit = cj == pc0 || cj == pc1 || (nps > 2 && cj >= pcLo && cj <= pcHi);
-    if (__any_sync(0xffffffffu, hit)) {
+    float jx[kClusterSize], jy[kClusterSize], jz[kClusterSize];
 #pragma unroll
-      for (int r = 0; r < kExclRegs; ++r) {
-        if (r < nps) {
-          oka = oka && (ps[r] != sa);
-          okb = okb && (ps[r] != sb);
-        }
+    for (int j = 0; j < kClusterSize; ++j) {
+      const float4 v = B.sj[j * kItemMax + k];
+      jx[j] = v.x;
+      jy[j] = v.y;
+      jz[j] = v.z;
+    }
+    unsigned lo = 0u, hi = 0u;
+#pragma unroll
+    for (int i = 0; i < kClusterSize; ++i) {
+      // pair distances at build time: FP32 shift from the FP32 origins
+      // (rlist2 carries a 1e-5 margin)
+      const float4 xi = B.si[i];
+      const float tx = sh.x - xi.x, ty = sh.y - xi.y, tz = sh.z - xi.z;
+#pragma unroll
+      for (int j = 0; j < kClusterSize; ++j) {
+        const float ax = jx[j] + tx, ay = jy[j] + ty, az = jz[j] + tz;
+        const unsigned in = (ax * ax + ay * ay + az * az <= g.rlist2) ? 1u : 0u;
+        if (j < 4) lo |= in << (i + 8 * j);
+        else hi |= in << (i + 8 * (j - 4));
       }
-      if (nps > kExclRegs) {
-        for (int e = es + kExclRegs; e < ee; ++e) {
-          const int p = slotOf[__ldg(exclFlat + e)];
-          oka = oka && (p != sa);
-          okb = okb && (p != sb);
+    }
+    // padding slots of either cluster
+    const unsigned irow = (nreal_i >= 8 ? 0xffu : ((1u << nreal_i) - 1u)) * 0x01010101u;
+    lo &= irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
+    hi &= irow & (nrj >= 8 ? 0xffffffffu : (nrj <= 4 ? 0u : ((1u << (8 * (nrj - 4))) - 1u)));
+    if (cj == ci && B.sidx[k] == 13) {  // the cluster with itself: j > i
+      lo &= 0x07030100u;
+      hi &= 0x7f3f1f0fu;
+    }
+    if (cj >= pcLo && cj <= pcHi) {
+      for (int i = 0; i < kClusterSize; ++i) {
+        const int e0 = B.es[i], n = B.ee[i] - e0;
+        for (int r = 0; r < n; ++r) {
+          const int p = r < kExclRegs ? B.ps[i][r] : slotOf[__ldg(exclFlat + e0 + r)];
+          if ((p >> 3) == cj) {
+            const int j = p & 7;
+            if (j < 4) lo &= ~(1u << (i + 8 * j));
+            else hi &= ~(1u << (i + 8 * (j - 4)));
+          }
         }
       }
     }
-    if (frozen && fi) {
-      const int ja = slotAtom[sa], jb = slotAtom[sb];
-      if (oka && ja >= 0 && frozen[ja]) oka = false;
-      if (okb && jb >= 0 && frozen[jb]) okb = false;
+    if (frozen && fimask) {
+      for (int j = 0; j < kClusterSize; ++j) {
+        const int ja = slotAtom[cj * kClusterSize + j];
+        if (ja >= 0 && frozen[ja]) {
+          const unsigned m = fimask << (8 * (j & 3));
+          if (j < 4) lo &= ~m;
+          else hi &= ~m;
+        }
+      }
     }
-    const unsigned mlo = __ballot_sync(0xffffffffu, oka);
-    const unsigned mhi = __ballot_sync(0xffffffffu, okb);
-    if (lane == 0) B.mask[k] = make_uint2(mlo, mhi);
+    B.mask[k] = make_uint2(lo, hi);
   }
   __syncwarp();
   // keep the entries with at least one pair within the list radius
@@ -391,10 +405,16 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   }
   pcLo = __reduce_min_sync(0xffffffffu, pcLo);
   pcHi = __reduce_max_sync(0xffffffffu, pcHi);
-  const int pc0 = nps > 0 ? ps[0] / kClusterSize : -1;
-  const int pc1 = nps > 1 ? ps[1] / kClusterSize : -1;
   const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
-  const float4 xi = xq[ci * kClusterSize + (lane & 7)];
+  const unsigned fimask = __ballot_sync(0xffffffffu, lane < kClusterSize && fi) & 0xffu;
+  if (lane < kClusterSize) {
+    B.si[lane] = xq[ci * kClusterSize + lane];
+#pragma unroll
+    for (int r = 0; r < kExclRegs; ++r) B.ps[lane][r] = ps[r];
+    B.es[lane] = es;
+    B.ee[lane] = ee;
+  }
+  __syncwarp();
 
   const float rl = sqrtf(g.rlist2);
   const float Lx = (float)g.Lx, Ly = (float)g.Ly, Lz = (float)g.Lz;
@@ -549,9 +569,9 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
         cnt += __popc(m);
         __syncwarp();
         if (cnt >= kItemMax) {
-          flush_item(B, kItemMax, ci, lane, oi, xi, xq, g, nreal_i, ps, nps, pc0, pc1,
-                     pcLo, pcHi, es, ee, fi, exclFlat, slotOf, slotAtom, frozen, origin, entries,
-                     masks, items, counters, entryCap, itemCap);
+          flush_item(B, kItemMax, ci, lane, oi, xq, g, nreal_i, pcLo, pcHi, fimask, exclFlat,
+                     slotOf, slotAtom, frozen, origin, entries, masks, items, counters, entryCap,
+                     itemCap);
           __syncwarp();
           const int rem = cnt - kItemMax;
           if (lane < rem) {
@@ -569,10 +589,8 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
     __syncwarp();
   }
   if (cnt > 0)
-    flush_item(B, cnt, ci, lane, oi, xi, xq, g, nreal_i, ps, nps, pc0, pc1, pcLo, pcHi, es,
-               ee, fi,
-               exclFlat, slotOf, slotAtom, frozen, origin, entries, masks, items, counters,
-               entryCap, itemCap);
+    flush_item(B, cnt, ci, lane, oi, xq, g, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
+               slotAtom, frozen, origin, entries, masks, items, counters, entryCap, itemCap);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
   if (lane == 0)
