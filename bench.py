@@ -86,16 +86,61 @@ def _parse():
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clock and clock-event reasons of the benchmarked GPU while the timed
+    region runs.  NVML is polled every 5 ms from a thread (the GPU found by its
+    PCI address, so CUDA_VISIBLE_DEVICES cannot mislead it); start() returns
+    once the first sample is in, so even a region of a few milliseconds gets
+    samples.  Falls back to `nvidia-smi -lms` when NVML cannot be used."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40),
+               ("sw_thermal_slowdown", 0x20), ("sw_power_cap", 0x4))
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
         self.path = None
+        self.thread = None
+        self.rows = []
+        self.smax = None
+        self.stop_flag = False
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.dev)
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
 
     def start(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            first = threading.Event()
+
+            def poll():
+                while not self.stop_flag:
+                    try:
+                        self.rows.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                          int(get_reasons(h))))
+                    except Exception:
+                        pass
+                    first.set()
+                    time.sleep(0.005)
+
+            self.thread = threading.Thread(target=poll, daemon=True)
+            self.thread.start()
+            first.wait(timeout=2.0)
+            self.source = "nvml"
+            return
+        except Exception:
+            self.thread = None
         fd, self.path = tempfile.mkstemp(prefix="clocks", suffix=".csv")
         os.close(fd)
         try:
@@ -103,10 +148,21 @@ class ClockSampler:
                 ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi"
         except OSError:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag = True
+            self.thread.join(timeout=2.0)
+            rows = list(self.rows)
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.smax, "reasons": ["no samples"],
+                        "source": "nvml"}
+            reasons = sorted({name for _, bits in rows for name, m in self.REASONS if bits & m})
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": self.smax,
+                    "reasons": reasons, "samples": len(rows), "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -125,11 +181,11 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [n for n, _ in self.REASONS]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi"}
 
 
 # ---------------------------------------------------------------------------
