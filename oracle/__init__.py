@@ -251,6 +251,8 @@ class Reference:
             lib.ref_set_bonded.argtypes = [C.c_void_p] + [C.c_int, C.c_void_p] * 5
             lib.ref_set_kspace.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_int, C.c_int]
             lib.ref_set_kspace.restype = C.c_int
+            lib.ref_set_nonbond.argtypes = [C.c_void_p, C.c_int, C.c_int]
+            lib.ref_set_nonbond.restype = C.c_int
             lib.ref_bonded_energies.argtypes = [C.c_void_p, _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
@@ -295,6 +297,12 @@ class Reference:
         later energy() call, with the harness alpha and this m-range;
         returns the k-vector count."""
         return self.lib().ref_set_kspace(self.h, prec, *[int(v) for v in mmax])
+
+    def set_nonbond(self, elec_type: int, vdw_type: int) -> None:
+        """Cut-off electrostatics: later energy() calls take MDBas's
+        nonbond_energy (keyEwald = 0) with these elecType / vdwType."""
+        if self.lib().ref_set_nonbond(self.h, int(elec_type), int(vdw_type)) != 0:
+            raise ValueError("elecType / vdwType outside MDBas's enums")
 
     def bonded_energies(self) -> dict:
         """Bonded energies of the last energy() call."""

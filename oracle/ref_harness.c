@@ -65,6 +65,7 @@ typedef struct {
   ANGLE *angle;
   int bondedOn; /* ref_set_bonded: energy() evaluates the bonded terms */
   int kspaceKey; /* ref_set_kspace: energy()'s keyEwald (0: real space only, 3) */
+  int nonbondOn; /* ref_set_nonbond: energy() with keyEwald = 0 (nonbond_energy) */
   CONSTRAINT *constList;
   DIHE *dihe, *impr;
   double *x, *y, *z, *q, *eps, *sig, *fx, *fy, *fz, *vx, *vy, *vz;
@@ -258,6 +259,22 @@ int ref_set_kspace(RefSys *s, double prec, int m1, int m2, int m3)
   return s->ewald.mmax;
 }
 
+/*
+ * Cut-off electrostatics instead of Ewald: energy() with keyEwald = 0 calls
+ * nonbond_energy (src/energy.c:158-161), whose pair functions come from
+ * init_energy_ptrs (src/energy.c:35-92) for these elecType / vdwType values.
+ * Returns -1 for values MDBas would stop on (UNKNOWN_ELEC_ERROR and the like).
+ */
+int ref_set_nonbond(RefSys *s, int elecType, int vdwType)
+{
+  if (elecType < NOELEC || elecType > SWITCH || vdwType < NOVDW || vdwType > VSWITCH)
+    return -1;
+  s->ctrl.elecType = elecType;
+  s->ctrl.vdwType = vdwType;
+  s->nonbondOn = 1;
+  return 0;
+}
+
 int ref_n_pair14(const RefSys *s) { return s->neigh.nPair14; }
 
 void ref_get_list14(const RefSys *s, int *out)
@@ -391,7 +408,7 @@ void ref_set_positions(RefSys *s, const double *x, const double *y, const double
 void ref_energy(RefSys *s, double *fx, double *fy, double *fz, double out[6])
 {
   PARAM p = energy_param(s);
-  s->ctrl.keyEwald = s->kspaceKey ? s->kspaceKey : 3;
+  s->ctrl.keyEwald = s->nonbondOn ? 0 : (s->kspaceKey ? s->kspaceKey : 3);
   init_energy_ptrs(&s->ctrl);
   energy(&s->ctrl, &p, &s->ener, &s->ewald, &s->box, &s->neigh, s->bond, s->ub, s->angle,
          s->dihe, s->impr, s->x, s->y, s->z, s->vx, s->vy, s->vz, s->fx, s->fy, s->fz, s->q,

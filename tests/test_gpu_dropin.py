@@ -100,3 +100,35 @@ def test_status_forms_report_instead_of_exit(gpu):
         eng.build()
     assert ei.value.status == 11
     eng.close()
+
+
+@pytest.mark.parametrize("elec,vdw", [(nb.SHIFT1, nb.VSWITCH), (nb.SHIFT2, nb.VSWITCH),
+                                      (nb.SWITCH, nb.VSWITCH), (nb.SHIFT1, nb.NOVDW),
+                                      (nb.NOELEC, nb.VSWITCH)])
+@pytest.mark.parametrize("which", ["small", "link"])
+def test_energy_dropin_cutoff_coulomb(gpu, which, elec, vdw):
+    """energy() with keyEwald = 0: the drop-in's nonbond_energy (cut-off
+    Coulomb forms, FP64 on the GPU) against MDBas's own, in either mode."""
+    s = systems.config_small(4) if which == "small" else systems.water_box_for_atoms(18558, 6)
+    if not oracle.Reference.available():
+        pytest.skip("MDBas reference library not built")
+    r = oracle.Reference(s)
+    r.set_nonbond(elec, vdw)
+    r.makelist()
+    rfx, rfy, rfz, re = r.energy()
+    r.close()
+    L = nb.bind_dropin()
+    for mode in (0, 1):
+        L.mdbas_nb_set_mode(mode)
+        try:
+            d = DropinSystem(s, keyEwald=0)
+            d.ctrl.elecType = elec
+            d.ctrl.vdwType = vdw
+            d.makelist()
+            fx, fy, fz, e = d.energy()
+        finally:
+            L.mdbas_nb_set_mode(0)
+        assert force_rel_rms((fx, fy, fz), (rfx, rfy, rfz)) < 1e-12
+        for k in ("elec", "vdw", "virelec", "virvdw", "pot", "virpot"):
+            assert abs(e[k] - re[k]) <= 1e-12 * abs(re[k]), (mode, k)
+        d.free()
