@@ -253,6 +253,7 @@ class Reference:
             lib.ref_set_kspace.restype = C.c_int
             lib.ref_set_nonbond.argtypes = [C.c_void_p, C.c_int, C.c_int]
             lib.ref_set_nonbond.restype = C.c_int
+            lib.ref_set_nb14.argtypes = [C.c_void_p, C.c_double, C.c_int, C.c_void_p]
             lib.ref_bonded_energies.argtypes = [C.c_void_p, _dp]
             lib.ref_destroy.argtypes = [C.c_void_p]
             cls._lib = lib
@@ -297,6 +298,17 @@ class Reference:
         later energy() call, with the harness alpha and this m-range;
         returns the k-vector count."""
         return self.lib().ref_set_kspace(self.h, prec, *[int(v) for v in mmax])
+
+    def set_nb14(self, scal14: float, dihedrals) -> None:
+        """1-4 pairs of these dihedral quadruples (scaled by scal14) in every
+        later energy() call; their list is made at the next makelist."""
+        from mdbas_b200 import nb
+        d = np.asarray(dihedrals, dtype=np.int64).reshape(-1, 4)
+        arr = (nb.DIHE * max(1, len(d)))()
+        for k, (a, b, c, e) in enumerate(d.tolist()):
+            arr[k].a, arr[k].b, arr[k].c, arr[k].d = a, b, c, e
+        self._keep.append(arr)
+        self.lib().ref_set_nb14(self.h, float(scal14), len(d), C.cast(arr, C.c_void_p))
 
     def set_nonbond(self, elec_type: int, vdw_type: int) -> None:
         """Cut-off electrostatics: later energy() calls take MDBas's

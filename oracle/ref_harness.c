@@ -260,6 +260,25 @@ int ref_set_kspace(RefSys *s, double prec, int m1, int m2, int m3)
 }
 
 /*
+ * 1-4 pairs: with keyNb14 set, energy() adds ewald14_energy (keyEwald != 0)
+ * or nonbond14_energy (keyEwald = 0) over the 1-4 list (src/energy.c:
+ * 152-164), scaled by scal14.  The exclusion builders make that list from
+ * these dihedrals at the next makelist (src/list.c:439-441, :851-853); the
+ * dihedral energy terms themselves stay off unless ref_set_bonded is called.
+ * Call before the first makelist.
+ */
+void ref_set_nb14(RefSys *s, double scal14, int nDihedral, const DIHE *dihe)
+{
+  if (!s->bondedOn) {
+    free(s->dihe);
+    s->dihe = (DIHE *)dup_terms(dihe, nDihedral, sizeof(DIHE));
+    s->param.nDihedral = nDihedral;
+  }
+  s->param.scal14 = scal14;
+  s->ctrl.keyNb14 = 1;
+}
+
+/*
  * Cut-off electrostatics instead of Ewald: energy() with keyEwald = 0 calls
  * nonbond_energy (src/energy.c:158-161), whose pair functions come from
  * init_energy_ptrs (src/energy.c:35-92) for these elecType / vdwType values.

@@ -132,3 +132,43 @@ def test_energy_dropin_cutoff_coulomb(gpu, which, elec, vdw):
         for k in ("elec", "vdw", "virelec", "virvdw", "pot", "virpot"):
             assert abs(e[k] - re[k]) <= 1e-12 * abs(re[k]), (mode, k)
         d.free()
+
+
+@pytest.mark.parametrize("key", ["ewald", "shift1"])
+def test_energy_dropin_pairs14(gpu, key):
+    """energy() with keyNb14: the drop-in's 1-4 list (from the dihedrals) and
+    its ewald14_energy / nonbond14_energy (scal14 = 0.5) against MDBas's."""
+    if not oracle.Reference.available():
+        pytest.skip("MDBas reference library not built")
+    s = systems.flexible_chains(4, 26.0, seed=7, jitter=0.08)
+    dihe = np.asarray(s.meta["dihedrals"])
+    r = oracle.Reference(s)
+    if key == "shift1":
+        r.set_nonbond(nb.SHIFT1, nb.VSWITCH)
+    r.set_nb14(0.5, dihe)
+    r.makelist()
+    rl14 = r.list14()
+    rfx, rfy, rfz, re = r.energy()
+    r.close()
+    L = nb.bind_dropin()
+    L.mdbas_nb_set_mode(0)
+    d = DropinSystem(s, keyEwald=3 if key == "ewald" else 0)
+    if key == "shift1":
+        d.ctrl.elecType = nb.SHIFT1
+    d.ctrl.keyNb14 = 1
+    d.param.scal14 = 0.5
+    arr = (nb.DIHE * len(dihe))()
+    for k, (a, b, c, e4) in enumerate(dihe.tolist()):
+        arr[k].a, arr[k].b, arr[k].c, arr[k].d = a, b, c, e4
+    d.dihe = arr
+    d.param.nDihedral = len(dihe)
+    d.makelist()
+    n14 = d.neigh.nPair14
+    assert n14 == len(rl14) // 2 > 0
+    assert [d.neighList14[k] for k in range(2 * n14)] == rl14.tolist()
+    d.param.nDihedral = 0      # the dihedral terms themselves stay off, as in the reference
+    fx, fy, fz, e = d.energy()
+    assert force_rel_rms((fx, fy, fz), (rfx, rfy, rfz)) < 1e-12
+    for k in ("elec", "vdw", "virelec", "virvdw"):
+        assert abs(e[k] - re[k]) <= 1e-12 * abs(re[k]), k
+    d.free()
