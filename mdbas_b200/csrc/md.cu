@@ -627,13 +627,23 @@ __global__ void k_wrap(int n, const DevBox *__restrict__ boxes, const int *__res
   z[i] = zi;
 }
 
-// kinetic energy (src/utils.c:502-515), sum in fixed point (2^-24 units)
+// kinetic energy (src/utils.c:502-515), sum in fixed point (2^-24 units).
+// A term at or above termLimit (2^62 / n in fixed-point units, so that no
+// sum of n terms can wrap) or not finite raises FLAG_OVERFLOW in *flags.
 __global__ void k_kinetic(int n, const double *__restrict__ mass, const double *__restrict__ vx,
                           const double *__restrict__ vy, const double *__restrict__ vz,
-                          long long *__restrict__ acc) {
+                          double termLimit, long long *__restrict__ acc,
+                          long long *__restrict__ flags) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   long long v = 0;
-  if (i < n) v = fix_e(0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]));
+  if (i < n) {
+    const double t = 0.5 * mass[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+    if (!(t * kEnergyScale < termLimit)) {
+      atomicOr(reinterpret_cast<unsigned long long *>(flags), (unsigned long long)FLAG_OVERFLOW);
+    } else {
+      v = fix_e(t);
+    }
+  }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) red_add(acc, v);
@@ -960,7 +970,8 @@ int md_stage2(mdbas_nb_engine *e, cudaStream_t s, bool kin, double tauT, double 
   const bool thermo = tauT > 0.;
   if (kin || thermo) {
     MDB_CUDA(cudaMemsetAsync(word + W_KIN, 0, sizeof(long long), s));
-    MDB_LAUNCH(k_kinetic, g, 256, 0, s, n, e->mdMass.as<double>(), vx, vy, vz, word + W_KIN);
+    MDB_LAUNCH(k_kinetic, g, 256, 0, s, n, e->mdMass.as<double>(), vx, vy, vz,
+               4611686018427387904.0 / (double)(n > 0 ? n : 1), word + W_KIN, word + W_FLAGS);
   }
   if (thermo)
     MDB_LAUNCH(k_berendsen, g, 256, 0, s, n, e->mdDt / tauT, kinTemp0, word + W_KIN, vx, vy,
@@ -1239,7 +1250,7 @@ int md_run_graph(mdbas_nb_engine *e, int chunks, int energyEvery, double targetT
     const int st2[2] = {(int)(w[W_SHAKE] & 0xffffffff), (int)(w[W_SHAKE] >> 32)};
     MD_TRY(md_check_shake(e, st2));
     if (w[W_FLAGS] & FLAG_OVERFLOW) {
-      set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
+      set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point overflow (forces or kinetic energy)");
       return MDBAS_NB_ERR_OVERFLOW;
     }
     if (w[W_FLAGS] & FLAG_STAGE) {
@@ -1549,6 +1560,10 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   MDB_CUDA(cudaStreamSynchronize(s));
   const int st2[2] = {(int)(w[W_SHAKE] & 0xffffffff), (int)(w[W_SHAKE] >> 32)};
   MD_TRY(md_check_shake(e, st2));
+  if (w[W_FLAGS] & FLAG_OVERFLOW) {
+    set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point kinetic energy overflow");
+    return MDBAS_NB_ERR_OVERFLOW;
+  }
   e->computed = true;
   return MDBAS_NB_OK;
 }

@@ -110,3 +110,54 @@ def test_engine(gpu, kind):
         assert abs(elec - re["elec"]) <= tol * abs(re["elec"])
         assert abs(e["vdw"] - re["vdw"]) <= tol * abs(re["vdw"])
     r.close()
+
+
+@pytest.mark.parametrize("kind", ["orbic", "tclin"])
+def test_md_fp64_matches_mdbas(gpu, kind):
+    """10 velocity-Verlet steps of an LJ fluid in a non-cubic cell (list
+    rebuilt every 5 steps, positions wrapped by image_update): the engine's
+    FP64 dynamics against MDBas's integrator.  (This fluid, sampled with a
+    2 A minimum separation, blows up a few steps later: MDBas's kinetic
+    energy passes 1e22 at step 15.)"""
+    s = systems.lj_fluid(3000, 33.0, seed=4)
+    btype, cell = _cell(kind, 33.0)
+    vel = systems.thermal_velocities(s.mass, 150.0, seed=4)
+    pot = dict(cutOff=12.0, cutOn=10.0, delr=2.0, alpha=0.34)
+    r = _reference(s, cell, btype)
+    r.makelist()
+    r.md_init(s.mass, vel, time_step=0.002, list_update=5)
+    rrows = r.md_run(10)
+    rp = r.positions()
+    rself = r.self_energy()
+    r.close()
+    e = nb.Engine(s, precision=0, box_type=btype, cell=cell, **pot)
+    e.md_init(s.mass, vel, time_step=0.002, list_update=5)
+    grows = e.md_run(10, energy_every=1)
+    gp = e.positions()
+    e.close()
+    # positions up to a lattice vector of the cell (rows a, b, c)
+    h = cell.reshape(3, 3)
+    d = np.stack([np.asarray(gp[k]) - np.asarray(rp[k]) for k in range(3)], 1)
+    frac = d @ np.linalg.inv(h)
+    d = (frac - np.round(frac)) @ h
+    perr = np.max(np.abs(d))
+    tot_err = np.max(np.abs(grows[:, 3] - (rrows[:, 3] + rself))) / np.max(np.abs(rrows[:, 3]))
+    print(f"{kind}: pos {perr:.3e} A, total energy {tot_err:.3e}")
+    assert tot_err < 1e-10
+    assert perr < 1e-9
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_md_kinetic_overflow_is_reported(gpu, precision):
+    """A kinetic energy beyond the 64-bit fixed-point range (one atom at
+    1e8 A/ps) stops the run with MDBAS_NB_ERR_OVERFLOW instead of reporting
+    a wrapped sum."""
+    s = systems.lj_fluid(3000, 33.0, seed=4)
+    vel = [np.array(v) for v in systems.thermal_velocities(s.mass, 150.0, seed=4)]
+    vel[0][7] = 1.0e8
+    e = nb.Engine(s, precision=precision, cutOff=12.0, cutOn=10.0, delr=2.0, alpha=0.34)
+    e.md_init(s.mass, vel, time_step=0.002, list_update=5)
+    with pytest.raises(nb.MdbasNbError) as err:
+        e.md_run(2, energy_every=1)
+    assert err.value.status == 10 and "overflow" in str(err.value)   # MDBAS_NB_ERR_OVERFLOW
+    e.close()
