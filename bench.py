@@ -772,7 +772,11 @@ def run_ours(args, rank, world):
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": "measured FFMA probe (mdbas_nb_fp32_peak)",
-                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32x2"},
+                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32x2",
+                         # the same flops counted on every listed pair slot (8 x 8
+                         # per cluster pair, in the cut-off or not); frac = this x
+                         # the pair efficiency of the cluster list
+                         "frac_of_listed_slots": achieved / peak / max(1e-30, pairs / max(1, stats[2]))},
             "precision": prec,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 3 * 8 * n,
