@@ -379,7 +379,13 @@ int mdbas_nb_engine_set_topology(mdbas_nb_engine *e, const double *q, const doub
 int mdbas_nb_engine_set_positions(mdbas_nb_engine *e, const double *x, const double *y,
                                   const double *z, int device_ptrs);
 /* Sort atoms into cells/clusters and build the cluster-pair list (precision 1)
- * or the MDBas-format half list (precision 0). */
+ * or the MDBas-format half list (precision 0).  A precision-1 rebuild on the
+ * grid and list room of the previous build returns without waiting for the
+ * list counts; its outcome is settled by the next call that returns results
+ * (get_forces, energies, list_stats, export_pairs, autotune, set_positions,
+ * md_init, md_run): a list that outgrew its room is built again with more
+ * room and the evaluation redone, and non-finite positions return
+ * MDBAS_NB_ERR_NONFINITE there. */
 int mdbas_nb_engine_build(mdbas_nb_engine *e);
 /* Refresh the per-atom float4 layout from the current FP64 positions without
  * rebuilding the list (between rebuilds during dynamics). */

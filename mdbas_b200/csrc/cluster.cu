@@ -686,8 +686,20 @@ k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
   }
 }
 
-__global__ void k_latch(const long long *__restrict__ counters, long long *__restrict__ sticky) {
-  if (threadIdx.x == 0) sticky[0] |= counters[2];
+// Latch a search's (or prune's) error bits into the sticky word.  A list
+// that overflowed is unusable: its item count may point past the item buffer
+// and some items were never written, so both counts are zeroed and the pair
+// kernels that follow in the same stream (or graph) see an empty list until
+// the host rebuilds with room.
+__global__ void k_latch(long long *__restrict__ counters, long long *__restrict__ sticky) {
+  if (threadIdx.x == 0) {
+    const long long f = counters[2];
+    sticky[0] |= f;
+    if (f & CL_OVERFLOW) {
+      counters[0] = 0;
+      counters[1] = 0;
+    }
+  }
 }
 
 unsigned morton2(unsigned x, unsigned y) {

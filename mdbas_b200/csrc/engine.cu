@@ -144,6 +144,37 @@ static int upload_boxes(mdbas_nb_engine *e) {
   return MDBAS_NB_OK;
 }
 
+// The cluster-pair list built and its counts read back (grows the list until
+// it fits).
+static int sync_build(mdbas_nb_engine *e) {
+  const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
+  return cluster_build(e->cl, e->n, e->nRep, e->repBoxes.data(), e->repOff.data(),
+                       e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(),
+                       e->y.as<double>(), e->z.as<double>(), e->q.as<double>(),
+                       e->eps.as<double>(), e->sig.as<double>(), frozen,
+                       e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream);
+}
+
+int mdbas::engine_resolve_build(mdbas_nb_engine *e) {
+  if (!e->buildPending) return MDBAS_NB_OK;
+  e->buildPending = false;
+  long long sticky = 0;
+  MDB_CUDA(cudaMemcpyAsync(&sticky, e->cl.sticky.p, sizeof(sticky), cudaMemcpyDeviceToHost,
+                           e->stream));
+  MDB_CUDA(cudaStreamSynchronize(e->stream));
+  if (!(sticky & (CL_OVERFLOW | CL_NONFINITE))) return MDBAS_NB_OK;
+  MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), e->stream));
+  if (sticky & CL_NONFINITE) {
+    e->built = false;
+    set_last_status(MDBAS_NB_ERR_NONFINITE, "non-finite position in the list build");
+    return MDBAS_NB_ERR_NONFINITE;
+  }
+  const bool redo = e->computed;
+  ENG_TRY(e, sync_build(e));
+  if (redo) return mdbas_nb_engine_compute(e);
+  return MDBAS_NB_OK;
+}
+
 extern "C" {
 
 int mdbas_nb_engine_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *cfg,
@@ -319,6 +350,8 @@ int mdbas_nb_engine_set_positions(mdbas_nb_engine *e, const double *x, const dou
                                   const double *z, int device_ptrs) {
   if (!e || !x || !y || !z) return MDBAS_NB_ERR_ARG;
   ENG_TRY(e, set_dev(e));
+  // a pending build belongs to the positions about to be replaced
+  ENG_TRY(e, engine_resolve_build(e));
   const int n = e->n;
   ENG_TRY(e, e->x.ensure(sizeof(double) * n));
   ENG_TRY(e, e->y.ensure(sizeof(double) * n));
@@ -346,11 +379,25 @@ int mdbas_nb_engine_build(mdbas_nb_engine *e) {
                               frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream));
   } else {
     e->cl.useInner = false;  // a new list; dynamics prune it again
-    ENG_TRY(e, cluster_build(e->cl, n, e->nRep, e->repBoxes.data(), e->repOff.data(),
-                             e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
-                             e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),
-                             e->sig.as<double>(), frozen, e->exclStart.as<int>(),
-                             e->exclFlat.as<int>(), e->stream));
+    e->buildPending = false;
+    if (e->built && e->cl.entryCap > 0 && e->cl.sticky.p) {
+      // Grid, tables and capacities of the previous build still fit: build
+      // without waiting for the counts.  An overflow zeroes the list on the
+      // device and is settled by the next call that returns results.
+      MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), e->stream));
+      const int st = cluster_build(e->cl, n, e->nRep, e->repBoxes.data(), e->repOff.data(),
+                                   e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst),
+                                   e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                                   e->q.as<double>(), e->eps.as<double>(), e->sig.as<double>(),
+                                   frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(),
+                                   e->stream, false);
+      if (st == MDBAS_NB_OK) {
+        e->buildPending = true;
+        return MDBAS_NB_OK;
+      }
+      if (st != MDBAS_NB_ERR_STATE) ENG_TRY(e, st);
+    }
+    ENG_TRY(e, sync_build(e));
   }
   e->built = true;
   return MDBAS_NB_OK;
@@ -423,6 +470,7 @@ int mdbas_nb_engine_get_forces(mdbas_nb_engine *e, double *fx, double *fy, doubl
   if (!e || !fx || !fy || !fz) return MDBAS_NB_ERR_ARG;
   if (!e->computed) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
   LaunchScope ls(e);
   const int n = e->n;
   cudaStream_t s = e->stream;
@@ -446,6 +494,7 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
   if (!e || !out) return MDBAS_NB_ERR_ARG;
   if (!e->computed) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
   cudaStream_t s = e->stream;
   memset(out, 0, sizeof(*out));
   out->elec_self = e->selfE;
@@ -487,6 +536,8 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
 int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
   if (!e || !out) return MDBAS_NB_ERR_ARG;
   if (!e->built) return MDBAS_NB_ERR_STATE;
+  ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
   if (e->cfg.precision == 0) {
     out[0] = e->n;
     out[1] = e->ref.entries;
@@ -498,7 +549,7 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
     out[0] = e->cl.nClusters;
     out[1] = e->cl.nEntries;
     out[2] = e->cl.nEntries * 64;
-    out[3] = e->cl.nItems;
+    out[3] = e->cl.entryCap;
   }
   return MDBAS_NB_OK;
 }
@@ -508,6 +559,7 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs,
   if (!e || !count) return MDBAS_NB_ERR_ARG;
   if (!e->built) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
   LaunchScope ls(e);
   cudaStream_t s = e->stream;
   ENG_TRY(e, e->exportCount.ensure(sizeof(unsigned long long)));
@@ -546,6 +598,7 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   if (e->cfg.precision != 1) return MDBAS_NB_ERR_UNSUPPORTED;
   if (!e->built) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
   LaunchScope ls(e);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);

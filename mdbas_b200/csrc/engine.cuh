@@ -58,6 +58,10 @@ struct mdbas_nb_engine {
   mdbas::DBuf kspaceFix, kspaceF;  // int64 energy word; scratch forces (3n)
   // bookkeeping
   bool built = false, computed = false;
+  // a build ran without reading its counts back (precision 1, same grid and
+  // capacities as the build before): its error bits wait in cl.sticky until
+  // the next call that returns results (engine_resolve_build)
+  bool buildPending = false;
   long long launches = 0;
   bool timing = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -105,6 +109,10 @@ void md_release(mdbas_nb_engine *e);
 // Reciprocal forces added to f (3n, caller order) and the reciprocal plus
 // non-neutral energy into kspaceFix (md_kspace.cu); no-op when off.
 int md_kspace(mdbas_nb_engine *e, double *f, cudaStream_t s);
+// Settle a pending build (see buildPending): read its error bits; on an
+// overflowing list build again with room, synchronously, and redo the
+// evaluation if one ran on the empty list; non-finite positions are an error.
+int engine_resolve_build(mdbas_nb_engine *e);
 void kspace_release(mdbas_nb_engine *e);
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);

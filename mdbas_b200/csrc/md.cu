@@ -827,6 +827,7 @@ int md_save_build_positions(mdbas_nb_engine *e, cudaStream_t s) {
 // Synchronising list build (either precision) at the current positions.
 int md_build(mdbas_nb_engine *e) {
   MD_TRY(mdbas_nb_engine_build(e));
+  MD_TRY(engine_resolve_build(e));  // the step uses the list right away
   MD_TRY(md_save_build_positions(e, e->stream));
   e->mdRebuilds += 1;
   return MDBAS_NB_OK;
@@ -1293,6 +1294,7 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   if (!e->topoSet || !e->posSet) return MDBAS_NB_ERR_STATE;
   if (nConst > 0 && (!constAtoms || !constLen2)) return MDBAS_NB_ERR_ARG;
   MDB_CUDA(cudaSetDevice(e->device));
+  MD_TRY(engine_resolve_build(e));
   const int n = e->n;
   std::vector<double> rm(n);
   for (int i = 0; i < n; ++i) {
@@ -1493,6 +1495,7 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   if (!e || nSteps < 0) return MDBAS_NB_ERR_ARG;
   if (!e->mdReady) return MDBAS_NB_ERR_STATE;
   MDB_CUDA(cudaSetDevice(e->device));
+  MD_TRY(engine_resolve_build(e));
   LaunchScope ls(e);
   cudaStream_t s = e->stream;
   long long *word = e->mdWord.as<long long>();
