@@ -155,6 +155,21 @@ static int sync_build(mdbas_nb_engine *e) {
                        e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream);
 }
 
+// Error bits of the cached accumulators (mixed precision only).
+static int acc_status(const mdbas_nb_engine *e) {
+  if (e->cfg.precision == 0) return MDBAS_NB_OK;
+  const long long f = e->accCache[ACC_FLAGS];
+  if (f & FLAG_OVERFLOW) {
+    set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
+    return MDBAS_NB_ERR_OVERFLOW;
+  }
+  if (f & FLAG_STAGE) {
+    set_last_status(MDBAS_NB_ERR_CUDA, "a bulk copy into shared memory timed out");
+    return MDBAS_NB_ERR_CUDA;
+  }
+  return MDBAS_NB_OK;
+}
+
 int mdbas::engine_resolve_build(mdbas_nb_engine *e) {
   if (!e->buildPending) return MDBAS_NB_OK;
   e->buildPending = false;
@@ -334,6 +349,7 @@ int mdbas_nb_engine_set_topology(mdbas_nb_engine *e, const double *q, const doub
   for (int i = 0; i < n; ++i) qmax2 = fmax(qmax2, q[i] * q[i]);
   if (qmax2 * (double)n >= 8.0e6) return MDBAS_NB_ERR_OVERFLOW;  // 2^63 / 2^40
   ENG_TRY(e, e->acc64.ensure(sizeof(double) * kFp64AccCount));
+  e->accCached = false;  // the accumulators serve as scratch here
   MDB_CUDA(cudaMemsetAsync(e->acc64.p, 0, sizeof(double) * kFp64AccCount, s));
   ENG_TRY(e, sum_q2(n, e->q.as<double>(), reinterpret_cast<long long *>(e->acc64.p), s));
   long long q2 = 0;
@@ -462,6 +478,7 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
     e->pairCount += 1;
   }
   e->computed = true;
+  e->accCached = false;
   return MDBAS_NB_OK;
 }
 
@@ -486,8 +503,18 @@ int mdbas_nb_engine_get_forces(mdbas_nb_engine *e, double *fx, double *fy, doubl
   MDB_CUDA(cudaMemcpyAsync(fx, src, sizeof(double) * n, k, s));
   MDB_CUDA(cudaMemcpyAsync(fy, src + n, sizeof(double) * n, k, s));
   MDB_CUDA(cudaMemcpyAsync(fz, src + 2 * (size_t)n, sizeof(double) * n, k, s));
-  if (!device_ptrs) MDB_CUDA(cudaStreamSynchronize(s));
-  return MDBAS_NB_OK;
+  if (device_ptrs) return MDBAS_NB_OK;
+  // the energy words ride along with the forces: one wait for both, and the
+  // fixed-point error bits checked here too
+  if (e->cfg.precision == 0)
+    MDB_CUDA(cudaMemcpyAsync(e->acc64Cache, e->acc64.p, sizeof(e->acc64Cache),
+                             cudaMemcpyDeviceToHost, s));
+  else
+    MDB_CUDA(cudaMemcpyAsync(e->accCache, e->cl.acc.p, sizeof(e->accCache),
+                             cudaMemcpyDeviceToHost, s));
+  MDB_CUDA(cudaStreamSynchronize(s));
+  e->accCached = true;
+  return acc_status(e);
 }
 
 int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
@@ -498,10 +525,18 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
   cudaStream_t s = e->stream;
   memset(out, 0, sizeof(*out));
   out->elec_self = e->selfE;
-  if (e->cfg.precision == 0) {
-    double a[kFp64AccCount];
-    MDB_CUDA(cudaMemcpyAsync(a, e->acc64.p, sizeof(a), cudaMemcpyDeviceToHost, s));
+  if (!e->accCached) {
+    if (e->cfg.precision == 0)
+      MDB_CUDA(cudaMemcpyAsync(e->acc64Cache, e->acc64.p, sizeof(e->acc64Cache),
+                               cudaMemcpyDeviceToHost, s));
+    else
+      MDB_CUDA(cudaMemcpyAsync(e->accCache, e->cl.acc.p, sizeof(e->accCache),
+                               cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaStreamSynchronize(s));
+    e->accCached = true;
+  }
+  if (e->cfg.precision == 0) {
+    const double *a = e->acc64Cache;
     out->elec_direct = a[0];
     out->vdw = a[1];
     out->vir_direct = a[2];
@@ -511,9 +546,7 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
     out->vir_corr = a[6];
     return MDBAS_NB_OK;
   }
-  long long a[ACC_COUNT];
-  MDB_CUDA(cudaMemcpyAsync(a, e->cl.acc.p, sizeof(a), cudaMemcpyDeviceToHost, s));
-  MDB_CUDA(cudaStreamSynchronize(s));
+  const long long *a = e->accCache;
   const double inv = 1.0 / kEnergyScale;
   out->elec_direct = (double)a[ACC_E_DIR] * inv;
   out->elec_corr = (double)a[ACC_E_CORR] * inv;
@@ -522,15 +555,7 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
   out->vir_corr = (double)a[ACC_V_CORR] * inv;
   out->vir_vdw = (double)a[ACC_V_VDW] * inv;
   out->n_pairs = (double)a[ACC_NPAIR];
-  if (a[ACC_FLAGS] & FLAG_OVERFLOW) {
-    set_last_status(MDBAS_NB_ERR_OVERFLOW, "fixed-point force overflow");
-    return MDBAS_NB_ERR_OVERFLOW;
-  }
-  if (a[ACC_FLAGS] & FLAG_STAGE) {
-    set_last_status(MDBAS_NB_ERR_CUDA, "a bulk copy into shared memory timed out");
-    return MDBAS_NB_ERR_CUDA;
-  }
-  return MDBAS_NB_OK;
+  return acc_status(e);
 }
 
 int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
@@ -599,6 +624,7 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   if (!e->built) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
   ENG_TRY(e, engine_resolve_build(e));
+  e->accCached = false;  // the trial launches overwrite the accumulators
   LaunchScope ls(e);
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, e->device);

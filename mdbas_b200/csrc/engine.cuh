@@ -62,6 +62,11 @@ struct mdbas_nb_engine {
   // capacities as the build before): its error bits wait in cl.sticky until
   // the next call that returns results (engine_resolve_build)
   bool buildPending = false;
+  // energy accumulators read back with the forces (same synchronisation);
+  // energies() uses them until the next evaluation
+  bool accCached = false;
+  long long accCache[8] = {};
+  double acc64Cache[8] = {};
   long long launches = 0;
   bool timing = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;

@@ -1295,6 +1295,7 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   if (nConst > 0 && (!constAtoms || !constLen2)) return MDBAS_NB_ERR_ARG;
   MDB_CUDA(cudaSetDevice(e->device));
   MD_TRY(engine_resolve_build(e));
+  e->accCached = false;
   const int n = e->n;
   std::vector<double> rm(n);
   for (int i = 0; i < n; ++i) {
@@ -1496,6 +1497,7 @@ int mdbas_nb_engine_md_run(mdbas_nb_engine *e, int nSteps, int energyEvery, doub
   if (!e->mdReady) return MDBAS_NB_ERR_STATE;
   MDB_CUDA(cudaSetDevice(e->device));
   MD_TRY(engine_resolve_build(e));
+  e->accCached = false;  // the steps evaluate again
   LaunchScope ls(e);
   cudaStream_t s = e->stream;
   long long *word = e->mdWord.as<long long>();
