@@ -262,7 +262,7 @@ def run_reference(args, rank, world):
                    "processes": procs_n},
         "cpu_baseline": {"value": value, "unit": "pairs/s", "cores": procs_n, "kind": "reference",
                          "sample": f"{procs_n} processes x {steps} steps, one 96k-atom list "
-                                   f"rebuild + energy() each"},
+                                   f"rebuild + energy() each", "host": _host_cpu()},
         "e2e": {"value": value, "unit": "pairs/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
         "ns_per_day": 86400.0 / t * FS_PER_STEP * 1e-6,
@@ -282,18 +282,38 @@ def cpu_baseline_sample(seed: int) -> dict:
     r.makelist()
     x, y, z = r.positions()
     pairs = _count_pairs(seed)
-    ts = []
+    ts, tl, te = [], [], []
     t_start = time.perf_counter()
     while len(ts) < 3 or (time.perf_counter() - t_start < 10 and len(ts) < 6):
         t0 = r.now()
         r.update_list(x, y, z)
+        t1 = r.now()
         r.energy()
-        ts.append(r.now() - t0)
+        t2 = r.now()
+        ts.append(t2 - t0)
+        tl.append(t1 - t0)
+        te.append(t2 - t1)
     r.close()
     t = statistics.median(ts)
     return {"value": pairs / t, "unit": "pairs/s", "cores": 1, "kind": "reference",
             "sample": f"{len(ts)} x (96k-atom link_cell_verlet_list_update + energy()), "
-                      f"median {t:.2f} s"}
+                      f"median {t:.2f} s",
+            "list_update_s": statistics.median(tl), "energy_s": statistics.median(te),
+            "host": _host_cpu()}
+
+
+def _host_cpu() -> dict:
+    """CPU model and logical core count of the host the baseline ran on."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
 
 
 # ---------------------------------------------------------------------------
