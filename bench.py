@@ -270,8 +270,13 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
-def cpu_baseline_sample(seed: int) -> dict:
-    """MDBas single-threaded on the host: list rebuild + energy(), ~3 steps."""
+def cpu_baseline_sample(seed: int, gpu_list=None) -> dict:
+    """MDBas single-threaded on the host: list rebuild + energy(), ~3 steps.
+    With gpu_list (a function of the wrapped positions returning the GPU
+    list's unordered pairs), the result also carries "list_parity": MDBas's
+    neighbour pair set against the GPU list builder's on the same 96k
+    coordinates."""
+    import numpy as np
     import oracle
     from mdbas_b200 import systems
     if not oracle.Reference.available():
@@ -293,13 +298,35 @@ def cpu_baseline_sample(seed: int) -> dict:
         ts.append(t2 - t0)
         tl.append(t1 - t0)
         te.append(t2 - t1)
+    parity = None
+    if gpu_list is not None:
+        lst, pair, order = r.get_list()
+        gp = gpu_list(x, y, z)
+        parity = _same_pair_set(s.n, np.repeat(order, pair[order]), lst, gp[:, 0], gp[:, 1])
     r.close()
     t = statistics.median(ts)
-    return {"value": pairs / t, "unit": "pairs/s", "cores": 1, "kind": "reference",
+    return {"list_parity": parity,
+            "value": pairs / t, "unit": "pairs/s", "cores": 1, "kind": "reference",
             "sample": f"{len(ts)} x (96k-atom link_cell_verlet_list_update + energy()), "
                       f"median {t:.2f} s",
             "list_update_s": statistics.median(tl), "energy_s": statistics.median(te),
             "host": _host_cpu()}
+
+
+def _same_pair_set(n, ai, aj, bi, bj) -> dict:
+    """Set equality of two unordered pair lists (keys min * n + max, sorted
+    on the GPU)."""
+    import numpy as np
+    import torch
+    def keys(i, j):
+        i = torch.as_tensor(np.asarray(i, dtype=np.int64), device="cuda")
+        j = torch.as_tensor(np.asarray(j, dtype=np.int64), device="cuda")
+        return torch.sort(torch.minimum(i, j) * n + torch.maximum(i, j)).values
+    ka, kb = keys(ai, aj), keys(bi, bj)
+    same = ka.numel() == kb.numel() and bool(torch.equal(ka, kb))
+    return {"mdbas_pairs": int(ka.numel()), "gpu_pairs": int(kb.numel()), "bit_exact": same,
+            "what": "set of unordered (i, j) of MDBas's link-cell list (r <= 14 A) and the "
+                    "GPU builder's, same wrapped 96k coordinates"}
 
 
 def _host_cpu() -> dict:
@@ -757,8 +784,18 @@ def run_ours(args, rank, world):
                                     args.replica_steps, world)
 
     cpu = None
+    list_parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(args.seed)
+        def gpu_list(x, y, z):
+            sw = systems.config_96k(seed=args.seed, temperature=None)
+            sw.x, sw.y, sw.z = x, y, z
+            e0 = nb.Engine(sw, precision=0, device=dev)
+            e0.build()
+            p = e0.export_pairs(1e30)
+            e0.close()
+            return p
+        cpu = cpu_baseline_sample(args.seed, gpu_list)
+        list_parity = cpu.pop("list_parity", None)
 
     if rank == 0:
         line = {
@@ -804,6 +841,7 @@ def run_ours(args, rank, world):
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu,
+            "list_parity": list_parity,
         }
         print(json.dumps(line))
     eng.close()
