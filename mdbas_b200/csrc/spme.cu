@@ -528,7 +528,7 @@ __global__ void k_spme_energy(long long mm, const cufftDoubleComplex *__restrict
 // memory, one warp per row, then takes the bin's atoms, `group` lanes per
 // atom.  fsum gets one partial per tile, accumulated in atom order.
 template <int P>  // the B-spline order, or 0: given at run time
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 4)  // four blocks per SM (64 registers)
     k_spme_forces_tiled(int n, int m1, int m2, int m3, int nbspRun, int group, int nt2, int nt3,
                         SpmeBox b, double fact1, const double *__restrict__ q,
                         const double *__restrict__ spl, const int *__restrict__ cell,
