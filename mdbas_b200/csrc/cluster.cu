@@ -110,9 +110,18 @@ __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
         sz[t] = atomZ[a];
       }
       __syncthreads();
-      if (m < e)
-        for (int t = 0; t < cnt; ++t)
-          rank += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+      if (m < e) {
+        // four independent counts: the comparisons do not wait on each other
+        int r0 = 0, r1 = 0, r2 = 0, r3 = 0, t = 0;
+        for (; t + 3 < cnt; t += 4) {
+          r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+          r1 += (sz[t + 1] < mz) || (sz[t + 1] == mz && si[t + 1] < mi);
+          r2 += (sz[t + 2] < mz) || (sz[t + 2] == mz && si[t + 2] < mi);
+          r3 += (sz[t + 3] < mz) || (sz[t + 3] == mz && si[t + 3] < mi);
+        }
+        for (; t < cnt; ++t) r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+        rank += (r0 + r1) + (r2 + r3);
+      }
     }
     if (m < e) slotAtom[ps + rank] = mi;
   }
@@ -174,21 +183,40 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
   hz = grp_max8(hz);
   const int nreal = __popc(__ballot_sync(0xffffffffu, a >= 0) >> (threadIdx.x & 24) & 0xffu);
   const double ox = 0.5 * (lx + hx), oy = 0.5 * (ly + hy), oz = 0.5 * (lz + hz);
+  // Half extents rounded up so that the FP32 box always contains its atoms;
+  // w holds the number of real (non-padding) atoms.
+  const float4 h = make_float4(__double2float_ru(0.5 * (hx - lx) * (1.0 + 1e-6) + 1e-6),
+                               __double2float_ru(0.5 * (hy - ly) * (1.0 + 1e-6) + 1e-6),
+                               __double2float_ru(0.5 * (hz - lz) * (1.0 + 1e-6) + 1e-6),
+                               (float)nreal);
+  // The largest half extents per box, one atomic per warp and dimension
+  // when the warp's clusters share a box (non-negative floats order like
+  // their bits); every lane is still present here.
+  {
+    const bool mine = active && k == 0;
+    const int bx = mine ? __float_as_int(h.x) : 0, by = mine ? __float_as_int(h.y) : 0,
+              bz = mine ? __float_as_int(h.z) : 0;
+    const int rep0 = __shfl_sync(0xffffffffu, rep, 0);
+    if (__all_sync(0xffffffffu, !active || rep == rep0)) {
+      const int mx = __reduce_max_sync(0xffffffffu, bx), my = __reduce_max_sync(0xffffffffu, by),
+                mz = __reduce_max_sync(0xffffffffu, bz);
+      if ((threadIdx.x & 31) == 0 && active) {
+        atomicMax(hmaxBits + 4 * rep0 + 0, mx);
+        atomicMax(hmaxBits + 4 * rep0 + 1, my);
+        atomicMax(hmaxBits + 4 * rep0 + 2, mz);
+      }
+    } else if (mine) {
+      atomicMax(hmaxBits + 4 * rep + 0, bx);
+      atomicMax(hmaxBits + 4 * rep + 1, by);
+      atomicMax(hmaxBits + 4 * rep + 2, bz);
+    }
+  }
   if (!active) return;
   if (k == 0) {
     if (clusterRep) clusterRep[c] = rep;
     origin[c] = make_double4(ox, oy, oz, 0.0);
     originF[c] = make_float4((float)ox, (float)oy, (float)oz, (float)nreal);
-    // Half extents rounded up so that the FP32 box always contains its
-    // atoms; w holds the number of real (non-padding) atoms.
-    const float4 h = make_float4(__double2float_ru(0.5 * (hx - lx) * (1.0 + 1e-6) + 1e-6),
-                                 __double2float_ru(0.5 * (hy - ly) * (1.0 + 1e-6) + 1e-6),
-                                 __double2float_ru(0.5 * (hz - lz) * (1.0 + 1e-6) + 1e-6),
-                                 (float)nreal);
     half[c] = h;
-    atomicMax(hmaxBits + 4 * rep + 0, __float_as_int(h.x));
-    atomicMax(hmaxBits + 4 * rep + 1, __float_as_int(h.y));
-    atomicMax(hmaxBits + 4 * rep + 2, __float_as_int(h.z));
     clusterXY[c] = colXY[atomCol[a0]];
   }
   float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
