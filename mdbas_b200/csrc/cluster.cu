@@ -86,46 +86,89 @@ __global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
   tmpIdx[colStart[c] + atomicAdd(colFill + c, 1)] = i;
 }
 
-// Sort a cell's atoms by (z, index): rank = members ordered before this one.
+// One column per block: its atoms in ascending (z, atom index) order into
+// the column's slots, padding slots set to -1.  Columns of up to 1,024 atoms
+// are sorted in shared memory by a bitonic network (keys padded to a power
+// of two with +inf); longer ones by rank counting.  Both give the same total
+// order, so the same slots.
 __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
                            const int *__restrict__ colPadStart, const int *__restrict__ tmpIdx,
                            const double *__restrict__ atomZ, int *__restrict__ slotAtom) {
-  __shared__ double sz[512];
-  __shared__ int si[512];
+  constexpr int kMax = 1024;
+  __shared__ double sz[kMax];
+  __shared__ int si[kMax];
   const int c = blockIdx.x;
   if (c >= nCols) return;
   const int s = colStart[c], e = colStart[c + 1];
   const int ps = colPadStart[c], pe = colPadStart[c + 1];
-  for (int base = s; base < e; base += blockDim.x) {
-    const int m = base + threadIdx.x;
-    const int mi = (m < e) ? tmpIdx[m] : 0;
-    const double mz = (m < e) ? atomZ[mi] : 0.0;
-    int rank = 0;
-    for (int cb = s; cb < e; cb += 512) {
-      const int cnt = min(512, e - cb);
-      __syncthreads();
-      for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
-        const int a = tmpIdx[cb + t];
+  const int n = e - s;
+  if (n <= kMax) {
+    int P = 2;
+    while (P < n) P <<= 1;
+    for (int t = threadIdx.x; t < P; t += blockDim.x) {
+      if (t < n) {
+        const int a = tmpIdx[s + t];
         si[t] = a;
         sz[t] = atomZ[a];
-      }
-      __syncthreads();
-      if (m < e) {
-        // four independent counts: the comparisons do not wait on each other
-        int r0 = 0, r1 = 0, r2 = 0, r3 = 0, t = 0;
-        for (; t + 3 < cnt; t += 4) {
-          r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
-          r1 += (sz[t + 1] < mz) || (sz[t + 1] == mz && si[t + 1] < mi);
-          r2 += (sz[t + 2] < mz) || (sz[t + 2] == mz && si[t + 2] < mi);
-          r3 += (sz[t + 3] < mz) || (sz[t + 3] == mz && si[t + 3] < mi);
-        }
-        for (; t < cnt; ++t) r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
-        rank += (r0 + r1) + (r2 + r3);
+      } else {
+        si[t] = 0x7fffffff;
+        sz[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
       }
     }
-    if (m < e) slotAtom[ps + rank] = mi;
+    __syncthreads();
+    for (int k = 2; k <= P; k <<= 1) {
+      for (int j = k >> 1; j > 0; j >>= 1) {
+        for (int t = threadIdx.x; t < P; t += blockDim.x) {
+          const int u = t ^ j;
+          if (u > t) {
+            const double zt = sz[t], zu = sz[u];
+            const int it = si[t], iu = si[u];
+            const bool uLess = (zu < zt) || (zu == zt && iu < it);
+            // ascending where (t & k) == 0, descending elsewhere
+            if (uLess == ((t & k) == 0)) {
+              sz[t] = zu;
+              sz[u] = zt;
+              si[t] = iu;
+              si[u] = it;
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    for (int t = threadIdx.x; t < n; t += blockDim.x) slotAtom[ps + t] = si[t];
+  } else {
+    for (int base = s; base < e; base += blockDim.x) {
+      const int m = base + threadIdx.x;
+      const int mi = (m < e) ? tmpIdx[m] : 0;
+      const double mz = (m < e) ? atomZ[mi] : 0.0;
+      int rank = 0;
+      for (int cb = s; cb < e; cb += kMax) {
+        const int cnt = min(kMax, e - cb);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt; t += blockDim.x) {
+          const int a = tmpIdx[cb + t];
+          si[t] = a;
+          sz[t] = atomZ[a];
+        }
+        __syncthreads();
+        if (m < e) {
+          // four independent counts: the comparisons do not wait on each other
+          int r0 = 0, r1 = 0, r2 = 0, r3 = 0, t = 0;
+          for (; t + 3 < cnt; t += 4) {
+            r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+            r1 += (sz[t + 1] < mz) || (sz[t + 1] == mz && si[t + 1] < mi);
+            r2 += (sz[t + 2] < mz) || (sz[t + 2] == mz && si[t + 2] < mi);
+            r3 += (sz[t + 3] < mz) || (sz[t + 3] == mz && si[t + 3] < mi);
+          }
+          for (; t < cnt; ++t) r0 += (sz[t] < mz) || (sz[t] == mz && si[t] < mi);
+          rank += (r0 + r1) + (r2 + r3);
+        }
+      }
+      if (m < e) slotAtom[ps + rank] = mi;
+    }
   }
-  for (int p = ps + (e - s) + threadIdx.x; p < pe; p += blockDim.x) slotAtom[p] = -1;
+  for (int p = ps + n + threadIdx.x; p < pe; p += blockDim.x) slotAtom[p] = -1;
 }
 
 // One thread per slot, 8 consecutive lanes per cluster: FP64 origin and half
