@@ -47,6 +47,7 @@ __global__ void k_col_bin(int n, const ClusterGeom *__restrict__ geoms,
                           int *__restrict__ atomCol, double *__restrict__ atomZ,
                           int *__restrict__ colCount, long long *__restrict__ counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned act = __ballot_sync(0xffffffffu, i < n);  // lanes that go on
   if (i >= n) return;
   const int rep = atomRep ? atomRep[i] : 0;
   const ClusterGeom &g = geoms[rep];
@@ -63,7 +64,10 @@ __global__ void k_col_bin(int n, const ClusterGeom *__restrict__ geoms,
   const int col = colRank[colOff[rep] + cy * g.ncx + cx];
   atomCol[i] = col;
   atomZ[i] = sz;
-  atomicAdd(colCount + col, 1);
+  // one atomic per column among the warp's atoms (neighbouring atoms of a
+  // molecule-ordered system mostly share a column)
+  const unsigned same = __match_any_sync(act, col);
+  if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(colCount + col, __popc(same));
 }
 
 __global__ void k_col_pad(int nCols, const int *__restrict__ colCount, int *__restrict__ colPad) {
@@ -81,9 +85,17 @@ __global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
                               const int *__restrict__ colStart, int *__restrict__ colFill,
                               int *__restrict__ tmpIdx) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned act = __ballot_sync(0xffffffffu, i < n);  // lanes that go on
   if (i >= n) return;
   const int c = atomCol[i];
-  tmpIdx[colStart[c] + atomicAdd(colFill + c, 1)] = i;
+  // one atomic per column among the warp's atoms; lanes take consecutive
+  // places in lane order (the column sort fixes the final order anyway)
+  const unsigned same = __match_any_sync(act, c);
+  const int lane = threadIdx.x & 31, leader = __ffs(same) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(colFill + c, __popc(same));
+  base = __shfl_sync(same, base, leader);
+  tmpIdx[colStart[c] + base + __popc(same & ((1u << lane) - 1u))] = i;
 }
 
 // One column per block: its atoms in ascending (z, atom index) order into
