@@ -273,6 +273,12 @@ int mdbas_nb_engine_destroy(mdbas_nb_engine *e) {
   kspace_release(e);
   if (e->ev0) cudaEventDestroy(e->ev0);
   if (e->ev1) cudaEventDestroy(e->ev1);
+  if (e->side) {
+    cudaStreamSynchronize(e->side);
+    cudaStreamDestroy(e->side);
+    cudaEventDestroy(e->evFork);
+    cudaEventDestroy(e->evJoin);
+  }
   if (e->ownStream) cudaStreamDestroy(e->stream);
   delete e;
   return MDBAS_NB_OK;
@@ -463,12 +469,23 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
       e->grid = sms * 8;
       e->block = 256;
     }
+    if (!e->side) {
+      MDB_CUDA(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+      MDB_CUDA(cudaEventCreateWithFlags(&e->evFork, cudaEventDisableTiming));
+      MDB_CUDA(cudaEventCreateWithFlags(&e->evJoin, cudaEventDisableTiming));
+    }
+    // the exclusion correction on the side stream, overlapping the pair
+    // kernel's tail; the main stream waits for it before anything reads
+    MDB_CUDA(cudaEventRecord(e->evFork, s));
+    MDB_CUDA(cudaStreamWaitEvent(e->side, e->evFork, 0));
+    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(),
+                               e->exclFlat.as<int>(), e->x.as<double>(), e->y.as<double>(),
+                               e->z.as<double>(), e->q.as<double>(), e->side));
+    MDB_CUDA(cudaEventRecord(e->evJoin, e->side));
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev0, s));
     ENG_TRY(e, pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev1, s));
-    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(),
-                               e->exclFlat.as<int>(), e->x.as<double>(), e->y.as<double>(),
-                               e->z.as<double>(), e->q.as<double>(), s));
+    MDB_CUDA(cudaStreamWaitEvent(s, e->evJoin, 0));
   }
   if (e->timing) {
     MDB_CUDA(cudaEventSynchronize(e->ev1));

@@ -70,6 +70,10 @@ struct mdbas_nb_engine {
   long long launches = 0;
   bool timing = false;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // second stream of compute(): the exclusion correction runs beside the
+  // pair kernel (both add into the same fixed-point words)
+  cudaStream_t side = nullptr;
+  cudaEvent_t evFork = nullptr, evJoin = nullptr;
   double pairMs = 0.0;
   long long pairCount = 0;
   // velocity-Verlet state (md.cu)
