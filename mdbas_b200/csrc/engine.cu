@@ -170,6 +170,14 @@ static int acc_status(const mdbas_nb_engine *e) {
   return MDBAS_NB_OK;
 }
 
+int mdbas::engine_side_stream(mdbas_nb_engine *e) {
+  if (e->side) return MDBAS_NB_OK;
+  MDB_CUDA(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
+  MDB_CUDA(cudaEventCreateWithFlags(&e->evFork, cudaEventDisableTiming));
+  MDB_CUDA(cudaEventCreateWithFlags(&e->evJoin, cudaEventDisableTiming));
+  return MDBAS_NB_OK;
+}
+
 int mdbas::engine_resolve_build(mdbas_nb_engine *e) {
   if (!e->buildPending) return MDBAS_NB_OK;
   e->buildPending = false;
@@ -469,11 +477,7 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
       e->grid = sms * 8;
       e->block = 256;
     }
-    if (!e->side) {
-      MDB_CUDA(cudaStreamCreateWithFlags(&e->side, cudaStreamNonBlocking));
-      MDB_CUDA(cudaEventCreateWithFlags(&e->evFork, cudaEventDisableTiming));
-      MDB_CUDA(cudaEventCreateWithFlags(&e->evJoin, cudaEventDisableTiming));
-    }
+    ENG_TRY(e, engine_side_stream(e));
     // the exclusion correction on the side stream, overlapping the pair
     // kernel's tail; the main stream waits for it before anything reads
     MDB_CUDA(cudaEventRecord(e->evFork, s));

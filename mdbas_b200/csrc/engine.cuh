@@ -122,6 +122,9 @@ int md_kspace(mdbas_nb_engine *e, double *f, cudaStream_t s);
 // overflowing list build again with room, synchronously, and redo the
 // evaluation if one ran on the empty list; non-finite positions are an error.
 int engine_resolve_build(mdbas_nb_engine *e);
+// The engine's side stream and its fork/join events (created once, outside
+// any stream capture).
+int engine_side_stream(mdbas_nb_engine *e);
 void kspace_release(mdbas_nb_engine *e);
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);
