@@ -405,14 +405,20 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]);
  * the number of pairs; pairs (2*capacity ints) may be NULL to query it. */
 int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, long long capacity,
                                  long long *count);
-/* Pair kernel variant of the mixed-precision path: 2 (default) computes every
- * pair of each 8x8 cluster pair in one warp step per cluster pair, a lane's
- * two pairs in packed f32x2 arithmetic, with each chunk of 8 cluster pairs
- * staged in shared memory; 0 is the same in scalar FP32 without staging;
- * 1 filters the pairs first and computes only in-cut-off pairs from per-atom
- * queues; 3 is variant 2 with each chunk's j data brought into shared memory
- * by asynchronous bulk copies (cp.async.bulk with an mbarrier, double
- * buffered) instead of per-lane loads -- the same results bit for bit. */
+/* Pair kernel variant of the mixed-precision path: 4 (default) takes two
+ * 4-atom halves of j clusters per warp step against an 8-atom i cluster, a
+ * lane's two pairs in packed f32x2 arithmetic, over the inner list (the
+ * halves holding a pair within the cut-off, written by the list build for
+ * the build's positions, or within the pruning radius during dynamics) and
+ * over the full list once positions have changed since the build; 2 computes
+ * every pair of each 8x8 cluster pair in one warp step, a lane's two pairs in
+ * packed f32x2 arithmetic, with each chunk of 8 cluster pairs staged in
+ * shared memory; 0 is the same in scalar FP32 without staging; 1 filters the
+ * pairs first and computes only in-cut-off pairs from per-atom queues; 3 is
+ * variant 2 with each chunk's j data brought into shared memory by
+ * asynchronous bulk copies (cp.async.bulk with an mbarrier, double buffered)
+ * instead of per-lane loads -- the same results as 2 bit for bit.  Variants
+ * 0-3 always walk the full list. */
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
 /* Autotuner of the mixed-precision pair kernel: times each variant and
  * launch shape (threads per block x blocks per SM) on the current list with

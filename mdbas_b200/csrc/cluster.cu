@@ -28,6 +28,7 @@
 #include <vector>
 
 #include "cluster.cuh"
+#include "list_ref.cuh"
 
 namespace mdbas {
 
@@ -316,63 +317,133 @@ struct SearchCols {
   int prefix[kSearchCols + 1];  // cluster counts before the column
 };
 
+// Outputs of the search: the list (entries with 64-bit masks at the list
+// radius, exactly MDBas's pairs) and the inner list (j-cluster halves with a
+// pair within sqrt(rin2), 32-bit masks).
+struct SearchOut {
+  CPairEntry *entries;
+  uint2 *masks;
+  int4 *items;
+  long long *counters;
+  long long entryCap, itemCap;
+  HalfEntry *hent;
+  unsigned *hmask;
+  int4 *hitems;
+  long long *hcounters;
+  long long hEntryCap, hItemCap;
+  float rin2;
+};
+
+// MDBas's FP64 squared distance of atoms a and c, the expression of the list
+// builder it would run (either order of the two atoms gives the same bits).
+// listMode 1: link cells (src/list.c:1932-1936, 2051-2055): fractional
+// coordinates + 0.5, their difference plus the cell wrap's shift (the one
+// image within the list radius: the box holds at least three cells of that
+// width), mapped back by the box rows.  listMode 0: dist() (src/utils.c:
+// 38-80) of x[c] - x[a].
+__device__ __noinline__ double mdbas_pair_r2(const DevBox &b, int listMode,
+                                             const double *__restrict__ x,
+                                             const double *__restrict__ y,
+                                             const double *__restrict__ z, int a, int c) {
+  if (listMode) {
+    const double xa = dadd(dadd(dadd(dmul(x[a], b.u1), dmul(y[a], b.u2)), dmul(z[a], b.u3)), 0.5);
+    const double ya = dadd(dadd(dadd(dmul(x[a], b.v1), dmul(y[a], b.v2)), dmul(z[a], b.v3)), 0.5);
+    const double za = dadd(dadd(dadd(dmul(x[a], b.w1), dmul(y[a], b.w2)), dmul(z[a], b.w3)), 0.5);
+    const double xc = dadd(dadd(dadd(dmul(x[c], b.u1), dmul(y[c], b.u2)), dmul(z[c], b.u3)), 0.5);
+    const double yc = dadd(dadd(dadd(dmul(x[c], b.v1), dmul(y[c], b.v2)), dmul(z[c], b.v3)), 0.5);
+    const double zc = dadd(dadd(dadd(dmul(x[c], b.w1), dmul(y[c], b.w2)), dmul(z[c], b.w3)), 0.5);
+    double xt = dsub(xc, xa), yt = dsub(yc, ya), zt = dsub(zc, za);
+    xt = dadd(xt, -rint(xt));
+    yt = dadd(yt, -rint(yt));
+    zt = dadd(zt, -rint(zt));
+    const double xd = dadd(dadd(dmul(xt, b.a1), dmul(yt, b.b1)), dmul(zt, b.c1));
+    const double yd = dadd(dadd(dmul(xt, b.a2), dmul(yt, b.b2)), dmul(zt, b.c2));
+    const double zd = dadd(dadd(dmul(xt, b.a3), dmul(yt, b.b3)), dmul(zt, b.c3));
+    return dadd(dadd(dmul(xd, xd), dmul(yd, yd)), dmul(zd, zd));
+  }
+  double dx = dsub(x[c], x[a]), dy = dsub(y[c], y[a]), dz = dsub(z[c], z[a]);
+  return dist_d(b, dx, dy, dz);
+}
+
 // Flush the first cnt (<= kItemMax) buffered entries as one work item.  Lane
 // k builds entry k's 64-bit interaction mask on its own: bit i + 8 j (j < 4
 // in .x, j >= 4 in .y at i + 8 (j - 4)) for the pair (i atom i, j atom j)
 // within the list radius, both slots real, j > i on the cluster's own entry,
 // not an exclusion (checked only when the j cluster lies in the range of
 // clusters holding a partner of the i cluster's atoms: [pcLo, pcHi]) and not
-// both frozen.  The j clusters are staged transposed so that the 32 lanes
-// read 32 different entries without bank conflicts.
+// both frozen.  Distances are FP32; pairs in the band around the list radius
+// are settled by MDBas's FP64 expression, so the list's pairs are MDBas's.
+// The same pass marks the pairs within the inner radius; the halves of the
+// entries holding such pairs become the item's inner-list entries.  The j
+// clusters are staged transposed so that the 32 lanes read 32 different
+// entries without bank conflicts.
 __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double4 oi,
-                           const float4 *__restrict__ xq, const ClusterGeom &g, int nreal_i,
-                           int pcLo, int pcHi, unsigned fimask,
+                           const float4 *__restrict__ xq, const ClusterGeom &g,
+                           const DevBox &box, int nreal_i, int pcLo, int pcHi, unsigned fimask,
                            const int *__restrict__ exclFlat, const int *__restrict__ slotOf,
                            const int *__restrict__ slotAtom, const int *__restrict__ frozen,
-                           const double4 *__restrict__ origin,
-                           CPairEntry *__restrict__ entries, uint2 *__restrict__ masks,
-                           int4 *__restrict__ items, long long *__restrict__ counters,
-                           long long entryCap, long long itemCap) {
+                           const double *__restrict__ px, const double *__restrict__ py,
+                           const double *__restrict__ pz, const double4 *__restrict__ origin,
+                           const SearchOut &o) {
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
     const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
     if (k < cnt) B.sj[j * kItemMax + k] = xq[B.j[k] * kClusterSize + j];
   }
   __syncwarp();
+  uint2 inner = make_uint2(0u, 0u);
   if (lane < cnt) {
     const int k = lane;
     const int cj = B.j[k], nrj = B.nreal[k];
     const float4 sh = B.sh[k];
-    float jx[kClusterSize], jy[kClusterSize], jz[kClusterSize];
+    // the j atoms h and h + 4 side by side, for packed distances
+    float2 jx[4], jy[4], jz[4];
 #pragma unroll
-    for (int j = 0; j < kClusterSize; ++j) {
-      const float4 v = B.sj[j * kItemMax + k];
-      jx[j] = v.x;
-      jy[j] = v.y;
-      jz[j] = v.z;
+    for (int h = 0; h < 4; ++h) {
+      const float4 a = B.sj[h * kItemMax + k], b = B.sj[(h + 4) * kItemMax + k];
+      jx[h] = make_float2(a.x, b.x);
+      jy[h] = make_float2(a.y, b.y);
+      jz[h] = make_float2(a.z, b.z);
     }
-    unsigned lo = 0u, hi = 0u;
-#pragma unroll
+    // per pair: inside the band's lower edge (lo), inside its upper edge
+    // (cand), inside the inner radius (in)
+    unsigned lo0 = 0u, lo1 = 0u, ca0 = 0u, ca1 = 0u, in0 = 0u, in1 = 0u;
+    // the i loop stays rolled (a small loop body keeps the instruction cache
+    // warm); per i atom the four j pairs give byte-strided rows of bits
+#pragma unroll 1
     for (int i = 0; i < kClusterSize; ++i) {
-      // pair distances at build time: FP32 shift from the FP32 origins
-      // (rlist2 carries a 1e-5 margin)
       const float4 xi = B.si[i];
-      const float tx = sh.x - xi.x, ty = sh.y - xi.y, tz = sh.z - xi.z;
+      const float2 tx = make_float2(sh.x - xi.x, sh.x - xi.x);
+      const float2 ty = make_float2(sh.y - xi.y, sh.y - xi.y);
+      const float2 tz = make_float2(sh.z - xi.z, sh.z - xi.z);
+      unsigned rl0 = 0u, rl1 = 0u, rc0 = 0u, rc1 = 0u, ri0 = 0u, ri1 = 0u;
 #pragma unroll
-      for (int j = 0; j < kClusterSize; ++j) {
-        const float ax = jx[j] + tx, ay = jy[j] + ty, az = jz[j] + tz;
-        const unsigned in = (ax * ax + ay * ay + az * az <= g.rlist2) ? 1u : 0u;
-        if (j < 4) lo |= in << (i + 8 * j);
-        else hi |= in << (i + 8 * (j - 4));
+      for (int h = 0; h < 4; ++h) {
+        const float2 ax = __fadd2_rn(jx[h], tx), ay = __fadd2_rn(jy[h], ty),
+                     az = __fadd2_rn(jz[h], tz);
+        const float2 r2 = __ffma2_rn(ax, ax, __ffma2_rn(ay, ay, __fmul2_rn(az, az)));
+        const unsigned bit = 1u << (8 * h);
+        if (r2.x <= g.rlo2) rl0 |= bit;
+        if (r2.y <= g.rlo2) rl1 |= bit;
+        if (r2.x <= g.rhi2) rc0 |= bit;
+        if (r2.y <= g.rhi2) rc1 |= bit;
+        if (r2.x <= o.rin2) ri0 |= bit;
+        if (r2.y <= o.rin2) ri1 |= bit;
       }
+      lo0 |= rl0 << i;
+      lo1 |= rl1 << i;
+      ca0 |= rc0 << i;
+      ca1 |= rc1 << i;
+      in0 |= ri0 << i;
+      in1 |= ri1 << i;
     }
     // padding slots of either cluster
     const unsigned irow = (nreal_i >= 8 ? 0xffu : ((1u << nreal_i) - 1u)) * 0x01010101u;
-    lo &= irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
-    hi &= irow & (nrj >= 8 ? 0xffffffffu : (nrj <= 4 ? 0u : ((1u << (8 * (nrj - 4))) - 1u)));
+    unsigned m0 = irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
+    unsigned m1 = irow & (nrj >= 8 ? 0xffffffffu : (nrj <= 4 ? 0u : ((1u << (8 * (nrj - 4))) - 1u)));
     if (cj == ci && B.sidx[k] == 13) {  // the cluster with itself: j > i
-      lo &= 0x07030100u;
-      hi &= 0x7f3f1f0fu;
+      m0 &= 0x07030100u;
+      m1 &= 0x7f3f1f0fu;
     }
     if (cj >= pcLo && cj <= pcHi) {
       for (int i = 0; i < kClusterSize; ++i) {
@@ -381,8 +452,8 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
           const int p = r < kExclRegs ? B.ps[i][r] : slotOf[__ldg(exclFlat + e0 + r)];
           if ((p >> 3) == cj) {
             const int j = p & 7;
-            if (j < 4) lo &= ~(1u << (i + 8 * j));
-            else hi &= ~(1u << (i + 8 * (j - 4)));
+            if (j < 4) m0 &= ~(1u << (i + 8 * j));
+            else m1 &= ~(1u << (i + 8 * (j - 4)));
           }
         }
       }
@@ -392,12 +463,27 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
         const int ja = slotAtom[cj * kClusterSize + j];
         if (ja >= 0 && frozen[ja]) {
           const unsigned m = fimask << (8 * (j & 3));
-          if (j < 4) lo &= ~m;
-          else hi &= ~m;
+          if (j < 4) m0 &= ~m;
+          else m1 &= ~m;
         }
       }
     }
-    B.mask[k] = make_uint2(lo, hi);
+    // pairs in the band: MDBas's own FP64 distance decides
+    unsigned amb0 = ca0 & ~lo0 & m0, amb1 = ca1 & ~lo1 & m1;
+    unsigned fin0 = lo0 & m0, fin1 = lo1 & m1;
+    while (amb0 | amb1) {
+      const bool second = amb0 == 0u;
+      const unsigned v = second ? amb1 : amb0;
+      const int b = __ffs(v) - 1;
+      if (second) amb1 &= amb1 - 1u; else amb0 &= amb0 - 1u;
+      const int i = b & 7, j = (b >> 3) + (second ? 4 : 0);
+      const int a = slotAtom[ci * kClusterSize + i], c = slotAtom[cj * kClusterSize + j];
+      if (mdbas_pair_r2(box, g.listMode, px, py, pz, a, c) <= g.cutnb2) {
+        if (second) fin1 |= 1u << b; else fin0 |= 1u << b;
+      }
+    }
+    B.mask[k] = make_uint2(fin0, fin1);
+    inner = make_uint2(in0 & fin0, in1 & fin1);
   }
   __syncwarp();
   // keep the entries with at least one pair within the list radius
@@ -405,17 +491,28 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
   const unsigned km = __ballot_sync(0xffffffffu, keep);
   const int nkeep = __popc(km);
   if (nkeep == 0) return;
-  long long e0 = 0, it = 0;
+  const unsigned hA = __ballot_sync(0xffffffffu, inner.x != 0u);
+  const unsigned hB = __ballot_sync(0xffffffffu, inner.y != 0u);
+  const int nA = __popc(hA), nin = nA + __popc(hB);
+  long long e0 = 0, it = 0, h0 = 0, hit = 0;
   if (lane == 0) {
-    e0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 0),
+    e0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 0),
                               (unsigned long long)nkeep);
-    it = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(counters + 1), 1ull);
+    it = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 1), 1ull);
+    if (nin > 0) {
+      h0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 0),
+                                (unsigned long long)nin);
+      hit = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 1), 1ull);
+    }
   }
   e0 = __shfl_sync(0xffffffffu, e0, 0);
   it = __shfl_sync(0xffffffffu, it, 0);
-  if (e0 + nkeep > entryCap || it >= itemCap) {
+  h0 = __shfl_sync(0xffffffffu, h0, 0);
+  hit = __shfl_sync(0xffffffffu, hit, 0);
+  if (e0 + nkeep > o.entryCap || it >= o.itemCap ||
+      (nin > 0 && (h0 + nin > o.hEntryCap || hit >= o.hItemCap))) {
     if (lane == 0)
-      atomicOr(reinterpret_cast<unsigned long long *>(counters + 2),
+      atomicOr(reinterpret_cast<unsigned long long *>(o.counters + 2),
                (unsigned long long)CL_OVERFLOW);
     return;
   }
@@ -430,15 +527,40 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
     en.sx = (float)(oj.x + sx * g.Lx - oi.x);
     en.sy = (float)(oj.y + sy * g.Ly - oi.y);
     en.sz = (float)(oj.z + sz * g.Lz - oi.z);
-    entries[e0 + pos] = en;
-    masks[e0 + pos] = B.mask[k];
+    o.entries[e0 + pos] = en;
+    o.masks[e0 + pos] = B.mask[k];
+    const unsigned lt = (1u << lane) - 1u;
+    if (inner.x != 0u) {
+      const long long q = h0 + __popc(hA & lt);
+      HalfEntry he;
+      he.jh = 2 * cj;
+      he.sx = en.sx;
+      he.sy = en.sy;
+      he.sz = en.sz;
+      o.hent[q] = he;
+      o.hmask[q] = inner.x;
+    }
+    if (inner.y != 0u) {
+      const long long q = h0 + nA + __popc(hB & lt);
+      HalfEntry he;
+      he.jh = 2 * cj + 1;
+      he.sx = en.sx;
+      he.sy = en.sy;
+      he.sz = en.sz;
+      o.hent[q] = he;
+      o.hmask[q] = inner.y;
+    }
   }
-  if (lane == 0) items[it] = make_int4(ci, (int)e0, nkeep, 0);
+  if (lane == 0) {
+    o.items[it] = make_int4(ci, (int)e0, nkeep, 0);
+    if (nin > 0) o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
+  }
 }
 
 // (at most 96 registers: five blocks of four warps per SM)
 __global__ void __launch_bounds__(kSearchThreads, 5)
 k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
+         const DevBox *__restrict__ boxes,
          const int *__restrict__ clusterRep, const int *__restrict__ colOff,
          const int *__restrict__ colRank,
          const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
@@ -447,9 +569,8 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
          const int *__restrict__ slotOf, const int *__restrict__ frozen,
          const int *__restrict__ exclStart, const int *__restrict__ exclFlat,
          const int *__restrict__ hmaxBits, const float4 *__restrict__ xq,
-         CPairEntry *__restrict__ entries,
-         uint2 *__restrict__ masks, int4 *__restrict__ items, long long *__restrict__ counters,
-         long long entryCap, long long itemCap) {
+         const double *__restrict__ px, const double *__restrict__ py,
+         const double *__restrict__ pz, const SearchOut o) {
   __shared__ SearchBuf bufs[kSearchThreads / 32];
   __shared__ SearchCols colbufs[kSearchThreads / 32];
   const int lane = threadIdx.x & 31;
@@ -458,6 +579,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   SearchBuf &B = bufs[threadIdx.x >> 5];
   const int rep = clusterRep ? clusterRep[ci] : 0;
   const ClusterGeom g = geoms[rep];
+  const DevBox &box = boxes[rep];
   const int colBase = colOff[rep];
   hmaxBits += 4 * rep;
 
@@ -652,9 +774,8 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
         cnt += __popc(m);
         __syncwarp();
         if (cnt >= kItemMax) {
-          flush_item(B, kItemMax, ci, lane, oi, xq, g, nreal_i, pcLo, pcHi, fimask, exclFlat,
-                     slotOf, slotAtom, frozen, origin, entries, masks, items, counters, entryCap,
-                     itemCap);
+          flush_item(B, kItemMax, ci, lane, oi, xq, g, box, nreal_i, pcLo, pcHi, fimask,
+                     exclFlat, slotOf, slotAtom, frozen, px, py, pz, origin, o);
           __syncwarp();
           const int rem = cnt - kItemMax;
           if (lane < rem) {
@@ -672,12 +793,12 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
     __syncwarp();
   }
   if (cnt > 0)
-    flush_item(B, cnt, ci, lane, oi, xq, g, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
-               slotAtom, frozen, origin, entries, masks, items, counters, entryCap, itemCap);
+    flush_item(B, cnt, ci, lane, oi, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
+               slotAtom, frozen, px, py, pz, origin, o);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, o);
   if (lane == 0)
-    atomicAdd(reinterpret_cast<unsigned long long *>(counters + 3), (unsigned long long)cand);
+    atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 3), (unsigned long long)cand);
 }
 
 __global__ void k_refresh(const int *__restrict__ nSlotsDev,
@@ -707,15 +828,16 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev,
   p[6] = v.w;
 }
 
-// One warp per item of the list: recompute each entry's mask at the inner
-// radius from the current layout (same lane/bit mapping as the pair kernel)
-// and append the entries that keep a pair to the inner list.
+// One warp per item of the list: recompute each entry's pairs within the
+// inner radius from the current layout (lane = (i atom, j atoms h and h + 4),
+// as in the search's bit order) and append the entry halves that keep a pair
+// to the inner list.
 __global__ void __launch_bounds__(128)
 k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
         const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
-        const float4 *__restrict__ xq, float rin2, CPairEntry *__restrict__ entriesOut,
-        uint2 *__restrict__ masksOut, int4 *__restrict__ itemsOut,
-        long long *__restrict__ countersOut, long long entryCap, long long itemCap) {
+        const float4 *__restrict__ xq, float rin2, HalfEntry *__restrict__ hent,
+        unsigned *__restrict__ hmask, int4 *__restrict__ hitems,
+        long long *__restrict__ hcounters, long long hEntryCap, long long hItemCap) {
   const int lane = threadIdx.x & 31;
   const int il = lane & 7, jl = lane >> 3;
   const long long nItems = counters[1];
@@ -742,45 +864,64 @@ k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
         myEn = en;
       }
     }
-    const bool keep = lane < ne && (mine.x | mine.y) != 0u;
-    const unsigned km = __ballot_sync(0xffffffffu, keep);
-    const int nkeep = __popc(km);
-    if (nkeep == 0) continue;
-    long long eo = 0, io = 0;
+    const unsigned hA = __ballot_sync(0xffffffffu, lane < ne && mine.x != 0u);
+    const unsigned hB = __ballot_sync(0xffffffffu, lane < ne && mine.y != 0u);
+    const int nA = __popc(hA), nin = nA + __popc(hB);
+    if (nin == 0) continue;
+    long long h0 = 0, io = 0;
     if (lane == 0) {
-      eo = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(countersOut + 0),
-                                (unsigned long long)nkeep);
-      io = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(countersOut + 1), 1ull);
+      h0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 0),
+                                (unsigned long long)nin);
+      io = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 1), 1ull);
     }
-    eo = __shfl_sync(0xffffffffu, eo, 0);
+    h0 = __shfl_sync(0xffffffffu, h0, 0);
     io = __shfl_sync(0xffffffffu, io, 0);
-    if (eo + nkeep > entryCap || io >= itemCap) {
+    if (h0 + nin > hEntryCap || io >= hItemCap) {
       if (lane == 0)
-        atomicOr(reinterpret_cast<unsigned long long *>(countersOut + 2),
+        atomicOr(reinterpret_cast<unsigned long long *>(hcounters + 2),
                  (unsigned long long)CL_OVERFLOW);
       continue;
     }
-    if (keep) {
-      const int pos = __popc(km & ((1u << lane) - 1u));
-      entriesOut[eo + pos] = myEn;
-      masksOut[eo + pos] = mine;
+    const unsigned lt = (1u << lane) - 1u;
+    if (lane < ne && mine.x != 0u) {
+      const long long q = h0 + __popc(hA & lt);
+      HalfEntry he;
+      he.jh = 2 * myEn.j;
+      he.sx = myEn.sx;
+      he.sy = myEn.sy;
+      he.sz = myEn.sz;
+      hent[q] = he;
+      hmask[q] = mine.x;
     }
-    if (lane == 0) itemsOut[io] = make_int4(ci, (int)eo, nkeep, 0);
+    if (lane < ne && mine.y != 0u) {
+      const long long q = h0 + nA + __popc(hB & lt);
+      HalfEntry he;
+      he.jh = 2 * myEn.j + 1;
+      he.sx = myEn.sx;
+      he.sy = myEn.sy;
+      he.sz = myEn.sz;
+      hent[q] = he;
+      hmask[q] = mine.y;
+    }
+    if (lane == 0) hitems[io] = make_int4(ci, (int)h0, nin, 0);
   }
 }
 
 // Latch a search's (or prune's) error bits into the sticky word.  A list
 // that overflowed is unusable: its item count may point past the item buffer
-// and some items were never written, so both counts are zeroed and the pair
-// kernels that follow in the same stream (or graph) see an empty list until
-// the host rebuilds with room.
-__global__ void k_latch(long long *__restrict__ counters, long long *__restrict__ sticky) {
+// and some items were never written, so the counts of both lists are zeroed
+// and the pair kernels that follow in the same stream (or graph) see an
+// empty list until the host rebuilds with room.
+__global__ void k_latch(long long *__restrict__ counters, long long *__restrict__ hcounters,
+                        long long *__restrict__ sticky) {
   if (threadIdx.x == 0) {
-    const long long f = counters[2];
+    const long long f = counters[2] | hcounters[2];
     sticky[0] |= f;
     if (f & CL_OVERFLOW) {
       counters[0] = 0;
       counters[1] = 0;
+      hcounters[0] = 0;
+      hcounters[1] = 0;
     }
   }
 }
@@ -802,7 +943,7 @@ unsigned morton2(unsigned x, unsigned y) {
 namespace {
 
 // Column grid of one box (orthorhombic), or an error status.
-int make_geom(const DevBox &b, int n, double cutOff, double delr, ClusterGeom &g) {
+int make_geom(const DevBox &b, int n, double cutOff, double delr, int listRule, ClusterGeom &g) {
   if (b.type != CUBIC && b.type != ORBIC) return MDBAS_NB_ERR_UNSUPPORTED;
   if (n <= 0) return MDBAS_NB_ERR_ARG;
   g = ClusterGeom{};
@@ -827,28 +968,34 @@ int make_geom(const DevBox &b, int n, double cutOff, double delr, ClusterGeom &g
     if (g.Dx >= g.ncx) g.Dx = g.ncx - 1;
     if (g.Dy >= g.ncy) g.Dy = g.ncy - 1;
   }
-  g.rlist2 = (float)(rlist * rlist * (1.0 + 1e-5));
+  // MDBas's list radius (src/list.c: cutnb = cutOff + delr, compared with its
+  // square) and the FP32 band around it
+  g.cutnb2 = rlist * rlist;
+  g.rlo2 = (float)(g.cutnb2 * (1.0 - 2e-5));
+  g.rhi2 = (float)(g.cutnb2 * (1.0 + 2e-5));
+  g.rlist2 = g.rhi2;
+  g.listMode = makelist_uses_link_cells(b, cutOff, delr, listRule & 7, (listRule >> 3) & 1);
   return MDBAS_NB_OK;
 }
 
 bool same_geom(const ClusterGeom &a, const ClusterGeom &b) {
   return a.ncx == b.ncx && a.ncy == b.ncy && a.Dx == b.Dx && a.Dy == b.Dy && a.Lx == b.Lx &&
-         a.Ly == b.Ly && a.Lz == b.Lz && a.rlist2 == b.rlist2;
+         a.Ly == b.Ly && a.Lz == b.Lz && a.rlist2 == b.rlist2 && a.listMode == b.listMode;
 }
 
 }  // namespace
 
 int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const int *atomOff,
-                  double cutOff, double delr, double sqrtC, const double *x, const double *y,
-                  const double *z, const double *q, const double *eps, const double *sig,
-                  const int *frozen, const int *exclStart, const int *exclFlat, cudaStream_t s,
-                  bool sync) {
+                  double cutOff, double delr, int listRule, double sqrtC, const double *x,
+                  const double *y, const double *z, const double *q, const double *eps,
+                  const double *sig, const int *frozen, const int *exclStart,
+                  const int *exclFlat, cudaStream_t s, bool sync) {
   if (nRep <= 0 || n <= 0 || atomOff[0] != 0 || atomOff[nRep] != n) return MDBAS_NB_ERR_ARG;
   std::vector<ClusterGeom> geoms(nRep);
   std::vector<int> colOff(nRep + 1, 0);
   for (int r = 0; r < nRep; ++r) {
     const int nr = atomOff[r + 1] - atomOff[r];
-    MDB_TRY(make_geom(boxes[r], nr, cutOff, delr, geoms[r]));
+    MDB_TRY(make_geom(boxes[r], nr, cutOff, delr, listRule, geoms[r]));
     colOff[r + 1] = colOff[r] + geoms[r].ncx * geoms[r].ncy;
   }
   const int nCols = colOff[nRep];
@@ -969,37 +1116,59 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
              w.ljp.as<float>(), w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
 
   // Cluster-pair search; in the synchronising form grow the list and search
-  // again if it overflowed.
+  // again if it overflowed.  The inner list holds at most two halves per
+  // entry, so it never overflows on its own.
   if (w.entryCap == 0) {
     w.entryCap = (long long)w.clCap * 160 + 4096;
     w.itemCap = w.entryCap / kItemMax + w.clCap + 1024;
   }
+  const float rin2 = w.rin2 > 0.f ? w.rin2 : (float)(cutOff * cutOff * (1.0 + 1e-5));
   for (int attempt = 0; attempt < 4; ++attempt) {
+    w.inEntryCap = 2 * w.entryCap;
+    w.inItemCap = w.itemCap;
     if (sync) {
       MDB_TRY(w.entries.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
       MDB_TRY(w.masks.ensure(sizeof(uint2) * (size_t)w.entryCap));
       MDB_TRY(w.items.ensure(sizeof(int4) * (size_t)w.itemCap));
-      MDB_TRY(w.entriesIn.ensure(sizeof(CPairEntry) * (size_t)w.entryCap));
-      MDB_TRY(w.masksIn.ensure(sizeof(uint2) * (size_t)w.entryCap));
-      MDB_TRY(w.itemsIn.ensure(sizeof(int4) * (size_t)w.itemCap));
+      MDB_TRY(w.entriesIn.ensure(sizeof(HalfEntry) * (size_t)w.inEntryCap));
+      MDB_TRY(w.masksIn.ensure(sizeof(unsigned) * (size_t)w.inEntryCap));
+      MDB_TRY(w.itemsIn.ensure(sizeof(int4) * (size_t)w.inItemCap));
       MDB_TRY(w.countersIn.ensure(sizeof(long long) * 4));
     }
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
     MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long), s));
+    MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 4, s));
+    SearchOut o;
+    o.entries = w.entries.as<CPairEntry>();
+    o.masks = w.masks.as<uint2>();
+    o.items = w.items.as<int4>();
+    o.counters = w.counters.as<long long>();
+    o.entryCap = w.entryCap;
+    o.itemCap = w.itemCap;
+    o.hent = w.entriesIn.as<HalfEntry>();
+    o.hmask = w.masksIn.as<unsigned>();
+    o.hitems = w.itemsIn.as<int4>();
+    o.hcounters = w.countersIn.as<long long>();
+    o.hEntryCap = w.inEntryCap;
+    o.hItemCap = w.inItemCap;
+    o.rin2 = rin2;
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
-               w.nSlotsDev(), gd, w.clusterRepDev(), w.colOff.as<int>(), w.colRank.as<int>(),
-               w.colClStart.as<int>(), w.clusterXY.as<int>(), w.origin.as<double4>(),
-               w.originF.as<float4>(), w.half.as<float4>(), w.slotAtom.as<int>(),
-               w.slotOf.as<int>(), frozen, exclStart, exclFlat, w.hmax.as<int>(),
-               w.xq.as<float4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
-               w.items.as<int4>(), w.counters.as<long long>(), w.entryCap, w.itemCap);
+               w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
+               w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
+               w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
+               w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
+               w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
+    w.innerRin2 = rin2;
     if (!sync) {
-      MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.sticky.as<long long>());
+      w.useInner = true;
+      MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.countersIn.as<long long>(),
+                 w.sticky.as<long long>());
       return MDBAS_NB_OK;
     }
-    long long flags[4];
+    long long flags[4], hflags[4];
     int nSlots = 0;
     MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+    MDB_CUDA(cudaMemcpyAsync(hflags, w.countersIn.p, sizeof(hflags), cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaMemcpyAsync(&nSlots, w.nSlotsDev(), sizeof(int), cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaStreamSynchronize(s));
     if (flags[2] & CL_NONFINITE) return MDBAS_NB_ERR_NONFINITE;
@@ -1007,7 +1176,12 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     w.nClusters = nSlots / kClusterSize;
     w.nEntries = flags[0];
     w.nItems = flags[1];
-    if (!(flags[2] & CL_OVERFLOW)) return MDBAS_NB_OK;
+    w.nInEntries = hflags[0];
+    w.nInItems = hflags[1];
+    if (!(flags[2] & CL_OVERFLOW)) {
+      w.useInner = true;
+      return MDBAS_NB_OK;
+    }
     // the search does not clear the overflow bit; the next attempt starts clean
     MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 2, 0, sizeof(long long), s));
     w.entryCap = (long long)(flags[0] * 1.25) + 4096;
@@ -1017,12 +1191,34 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
 }
 
 int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
-                  double sqrtC, const double *x, const double *y, const double *z,
-                  const double *q, const double *eps, const double *sig, const int *frozen,
-                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync) {
+                  int listRule, double sqrtC, const double *x, const double *y,
+                  const double *z, const double *q, const double *eps, const double *sig,
+                  const int *frozen, const int *exclStart, const int *exclFlat, cudaStream_t s,
+                  bool sync) {
   const int off[2] = {0, n};
-  return cluster_build(w, n, 1, &b, off, cutOff, delr, sqrtC, x, y, z, q, eps, sig, frozen,
-                       exclStart, exclFlat, s, sync);
+  return cluster_build(w, n, 1, &b, off, cutOff, delr, listRule, sqrtC, x, y, z, q, eps, sig,
+                       frozen, exclStart, exclFlat, s, sync);
+}
+
+void cluster_symmetric_excl(int n, const int *start, const int *flat, std::vector<int> &outStart,
+                            std::vector<int> &outFlat) {
+  std::vector<std::vector<int>> rows(n);
+  for (int i = 0; i < n; ++i)
+    for (int k = start[i]; k < start[i + 1]; ++k) {
+      const int j = flat[k];
+      if (j == i) continue;
+      rows[i].push_back(j);
+      rows[j].push_back(i);
+    }
+  outStart.assign(n + 1, 0);
+  outFlat.clear();
+  for (int i = 0; i < n; ++i) {
+    std::vector<int> &r = rows[i];
+    std::sort(r.begin(), r.end());
+    r.erase(std::unique(r.begin(), r.end()), r.end());
+    outFlat.insert(outFlat.end(), r.begin(), r.end());
+    outStart[i + 1] = (int)outFlat.size();
+  }
 }
 
 int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s) {
@@ -1033,29 +1229,39 @@ int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s) {
   MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 4, s));
   MDB_LAUNCH(k_prune, sms * 16, 128, 0, s, w.counters.as<long long>(), w.items.as<int4>(),
              w.entries.as<CPairEntry>(), w.masks.as<uint2>(), w.xq.as<float4>(), rin2,
-             w.entriesIn.as<CPairEntry>(), w.masksIn.as<uint2>(), w.itemsIn.as<int4>(),
-             w.countersIn.as<long long>(), w.entryCap, w.itemCap);
-  MDB_LAUNCH(k_latch, 1, 32, 0, s, w.countersIn.as<long long>(), w.sticky.as<long long>());
+             w.entriesIn.as<HalfEntry>(), w.masksIn.as<unsigned>(), w.itemsIn.as<int4>(),
+             w.countersIn.as<long long>(), w.inEntryCap, w.inItemCap);
+  MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.countersIn.as<long long>(),
+             w.sticky.as<long long>());
+  w.innerRin2 = rin2;
+  w.useInner = true;
   return MDBAS_NB_OK;
 }
 
 int cluster_read_counts(ClusterWork &w, cudaStream_t s) {
   if (!w.counters.p || w.nCols <= 0) return MDBAS_NB_ERR_STATE;
-  long long flags[4];
+  long long flags[4], hflags[4] = {0, 0, 0, 0};
   int nSlots = 0;
   MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
+  if (w.countersIn.p)
+    MDB_CUDA(cudaMemcpyAsync(hflags, w.countersIn.p, sizeof(hflags), cudaMemcpyDeviceToHost, s));
   MDB_CUDA(cudaMemcpyAsync(&nSlots, w.nSlotsDev(), sizeof(int), cudaMemcpyDeviceToHost, s));
   MDB_CUDA(cudaStreamSynchronize(s));
   w.nSlots = nSlots;
   w.nClusters = nSlots / kClusterSize;
   w.nEntries = flags[0];
   w.nItems = flags[1];
+  w.nInEntries = hflags[0];
+  w.nInItems = hflags[1];
   return MDBAS_NB_OK;
 }
 
 int cluster_refresh(ClusterWork &w, const double *x, const double *y, const double *z,
                     const double *q, double sqrtC, cudaStream_t s) {
   if (w.slotCap <= 0) return MDBAS_NB_ERR_STATE;
+  // an inner list at the plain cut-off holds the pairs of the build's
+  // positions only
+  if (w.rin2 == 0.f) w.useInner = false;
   MDB_LAUNCH(k_refresh, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(),
              w.geoms.as<ClusterGeom>(), w.clusterRepDev(), w.slotAtom.as<int>(),
              w.origin.as<double4>(), x, y, z, q, sqrtC, w.xq.as<float4>(), w.xp.as<float>());

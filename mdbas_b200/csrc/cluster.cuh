@@ -11,12 +11,32 @@ constexpr int kClusterSize = 8;
 constexpr int kItemMax = 32;  // j-clusters per work item of the pair kernel
 
 // Geometry of the column grid (x-y cells, atoms sorted by z inside a cell).
+//
+// The list keeps exactly the pairs MDBas's list builder keeps.  Pair
+// distances are tested in FP32 against a band around the list radius:
+// r2 <= rlo2 is in, r2 > rhi2 is out, and a pair inside the band is decided
+// by MDBas's own FP64 expression (listMode 1: link cells, fractional
+// coordinates of src/list.c:1932-1936 and 2051-2057; listMode 0: all pairs,
+// dist() of src/utils.c:38-80) against cutnb2 = (rc + delr)^2.  The band
+// (2e-5 relative, ~0.004 A^2 at 14 A) is ten times the FP32 error of the
+// cluster-relative distances.
 struct ClusterGeom {
   int ncx, ncy;       // cells per side in x and y
   int Dx, Dy;         // cell offsets searched on each side
   double Lx, Ly, Lz;  // orthorhombic box edges
   double wx, wy;      // cell widths
-  float rlist2;       // (rc + delr)^2 with a small safety margin
+  float rlist2;       // candidate test: rhi2
+  float rlo2, rhi2;   // FP32 band around the list radius
+  double cutnb2;      // MDBas's list radius squared (FP64)
+  int listMode;       // 1: MDBas's link-cell list, 0: its all-pairs list
+};
+
+// One entry of the inner list: a 4-atom half of a j cluster (jh = 2 j + h,
+// atoms 4h..4h+3) with the cluster pair's FP32 shift; its 32-bit mask holds
+// bit i + 8 k for i atom i and half atom k.
+struct HalfEntry {
+  int jh;
+  float sx, sy, sz;
 };
 
 // One cluster-pair entry: j cluster and the FP32 shift vector
@@ -82,10 +102,19 @@ struct ClusterWork {
   DBuf counters;      // int64[4]: entries, items, overflow flag, candidates
   long long entryCap = 0, itemCap = 0;
   long long nEntries = 0, nItems = 0;
-  // Inner list for dynamics ("dynamic pruning"): the entries of the list
-  // above whose masks keep only the pairs found within an inner radius at the
-  // last prune; the pair kernel reads it instead while useInner is set.
-  DBuf entriesIn, masksIn, itemsIn, countersIn;
+  // Inner list: the j-cluster halves of the list above that hold a pair
+  // within the inner radius (rin2), with 32-bit masks of those pairs, written
+  // by the search at build time and by the prune pass during dynamics.  The
+  // half-cluster pair kernel reads it while useInner is set, the full list
+  // otherwise.  Items hold up to 2 * kItemMax half entries.
+  DBuf entriesIn;     // HalfEntry
+  DBuf masksIn;       // uint32
+  DBuf itemsIn;       // int4: i cluster, first half entry, count, 0
+  DBuf countersIn;    // int64[4] as counters
+  long long inEntryCap = 0, inItemCap = 0;
+  float rin2 = 0.f;   // radius^2 of the inner list the search writes
+  float innerRin2 = 0.f;  // radius^2 of the inner list as last written
+  long long nInEntries = 0, nInItems = 0;  // host copies (synchronising builds)
   bool useInner = false;
   DBuf sticky;        // int64: OR of every build's error bits since last read
   // accumulators
@@ -106,16 +135,26 @@ enum ClusterFlag { CL_OVERFLOW = 1, CL_NONFINITE = 2 };
 // have been set up by an earlier synchronising build of the same geometry,
 // and an overflow only raises CL_OVERFLOW in `sticky`.
 // Batch form: nRep boxes, atomOff[nRep + 1] atom ranges (host arrays).
+// listRule: MDBas's makelist choice of list builder (bits 0-2 linkRatio,
+// bit 3 noLink), which decides the FP64 expression that settles pairs at the
+// list radius.  Exclusion rows must be symmetric (cluster_symmetric_excl).
+// The inner list is written at w.rin2 (0: rc^2 with a 1e-5 margin).
 int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const int *atomOff,
-                  double cutOff, double delr, double sqrtC, const double *x, const double *y,
+                  double cutOff, double delr, int listRule, double sqrtC, const double *x,
+                  const double *y, const double *z, const double *q, const double *eps,
+                  const double *sig, const int *frozen, const int *exclStart,
+                  const int *exclFlat, cudaStream_t s, bool sync = true);
+// Single box.
+int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
+                  int listRule, double sqrtC, const double *x, const double *y,
                   const double *z, const double *q, const double *eps, const double *sig,
                   const int *frozen, const int *exclStart, const int *exclFlat, cudaStream_t s,
                   bool sync = true);
-// Single box.
-int cluster_build(ClusterWork &w, int n, const DevBox &b, double cutOff, double delr,
-                  double sqrtC, const double *x, const double *y, const double *z,
-                  const double *q, const double *eps, const double *sig, const int *frozen,
-                  const int *exclStart, const int *exclFlat, cudaStream_t s, bool sync = true);
+// Exclusion rows as the cluster search reads them: each excluded pair in
+// both atoms' rows, once (MDBas's all-pairs builder keeps half rows).
+void cluster_symmetric_excl(int n, const int *start, const int *flat, std::vector<int> &outStart,
+                            std::vector<int> &outFlat);
+inline int list_rule(int linkRatio, int noLink) { return (linkRatio & 7) | (noLink ? 8 : 0); }
 // Prune the list into the inner list: keep the pairs within sqrt(rin2) at the
 // current layout (after cluster_refresh), drop entries left without pairs.
 // No host interaction (graph-capturable); requires a synchronising build.

@@ -170,6 +170,13 @@ __device__ __forceinline__ long long fix_e(double v) { return __double2ll_rn(v *
 __device__ __forceinline__ void red_add(long long *addr, long long v) {
   atomicAdd(reinterpret_cast<unsigned long long *>(addr), static_cast<unsigned long long>(v));
 }
+// The same reduction issued under a predicate (no branch around it).
+__device__ __forceinline__ void red_add_if(bool p, long long *addr, long long v) {
+  asm volatile(
+      "{\n .reg .pred q;\n setp.ne.u32 q, %2, 0;\n @q red.global.add.u64 [%0], %1;\n}"
+      ::"l"(addr), "l"(v), "r"((unsigned)p)
+      : "memory");
+}
 
 // Accumulator slots (int64, units 2^-24) of one evaluation.
 enum AccSlot {

@@ -101,8 +101,10 @@ struct Ctx {
   cudaStream_t s = nullptr;
   int n = 0;
   DBuf x, y, z, q, eps, sig, frozen, exclStart, exclFlat, f3, acc64, list14;
+  // the exclusion rows made symmetric for the cluster search
+  DBuf exclStartSym, exclFlatSym;
   std::vector<double> hq, heps, hsig;
-  std::vector<int> hExclStart, hExclFlat, hFrozen;
+  std::vector<int> hExclStart, hExclFlat, hFrozen, hExclStartSym, hExclFlatSym;
   bool hasFrozen = false;
   RefListWork ref;
   ClusterWork cl;
@@ -113,6 +115,7 @@ struct Ctx {
   // mixed mode: positions at the last cluster build (displacement check)
   std::vector<double> bx, by, bz;
   bool clValid = false;
+  bool clMoved = false;  // positions changed since the last cluster build
   DevBox clBox{};
   int elecType = FULL, vdwType = VSWITCH;
   bool ptrsSet = false;
@@ -153,6 +156,7 @@ int upload_vec(DBuf &d, std::vector<double> &cache, const double *h, int n) {
   cache.assign(h, h + n);
   ST_TRY(d.ensure(sizeof(double) * n));
   MDB_CUDA(cudaMemcpyAsync(d.p, cache.data(), sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
+  g.clValid = false;  // the cluster layout holds charges and LJ parameters
   return MDBAS_NB_OK;
 }
 
@@ -182,6 +186,17 @@ int upload_exclusions(int n, int **exclList, const int *exclPair) {
   if (!g.hExclFlat.empty())
     MDB_CUDA(cudaMemcpyAsync(g.exclFlat.p, g.hExclFlat.data(), sizeof(int) * g.hExclFlat.size(),
                              cudaMemcpyHostToDevice, g.s));
+  // MDBas's all-pairs builder keeps half rows; the cluster search checks the
+  // rows of the i cluster's atoms only, so it reads both directions
+  cluster_symmetric_excl(n, g.hExclStart.data(), g.hExclFlat.data(), g.hExclStartSym,
+                         g.hExclFlatSym);
+  ST_TRY(g.exclStartSym.ensure(sizeof(int) * (n + 1)));
+  ST_TRY(g.exclFlatSym.ensure(sizeof(int) * std::max<size_t>(1, g.hExclFlatSym.size())));
+  MDB_CUDA(cudaMemcpyAsync(g.exclStartSym.p, g.hExclStartSym.data(), sizeof(int) * (n + 1),
+                           cudaMemcpyHostToDevice, g.s));
+  if (!g.hExclFlatSym.empty())
+    MDB_CUDA(cudaMemcpyAsync(g.exclFlatSym.p, g.hExclFlatSym.data(),
+                             sizeof(int) * g.hExclFlatSym.size(), cudaMemcpyHostToDevice, g.s));
   g.clValid = false;
   return MDBAS_NB_OK;
 }
@@ -333,11 +348,19 @@ int add_forces(int n, const double *dsrc, double *fx, double *fy, double *fz) {
   return MDBAS_NB_OK;
 }
 
-// Max displacement since the last cluster build exceeds half the skin?
-bool needs_cluster_rebuild(int n, const double *x, const double *y, const double *z,
-                           const DevBox &b, double delr) {
-  if (!g.clValid || (int)g.bx.size() != n) return true;
-  if (memcmp(&b, &g.clBox, sizeof(DevBox)) != 0) return true;
+// What the cluster list needs for these positions: a rebuild (max
+// displacement since the last build beyond half the skin, or no list), a
+// refresh of the FP32 layout (moved, within half the skin), or nothing (the
+// build's own positions: the inner list written by the build still holds).
+enum ClusterNeed { CL_NEED_NONE = 0, CL_NEED_REFRESH = 1, CL_NEED_REBUILD = 2 };
+int cluster_need(int n, const double *x, const double *y, const double *z, const DevBox &b,
+                 double delr) {
+  if (!g.clValid || (int)g.bx.size() != n) return CL_NEED_REBUILD;
+  if (memcmp(&b, &g.clBox, sizeof(DevBox)) != 0) return CL_NEED_REBUILD;
+  if (memcmp(x, g.bx.data(), sizeof(double) * n) == 0 &&
+      memcmp(y, g.by.data(), sizeof(double) * n) == 0 &&
+      memcmp(z, g.bz.data(), sizeof(double) * n) == 0)
+    return g.clMoved ? CL_NEED_REFRESH : CL_NEED_NONE;
   const double lim2 = 0.25 * delr * delr;
   const double L[3] = {b.a1, b.type == CUBIC ? b.a1 : b.b2, b.type == CUBIC ? b.a1 : b.c3};
   for (int i = 0; i < n; ++i) {
@@ -347,14 +370,15 @@ bool needs_cluster_rebuild(int n, const double *x, const double *y, const double
       d[k] -= L[k] * rint(d[k] / L[k]);
       r2 += d[k] * d[k];
     }
-    if (r2 > lim2) return true;
+    if (r2 > lim2) return CL_NEED_REBUILD;
   }
-  return false;
+  return CL_NEED_REFRESH;
 }
 
 // The real-space work of ewald_energy (or the plugin): forces added into
 // fx/fy/fz; e[0..5] = eDir, eCorr, evdw, virDir, virCorr, virvdw.
-int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch, const PBC *box,
+int real_space(int mode, int listRule, int n, const PARAM *param, double alpha, int vdwSwitch,
+               const PBC *box,
                const double *x, const double *y, const double *z, double *fx, double *fy,
                double *fz, const double *q, const double *eps, const double *sig,
                const int *neighList, const int *neighPair, const int *neighOrder,
@@ -393,20 +417,23 @@ int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch,
   }
   // mixed precision over the library's own cluster-pair list
   ST_TRY(upload_frozen(n, frozen));
-  if (needs_cluster_rebuild(n, x, y, z, b, param->delr)) {
-    ST_TRY(cluster_build(g.cl, n, b, param->cutOff, param->delr, sqrt(param->chargeConst),
-                         g.x.as<double>(), g.y.as<double>(), g.z.as<double>(), g.q.as<double>(),
-                         g.eps.as<double>(), g.sig.as<double>(),
-                         g.hasFrozen ? g.frozen.as<int>() : nullptr, g.exclStart.as<int>(),
-                         g.exclFlat.as<int>(), g.s));
+  const int need = cluster_need(n, x, y, z, b, param->delr);
+  if (need == CL_NEED_REBUILD) {
+    ST_TRY(cluster_build(g.cl, n, b, param->cutOff, param->delr, listRule,
+                         sqrt(param->chargeConst), g.x.as<double>(), g.y.as<double>(),
+                         g.z.as<double>(), g.q.as<double>(), g.eps.as<double>(),
+                         g.sig.as<double>(), g.hasFrozen ? g.frozen.as<int>() : nullptr,
+                         g.exclStartSym.as<int>(), g.exclFlatSym.as<int>(), g.s));
     g.bx.assign(x, x + n);
     g.by.assign(y, y + n);
     g.bz.assign(z, z + n);
     g.clBox = b;
     g.clValid = true;
-  } else {
+    g.clMoved = false;
+  } else if (need == CL_NEED_REFRESH) {
     ST_TRY(cluster_refresh(g.cl, g.x.as<double>(), g.y.as<double>(), g.z.as<double>(),
                            g.q.as<double>(), sqrt(param->chargeConst), g.s));
+    g.clMoved = true;
   }
   ClusterWork &w = g.cl;
   MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, g.s));
@@ -414,7 +441,7 @@ int real_space(int mode, int n, const PARAM *param, double alpha, int vdwSwitch,
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g.device);
   ST_TRY(pair_fp32_launch(w, p, sms * 8, 256, g.s));
-  ST_TRY(excl_fix_launch(w, n, p, g.exclStart.as<int>(), g.exclFlat.as<int>(),
+  ST_TRY(excl_fix_launch(w, n, p, g.exclStartSym.as<int>(), g.exclFlatSym.as<int>(),
                          g.x.as<double>(), g.y.as<double>(), g.z.as<double>(), g.q.as<double>(),
                          g.s));
   double *fxd = g.f3.as<double>();
@@ -723,7 +750,8 @@ int mdbas_nb_ewald_energy_status(CTRL *ctrl, PARAM *param, ENERGY *ener, EWALD *
     eRec = spme_energy(param, ewald, box, x, y, z, fx, fy, fz, q, stress1, &virRec);
   const int vdwSwitch = (g.ptrsSet ? g.vdwType : ctrl->vdwType) == VSWITCH;
   double e[6];
-  ST_TRY(real_space(mdbas_nb_get_mode(), param->nAtom, param, ewald->alpha, vdwSwitch, box, x, y,
+  ST_TRY(real_space(mdbas_nb_get_mode(), list_rule(1, ctrl ? ctrl->noLink : 0), param->nAtom,
+                    param, ewald->alpha, vdwSwitch, box, x, y,
                     z, fx, fy, fz, q, eps, sig, neighList, neighPair, neighOrder, exclList,
                     exclPair, nullptr, e));
   ener->elec += e[0] + eRec + e[1];
@@ -1000,7 +1028,7 @@ double mdbas_nb_user_energy(const PARAM *param, const PBC *box, const double x[]
     fail(MDBAS_NB_ERR_STATE, "mdbas_nb_user_energy");
   }
   double e[6];
-  DROP_TRY(real_space(mdbas_nb_get_mode(), param->nAtom, param, g_plugin.alpha,
+  DROP_TRY(real_space(mdbas_nb_get_mode(), list_rule(1, 0), param->nAtom, param, g_plugin.alpha,
                       g_plugin.vdwSwitch, box, x, y, z, fx, fy, fz, g_plugin.q.data(),
                       g_plugin.eps.data(), g_plugin.sig.data(), neighList, neighPair, neighOrder,
                       g_plugin.rowPtr.data(), g_plugin.exclPair.data(), nullptr, e),

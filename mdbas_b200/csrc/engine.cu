@@ -149,10 +149,10 @@ static int upload_boxes(mdbas_nb_engine *e) {
 static int sync_build(mdbas_nb_engine *e) {
   const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
   return cluster_build(e->cl, e->n, e->nRep, e->repBoxes.data(), e->repOff.data(),
-                       e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(),
-                       e->y.as<double>(), e->z.as<double>(), e->q.as<double>(),
-                       e->eps.as<double>(), e->sig.as<double>(), frozen,
-                       e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream);
+                       e->cfg.cutOff, e->cfg.delr, engine_list_rule(e), sqrt(e->cfg.chargeConst),
+                       e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                       e->q.as<double>(), e->eps.as<double>(), e->sig.as<double>(), frozen,
+                       e->exclStartSym.as<int>(), e->exclFlatSym.as<int>(), e->stream);
 }
 
 // Error bits of the cached accumulators (mixed precision only).
@@ -347,6 +347,15 @@ int mdbas_nb_engine_set_topology(mdbas_nb_engine *e, const double *q, const doub
   if (nex > 0)
     MDB_CUDA(cudaMemcpyAsync(e->exclFlat.p, exclFlat, sizeof(int) * nex, cudaMemcpyHostToDevice,
                              s));
+  // the cluster search reads each excluded pair from both atoms' rows
+  cluster_symmetric_excl(n, start.data(), exclFlat, e->hExclStartSym, e->hExclFlatSym);
+  ENG_TRY(e, e->exclStartSym.ensure(sizeof(int) * (n + 1)));
+  ENG_TRY(e, e->exclFlatSym.ensure(sizeof(int) * std::max<size_t>(1, e->hExclFlatSym.size())));
+  MDB_CUDA(cudaMemcpyAsync(e->exclStartSym.p, e->hExclStartSym.data(), sizeof(int) * (n + 1),
+                           cudaMemcpyHostToDevice, s));
+  if (!e->hExclFlatSym.empty())
+    MDB_CUDA(cudaMemcpyAsync(e->exclFlatSym.p, e->hExclFlatSym.data(),
+                             sizeof(int) * e->hExclFlatSym.size(), cudaMemcpyHostToDevice, s));
   e->hasFrozen = false;
   if (frozen) {
     bool any = false;
@@ -408,7 +417,6 @@ int mdbas_nb_engine_build(mdbas_nb_engine *e) {
                               lc, e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                               frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(), e->stream));
   } else {
-    e->cl.useInner = false;  // a new list; dynamics prune it again
     e->buildPending = false;
     if (e->built && e->cl.entryCap > 0 && e->cl.sticky.p) {
       // Grid, tables and capacities of the previous build still fit: build
@@ -416,10 +424,11 @@ int mdbas_nb_engine_build(mdbas_nb_engine *e) {
       // device and is settled by the next call that returns results.
       MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), e->stream));
       const int st = cluster_build(e->cl, n, e->nRep, e->repBoxes.data(), e->repOff.data(),
-                                   e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst),
-                                   e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
-                                   e->q.as<double>(), e->eps.as<double>(), e->sig.as<double>(),
-                                   frozen, e->exclStart.as<int>(), e->exclFlat.as<int>(),
+                                   e->cfg.cutOff, e->cfg.delr, engine_list_rule(e),
+                                   sqrt(e->cfg.chargeConst), e->x.as<double>(),
+                                   e->y.as<double>(), e->z.as<double>(), e->q.as<double>(),
+                                   e->eps.as<double>(), e->sig.as<double>(), frozen,
+                                   e->exclStartSym.as<int>(), e->exclFlatSym.as<int>(),
                                    e->stream, false);
       if (st == MDBAS_NB_OK) {
         e->buildPending = true;
@@ -482,8 +491,8 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
     // kernel's tail; the main stream waits for it before anything reads
     MDB_CUDA(cudaEventRecord(e->evFork, s));
     MDB_CUDA(cudaStreamWaitEvent(e->side, e->evFork, 0));
-    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(),
-                               e->exclFlat.as<int>(), e->x.as<double>(), e->y.as<double>(),
+    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStartSym.as<int>(),
+                               e->exclFlatSym.as<int>(), e->x.as<double>(), e->y.as<double>(),
                                e->z.as<double>(), e->q.as<double>(), e->side));
     MDB_CUDA(cudaEventRecord(e->evJoin, e->side));
     if (e->timing) MDB_CUDA(cudaEventRecord(e->ev0, s));
@@ -652,7 +661,7 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   struct Cand { int variant, block, bps; };
   std::vector<Cand> cands;
   // the dense kernel takes at most 256 threads per block (launch bounds)
-  for (int variant : {kPairPacked, kPairBulk, kPairDense})
+  for (int variant : {kPairHalf, kPairHalf3, kPairPacked, kPairBulk, kPairDense})
     for (int block : {64, 128, 256})
       for (int bps : {2, 4, 8, 16, 32})
         if (block * bps <= 2048 && bps <= 24) cands.push_back({variant, block, bps});
@@ -693,7 +702,7 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
 
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
   if (!e || (variant != kPairDense && variant != kPairCompact && variant != kPairPacked &&
-             variant != kPairBulk))
+             variant != kPairBulk && variant != kPairHalf && variant != kPairHalf3))
     return MDBAS_NB_ERR_ARG;
   e->variant = variant;
   return MDBAS_NB_OK;

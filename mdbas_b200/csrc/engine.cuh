@@ -26,6 +26,10 @@ struct mdbas_nb_engine {
   bool ownStream = false;
   // topology (caller's atom order)
   mdbas::DBuf q, eps, sig, frozen, exclStart, exclFlat;
+  // the exclusion rows made symmetric (each excluded pair in both atoms'
+  // rows, once), as the cluster search reads them
+  mdbas::DBuf exclStartSym, exclFlatSym;
+  std::vector<int> hExclStartSym, hExclFlatSym;
   bool hasFrozen = false;
   bool topoSet = false;
   double selfE = 0.0;
@@ -39,7 +43,7 @@ struct mdbas_nb_engine {
   mdbas::ClusterWork cl;
   mdbas::DBuf fout;
   int grid = 0, block = 0;
-  int variant = 2;  // pair kernel variant (kPairPacked)
+  int variant = 4;  // pair kernel variant (kPairHalf)
   // export scratch
   mdbas::DBuf exportBuf, exportCount;
   // adjoint scratch (adjoint.cu)
@@ -126,6 +130,10 @@ int engine_resolve_build(mdbas_nb_engine *e);
 // any stream capture).
 int engine_side_stream(mdbas_nb_engine *e);
 void kspace_release(mdbas_nb_engine *e);
+// MDBas's choice of list builder for this engine (cluster_build's listRule).
+inline int engine_list_rule(const mdbas_nb_engine *e) {
+  return list_rule(e->cfg.linkRatio, e->cfg.noLink);
+}
 PairParams make_params(double cutOff, double cutOn, double alpha, double chargeConst,
                        int vdwSwitch, int elecType);
 }  // namespace mdbas

@@ -923,7 +923,7 @@ int md_forces_cluster(mdbas_nb_engine *e, cudaStream_t s) {
   MDB_CUDA(cudaMemsetAsync(w.facc.p, 0, sizeof(long long) * 3 * (size_t)w.slotCap, s));
   MDB_CUDA(cudaMemsetAsync(w.acc.p, 0, sizeof(long long) * ACC_COUNT, s));
   MDB_TRY(pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
-  MDB_TRY(excl_fix_launch(w, n, e->pp, e->exclStart.as<int>(), e->exclFlat.as<int>(),
+  MDB_TRY(excl_fix_launch(w, n, e->pp, e->exclStartSym.as<int>(), e->exclFlatSym.as<int>(),
                           e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
                           e->q.as<double>(), s));
   return md_forces(e, s);
@@ -1023,11 +1023,11 @@ int md_capture_rebuild_body(mdbas_nb_engine *e, cudaGraph_t body, long long *cou
   g_launch_counter = counter;
   const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
   int st = cluster_build(e->cl, e->n, e->nRep, e->repBoxes.data(), e->repOff.data(),
-                         e->cfg.cutOff, e->cfg.delr, sqrt(e->cfg.chargeConst), e->x.as<double>(),
-                         e->y.as<double>(),
+                         e->cfg.cutOff, e->cfg.delr, engine_list_rule(e),
+                         sqrt(e->cfg.chargeConst), e->x.as<double>(), e->y.as<double>(),
                          e->z.as<double>(), e->q.as<double>(), e->eps.as<double>(),
-                         e->sig.as<double>(), frozen, e->exclStart.as<int>(),
-                         e->exclFlat.as<int>(), side, false);
+                         e->sig.as<double>(), frozen, e->exclStartSym.as<int>(),
+                         e->exclFlatSym.as<int>(), side, false);
   if (st == MDBAS_NB_OK) st = md_save_build_positions(e, side);
   if (st == MDBAS_NB_OK) {
     k_count<<<1, 32, 0, side>>>(e->mdWord.as<long long>() + W_BUILDS);
@@ -1472,6 +1472,9 @@ int mdbas_nb_engine_md_init(mdbas_nb_engine *e, const double *mass, const double
   LaunchScope ls(e);
   e->mdPrunes = 0;
   if (md_prune_on(e)) MD_TRY(e->mdXp.ensure(sizeof(double) * 3 * (size_t)n));
+  // the search writes the inner list at the pruning radius (or, without
+  // pruning, at the cut-off for the build's own positions only)
+  e->cl.rin2 = md_prune_on(e) ? md_rin2(e) : 0.f;
   MD_TRY(md_build(e));
   if (e->cfg.precision == 1) MD_TRY(mdbas_nb_engine_refresh(e));
   if (md_prune_on(e)) MD_TRY(md_prune_sync(e));

@@ -686,6 +686,253 @@ k_pair_fp32x2_bulk(const long long *__restrict__ counters, const int4 *__restric
 //     adds the sum to the global fixed-point accumulators -- no atomics on
 //     shared memory, and the order of every FP32 sum is fixed.
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Half-cluster kernel (kPairHalf, the default).  One warp runs one work item,
+// an i cluster (8 atoms) against a run of j-cluster halves (4 atoms each),
+// two halves A and B per step: lane L owns i atom L % 8 and half atom L / 8,
+// its pair with half A in the .x and its pair with half B in the .y lane of
+// packed f32x2 arithmetic, and bit L of each half's 32-bit mask.  INNER: the
+// halves come from the inner list (any two halves of the item, each with its
+// own shift and mask: only halves holding a pair within the inner radius);
+// otherwise each entry of the full list supplies its own two halves, and a
+// step whose pairs all lie beyond the cut-off is skipped after the distance
+// test.  Per chunk of kHIt steps the warp stages, per step and half atom,
+// the j coordinates with the step's shift already added, the charges and the
+// LJ parameters, interleaved so that each lane reads its two pairs' operands
+// as register pairs (three 16-byte shared loads per step).
+//
+// Arithmetic per pair (MDBas's formulas, src/ewald.c:356-369 and
+// src/vdw.c:144-184, rearranged):
+//   Coulomb: erfc(x) = t P(t) e^{-x^2}, t = 1/(1 + p x) (own fit, max
+//     relative error 2.4e-8); with w = t P(t)/r + 2a/sqrt(pi) and
+//     qe = q_i q_j e^{-(a r)^2}: g = qe w = -r dE/dr, E = g - qe 2a/sqrt(pi);
+//   LJ: p = 4 eps (s^12 - s^6), r dp/dr = -6 eps' (2 s^12 - s^6) with
+//     eps' = 4 eps; switch with u = max(r^2 - ron^2, 0) and D = rc^2 - ron^2:
+//     S = 1 - u^2 (3D - 2u)/D^3 (exactly 1 inside ron), r dS/dr =
+//     -12 r^2 (D - u) u / D^3 (exactly 0 inside ron);
+//   force on i: (r dE/dr) / r^2 * (x_j - x_i).
+// Energies and virials are summed per lane in FP32 within an item and
+// converted to fixed point per lane and item; j forces are reduce-scattered
+// over the 8 i lanes and added once per step and j atom in fixed point; i
+// forces once per item.  Totals do not depend on which warp ran which item.
+// ---------------------------------------------------------------------------
+constexpr int kHIt = 8;  // steps per staged chunk
+struct HalfStage {
+  float4 jd[kHIt * 4 * 3];  // [step][half atom]: (xA,xB,yA,yB), (zA,zB,qA,qB), (eA,eB,sA,sB)
+  float sh[kHIt][8];        // per step: sxA, sxB, syA, syB, szA, szB
+  int2 js[kHIt];            // per step: first slot of half A, of half B
+  uint2 mk[kHIt];           // per step: masks of half A, of half B
+};
+
+template <bool VDW, bool INNER, int MINB>
+__global__ void __launch_bounds__(256, MINB)
+k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ items,
+            const void *__restrict__ entriesV, const void *__restrict__ masksV,
+            const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
+            long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
+  __shared__ __align__(16) HalfStage stage[8];
+  HalfStage &S = stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jl = lane >> 3;
+  const bool up = il & 4, mid = il & 2, lo = il & 1;
+  const int comp = mid ? (lo ? 3 : 2) : (lo ? 1 : 0);
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * fstride;
+  const float two_a = c.two_a_sqrtpi;
+  const unsigned lanebit = 1u << lane;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;  // fixed point, per lane and item
+  int npair = 0;
+  bool overflow = false;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const int nsteps = INNER ? (ne + 1) >> 1 : ne;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    const float2 nx = f2(-xi.x), ny = f2(-xi.y), nz = f2(-xi.z);
+    float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
+    float2 ec = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
+    for (int s0 = 0; s0 < nsteps; s0 += kHIt) {
+      const int nIt = min(kHIt, nsteps - s0);
+      if (INNER) {
+        const HalfEntry *__restrict__ hent = static_cast<const HalfEntry *>(entriesV);
+        const unsigned *__restrict__ hmask = static_cast<const unsigned *>(masksV);
+        const int nh = min(2 * kHIt, ne - 2 * s0);
+        if (lane < nh) {
+          const HalfEntry he = hent[e0 + 2 * s0 + lane];
+          const unsigned m = hmask[e0 + 2 * s0 + lane];
+          const int k = lane >> 1, side = lane & 1;
+          float *sh = S.sh[k];
+          int *js = reinterpret_cast<int *>(&S.js[k]);
+          unsigned *mk = reinterpret_cast<unsigned *>(&S.mk[k]);
+          sh[side] = he.sx;
+          sh[2 + side] = he.sy;
+          sh[4 + side] = he.sz;
+          js[side] = he.jh * 4;
+          mk[side] = m;
+          if (side == 0 && lane == nh - 1) {  // a last half without a partner
+            sh[1] = he.sx;
+            sh[3] = he.sy;
+            sh[5] = he.sz;
+            js[1] = he.jh * 4;
+            mk[1] = 0u;
+          }
+        }
+      } else {
+        const CPairEntry *__restrict__ ent = static_cast<const CPairEntry *>(entriesV);
+        const uint2 *__restrict__ msk = static_cast<const uint2 *>(masksV);
+        if (lane < nIt) {
+          const CPairEntry en = ent[e0 + s0 + lane];
+          *reinterpret_cast<float4 *>(S.sh[lane]) = make_float4(en.sx, en.sx, en.sy, en.sy);
+          *reinterpret_cast<float2 *>(S.sh[lane] + 4) = make_float2(en.sz, en.sz);
+          S.js[lane] = make_int2(en.j * kClusterSize, en.j * kClusterSize + 4);
+          S.mk[lane] = msk[e0 + s0 + lane];
+        }
+      }
+      __syncwarp();
+      {
+        const int k = lane >> 2, a = lane & 3;
+        if (k < nIt) {
+          const int2 js = S.js[k];
+          const float4 sxy = *reinterpret_cast<const float4 *>(S.sh[k]);
+          const float2 sz = *reinterpret_cast<const float2 *>(S.sh[k] + 4);
+          const float4 xa = xq[js.x + a], xb = xq[js.y + a];
+          const float2 la = lj[js.x + a], lb = lj[js.y + a];
+          float4 *d = &S.jd[(k * 4 + a) * 3];
+          d[0] = make_float4(xa.x + sxy.x, xb.x + sxy.y, xa.y + sxy.z, xb.y + sxy.w);
+          d[1] = make_float4(xa.z + sz.x, xb.z + sz.y, xa.w, xb.w);
+          d[2] = make_float4(la.x, lb.x, la.y, lb.y);
+        }
+      }
+      __syncwarp();
+      for (int k = 0; k < nIt; ++k) {
+        const float4 p0 = S.jd[(k * 4 + jl) * 3], p1 = S.jd[(k * 4 + jl) * 3 + 1];
+        const uint2 mk = S.mk[k];
+        const float2 dx = __fadd2_rn(make_float2(p0.x, p0.y), nx);
+        const float2 dy = __fadd2_rn(make_float2(p0.z, p0.w), ny);
+        const float2 dz = __fadd2_rn(make_float2(p1.x, p1.y), nz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        const bool ina = (mk.x & lanebit) && r2.x <= c.rc2;
+        const bool inb = (mk.y & lanebit) && r2.y <= c.rc2;
+        if (!INNER && !__any_sync(0xffffffffu, ina || inb)) continue;
+        if (ina) ++npair;
+        if (inb) ++npair;
+        const float2 r2s = make_float2(ina ? r2.x : 1.0f, inb ? r2.y : 1.0f);
+        const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
+        const float2 rinv2 = __fmul2_rn(rinv, rinv);
+        const float2 r = __fmul2_rn(r2s, rinv);
+        const float2 qq0 = __fmul2_rn(f2(xi.w), make_float2(p1.z, p1.w));
+        const float2 qq = make_float2(ina ? qq0.x : 0.f, inb ? qq0.y : 0.f);
+        const float2 targ = __ffma2_rn(f2(c.p_alpha), r, f2(1.0f));
+        const float2 t = make_float2(rcp_approx(targ.x), rcp_approx(targ.y));
+        const float2 earg = __fmul2_rn(f2(-c.c_ex), r2s);
+        const float2 ex = make_float2(ex2_approx(earg.x), ex2_approx(earg.y));
+        float2 poly = __ffma2_rn(f2(kErfcC7), t, f2(kErfcC6));
+        poly = __ffma2_rn(poly, t, f2(kErfcC5));
+        poly = __ffma2_rn(poly, t, f2(kErfcC4));
+        poly = __ffma2_rn(poly, t, f2(kErfcC3));
+        poly = __ffma2_rn(poly, t, f2(kErfcC2));
+        poly = __ffma2_rn(poly, t, f2(kErfcC1));
+        poly = __ffma2_rn(poly, t, f2(kErfcC0));
+        const float2 w = __ffma2_rn(__fmul2_rn(rinv, t), poly, f2(two_a));
+        const float2 qe = __fmul2_rn(qq, ex);
+        const float2 g = __fmul2_rn(qe, w);  // -r dE_c/dr
+        ec = __fadd2_rn(ec, __ffma2_rn(qe, f2(-two_a), g));
+        gs = __fadd2_rn(gs, g);
+        float2 F = g;  // -(r dE/dr) while VDW adds to it below
+        if (VDW) {
+          const float4 lp = S.jd[(k * 4 + jl) * 3 + 2];
+          const float2 eps0 = __fmul2_rn(f2(li.x), make_float2(lp.x, lp.y));
+          const float2 eps = make_float2(ina ? eps0.x : 0.f, inb ? eps0.y : 0.f);
+          const float2 sg = __fadd2_rn(f2(li.y), make_float2(lp.z, lp.w));
+          const float2 s2 = __fmul2_rn(__fmul2_rn(sg, sg), rinv2);
+          const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+          const float2 s12 = __fmul2_rn(s6, s6);
+          const float2 a = __ffma2_rn(s6, f2(-1.0f), s12);  // s12 - s6
+          const float2 b = __fadd2_rn(a, s12);              // 2 s12 - s6
+          const float2 u0 = __fadd2_rn(r2s, f2(-c.ron2));
+          const float2 u = make_float2(fmaxf(u0.x, 0.f), fmaxf(u0.y, 0.f));
+          const float2 m = __fmul2_rn(__fmul2_rn(u, u), __ffma2_rn(u, f2(-2.0f), f2(c.sw_3d)));
+          const float2 S6 = __ffma2_rn(m, f2(c.sw_6), f2(-6.0f));  // -6 S
+          const float2 dS = __fmul2_rn(__fmul2_rn(__ffma2_rn(u, f2(-1.0f), f2(c.sw_d)), u),
+                                       __fmul2_rn(r2s, f2(c.sw_m12)));  // r dS/dr
+          const float2 pv = __fmul2_rn(eps, a);
+          ev6 = __ffma2_rn(pv, S6, ev6);
+          const float2 hv = __fmul2_rn(eps, __ffma2_rn(a, dS, __fmul2_rn(b, S6)));  // r dE_v/dr
+          hs = __fadd2_rn(hs, hv);
+          F = __ffma2_rn(F, f2(-1.0f), hv);  // r dE/dr
+        } else {
+          F = __fmul2_rn(F, f2(-1.0f));
+        }
+        // F = r dE/dr: the force on i is F / r^2 (x_j - x_i)
+        const float2 Fr = __fmul2_rn(F, rinv2);
+        const float2 fx = __fmul2_rn(Fr, dx), fy = __fmul2_rn(Fr, dy), fz = __fmul2_rn(Fr, dz);
+        fi_x = __fadd2_rn(fi_x, fx);
+        fi_y = __fadd2_rn(fi_y, fy);
+        fi_z = __fadd2_rn(fi_z, fz);
+        // reduce-scatter of the two j atoms' forces over the 8 i lanes
+        const float ax = fx.x, ay = fy.x, az = fz.x, bx = fx.y, by = fy.y, bz = fz.y;
+        float k0 = up ? bx : ax, k1 = up ? by : ay, k2 = up ? bz : az;
+        const float s0v = up ? ax : bx, s1v = up ? ay : by, s2v = up ? az : bz;
+        k0 += __shfl_xor_sync(0xffffffffu, s0v, 4);
+        k1 += __shfl_xor_sync(0xffffffffu, s1v, 4);
+        k2 += __shfl_xor_sync(0xffffffffu, s2v, 4);
+        const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
+        float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
+        u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
+        u1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+        const float wv = lo ? u0 : u1;
+        float v = lo ? u1 : u0;
+        v += __shfl_xor_sync(0xffffffffu, wv, 1);
+        const bool put = comp < 3 && v != 0.f;
+        overflow |= put && !(fabsf(v) < kForceLimitF);
+        const int2 js = S.js[k];
+        red_add_if(put, fcomp + (up ? js.y : js.x) + jl, fix_f(-v));
+      }
+      __syncwarp();
+    }
+    // i forces: the lane's two pairs, then the four j lanes of each i atom
+    float fix = fi_x.x + fi_x.y, fiy = fi_y.x + fi_y.y, fiz = fi_z.x + fi_z.y;
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jl < 3) {
+      const float v = (jl == 0) ? fix : (jl == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)jl * fstride + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    // each lane's share of the item in fixed point on its own
+    Ec += fix_e((double)ec.x + (double)ec.y);
+    Ev += fix_e(((double)ev6.x + (double)ev6.y) * (-1.0 / 6.0));
+    Vc += fix_e(-((double)gs.x + (double)gs.y));
+    Vv += fix_e((double)hs.x + (double)hs.y);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Ec += __shfl_xor_sync(0xffffffffu, Ec, o);
+    Ev += __shfl_xor_sync(0xffffffffu, Ev, o);
+    Vc += __shfl_xor_sync(0xffffffffu, Vc, o);
+    Vv += __shfl_xor_sync(0xffffffffu, Vv, o);
+    npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    red_add(acc + ACC_NPAIR, (long long)npair);
+  }
+}
+
 constexpr int kChunk = 8;    // entries per filter/compute chunk
 constexpr int kCWarps = 4;   // warps per block
 
@@ -981,6 +1228,11 @@ PairConstF make_pair_const(const PairParams &p) {
   c.sw_a = (float)(2.0 * p.switch2);
   c.sw_b = (float)((p.cutOff2 - 3.0 * p.cutOn2) * p.switch2);
   c.sw_c = (float)(12.0 * p.switch2);
+  const double D = p.cutOff2 - p.cutOn2;
+  c.sw_d = (float)D;
+  c.sw_3d = (float)(3.0 * D);
+  c.sw_6 = (float)(6.0 * p.switch2);
+  c.sw_m12 = (float)(-12.0 * p.switch2);
   c.vdw = p.vdwSwitch;
   return c;
 }
@@ -990,10 +1242,27 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   const PairConstF c = make_pair_const(p);
   // the list the kernel walks: the built list or, during dynamics, its
   // pruned inner copy
-  DBuf &counters = w.useInner ? w.countersIn : w.counters;
-  DBuf &items = w.useInner ? w.itemsIn : w.items;
-  DBuf &entries = w.useInner ? w.entriesIn : w.entries;
-  DBuf &masks = w.useInner ? w.masksIn : w.masks;
+  if (variant == kPairHalf || variant == kPairHalf3) {
+    const bool in = w.useInner;
+    auto kv = in ? (p.vdwSwitch ? k_pair_half<true, true, 4> : k_pair_half<false, true, 4>)
+                 : (p.vdwSwitch ? k_pair_half<true, false, 4> : k_pair_half<false, false, 4>);
+    if (variant == kPairHalf3)
+      kv = in ? (p.vdwSwitch ? k_pair_half<true, true, 3> : k_pair_half<false, true, 3>)
+              : (p.vdwSwitch ? k_pair_half<true, false, 3> : k_pair_half<false, false, 3>);
+    const DBuf &counters = in ? w.countersIn : w.counters;
+    const DBuf &items = in ? w.itemsIn : w.items;
+    const DBuf &entries = in ? w.entriesIn : w.entries;
+    const DBuf &masks = in ? w.masksIn : w.masks;
+    MDB_LAUNCH(kv, grid, block, 0, s, counters.as<long long>(), items.as<int4>(), entries.p,
+               masks.p, w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(),
+               w.slotCap, w.acc.as<long long>());
+    return MDBAS_NB_OK;
+  }
+  // the 8 x 8 kernels read the full list
+  DBuf &counters = w.counters;
+  DBuf &items = w.items;
+  DBuf &entries = w.entries;
+  DBuf &masks = w.masks;
   if (variant == kPairPacked) {
     auto kv = p.vdwSwitch ? k_pair_fp32x2<true> : k_pair_fp32x2<false>;
     MDB_LAUNCH(kv, grid, block, 0, s, counters.as<long long>(), items.as<int4>(),

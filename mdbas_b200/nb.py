@@ -473,8 +473,9 @@ class Engine:
         return int(lib().mdbas_nb_engine_launch_count(self.h))
 
     def set_variant(self, variant: int):
-        """Pair kernel: 2 = packed f32x2, staged (default), 0 = scalar dense 8x8,
-        1 = filtered and compacted, 3 = packed with bulk-copy staging."""
+        """Pair kernel: 4 = half clusters, packed f32x2, inner list (default),
+        2 = packed f32x2 8x8, staged, 0 = scalar dense 8x8, 1 = filtered and
+        compacted, 3 = packed with bulk-copy staging."""
         check(lib().mdbas_nb_engine_set_variant(self.h, variant), "engine_set_variant")
 
     def set_timing(self, on: bool):

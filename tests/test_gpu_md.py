@@ -286,19 +286,25 @@ def test_md_large_molecule_shake_matches_mdbas(gpu, ref_available):
 
 
 @pytest.mark.parametrize("graph", [0, 20])
-def test_md_pruned_list_bitwise_equal(gpu, water, graph):
+def test_md_pruned_list_matches_unpruned(gpu, water, graph):
     """Dynamic pruning (inner list at rc + 0.5 A, re-pruned after half that
-    displacement) drops only cluster pairs whose every pair lies beyond the
-    cut-off, whose contributions are exact zeros: the trajectory equals the
-    unpruned one bit for bit."""
+    displacement) drops only pairs beyond the cut-off, whose contributions
+    are exact zeros.  The half-cluster kernel then walks a different sequence
+    of j-cluster halves than over the full list, so its FP32 sums of the i
+    forces run in another order: the trajectories agree to FP32 rounding,
+    and each is bit-for-bit reproducible."""
     vel = (water.vx, water.vy, water.vz)
     cons = water.water_constraints()
     ap, av, arows, ast, _ = _gpu_md(water, vel, 0.002, 60, 0, 1, cons, graph=graph, prune=0.5)
+    cp, cv, crows, cst, _ = _gpu_md(water, vel, 0.002, 60, 0, 1, cons, graph=graph, prune=0.5)
     bp, bv, brows, bst, _ = _gpu_md(water, vel, 0.002, 60, 0, 1, cons, graph=graph, prune=0.0)
     print(f"pruned: {ast['prunes']} prunes, {ast['rebuilds']} rebuilds")
     assert ast["pruned_list"] and not bst["pruned_list"]
     assert ast["prunes"] > ast["rebuilds"]
     for k in range(3):
-        assert np.array_equal(ap[k], bp[k])
-        assert np.array_equal(av[k], bv[k])
-    assert np.array_equal(arows, brows)
+        assert np.array_equal(ap[k], cp[k]) and np.array_equal(av[k], cv[k])
+    assert np.array_equal(arows, crows)
+    perr = _pos_err(ap, bp, water.box)
+    print(f"pruned vs unpruned: pos {perr:.3e} A")
+    assert perr < 1e-5
+    assert np.allclose(arows[:, 1:], brows[:, 1:], rtol=1e-6, atol=0.0)
