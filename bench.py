@@ -78,7 +78,9 @@ def _parse():
                         "list build + 4 force evaluations, 'md' = --md-steps dynamics steps "
                         "driven from the host (a profiler sees no kernels inside graphs with "
                         "conditional nodes)")
-    p.add_argument("--variant", type=int, default=2, help="pair kernel variant of --case pair")
+    p.add_argument("--variant", type=int, default=4, help="pair kernel variant of --case pair")
+    p.add_argument("--dropin-steps", type=int, default=10,
+                   help="steps of the drop-in e2e leg (0 skips it)")
     return p.parse_args()
 
 
@@ -270,12 +272,15 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
-def cpu_baseline_sample(seed: int, gpu_list=None) -> dict:
+def cpu_baseline_sample(seed: int, gpu_list=None, gpu_list64=None, gpu_forces=None) -> dict:
     """MDBas single-threaded on the host: list rebuild + energy(), ~3 steps.
-    With gpu_list (a function of the wrapped positions returning the GPU
-    list's unordered pairs), the result also carries "list_parity": MDBas's
-    neighbour pair set against the GPU list builder's on the same 96k
-    coordinates."""
+    With gpu_list / gpu_list64 (functions of the wrapped positions returning
+    a GPU list's unordered pairs: the timed mixed path's cluster list, the
+    FP64 form's MDBas-order list), the result also carries "list_parity" /
+    "list_parity_fp64_form": MDBas's neighbour pair set against them on the
+    same 96k coordinates.  With gpu_forces (positions -> forces, energies of
+    the timed mixed path), "vs_mdbas" compares them with MDBas's energy() of
+    the last sample."""
     import numpy as np
     import oracle
     from mdbas_b200 import systems
@@ -293,24 +298,192 @@ def cpu_baseline_sample(seed: int, gpu_list=None) -> dict:
         t0 = r.now()
         r.update_list(x, y, z)
         t1 = r.now()
-        r.energy()
+        ref_out = r.energy()
         t2 = r.now()
         ts.append(t2 - t0)
         tl.append(t1 - t0)
         te.append(t2 - t1)
-    parity = None
-    if gpu_list is not None:
+    parity = parity64 = vs = None
+    if gpu_list is not None or gpu_list64 is not None:
         lst, pair, order = r.get_list()
-        gp = gpu_list(x, y, z)
-        parity = _same_pair_set(s.n, np.repeat(order, pair[order]), lst, gp[:, 0], gp[:, 1])
+        if gpu_list is not None:
+            gp = gpu_list(x, y, z)
+            parity = _same_pair_set(s.n, np.repeat(order, pair[order]), lst, gp[:, 0], gp[:, 1])
+            parity["gpu_list"] = "cluster-pair list of the timed mixed path (precision 1)"
+        if gpu_list64 is not None:
+            gp = gpu_list64(x, y, z)
+            parity64 = _same_pair_set(s.n, np.repeat(order, pair[order]), lst, gp[:, 0],
+                                      gp[:, 1])
+            parity64["gpu_list"] = "MDBas-order list of the plain FP64 form (precision 0)"
+    if gpu_forces is not None:
+        rfx, rfy, rfz, re = ref_out
+        (gx, gy, gz), ge = gpu_forces(x, y, z)
+        num = ((gx - rfx) ** 2 + (gy - rfy) ** 2 + (gz - rfz) ** 2).sum()
+        den = (rfx ** 2 + rfy ** 2 + rfz ** 2).sum()
+        elec = ge["elec_direct"] + ge["elec_corr"]
+        vs = {"force_rel_rms_vs_mdbas": float(np.sqrt(num / den)),
+              "elec_rel_vs_mdbas": abs(elec - re["elec"]) / abs(re["elec"]),
+              "vdw_rel_vs_mdbas": abs(ge["vdw"] - re["vdw"]) / abs(re["vdw"]),
+              "what": "timed mixed path vs MDBas energy() (keyEwald 3), 96k seed "
+                      f"{seed}, MDBas's wrapped coordinates"}
     r.close()
     t = statistics.median(ts)
-    return {"list_parity": parity,
+    return {"list_parity": parity, "list_parity_fp64_form": parity64, "vs_mdbas": vs,
             "value": pairs / t, "unit": "pairs/s", "cores": 1, "kind": "reference",
             "sample": f"{len(ts)} x (96k-atom link_cell_verlet_list_update + energy()), "
                       f"median {t:.2f} s",
             "list_update_s": statistics.median(tl), "energy_s": statistics.median(te),
             "host": _host_cpu()}
+
+
+def mdbas_errors(nb, systems, dev) -> dict:
+    """Mixed-form forces and energies against MDBas itself (oracle/_ref:
+    energy() with real-space Ewald, keyEwald 3) on the small water box and
+    the charged LJ fluid of the gradient case; the 96k box is compared in
+    cpu_baseline_sample."""
+    import numpy as np
+    import oracle
+    if not oracle.Reference.available():
+        return {"unavailable": "oracle/_ref not built"}
+    out = {}
+    for name, s in (("water_3k_seed1", systems.config_small(seed=1)),
+                    ("lj_fluid_12k_seed1", systems.lj_fluid(seed=1))):
+        r = oracle.Reference(s)
+        r.makelist()
+        x, y, z = r.positions()
+        rfx, rfy, rfz, re = r.energy()
+        r.close()
+        sp = systems.System(s.name, s.box, x, y, z, s.q, s.eps, s.sig, s.mass, s.bonds,
+                            s.angles)
+        e = nb.Engine(sp, precision=1, device=dev)
+        e.build()
+        e.compute()
+        fx, fy, fz = e.forces()
+        en = e.energies()
+        e.close()
+        num = ((fx - rfx) ** 2 + (fy - rfy) ** 2 + (fz - rfz) ** 2).sum()
+        den = (rfx ** 2 + rfy ** 2 + rfz ** 2).sum()
+        elec = en["elec_direct"] + en["elec_corr"]
+        out[name] = {"n_atoms": s.n, "force_rel_rms": float(np.sqrt(num / den)),
+                     "elec_rel": abs(elec - re["elec"]) / abs(re["elec"]),
+                     "vdw_rel": abs(en["vdw"] - re["vdw"]) / max(abs(re["vdw"]), 1e-300)}
+    return out
+
+
+def dropin_e2e(nb, systems, seed, steps) -> dict:
+    """The calls MDBas makes, timed end to end on host arrays through the C
+    ABI (wall clock around each synchronous call, which copies the positions
+    in and the forces out):
+      * energy() (include/energy.h:30-37) in mixed mode;
+      * mdbas_nb_user_energy (the UserEnergyPtr plugin, include/user.h:29-33)
+        in mixed mode;
+      * the plugin in the plain FP64 form over a caller-built MDBas list (the
+        library's own list copied into the caller's arrays, so it is uploaded
+        on every call, as a list from MDBas's list.c would be).
+    Every step moves all atoms by 1.2 A (a rigid shift back and forth), past
+    half the skin, so the mixed calls rebuild their cluster list each time,
+    like the step of the headline figure."""
+    import ctypes as C
+
+    import numpy as np
+    L = nb.bind_dropin()
+    s = systems.config_96k(seed=seed, temperature=None)
+    n = s.n
+    P = C.POINTER
+    ctrl = nb.CTRL()
+    ctrl.newjob = 1
+    ctrl.keyEwald = 3
+    ctrl.elecType = nb.FULL
+    ctrl.vdwType = nb.VSWITCH
+    param = nb.make_param(n, 12.0, 10.0, 2.0)
+    param.nBond = len(s.bonds)
+    param.nAngle = len(s.angles)
+    box = nb.make_pbc(s.cell())
+    neigh = nb.NEIGH()
+    neigh.update = 1
+    neigh.linkRatio = 1
+    ewald = nb.EWALD()
+    ewald.alpha = 0.34
+    ener = nb.ENERGY()
+    bond = (nb.BOND * len(s.bonds))()
+    for k, (a, b) in enumerate(s.bonds.tolist()):
+        bond[k].a, bond[k].b = a, b
+    angle = (nb.ANGLE * len(s.angles))()
+    for k, (a, b, c) in enumerate(s.angles.tolist()):
+        angle[k].a, angle[k].b, angle[k].c = a, b, c
+    const, dihe, impr = (nb.CONSTRAINT * 1)(), (nb.DIHE * 1)(), (nb.DIHE * 1)()
+    x = np.ascontiguousarray(s.x).copy()
+    y = np.ascontiguousarray(s.y).copy()
+    z = np.ascontiguousarray(s.z).copy()
+    q, eps, sig = (np.ascontiguousarray(a, dtype=np.float64) for a in (s.q, s.eps, s.sig))
+    frozen = np.zeros(n, np.int32)
+    vx, vy, vz = np.zeros(n), np.zeros(n), np.zeros(n)
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    lst, pair, order, l14 = (P(C.c_int)() for _ in range(4))
+    excl, epair = P(P(C.c_int))(), P(C.c_int)()
+    L.mdbas_nb_set_mode(0)
+    L.makelist(C.byref(ctrl), C.byref(param), C.byref(box), C.byref(neigh), const, bond, angle,
+               dihe, impr, nb.as_dp(x), nb.as_dp(y), nb.as_dp(z), nb.as_ip(frozen),
+               C.byref(lst), C.byref(pair), C.byref(order), C.byref(l14), C.byref(excl),
+               C.byref(epair))
+    L.init_energy_ptrs(C.byref(ctrl))
+    pe = nb.PARAM.from_buffer_copy(param)
+    pe.nBond = 0  # the nonbonded path only (no bonded terms)
+    pe.nAngle = 0
+    assert L.mdbas_nb_plugin_init(n, nb.as_dp(q), nb.as_dp(eps), nb.as_dp(sig), epair, excl,
+                                  0.34, 1) == 0
+    xs = [(x, y, z), (x + 1.2, y + 1.2, z + 1.2)]
+    xs = [tuple(np.ascontiguousarray(a) for a in t) for t in xs]
+
+    def call_energy(k):
+        a, b, c = xs[k & 1]
+        L.energy(C.byref(ctrl), C.byref(pe), C.byref(ener), C.byref(ewald), C.byref(box),
+                 C.byref(neigh), bond, bond, angle, dihe, impr, nb.as_dp(a), nb.as_dp(b),
+                 nb.as_dp(c), nb.as_dp(vx), nb.as_dp(vy), nb.as_dp(vz), nb.as_dp(fx),
+                 nb.as_dp(fy), nb.as_dp(fz), nb.as_dp(q), nb.as_dp(eps), nb.as_dp(sig),
+                 nb.as_dp(eps), nb.as_dp(sig), nb.as_ip(frozen), lst, pair, order, l14, excl,
+                 epair)
+
+    def call_plugin(k, lists):
+        a, b, c = xs[k & 1]
+        fx[:] = 0.
+        fy[:] = 0.
+        fz[:] = 0.
+        L.mdbas_nb_user_energy(C.byref(pe), C.byref(box), nb.as_dp(a), nb.as_dp(b),
+                               nb.as_dp(c), nb.as_dp(fx), nb.as_dp(fy), nb.as_dp(fz), *lists)
+
+    def timed(fn, k_steps):
+        for k in range(3):
+            fn(k)
+        ts = []
+        for k in range(k_steps):
+            t0 = time.perf_counter()
+            fn(k)
+            ts.append(time.perf_counter() - t0)
+        return statistics.median(ts) * 1e3
+
+    out = {}
+    try:
+        L.mdbas_nb_set_mode(1)
+        out["energy_mixed_ms"] = timed(call_energy, steps)
+        out["plugin_mixed_ms"] = timed(lambda k: call_plugin(k, (lst, pair, order, l14)), steps)
+        L.mdbas_nb_set_mode(0)
+        # the same list in caller-owned arrays: uploaded on every call
+        tot = int(np.ctypeslib.as_array(pair, (n,)).sum())
+        cl = np.ctypeslib.as_array(lst, (tot,)).copy()
+        cp = np.ctypeslib.as_array(pair, (n,)).copy()
+        co = np.ctypeslib.as_array(order, (n,)).copy()
+        own = (nb.as_ip(cl), nb.as_ip(cp), nb.as_ip(co), l14)
+        out["plugin_fp64_caller_list_ms"] = timed(lambda k: call_plugin(0, own),
+                                                  max(3, steps // 4))
+        out["caller_list_bytes"] = int(4 * (tot + 2 * n))
+    finally:
+        L.mdbas_nb_set_mode(0)
+    out["h2d_bytes_per_step"] = 3 * 8 * n
+    out["d2h_bytes_per_step"] = 3 * 8 * n
+    out["what"] = ("96k water, host arrays, synchronous C-ABI calls timed by wall clock; each "
+                   "mixed call rebuilds the cluster list (positions moved past half the skin)")
+    return out
 
 
 def _same_pair_set(n, ai, aj, bi, bj) -> dict:
@@ -327,6 +500,20 @@ def _same_pair_set(n, ai, aj, bi, bj) -> dict:
     return {"mdbas_pairs": int(ka.numel()), "gpu_pairs": int(kb.numel()), "bit_exact": same,
             "what": "set of unordered (i, j) of MDBas's link-cell list (r <= 14 A) and the "
                     "GPU builder's, same wrapped 96k coordinates"}
+
+
+def fp32_peaks(device: int) -> tuple:
+    """Measured FP32 FMA throughput of the device (TFLOP/s): scalar FFMA and
+    packed f32x2 FMA, from the bench-side probe library."""
+    import ctypes as C
+
+    from mdbas_b200 import build as nb_build
+    lib = C.CDLL(nb_build.build_peak())
+    tf, ms = (C.c_double * 2)(), (C.c_double * 2)()
+    st = lib.mdbas_peak_fp32(device, tf, ms)
+    if st != 0:
+        raise RuntimeError(f"FP32 peak probe failed (CUDA error {st})")
+    return tf[0], tf[1]
 
 
 def _host_cpu() -> dict:
@@ -673,13 +860,13 @@ def run_ours(args, rank, world):
     pair_ms, _ = eng.pair_kernel_ms(reset=True)
     # the other variants of the same kernel, for comparison
     other_ms = {}
-    for v, name in ((0, "scalar_dense"), (1, "compacted")):
+    for v, name in ((2, "packed_8x8"), (0, "scalar_dense_8x8"), (1, "compacted_8x8")):
         eng.set_variant(v)
         for _ in range(args.steps):
             flush.zero_()
             eng.compute()
         other_ms[name], _ = eng.pair_kernel_ms(reset=True)
-    eng.set_variant(2)
+    eng.set_variant(4)
     eng.set_timing(False)
     # list build alone
     ms_build = _time_steps(torch, eng, stream, flush, args.steps, eng.build)
@@ -720,7 +907,8 @@ def run_ours(args, rank, world):
     e2e_value = total_pairs / (t_e2e * 1e-3)
 
     # ---- roofline of the pair kernel ---------------------------------------
-    peak = nb.fp32_peak_tflops(dev)
+    peaks = fp32_peaks(dev)
+    peak = max(peaks)
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic = None
     prof = os.path.join(ROOT, "profiles", "pair_fp32x2_96k_traffic.json")
@@ -785,17 +973,49 @@ def run_ours(args, rank, world):
 
     cpu = None
     list_parity = None
+    list_parity64 = vs_mdbas = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        def gpu_list(x, y, z):
+        def _engine_at(x, y, z, precision):
             sw = systems.config_96k(seed=args.seed, temperature=None)
             sw.x, sw.y, sw.z = x, y, z
-            e0 = nb.Engine(sw, precision=0, device=dev)
+            e0 = nb.Engine(sw, precision=precision, device=dev)
             e0.build()
+            return e0
+
+        def gpu_list(x, y, z):
+            e0 = _engine_at(x, y, z, 1)
+            p = e0.export_pairs(1e30)  # every pair of the list masks
+            e0.close()
+            return p
+
+        def gpu_list64(x, y, z):
+            e0 = _engine_at(x, y, z, 0)
             p = e0.export_pairs(1e30)
             e0.close()
             return p
-        cpu = cpu_baseline_sample(args.seed, gpu_list)
+
+        def gpu_forces(x, y, z):
+            e0 = _engine_at(x, y, z, 1)
+            e0.compute()
+            f, en = e0.forces(), e0.energies()
+            e0.close()
+            return f, en
+
+        cpu = cpu_baseline_sample(args.seed, gpu_list, gpu_list64, gpu_forces)
         list_parity = cpu.pop("list_parity", None)
+        list_parity64 = cpu.pop("list_parity_fp64_form", None)
+        vs_mdbas = cpu.pop("vs_mdbas", None)
+        # the other configurations against MDBas, as checks beside the baseline
+        if vs_mdbas is not None:
+            vs_mdbas = {"water_96k_seed%d" % args.seed: vs_mdbas,
+                        **mdbas_errors(nb, systems, dev)}
+
+    dropin = None
+    if rank == 0 and args.dropin_steps > 0:
+        dropin = dropin_e2e(nb, systems, args.seed, args.dropin_steps)
+        for k in ("energy_mixed_ms", "plugin_mixed_ms", "plugin_fp64_caller_list_ms"):
+            if dropin.get(k):
+                dropin[k.replace("_ms", "_pairs_per_s")] = pairs / (dropin[k] * 1e-3)
 
     if rank == 0:
         line = {
@@ -818,7 +1038,8 @@ def run_ours(args, rank, world):
             "spme": spme,
             "replicas": replicas,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
-                            "variant": "packed f32x2, 8x8 cluster pairs, staged",
+                            "variant": "half clusters: 8-atom i x two 4-atom j halves per "
+                                       "warp step, packed f32x2, inner list",
                             "other_variants_ms": other_ms},
             "list_build": {"ms": t_build,
                            "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9},
@@ -828,13 +1049,17 @@ def run_ours(args, rank, world):
             "speedup_vs_fp64_form": {"step": t64 / t_step, "pair_kernel": pair64_ms / pair_ms},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": traffic,
-                         "peak_source": "measured FFMA probe (mdbas_nb_fp32_peak)",
-                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_fp32x2",
+                         "peak_source": "measured FMA probe, the larger of scalar FFMA and "
+                                        "packed f32x2 FMA (mdbas_b200/peak/fp32_peak.cu)",
+                         "peak_probe_tflops": {"ffma": peaks[0], "ffma2": peaks[1]},
+                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_half",
                          # the same flops counted on every listed pair slot (8 x 8
                          # per cluster pair, in the cut-off or not); frac = this x
                          # the pair efficiency of the cluster list
                          "frac_of_listed_slots": achieved / peak / max(1e-30, pairs / max(1, stats[2]))},
             "precision": prec,
+            "precision_vs_mdbas": vs_mdbas,
+            "e2e_dropin": dropin,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 3 * 8 * n,
                     "d2h_bytes_per_step": 3 * 8 * n + 8 * 8},
@@ -842,6 +1067,7 @@ def run_ours(args, rank, world):
             "clocks": clk,
             "cpu_baseline": cpu,
             "list_parity": list_parity,
+            "list_parity_fp64_form": list_parity64,
         }
         print(json.dumps(line))
     eng.close()

@@ -638,10 +638,6 @@ int mdbas_nb_batch_create(mdbas_nb_engine **out, const mdbas_nb_engine_config *c
 /* Number of replicas of an engine (1 for a single system). */
 int mdbas_nb_batch_count(mdbas_nb_engine *e);
 
-/* Measured FP32 FFMA throughput of a device (TFLOP/s, 2 flops per FFMA), the
- * peak the FP32 pair kernel's roofline fraction is quoted against; ms gets the
- * probe kernel's duration. */
-int mdbas_nb_fp32_peak(int device, double *tflops, double *ms);
 
 /* ------------------------------------------------------------------------ */
 /* Evaluation without device allocation (no counterpart in MDBas).           */

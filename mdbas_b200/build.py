@@ -20,6 +20,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libmdbas_nb.so")
+# bench-side FP32 peak probe, a library of its own (not part of libmdbas_nb.so)
+PEAK_SRC = os.path.join(HERE, "peak", "fp32_peak.cu")
+PEAK_LIB = os.path.join(HERE, "libmdbas_peak.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NO_FMAD = {"pair_fp64.cu", "bonded.cu", "ewald_rec.cu"}
 
@@ -81,7 +84,21 @@ def build(verbose: bool = False, jobs: int | None = None) -> str:
         if verbose:
             print(" ".join(link))
         subprocess.run(link, check=True)
+    build_peak(cc, verbose)
     return LIB
+
+
+def build_peak(cc: str | None = None, verbose: bool = False) -> str:
+    """The FP32 peak probe library of the benchmark (libmdbas_peak.so)."""
+    if (os.path.exists(PEAK_LIB)
+            and os.path.getmtime(PEAK_LIB) >= os.path.getmtime(PEAK_SRC)):
+        return PEAK_LIB
+    cmd = [cc or nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler",
+           "-fPIC", PEAK_SRC, "-o", PEAK_LIB]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return PEAK_LIB
 
 
 if __name__ == "__main__":

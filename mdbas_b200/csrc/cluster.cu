@@ -553,7 +553,12 @@ __device__ void flush_item(SearchBuf &B, int cnt, int ci, int lane, const double
   }
   if (lane == 0) {
     o.items[it] = make_int4(ci, (int)e0, nkeep, 0);
-    if (nin > 0) o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
+    if (nin > 0) {
+      o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
+      // warp steps of the half-cluster kernel over this item
+      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 3),
+                (unsigned long long)((nin + 1) >> 1));
+    }
   }
 }
 
@@ -903,7 +908,11 @@ k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
       hent[q] = he;
       hmask[q] = mine.y;
     }
-    if (lane == 0) hitems[io] = make_int4(ci, (int)h0, nin, 0);
+    if (lane == 0) {
+      hitems[io] = make_int4(ci, (int)h0, nin, 0);
+      atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 3),
+                (unsigned long long)((nin + 1) >> 1));
+    }
   }
 }
 
@@ -1178,6 +1187,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     w.nItems = flags[1];
     w.nInEntries = hflags[0];
     w.nInItems = hflags[1];
+    w.nInSteps = hflags[3];
     if (!(flags[2] & CL_OVERFLOW)) {
       w.useInner = true;
       return MDBAS_NB_OK;
@@ -1253,6 +1263,7 @@ int cluster_read_counts(ClusterWork &w, cudaStream_t s) {
   w.nItems = flags[1];
   w.nInEntries = hflags[0];
   w.nInItems = hflags[1];
+  w.nInSteps = hflags[3];
   return MDBAS_NB_OK;
 }
 

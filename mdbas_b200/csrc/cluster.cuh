@@ -110,11 +110,11 @@ struct ClusterWork {
   DBuf entriesIn;     // HalfEntry
   DBuf masksIn;       // uint32
   DBuf itemsIn;       // int4: i cluster, first half entry, count, 0
-  DBuf countersIn;    // int64[4] as counters
+  DBuf countersIn;    // int64[4]: entries, items, overflow flag, warp steps
   long long inEntryCap = 0, inItemCap = 0;
   float rin2 = 0.f;   // radius^2 of the inner list the search writes
   float innerRin2 = 0.f;  // radius^2 of the inner list as last written
-  long long nInEntries = 0, nInItems = 0;  // host copies (synchronising builds)
+  long long nInEntries = 0, nInItems = 0, nInSteps = 0;  // host copies (synchronising builds)
   bool useInner = false;
   DBuf sticky;        // int64: OR of every build's error bits since last read
   // accumulators

@@ -109,9 +109,18 @@ struct Ctx {
   RefListWork ref;
   ClusterWork cl;
   // The device list equals the caller's host list while these match.
+  // The device copy of a MDBas-format list stays resident between calls only
+  // when this library's own builder wrote it (resOwned) into the caller's
+  // arrays and those arrays still hold what it wrote: same pointers, same
+  // counts and the same checksum of neighPair and of a sample of the list.  A
+  // list built elsewhere (MDBas's own list.c behind the plugin entry) is
+  // uploaded on every call, since its builder may refill the same arrays in
+  // place (src/list.c:2276-2279, 2565-2574).
   const int *resList = nullptr, *resPair = nullptr, *resOrder = nullptr;
   long long resEntries = -1;
   int resN = -1;
+  bool resOwned = false;
+  unsigned long long resSum = 0;
   // mixed mode: positions at the last cluster build (displacement check)
   std::vector<double> bx, by, bz;
   bool clValid = false;
@@ -227,6 +236,18 @@ void print_grow(int from, int to) {
   fprintf(f, "WARNING: List larger than estimated. Size increased from %d to %d.\n", from, to);
 }
 
+// FNV-1a style hash of neighPair and of every 61st list entry plus the last
+// ones: a guard against arrays refilled since the library's build.
+unsigned long long list_checksum(int n, const int *neighList, const int *neighPair,
+                                 long long total) {
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&h](unsigned v) { h = (h ^ v) * 1099511628211ull; };
+  for (int i = 0; i < n; ++i) mix((unsigned)neighPair[i]);
+  for (long long k = 0; k < total; k += 61) mix((unsigned)neighList[k]);
+  for (long long k = total > 64 ? total - 64 : 0; k < total; ++k) mix((unsigned)neighList[k]);
+  return h;
+}
+
 // Build MDBas's list on the device and hand it to the caller's arrays.
 //   first != 0: allocate *neighList / *neighPair / *neighOrder (first build);
 //   first == 0: reuse them, growing *neighList by MDBas's 1% steps.
@@ -303,16 +324,20 @@ int list_common(int linkCells, int first, PARAM *param, PBC *box, NEIGH *neigh, 
   g.resOrder = orderArr;
   g.resEntries = total;
   g.resN = n;
+  g.resOwned = orderArr != nullptr;
+  g.resSum = list_checksum(n, *neighList, pairArr, total);
   return MDBAS_NB_OK;
 }
 
-// Bring the caller's list to the device unless it is the one built here.
+// Bring the caller's list to the device unless it is the one this library
+// built and still holds what the build wrote.
 int ensure_list_on_device(int n, const int *neighList, const int *neighPair,
                           const int *neighOrder) {
   long long total = 0;
   for (int i = 0; i < n; ++i) total += neighPair[i];
-  if (resident_enabled() && neighList == g.resList && neighPair == g.resPair &&
-      neighOrder == g.resOrder && total == g.resEntries && n == g.resN && g.ref.off.p)
+  if (resident_enabled() && g.resOwned && neighList == g.resList && neighPair == g.resPair &&
+      neighOrder == g.resOrder && total == g.resEntries && n == g.resN && g.ref.off.p &&
+      list_checksum(n, neighList, neighPair, total) == g.resSum)
     return MDBAS_NB_OK;
   ST_TRY(g.ref.list.ensure(sizeof(int) * (size_t)std::max<long long>(1, total)));
   ST_TRY(g.ref.neighPair.ensure(sizeof(int) * n));
@@ -330,6 +355,7 @@ int ensure_list_on_device(int n, const int *neighList, const int *neighPair,
   g.resOrder = neighOrder;
   g.resEntries = total;
   g.resN = n;
+  g.resOwned = false;  // a caller-built list: uploaded again on the next call
   return MDBAS_NB_OK;
 }
 

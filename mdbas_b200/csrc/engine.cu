@@ -603,7 +603,9 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
     ENG_TRY(e, cluster_read_counts(e->cl, e->stream));
     out[0] = e->cl.nClusters;
     out[1] = e->cl.nEntries;
-    out[2] = e->cl.nEntries * 64;
+    // pair slots the default kernel evaluates: 64 per warp step, one step
+    // per two inner-list halves (rounded up per item), or per full-list entry
+    out[2] = (e->cl.useInner ? e->cl.nInSteps : e->cl.nEntries) * 64;
     out[3] = e->cl.entryCap;
   }
   return MDBAS_NB_OK;

@@ -214,7 +214,6 @@ def lib():
     L.mdbas_nb_engine_set_variant.argtypes = [C.c_void_p, C.c_int]
     L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
-    L.mdbas_nb_fp32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.mdbas_nb_engine_md_init.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
                                           C.c_int, _ip, _dp, C.c_double, C.c_int]
     L.mdbas_nb_engine_md_run.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double,
@@ -246,13 +245,6 @@ def lib():
         C.c_int, C.POINTER(C.c_double)]
     _LIB = L
     return L
-
-
-def fp32_peak_tflops(device: int = 0) -> float:
-    """Measured FFMA throughput (TFLOP/s) of the device."""
-    tf, ms = C.c_double(0), C.c_double(0)
-    check(lib().mdbas_nb_fp32_peak(device, C.byref(tf), C.byref(ms)), "fp32_peak")
-    return tf.value
 
 
 def check(st: int, where: str) -> None:

@@ -227,6 +227,7 @@ class Reference:
                 getattr(lib, f).restype = C.c_long
                 getattr(lib, f).argtypes = [C.c_void_p]
             lib.ref_get_list.argtypes = [C.c_void_p, _ip, _ip, _ip]
+            lib.ref_list_ptrs.argtypes = [C.c_void_p] + [C.POINTER(C.POINTER(C.c_int))] * 3
             lib.ref_get_excl.argtypes = [C.c_void_p, _ip, _ip]
             lib.ref_get_positions.argtypes = [C.c_void_p, _dp, _dp, _dp]
             lib.ref_set_positions.argtypes = [C.c_void_p, _dp, _dp, _dp]
@@ -369,6 +370,13 @@ class Reference:
         order = np.zeros(self.n, np.int32)
         lib.ref_get_list(self.h, lst, pair, order)
         return lst[:cnt], pair, order
+
+    def list_ptrs(self):
+        """MDBas's own neighList, neighPair and neighOrder arrays (pointers
+        into the reference's memory, rebuilt in place by update_list)."""
+        p = [C.POINTER(C.c_int)() for _ in range(3)]
+        self.lib().ref_list_ptrs(self.h, *(C.byref(q) for q in p))
+        return tuple(p)
 
     def get_excl(self):
         lib = self.lib()

@@ -386,6 +386,15 @@ void ref_get_list(const RefSys *s, int *neighList, int *neighPair, int *neighOrd
   memcpy(neighOrder, s->neighOrder, (size_t)s->param.nAtom * sizeof(int));
 }
 
+/* The reference's own list arrays (not copies), for callers that hand them
+ * to another routine the way MDBas's driver does. */
+void ref_list_ptrs(const RefSys *s, int **neighList, int **neighPair, int **neighOrder)
+{
+  *neighList = s->neighList;
+  *neighPair = s->neighPair;
+  *neighOrder = s->neighOrder;
+}
+
 /* Exclusions as built by the reference: count per atom and flattened rows. */
 long ref_excl_entries(const RefSys *s)
 {

@@ -172,3 +172,65 @@ def test_energy_dropin_pairs14(gpu, key):
     for k in ("elec", "vdw", "virelec", "virvdw"):
         assert abs(e[k] - re[k]) <= 1e-12 * abs(re[k]), k
     d.free()
+
+
+def _excl_rows(start, flat):
+    """MDBas-style exclusion rows (int **, int *) from CSR arrays."""
+    n = len(start) - 1
+    rows = [(C.c_int * max(1, int(start[i + 1] - start[i])))(*flat[start[i]:start[i + 1]])
+            for i in range(n)]
+    lst = (C.POINTER(C.c_int) * n)(*[C.cast(r, C.POINTER(C.c_int)) for r in rows])
+    pair = np.diff(start).astype(np.int32)
+    return rows, lst, pair
+
+
+def test_plugin_follows_list_rebuilt_in_place(gpu):
+    """Behind the plugin entry MDBas's own list.c owns the list and refills
+    the same arrays in place (src/list.c:2276-2279, 2565-2574).  Two water
+    molecules swap places: the update keeps the arrays and the entry count
+    but changes which atoms pair up, and the plugin must use the new list."""
+    s = systems.water_box_for_atoms(18558, 3)
+    if not oracle.Reference.available():
+        pytest.skip("MDBas reference library not built")
+    r = oracle.Reference(s)
+    assert r.makelist() == 1
+    x, y, z = r.positions()
+    es, ef = r.get_excl()
+    rows, excl, epair = _excl_rows(es, ef)
+    L = nb.bind_dropin()
+    L.mdbas_nb_set_mode(0)
+    d = DropinSystem(s)
+    assert L.mdbas_nb_plugin_init(s.n, nb.as_dp(d.q), nb.as_dp(d.eps), nb.as_dp(d.sig),
+                                  nb.as_ip(epair), excl, 0.34, 1) == 0
+    lst, pair, order = r.list_ptrs()
+    none = C.POINTER(C.c_int)()
+
+    def plugin(xa, ya, za):
+        fx, fy, fz = np.zeros(s.n), np.zeros(s.n), np.zeros(s.n)
+        xa, ya, za = (np.ascontiguousarray(a, dtype=np.float64) for a in (xa, ya, za))
+        L.mdbas_nb_user_energy(C.byref(d.param), C.byref(d.box), nb.as_dp(xa), nb.as_dp(ya),
+                               nb.as_dp(za), nb.as_dp(fx), nb.as_dp(fy), nb.as_dp(fz), lst,
+                               pair, order, none)
+        return fx, fy, fz
+
+    f1 = plugin(x, y, z)
+    rfx, rfy, rfz, _ = r.energy()
+    assert force_rel_rms(f1, (rfx, rfy, rfz)) < 1e-12
+    before = r.get_list()
+    # swap two molecules far apart (every atom keeps its role: O with O)
+    m1, m2 = 10, s.n // 3 - 10
+    for a in (x, y, z):
+        t = a[3 * m1:3 * m1 + 3].copy()
+        a[3 * m1:3 * m1 + 3] = a[3 * m2:3 * m2 + 3]
+        a[3 * m2:3 * m2 + 3] = t
+    r.update_list(x, y, z)
+    after = r.get_list()
+    assert len(after[0]) == len(before[0]), "the swap keeps the entry count"
+    assert not np.array_equal(after[0], before[0]), "the swap changes the list"
+    addr = [C.cast(q, C.c_void_p).value for q in (lst, pair, order)]
+    assert [C.cast(q, C.c_void_p).value for q in r.list_ptrs()] == addr, "same arrays"
+    f2 = plugin(x, y, z)
+    rfx, rfy, rfz, _ = r.energy()
+    assert force_rel_rms(f2, (rfx, rfy, rfz)) < 1e-12
+    d.free()
+    r.close()
