@@ -68,6 +68,7 @@ struct ClusterWork {
   DBuf colRank;       // colOff[r] + (cy*ncx+cx) -> global column, Morton order inside r
   DBuf colXY;         // global column -> cx | cy << 16
   DBuf colCount, colFill, colStart, colPad, colPadStart;
+  DBuf chunkCount, chunkStart, chunks;  // search blocks: per column, chunks of i clusters
   DBuf atomCol, tmpIdx;
   DBuf atomZ;         // wrapped fractional z (FP64)
   DBuf scanTmp;
@@ -110,9 +111,11 @@ struct ClusterWork {
   DBuf entriesIn;     // HalfEntry
   DBuf masksIn;       // uint32
   DBuf itemsIn;       // int4: i cluster, first half entry, count, 0
-  DBuf countersIn;    // int64[4]: entries, items, overflow flag, warp steps
+  DBuf countersIn;    // int64[8]: entries, items, overflow flag, warp steps, pairs
+                      // within the inner radius
   long long inEntryCap = 0, inItemCap = 0;
-  float rin2 = 0.f;   // radius^2 of the inner list the search writes
+  float rin2 = 0.f;   // radius^2 of the inner list the search writes (0: the
+                      // pair kernel's own FP32 rc^2, an exact inner list)
   float innerRin2 = 0.f;  // radius^2 of the inner list as last written
   long long nInEntries = 0, nInItems = 0, nInSteps = 0;  // host copies (synchronising builds)
   bool useInner = false;

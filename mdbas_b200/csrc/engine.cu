@@ -131,6 +131,11 @@ PairParams make_params(double cutOff, double cutOn, double alpha, double chargeC
     }                                                                          \
   } while (0)
 
+static int ev_record(cudaEvent_t ev, cudaStream_t s) {
+  MDB_CUDA(cudaEventRecord(ev, s));
+  return MDBAS_NB_OK;
+}
+
 static int set_dev(mdbas_nb_engine *e) {
   MDB_CUDA(cudaSetDevice(e->device));
   return MDBAS_NB_OK;
@@ -488,17 +493,25 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e) {
     }
     ENG_TRY(e, engine_side_stream(e));
     // the exclusion correction on the side stream, overlapping the pair
-    // kernel's tail; the main stream waits for it before anything reads
+    // kernel's tail; the main stream waits for it before anything reads.
+    // Once forked, the join is made whatever fails in between, so no later
+    // work on the main stream can run beside the side stream's kernel.
     MDB_CUDA(cudaEventRecord(e->evFork, s));
     MDB_CUDA(cudaStreamWaitEvent(e->side, e->evFork, 0));
-    ENG_TRY(e, excl_fix_launch(w, n, e->pp, e->exclStartSym.as<int>(),
-                               e->exclFlatSym.as<int>(), e->x.as<double>(), e->y.as<double>(),
-                               e->z.as<double>(), e->q.as<double>(), e->side));
-    MDB_CUDA(cudaEventRecord(e->evJoin, e->side));
-    if (e->timing) MDB_CUDA(cudaEventRecord(e->ev0, s));
-    ENG_TRY(e, pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant));
-    if (e->timing) MDB_CUDA(cudaEventRecord(e->ev1, s));
-    MDB_CUDA(cudaStreamWaitEvent(s, e->evJoin, 0));
+    int st = excl_fix_launch(w, n, e->pp, e->exclStartSym.as<int>(), e->exclFlatSym.as<int>(),
+                             e->x.as<double>(), e->y.as<double>(), e->z.as<double>(),
+                             e->q.as<double>(), e->side);
+    const cudaError_t rj = cudaEventRecord(e->evJoin, e->side);
+    if (st == MDBAS_NB_OK && e->timing) st = ev_record(e->ev0, s);
+    if (st == MDBAS_NB_OK) st = pair_fp32_launch(w, e->pp, e->grid, e->block, s, e->variant);
+    if (st == MDBAS_NB_OK && e->timing) st = ev_record(e->ev1, s);
+    if (rj == cudaSuccess) {
+      MDB_CUDA(cudaStreamWaitEvent(s, e->evJoin, 0));
+    } else {
+      MDB_CUDA(cudaStreamSynchronize(e->side));  // no join event: wait for the side work
+      MDB_CUDA(rj);
+    }
+    ENG_TRY(e, st);
   }
   if (e->timing) {
     MDB_CUDA(cudaEventSynchronize(e->ev1));

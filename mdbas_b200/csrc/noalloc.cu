@@ -18,8 +18,14 @@
 // Host code cannot use the array's name as a device address (in host code it
 // names a host-side shadow).  The first call on each device, with that device
 // current, asks the runtime for the array's device address with
-// cudaGetSymbolAddress and remembers it; make that first call before any
-// stream capture.
+// cudaGetSymbolAddress and remembers it (one atomic slot per device, so
+// threads making their first calls at once store the same value without a
+// data race); make that first call before any stream capture.  A
+// cudaDeviceReset unloads the library's device code and the remembered
+// address with it: after a reset, do not call this entry point again on that
+// device in the same process.
+#include <atomic>
+
 #include "common.cuh"
 #include "pair_fp64.cuh"
 
@@ -45,7 +51,7 @@ static_assert(kScratchBytes == MDBAS_NB_NOALLOC_SCRATCH_BYTES, "scratch size cha
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void *g_scratch_addr[kMaxDevices] = {nullptr};
+std::atomic<void *> g_scratch_addr[kMaxDevices];
 
 __global__ void k_noalloc_counts(int n, const int *__restrict__ order,
                                  const int *__restrict__ neighPair, int *__restrict__ cnt) {
@@ -57,12 +63,12 @@ int scratch_for_current_device(unsigned char **out) {
   int dev = 0;
   MDB_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return MDBAS_NB_ERR_ARG;
-  if (!g_scratch_addr[dev]) {
-    void *p = nullptr;
+  void *p = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
     MDB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-    g_scratch_addr[dev] = p;
+    g_scratch_addr[dev].store(p, std::memory_order_release);
   }
-  *out = static_cast<unsigned char *>(g_scratch_addr[dev]);
+  *out = static_cast<unsigned char *>(p);
   return MDBAS_NB_OK;
 }
 

@@ -434,7 +434,11 @@ k_pair_fp32x2(const long long *__restrict__ counters, const int4 *__restrict__ i
 // contiguous blocks (xp: 128 B, ljp: 64 B), one copy each.  Two buffers per
 // warp: while a chunk is computed the next chunk's copies are in flight and
 // the entries of the one after are being loaded.  Waits are bounded: a copy
-// that does not complete sets FLAG_STAGE and the warp stops.
+// that does not complete sets FLAG_STAGE and the warp stops.  Once FLAG_STAGE
+// is raised every force, energy and virial of that evaluation is invalid (a
+// late copy may still land in shared memory the next block on the SM uses):
+// the engine's result calls (get_forces, energies) and the dynamics return
+// MDBAS_NB_ERR_CUDA for it instead of any result.
 // ---------------------------------------------------------------------------
 struct BulkBuf {
   float4 en[kStage];       // j (as int bits), shift x, y, z
@@ -717,14 +721,18 @@ k_pair_fp32x2_bulk(const long long *__restrict__ counters, const int4 *__restric
 // forces once per item.  Totals do not depend on which warp ran which item.
 // ---------------------------------------------------------------------------
 constexpr int kHIt = 8;  // steps per staged chunk
+// Two copies of each step's data: in order (half A in .x, B in .y) for lanes
+// with i atom 0-3, swapped for lanes with i atom 4-7, so that in the first
+// round of the j-force reduce-scatter every lane keeps .x and passes .y.
 struct HalfStage {
-  float4 jd[kHIt * 4 * 3];  // [step][half atom]: (xA,xB,yA,yB), (zA,zB,qA,qB), (eA,eB,sA,sB)
-  float sh[kHIt][8];        // per step: sxA, sxB, syA, syB, szA, szB
-  int2 js[kHIt];            // per step: first slot of half A, of half B
-  uint2 mk[kHIt];           // per step: masks of half A, of half B
+  float4 jd[2][kHIt * 4 * 3];  // [order][step][half atom]: (x,x,y,y), (z,z,q,q), (eps,eps,sig,sig)
+  int4 mj[2][kHIt];            // [order][step]: masks of the two halves, their first slots
+  float sh[kHIt][8];           // per step: sxA, sxB, syA, syB, szA, szB
+  int2 js[kHIt];               // per step: first slot of half A, of half B
+  uint2 mk[kHIt];              // per step: masks of half A, of half B
 };
 
-template <bool VDW, bool INNER, int MINB>
+template <bool VDW, bool INNER, int MINB, bool EXACT>
 __global__ void __launch_bounds__(256, MINB)
 k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ items,
             const void *__restrict__ entriesV, const void *__restrict__ masksV,
@@ -801,25 +809,44 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
           const float2 sz = *reinterpret_cast<const float2 *>(S.sh[k] + 4);
           const float4 xa = xq[js.x + a], xb = xq[js.y + a];
           const float2 la = lj[js.x + a], lb = lj[js.y + a];
-          float4 *d = &S.jd[(k * 4 + a) * 3];
-          d[0] = make_float4(xa.x + sxy.x, xb.x + sxy.y, xa.y + sxy.z, xb.y + sxy.w);
-          d[1] = make_float4(xa.z + sz.x, xb.z + sz.y, xa.w, xb.w);
+          const float ax = xa.x + sxy.x, bx = xb.x + sxy.y, ay = xa.y + sxy.z, by = xb.y + sxy.w;
+          const float az = xa.z + sz.x, bz = xb.z + sz.y;
+          float4 *d = &S.jd[0][(k * 4 + a) * 3];
+          d[0] = make_float4(ax, bx, ay, by);
+          d[1] = make_float4(az, bz, xa.w, xb.w);
           d[2] = make_float4(la.x, lb.x, la.y, lb.y);
+          float4 *e = &S.jd[1][(k * 4 + a) * 3];
+          e[0] = make_float4(bx, ax, by, ay);
+          e[1] = make_float4(bz, az, xb.w, xa.w);
+          e[2] = make_float4(lb.x, la.x, lb.y, la.y);
+          if (a == 0) {
+            const uint2 mk = S.mk[k];
+            S.mj[0][k] = make_int4((int)mk.x, (int)mk.y, js.x, js.y);
+            S.mj[1][k] = make_int4((int)mk.y, (int)mk.x, js.y, js.x);
+          }
         }
       }
       __syncwarp();
+      const float4 *__restrict__ jdl = S.jd[up ? 1 : 0];
+      const int4 *__restrict__ mjl = S.mj[up ? 1 : 0];
       for (int k = 0; k < nIt; ++k) {
-        const float4 p0 = S.jd[(k * 4 + jl) * 3], p1 = S.jd[(k * 4 + jl) * 3 + 1];
-        const uint2 mk = S.mk[k];
+        // this lane's two pairs: .x with the half it keeps in the reduction
+        const float4 p0 = jdl[(k * 4 + jl) * 3], p1 = jdl[(k * 4 + jl) * 3 + 1];
+        const int4 mj = mjl[k];
+        const uint2 mk = make_uint2((unsigned)mj.x, (unsigned)mj.y);
         const float2 dx = __fadd2_rn(make_float2(p0.x, p0.y), nx);
         const float2 dy = __fadd2_rn(make_float2(p0.z, p0.w), ny);
         const float2 dz = __fadd2_rn(make_float2(p1.x, p1.y), nz);
         const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-        const bool ina = (mk.x & lanebit) && r2.x <= c.rc2;
-        const bool inb = (mk.y & lanebit) && r2.y <= c.rc2;
+        // EXACT: the inner list was written by the search from these same
+        // FP32 distances against this same rc^2, so its bits are the test
+        const bool ina = (mk.x & lanebit) && (EXACT || r2.x <= c.rc2);
+        const bool inb = (mk.y & lanebit) && (EXACT || r2.y <= c.rc2);
         if (!INNER && !__any_sync(0xffffffffu, ina || inb)) continue;
-        if (ina) ++npair;
-        if (inb) ++npair;
+        if (!EXACT) {
+          if (ina) ++npair;
+          if (inb) ++npair;
+        }
         const float2 r2s = make_float2(ina ? r2.x : 1.0f, inb ? r2.y : 1.0f);
         const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
         const float2 rinv2 = __fmul2_rn(rinv, rinv);
@@ -844,7 +871,7 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
         gs = __fadd2_rn(gs, g);
         float2 F = g;  // -(r dE/dr) while VDW adds to it below
         if (VDW) {
-          const float4 lp = S.jd[(k * 4 + jl) * 3 + 2];
+          const float4 lp = jdl[(k * 4 + jl) * 3 + 2];
           const float2 eps0 = __fmul2_rn(f2(li.x), make_float2(lp.x, lp.y));
           const float2 eps = make_float2(ina ? eps0.x : 0.f, inb ? eps0.y : 0.f);
           const float2 sg = __fadd2_rn(f2(li.y), make_float2(lp.z, lp.w));
@@ -873,13 +900,12 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
         fi_x = __fadd2_rn(fi_x, fx);
         fi_y = __fadd2_rn(fi_y, fy);
         fi_z = __fadd2_rn(fi_z, fz);
-        // reduce-scatter of the two j atoms' forces over the 8 i lanes
-        const float ax = fx.x, ay = fy.x, az = fz.x, bx = fx.y, by = fy.y, bz = fz.y;
-        float k0 = up ? bx : ax, k1 = up ? by : ay, k2 = up ? bz : az;
-        const float s0v = up ? ax : bx, s1v = up ? ay : by, s2v = up ? az : bz;
-        k0 += __shfl_xor_sync(0xffffffffu, s0v, 4);
-        k1 += __shfl_xor_sync(0xffffffffu, s1v, 4);
-        k2 += __shfl_xor_sync(0xffffffffu, s2v, 4);
+        // reduce-scatter of the two j atoms' forces over the 8 i lanes: every
+        // lane keeps its .x atom (half A for i atoms 0-3, B for 4-7) and
+        // passes its .y atom to the lane of i atom i ^ 4, which keeps it
+        float k0 = fx.x + __shfl_xor_sync(0xffffffffu, fx.y, 4);
+        float k1 = fy.x + __shfl_xor_sync(0xffffffffu, fy.y, 4);
+        float k2 = fz.x + __shfl_xor_sync(0xffffffffu, fz.y, 4);
         const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
         float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
         u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
@@ -889,8 +915,7 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
         v += __shfl_xor_sync(0xffffffffu, wv, 1);
         const bool put = comp < 3 && v != 0.f;
         overflow |= put && !(fabsf(v) < kForceLimitF);
-        const int2 js = S.js[k];
-        red_add_if(put, fcomp + (up ? js.y : js.x) + jl, fix_f(-v));
+        red_add_if(put, fcomp + mj.z + jl, fix_f(-v));
       }
       __syncwarp();
     }
@@ -929,7 +954,12 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
     red_add(acc + ACC_E_VDW, Ev);
     red_add(acc + ACC_V_DIR, Vc);
     red_add(acc + ACC_V_VDW, Vv);
-    red_add(acc + ACC_NPAIR, (long long)npair);
+    // EXACT: the pairs were counted by the search (inner-list counter 4)
+    if (EXACT) {
+      if (gw == 0) red_add(acc + ACC_NPAIR, counters[4]);
+    } else {
+      red_add(acc + ACC_NPAIR, (long long)npair);
+    }
   }
 }
 
@@ -1244,11 +1274,21 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   // pruned inner copy
   if (variant == kPairHalf || variant == kPairHalf3) {
     const bool in = w.useInner;
-    auto kv = in ? (p.vdwSwitch ? k_pair_half<true, true, 4> : k_pair_half<false, true, 4>)
-                 : (p.vdwSwitch ? k_pair_half<true, false, 4> : k_pair_half<false, false, 4>);
-    if (variant == kPairHalf3)
-      kv = in ? (p.vdwSwitch ? k_pair_half<true, true, 3> : k_pair_half<false, true, 3>)
-              : (p.vdwSwitch ? k_pair_half<true, false, 3> : k_pair_half<false, false, 3>);
+    // the inner list written by the search at the kernel's own rc^2
+    const bool ex = in && w.innerRin2 == make_pair_const(p).rc2 && w.rin2 == 0.f;
+    auto kv = p.vdwSwitch ? k_pair_half<true, false, 4, false> : k_pair_half<false, false, 4, false>;
+    if (variant == kPairHalf3) {
+      if (in && ex)
+        kv = p.vdwSwitch ? k_pair_half<true, true, 3, true> : k_pair_half<false, true, 3, true>;
+      else if (in)
+        kv = p.vdwSwitch ? k_pair_half<true, true, 3, false> : k_pair_half<false, true, 3, false>;
+      else
+        kv = p.vdwSwitch ? k_pair_half<true, false, 3, false> : k_pair_half<false, false, 3, false>;
+    } else if (in && ex) {
+      kv = p.vdwSwitch ? k_pair_half<true, true, 4, true> : k_pair_half<false, true, 4, true>;
+    } else if (in) {
+      kv = p.vdwSwitch ? k_pair_half<true, true, 4, false> : k_pair_half<false, true, 4, false>;
+    }
     const DBuf &counters = in ? w.countersIn : w.counters;
     const DBuf &items = in ? w.itemsIn : w.items;
     const DBuf &entries = in ? w.entriesIn : w.entries;

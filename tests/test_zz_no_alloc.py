@@ -57,9 +57,14 @@ def test_noalloc_matches_regular_entry_point_twice(gpu):
     t = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in dict(
         x=d.x, y=d.y, z=d.z, q=d.q, eps=d.eps, sig=d.sig, lst=lst, pair=pair, order=order,
         start=start, flat=flat if len(flat) else np.zeros(1, np.int32)).items()}
+    outs = [[torch.zeros(s.n, dtype=torch.float64, device=dev) for _ in range(3)]
+            for _ in range(2)]
+    torch.cuda.synchronize()
+    free = []
     for call in range(2):
-        out = [torch.zeros(s.n, dtype=torch.float64, device=dev) for _ in range(3)]
+        out = outs[call]
         en = (C.c_double * 6)()
+        free.append(torch.cuda.mem_get_info(dev)[0])
         st = fn(s.n, C.byref(d.box), d.param.cutOff, d.param.cutOn, d.ewald.alpha,
                 d.param.chargeConst, 1, *(t[k].data_ptr() for k in
                                           ("x", "y", "z", "q", "eps", "sig", "lst", "pair",
@@ -74,6 +79,9 @@ def test_noalloc_matches_regular_entry_point_twice(gpu):
         assert abs(en[2] - ener.vdw) <= TOL * abs(ener.vdw), call
         assert abs((en[3] + en[4]) - ener.virelec) <= TOL * abs(ener.virelec), call
         assert abs(en[5] - ener.virvdw) <= TOL * abs(ener.virvdw), call
+    # the point of the entry point: the second call (set-up done by the
+    # first) leaves the device's free memory exactly as it found it
+    assert torch.cuda.mem_get_info(dev)[0] == free[1]
     d.free()
 
 
