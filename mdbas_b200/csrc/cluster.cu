@@ -295,29 +295,14 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
 }
 
 constexpr int kExclRegs = 8;  // exclusion partners per atom kept in registers
-constexpr int kColTab = 256;   // neighbour columns of a column ((2D+1)^2, D <= 7)
-constexpr int kColZ = 2048;    // neighbour clusters whose origin z is staged in shared memory
-constexpr int kSearchCols = 128;  // z-windowed ranges listed per warp before a candidate scan
+constexpr int kSearchCols = 192;  // z-windowed ranges listed per warp before a candidate scan
 
-// Per block: the columns within reach of the block's column (x-y cell gap
-// within the list radius), in the order of their (dx, dy) offsets, and the
-// origin z of every cluster of those columns (cluster order, z-sorted within
-// each column) for the warps' z-window searches.
-struct ColTable {
-  int start[kColTab];  // first cluster
-  int count[kColTab];  // clusters
-  int code[kColTab];   // periodic shift (sx + 1) | (sy + 1) << 2
-  int xy[kColTab];     // cell jx | jy << 16
-  int pre[kColTab + 1];
-  float z[kColZ];
-  int n;
-};
-
-// Per warp: the i cluster, the candidates found so far and the ranges of
-// the current candidate scan.
+// Per warp: the i cluster, the candidates found so far (with their FP32
+// shifts) and the z-windowed column ranges of the current candidate scan.
 struct WarpBuf {
   int j[kBufCap];
   int code[kBufCap];                   // image index (0..26) | real j atoms << 8
+  float4 sh[kBufCap];                  // FP32 shift: (float)(j origin + image - i origin)
   uint2 mask[kItemMax];
   float4 sj[kClusterSize * kItemMax];  // staged j atoms (xq), sj[j * kItemMax + entry]
   float4 si[kClusterSize];             // the i cluster's atoms (xq)
@@ -332,6 +317,10 @@ struct WarpBuf {
 // Outputs of the search: the list (entries with 64-bit masks at the list
 // radius, exactly MDBas's pairs) and the inner list (j-cluster halves with a
 // pair within sqrt(rin2), 32-bit masks).
+// Both lists take their room with one 64-bit atomic per flush on a packed
+// counter (items << 40 | entries): counters[4] and hcounters[5]; a one-thread
+// kernel unpacks them into counters[0..1] / hcounters[0..1] for the readers.
+constexpr int kPackShift = 40;
 struct SearchOut {
   CPairEntry *entries;
   uint2 *masks;
@@ -390,14 +379,14 @@ __device__ __noinline__ double mdbas_pair_r2(const DevBox &b, int listMode,
 // radius are settled by MDBas's FP64 expression, so the list's pairs are
 // MDBas's.  The halves of the entries holding inner pairs become the item's
 // inner-list entries, halves 0 first.
-__device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane, const double4 oi,
+__device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
                            const float4 *__restrict__ xq, const ClusterGeom &g,
                            const DevBox &box, int nreal_i, int pcLo, int pcHi, unsigned fimask,
                            const int *__restrict__ exclFlat, const int *__restrict__ slotOf,
                            const int *__restrict__ slotAtom, const int *__restrict__ frozen,
                            const double *__restrict__ px, const double *__restrict__ py,
-                           const double *__restrict__ pz, const double4 *__restrict__ origin,
-                           const SearchOut &o) {
+                           const double *__restrict__ pz, const SearchOut &o,
+                           int &npinAcc, int &stepAcc) {
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
     const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
@@ -411,12 +400,11 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane, const double4 
     const int k = lane;
     const int cj = B.j[k], code = B.code[k];
     const int sidx = code & 31, nrj = code >> 8;
-    const double4 oj = origin[cj];
-    const int sx = sidx % 3 - 1, sy = (sidx / 3) % 3 - 1, sz = sidx / 9 - 1;
+    const float4 shk = B.sh[k];
     en.j = cj;
-    en.sx = (float)(oj.x + sx * g.Lx - oi.x);
-    en.sy = (float)(oj.y + sy * g.Ly - oi.y);
-    en.sz = (float)(oj.z + sz * g.Lz - oi.z);
+    en.sx = shk.x;
+    en.sy = shk.y;
+    en.sz = shk.z;
     // the j atoms h and h + 4 side by side, shifted as the pair kernel does
     float2 jx[4], jy[4], jz[4];
 #pragma unroll
@@ -517,27 +505,29 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane, const double4 
   const int nA = __popc(hA), nin = nA + __popc(hB);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) npin += __shfl_xor_sync(0xffffffffu, npin, off);
-  long long e0 = 0, it = 0, h0 = 0, hit = 0;
+  unsigned long long pk = 0ull, hpk = 0ull;
   if (lane == 0) {
-    e0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 0),
-                              (unsigned long long)nkeep);
-    it = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 1), 1ull);
-    if (nin > 0) {
-      h0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 0),
-                                (unsigned long long)nin);
-      hit = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 1), 1ull);
-    }
+    pk = atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 4),
+                   (1ull << kPackShift) | (unsigned long long)nkeep);
+    if (nin > 0)
+      hpk = atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 5),
+                      (1ull << kPackShift) | (unsigned long long)nin);
   }
-  e0 = __shfl_sync(0xffffffffu, e0, 0);
-  it = __shfl_sync(0xffffffffu, it, 0);
-  h0 = __shfl_sync(0xffffffffu, h0, 0);
-  hit = __shfl_sync(0xffffffffu, hit, 0);
+  pk = __shfl_sync(0xffffffffu, pk, 0);
+  hpk = __shfl_sync(0xffffffffu, hpk, 0);
+  const unsigned long long lowMask = (1ull << kPackShift) - 1ull;
+  const long long e0 = (long long)(pk & lowMask), it = (long long)(pk >> kPackShift);
+  const long long h0 = (long long)(hpk & lowMask), hit = (long long)(hpk >> kPackShift);
   if (e0 + nkeep > o.entryCap || it >= o.itemCap ||
       (nin > 0 && (h0 + nin > o.hEntryCap || hit >= o.hItemCap))) {
     if (lane == 0)
       atomicOr(reinterpret_cast<unsigned long long *>(o.counters + 2),
                (unsigned long long)CL_OVERFLOW);
     return;
+  }
+  if (nin > 0) {
+    npinAcc += npin;
+    stepAcc += (nin + 1) >> 1;
   }
   if (keep) {
     const int pos = __popc(km & ((1u << lane) - 1u));
@@ -567,36 +557,29 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane, const double4 
   }
   if (lane == 0) {
     o.items[it] = make_int4(ci, (int)e0, nkeep, 0);
-    if (nin > 0) {
-      o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
-      // warp steps of the half-cluster kernel over this item, inner pairs
-      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 3),
-                (unsigned long long)((nin + 1) >> 1));
-      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 4),
-                (unsigned long long)npin);
-    }
+    if (nin > 0) o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
   }
 }
 
-// Cluster-pair search ("cell sweep"): one block per chunk of up to four i
-// clusters of one column, one i cluster per warp.  The block lists the
-// columns within reach of its column (periodic images as explicit shifts)
-// and stages the origin z of all their clusters; each warp then takes its i
-// cluster: per listed column (lanes in
-// parallel) the clusters whose origin z lies within the i box's reach, by
-// binary search in shared memory, per z image within reach; then all
-// candidates are tested against the i bounding box as one flat index space,
-// 32 per round, compacted by ballot into the warp's buffer and flushed as
-// work items of up to 32 entries.  Newton's third law: each unordered
-// cluster pair is kept once (j > i, or j == i with a positive or zero shift,
-// the latter with only the upper triangle of atom pairs).
-// (at most 96 registers and 43 KB of shared memory: five blocks per SM)
+// Cluster-pair search ("cell sweep"): one warp per i cluster.  The columns
+// within reach in x-y (periodic images as explicit shifts) are listed, 32 at
+// a time, with per z image within reach the clusters (z-sorted in their
+// column) whose origin lies within the i box's reach, found by binary
+// search; then all candidates of the listed ranges are tested against the i
+// bounding box as one flat index space, 32 per round, so every lane has work
+// and all loads of a round are independent.  Survivors are compacted by
+// ballot into the warp's buffer with their FP32 shift (the FP64 origin
+// difference plus the image, rounded once) and flushed as work items of up to
+// 32 entries.  Newton's third law: each unordered cluster pair is kept once
+// (j > i, or j == i with a positive or zero shift, the latter with only the
+// upper triangle of atom pairs).
+// (at most 96 registers and ~40 KB of shared memory per block: five blocks
+// of four warps per SM)
 __global__ void __launch_bounds__(kSearchThreads, 5)
-k_search(const int *__restrict__ nSlotsDev, const int *__restrict__ chunkStart,
-         const int2 *__restrict__ chunks, int nCols, const ClusterGeom *__restrict__ geoms,
+k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
          const DevBox *__restrict__ boxes, const int *__restrict__ clusterRep,
          const int *__restrict__ colOff, const int *__restrict__ colRank,
-         const int *__restrict__ colXY, const int *__restrict__ colClStart,
+         const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
          const double4 *__restrict__ origin, const float4 *__restrict__ originF,
          const float4 *__restrict__ half, const int *__restrict__ slotAtom,
          const int *__restrict__ slotOf, const int *__restrict__ frozen,
@@ -604,72 +587,138 @@ k_search(const int *__restrict__ nSlotsDev, const int *__restrict__ chunkStart,
          const int *__restrict__ hmaxBits, const float4 *__restrict__ xq,
          const double *__restrict__ px, const double *__restrict__ py,
          const double *__restrict__ pz, const SearchOut o) {
-  __shared__ ColTable T;
   __shared__ WarpBuf bufs[kSearchThreads / 32];
-  // this block's chunk: up to one i cluster per warp, all of one column
-  if ((int)blockIdx.x >= chunkStart[nCols]) return;
-  const int2 ch = chunks[blockIdx.x];
-  const int col = ch.x;
-  const int c0 = ch.y, c1 = min(ch.y + kSearchThreads / 32, colClStart[col + 1]);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int rep = clusterRep ? clusterRep[c0] : 0;
+  const int lane = threadIdx.x & 31;
+  const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (ci >= (*nSlotsDev >> 3)) return;
+  WarpBuf &B = bufs[threadIdx.x >> 5];
+  const int rep = clusterRep ? clusterRep[ci] : 0;
   const ClusterGeom &g = geoms[rep];
   const DevBox &box = boxes[rep];
   const int colBase = colOff[rep];
   hmaxBits += 4 * rep;
-  const int xy0 = colXY[col];
-  const int cx = xy0 & 0xffff, cy = xy0 >> 16;
+
+  const double4 oi = origin[ci];
+  const float4 oif = originF[ci];
+  const float4 hi = half[ci];
+  const int nreal_i = (int)hi.w;
+  const int xy = clusterXY[ci];
+  const int cx = xy & 0xffff, cy = xy >> 16;
+  // this lane's i atom, its exclusion partners as slots
+  const int ia = slotAtom[ci * kClusterSize + (lane & 7)];
+  int es = 0, ee = 0;
+  if (ia >= 0) {
+    es = exclStart[ia];
+    ee = exclStart[ia + 1];
+  }
+  const int nps = ee - es;
+  int ps[kExclRegs];
+#pragma unroll
+  for (int r = 0; r < kExclRegs; ++r) ps[r] = (r < nps) ? slotOf[__ldg(exclFlat + es + r)] : -1;
+  // the clusters holding any exclusion partner of the i cluster's atoms
+  int pcLo = 0x7fffffff, pcHi = -1;
+  for (int e = es; e < ee; ++e) {
+    const int pc = (e - es < kExclRegs ? ps[min(e - es, kExclRegs - 1)]
+                                       : slotOf[__ldg(exclFlat + e)]) / kClusterSize;
+    pcLo = min(pcLo, pc);
+    pcHi = max(pcHi, pc);
+  }
+  pcLo = __reduce_min_sync(0xffffffffu, pcLo);
+  pcHi = __reduce_max_sync(0xffffffffu, pcHi);
+  const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
+  const unsigned fimask = __ballot_sync(0xffffffffu, lane < kClusterSize && fi) & 0xffu;
+  if (lane < kClusterSize) {
+    B.si[lane] = xq[ci * kClusterSize + lane];
+#pragma unroll
+    for (int r = 0; r < kExclRegs; ++r) B.ps[lane][r] = ps[r];
+    B.es[lane] = es;
+    B.ee[lane] = ee;
+  }
+  __syncwarp();
+
+  const float rlist2 = g.rlist2;
+  const float rl = sqrtf(rlist2);
   const float Lx = (float)g.Lx, Ly = (float)g.Ly, Lz = (float)g.Lz;
   const float wx = (float)g.wx, wy = (float)g.wy;
-  const float rlist2 = g.rlist2;
+  // z images that can reach any cluster at all: cluster centres lie in
+  // [-Lz/2, Lz/2) and no cluster extends more than hmax[2] from its centre
+  const float hzmax = __int_as_float(hmaxBits[2]);
+  const float zwlo = oif.z - hi.z - rl - hzmax, zwhi = oif.z + hi.z + rl + hzmax;
+  const bool zm = zwlo < -0.5f * Lz;  // the image below can be within reach
+  const bool zp = zwhi > 0.5f * Lz;   // the image above can be within reach
+  int cnt = 0, npinAcc = 0, stepAcc = 0;
+  long long cand = 0;
 
-  // ---- the block's neighbour columns (warp 0), then their clusters' z ----
-  if (warp == 0) {
-    const int nx = 2 * g.Dx + 1, ncomb = nx * (2 * g.Dy + 1);
-    const float ixlo = -0.5f * Lx + cx * wx, ixhi = ixlo + wx;
-    const float iylo = -0.5f * Ly + cy * wy, iyhi = iylo + wy;
-    int n = 0;
-    for (int b0 = 0; b0 < ncomb; b0 += 32) {
-      const int cb = b0 + lane;
-      bool pass = false;
-      int cs = 0, cc = 0, code = 0, jxy = 0;
-      if (cb < ncomb) {
-        const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
-        int jy = cy + dy, sy = 0;
-        if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
-        int jx = cx + dx, sx = 0;
-        if (jx < 0) { jx += g.ncx; sx = -1; } else if (jx >= g.ncx) { jx -= g.ncx; sx = 1; }
-        const float jxlo = -0.5f * Lx + jx * wx + sx * Lx, jxhi = jxlo + wx;
-        const float jylo = -0.5f * Ly + jy * wy + sy * Ly, jyhi = jylo + wy;
-        // the cells' x-y gap, with a margin for the FP32 cell bounds
-        const float gx = fmaxf(fmaxf(jxlo - ixhi, ixlo - jxhi) - 1e-3f, 0.f);
-        const float gy = fmaxf(fmaxf(jylo - iyhi, iylo - jyhi) - 1e-3f, 0.f);
-        if (gx * gx + gy * gy <= rlist2) {
-          const int jc = colRank[colBase + jy * g.ncx + jx];
-          cs = colClStart[jc];
-          cc = colClStart[jc + 1] - cs;
-          code = (sx + 1) | ((sy + 1) << 2);
-          jxy = jx | (jy << 16);
-          pass = cc > 0;
+  const int nx = 2 * g.Dx + 1, ncomb = nx * (2 * g.Dy + 1);
+  int ncol = 0;
+  for (int c0 = 0; c0 < ncomb; c0 += 32) {
+    const int cb = c0 + lane;
+    bool pass = false;
+    int cs = 0, cc = 0, code = 0;
+    if (cb < ncomb) {
+      const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
+      int jy = cy + dy, sy = 0;
+      if (jy < 0) { jy += g.ncy; sy = -1; } else if (jy >= g.ncy) { jy -= g.ncy; sy = 1; }
+      int jx = cx + dx, sx = 0;
+      if (jx < 0) { jx += g.ncx; sx = -1; } else if (jx >= g.ncx) { jx -= g.ncx; sx = 1; }
+      const float ylo = -0.5f * Ly + jy * wy + sy * Ly, yhi = ylo + wy;
+      const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
+      const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
+      const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
+      if (gx * gx + gy * gy <= rlist2) {
+        const int col = colRank[colBase + jy * g.ncx + jx];
+        cs = colClStart[col];
+        cc = colClStart[col + 1];
+        code = (sx + 1) | ((sy + 1) << 2);
+        pass = cc > cs;
+      }
+    }
+    // Per z image within reach, the column's clusters (z-sorted) whose
+    // origin lies within the i box's reach: one listed range each.
+#pragma unroll
+    for (int sz = -1; sz <= 1; ++sz) {
+      int first = 0, n = 0;
+      if (pass && !((sz < 0 && !zm) || (sz > 0 && !zp))) {
+        const float lo = zwlo - sz * Lz, hiz = zwhi - sz * Lz;
+        int a = cs, b = cc;
+        while (a < b) {  // first origin z >= lo
+          const int mid = (a + b) >> 1;
+          if (__ldg(&originF[mid].z) < lo) a = mid + 1; else b = mid;
+        }
+        first = a;
+        b = cc;
+        while (a < b) {  // first origin z > hiz
+          const int mid = (a + b) >> 1;
+          if (__ldg(&originF[mid].z) <= hiz) a = mid + 1; else b = mid;
+        }
+        n = a - first;
+        // half list: a pair with cj < ci is listed from cj's side, so the
+        // range starts at ci at the earliest (cluster indices ascend within
+        // a column)
+        if (first < ci) {
+          n = max(0, first + n - ci);
+          first = ci;
         }
       }
-      const unsigned m = __ballot_sync(0xffffffffu, pass);
-      if (pass) {
-        const int k = n + __popc(m & ((1u << lane) - 1u));
-        T.start[k] = cs;
-        T.count[k] = cc;
-        T.code[k] = code;
-        T.xy[k] = jxy;
+      const bool has = n > 0;
+      const unsigned pm = __ballot_sync(0xffffffffu, has);
+      if (has) {
+        const int k = ncol + __popc(pm & ((1u << lane) - 1u));
+        B.rstart[k] = first;
+        B.rcount[k] = n;
+        B.rcode[k] = code | ((sz + 1) << 4);
       }
-      n += __popc(m);
+      ncol += __popc(pm);
     }
+    if (ncol <= kSearchCols - 96 && c0 + 32 < ncomb) continue;
     __syncwarp();
-    // prefix of the listed columns' cluster counts (8 per lane)
-    int v[kColTab / 32], tot = 0;
+    // prefix of the listed ranges' cluster counts (kPer ranges per lane)
+    constexpr int kPer = kSearchCols / 32;
+    int v[kPer], tot = 0;
 #pragma unroll
-    for (int r = 0; r < kColTab / 32; ++r) {
-      const int k = (kColTab / 32) * lane + r;
-      v[r] = k < n ? T.count[k] : 0;
+    for (int r = 0; r < kPer; ++r) {
+      const int k = kPer * lane + r;
+      v[r] = k < ncol ? B.rcount[k] : 0;
       tot += v[r];
     }
     int incl = tot;
@@ -679,235 +728,108 @@ k_search(const int *__restrict__ nSlotsDev, const int *__restrict__ chunkStart,
       if (lane >= off) incl += t;
     }
     int run = incl - tot;
+    __syncwarp();
 #pragma unroll
-    for (int r = 0; r < kColTab / 32; ++r) {
-      const int k = (kColTab / 32) * lane + r;
-      if (k <= n) T.pre[k] = run;
+    for (int r = 0; r < kPer; ++r) {
+      const int k = kPer * lane + r;
+      if (k <= ncol) B.rpre[k] = run;  // rpre[ncol] = total
       run += v[r];
     }
-    if (lane == 0) T.n = n;
-  }
-  __syncthreads();
-  const int ntab = T.n;
-  const bool zStaged = T.pre[ntab] <= kColZ;
-  if (zStaged)
-    for (int k = warp; k < ntab; k += kSearchThreads / 32)
-      for (int m = lane; m < T.count[k]; m += 32) T.z[T.pre[k] + m] = originF[T.start[k] + m].z;
-  __syncthreads();
-
-  WarpBuf &B = bufs[warp];
-  const float rl = sqrtf(rlist2);
-  const float hzmax = __int_as_float(hmaxBits[2]);
-  for (int ci = c0 + warp; ci < c1; ci += kSearchThreads / 32) {
-    const double4 oi = origin[ci];
-    const float4 oif = originF[ci];
-    const float4 hi = half[ci];
-    const int nreal_i = (int)hi.w;
-    // this lane's i atom, its exclusion partners as slots
-    const int ia = slotAtom[ci * kClusterSize + (lane & 7)];
-    int es = 0, ee = 0;
-    if (ia >= 0) {
-      es = exclStart[ia];
-      ee = exclStart[ia + 1];
-    }
-    const int nps = ee - es;
-    int ps[kExclRegs];
-#pragma unroll
-    for (int r = 0; r < kExclRegs; ++r) ps[r] = (r < nps) ? slotOf[__ldg(exclFlat + es + r)] : -1;
-    // the clusters holding any exclusion partner of the i cluster's atoms
-    int pcLo = 0x7fffffff, pcHi = -1;
-    for (int e = es; e < ee; ++e) {
-      const int pc = (e - es < kExclRegs ? ps[min(e - es, kExclRegs - 1)]
-                                         : slotOf[__ldg(exclFlat + e)]) / kClusterSize;
-      pcLo = min(pcLo, pc);
-      pcHi = max(pcHi, pc);
-    }
-    pcLo = __reduce_min_sync(0xffffffffu, pcLo);
-    pcHi = __reduce_max_sync(0xffffffffu, pcHi);
-    const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
-    const unsigned fimask = __ballot_sync(0xffffffffu, lane < kClusterSize && fi) & 0xffu;
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
     __syncwarp();
-    if (lane < kClusterSize) {
-      B.si[lane] = xq[ci * kClusterSize + lane];
-#pragma unroll
-      for (int r = 0; r < kExclRegs; ++r) B.ps[lane][r] = ps[r];
-      B.es[lane] = es;
-      B.ee[lane] = ee;
-    }
-    __syncwarp();
-    // z images that can reach any cluster at all: cluster centres lie in
-    // [-Lz/2, Lz/2) and no cluster extends more than hmax[2] from its centre
-    const float zwlo = oif.z - hi.z - rl - hzmax, zwhi = oif.z + hi.z + rl + hzmax;
-    const bool zm = zwlo < -0.5f * Lz;  // the image below can be within reach
-    const bool zp = zwhi > 0.5f * Lz;   // the image above can be within reach
-    int cnt = 0;
-    long long cand = 0;
-    int ncol = 0;
-    for (int k0 = 0; k0 < ntab; k0 += 32) {
-      const int k = k0 + lane;
-      bool pass = false;
-      int code = 0;
-      if (k < ntab) {
-        // the j column's cell against the i cluster's bounding box
-        const int jxy = T.xy[k];
-        code = T.code[k];
-        const int jx = jxy & 0xffff, jy = jxy >> 16;
-        const int sx = (code & 3) - 1, sy = ((code >> 2) & 3) - 1;
-        const float ylo = -0.5f * Ly + jy * wy + sy * Ly, yhi = ylo + wy;
-        const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
-        const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
-        const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
-        pass = gx * gx + gy * gy <= rlist2;
-      }
-      // Per z image within reach, the column's clusters (z-sorted) whose
-      // origin lies within the i box's reach: one listed range each.
-#pragma unroll
-      for (int sz = -1; sz <= 1; ++sz) {
-        int first = 0, n = 0;
-        if (pass && !((sz < 0 && !zm) || (sz > 0 && !zp))) {
-          const float lo = zwlo - sz * Lz, hiz = zwhi - sz * Lz;
-          const int base = T.start[k], cntk = T.count[k], zb = T.pre[k];
-          int a = 0, b = cntk;
-          while (a < b) {  // first origin z >= lo
-            const int mid = (a + b) >> 1;
-            const float zmid = zStaged ? T.z[zb + mid] : __ldg(&originF[base + mid].z);
-            if (zmid < lo) a = mid + 1; else b = mid;
-          }
-          first = a;
-          b = cntk;
-          while (a < b) {  // first origin z > hiz
-            const int mid = (a + b) >> 1;
-            const float zmid = zStaged ? T.z[zb + mid] : __ldg(&originF[base + mid].z);
-            if (zmid <= hiz) a = mid + 1; else b = mid;
-          }
-          n = a - first;
-          first += base;
-          // half list: a pair with cj < ci is listed from cj's side, so the
-          // range starts at ci at the earliest (cluster indices ascend within
-          // a column)
-          if (first < ci) {
-            n = max(0, first + n - ci);
-            first = ci;
-          }
+    for (int b0 = 0; b0 < total; b0 += 32) {
+      const int t = b0 + lane;
+      const bool valid = t < total;
+      int cj = 0, sx = 0, sy = 0, sz = 0;
+      float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
+      float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
+      double4 ojd = make_double4(0., 0., 0., 0.);
+      if (valid) {
+        // the listed range holding flat index t
+        int lo = 0, hi2 = ncol - 1;
+        while (lo < hi2) {
+          const int mid = (lo + hi2 + 1) >> 1;
+          if (B.rpre[mid] <= t) lo = mid; else hi2 = mid - 1;
         }
-        const bool has = n > 0;
-        const unsigned pm = __ballot_sync(0xffffffffu, has);
-        if (has) {
-          const int r = ncol + __popc(pm & ((1u << lane) - 1u));
-          B.rstart[r] = first;
-          B.rcount[r] = n;
-          B.rcode[r] = code | ((sz + 1) << 4);
-        }
-        ncol += __popc(pm);
+        cj = B.rstart[lo] + (t - B.rpre[lo]);
+        const int rc = B.rcode[lo];
+        sx = (rc & 3) - 1;
+        sy = ((rc >> 2) & 3) - 1;
+        sz = ((rc >> 4) & 3) - 1;
+        oj = originF[cj];
+        hj = half[cj];
+        ojd = origin[cj];
       }
-      if (ncol <= kSearchCols - 96 && k0 + 32 < ntab) continue;
+      const float fx = oj.x + sx * Lx - oif.x;
+      const float fy = oj.y + sy * Ly - oif.y;
+      const float fz = oj.z + sz * Lz - oif.z;
+      const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
+      const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
+      const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
+      cand += valid;
+      const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
+      const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
+      const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
+      const bool ok = valid && half_ok && (gxx * gxx + gyy * gyy + gzz * gzz <= rlist2);
+      const unsigned m = __ballot_sync(0xffffffffu, ok);
+      if (ok) {
+        const int pos = cnt + __popc(m & ((1u << lane) - 1u));
+        B.j[pos] = cj;
+        B.code[pos] = sidx | ((int)hj.w << 8);
+        // the entry's shift, formed in FP64 and rounded once: the value the
+        // pair kernel adds to the j atoms
+        B.sh[pos] = make_float4((float)(ojd.x + sx * g.Lx - oi.x),
+                                (float)(ojd.y + sy * g.Ly - oi.y),
+                                (float)(ojd.z + sz * g.Lz - oi.z), 0.f);
+      }
+      cnt += __popc(m);
       __syncwarp();
-      // prefix of the listed ranges' cluster counts (kPer ranges per lane)
-      constexpr int kPer = kSearchCols / 32;
-      int v[kPer], tot = 0;
-#pragma unroll
-      for (int r = 0; r < kPer; ++r) {
-        const int q = kPer * lane + r;
-        v[r] = q < ncol ? B.rcount[q] : 0;
-        tot += v[r];
-      }
-      int incl = tot;
-#pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, incl, off);
-        if (lane >= off) incl += t;
-      }
-      int run = incl - tot;
-      __syncwarp();
-#pragma unroll
-      for (int r = 0; r < kPer; ++r) {
-        const int q = kPer * lane + r;
-        if (q <= ncol) B.rpre[q] = run;  // rpre[ncol] = total
-        run += v[r];
-      }
-      const int total = __shfl_sync(0xffffffffu, incl, 31);
-      __syncwarp();
-      for (int b0 = 0; b0 < total; b0 += 32) {
-        const int t = b0 + lane;
-        const bool valid = t < total;
-        int cj = 0, sx = 0, sy = 0, sz = 0;
-        float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
-        float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (valid) {
-          // the listed range holding flat index t
-          int lo = 0, hi2 = ncol - 1;
-          while (lo < hi2) {
-            const int mid = (lo + hi2 + 1) >> 1;
-            if (B.rpre[mid] <= t) lo = mid; else hi2 = mid - 1;
-          }
-          cj = B.rstart[lo] + (t - B.rpre[lo]);
-          const int rc = B.rcode[lo];
-          sx = (rc & 3) - 1;
-          sy = ((rc >> 2) & 3) - 1;
-          sz = ((rc >> 4) & 3) - 1;
-          oj = originF[cj];
-          hj = half[cj];
-        }
-        const float fx = oj.x + sx * Lx - oif.x;
-        const float fy = oj.y + sy * Ly - oif.y;
-        const float fz = oj.z + sz * Lz - oif.z;
-        const float gxx = fmaxf(fabsf(fx) - hi.x - hj.x, 0.f);
-        const float gyy = fmaxf(fabsf(fy) - hi.y - hj.y, 0.f);
-        const float gzz = fmaxf(fabsf(fz) - hi.z - hj.z, 0.f);
-        cand += valid;
-        const int sidx = (sx + 1) + 3 * (sy + 1) + 9 * (sz + 1);
-        const bool positive = sz > 0 || (sz == 0 && (sy > 0 || (sy == 0 && sx > 0)));
-        const bool half_ok = (cj > ci) || (cj == ci && (sidx == 13 || positive));
-        const bool ok = valid && half_ok && (gxx * gxx + gyy * gyy + gzz * gzz <= rlist2);
-        const unsigned m = __ballot_sync(0xffffffffu, ok);
-        if (ok) {
-          const int pos = cnt + __popc(m & ((1u << lane) - 1u));
-          B.j[pos] = cj;
-          B.code[pos] = sidx | ((int)hj.w << 8);
-        }
-        cnt += __popc(m);
+      if (cnt >= kItemMax) {
+        flush_item(B, kItemMax, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat,
+                   slotOf, slotAtom, frozen, px, py, pz, o, npinAcc, stepAcc);
         __syncwarp();
-        if (cnt >= kItemMax) {
-          flush_item(B, kItemMax, ci, lane, oi, xq, g, box, nreal_i, pcLo, pcHi, fimask,
-                     exclFlat, slotOf, slotAtom, frozen, px, py, pz, origin, o);
-          __syncwarp();
-          const int rem = cnt - kItemMax;
-          if (lane < rem) {
-            B.j[lane] = B.j[kItemMax + lane];
-            B.code[lane] = B.code[kItemMax + lane];
-          }
-          cnt = rem;
-          __syncwarp();
+        const int rem = cnt - kItemMax;
+        if (lane < rem) {
+          B.j[lane] = B.j[kItemMax + lane];
+          B.code[lane] = B.code[kItemMax + lane];
+          B.sh[lane] = B.sh[kItemMax + lane];
         }
+        cnt = rem;
+        __syncwarp();
       }
-      ncol = 0;
-      __syncwarp();
     }
-    if (cnt > 0)
-      flush_item(B, cnt, ci, lane, oi, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat,
-                 slotOf, slotAtom, frozen, px, py, pz, origin, o);
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, off);
-    if (lane == 0)
-      atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 3), (unsigned long long)cand);
+    ncol = 0;
     __syncwarp();
+  }
+  if (cnt > 0)
+    flush_item(B, cnt, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
+               slotAtom, frozen, px, py, pz, o, npinAcc, stepAcc);
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, off);
+  if (lane == 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 3), (unsigned long long)cand);
+    // warp steps of the half-cluster kernel over this i cluster's inner
+    // items, and its inner pairs
+    if (stepAcc > 0) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 3),
+                (unsigned long long)stepAcc);
+      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 4),
+                (unsigned long long)npinAcc);
+    }
   }
 }
 
-// Chunks of the search: per column, ceil(clusters / 4) chunks of up to four
-// consecutive i clusters.
-__global__ void k_col_chunks(int nCols, const int *__restrict__ colClStart, int *__restrict__ n) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < nCols) n[c] = (colClStart[c + 1] - colClStart[c] + kSearchThreads / 32 - 1) /
-                        (kSearchThreads / 32);
-}
-__global__ void k_col_chunk_fill(int nCols, const int *__restrict__ colClStart,
-                                 const int *__restrict__ chunkStart, int2 *__restrict__ chunks) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nCols) return;
-  const int n = chunkStart[c + 1] - chunkStart[c];
-  for (int k = 0; k < n; ++k)
-    chunks[chunkStart[c] + k] = make_int2(c, colClStart[c] + k * (kSearchThreads / 32));
+// The packed list counters (items << 40 | entries) unpacked for the readers.
+__global__ void k_unpack_counts(long long *__restrict__ counters, long long *__restrict__ hcounters) {
+  if (threadIdx.x == 0) {
+    const unsigned long long m = (1ull << kPackShift) - 1ull;
+    const unsigned long long a = (unsigned long long)counters[4];
+    const unsigned long long b = (unsigned long long)hcounters[5];
+    counters[0] = (long long)(a & m);
+    counters[1] = (long long)(a >> kPackShift);
+    hcounters[0] = (long long)(b & m);
+    hcounters[1] = (long long)(b >> kPackShift);
+  }
 }
 
 __global__ void k_refresh(const int *__restrict__ nSlotsDev,
@@ -1182,7 +1104,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
     MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
     MDB_TRY(w.scanTmp.ensure(scan_tmp_bytes(std::max(n, nCols) + 1)));
-    MDB_TRY(w.counters.ensure(sizeof(long long) * 4));
+    MDB_TRY(w.counters.ensure(sizeof(long long) * 8));
     MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
     if (!w.sticky.p) {
       MDB_TRY(w.sticky.ensure(sizeof(long long)));
@@ -1209,7 +1131,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
 
   MDB_CUDA(cudaMemsetAsync(w.colCount.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
-  MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 4, s));
+  MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 8, s));
   MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4 * nRep, s));
   MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, gd, w.atomRepDev(), w.colOff.as<int>(),
              w.colRank.as<int>(), x, y, z, w.atomCol.as<int>(), w.atomZ.as<double>(),
@@ -1220,19 +1142,6 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
   MDB_TRY(exclusive_scan32(w.colPad.as<int>(), w.colPadStart.as<int>(), nCols, w.scanTmp.p, s));
   MDB_LAUNCH(k_col_clstart, grid_for(nCols + 1, 256), 256, 0, s, nCols, w.colPadStart.as<int>(),
              w.colClStart.as<int>());
-  // search chunks (at most clusters / 4 + one per column)
-  const int chunkCap = w.clCap / (kSearchThreads / 32) + nCols + 1;
-  if (sync) {
-    MDB_TRY(w.chunkCount.ensure(sizeof(int) * (nCols + 1)));
-    MDB_TRY(w.chunkStart.ensure(sizeof(int) * (nCols + 2)));
-    MDB_TRY(w.chunks.ensure(sizeof(int2) * chunkCap));
-  }
-  MDB_LAUNCH(k_col_chunks, grid_for(nCols, 256), 256, 0, s, nCols, w.colClStart.as<int>(),
-             w.chunkCount.as<int>());
-  MDB_TRY(exclusive_scan32(w.chunkCount.as<int>(), w.chunkStart.as<int>(), nCols, w.scanTmp.p,
-                           s));
-  MDB_LAUNCH(k_col_chunk_fill, grid_for(nCols, 256), 256, 0, s, nCols, w.colClStart.as<int>(),
-             w.chunkStart.as<int>(), w.chunks.as<int2>());
   MDB_LAUNCH(k_col_scatter, grid_for(n, 256), 256, 0, s, n, w.atomCol.as<int>(),
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
   MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
@@ -1266,7 +1175,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
       MDB_TRY(w.countersIn.ensure(sizeof(long long) * 8));
     }
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
-    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long), s));
+    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 2, s));
     MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
     SearchOut o;
     o.entries = w.entries.as<CPairEntry>();
@@ -1282,13 +1191,14 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     o.hEntryCap = w.inEntryCap;
     o.hItemCap = w.inItemCap;
     o.rin2 = rin2;
-    MDB_LAUNCH(k_search, chunkCap, kSearchThreads, 0, s, w.nSlotsDev(), w.chunkStart.as<int>(),
-               w.chunks.as<int2>(), nCols, gd,
-               w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(), w.colRank.as<int>(),
-               w.colXY.as<int>(), w.colClStart.as<int>(), w.origin.as<double4>(),
-               w.originF.as<float4>(), w.half.as<float4>(), w.slotAtom.as<int>(),
-               w.slotOf.as<int>(), frozen, exclStart, exclFlat, w.hmax.as<int>(),
-               w.xq.as<float4>(), x, y, z, o);
+    MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
+               w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
+               w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
+               w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
+               w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
+               w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
+    MDB_LAUNCH(k_unpack_counts, 1, 32, 0, s, w.counters.as<long long>(),
+               w.countersIn.as<long long>());
     w.innerRin2 = rin2;
     if (!sync) {
       w.useInner = true;

@@ -68,7 +68,6 @@ struct ClusterWork {
   DBuf colRank;       // colOff[r] + (cy*ncx+cx) -> global column, Morton order inside r
   DBuf colXY;         // global column -> cx | cy << 16
   DBuf colCount, colFill, colStart, colPad, colPadStart;
-  DBuf chunkCount, chunkStart, chunks;  // search blocks: per column, chunks of i clusters
   DBuf atomCol, tmpIdx;
   DBuf atomZ;         // wrapped fractional z (FP64)
   DBuf scanTmp;
@@ -100,7 +99,8 @@ struct ClusterWork {
   DBuf entries;       // CPairEntry
   DBuf masks;         // uint2 (64 interaction bits)
   DBuf items;         // int4: i cluster, first entry, entry count, 0
-  DBuf counters;      // int64[4]: entries, items, overflow flag, candidates
+  DBuf counters;      // int64[8]: entries, items, overflow flag, candidates, and the
+                      // search's packed count (items << 40 | entries)
   long long entryCap = 0, itemCap = 0;
   long long nEntries = 0, nItems = 0;
   // Inner list: the j-cluster halves of the list above that hold a pair
@@ -112,7 +112,7 @@ struct ClusterWork {
   DBuf masksIn;       // uint32
   DBuf itemsIn;       // int4: i cluster, first half entry, count, 0
   DBuf countersIn;    // int64[8]: entries, items, overflow flag, warp steps, pairs
-                      // within the inner radius
+                      // within the inner radius, the search's packed count
   long long inEntryCap = 0, inItemCap = 0;
   float rin2 = 0.f;   // radius^2 of the inner list the search writes (0: the
                       // pair kernel's own FP32 rc^2, an exact inner list)

@@ -514,8 +514,12 @@ class Engine:
         and keep the fastest (call after build; recompute afterwards)."""
         out = (C.c_int * 4)()
         check(lib().mdbas_nb_engine_autotune(self.h, out), "engine_autotune")
+        # the variants differ in their cluster shapes: the half-cluster ones
+        # (4, 5) pair 8-atom i clusters with 4-atom j-cluster halves, the
+        # others 8-atom i with 8-atom j clusters
         return {"variant": out[0], "block": out[1], "blocks_per_sm": out[2],
-                "candidates": out[3]}
+                "candidates": out[3], "i_cluster_atoms": 8,
+                "j_cluster_atoms": 4 if out[0] in (4, 5) else 8}
 
     def split(self, arrays):
         """Per-replica views of concatenated per-atom arrays."""
