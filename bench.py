@@ -47,10 +47,16 @@ WORKLOAD = ("96,000-atom rigid water box (32,000 molecules, 98.6 A cube, 0.0334/
 # LJ core 14, switch 15, force scalar 2, force vector + i/j accumulation 9,
 # energy + virial 4
 FLOPS_PER_PAIR = 77
-# algorithmic HBM bytes per atom of one list rebuild (cell sort + cluster layout):
-# read FP64 xyz 24 + q/eps/sig 24, write cell keys 4 + permutation 8 + float4 16
-# + float2 8, sort passes 24
-LIST_BYTES_PER_ATOM = 108
+# algorithmic HBM bytes per atom of the list build's sort and layout stages:
+#   bin: read FP64 x, y, z 24, write column 4 + fractional z 8
+#   scatter: read column 4, write the column-ordered index 4 (+ column starts)
+#   column sort: read index 4 + z 8, write the slot's atom 4
+#   cluster layout, per slot (1.09 slots per atom at 96k, padding): read the
+#     slot's atom 4, x, y, z 24, q, eps, sig 24; write float4 16 + float2 8,
+#     their pair-interleaved copies 16 + 8, the atom's slot 4, per cluster
+#     FP64 origin, FP32 origin and half extents (64 B / 8 slots) -> 112
+BUILD_STAGE_BYTES = {"bin": 36, "scatter": 12, "column_sort": 16, "cluster_layout": 122}
+LIST_BYTES_PER_ATOM = 36 + 12 + 16 + 122
 FS_PER_STEP = 1.0
 
 
@@ -73,7 +79,7 @@ def _parse():
                    help="timed steps of the 999,999-atom box; 0 skips it")
     p.add_argument("--replica-steps", type=int, default=100,
                    help="timed dynamics steps of the 64-replica batch (one CUDA graph); 0 skips")
-    p.add_argument("--case", choices=["pair", "md"], default=None,
+    p.add_argument("--case", choices=["pair", "md", "build1m"], default=None,
                    help="run one small case of the 96k box for a profiler and exit: 'pair' = "
                         "list build + 4 force evaluations, 'md' = --md-steps dynamics steps "
                         "driven from the host (a profiler sees no kernels inside graphs with "
@@ -502,6 +508,15 @@ def _same_pair_set(n, ai, aj, bi, bj) -> dict:
                     "GPU builder's, same wrapped 96k coordinates"}
 
 
+def hbm_peak() -> float:
+    """Measured HBM copy bandwidth (GB/s) of this pool's B200s, from the
+    driver-written MEASURED_PEAKS.json, else the recipe's fallback."""
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+    except Exception:
+        return 6650.0
+
+
 def fp32_peaks(device: int) -> tuple:
     """Measured FP32 FMA throughput of the device (TFLOP/s): scalar FFMA and
     packed f32x2 FMA, from the bench-side probe library."""
@@ -629,6 +644,21 @@ def large_box_measure(torch, nb, systems, dev, stream, flush, seed, steps):
 
     ms = _time_steps(torch, eng, stream, flush, steps, step)
     ms_build = _time_steps(torch, eng, stream, flush, steps, eng.build)
+    # the build stage by stage (CUDA events between the launches, L2 flushed
+    # first), with each stage's algorithmic HBM bytes
+    stage_runs = []
+    for _ in range(max(3, steps)):
+        flush.zero_()
+        torch.cuda.synchronize()
+        stage_runs.append(eng.build_stages())
+    stages = {}
+    for k in stage_runs[0]:
+        t = statistics.median(r[k] for r in stage_runs)
+        b = BUILD_STAGE_BYTES.get(k)
+        stages[k] = {"ms": t}
+        if b is not None:
+            stages[k]["bytes_per_atom"] = b
+            stages[k]["hbm_gbs"] = b * n / (t * 1e-3) / 1e9
     eng.set_timing(True)
     eng.pair_kernel_ms(reset=True)
     for _ in range(steps):
@@ -659,7 +689,8 @@ def large_box_measure(torch, nb, systems, dev, stream, flush, seed, steps):
         "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3)},
         "list_build": {"ms": t_build,
                        "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9,
-                       "bytes_per_atom": LIST_BYTES_PER_ATOM},
+                       "bytes_per_atom": LIST_BYTES_PER_ATOM, "stages": stages,
+                       "stage_peak_gbs": hbm_peak()},
         "force_rel_rms_vs_fp64_form": float(np.sqrt(num / den)),
         "energy_rel_vs_fp64_form": abs(tot_a - tot_b) / abs(tot_b),
         "fp64_form_pairs": int(eb["n_pairs"]),
@@ -1085,6 +1116,14 @@ def run_case(args):
             e.compute()
         print(json.dumps({"case": "pair", "variant": args.variant,
                           "pairs": e.energies()["n_pairs"], "list": e.list_stats()}))
+    elif args.case == "build1m":
+        # the 999,999-atom box: three list builds (for a profiler capture of
+        # the build kernels at full size)
+        s = systems.config_1m(seed=args.seed)
+        e = nb.Engine(s, precision=1)
+        for _ in range(3):
+            e.build()
+        print(json.dumps({"case": "build1m", "list": e.list_stats()}))
     else:
         s = systems.config_96k(seed=args.seed, temperature=300.0)
         e = nb.Engine(s, precision=1)

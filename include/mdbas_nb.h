@@ -426,6 +426,11 @@ int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
  * block, blocks per SM, candidates tried}.  Call after build; the
  * accumulators are left dirty, so compute again before reading forces. */
 int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]);
+/* Mixed precision: one synchronising list build with CUDA events between its
+ * stages (no counterpart in MDBas; measurement of the build).  ms[0..5] =
+ * binning into columns, the columns' scans and padding, scatter into
+ * columns, in-column z sort, cluster layout, cluster-pair search. */
+int mdbas_nb_engine_build_stages(mdbas_nb_engine *e, double ms[6]);
 /* Kernels this engine launched since creation. */
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e);
 /* Average duration (ms) of the pair kernel over the launches recorded since

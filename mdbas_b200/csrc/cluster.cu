@@ -1133,19 +1133,24 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
   MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
   MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 8, s));
   MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4 * nRep, s));
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[0], s));
   MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, gd, w.atomRepDev(), w.colOff.as<int>(),
              w.colRank.as<int>(), x, y, z, w.atomCol.as<int>(), w.atomZ.as<double>(),
              w.colCount.as<int>(), w.counters.as<long long>());
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[1], s));
   MDB_TRY(exclusive_scan32(w.colCount.as<int>(), w.colStart.as<int>(), nCols, w.scanTmp.p, s));
   MDB_LAUNCH(k_col_pad, grid_for(nCols, 256), 256, 0, s, nCols, w.colCount.as<int>(),
              w.colPad.as<int>());
   MDB_TRY(exclusive_scan32(w.colPad.as<int>(), w.colPadStart.as<int>(), nCols, w.scanTmp.p, s));
   MDB_LAUNCH(k_col_clstart, grid_for(nCols + 1, 256), 256, 0, s, nCols, w.colPadStart.as<int>(),
              w.colClStart.as<int>());
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[2], s));
   MDB_LAUNCH(k_col_scatter, grid_for(n, 256), 256, 0, s, n, w.atomCol.as<int>(),
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[3], s));
   MDB_LAUNCH(k_col_sort, nCols, 256, 0, s, nCols, w.colStart.as<int>(), w.colPadStart.as<int>(),
              w.tmpIdx.as<int>(), w.atomZ.as<double>(), w.slotAtom.as<int>());
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[4], s));
   MDB_LAUNCH(k_clusters, grid_for(w.slotCap, 256), 256, 0, s, w.nSlotsDev(), gd, w.atomRepDev(),
              nRep > 1 ? w.clusterRep.as<int>() : nullptr, w.slotAtom.as<int>(), w.atomCol.as<int>(), w.colXY.as<int>(), x,
              y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
@@ -1191,6 +1196,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     o.hEntryCap = w.inEntryCap;
     o.hItemCap = w.inItemCap;
     o.rin2 = rin2;
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[5], s));
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
                w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
                w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
@@ -1199,6 +1205,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
                w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
     MDB_LAUNCH(k_unpack_counts, 1, 32, 0, s, w.counters.as<long long>(),
                w.countersIn.as<long long>());
+  if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[6], s));
     w.innerRin2 = rin2;
     if (!sync) {
       w.useInner = true;
@@ -1277,6 +1284,28 @@ int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s) {
              w.sticky.as<long long>());
   w.innerRin2 = rin2;
   w.useInner = true;
+  return MDBAS_NB_OK;
+}
+
+int cluster_build_stages(ClusterWork &w, int n, int nRep, const DevBox *boxes,
+                         const int *atomOff, double cutOff, double delr, int listRule,
+                         double sqrtC, const double *x, const double *y, const double *z,
+                         const double *q, const double *eps, const double *sig,
+                         const int *frozen, const int *exclStart, const int *exclFlat,
+                         cudaStream_t s, double ms[6]) {
+  for (cudaEvent_t &ev : w.stageEv)
+    if (!ev) MDB_CUDA(cudaEventCreate(&ev));
+  w.timeStages = true;
+  const int st = cluster_build(w, n, nRep, boxes, atomOff, cutOff, delr, listRule, sqrtC, x, y,
+                               z, q, eps, sig, frozen, exclStart, exclFlat, s, true);
+  w.timeStages = false;
+  MDB_TRY(st);
+  MDB_CUDA(cudaStreamSynchronize(s));
+  for (int k = 0; k < 6; ++k) {
+    float t = 0.f;
+    MDB_CUDA(cudaEventElapsedTime(&t, w.stageEv[k], w.stageEv[k + 1]));
+    ms[k] = t;
+  }
   return MDBAS_NB_OK;
 }
 

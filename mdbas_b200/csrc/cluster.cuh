@@ -120,9 +120,18 @@ struct ClusterWork {
   long long nInEntries = 0, nInItems = 0, nInSteps = 0;  // host copies (synchronising builds)
   bool useInner = false;
   DBuf sticky;        // int64: OR of every build's error bits since last read
+  // stage timing of a synchronising build (cluster_build_stages): events
+  // after binning, the grid scans, the scatter, the column sort, the cluster
+  // layout and the search
+  bool timeStages = false;
+  cudaEvent_t stageEv[7] = {};
   // accumulators
   DBuf facc;          // int64 fixed-point forces, SoA [3][slotCap]
   DBuf acc;           // int64[ACC_COUNT]
+  ~ClusterWork() {
+    for (cudaEvent_t ev : stageEv)
+      if (ev) cudaEventDestroy(ev);
+  }
   const int *nSlotsDev() const { return colPadStart.as<int>() + nCols; }
   const int *atomRepDev() const { return nRep > 1 ? atomRep.as<int>() : nullptr; }
   const int *clusterRepDev() const { return nRep > 1 ? clusterRep.as<int>() : nullptr; }
@@ -162,6 +171,14 @@ inline int list_rule(int linkRatio, int noLink) { return (linkRatio & 7) | (noLi
 // current layout (after cluster_refresh), drop entries left without pairs.
 // No host interaction (graph-capturable); requires a synchronising build.
 int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s);
+// A synchronising build with CUDA events between its stages; ms[0..5] =
+// binning, grid scans, scatter, column sort, cluster layout, search.
+int cluster_build_stages(ClusterWork &w, int n, int nRep, const DevBox *boxes,
+                         const int *atomOff, double cutOff, double delr, int listRule,
+                         double sqrtC, const double *x, const double *y, const double *z,
+                         const double *q, const double *eps, const double *sig,
+                         const int *frozen, const int *exclStart, const int *exclFlat,
+                         cudaStream_t s, double ms[6]);
 // Host copies of the list counts (synchronises the stream).
 int cluster_read_counts(ClusterWork &w, cudaStream_t s);
 // Refresh xq from the current FP64 positions (list kept).

@@ -663,6 +663,27 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs,
 
 long long mdbas_nb_engine_launch_count(mdbas_nb_engine *e) { return e ? e->launches : -1; }
 
+int mdbas_nb_engine_build_stages(mdbas_nb_engine *e, double ms[6]) {
+  if (!e || !ms) return MDBAS_NB_ERR_ARG;
+  if (e->cfg.precision != 1) return MDBAS_NB_ERR_UNSUPPORTED;
+  if (!e->topoSet || !e->posSet) return MDBAS_NB_ERR_STATE;
+  ENG_TRY(e, set_dev(e));
+  ENG_TRY(e, engine_resolve_build(e));
+  LaunchScope ls(e);
+  const int *frozen = e->hasFrozen ? e->frozen.as<int>() : nullptr;
+  ENG_TRY(e, cluster_build_stages(e->cl, e->n, e->nRep, e->repBoxes.data(), e->repOff.data(),
+                                  e->cfg.cutOff, e->cfg.delr, engine_list_rule(e),
+                                  sqrt(e->cfg.chargeConst), e->x.as<double>(),
+                                  e->y.as<double>(), e->z.as<double>(), e->q.as<double>(),
+                                  e->eps.as<double>(), e->sig.as<double>(), frozen,
+                                  e->exclStartSym.as<int>(), e->exclFlatSym.as<int>(),
+                                  e->stream, ms));
+  e->built = true;
+  e->buildPending = false;
+  e->computed = false;
+  return MDBAS_NB_OK;
+}
+
 int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   if (!e || !out) return MDBAS_NB_ERR_ARG;
   if (e->cfg.precision != 1) return MDBAS_NB_ERR_UNSUPPORTED;

@@ -212,6 +212,7 @@ def lib():
     L.mdbas_nb_engine_launch_count.argtypes = [C.c_void_p]
     L.mdbas_nb_engine_set_timing.argtypes = [C.c_void_p, C.c_int]
     L.mdbas_nb_engine_set_variant.argtypes = [C.c_void_p, C.c_int]
+    L.mdbas_nb_engine_build_stages.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     L.mdbas_nb_engine_kernel_time.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double),
                                               C.POINTER(C.c_longlong), C.c_int]
     L.mdbas_nb_engine_md_init.argtypes = [C.c_void_p, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
@@ -460,6 +461,13 @@ class Engine:
         check(lib().mdbas_nb_engine_export_pairs(self.h, r2max, _ptr(buf), cnt.value,
                                                  C.byref(cnt)), "engine_export_pairs")
         return buf[:2 * cnt.value].reshape(-1, 2)
+
+    def build_stages(self) -> dict:
+        """One synchronising list build timed stage by stage (ms)."""
+        ms = (C.c_double * 6)()
+        check(lib().mdbas_nb_engine_build_stages(self.h, ms), "engine_build_stages")
+        return dict(zip(("bin", "grid_scans", "scatter", "column_sort", "cluster_layout",
+                         "search"), list(ms)))
 
     def launches(self) -> int:
         return int(lib().mdbas_nb_engine_launch_count(self.h))
