@@ -566,6 +566,23 @@ def _time_steps(torch, eng, stream, flush, steps, fn):
     return [a.elapsed_time(b) for a, b in evs]
 
 
+def _time_split_steps(torch, stream, flush, steps, first, second):
+    """Steps of first() then second(), with an event between them: per step
+    (first ms, second ms), so the two parts add up to the step time."""
+    evs = []
+    for _ in range(steps):
+        flush.zero_()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        first()
+        e[1].record(stream)
+        second()
+        e[2].record(stream)
+        evs.append(e)
+    torch.cuda.synchronize()
+    return [(a.elapsed_time(b), b.elapsed_time(c)) for a, b, c in evs]
+
+
 def md_measure(torch, nb, systems, dev, stream, seed, precision, steps, nve_steps, world,
                kspace=None):
     """Velocity-Verlet dynamics of the 96k water box (rigid SHAKE/RATTLE
@@ -886,6 +903,14 @@ def run_ours(args, rank, world):
         dist.barrier()
     value = total_pairs / (t_step * 1e-3)
 
+    # the same step with an event between the list build and the force
+    # evaluation: a decomposition of the step that adds up to it
+    parts = _time_split_steps(torch, stream, flush, args.steps, eng.build, eng.compute)
+    step_parts = {"list_build_ms": statistics.mean(p[0] for p in parts),
+                  "forces_ms": statistics.mean(p[1] for p in parts),
+                  "what": "one build + one force evaluation per step, events between them "
+                          "(L2 flushed before each step); the two add up to the step"}
+
     # ---- pair kernel alone (CUDA events on the launching stream) ----------
     eng.set_timing(True)
     eng.pair_kernel_ms(reset=True)
@@ -895,13 +920,14 @@ def run_ours(args, rank, world):
     pair_ms, _ = eng.pair_kernel_ms(reset=True)
     # the other variants of the same kernel, for comparison
     other_ms = {}
-    for v, name in ((2, "packed_8x8"), (0, "scalar_dense_8x8"), (1, "compacted_8x8")):
+    for v, name in ((4, "half_8x4"), (6, "quad_4x4"), (5, "half_8x4_80reg"), (2, "packed_8x8"),
+                    (0, "scalar_dense_8x8"), (1, "compacted_8x8")):
         eng.set_variant(v)
         for _ in range(args.steps):
             flush.zero_()
             eng.compute()
         other_ms[name], _ = eng.pair_kernel_ms(reset=True)
-    eng.set_variant(4)
+    eng.set_variant(7)
     eng.set_timing(False)
     # list build alone
     ms_build = _time_steps(torch, eng, stream, flush, args.steps, eng.build)
@@ -1073,9 +1099,10 @@ def run_ours(args, rank, world):
             "spme": spme,
             "replicas": replicas,
             "pair_kernel": {"ms": pair_ms, "pairs_per_s": pairs / (pair_ms * 1e-3),
-                            "variant": "half clusters: 8-atom i x two 4-atom j halves per "
-                                       "warp step, packed f32x2, inner list",
+                            "variant": "half clusters, lean form: 8-atom i x two 4-atom j "
+                                       "halves per warp step, packed f32x2, exact inner list",
                             "other_variants_ms": other_ms},
+            "step_parts": step_parts,
             "list_build": {"ms": t_build,
                            "hbm_gbs": LIST_BYTES_PER_ATOM * n / (t_build * 1e-3) / 1e9},
             "fp64_form": {"ms_per_step": t64, "pairs_per_s": pairs / (t64 * 1e-3),
@@ -1087,7 +1114,7 @@ def run_ours(args, rank, world):
                          "peak_source": "measured FMA probe, the larger of scalar FFMA and "
                                         "packed f32x2 FMA (mdbas_b200/peak/fp32_peak.cu)",
                          "peak_probe_tflops": {"ffma": peaks[0], "ffma2": peaks[1]},
-                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_half",
+                         "flops_per_pair": FLOPS_PER_PAIR, "kernel": "k_pair_half_lean",
                          # the same flops counted on every listed pair slot (8 x 8
                          # per cluster pair, in the cut-off or not); frac = this x
                          # the pair efficiency of the cluster list

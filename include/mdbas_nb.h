@@ -405,7 +405,9 @@ int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]);
  * the number of pairs; pairs (2*capacity ints) may be NULL to query it. */
 int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, long long capacity,
                                  long long *count);
-/* Pair kernel variant of the mixed-precision path: 4 (default) takes two
+/* Pair kernel variant of the mixed-precision path: 7 (default) is variant 4
+ * in a lean form (pairs outside the mask placed at r^2 = 1e30 instead of
+ * zeroed products, fewer registers; the same forces bit for bit); 4 takes two
  * 4-atom halves of j clusters per warp step against an 8-atom i cluster, a
  * lane's two pairs in packed f32x2 arithmetic, over the inner list (the
  * halves holding a pair within the cut-off, written by the list build for
@@ -418,7 +420,10 @@ int mdbas_nb_engine_export_pairs(mdbas_nb_engine *e, double r2max, int *pairs, l
  * variant 2 with each chunk's j data brought into shared memory by
  * asynchronous bulk copies (cp.async.bulk with an mbarrier, double buffered)
  * instead of per-lane loads -- the same results as 2 bit for bit.  Variants
- * 0-3 always walk the full list. */
+ * 0-3 always walk the full list.  5 is variant 4 at up to 80 registers.
+ * 6 splits each inner-list half into its two 4-atom i halves and computes
+ * 4 x 4 units, four per warp step (i clusters of 4 atoms: fewer pairs beyond
+ * the cut-off); without a current inner list it runs as variant 4. */
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant);
 /* Autotuner of the mixed-precision pair kernel: times each variant and
  * launch shape (threads per block x blocks per SM) on the current list with

@@ -697,7 +697,8 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
   struct Cand { int variant, block, bps; };
   std::vector<Cand> cands;
   // the dense kernel takes at most 256 threads per block (launch bounds)
-  for (int variant : {kPairHalf, kPairHalf3, kPairPacked, kPairBulk, kPairDense})
+  for (int variant : {kPairHalf, kPairHalfLean, kPairHalf3, kPairQuad, kPairPacked, kPairBulk,
+                      kPairDense})
     for (int block : {64, 128, 256})
       for (int bps : {2, 4, 8, 16, 32})
         if (block * bps <= 2048 && bps <= 24) cands.push_back({variant, block, bps});
@@ -738,7 +739,8 @@ int mdbas_nb_engine_autotune(mdbas_nb_engine *e, int out[4]) {
 
 int mdbas_nb_engine_set_variant(mdbas_nb_engine *e, int variant) {
   if (!e || (variant != kPairDense && variant != kPairCompact && variant != kPairPacked &&
-             variant != kPairBulk && variant != kPairHalf && variant != kPairHalf3))
+             variant != kPairBulk && variant != kPairHalf && variant != kPairHalf3 &&
+             variant != kPairQuad && variant != kPairHalfLean))
     return MDBAS_NB_ERR_ARG;
   e->variant = variant;
   return MDBAS_NB_OK;

@@ -43,7 +43,7 @@ struct mdbas_nb_engine {
   mdbas::ClusterWork cl;
   mdbas::DBuf fout;
   int grid = 0, block = 0;
-  int variant = 4;  // pair kernel variant (kPairHalf)
+  int variant = 7;  // pair kernel variant (kPairHalfLean)
   // export scratch
   mdbas::DBuf exportBuf, exportCount;
   // adjoint scratch (adjoint.cu)

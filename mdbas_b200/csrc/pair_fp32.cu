@@ -963,6 +963,476 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
   }
 }
 
+// Lean form of k_pair_half over the exact inner list (the default): the same
+// pairs and arithmetic with fewer instructions and registers per step --
+// pairs outside the mask get r^2 = 1e30 instead of zeroed charge and LJ
+// products (their terms vanish: exp underflows to 0, the LJ powers to 0, the
+// switch variable is clamped at D so S and dS stay finite), the Coulomb
+// energy is summed as sum g - (2 alpha / sqrt pi) sum q q e^{-(alpha r)^2},
+// per step only the largest |j force| is kept for the range check (a NaN
+// shows up in the i forces, checked per item), and the per-lane 64-bit
+// energy sums live in shared memory.
+template <bool VDW, bool EXACT>
+__global__ void __launch_bounds__(256, 4)
+k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict__ items,
+            const void *__restrict__ entriesV, const void *__restrict__ masksV,
+            const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
+            long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
+  __shared__ __align__(16) HalfStage stage[8];
+  __shared__ long long esum[4][256];  // per lane: Ec, Ev, Vc, Vv
+  HalfStage &S = stage[threadIdx.x >> 5];
+  constexpr bool INNER = true;
+  const float kFar = 1e30f;
+  const int lane = threadIdx.x & 31;
+  const int il = lane & 7, jl = lane >> 3;
+  const bool up = il & 4, mid = il & 2, lo = il & 1;
+  const int comp = mid ? (lo ? 3 : 2) : (lo ? 1 : 0);
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *fcomp = facc + (size_t)(comp < 3 ? comp : 0) * fstride;
+  const float two_a = c.two_a_sqrtpi;
+  const unsigned lanebit = 1u << lane;
+  esum[0][threadIdx.x] = 0;
+  esum[1][threadIdx.x] = 0;
+  esum[2][threadIdx.x] = 0;
+  esum[3][threadIdx.x] = 0;
+  int npair = 0;
+  bool overflow = false;
+  float vmax = 0.f;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    const int nsteps = INNER ? (ne + 1) >> 1 : ne;
+    const float4 xi = xq[ci * kClusterSize + il];
+    const float2 li = lj[ci * kClusterSize + il];
+    const float2 nx = f2(-xi.x), ny = f2(-xi.y), nz = f2(-xi.z);
+    float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
+    float2 qs = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
+    for (int s0 = 0; s0 < nsteps; s0 += kHIt) {
+      const int nIt = min(kHIt, nsteps - s0);
+      {
+        const HalfEntry *__restrict__ hent = static_cast<const HalfEntry *>(entriesV);
+        const unsigned *__restrict__ hmask = static_cast<const unsigned *>(masksV);
+        const int nh = min(2 * kHIt, ne - 2 * s0);
+        if (lane < nh) {
+          const HalfEntry he = hent[e0 + 2 * s0 + lane];
+          const unsigned m = hmask[e0 + 2 * s0 + lane];
+          const int k = lane >> 1, side = lane & 1;
+          float *sh = S.sh[k];
+          int *js = reinterpret_cast<int *>(&S.js[k]);
+          unsigned *mk = reinterpret_cast<unsigned *>(&S.mk[k]);
+          sh[side] = he.sx;
+          sh[2 + side] = he.sy;
+          sh[4 + side] = he.sz;
+          js[side] = he.jh * 4;
+          mk[side] = m;
+          if (side == 0 && lane == nh - 1) {  // a last half without a partner
+            sh[1] = he.sx;
+            sh[3] = he.sy;
+            sh[5] = he.sz;
+            js[1] = he.jh * 4;
+            mk[1] = 0u;
+          }
+        }
+      }
+      __syncwarp();
+      {
+        const int k = lane >> 2, a = lane & 3;
+        if (k < nIt) {
+          const int2 js = S.js[k];
+          const float4 sxy = *reinterpret_cast<const float4 *>(S.sh[k]);
+          const float2 sz = *reinterpret_cast<const float2 *>(S.sh[k] + 4);
+          const float4 xa = xq[js.x + a], xb = xq[js.y + a];
+          const float2 la = lj[js.x + a], lb = lj[js.y + a];
+          const float ax = xa.x + sxy.x, bx = xb.x + sxy.y, ay = xa.y + sxy.z, by = xb.y + sxy.w;
+          const float az = xa.z + sz.x, bz = xb.z + sz.y;
+          float4 *d = &S.jd[0][(k * 4 + a) * 3];
+          d[0] = make_float4(ax, bx, ay, by);
+          d[1] = make_float4(az, bz, xa.w, xb.w);
+          d[2] = make_float4(la.x, lb.x, la.y, lb.y);
+          float4 *e = &S.jd[1][(k * 4 + a) * 3];
+          e[0] = make_float4(bx, ax, by, ay);
+          e[1] = make_float4(bz, az, xb.w, xa.w);
+          e[2] = make_float4(lb.x, la.x, lb.y, la.y);
+          if (a == 0) {
+            const uint2 mk = S.mk[k];
+            S.mj[0][k] = make_int4((int)mk.x, (int)mk.y, js.x, js.y);
+            S.mj[1][k] = make_int4((int)mk.y, (int)mk.x, js.y, js.x);
+          }
+        }
+      }
+      __syncwarp();
+      const float4 *__restrict__ jdl = S.jd[up ? 1 : 0];
+      const int4 *__restrict__ mjl = S.mj[up ? 1 : 0];
+      for (int k = 0; k < nIt; ++k) {
+        // this lane's two pairs: .x with the half it keeps in the reduction
+        const float4 p0 = jdl[(k * 4 + jl) * 3], p1 = jdl[(k * 4 + jl) * 3 + 1];
+        const int4 mj = mjl[k];
+        const uint2 mk = make_uint2((unsigned)mj.x, (unsigned)mj.y);
+        const float2 dx = __fadd2_rn(make_float2(p0.x, p0.y), nx);
+        const float2 dy = __fadd2_rn(make_float2(p0.z, p0.w), ny);
+        const float2 dz = __fadd2_rn(make_float2(p1.x, p1.y), nz);
+        const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        // EXACT: the inner list was written by the search from these same
+        // FP32 distances against this same rc^2, so its bits are the test
+        const bool ina = (mk.x & lanebit) && (EXACT || r2.x <= c.rc2);
+        const bool inb = (mk.y & lanebit) && (EXACT || r2.y <= c.rc2);
+        if (!EXACT) npair += (int)ina + (int)inb;
+        const float2 r2s = make_float2(ina ? r2.x : kFar, inb ? r2.y : kFar);
+        const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
+        const float2 rinv2 = __fmul2_rn(rinv, rinv);
+        const float2 r = __fmul2_rn(r2s, rinv);
+        const float2 qq = __fmul2_rn(f2(xi.w), make_float2(p1.z, p1.w));
+        const float2 targ = __ffma2_rn(f2(c.p_alpha), r, f2(1.0f));
+        const float2 t = make_float2(rcp_approx(targ.x), rcp_approx(targ.y));
+        const float2 earg = __fmul2_rn(f2(-c.c_ex), r2s);
+        const float2 ex = make_float2(ex2_approx(earg.x), ex2_approx(earg.y));
+        float2 poly = __ffma2_rn(f2(kErfcC7), t, f2(kErfcC6));
+        poly = __ffma2_rn(poly, t, f2(kErfcC5));
+        poly = __ffma2_rn(poly, t, f2(kErfcC4));
+        poly = __ffma2_rn(poly, t, f2(kErfcC3));
+        poly = __ffma2_rn(poly, t, f2(kErfcC2));
+        poly = __ffma2_rn(poly, t, f2(kErfcC1));
+        poly = __ffma2_rn(poly, t, f2(kErfcC0));
+        const float2 w = __ffma2_rn(__fmul2_rn(rinv, t), poly, f2(two_a));
+        const float2 qe = __fmul2_rn(qq, ex);
+        const float2 g = __fmul2_rn(qe, w);  // -r dE_c/dr
+        qs = __fadd2_rn(qs, qe);
+        gs = __fadd2_rn(gs, g);
+        float2 F = g;  // -(r dE/dr) while VDW adds to it below
+        if (VDW) {
+          const float4 lp = jdl[(k * 4 + jl) * 3 + 2];
+          const float2 eps = __fmul2_rn(f2(li.x), make_float2(lp.x, lp.y));
+          const float2 sg = __fadd2_rn(f2(li.y), make_float2(lp.z, lp.w));
+          const float2 s2 = __fmul2_rn(__fmul2_rn(sg, sg), rinv2);
+          const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+          const float2 s12 = __fmul2_rn(s6, s6);
+          const float2 a = __ffma2_rn(s6, f2(-1.0f), s12);  // s12 - s6
+          const float2 b = __fadd2_rn(a, s12);              // 2 s12 - s6
+          const float2 u0 = __fadd2_rn(r2s, f2(-c.ron2));
+          const float2 u = make_float2(fminf(fmaxf(u0.x, 0.f), c.sw_d),
+                                       fminf(fmaxf(u0.y, 0.f), c.sw_d));
+          const float2 m = __fmul2_rn(__fmul2_rn(u, u), __ffma2_rn(u, f2(-2.0f), f2(c.sw_3d)));
+          const float2 S6 = __ffma2_rn(m, f2(c.sw_6), f2(-6.0f));  // -6 S
+          const float2 dS = __fmul2_rn(__fmul2_rn(__ffma2_rn(u, f2(-1.0f), f2(c.sw_d)), u),
+                                       __fmul2_rn(r2s, f2(c.sw_m12)));  // r dS/dr
+          const float2 pv = __fmul2_rn(eps, a);
+          ev6 = __ffma2_rn(pv, S6, ev6);
+          const float2 hv = __fmul2_rn(eps, __ffma2_rn(a, dS, __fmul2_rn(b, S6)));  // r dE_v/dr
+          hs = __fadd2_rn(hs, hv);
+          F = __ffma2_rn(F, f2(-1.0f), hv);  // r dE/dr
+        } else {
+          F = __fmul2_rn(F, f2(-1.0f));
+        }
+        // F = r dE/dr: the force on i is F / r^2 (x_j - x_i)
+        const float2 Fr = __fmul2_rn(F, rinv2);
+        const float2 fx = __fmul2_rn(Fr, dx), fy = __fmul2_rn(Fr, dy), fz = __fmul2_rn(Fr, dz);
+        fi_x = __fadd2_rn(fi_x, fx);
+        fi_y = __fadd2_rn(fi_y, fy);
+        fi_z = __fadd2_rn(fi_z, fz);
+        // reduce-scatter of the two j atoms' forces over the 8 i lanes: every
+        // lane keeps its .x atom (half A for i atoms 0-3, B for 4-7) and
+        // passes its .y atom to the lane of i atom i ^ 4, which keeps it
+        float k0 = fx.x + __shfl_xor_sync(0xffffffffu, fx.y, 4);
+        float k1 = fy.x + __shfl_xor_sync(0xffffffffu, fy.y, 4);
+        float k2 = fz.x + __shfl_xor_sync(0xffffffffu, fz.y, 4);
+        const float t0 = mid ? k0 : k2, t1 = mid ? k1 : 0.f;
+        float u0 = mid ? k2 : k0, u1 = mid ? 0.f : k1;
+        u0 += __shfl_xor_sync(0xffffffffu, t0, 2);
+        u1 += __shfl_xor_sync(0xffffffffu, t1, 2);
+        const float wv = lo ? u0 : u1;
+        float v = lo ? u1 : u0;
+        v += __shfl_xor_sync(0xffffffffu, wv, 1);
+        const bool put = comp < 3 && v != 0.f;
+        vmax = fmaxf(vmax, fabsf(v));
+        red_add_if(put, fcomp + mj.z + jl, fix_f(-v));
+      }
+      __syncwarp();
+    }
+    // i forces: the lane's two pairs, then the four j lanes of each i atom
+    float fix = fi_x.x + fi_x.y, fiy = fi_y.x + fi_y.y, fiz = fi_z.x + fi_z.y;
+    fix += __shfl_xor_sync(0xffffffffu, fix, 8);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 8);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 8);
+    fix += __shfl_xor_sync(0xffffffffu, fix, 16);
+    fiy += __shfl_xor_sync(0xffffffffu, fiy, 16);
+    fiz += __shfl_xor_sync(0xffffffffu, fiz, 16);
+    if (jl < 3) {
+      const float v = (jl == 0) ? fix : (jl == 1 ? fiy : fiz);
+      if (v != 0.f) {
+        overflow |= !(fabsf(v) < kForceLimitF);
+        red_add(facc + (size_t)jl * fstride + ci * kClusterSize + il, fix_f(v));
+      }
+    }
+    // each lane's share of the item in fixed point on its own
+    const double gsum = (double)gs.x + (double)gs.y;
+    esum[0][threadIdx.x] += fix_e(gsum - (double)two_a * ((double)qs.x + (double)qs.y));
+    esum[1][threadIdx.x] += fix_e(((double)ev6.x + (double)ev6.y) * (-1.0 / 6.0));
+    esum[2][threadIdx.x] += fix_e(-gsum);
+    esum[3][threadIdx.x] += fix_e((double)hs.x + (double)hs.y);
+  }
+  long long Ec = esum[0][threadIdx.x], Ev = esum[1][threadIdx.x], Vc = esum[2][threadIdx.x],
+            Vv = esum[3][threadIdx.x];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Ec += __shfl_xor_sync(0xffffffffu, Ec, o);
+    Ev += __shfl_xor_sync(0xffffffffu, Ev, o);
+    Vc += __shfl_xor_sync(0xffffffffu, Vc, o);
+    Vv += __shfl_xor_sync(0xffffffffu, Vv, o);
+    if (!EXACT) npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  }
+  overflow |= comp < 3 && !(vmax < kForceLimitF);
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    // EXACT: the pairs were counted by the search (inner-list counter 4)
+    if (EXACT) {
+      if (gw == 0) red_add(acc + ACC_NPAIR, counters[4]);
+    } else {
+      red_add(acc + ACC_NPAIR, (long long)npair);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Quarter-cluster kernel (kPairQuad).  Units of 4 x 4 atoms: an i-cluster
+// half (i atoms 4 ih .. 4 ih + 3) against a j-cluster half.  The kernel reads
+// the same inner list as k_pair_half (halves with 32-bit masks, bit i + 8 k)
+// and splits each half's mask into its two i halves; a unit is kept when its
+// 16 bits hold a pair, which drops the i half that lies out of reach (pair
+// efficiency of water at rc = 12 A: ~0.57 against ~0.49 for 8 x 4).  One warp
+// runs one work item in two passes, i half 0 then 1; per pass the item's
+// halves are compacted (ballot) into the units of that i half, and each
+// warp step computes four units: lane L owns i atom a = L % 4 of the pass's
+// i half, j atom k = (L / 4) % 4 of units 2p and 2p + 1 (p = L / 16) in the
+// .x and .y lanes of packed f32x2 arithmetic.  Same arithmetic as
+// k_pair_half.  j forces: reduce-scatter over the four i lanes (xor 2 with
+// the swapped staging order making it select-free, then xor 1), two
+// fixed-point additions per lane and step; i forces once per pass.
+// ---------------------------------------------------------------------------
+constexpr int kQIt = 8;     // steps per staged chunk (32 units)
+constexpr int kQWarps = 4;  // warps per block (6.9 KB of staging each)
+struct QuadStage {
+  float4 jd[2][kQIt * 2 * 4 * 3];  // [order][(step * 2 + p) * 4 + k][3]
+  int4 mj[2][kQIt * 2];            // [order][step * 2 + p]: masks of units .x, .y; first slots
+  HalfEntry ue[32];                // the pass's units: their half entries
+  unsigned um[32];                 // their masks, bit a + 8 k
+};
+
+template <bool VDW, bool EXACT>
+__global__ void __launch_bounds__(kQWarps * 32, 6)
+k_pair_quad(const long long *__restrict__ counters, const int4 *__restrict__ items,
+            const HalfEntry *__restrict__ hent, const unsigned *__restrict__ hmask,
+            const float4 *__restrict__ xq, const float2 *__restrict__ lj, PairConstF c,
+            long long *__restrict__ facc, int fstride, long long *__restrict__ acc) {
+  __shared__ __align__(16) QuadStage stage[kQWarps];
+  QuadStage &S = stage[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int a = lane & 3, k = (lane >> 2) & 3, p = lane >> 4;
+  const int ord = a >> 1;          // lanes a >= 2 read the swapped order
+  const bool odd = a & 1;
+  const int sb = a + 8 * k;        // this lane's bit in a unit mask
+  const long long nItems = counters[1];
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  long long *f0 = facc + (size_t)(odd ? 2 : 0) * fstride;  // first addition: x (even) or z (odd)
+  long long *f1 = facc + (size_t)fstride;                  // second (even lanes): y
+  const float two_a = c.two_a_sqrtpi;
+  long long Ec = 0, Ev = 0, Vc = 0, Vv = 0;
+  int npair = 0;
+  bool overflow = false;
+
+  for (long long it = gw; it < nItems; it += nw) {
+    const int4 item = items[it];
+    const int ci = item.x, e0 = item.y, ne = item.z;
+    for (int ih = 0; ih < 2; ++ih) {
+      const int islot = ci * kClusterSize + 4 * ih + a;
+      const float4 xi = xq[islot];
+      const float2 li = lj[islot];
+      const float2 nx = f2(-xi.x), ny = f2(-xi.y), nz = f2(-xi.z);
+      float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
+      float2 ec = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
+      for (int h0 = 0; h0 < ne; h0 += 32) {
+        // the units of this i half among the next 32 halves
+        unsigned mu = 0u;
+        HalfEntry he{};
+        if (h0 + lane < ne) {
+          he = hent[e0 + h0 + lane];
+          mu = (hmask[e0 + h0 + lane] >> (4 * ih)) & 0x0f0f0f0fu;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, mu != 0u);
+        const int nU = __popc(bal);
+        if (mu != 0u) {
+          const int pos = __popc(bal & ((1u << lane) - 1u));
+          S.ue[pos] = he;
+          S.um[pos] = mu;
+        }
+        __syncwarp();
+        const int nSteps = (nU + 3) >> 2;
+        // stage: tuple t = (step, p, k), two per lane
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const int t = lane + 32 * r;
+          const int st = t >> 3, pp = (t >> 2) & 1, kk = t & 3;
+          const int ua = 4 * st + 2 * pp, ub = ua + 1;
+          if (st < nSteps) {
+            const bool va = ua < nU, vb = ub < nU;
+            const HalfEntry ea = S.ue[va ? ua : 0];
+            const HalfEntry eb = S.ue[vb ? ub : (va ? ua : 0)];
+            const float4 xa = xq[ea.jh * 4 + kk], xb = xq[eb.jh * 4 + kk];
+            const float2 la = lj[ea.jh * 4 + kk], lb = lj[eb.jh * 4 + kk];
+            const float ax = xa.x + ea.sx, bx = xb.x + eb.sx, ay = xa.y + ea.sy,
+                        by = xb.y + eb.sy, az = xa.z + ea.sz, bz = xb.z + eb.sz;
+            const int q = ((st * 2 + pp) * 4 + kk) * 3;
+            float4 *d = &S.jd[0][q];
+            d[0] = make_float4(ax, bx, ay, by);
+            d[1] = make_float4(az, bz, xa.w, xb.w);
+            d[2] = make_float4(la.x, lb.x, la.y, lb.y);
+            float4 *e = &S.jd[1][q];
+            e[0] = make_float4(bx, ax, by, ay);
+            e[1] = make_float4(bz, az, xb.w, xa.w);
+            e[2] = make_float4(lb.x, la.x, lb.y, la.y);
+            if (kk == 0) {
+              const int ma = va ? (int)S.um[ua] : 0, mb = vb ? (int)S.um[ub] : 0;
+              S.mj[0][st * 2 + pp] = make_int4(ma, mb, ea.jh * 4, eb.jh * 4);
+              S.mj[1][st * 2 + pp] = make_int4(mb, ma, eb.jh * 4, ea.jh * 4);
+            }
+          }
+        }
+        __syncwarp();
+        const float4 *__restrict__ jdl = S.jd[ord];
+        const int4 *__restrict__ mjl = S.mj[ord];
+        for (int st = 0; st < nSteps; ++st) {
+          const int q = ((st * 2 + p) * 4 + k) * 3;
+          const float4 p0 = jdl[q], p1 = jdl[q + 1];
+          const int4 mj = mjl[st * 2 + p];
+          const float2 dx = __fadd2_rn(make_float2(p0.x, p0.y), nx);
+          const float2 dy = __fadd2_rn(make_float2(p0.z, p0.w), ny);
+          const float2 dz = __fadd2_rn(make_float2(p1.x, p1.y), nz);
+          const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+          const bool ina = ((unsigned)mj.x >> sb) & 1u && (EXACT || r2.x <= c.rc2);
+          const bool inb = ((unsigned)mj.y >> sb) & 1u && (EXACT || r2.y <= c.rc2);
+          if (!EXACT) {
+            if (ina) ++npair;
+            if (inb) ++npair;
+          }
+          const float2 r2s = make_float2(ina ? r2.x : 1.0f, inb ? r2.y : 1.0f);
+          const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
+          const float2 rinv2 = __fmul2_rn(rinv, rinv);
+          const float2 r = __fmul2_rn(r2s, rinv);
+          const float2 qq0 = __fmul2_rn(f2(xi.w), make_float2(p1.z, p1.w));
+          const float2 qq = make_float2(ina ? qq0.x : 0.f, inb ? qq0.y : 0.f);
+          const float2 targ = __ffma2_rn(f2(c.p_alpha), r, f2(1.0f));
+          const float2 t = make_float2(rcp_approx(targ.x), rcp_approx(targ.y));
+          const float2 earg = __fmul2_rn(f2(-c.c_ex), r2s);
+          const float2 ex = make_float2(ex2_approx(earg.x), ex2_approx(earg.y));
+          float2 poly = __ffma2_rn(f2(kErfcC7), t, f2(kErfcC6));
+          poly = __ffma2_rn(poly, t, f2(kErfcC5));
+          poly = __ffma2_rn(poly, t, f2(kErfcC4));
+          poly = __ffma2_rn(poly, t, f2(kErfcC3));
+          poly = __ffma2_rn(poly, t, f2(kErfcC2));
+          poly = __ffma2_rn(poly, t, f2(kErfcC1));
+          poly = __ffma2_rn(poly, t, f2(kErfcC0));
+          const float2 w = __ffma2_rn(__fmul2_rn(rinv, t), poly, f2(two_a));
+          const float2 qe = __fmul2_rn(qq, ex);
+          const float2 g = __fmul2_rn(qe, w);  // -r dE_c/dr
+          ec = __fadd2_rn(ec, __ffma2_rn(qe, f2(-two_a), g));
+          gs = __fadd2_rn(gs, g);
+          float2 F = g;
+          if (VDW) {
+            const float4 lp = jdl[q + 2];
+            const float2 eps0 = __fmul2_rn(f2(li.x), make_float2(lp.x, lp.y));
+            const float2 eps = make_float2(ina ? eps0.x : 0.f, inb ? eps0.y : 0.f);
+            const float2 sg = __fadd2_rn(f2(li.y), make_float2(lp.z, lp.w));
+            const float2 s2 = __fmul2_rn(__fmul2_rn(sg, sg), rinv2);
+            const float2 s6 = __fmul2_rn(__fmul2_rn(s2, s2), s2);
+            const float2 s12 = __fmul2_rn(s6, s6);
+            const float2 av = __ffma2_rn(s6, f2(-1.0f), s12);  // s12 - s6
+            const float2 bv = __fadd2_rn(av, s12);              // 2 s12 - s6
+            const float2 u0 = __fadd2_rn(r2s, f2(-c.ron2));
+            const float2 u = make_float2(fmaxf(u0.x, 0.f), fmaxf(u0.y, 0.f));
+            const float2 m = __fmul2_rn(__fmul2_rn(u, u), __ffma2_rn(u, f2(-2.0f), f2(c.sw_3d)));
+            const float2 S6 = __ffma2_rn(m, f2(c.sw_6), f2(-6.0f));  // -6 S
+            const float2 dS = __fmul2_rn(__fmul2_rn(__ffma2_rn(u, f2(-1.0f), f2(c.sw_d)), u),
+                                         __fmul2_rn(r2s, f2(c.sw_m12)));  // r dS/dr
+            const float2 pv = __fmul2_rn(eps, av);
+            ev6 = __ffma2_rn(pv, S6, ev6);
+            const float2 hv = __fmul2_rn(eps, __ffma2_rn(av, dS, __fmul2_rn(bv, S6)));
+            hs = __fadd2_rn(hs, hv);
+            F = __ffma2_rn(F, f2(-1.0f), hv);  // r dE/dr
+          } else {
+            F = __fmul2_rn(F, f2(-1.0f));
+          }
+          const float2 Fr = __fmul2_rn(F, rinv2);
+          const float2 fx = __fmul2_rn(Fr, dx), fy = __fmul2_rn(Fr, dy), fz = __fmul2_rn(Fr, dz);
+          fi_x = __fadd2_rn(fi_x, fx);
+          fi_y = __fadd2_rn(fi_y, fy);
+          fi_z = __fadd2_rn(fi_z, fz);
+          // j forces over the four i lanes: keep .x, pass .y to lane a ^ 2
+          // (which keeps that unit), then x, y to the even and z to the odd
+          // lane of each pair
+          const float k0 = fx.x + __shfl_xor_sync(0xffffffffu, fx.y, 2);
+          const float k1 = fy.x + __shfl_xor_sync(0xffffffffu, fy.y, 2);
+          const float k2 = fz.x + __shfl_xor_sync(0xffffffffu, fz.y, 2);
+          const float v0 = (odd ? k2 : k0) + __shfl_xor_sync(0xffffffffu, odd ? k0 : k2, 1);
+          const float v1 = k1 + __shfl_xor_sync(0xffffffffu, k1, 1);
+          const int js = mj.z + k;
+          const bool put0 = v0 != 0.f, put1 = !odd && v1 != 0.f;
+          overflow |= (put0 && !(fabsf(v0) < kForceLimitF)) || (put1 && !(fabsf(v1) < kForceLimitF));
+          red_add_if(put0, f0 + js, fix_f(-v0));
+          red_add_if(put1, f1 + js, fix_f(-v1));
+        }
+        __syncwarp();
+      }
+      // i forces of the pass: the lane's two units, then the eight lanes of
+      // each i atom
+      float fix = fi_x.x + fi_x.y, fiy = fi_y.x + fi_y.y, fiz = fi_z.x + fi_z.y;
+#pragma unroll
+      for (int o = 4; o < 32; o <<= 1) {
+        fix += __shfl_xor_sync(0xffffffffu, fix, o);
+        fiy += __shfl_xor_sync(0xffffffffu, fiy, o);
+        fiz += __shfl_xor_sync(0xffffffffu, fiz, o);
+      }
+      if (p == 0 && k < 3) {
+        const float v = (k == 0) ? fix : (k == 1 ? fiy : fiz);
+        if (v != 0.f) {
+          overflow |= !(fabsf(v) < kForceLimitF);
+          red_add(facc + (size_t)k * fstride + islot, fix_f(v));
+        }
+      }
+      Ec += fix_e((double)ec.x + (double)ec.y);
+      Ev += fix_e(((double)ev6.x + (double)ev6.y) * (-1.0 / 6.0));
+      Vc += fix_e(-((double)gs.x + (double)gs.y));
+      Vv += fix_e((double)hs.x + (double)hs.y);
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    Ec += __shfl_xor_sync(0xffffffffu, Ec, o);
+    Ev += __shfl_xor_sync(0xffffffffu, Ev, o);
+    Vc += __shfl_xor_sync(0xffffffffu, Vc, o);
+    Vv += __shfl_xor_sync(0xffffffffu, Vv, o);
+    npair += __shfl_xor_sync(0xffffffffu, npair, o);
+  }
+  if (__any_sync(0xffffffffu, overflow) && lane == 0) raise_flag(acc, FLAG_OVERFLOW);
+  if (lane == 0) {
+    red_add(acc + ACC_E_DIR, Ec);
+    red_add(acc + ACC_E_VDW, Ev);
+    red_add(acc + ACC_V_DIR, Vc);
+    red_add(acc + ACC_V_VDW, Vv);
+    if (EXACT) {
+      if (gw == 0) red_add(acc + ACC_NPAIR, counters[4]);
+    } else {
+      red_add(acc + ACC_NPAIR, (long long)npair);
+    }
+  }
+}
+
 constexpr int kChunk = 8;    // entries per filter/compute chunk
 constexpr int kCWarps = 4;   // warps per block
 
@@ -1272,7 +1742,22 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
   const PairConstF c = make_pair_const(p);
   // the list the kernel walks: the built list or, during dynamics, its
   // pruned inner copy
-  if (variant == kPairHalf || variant == kPairHalf3) {
+  if (variant == kPairQuad && w.useInner) {
+    // the inner list written by the search at the kernel's own rc^2 (exact)
+    // or a pruned one at rc + buffer; fixed blocks of kQWarps warps, the
+    // same number of warps as grid x block
+    const bool ex = w.innerRin2 == c.rc2 && w.rin2 == 0.f;
+    auto kv = p.vdwSwitch ? (ex ? k_pair_quad<true, true> : k_pair_quad<true, false>)
+                          : (ex ? k_pair_quad<false, true> : k_pair_quad<false, false>);
+    const int qgrid = std::max(1, grid * block / (kQWarps * 32));
+    MDB_LAUNCH(kv, qgrid, kQWarps * 32, 0, s, w.countersIn.as<long long>(),
+               w.itemsIn.as<int4>(), w.entriesIn.as<HalfEntry>(), w.masksIn.as<unsigned>(),
+               w.xq.as<float4>(), w.lj.as<float2>(), c, w.facc.as<long long>(), w.slotCap,
+               w.acc.as<long long>());
+    return MDBAS_NB_OK;
+  }
+  if (variant == kPairHalf || variant == kPairHalf3 || variant == kPairQuad ||
+      variant == kPairHalfLean) {
     const bool in = w.useInner;
     // the inner list written by the search at the kernel's own rc^2
     const bool ex = in && w.innerRin2 == make_pair_const(p).rc2 && w.rin2 == 0.f;
@@ -1284,6 +1769,9 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
         kv = p.vdwSwitch ? k_pair_half<true, true, 3, false> : k_pair_half<false, true, 3, false>;
       else
         kv = p.vdwSwitch ? k_pair_half<true, false, 3, false> : k_pair_half<false, false, 3, false>;
+    } else if (in && variant == kPairHalfLean) {
+      kv = p.vdwSwitch ? (ex ? k_pair_half_lean<true, true> : k_pair_half_lean<true, false>)
+                       : (ex ? k_pair_half_lean<false, true> : k_pair_half_lean<false, false>);
     } else if (in && ex) {
       kv = p.vdwSwitch ? k_pair_half<true, true, 4, true> : k_pair_half<false, true, 4, true>;
     } else if (in) {

@@ -25,10 +25,12 @@ PairConstF make_pair_const(const PairParams &p);
 // by bulk copies) -- these four walk the full list -- and half (two 4-atom
 // j-cluster halves per warp step in f32x2 arithmetic over the inner list
 // while it is current, else over the full list; the default), half3 (the
-// same at up to 80 registers, three blocks of 256 threads per SM).
+// same at up to 80 registers, three blocks of 256 threads per SM), quad
+// (4 x 4 units: i-cluster halves against j-cluster halves of the inner list;
+// over the full list it runs as half).
 enum {
   kPairDense = 0, kPairCompact = 1, kPairPacked = 2, kPairBulk = 3, kPairHalf = 4,
-  kPairHalf3 = 5
+  kPairHalf3 = 5, kPairQuad = 6, kPairHalfLean = 7
 };
 // The pair kernel over all work items (grid-stride, item count read on the
 // device, so the launch needs no host synchronisation).  grid*block is the

@@ -473,9 +473,12 @@ class Engine:
         return int(lib().mdbas_nb_engine_launch_count(self.h))
 
     def set_variant(self, variant: int):
-        """Pair kernel: 4 = half clusters, packed f32x2, inner list (default),
-        2 = packed f32x2 8x8, staged, 0 = scalar dense 8x8, 1 = filtered and
-        compacted, 3 = packed with bulk-copy staging."""
+        """Pair kernel: 7 = half clusters (8-atom i x 4-atom j), packed
+        f32x2, inner list, lean form (default), 4 = the same in its first
+        form, 5 = that at 80 registers, 6 = quad
+        (4-atom i x 4-atom j units of the inner list), 2 = packed f32x2 8x8,
+        staged, 0 = scalar dense 8x8, 1 = filtered and compacted, 3 = packed
+        with bulk-copy staging."""
         check(lib().mdbas_nb_engine_set_variant(self.h, variant), "engine_set_variant")
 
     def set_timing(self, on: bool):
@@ -522,12 +525,13 @@ class Engine:
         and keep the fastest (call after build; recompute afterwards)."""
         out = (C.c_int * 4)()
         check(lib().mdbas_nb_engine_autotune(self.h, out), "engine_autotune")
-        # the variants differ in their cluster shapes: the half-cluster ones
-        # (4, 5) pair 8-atom i clusters with 4-atom j-cluster halves, the
-        # others 8-atom i with 8-atom j clusters
+        # the variants differ in their cluster shapes: the quad one (6) pairs
+        # 4-atom i-cluster halves with 4-atom j-cluster halves, the half ones
+        # (4, 5, 7) 8-atom i clusters with 4-atom j-cluster halves, the others
+        # 8-atom i with 8-atom j clusters
         return {"variant": out[0], "block": out[1], "blocks_per_sm": out[2],
-                "candidates": out[3], "i_cluster_atoms": 8,
-                "j_cluster_atoms": 4 if out[0] in (4, 5) else 8}
+                "candidates": out[3], "i_cluster_atoms": 4 if out[0] == 6 else 8,
+                "j_cluster_atoms": 4 if out[0] in (4, 5, 6, 7) else 8}
 
     def split(self, arrays):
         """Per-replica views of concatenated per-atom arrays."""

@@ -192,3 +192,77 @@ def test_pair_kernel_variants_agree(gpu):
     scale = abs(e0["elec_direct"] + e0["elec_corr"])
     assert abs(e1["elec_direct"] - e0["elec_direct"]) <= 1e-6 * scale
     eng.close()
+
+
+def test_quad_kernel_variants(gpu):
+    """The 4 x 4 kernel (i-cluster halves against j-cluster halves of the
+    inner list) gives the same pair count as the 8 x 4 half kernel and its
+    forces within FP32 rounding; repeated evaluations are bitwise
+    identical."""
+    s = systems.water_box_for_atoms(18558, 3)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    out = {}
+    for v in (4, 6):
+        eng.set_variant(v)
+        eng.compute()
+        out[v] = (eng.forces(), eng.energies())
+    eng.compute()
+    again = (eng.forces(), eng.energies())
+    for k in range(3):
+        assert np.array_equal(out[6][0][k], again[0][k])
+    assert out[6][1] == again[1]
+    assert out[6][1]["n_pairs"] == out[4][1]["n_pairs"]
+    assert force_rel_rms(out[6][0], out[4][0]) < 2e-6
+    e4, e6 = out[4][1], out[6][1]
+    scale = abs(e4["elec_direct"] + e4["elec_corr"])
+    assert abs(e6["elec_direct"] - e4["elec_direct"]) <= 1e-6 * scale
+    assert abs(e6["vdw"] - e4["vdw"]) <= 1e-6 * abs(e4["vdw"])
+    assert abs(e6["vir_direct"] - e4["vir_direct"]) <= 1e-6 * abs(e4["vir_direct"])
+    eng.close()
+
+
+def test_quad_kernel_in_pruned_dynamics(gpu):
+    """Dynamics with a pruned inner list (rc + 0.5 A, so the kernel tests
+    the cut-off itself) on the 4 x 4 kernel follow the 8 x 4 kernel's
+    trajectory to FP32 rounding."""
+    s = systems.water_box(1000, 31.0, seed=5, temperature=300.0)
+    rows = {}
+    pos = {}
+    for v in (4, 6):
+        e = nb.Engine(s, precision=1)
+        e.set_variant(v)
+        e.md_set_graph(0)
+        e.md_set_prune(0.5)
+        e.md_init(s.mass, (s.vx, s.vy, s.vz), time_step=0.002, list_update=0,
+                  constraints=s.water_constraints())
+        rows[v] = e.md_run(40, energy_every=1)
+        pos[v] = e.positions()
+        assert e.md_stats()["pruned_list"]
+        e.close()
+    err = max(np.max(np.abs(pos[4][k] - pos[6][k])) for k in range(3))
+    assert err < 5e-4, err
+    assert np.allclose(rows[4][:, 1:], rows[6][:, 1:], rtol=1e-6, atol=0.0)
+
+
+def test_lean_half_kernel_matches_half(gpu):
+    """The lean form of the half-cluster kernel (variant 7: masked pairs at
+    r^2 = 1e30 instead of zeroed products, Coulomb energy from two running
+    sums) gives the default kernel's forces bit for bit, the same LJ energy,
+    virials and pair count, and the Coulomb energy to FP32 summation order."""
+    s = systems.water_box_for_atoms(18558, 3)
+    eng = nb.Engine(s, precision=1)
+    eng.build()
+    out = {}
+    for v in (4, 7):
+        eng.set_variant(v)
+        eng.compute()
+        out[v] = (eng.forces(), eng.energies())
+    for k in range(3):
+        assert np.array_equal(out[4][0][k], out[7][0][k])
+    e4, e7 = out[4][1], out[7][1]
+    for k in ("vdw", "vir_direct", "vir_vdw", "n_pairs", "elec_corr"):
+        assert e4[k] == e7[k], k
+    scale = abs(e4["elec_direct"] + e4["elec_corr"])
+    assert abs(e7["elec_direct"] - e4["elec_direct"]) <= 1e-7 * scale
+    eng.close()
