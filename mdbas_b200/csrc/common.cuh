@@ -181,7 +181,10 @@ __device__ __forceinline__ void red_add_if(bool p, long long *addr, long long v)
 // Accumulator slots (int64, units 2^-24) of one evaluation.
 enum AccSlot {
   ACC_E_DIR = 0, ACC_E_CORR, ACC_E_VDW, ACC_V_DIR, ACC_V_CORR, ACC_V_VDW, ACC_NPAIR,
-  ACC_FLAGS, ACC_COUNT = 8
+  ACC_FLAGS,
+  ACC_WORK,       // work counter of kernels that hand out items dynamically (zeroed
+                  // with the accumulators before every evaluation)
+  ACC_COUNT = 9
 };
 // Bits of the device error word (ACC_FLAGS slot).
 enum DevFlag {

@@ -754,7 +754,15 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
   int npair = 0;
   bool overflow = false;
 
-  for (long long it = gw; it < nItems; it += nw) {
+  // items handed out by a counter, the next index fetched while the
+  // current item runs
+  unsigned long long *work = reinterpret_cast<unsigned long long *>(acc + ACC_WORK);
+  unsigned long long nxt = 0ull;
+  if (lane == 0) nxt = atomicAdd(work, 1ull);
+  long long it = (long long)__shfl_sync(0xffffffffu, nxt, 0);
+  (void)nw;
+  while (it < nItems) {
+    if (lane == 0) nxt = atomicAdd(work, 1ull);
     const int4 item = items[it];
     const int ci = item.x, e0 = item.y, ne = item.z;
     const int nsteps = INNER ? (ne + 1) >> 1 : ne;
@@ -939,6 +947,7 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
     Ev += fix_e(((double)ev6.x + (double)ev6.y) * (-1.0 / 6.0));
     Vc += fix_e(-((double)gs.x + (double)gs.y));
     Vv += fix_e((double)hs.x + (double)hs.y);
+    it = (long long)__shfl_sync(0xffffffffu, nxt, 0);
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
@@ -963,15 +972,15 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
   }
 }
 
-// Lean form of k_pair_half over the exact inner list (the default): the same
-// pairs and arithmetic with fewer instructions and registers per step --
-// pairs outside the mask get r^2 = 1e30 instead of zeroed charge and LJ
-// products (their terms vanish: exp underflows to 0, the LJ powers to 0, the
-// switch variable is clamped at D so S and dS stay finite), the Coulomb
-// energy is summed as sum g - (2 alpha / sqrt pi) sum q q e^{-(alpha r)^2},
-// per step only the largest |j force| is kept for the range check (a NaN
-// shows up in the i forces, checked per item), and the per-lane 64-bit
-// energy sums live in shared memory.
+// Lean form of k_pair_half over the inner list (exact, or pruned with the
+// cut-off tested here; the default): the same pairs and arithmetic with fewer
+// instructions and registers per step -- pairs outside the mask get
+// r^2 = 1e30 instead of zeroed charge and LJ products (their terms vanish:
+// exp underflows to 0, the LJ powers to 0, the switch variable is clamped at
+// D so S and dS stay finite), per step only the largest |j force| is kept
+// for the range check (a NaN shows up in the i forces, checked per item),
+// the per-lane 64-bit energy sums live in shared memory, and warps take items
+// from a counter.  Forces and energies equal k_pair_half's bit for bit.
 template <bool VDW, bool EXACT>
 __global__ void __launch_bounds__(256, 4)
 k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict__ items,
@@ -1001,7 +1010,17 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
   bool overflow = false;
   float vmax = 0.f;
 
-  for (long long it = gw; it < nItems; it += nw) {
+  // items handed out by a counter (each warp takes the next one when it is
+  // done, the following index fetched while the current item runs), so no
+  // warp is left with a long tail of large items
+  unsigned long long *work = reinterpret_cast<unsigned long long *>(acc + ACC_WORK);
+  unsigned long long nxt = 0ull;
+  if (lane == 0) nxt = atomicAdd(work, 1ull);
+  long long it = (long long)__shfl_sync(0xffffffffu, nxt, 0);
+  (void)gw;
+  (void)nw;
+  while (it < nItems) {
+    if (lane == 0) nxt = atomicAdd(work, 1ull);
     const int4 item = items[it];
     const int ci = item.x, e0 = item.y, ne = item.z;
     const int nsteps = INNER ? (ne + 1) >> 1 : ne;
@@ -1009,7 +1028,7 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
     const float2 li = lj[ci * kClusterSize + il];
     const float2 nx = f2(-xi.x), ny = f2(-xi.y), nz = f2(-xi.z);
     float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
-    float2 qs = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
+    float2 ec = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
     for (int s0 = 0; s0 < nsteps; s0 += kHIt) {
       const int nIt = min(kHIt, nsteps - s0);
       {
@@ -1099,7 +1118,7 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
         const float2 w = __ffma2_rn(__fmul2_rn(rinv, t), poly, f2(two_a));
         const float2 qe = __fmul2_rn(qq, ex);
         const float2 g = __fmul2_rn(qe, w);  // -r dE_c/dr
-        qs = __fadd2_rn(qs, qe);
+        ec = __fadd2_rn(ec, __ffma2_rn(qe, f2(-two_a), g));
         gs = __fadd2_rn(gs, g);
         float2 F = g;  // -(r dE/dr) while VDW adds to it below
         if (VDW) {
@@ -1167,11 +1186,11 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
       }
     }
     // each lane's share of the item in fixed point on its own
-    const double gsum = (double)gs.x + (double)gs.y;
-    esum[0][threadIdx.x] += fix_e(gsum - (double)two_a * ((double)qs.x + (double)qs.y));
+    esum[0][threadIdx.x] += fix_e((double)ec.x + (double)ec.y);
     esum[1][threadIdx.x] += fix_e(((double)ev6.x + (double)ev6.y) * (-1.0 / 6.0));
-    esum[2][threadIdx.x] += fix_e(-gsum);
+    esum[2][threadIdx.x] += fix_e(-((double)gs.x + (double)gs.y));
     esum[3][threadIdx.x] += fix_e((double)hs.x + (double)hs.y);
+    it = (long long)__shfl_sync(0xffffffffu, nxt, 0);
   }
   long long Ec = esum[0][threadIdx.x], Ev = esum[1][threadIdx.x], Vc = esum[2][threadIdx.x],
             Vv = esum[3][threadIdx.x];

@@ -247,9 +247,8 @@ def test_quad_kernel_in_pruned_dynamics(gpu):
 
 def test_lean_half_kernel_matches_half(gpu):
     """The lean form of the half-cluster kernel (variant 7: masked pairs at
-    r^2 = 1e30 instead of zeroed products, Coulomb energy from two running
-    sums) gives the default kernel's forces bit for bit, the same LJ energy,
-    virials and pair count, and the Coulomb energy to FP32 summation order."""
+    r^2 = 1e30 instead of zeroed products, items from a counter) gives the
+    first form's forces and energies bit for bit."""
     s = systems.water_box_for_atoms(18558, 3)
     eng = nb.Engine(s, precision=1)
     eng.build()
@@ -260,9 +259,5 @@ def test_lean_half_kernel_matches_half(gpu):
         out[v] = (eng.forces(), eng.energies())
     for k in range(3):
         assert np.array_equal(out[4][0][k], out[7][0][k])
-    e4, e7 = out[4][1], out[7][1]
-    for k in ("vdw", "vir_direct", "vir_vdw", "n_pairs", "elec_corr"):
-        assert e4[k] == e7[k], k
-    scale = abs(e4["elec_direct"] + e4["elec_corr"])
-    assert abs(e7["elec_direct"] - e4["elec_direct"]) <= 1e-7 * scale
+    assert out[4][1] == out[7][1]
     eng.close()
