@@ -84,7 +84,7 @@ def _parse():
                         "list build + 4 force evaluations, 'md' = --md-steps dynamics steps "
                         "driven from the host (a profiler sees no kernels inside graphs with "
                         "conditional nodes)")
-    p.add_argument("--variant", type=int, default=4, help="pair kernel variant of --case pair")
+    p.add_argument("--variant", type=int, default=7, help="pair kernel variant of --case pair")
     p.add_argument("--dropin-steps", type=int, default=10,
                    help="steps of the drop-in e2e leg (0 skips it)")
     p.add_argument("--decomp", choices=["replicas", "slab"], default="replicas",

@@ -71,15 +71,67 @@ __global__ void k_col_bin(int n, const ClusterGeom *__restrict__ geoms,
   if ((threadIdx.x & 31) == __ffs(same) - 1) atomicAdd(colCount + col, __popc(same));
 }
 
-__global__ void k_col_pad(int nCols, const int *__restrict__ colCount, int *__restrict__ colPad) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < nCols) colPad[c] = (colCount[c] + kClusterSize - 1) & ~(kClusterSize - 1);
-}
-
-__global__ void k_col_clstart(int nCols, const int *__restrict__ colPadStart,
-                              int *__restrict__ colClStart) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c <= nCols) colClStart[c] = colPadStart[c] / kClusterSize;
+// Column offsets in one block of 1,024 threads (the grid has at most a few
+// tens of thousands of columns): colStart = exclusive scan of the atom
+// counts, colPadStart = exclusive scan of the counts padded to whole
+// clusters, colClStart = colPadStart / 8, each with its total at index nCols.
+// One launch instead of two multi-kernel scans and two small kernels.
+__global__ void __launch_bounds__(1024)
+k_col_scan(int nCols, const int *__restrict__ colCount, int *__restrict__ colStart,
+           int *__restrict__ colPadStart, int *__restrict__ colClStart) {
+  __shared__ int wsum[2][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int run0 = 0, run1 = 0;  // totals of the chunks before this one
+  for (int c0 = 0; c0 < nCols; c0 += 1024) {
+    const int c = c0 + threadIdx.x;
+    const int v0 = c < nCols ? colCount[c] : 0;
+    const int v1 = (v0 + kClusterSize - 1) & ~(kClusterSize - 1);
+    int x0 = v0, x1 = v1;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y0 = __shfl_up_sync(0xffffffffu, x0, o);
+      const int y1 = __shfl_up_sync(0xffffffffu, x1, o);
+      if (lane >= o) {
+        x0 += y0;
+        x1 += y1;
+      }
+    }
+    if (lane == 31) {
+      wsum[0][warp] = x0;
+      wsum[1][warp] = x1;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      int t0 = wsum[0][lane], t1 = wsum[1][lane];
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y0 = __shfl_up_sync(0xffffffffu, t0, o);
+        const int y1 = __shfl_up_sync(0xffffffffu, t1, o);
+        if (lane >= o) {
+          t0 += y0;
+          t1 += y1;
+        }
+      }
+      wsum[0][lane] = t0;
+      wsum[1][lane] = t1;
+    }
+    __syncthreads();
+    const int e0 = run0 + x0 - v0 + (warp > 0 ? wsum[0][warp - 1] : 0);
+    const int e1 = run1 + x1 - v1 + (warp > 0 ? wsum[1][warp - 1] : 0);
+    if (c < nCols) {
+      colStart[c] = e0;
+      colPadStart[c] = e1;
+      colClStart[c] = e1 / kClusterSize;
+    }
+    run0 += wsum[0][31];
+    run1 += wsum[1][31];
+    __syncthreads();  // wsum is rewritten by the next chunk
+  }
+  if (threadIdx.x == 0) {
+    colStart[nCols] = run0;
+    colPadStart[nCols] = run1;
+    colClStart[nCols] = run1 / kClusterSize;
+  }
 }
 
 __global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
@@ -1096,14 +1148,12 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     MDB_TRY(w.colCount.ensure(sizeof(int) * (nCols + 1)));
     MDB_TRY(w.colFill.ensure(sizeof(int) * (nCols + 1)));
     MDB_TRY(w.colStart.ensure(sizeof(int) * (nCols + 2)));
-    MDB_TRY(w.colPad.ensure(sizeof(int) * (nCols + 1)));
     MDB_TRY(w.colPadStart.ensure(sizeof(int) * (nCols + 2)));
     MDB_TRY(w.colClStart.ensure(sizeof(int) * (nCols + 2)));
     MDB_TRY(w.atomCol.ensure(sizeof(int) * n));
     MDB_TRY(w.atomZ.ensure(sizeof(double) * n));
     MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
     MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
-    MDB_TRY(w.scanTmp.ensure(scan_tmp_bytes(std::max(n, nCols) + 1)));
     MDB_TRY(w.counters.ensure(sizeof(long long) * 8));
     MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
     if (!w.sticky.p) {
@@ -1138,12 +1188,8 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
              w.colRank.as<int>(), x, y, z, w.atomCol.as<int>(), w.atomZ.as<double>(),
              w.colCount.as<int>(), w.counters.as<long long>());
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[1], s));
-  MDB_TRY(exclusive_scan32(w.colCount.as<int>(), w.colStart.as<int>(), nCols, w.scanTmp.p, s));
-  MDB_LAUNCH(k_col_pad, grid_for(nCols, 256), 256, 0, s, nCols, w.colCount.as<int>(),
-             w.colPad.as<int>());
-  MDB_TRY(exclusive_scan32(w.colPad.as<int>(), w.colPadStart.as<int>(), nCols, w.scanTmp.p, s));
-  MDB_LAUNCH(k_col_clstart, grid_for(nCols + 1, 256), 256, 0, s, nCols, w.colPadStart.as<int>(),
-             w.colClStart.as<int>());
+  MDB_LAUNCH(k_col_scan, 1, 1024, 0, s, nCols, w.colCount.as<int>(), w.colStart.as<int>(),
+             w.colPadStart.as<int>(), w.colClStart.as<int>());
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[2], s));
   MDB_LAUNCH(k_col_scatter, grid_for(n, 256), 256, 0, s, n, w.atomCol.as<int>(),
              w.colStart.as<int>(), w.colFill.as<int>(), w.tmpIdx.as<int>());

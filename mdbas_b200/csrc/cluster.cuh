@@ -67,10 +67,9 @@ struct ClusterWork {
   int nCols = 0;      // columns of all replicas
   DBuf colRank;       // colOff[r] + (cy*ncx+cx) -> global column, Morton order inside r
   DBuf colXY;         // global column -> cx | cy << 16
-  DBuf colCount, colFill, colStart, colPad, colPadStart;
+  DBuf colCount, colFill, colStart, colPadStart;
   DBuf atomCol, tmpIdx;
   DBuf atomZ;         // wrapped fractional z (FP64)
-  DBuf scanTmp;
   // layout.  Slot-indexed buffers hold slotCap = n + 7 * nCols slots (rounded
   // up to a whole cluster), the most that per-column padding can produce, so
   // a rebuild never reallocates and kernels read the actual count on the

@@ -128,7 +128,10 @@ struct Ctx {
   DevBox clBox{};
   int elecType = FULL, vdwType = VSWITCH;
   bool ptrsSet = false;
-  std::vector<double> hf;  // force download buffer
+  // page-locked staging for the positions going up and the forces coming
+  // down (the caller's arrays are pageable), grown on demand
+  double *pinIn = nullptr, *pinOut = nullptr;
+  size_t pinInCap = 0, pinOutCap = 0;
 };
 
 Ctx g;
@@ -149,13 +152,33 @@ bool resident_enabled() {
   return !(v && v[0] == '0');
 }
 
+// Page-locked host buffer of at least `count` doubles.  Every call that uses
+// one ends with a stream synchronisation, so a buffer is never refilled while
+// a copy from or into it is in flight.
+int pinned(double *&buf, size_t &cap, size_t count) {
+  if (cap >= count && buf) return MDBAS_NB_OK;
+  if (buf) cudaFreeHost(buf);
+  buf = nullptr;
+  cap = 0;
+  MDB_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&buf), sizeof(double) * count,
+                         cudaHostAllocDefault));
+  cap = count;
+  return MDBAS_NB_OK;
+}
+
 int upload_positions(int n, const double *x, const double *y, const double *z) {
   ST_TRY(g.x.ensure(sizeof(double) * n));
   ST_TRY(g.y.ensure(sizeof(double) * n));
   ST_TRY(g.z.ensure(sizeof(double) * n));
-  MDB_CUDA(cudaMemcpyAsync(g.x.p, x, sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
-  MDB_CUDA(cudaMemcpyAsync(g.y.p, y, sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
-  MDB_CUDA(cudaMemcpyAsync(g.z.p, z, sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
+  ST_TRY(pinned(g.pinIn, g.pinInCap, 3 * (size_t)n));
+  double *h = g.pinIn;
+  memcpy(h, x, sizeof(double) * n);
+  memcpy(h + n, y, sizeof(double) * n);
+  memcpy(h + 2 * (size_t)n, z, sizeof(double) * n);
+  MDB_CUDA(cudaMemcpyAsync(g.x.p, h, sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
+  MDB_CUDA(cudaMemcpyAsync(g.y.p, h + n, sizeof(double) * n, cudaMemcpyHostToDevice, g.s));
+  MDB_CUDA(cudaMemcpyAsync(g.z.p, h + 2 * (size_t)n, sizeof(double) * n,
+                           cudaMemcpyHostToDevice, g.s));
   return MDBAS_NB_OK;
 }
 
@@ -178,6 +201,28 @@ int upload_params(int n, const double *q, const double *eps, const double *sig) 
 
 // MDBas exclusion rows (exclList[i][0..exclPair[i]-1]) -> device CSR.
 int upload_exclusions(int n, int **exclList, const int *exclPair) {
+  // rows as last uploaded (MDBas builds them once per run): compared in place
+  if (g.exclStart.p && (int)g.hExclStart.size() == n + 1) {
+    bool same = true;
+    if (exclPair) {
+      for (int i = 0; i < n && same; ++i) {
+        const int s0 = g.hExclStart[i], c = exclPair[i];
+        if (g.hExclStart[i + 1] - s0 != c) {
+          same = false;
+          break;
+        }
+        const int *row = exclList[i];
+        for (int k = 0; k < c; ++k)
+          if (row[k] != g.hExclFlat[s0 + k]) {
+            same = false;
+            break;
+          }
+      }
+    } else {
+      same = g.hExclStart[n] == 0;
+    }
+    if (same) return MDBAS_NB_OK;
+  }
   std::vector<int> start(n + 1, 0), flat;
   if (exclPair) {
     for (int i = 0; i < n; ++i) start[i + 1] = start[i] + exclPair[i];
@@ -361,11 +406,11 @@ int ensure_list_on_device(int n, const int *neighList, const int *neighPair,
 
 // Download device forces and add them into the caller's arrays.
 int add_forces(int n, const double *dsrc, double *fx, double *fy, double *fz) {
-  g.hf.resize(3 * (size_t)n);
-  MDB_CUDA(cudaMemcpyAsync(g.hf.data(), dsrc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
+  ST_TRY(pinned(g.pinOut, g.pinOutCap, 3 * (size_t)n));
+  MDB_CUDA(cudaMemcpyAsync(g.pinOut, dsrc, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost,
                            g.s));
   MDB_CUDA(cudaStreamSynchronize(g.s));
-  const double *h = g.hf.data();
+  const double *h = g.pinOut;
   for (int i = 0; i < n; ++i) {
     fx[i] += h[i];
     fy[i] += h[n + i];
@@ -383,21 +428,25 @@ int cluster_need(int n, const double *x, const double *y, const double *z, const
                  double delr) {
   if (!g.clValid || (int)g.bx.size() != n) return CL_NEED_REBUILD;
   if (memcmp(&b, &g.clBox, sizeof(DevBox)) != 0) return CL_NEED_REBUILD;
-  if (memcmp(x, g.bx.data(), sizeof(double) * n) == 0 &&
-      memcmp(y, g.by.data(), sizeof(double) * n) == 0 &&
-      memcmp(z, g.bz.data(), sizeof(double) * n) == 0)
-    return g.clMoved ? CL_NEED_REFRESH : CL_NEED_NONE;
+  // one pass: the largest displacement since the build (minimum image, only
+  // components beyond half a box are wrapped) and whether any atom moved
   const double lim2 = 0.25 * delr * delr;
   const double L[3] = {b.a1, b.type == CUBIC ? b.a1 : b.b2, b.type == CUBIC ? b.a1 : b.c3};
+  const double h[3] = {0.5 * L[0], 0.5 * L[1], 0.5 * L[2]};
+  const double *cur[3] = {x, y, z};
+  const double *ref[3] = {g.bx.data(), g.by.data(), g.bz.data()};
+  bool moved = false;
   for (int i = 0; i < n; ++i) {
-    double d[3] = {x[i] - g.bx[i], y[i] - g.by[i], z[i] - g.bz[i]};
     double r2 = 0.;
     for (int k = 0; k < 3; ++k) {
-      d[k] -= L[k] * rint(d[k] / L[k]);
-      r2 += d[k] * d[k];
+      double d = cur[k][i] - ref[k][i];
+      moved |= d != 0.0;
+      if (fabs(d) > h[k]) d -= L[k] * rint(d / L[k]);
+      r2 += d * d;
     }
     if (r2 > lim2) return CL_NEED_REBUILD;
   }
+  if (!moved) return g.clMoved ? CL_NEED_REFRESH : CL_NEED_NONE;
   return CL_NEED_REFRESH;
 }
 

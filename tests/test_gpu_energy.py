@@ -261,3 +261,4 @@ def test_lean_half_kernel_matches_half(gpu):
         assert np.array_equal(out[4][0][k], out[7][0][k])
     assert out[4][1] == out[7][1]
     eng.close()
+
