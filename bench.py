@@ -972,7 +972,7 @@ def run_ours(args, rank, world):
     peak = max(peaks)
     achieved = FLOPS_PER_PAIR * pairs / (pair_ms * 1e-3) / 1e12
     traffic = None
-    prof = os.path.join(ROOT, "profiles", "pair_half_96k_traffic.json")
+    prof = os.path.join(ROOT, "profiles", "pair_half_lean_96k_traffic.json")
     if os.path.exists(prof):
         try:
             traffic = json.load(open(prof)).get("dram_bytes_per_launch")
