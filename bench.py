@@ -79,11 +79,12 @@ def _parse():
                    help="timed steps of the 999,999-atom box; 0 skips it")
     p.add_argument("--replica-steps", type=int, default=100,
                    help="timed dynamics steps of the 64-replica batch (one CUDA graph); 0 skips")
-    p.add_argument("--case", choices=["pair", "md", "build1m"], default=None,
-                   help="run one small case of the 96k box for a profiler and exit: 'pair' = "
-                        "list build + 4 force evaluations, 'md' = --md-steps dynamics steps "
-                        "driven from the host (a profiler sees no kernels inside graphs with "
-                        "conditional nodes)")
+    p.add_argument("--case", choices=["pair", "md", "build1m", "pair1m"], default=None,
+                   help="run one case for a profiler and exit: 'pair' = 96k list build + 4 "
+                        "force evaluations, 'md' = --md-steps 96k dynamics steps driven from "
+                        "the host (a profiler sees no kernels inside graphs with conditional "
+                        "nodes), 'build1m' = three 999,999-atom list builds, 'pair1m' = one "
+                        "999,999-atom build + 2 force evaluations")
     p.add_argument("--variant", type=int, default=7, help="pair kernel variant of --case pair")
     p.add_argument("--dropin-steps", type=int, default=10,
                    help="steps of the drop-in e2e leg (0 skips it)")
@@ -348,9 +349,10 @@ def cpu_baseline_sample(seed: int, gpu_list=None, gpu_list64=None, gpu_forces=No
 
 def mdbas_errors(nb, systems, dev) -> dict:
     """Mixed-form forces and energies against MDBas itself (oracle/_ref:
-    energy() with real-space Ewald, keyEwald 3) on the small water box and
-    the charged LJ fluid of the gradient case; the 96k box is compared in
-    cpu_baseline_sample."""
+    energy() with real-space Ewald, keyEwald 3) on the small water box, the
+    charged LJ fluid of the gradient case and the median box of the replica
+    batch; the 999,999-atom box on a 10,000-atom subset against the FP64
+    restatement; the 96k box is compared in cpu_baseline_sample."""
     import numpy as np
     import oracle
     if not oracle.Reference.available():
@@ -377,6 +379,46 @@ def mdbas_errors(nb, systems, dev) -> dict:
         out[name] = {"n_atoms": s.n, "force_rel_rms": float(np.sqrt(num / den)),
                      "elec_rel": abs(elec - re["elec"]) / abs(re["elec"]),
                      "vdw_rel": abs(en["vdw"] - re["vdw"]) / max(abs(re["vdw"]), 1e-300)}
+    # one box of the replica batch (the median size) against MDBas
+    sizes = systems.replica_sizes(64, seed=1)
+    k = int(np.argsort(sizes)[len(sizes) // 2])
+    batch = systems.config_replicas(64, seed=1)
+    rep = systems.replica(batch, k)
+    r = oracle.Reference(rep)
+    r.makelist()
+    x, y, z = r.positions()
+    rfx, rfy, rfz, re = r.energy()
+    r.close()
+    sp = systems.System(rep.name, rep.box, x, y, z, rep.q, rep.eps, rep.sig, rep.mass,
+                        rep.bonds, rep.angles)
+    e = nb.Engine(sp, precision=1, device=dev)
+    e.build()
+    e.compute()
+    fx, fy, fz = e.forces()
+    en = e.energies()
+    e.close()
+    num = ((fx - rfx) ** 2 + (fy - rfy) ** 2 + (fz - rfz) ** 2).sum()
+    den = (rfx ** 2 + rfy ** 2 + rfz ** 2).sum()
+    elec = en["elec_direct"] + en["elec_corr"]
+    out[f"replica_{k}_of_64"] = {"n_atoms": rep.n, "force_rel_rms": float(np.sqrt(num / den)),
+                                  "elec_rel": abs(elec - re["elec"]) / abs(re["elec"]),
+                                  "vdw_rel": abs(en["vdw"] - re["vdw"]) / abs(re["vdw"])}
+    # the 999,999-atom box: the forces of a seeded 10,000-atom subset against
+    # the FP64 restatement (bit-exact with MDBas's ewald_energy on its pairs)
+    big = systems.config_1m(seed=1)
+    e = nb.Engine(big, precision=1, device=dev)
+    e.build()
+    e.compute()
+    fx, fy, fz = e.forces()
+    e.close()
+    o = oracle.Oracle()
+    sub = np.sort(np.random.default_rng(11).choice(big.n, 10000, replace=False)).astype(np.int32)
+    gx, gy, gz = o.forces_subset(o.box(big.cell()), big, big.exclusions(symmetric=True), sub)
+    num = ((fx[sub] - gx) ** 2 + (fy[sub] - gy) ** 2 + (fz[sub] - gz) ** 2).sum()
+    den = (gx ** 2 + gy ** 2 + gz ** 2).sum()
+    out["water_1m_seed1_subset10k"] = {"n_atoms": big.n, "subset": int(len(sub)),
+                                       "force_rel_rms": float(np.sqrt(num / den)),
+                                       "against": "FP64 C restatement (oracle), 10,000 atoms"}
     return out
 
 
@@ -1227,6 +1269,17 @@ def run_case(args):
         for _ in range(4):
             e.compute()
         print(json.dumps({"case": "pair", "variant": args.variant,
+                          "pairs": e.energies()["n_pairs"], "list": e.list_stats()}))
+    elif args.case == "pair1m":
+        # the 999,999-atom box: one list build, two force evaluations (for a
+        # profiler capture of the pair kernel at full size)
+        s = systems.config_1m(seed=args.seed)
+        e = nb.Engine(s, precision=1)
+        e.set_variant(args.variant)
+        e.build()
+        for _ in range(2):
+            e.compute()
+        print(json.dumps({"case": "pair1m", "variant": args.variant,
                           "pairs": e.energies()["n_pairs"], "list": e.list_stats()}))
     elif args.case == "build1m":
         # the 999,999-atom box: three list builds (for a profiler capture of
