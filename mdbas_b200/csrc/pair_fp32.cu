@@ -981,7 +981,7 @@ k_pair_half(const long long *__restrict__ counters, const int4 *__restrict__ ite
 // for the range check (a NaN shows up in the i forces, checked per item),
 // the per-lane 64-bit energy sums live in shared memory, and warps take items
 // from a counter.  Forces and energies equal k_pair_half's bit for bit.
-template <bool VDW, bool EXACT>
+template <bool VDW, bool INNER, bool EXACT>
 __global__ void __launch_bounds__(256, 4)
 k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict__ items,
             const void *__restrict__ entriesV, const void *__restrict__ masksV,
@@ -990,7 +990,6 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
   __shared__ __align__(16) HalfStage stage[8];
   __shared__ long long esum[4][256];  // per lane: Ec, Ev, Vc, Vv
   HalfStage &S = stage[threadIdx.x >> 5];
-  constexpr bool INNER = true;
   const float kFar = 1e30f;
   const int lane = threadIdx.x & 31;
   const int il = lane & 7, jl = lane >> 3;
@@ -1031,7 +1030,7 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
     float2 ec = f2(0.f), ev6 = f2(0.f), gs = f2(0.f), hs = f2(0.f);
     for (int s0 = 0; s0 < nsteps; s0 += kHIt) {
       const int nIt = min(kHIt, nsteps - s0);
-      {
+      if (INNER) {
         const HalfEntry *__restrict__ hent = static_cast<const HalfEntry *>(entriesV);
         const unsigned *__restrict__ hmask = static_cast<const unsigned *>(masksV);
         const int nh = min(2 * kHIt, ne - 2 * s0);
@@ -1054,6 +1053,17 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
             js[1] = he.jh * 4;
             mk[1] = 0u;
           }
+        }
+      } else {
+        // the full list: each entry supplies its own two halves
+        const CPairEntry *__restrict__ ent = static_cast<const CPairEntry *>(entriesV);
+        const uint2 *__restrict__ msk = static_cast<const uint2 *>(masksV);
+        if (lane < nIt) {
+          const CPairEntry en = ent[e0 + s0 + lane];
+          *reinterpret_cast<float4 *>(S.sh[lane]) = make_float4(en.sx, en.sx, en.sy, en.sy);
+          *reinterpret_cast<float2 *>(S.sh[lane] + 4) = make_float2(en.sz, en.sz);
+          S.js[lane] = make_int2(en.j * kClusterSize, en.j * kClusterSize + 4);
+          S.mk[lane] = msk[e0 + s0 + lane];
         }
       }
       __syncwarp();
@@ -1098,6 +1108,8 @@ k_pair_half_lean(const long long *__restrict__ counters, const int4 *__restrict_
         // FP32 distances against this same rc^2, so its bits are the test
         const bool ina = (mk.x & lanebit) && (EXACT || r2.x <= c.rc2);
         const bool inb = (mk.y & lanebit) && (EXACT || r2.y <= c.rc2);
+        // the full list: a step whose pairs all lie beyond the cut-off is skipped
+        if (!INNER && !__any_sync(0xffffffffu, ina || inb)) continue;
         if (!EXACT) npair += (int)ina + (int)inb;
         const float2 r2s = make_float2(ina ? r2.x : kFar, inb ? r2.y : kFar);
         const float2 rinv = make_float2(rsqrt_approx(r2s.x), rsqrt_approx(r2s.y));
@@ -1788,9 +1800,10 @@ int pair_fp32_launch(ClusterWork &w, const PairParams &p, int grid, int block, c
         kv = p.vdwSwitch ? k_pair_half<true, true, 3, false> : k_pair_half<false, true, 3, false>;
       else
         kv = p.vdwSwitch ? k_pair_half<true, false, 3, false> : k_pair_half<false, false, 3, false>;
-    } else if (in && variant == kPairHalfLean) {
-      kv = p.vdwSwitch ? (ex ? k_pair_half_lean<true, true> : k_pair_half_lean<true, false>)
-                       : (ex ? k_pair_half_lean<false, true> : k_pair_half_lean<false, false>);
+    } else if (variant == kPairHalfLean) {
+      kv = !in ? (p.vdwSwitch ? k_pair_half_lean<true, false, false> : k_pair_half_lean<false, false, false>)
+         : ex  ? (p.vdwSwitch ? k_pair_half_lean<true, true, true> : k_pair_half_lean<false, true, true>)
+               : (p.vdwSwitch ? k_pair_half_lean<true, true, false> : k_pair_half_lean<false, true, false>);
     } else if (in && ex) {
       kv = p.vdwSwitch ? k_pair_half<true, true, 4, true> : k_pair_half<false, true, 4, true>;
     } else if (in) {

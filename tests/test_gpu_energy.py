@@ -248,11 +248,24 @@ def test_quad_kernel_in_pruned_dynamics(gpu):
 def test_lean_half_kernel_matches_half(gpu):
     """The lean form of the half-cluster kernel (variant 7: masked pairs at
     r^2 = 1e30 instead of zeroed products, items from a counter) gives the
-    first form's forces and energies bit for bit."""
+    first form's forces and energies bit for bit, over the exact inner list
+    and over the full list once the atoms have moved."""
     s = systems.water_box_for_atoms(18558, 3)
     eng = nb.Engine(s, precision=1)
     eng.build()
     out = {}
+    for v in (4, 7):
+        eng.set_variant(v)
+        eng.compute()
+        out[v] = (eng.forces(), eng.energies())
+    for k in range(3):
+        assert np.array_equal(out[4][0][k], out[7][0][k])
+    assert out[4][1] == out[7][1]
+    # moved atoms, layout refreshed: the inner list is stale and both forms
+    # walk the full list
+    rng = np.random.default_rng(5)
+    eng.set_positions(*(v + rng.uniform(-0.3, 0.3, s.n) for v in (s.x, s.y, s.z)))
+    eng.refresh()
     for v in (4, 7):
         eng.set_variant(v)
         eng.compute()
