@@ -364,14 +364,16 @@ struct WarpBuf {
   int rcount[kSearchCols];
   int rcode[kSearchCols];              // (sx + 1) | (sy + 1) << 2 | (sz + 1) << 4
   int rpre[kSearchCols + 1];
+  int tally[4];  // entries kept, inner halves, warp steps and pairs of the inner items
 };
 
 // Outputs of the search: the list (entries with 64-bit masks at the list
 // radius, exactly MDBas's pairs) and the inner list (j-cluster halves with a
 // pair within sqrt(rin2), 32-bit masks).
 // Both lists take their room with one 64-bit atomic per flush on a packed
-// counter (items << 40 | entries): counters[4] and hcounters[5]; a one-thread
-// kernel unpacks them into counters[0..1] / hcounters[0..1] for the readers.
+// counter (items << 40 | entries taken): counters[4]; the inner list uses the
+// same item index and twice the entry index.  A one-thread kernel writes the
+// readers' counts into counters[0..1] / hcounters[0..1].
 constexpr int kPackShift = 40;
 struct SearchOut {
   CPairEntry *entries;
@@ -383,7 +385,6 @@ struct SearchOut {
   unsigned *hmask;
   int4 *hitems;
   long long *hcounters;
-  long long hEntryCap, hItemCap;
   float rin2;
 };
 
@@ -431,14 +432,22 @@ __device__ __noinline__ double mdbas_pair_r2(const DevBox &b, int listMode,
 // radius are settled by MDBas's FP64 expression, so the list's pairs are
 // MDBas's.  The halves of the entries holding inner pairs become the item's
 // inner-list entries, halves 0 first.
+// Room: one 64-bit atomic per flush takes an item and cnt entries (an upper
+// bound of the entries kept) before the mask pass, so its round trip overlaps
+// the pass; the inner list's item has the same index and its halves sit at
+// twice the entry index.  Entries not kept leave gaps, which no reader
+// visits: every reader goes through the items.
 __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
                            const float4 *__restrict__ xq, const ClusterGeom &g,
                            const DevBox &box, int nreal_i, int pcLo, int pcHi, unsigned fimask,
                            const int *__restrict__ exclFlat, const int *__restrict__ slotOf,
                            const int *__restrict__ slotAtom, const int *__restrict__ frozen,
                            const double *__restrict__ px, const double *__restrict__ py,
-                           const double *__restrict__ pz, const SearchOut &o,
-                           int &npinAcc, int &stepAcc) {
+                           const double *__restrict__ pz, const SearchOut &o) {
+  unsigned long long pk = 0ull;
+  if (lane == 0)
+    pk = atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 4),
+                   (1ull << kPackShift) | (unsigned long long)cnt);
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
     const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
@@ -551,35 +560,25 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
   const bool keep = lane < cnt && (B.mask[lane].x | B.mask[lane].y) != 0u;
   const unsigned km = __ballot_sync(0xffffffffu, keep);
   const int nkeep = __popc(km);
-  if (nkeep == 0) return;
   const unsigned hA = __ballot_sync(0xffffffffu, inner.x != 0u);
   const unsigned hB = __ballot_sync(0xffffffffu, inner.y != 0u);
   const int nA = __popc(hA), nin = nA + __popc(hB);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) npin += __shfl_xor_sync(0xffffffffu, npin, off);
-  unsigned long long pk = 0ull, hpk = 0ull;
-  if (lane == 0) {
-    pk = atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 4),
-                   (1ull << kPackShift) | (unsigned long long)nkeep);
-    if (nin > 0)
-      hpk = atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 5),
-                      (1ull << kPackShift) | (unsigned long long)nin);
-  }
   pk = __shfl_sync(0xffffffffu, pk, 0);
-  hpk = __shfl_sync(0xffffffffu, hpk, 0);
-  const unsigned long long lowMask = (1ull << kPackShift) - 1ull;
-  const long long e0 = (long long)(pk & lowMask), it = (long long)(pk >> kPackShift);
-  const long long h0 = (long long)(hpk & lowMask), hit = (long long)(hpk >> kPackShift);
-  if (e0 + nkeep > o.entryCap || it >= o.itemCap ||
-      (nin > 0 && (h0 + nin > o.hEntryCap || hit >= o.hItemCap))) {
+  const long long e0 = (long long)(pk & ((1ull << kPackShift) - 1ull));
+  const long long it = (long long)(pk >> kPackShift);
+  if (e0 + cnt > o.entryCap || it >= o.itemCap) {
     if (lane == 0)
       atomicOr(reinterpret_cast<unsigned long long *>(o.counters + 2),
                (unsigned long long)CL_OVERFLOW);
     return;
   }
-  if (nin > 0) {
-    npinAcc += npin;
-    stepAcc += (nin + 1) >> 1;
+  if (lane == 0) {
+    B.tally[0] += nkeep;
+    B.tally[1] += nin;
+    B.tally[2] += (nin + 1) >> 1;
+    B.tally[3] += npin;
   }
   if (keep) {
     const int pos = __popc(km & ((1u << lane) - 1u));
@@ -587,7 +586,7 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
     o.masks[e0 + pos] = B.mask[lane];
     const unsigned lt = (1u << lane) - 1u;
     if (inner.x != 0u) {
-      const long long q = h0 + __popc(hA & lt);
+      const long long q = 2 * e0 + __popc(hA & lt);
       HalfEntry he;
       he.jh = 2 * en.j;
       he.sx = en.sx;
@@ -597,7 +596,7 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
       o.hmask[q] = inner.x;
     }
     if (inner.y != 0u) {
-      const long long q = h0 + nA + __popc(hB & lt);
+      const long long q = 2 * e0 + nA + __popc(hB & lt);
       HalfEntry he;
       he.jh = 2 * en.j + 1;
       he.sx = en.sx;
@@ -607,17 +606,47 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
       o.hmask[q] = inner.y;
     }
   }
+  // an item whose entries all fell out stays in the list, empty
   if (lane == 0) {
     o.items[it] = make_int4(ci, (int)e0, nkeep, 0);
-    if (nin > 0) o.hitems[hit] = make_int4(ci, (int)h0, nin, 0);
+    o.hitems[it] = make_int4(ci, (int)(2 * e0), nin, 0);
   }
+}
+
+// Per column, the first cluster (clusters are z-sorted in their column)
+// whose FP32 origin z is at least -Lz/2 + b Lz / kZBins, for b = 0..kZBins
+// (b = 0: the column's first cluster, b = kZBins: one past its last).  The
+// search reads a z window's range from two entries of this table instead of
+// two binary searches over the column; a conservative bin on either side
+// keeps the range a superset, and the bounding-box test that follows drops
+// the extra clusters.  One block per column, one thread per bin.
+__global__ void __launch_bounds__((kZBins + 32) & ~31)
+k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restrict__ clusterRep,
+           const int *__restrict__ colClStart, const float4 *__restrict__ originF,
+           int *__restrict__ zTab) {
+  const int col = blockIdx.x, b = threadIdx.x;
+  if (col >= nCols || b > kZBins) return;
+  const int cs = colClStart[col], ce = colClStart[col + 1];
+  int a = cs;
+  if (b == kZBins) {
+    a = ce;
+  } else if (b > 0 && ce > cs) {
+    const float Lz = (float)geoms[clusterRep ? clusterRep[cs] : 0].Lz;
+    const float zb = -0.5f * Lz + (float)b * (Lz / (float)kZBins);
+    int hi = ce;
+    while (a < hi) {  // first origin z >= zb
+      const int mid = (a + hi) >> 1;
+      if (originF[mid].z < zb) a = mid + 1; else hi = mid;
+    }
+  }
+  zTab[(size_t)col * (kZBins + 1) + b] = a;
 }
 
 // Cluster-pair search ("cell sweep"): one warp per i cluster.  The columns
 // within reach in x-y (periodic images as explicit shifts) are listed, 32 at
 // a time, with per z image within reach the clusters (z-sorted in their
-// column) whose origin lies within the i box's reach, found by binary
-// search; then all candidates of the listed ranges are tested against the i
+// column) whose origin lies within the i box's reach, read from the column's
+// z table (k_col_ztab); then all candidates of the listed ranges are tested against the i
 // bounding box as one flat index space, 32 per round, so every lane has work
 // and all loads of a round are independent.  Survivors are compacted by
 // ballot into the warp's buffer with their FP32 shift (the FP64 origin
@@ -631,7 +660,7 @@ __global__ void __launch_bounds__(kSearchThreads, 5)
 k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
          const DevBox *__restrict__ boxes, const int *__restrict__ clusterRep,
          const int *__restrict__ colOff, const int *__restrict__ colRank,
-         const int *__restrict__ colClStart, const int *__restrict__ clusterXY,
+         const int *__restrict__ zTab, const int *__restrict__ clusterXY,
          const double4 *__restrict__ origin, const float4 *__restrict__ originF,
          const float4 *__restrict__ half, const int *__restrict__ slotAtom,
          const int *__restrict__ slotOf, const int *__restrict__ frozen,
@@ -650,7 +679,6 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   const int colBase = colOff[rep];
   hmaxBits += 4 * rep;
 
-  const double4 oi = origin[ci];
   const float4 oif = originF[ci];
   const float4 hi = half[ci];
   const int nreal_i = (int)hi.w;
@@ -679,6 +707,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   pcHi = __reduce_max_sync(0xffffffffu, pcHi);
   const int fi = (ia >= 0 && frozen) ? frozen[ia] : 0;
   const unsigned fimask = __ballot_sync(0xffffffffu, lane < kClusterSize && fi) & 0xffu;
+  if (lane < 4) B.tally[lane] = 0;
   if (lane < kClusterSize) {
     B.si[lane] = xq[ci * kClusterSize + lane];
 #pragma unroll
@@ -698,15 +727,19 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   const float zwlo = oif.z - hi.z - rl - hzmax, zwhi = oif.z + hi.z + rl + hzmax;
   const bool zm = zwlo < -0.5f * Lz;  // the image below can be within reach
   const bool zp = zwhi > 0.5f * Lz;   // the image above can be within reach
-  int cnt = 0, npinAcc = 0, stepAcc = 0;
-  long long cand = 0;
+  // z-table bins of the window's ends (image sz: minus sz * kZBins), widened
+  // by one bin below and two above since the bin of a coordinate is rounded
+  // (the table's bin b starts at -Lz/2 + b Lz / kZBins)
+  const int zbl = __float2int_rd((zwlo + 0.5f * Lz) * ((float)kZBins / Lz)) - 1;
+  const int zbh = __float2int_rd((zwhi + 0.5f * Lz) * ((float)kZBins / Lz)) + 2;
+  int cnt = 0, cand = 0;
 
   const int nx = 2 * g.Dx + 1, ncomb = nx * (2 * g.Dy + 1);
   int ncol = 0;
   for (int c0 = 0; c0 < ncomb; c0 += 32) {
     const int cb = c0 + lane;
     bool pass = false;
-    int cs = 0, cc = 0, code = 0;
+    int code = 0, tab = 0;  // tab: the column's row of zTab
     if (cb < ncomb) {
       const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
       int jy = cy + dy, sy = 0;
@@ -718,11 +751,9 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
       const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
       if (gx * gx + gy * gy <= rlist2) {
-        const int col = colRank[colBase + jy * g.ncx + jx];
-        cs = colClStart[col];
-        cc = colClStart[col + 1];
+        tab = colRank[colBase + jy * g.ncx + jx] * (kZBins + 1);
         code = (sx + 1) | ((sy + 1) << 2);
-        pass = cc > cs;
+        pass = true;
       }
     }
     // Per z image within reach, the column's clusters (z-sorted) whose
@@ -731,19 +762,11 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
     for (int sz = -1; sz <= 1; ++sz) {
       int first = 0, n = 0;
       if (pass && !((sz < 0 && !zm) || (sz > 0 && !zp))) {
-        const float lo = zwlo - sz * Lz, hiz = zwhi - sz * Lz;
-        int a = cs, b = cc;
-        while (a < b) {  // first origin z >= lo
-          const int mid = (a + b) >> 1;
-          if (__ldg(&originF[mid].z) < lo) a = mid + 1; else b = mid;
-        }
-        first = a;
-        b = cc;
-        while (a < b) {  // first origin z > hiz
-          const int mid = (a + b) >> 1;
-          if (__ldg(&originF[mid].z) <= hiz) a = mid + 1; else b = mid;
-        }
-        n = a - first;
+        // the clusters with origin z in the window (a superset)
+        const int bl = min(max(zbl - sz * kZBins, 0), kZBins);
+        const int bh = min(max(zbh - sz * kZBins, 0), kZBins);
+        first = __ldg(zTab + tab + bl);
+        n = max(__ldg(zTab + tab + bh) - first, 0);
         // half list: a pair with cj < ci is listed from cj's side, so the
         // range starts at ci at the earliest (cluster indices ascend within
         // a column)
@@ -830,6 +853,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
         B.code[pos] = sidx | ((int)hj.w << 8);
         // the entry's shift, formed in FP64 and rounded once: the value the
         // pair kernel adds to the j atoms
+        const double4 oi = origin[ci];  // re-read here: not held across the scan
         B.sh[pos] = make_float4((float)(ojd.x + sx * g.Lx - oi.x),
                                 (float)(ojd.y + sy * g.Ly - oi.y),
                                 (float)(ojd.z + sz * g.Lz - oi.z), 0.f);
@@ -838,7 +862,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       __syncwarp();
       if (cnt >= kItemMax) {
         flush_item(B, kItemMax, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat,
-                   slotOf, slotAtom, frozen, px, py, pz, o, npinAcc, stepAcc);
+                   slotOf, slotAtom, frozen, px, py, pz, o);
         __syncwarp();
         const int rem = cnt - kItemMax;
         if (lane < rem) {
@@ -855,32 +879,38 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   }
   if (cnt > 0)
     flush_item(B, cnt, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
-               slotAtom, frozen, px, py, pz, o, npinAcc, stepAcc);
+               slotAtom, frozen, px, py, pz, o);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, off);
   if (lane == 0) {
     atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 3), (unsigned long long)cand);
+    // entries kept and inner halves written (the counts of the two lists),
     // warp steps of the half-cluster kernel over this i cluster's inner
     // items, and its inner pairs
-    if (stepAcc > 0) {
+    if (B.tally[0] > 0)
+      atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 5),
+                (unsigned long long)B.tally[0]);
+    if (B.tally[1] > 0) {
+      atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 6),
+                (unsigned long long)B.tally[1]);
       atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 3),
-                (unsigned long long)stepAcc);
+                (unsigned long long)B.tally[2]);
       atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 4),
-                (unsigned long long)npinAcc);
+                (unsigned long long)B.tally[3]);
     }
   }
 }
 
-// The packed list counters (items << 40 | entries) unpacked for the readers.
+// The search's counts for the readers: entries kept (counters[5]) and inner
+// halves written (hcounters[6]); both lists have the packed counter's item
+// count (items << 40 | entries taken, counters[4]).
 __global__ void k_unpack_counts(long long *__restrict__ counters, long long *__restrict__ hcounters) {
   if (threadIdx.x == 0) {
-    const unsigned long long m = (1ull << kPackShift) - 1ull;
     const unsigned long long a = (unsigned long long)counters[4];
-    const unsigned long long b = (unsigned long long)hcounters[5];
-    counters[0] = (long long)(a & m);
+    counters[0] = counters[5];
     counters[1] = (long long)(a >> kPackShift);
-    hcounters[0] = (long long)(b & m);
-    hcounters[1] = (long long)(b >> kPackShift);
+    hcounters[0] = hcounters[6];
+    hcounters[1] = (long long)(a >> kPackShift);
   }
 }
 
@@ -1150,6 +1180,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     MDB_TRY(w.colStart.ensure(sizeof(int) * (nCols + 2)));
     MDB_TRY(w.colPadStart.ensure(sizeof(int) * (nCols + 2)));
     MDB_TRY(w.colClStart.ensure(sizeof(int) * (nCols + 2)));
+    MDB_TRY(w.zTab.ensure(sizeof(int) * (size_t)nCols * (kZBins + 1)));
     MDB_TRY(w.atomCol.ensure(sizeof(int) * n));
     MDB_TRY(w.atomZ.ensure(sizeof(double) * n));
     MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
@@ -1202,12 +1233,14 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
              y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
              w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.xp.as<float>(),
              w.ljp.as<float>(), w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
+  MDB_LAUNCH(k_col_ztab, nCols, (kZBins + 32) & ~31, 0, s, nCols, gd, w.clusterRepDev(), w.colClStart.as<int>(),
+             w.originF.as<float4>(), w.zTab.as<int>());
 
   // Cluster-pair search; in the synchronising form grow the list and search
   // again if it overflowed.  The inner list holds at most two halves per
   // entry, so it never overflows on its own.
   if (w.entryCap == 0) {
-    w.entryCap = (long long)w.clCap * 160 + 4096;
+    w.entryCap = (long long)w.clCap * 192 + 4096;
     w.itemCap = w.entryCap / kItemMax + w.clCap + 1024;
   }
   // 0: the pair kernel's own FP32 rc^2 (PairConstF::rc2), whose test on the
@@ -1226,7 +1259,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
       MDB_TRY(w.countersIn.ensure(sizeof(long long) * 8));
     }
     MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
-    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 2, s));
+    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 3, s));
     MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
     SearchOut o;
     o.entries = w.entries.as<CPairEntry>();
@@ -1239,13 +1272,11 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     o.hmask = w.masksIn.as<unsigned>();
     o.hitems = w.itemsIn.as<int4>();
     o.hcounters = w.countersIn.as<long long>();
-    o.hEntryCap = w.inEntryCap;
-    o.hItemCap = w.inItemCap;
     o.rin2 = rin2;
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[5], s));
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
                w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
-               w.colRank.as<int>(), w.colClStart.as<int>(), w.clusterXY.as<int>(),
+               w.colRank.as<int>(), w.zTab.as<int>(), w.clusterXY.as<int>(),
                w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
                w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
                w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
@@ -1259,7 +1290,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
                  w.sticky.as<long long>());
       return MDBAS_NB_OK;
     }
-    long long flags[4], hflags[4];
+    long long flags[8], hflags[4];
     int nSlots = 0;
     MDB_CUDA(cudaMemcpyAsync(flags, w.counters.p, sizeof(flags), cudaMemcpyDeviceToHost, s));
     MDB_CUDA(cudaMemcpyAsync(hflags, w.countersIn.p, sizeof(hflags), cudaMemcpyDeviceToHost, s));
@@ -1279,7 +1310,9 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     }
     // the search does not clear the overflow bit; the next attempt starts clean
     MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 2, 0, sizeof(long long), s));
-    w.entryCap = (long long)(flags[0] * 1.25) + 4096;
+    // room for the entries the search took (kept or not)
+    const long long taken = (long long)((unsigned long long)flags[4] & ((1ull << kPackShift) - 1ull));
+    w.entryCap = (long long)(taken * 1.25) + 4096;
     w.itemCap = (long long)(flags[1] * 1.25) + 1024;
   }
   return MDBAS_NB_ERR_CAPACITY;

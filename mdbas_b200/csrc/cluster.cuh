@@ -9,6 +9,7 @@ namespace mdbas {
 
 constexpr int kClusterSize = 8;
 constexpr int kItemMax = 32;  // j-clusters per work item of the pair kernel
+constexpr int kZBins = 64;    // z bins per column of the search's cluster lookup table
 
 // Geometry of the column grid (x-y cells, atoms sorted by z inside a cell).
 //
@@ -81,6 +82,8 @@ struct ClusterWork {
   DBuf slotOf;        // atom -> slot
   DBuf clusterXY;     // cluster -> cx | cy << 16
   DBuf colClStart;    // column slot -> first cluster (nCols + 1)
+  DBuf zTab;          // int[nCols * (kZBins + 1)]: per column and z bin b, the first
+                      // cluster whose origin z is at least -Lz/2 + b Lz / kZBins
   DBuf origin;        // double4 per cluster (FP64 origin)
   DBuf originF;       // float4 per cluster (FP32 origin, w = real atoms)
   DBuf hmax;          // int[4 * nRep]: largest half extent per axis (float bits)

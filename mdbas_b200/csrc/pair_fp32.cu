@@ -551,6 +551,9 @@ k_pair_fp32x2_bulk(const long long *__restrict__ counters, const int4 *__restric
   for (long long it = gw; it < nItems; it += nw) {
     const int4 item = items[it];
     const int ci = item.x, e0 = item.y, ne = item.z;
+    // an empty item stages nothing (an arrival with no copies would complete
+    // a buffer phase that no wait consumes)
+    if (ne == 0) continue;
     const float4 xi = xq[ci * kClusterSize + il];
     const float2 li = lj[ci * kClusterSize + il];
     float2 fi_x = f2(0.f), fi_y = f2(0.f), fi_z = f2(0.f);
