@@ -718,28 +718,18 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   __syncwarp();
 
   const float rlist2 = g.rlist2;
-  const float rl = sqrtf(rlist2);
   const float Lx = (float)g.Lx, Ly = (float)g.Ly, Lz = (float)g.Lz;
   const float wx = (float)g.wx, wy = (float)g.wy;
-  // z images that can reach any cluster at all: cluster centres lie in
-  // [-Lz/2, Lz/2) and no cluster extends more than hmax[2] from its centre
+  // no cluster extends more than hmax[2] from its centre in z
   const float hzmax = __int_as_float(hmaxBits[2]);
-  const float zwlo = oif.z - hi.z - rl - hzmax, zwhi = oif.z + hi.z + rl + hzmax;
-  const bool zm = zwlo < -0.5f * Lz;  // the image below can be within reach
-  const bool zp = zwhi > 0.5f * Lz;   // the image above can be within reach
-  // z-table bins of the window's ends (image sz: minus sz * kZBins), widened
-  // by one bin below and two above since the bin of a coordinate is rounded
-  // (the table's bin b starts at -Lz/2 + b Lz / kZBins)
-  const int zbl = __float2int_rd((zwlo + 0.5f * Lz) * ((float)kZBins / Lz)) - 1;
-  const int zbh = __float2int_rd((zwhi + 0.5f * Lz) * ((float)kZBins / Lz)) + 2;
   int cnt = 0, cand = 0;
 
   const int nx = 2 * g.Dx + 1, ncomb = nx * (2 * g.Dy + 1);
   int ncol = 0;
   for (int c0 = 0; c0 < ncomb; c0 += 32) {
     const int cb = c0 + lane;
-    bool pass = false;
-    int code = 0, tab = 0;  // tab: the column's row of zTab
+    bool pass = false, zm = false, zp = false;
+    int code = 0, tab = 0, zbl = 0, zbh = 0;  // tab: the column's row of zTab
     if (cb < ncomb) {
       const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
       int jy = cy + dy, sy = 0;
@@ -750,10 +740,27 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       const float gy = fmaxf(fmaxf(ylo - (oif.y + hi.y), (oif.y - hi.y) - yhi), 0.f);
       const float xlo = -0.5f * Lx + jx * wx + sx * Lx, xhi = xlo + wx;
       const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
-      if (gx * gx + gy * gy <= rlist2) {
+      const float gxy2 = gx * gx + gy * gy;
+      if (gxy2 <= rlist2) {
         tab = colRank[colBase + jy * g.ncx + jx] * (kZBins + 1);
         code = (sx + 1) | ((sy + 1) << 2);
         pass = true;
+        // the z reach left over the column's x-y gap (a cluster's x-y extent
+        // lies inside its column: the gaps less 0.01 A, which covers the
+        // rounding of both), the window of j origins it allows, and whether
+        // the images below and above can be within reach (cluster centres
+        // lie in [-Lz/2, Lz/2))
+        const float gxm = fmaxf(gx - 0.01f, 0.f), gym = fmaxf(gy - 0.01f, 0.f);
+        const float zr = sqrtf(fmaxf(rlist2 - (gxm * gxm + gym * gym), 0.f)) + 0.01f + hi.z + hzmax;
+        const float zwlo = oif.z - zr, zwhi = oif.z + zr;
+        zm = zwlo < -0.5f * Lz;
+        zp = zwhi > 0.5f * Lz;
+        // z-table bins of the window's ends (image sz: minus sz * kZBins),
+        // widened by one bin below and two above since the bin of a
+        // coordinate is rounded (the table's bin b starts at
+        // -Lz/2 + b Lz / kZBins)
+        zbl = __float2int_rd((zwlo + 0.5f * Lz) * ((float)kZBins / Lz)) - 1;
+        zbh = __float2int_rd((zwhi + 0.5f * Lz) * ((float)kZBins / Lz)) + 2;
       }
     }
     // Per z image within reach, the column's clusters (z-sorted) whose
