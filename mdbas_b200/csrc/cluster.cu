@@ -357,7 +357,8 @@ struct WarpBuf {
   float4 sh[kBufCap];                  // FP32 shift: (float)(j origin + image - i origin)
   uint2 mask[kItemMax];
   float4 sj[kClusterSize * kItemMax];  // staged j atoms (xq), sj[j * kItemMax + entry]
-  float4 si[kClusterSize];             // the i cluster's atoms (xq)
+  float4 sn[kClusterSize];             // the i cluster's atoms, negated and paired:
+  float2 snz[kClusterSize];            // (-x, -x, -y, -y) and (-z, -z)
   int ps[kClusterSize][kExclRegs];     // per i atom: its first exclusion partners' slots
   int es[kClusterSize], ee[kClusterSize];  // per i atom: its range of exclFlat
   int rstart[kSearchCols];             // first cluster of a z-windowed range
@@ -419,6 +420,25 @@ __device__ __noinline__ double mdbas_pair_r2(const DevBox &b, int listMode,
   return dist_d(b, dx, dy, dz);
 }
 
+// Shared-memory loads the compiler keeps where they are written (not hoisted
+// out of a loop into registers that the loop would then hold throughout).
+__device__ __forceinline__ float4 lds_keep(const float4 *p) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"((unsigned)__cvta_generic_to_shared(p))
+               : "memory");
+  return v;
+}
+__device__ __forceinline__ float2 lds_keep(const float2 *p) {
+  float2 v;
+  asm volatile("ld.shared.v2.f32 {%0, %1}, [%2];"
+               : "=f"(v.x), "=f"(v.y)
+               : "r"((unsigned)__cvta_generic_to_shared(p))
+               : "memory");
+  return v;
+}
+
 // Flush the first cnt (<= kItemMax) buffered candidates as one work item.
 // Lane k builds candidate k's 64-bit interaction mask on its own: bit i + 8 j
 // (j < 4 in .x, j >= 4 in .y at i + 8 (j - 4)) for the pair (i atom i, j atom
@@ -466,46 +486,47 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
     en.sx = shk.x;
     en.sy = shk.y;
     en.sz = shk.z;
-    // the j atoms h and h + 4 side by side, shifted as the pair kernel does
-    float2 jx[4], jy[4], jz[4];
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const float4 a = B.sj[h * kItemMax + k], b = B.sj[(h + 4) * kItemMax + k];
-      jx[h] = make_float2(a.x + en.sx, b.x + en.sx);
-      jy[h] = make_float2(a.y + en.sy, b.y + en.sy);
-      jz[h] = make_float2(a.z + en.sz, b.z + en.sz);
-    }
-    // per pair: inside the band's lower edge (lo), inside its upper edge
-    // (cand), inside the inner radius (in)
+    // Per pair the sign of (radius^2 - r^2), exact for the FP32 distance the
+    // pair kernel forms (j atom plus the shift, minus the i atom), is shifted
+    // into a word per radius and half: h from 3 down to 0, i from 7 down to
+    // 0 leaves pair (i, h) at bit i + 8 h.  A set bit is a pair beyond the
+    // radius; the words are inverted at the end.  Per radius: beyond the
+    // band's lower edge (lo), beyond its upper edge (ca), beyond the inner
+    // radius (in).
+    const float2 rlo = make_float2(g.rlo2, g.rlo2), rhi = make_float2(g.rhi2, g.rhi2),
+                 rin = make_float2(o.rin2, o.rin2);
     unsigned lo0 = 0u, lo1 = 0u, ca0 = 0u, ca1 = 0u, in0 = 0u, in1 = 0u;
-    // the i loop stays rolled (a small loop body keeps the instruction cache
-    // warm); per i atom the four j pairs give byte-strided rows of bits
 #pragma unroll 1
-    for (int i = 0; i < kClusterSize; ++i) {
-      const float4 xi = B.si[i];
-      const float2 nx = make_float2(-xi.x, -xi.x), ny = make_float2(-xi.y, -xi.y),
-                   nz = make_float2(-xi.z, -xi.z);
-      unsigned rl0 = 0u, rl1 = 0u, rc0 = 0u, rc1 = 0u, ri0 = 0u, ri1 = 0u;
+    for (int h = 3; h >= 0; --h) {
+      // the j atoms h and h + 4 side by side, shifted as the pair kernel does
+      const float4 a = B.sj[h * kItemMax + k], b = B.sj[(h + 4) * kItemMax + k];
+      const float2 jx = make_float2(a.x + en.sx, b.x + en.sx);
+      const float2 jy = make_float2(a.y + en.sy, b.y + en.sy);
+      const float2 jz = make_float2(a.z + en.sz, b.z + en.sz);
 #pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const float2 dx = __fadd2_rn(jx[h], nx), dy = __fadd2_rn(jy[h], ny),
-                     dz = __fadd2_rn(jz[h], nz);
+      for (int i = kClusterSize - 1; i >= 0; --i) {
+        const float4 nxy = lds_keep(&B.sn[i]);
+        const float2 dx = __fadd2_rn(jx, make_float2(nxy.x, nxy.y));
+        const float2 dy = __fadd2_rn(jy, make_float2(nxy.z, nxy.w));
+        const float2 dz = __fadd2_rn(jz, lds_keep(&B.snz[i]));
         const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-        const unsigned bit = 1u << (8 * h);
-        if (r2.x <= g.rlo2) rl0 |= bit;
-        if (r2.y <= g.rlo2) rl1 |= bit;
-        if (r2.x <= g.rhi2) rc0 |= bit;
-        if (r2.y <= g.rhi2) rc1 |= bit;
-        if (r2.x <= o.rin2) ri0 |= bit;
-        if (r2.y <= o.rin2) ri1 |= bit;
+        const float2 dl = __ffma2_rn(r2, make_float2(-1.f, -1.f), rlo);
+        const float2 dc = __ffma2_rn(r2, make_float2(-1.f, -1.f), rhi);
+        const float2 di = __ffma2_rn(r2, make_float2(-1.f, -1.f), rin);
+        lo0 = __funnelshift_l(__float_as_uint(dl.x), lo0, 1);
+        lo1 = __funnelshift_l(__float_as_uint(dl.y), lo1, 1);
+        ca0 = __funnelshift_l(__float_as_uint(dc.x), ca0, 1);
+        ca1 = __funnelshift_l(__float_as_uint(dc.y), ca1, 1);
+        in0 = __funnelshift_l(__float_as_uint(di.x), in0, 1);
+        in1 = __funnelshift_l(__float_as_uint(di.y), in1, 1);
       }
-      lo0 |= rl0 << i;
-      lo1 |= rl1 << i;
-      ca0 |= rc0 << i;
-      ca1 |= rc1 << i;
-      in0 |= ri0 << i;
-      in1 |= ri1 << i;
     }
+    lo0 = ~lo0;
+    lo1 = ~lo1;
+    ca0 = ~ca0;
+    ca1 = ~ca1;
+    in0 = ~in0;
+    in1 = ~in1;
     // padding slots of either cluster
     const unsigned irow = (nreal_i >= 8 ? 0xffu : ((1u << nreal_i) - 1u)) * 0x01010101u;
     unsigned m0 = irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
@@ -709,7 +730,9 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   const unsigned fimask = __ballot_sync(0xffffffffu, lane < kClusterSize && fi) & 0xffu;
   if (lane < 4) B.tally[lane] = 0;
   if (lane < kClusterSize) {
-    B.si[lane] = xq[ci * kClusterSize + lane];
+    const float4 xi = xq[ci * kClusterSize + lane];
+    B.sn[lane] = make_float4(-xi.x, -xi.x, -xi.y, -xi.y);
+    B.snz[lane] = make_float2(-xi.z, -xi.z);
 #pragma unroll
     for (int r = 0; r < kExclRegs; ++r) B.ps[lane][r] = ps[r];
     B.es[lane] = es;
