@@ -354,7 +354,6 @@ constexpr int kSearchCols = 192;  // z-windowed ranges listed per warp before a 
 struct WarpBuf {
   int j[kBufCap];
   int code[kBufCap];                   // image index (0..26) | real j atoms << 8
-  float4 sh[kBufCap];                  // FP32 shift: (float)(j origin + image - i origin)
   uint2 mask[kItemMax];
   float4 sj[kClusterSize * kItemMax];  // staged j atoms (xq), sj[j * kItemMax + entry]
   float4 sn[kClusterSize];             // the i cluster's atoms, negated and paired:
@@ -463,11 +462,16 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
                            const int *__restrict__ exclFlat, const int *__restrict__ slotOf,
                            const int *__restrict__ slotAtom, const int *__restrict__ frozen,
                            const double *__restrict__ px, const double *__restrict__ py,
-                           const double *__restrict__ pz, const SearchOut &o) {
+                           const double *__restrict__ pz,
+                           const double4 *__restrict__ origin, const SearchOut &o) {
   unsigned long long pk = 0ull;
   if (lane == 0)
     pk = atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 4),
                    (1ull << kPackShift) | (unsigned long long)cnt);
+  // the origins for this lane's entry shift, loaded with the staged atoms
+  const double4 oi = origin[ci];
+  double4 oj = make_double4(0., 0., 0., 0.);
+  if (lane < cnt) oj = origin[B.j[lane]];
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
     const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
@@ -481,11 +485,13 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
     const int k = lane;
     const int cj = B.j[k], code = B.code[k];
     const int sidx = code & 31, nrj = code >> 8;
-    const float4 shk = B.sh[k];
+    // the entry's shift, formed in FP64 and rounded once: the value the pair
+    // kernel adds to the j atoms
+    const int sx = sidx % 3 - 1, sy = (sidx / 3) % 3 - 1, sz = sidx / 9 - 1;
     en.j = cj;
-    en.sx = shk.x;
-    en.sy = shk.y;
-    en.sz = shk.z;
+    en.sx = (float)(oj.x + sx * g.Lx - oi.x);
+    en.sy = (float)(oj.y + sy * g.Ly - oi.y);
+    en.sz = (float)(oj.z + sz * g.Lz - oi.z);
     // Per pair the sign of (radius^2 - r^2), exact for the FP32 distance the
     // pair kernel forms (j atom plus the shift, minus the i atom), is shifted
     // into a word per radius and half: h from 3 down to 0, i from 7 down to
@@ -666,16 +672,17 @@ k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restri
 // Cluster-pair search ("cell sweep"): one warp per i cluster.  The columns
 // within reach in x-y (periodic images as explicit shifts) are listed, 32 at
 // a time, with per z image within reach the clusters (z-sorted in their
-// column) whose origin lies within the i box's reach, read from the column's
-// z table (k_col_ztab); then all candidates of the listed ranges are tested against the i
-// bounding box as one flat index space, 32 per round, so every lane has work
-// and all loads of a round are independent.  Survivors are compacted by
-// ballot into the warp's buffer with their FP32 shift (the FP64 origin
-// difference plus the image, rounded once) and flushed as work items of up to
-// 32 entries.  Newton's third law: each unordered cluster pair is kept once
-// (j > i, or j == i with a positive or zero shift, the latter with only the
-// upper triangle of atom pairs).
-// (at most 96 registers and ~40 KB of shared memory per block: five blocks
+// column) whose origin lies within the z reach left over the column's x-y
+// gap, read from the column's z table (k_col_ztab); then all candidates of
+// the listed ranges are tested against the i bounding box as one flat index
+// space, 32 per round, so every lane has work and all loads of a round are
+// independent.  Survivors are compacted by ballot into the warp's buffer
+// with their image and flushed as work items of up to 32 entries (the flush
+// forms each entry's FP32 shift: the FP64 origin difference plus the image,
+// rounded once).  Newton's third law: each unordered cluster pair is kept
+// once (j > i, or j == i with a positive or zero shift, the latter with only
+// the upper triangle of atom pairs).
+// (at most 96 registers and ~34 KB of shared memory per block: five blocks
 // of four warps per SM)
 __global__ void __launch_bounds__(kSearchThreads, 5)
 k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
@@ -848,7 +855,6 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       int cj = 0, sx = 0, sy = 0, sz = 0;
       float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
       float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
-      double4 ojd = make_double4(0., 0., 0., 0.);
       if (valid) {
         // the listed range holding flat index t
         int lo = 0, hi2 = ncol - 1;
@@ -863,7 +869,6 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
         sz = ((rc >> 4) & 3) - 1;
         oj = originF[cj];
         hj = half[cj];
-        ojd = origin[cj];
       }
       const float fx = oj.x + sx * Lx - oif.x;
       const float fy = oj.y + sy * Ly - oif.y;
@@ -881,24 +886,17 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
         const int pos = cnt + __popc(m & ((1u << lane) - 1u));
         B.j[pos] = cj;
         B.code[pos] = sidx | ((int)hj.w << 8);
-        // the entry's shift, formed in FP64 and rounded once: the value the
-        // pair kernel adds to the j atoms
-        const double4 oi = origin[ci];  // re-read here: not held across the scan
-        B.sh[pos] = make_float4((float)(ojd.x + sx * g.Lx - oi.x),
-                                (float)(ojd.y + sy * g.Ly - oi.y),
-                                (float)(ojd.z + sz * g.Lz - oi.z), 0.f);
       }
       cnt += __popc(m);
       __syncwarp();
       if (cnt >= kItemMax) {
         flush_item(B, kItemMax, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat,
-                   slotOf, slotAtom, frozen, px, py, pz, o);
+                   slotOf, slotAtom, frozen, px, py, pz, origin, o);
         __syncwarp();
         const int rem = cnt - kItemMax;
         if (lane < rem) {
           B.j[lane] = B.j[kItemMax + lane];
           B.code[lane] = B.code[kItemMax + lane];
-          B.sh[lane] = B.sh[kItemMax + lane];
         }
         cnt = rem;
         __syncwarp();
@@ -909,7 +907,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   }
   if (cnt > 0)
     flush_item(B, cnt, ci, lane, xq, g, box, nreal_i, pcLo, pcHi, fimask, exclFlat, slotOf,
-               slotAtom, frozen, px, py, pz, o);
+               slotAtom, frozen, px, py, pz, origin, o);
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) cand += __shfl_xor_sync(0xffffffffu, cand, off);
   if (lane == 0) {
