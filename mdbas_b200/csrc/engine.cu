@@ -191,6 +191,13 @@ int mdbas::engine_resolve_build(mdbas_nb_engine *e) {
                            e->stream));
   MDB_CUDA(cudaStreamSynchronize(e->stream));
   if (!(sticky & (CL_OVERFLOW | CL_NONFINITE))) return MDBAS_NB_OK;
+  return engine_settle_build(e, sticky);
+}
+
+// A pending build's error word read back with a failure in it: a list that
+// outgrew its room is rebuilt with room (and evaluated again if it had been);
+// a non-finite position is reported.
+int mdbas::engine_settle_build(mdbas_nb_engine *e, long long sticky) {
   MDB_CUDA(cudaMemsetAsync(e->cl.sticky.p, 0, sizeof(long long), e->stream));
   if (sticky & CL_NONFINITE) {
     e->built = false;
@@ -530,32 +537,48 @@ int mdbas_nb_engine_get_forces(mdbas_nb_engine *e, double *fx, double *fy, doubl
   if (!e || !fx || !fy || !fz) return MDBAS_NB_ERR_ARG;
   if (!e->computed) return MDBAS_NB_ERR_STATE;
   ENG_TRY(e, set_dev(e));
-  ENG_TRY(e, engine_resolve_build(e));
+  // Host arrays after a build that did not wait for its counts: the build's
+  // error word is read with the forces and the energy words, one wait for all
+  // three; a build that failed is settled (rebuilt and evaluated again) and
+  // the copies are made once more.
+  const bool settleAfter = !device_ptrs && e->buildPending;
+  if (!settleAfter) ENG_TRY(e, engine_resolve_build(e));
   LaunchScope ls(e);
   const int n = e->n;
   cudaStream_t s = e->stream;
-  double *src;
-  if (e->cfg.precision == 0) {
-    src = e->f64.as<double>();
-  } else {
-    ENG_TRY(e, e->fout.ensure(sizeof(double) * 3 * (size_t)n));
-    src = e->fout.as<double>();
-    ENG_TRY(e, forces_out_launch(e->cl, n, 0, src, src + n, src + 2 * (size_t)n, s));
+  for (int pass = 0;; ++pass) {
+    double *src;
+    if (e->cfg.precision == 0) {
+      src = e->f64.as<double>();
+    } else {
+      ENG_TRY(e, e->fout.ensure(sizeof(double) * 3 * (size_t)n));
+      src = e->fout.as<double>();
+      ENG_TRY(e, forces_out_launch(e->cl, n, 0, src, src + n, src + 2 * (size_t)n, s));
+    }
+    const cudaMemcpyKind k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    MDB_CUDA(cudaMemcpyAsync(fx, src, sizeof(double) * n, k, s));
+    MDB_CUDA(cudaMemcpyAsync(fy, src + n, sizeof(double) * n, k, s));
+    MDB_CUDA(cudaMemcpyAsync(fz, src + 2 * (size_t)n, sizeof(double) * n, k, s));
+    if (device_ptrs) return MDBAS_NB_OK;
+    // the energy words ride along with the forces: one wait for both, and the
+    // fixed-point error bits checked here too
+    if (e->cfg.precision == 0)
+      MDB_CUDA(cudaMemcpyAsync(e->acc64Cache, e->acc64.p, sizeof(e->acc64Cache),
+                               cudaMemcpyDeviceToHost, s));
+    else
+      MDB_CUDA(cudaMemcpyAsync(e->accCache, e->cl.acc.p, sizeof(e->accCache),
+                               cudaMemcpyDeviceToHost, s));
+    long long sticky = 0;
+    const bool settle = settleAfter && pass == 0 && e->buildPending;
+    if (settle)
+      MDB_CUDA(cudaMemcpyAsync(&sticky, e->cl.sticky.p, sizeof(sticky), cudaMemcpyDeviceToHost,
+                               s));
+    MDB_CUDA(cudaStreamSynchronize(s));
+    if (!settle) break;
+    e->buildPending = false;
+    if (!(sticky & (CL_OVERFLOW | CL_NONFINITE))) break;
+    ENG_TRY(e, engine_settle_build(e, sticky));
   }
-  const cudaMemcpyKind k = device_ptrs ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  MDB_CUDA(cudaMemcpyAsync(fx, src, sizeof(double) * n, k, s));
-  MDB_CUDA(cudaMemcpyAsync(fy, src + n, sizeof(double) * n, k, s));
-  MDB_CUDA(cudaMemcpyAsync(fz, src + 2 * (size_t)n, sizeof(double) * n, k, s));
-  if (device_ptrs) return MDBAS_NB_OK;
-  // the energy words ride along with the forces: one wait for both, and the
-  // fixed-point error bits checked here too
-  if (e->cfg.precision == 0)
-    MDB_CUDA(cudaMemcpyAsync(e->acc64Cache, e->acc64.p, sizeof(e->acc64Cache),
-                             cudaMemcpyDeviceToHost, s));
-  else
-    MDB_CUDA(cudaMemcpyAsync(e->accCache, e->cl.acc.p, sizeof(e->accCache),
-                             cudaMemcpyDeviceToHost, s));
-  MDB_CUDA(cudaStreamSynchronize(s));
   e->accCached = true;
   return acc_status(e);
 }

@@ -126,6 +126,8 @@ int md_kspace(mdbas_nb_engine *e, double *f, cudaStream_t s);
 // overflowing list build again with room, synchronously, and redo the
 // evaluation if one ran on the empty list; non-finite positions are an error.
 int engine_resolve_build(mdbas_nb_engine *e);
+// Settle a pending build whose error word (already read) holds a failure.
+int engine_settle_build(mdbas_nb_engine *e, long long sticky);
 // The engine's side stream and its fork/join events (created once, outside
 // any stream capture).
 int engine_side_stream(mdbas_nb_engine *e);
