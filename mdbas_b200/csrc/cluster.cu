@@ -153,12 +153,112 @@ __global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
 
 // One column per block: its atoms in ascending (z, atom index) order into
 // the column's slots, padding slots set to -1.  Columns of up to 1,024 atoms
-// are sorted in shared memory by a bitonic network (keys padded to a power
-// of two with +inf); longer ones by rank counting.  Both give the same total
-// order, so the same slots.
-__global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
-                           const int *__restrict__ colPadStart, const int *__restrict__ tmpIdx,
-                           const double *__restrict__ atomZ, int *__restrict__ slotAtom) {
+// are sorted by a bitonic network over 256, 512 or 1,024 keys (padded with
+// +inf) held in registers, R = 1, 2 or 4 per thread (element t + 256 r):
+// partners within a warp are exchanged by shuffles, partners in another warp
+// through shared memory, partners in the same thread directly.  Longer
+// columns are sorted by rank counting.  Both give the same total order, so
+// the same slots.
+__device__ __forceinline__ bool key_less(double za, int ia, double zb, int ib) {
+  return za < zb || (za == zb && ia < ib);
+}
+template <int R>
+__device__ __forceinline__ void col_bitonic(double (&key)[R], int (&idx)[R], double *xz, int *xi) {
+  constexpr int P = 256 * R;
+  const int t = threadIdx.x;
+  // fully unrolled: every partner index below is a constant, so the keys stay
+  // in registers
+#pragma unroll
+  for (int k = 2; k <= P; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      if (j >= 256) {
+        const int rj = j >> 8;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int rp = r ^ rj;
+          if (rp > r) {
+            // element t + 256 r is the lower of the pair
+            const bool asc = ((t + 256 * r) & k) == 0;
+            if (key_less(key[rp], idx[rp], key[r], idx[r]) == asc) {
+              const double kz = key[r];
+              const int ki = idx[r];
+              key[r] = key[rp];
+              idx[r] = idx[rp];
+              key[rp] = kz;
+              idx[rp] = ki;
+            }
+          }
+        }
+      } else {
+        double pz[R];
+        int pi[R];
+        if (j >= 32) {
+          __syncthreads();  // the previous exchange's reads are done
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            xz[t + 256 * r] = key[r];
+            xi[t + 256 * r] = idx[r];
+          }
+          __syncthreads();
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            pz[r] = xz[(t + 256 * r) ^ j];
+            pi[r] = xi[(t + 256 * r) ^ j];
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < R; ++r) {
+            pz[r] = __shfl_xor_sync(0xffffffffu, key[r], j);
+            pi[r] = __shfl_xor_sync(0xffffffffu, idx[r], j);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const int e = t + 256 * r;
+          // the lower element of an ascending pair keeps the smaller key, the
+          // upper one the larger; a descending pair the other way round
+          const bool wantMin = ((e & j) == 0) == ((e & k) == 0);
+          const bool take = wantMin ? key_less(pz[r], pi[r], key[r], idx[r])
+                                    : key_less(key[r], idx[r], pz[r], pi[r]);
+          if (take) {
+            key[r] = pz[r];
+            idx[r] = pi[r];
+          }
+        }
+      }
+    }
+  }
+}
+template <int R>
+__device__ __forceinline__ void col_sort_small(int n, int s, int ps, const int *__restrict__ tmpIdx,
+                                               const double *__restrict__ atomZ,
+                                               int *__restrict__ slotAtom, double *xz, int *xi) {
+  double key[R];
+  int idx[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = threadIdx.x + 256 * r;
+    if (e < n) {
+      idx[r] = tmpIdx[s + e];
+      key[r] = atomZ[idx[r]];
+    } else {
+      idx[r] = 0x7fffffff;
+      key[r] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    }
+  }
+  col_bitonic<R>(key, idx, xz, xi);
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int e = threadIdx.x + 256 * r;
+    if (e < n) slotAtom[ps + e] = idx[r];
+  }
+}
+
+__global__ void __launch_bounds__(256)
+k_col_sort(int nCols, const int *__restrict__ colStart,
+           const int *__restrict__ colPadStart, const int *__restrict__ tmpIdx,
+           const double *__restrict__ atomZ, int *__restrict__ slotAtom) {
   constexpr int kMax = 1024;
   __shared__ double sz[kMax];
   __shared__ int si[kMax];
@@ -167,41 +267,12 @@ __global__ void k_col_sort(int nCols, const int *__restrict__ colStart,
   const int s = colStart[c], e = colStart[c + 1];
   const int ps = colPadStart[c], pe = colPadStart[c + 1];
   const int n = e - s;
-  if (n <= kMax) {
-    int P = 2;
-    while (P < n) P <<= 1;
-    for (int t = threadIdx.x; t < P; t += blockDim.x) {
-      if (t < n) {
-        const int a = tmpIdx[s + t];
-        si[t] = a;
-        sz[t] = atomZ[a];
-      } else {
-        si[t] = 0x7fffffff;
-        sz[t] = __longlong_as_double(0x7ff0000000000000LL);  // +inf
-      }
-    }
-    __syncthreads();
-    for (int k = 2; k <= P; k <<= 1) {
-      for (int j = k >> 1; j > 0; j >>= 1) {
-        for (int t = threadIdx.x; t < P; t += blockDim.x) {
-          const int u = t ^ j;
-          if (u > t) {
-            const double zt = sz[t], zu = sz[u];
-            const int it = si[t], iu = si[u];
-            const bool uLess = (zu < zt) || (zu == zt && iu < it);
-            // ascending where (t & k) == 0, descending elsewhere
-            if (uLess == ((t & k) == 0)) {
-              sz[t] = zu;
-              sz[u] = zt;
-              si[t] = iu;
-              si[u] = it;
-            }
-          }
-        }
-        __syncthreads();
-      }
-    }
-    for (int t = threadIdx.x; t < n; t += blockDim.x) slotAtom[ps + t] = si[t];
+  if (n <= 256) {
+    col_sort_small<1>(n, s, ps, tmpIdx, atomZ, slotAtom, sz, si);
+  } else if (n <= 512) {
+    col_sort_small<2>(n, s, ps, tmpIdx, atomZ, slotAtom, sz, si);
+  } else if (n <= kMax) {
+    col_sort_small<4>(n, s, ps, tmpIdx, atomZ, slotAtom, sz, si);
   } else {
     for (int base = s; base < e; base += blockDim.x) {
       const int m = base + threadIdx.x;
