@@ -338,18 +338,21 @@ __global__ void k_clusters(const int *__restrict__ nSlotsDev,
   const int c = t / kClusterSize, k = t % kClusterSize;
   // every lane takes part in the shuffles; lanes past the last cluster only
   // do that (8-lane groups are whole clusters: blockDim is a multiple of 32)
+  // the slot loads do not wait for the slot count: the grid covers slotCap
+  // slots, all allocated (those past the count are not used)
   const bool active = c < (*nSlotsDev >> 3);
   // a cluster's first slot always holds an atom (columns are padded at the end)
-  const int a0 = active ? slotAtom[c * kClusterSize] : 0;
+  const int a0s = slotAtom[c * kClusterSize], as = slotAtom[t];
+  const int a0 = active ? a0s : 0;
   const int rep = (active && atomRep) ? atomRep[a0] : 0;
   const ClusterGeom &g = geoms[rep];
-  const int a = active ? slotAtom[t] : -1;
+  const int a = active ? as : -1;
   double px = 0., py = 0., pz = 0.;
   double lx = 1e300, ly = 1e300, lz = 1e300, hx = -1e300, hy = -1e300, hz = -1e300;
   if (a >= 0) {
-    px = wrap_pos(x[a], g.Lx, 1.0 / g.Lx);
-    py = wrap_pos(y[a], g.Ly, 1.0 / g.Ly);
-    pz = wrap_pos(z[a], g.Lz, 1.0 / g.Lz);
+    px = wrap_pos(x[a], g.Lx, g.invLx);
+    py = wrap_pos(y[a], g.Ly, g.invLy);
+    pz = wrap_pos(z[a], g.Lz, g.invLz);
     lx = hx = px;
     ly = hy = py;
     lz = hz = pz;
@@ -717,14 +720,23 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
 // search reads a z window's range from two entries of this table instead of
 // two binary searches over the column; a conservative bin on either side
 // keeps the range a superset, and the bounding-box test that follows drops
-// the extra clusters.  One block per column, one thread per bin.
+// the extra clusters.  One block per column, one thread per bin, binary
+// searches over the column's origins staged in shared memory.
 __global__ void __launch_bounds__((kZBins + 32) & ~31)
 k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restrict__ clusterRep,
            const int *__restrict__ colClStart, const float4 *__restrict__ originF,
            int *__restrict__ zTab) {
+  // the column's origin z in shared memory (one load each) when they fit
+  constexpr int kStaged = 512;
+  __shared__ float oz[kStaged];
   const int col = blockIdx.x, b = threadIdx.x;
-  if (col >= nCols || b > kZBins) return;
+  if (col >= nCols) return;
   const int cs = colClStart[col], ce = colClStart[col + 1];
+  const bool staged = ce - cs <= kStaged;
+  if (staged)
+    for (int k = threadIdx.x; k < ce - cs; k += blockDim.x) oz[k] = originF[cs + k].z;
+  __syncthreads();
+  if (b > kZBins) return;
   int a = cs;
   if (b == kZBins) {
     a = ce;
@@ -734,7 +746,7 @@ k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restri
     int hi = ce;
     while (a < hi) {  // first origin z >= zb
       const int mid = (a + hi) >> 1;
-      if (originF[mid].z < zb) a = mid + 1; else hi = mid;
+      if ((staged ? oz[mid - cs] : originF[mid].z) < zb) a = mid + 1; else hi = mid;
     }
   }
   zTab[(size_t)col * (kZBins + 1) + b] = a;
@@ -1166,6 +1178,9 @@ int make_geom(const DevBox &b, int n, double cutOff, double delr, int listRule, 
   g.Lx = b.a1;
   g.Ly = (b.type == CUBIC) ? b.a1 : b.b2;
   g.Lz = (b.type == CUBIC) ? b.a1 : b.c3;
+  g.invLx = 1.0 / g.Lx;
+  g.invLy = 1.0 / g.Ly;
+  g.invLz = 1.0 / g.Lz;
   const double rlist = cutOff + delr;
   // The pair kernel relies on a unique image within the cut-off.
   if (std::min(g.Lx, std::min(g.Ly, g.Lz)) <= 2.0 * cutOff) return MDBAS_NB_ERR_BOX;

@@ -25,6 +25,7 @@ struct ClusterGeom {
   int ncx, ncy;       // cells per side in x and y
   int Dx, Dy;         // cell offsets searched on each side
   double Lx, Ly, Lz;  // orthorhombic box edges
+  double invLx, invLy, invLz;  // 1 / edge (the FP64 quotient the device would form)
   double wx, wy;      // cell widths
   float rlist2;       // candidate test: rhi2
   float rlo2, rhi2;   // FP32 band around the list radius
