@@ -181,6 +181,41 @@ def water_box(n_molecules: int, box: float, seed: int = 1, jitter: float = 0.5,
     return sysm
 
 
+def water_box_ortho(lengths, seed: int = 1, jitter: float = 0.5,
+                    density: float = WATER_DENSITY, name: str | None = None) -> System:
+    """Rigid water filling an orthorhombic box (edges Lx, Ly, Lz): molecule
+    centres on a full nx x ny x nz lattice (n_a = round(L_a * density^(1/3)),
+    spacing L_a / n_a) with seeded jitter and random orientations, the same
+    molecule as water_box.  The box rows are in meta["cell"]."""
+    rng = np.random.default_rng(seed)
+    L = np.asarray(lengths, dtype=np.float64)
+    nl = np.maximum(1, np.rint(L * density ** (1.0 / 3.0)).astype(int))
+    spacing = L / nl
+    i, j, k = np.meshgrid(np.arange(nl[0]), np.arange(nl[1]), np.arange(nl[2]), indexing="ij")
+    centres = (np.stack([i.ravel(), j.ravel(), k.ravel()], 1) + 0.5) * spacing - 0.5 * L
+    m = centres.shape[0]
+    centres += rng.uniform(-jitter, jitter, size=(m, 3))
+    half = 0.5 * WATER_THETA
+    body = np.array([[0.0, 0.0, 0.0],
+                     [WATER_ROH * math.cos(half), WATER_ROH * math.sin(half), 0.0],
+                     [WATER_ROH * math.cos(half), -WATER_ROH * math.sin(half), 0.0]])
+    rot = _random_rotations(rng, m)
+    pos = (centres[:, None, :] + np.einsum('mij,aj->mai', rot, body)).reshape(-1, 3)
+    pos = pos - L * np.floor(pos / L + 0.5)
+    q = np.tile(np.array(WATER_Q), m)
+    eps = np.tile(np.array([math.sqrt(WATER_EPS_KCAL * KCAL_TO_IU), 0.0, 0.0]), m)
+    sig = np.tile(np.array([0.5 * WATER_SIGMA, 0.0, 0.0]), m)
+    mass = np.tile(np.array(WATER_MASS), m)
+    base = 3 * np.arange(m, dtype=np.int32)
+    bonds = np.stack([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1)],
+                     1).reshape(-1, 2).astype(np.int32)
+    angles = np.stack([base + 1, base, base + 2], 1).astype(np.int32)
+    cell = [L[0], 0.0, 0.0, 0.0, L[1], 0.0, 0.0, 0.0, L[2]]
+    return System(name or f"water{3 * m}_ortho", float(L[0]), pos[:, 0].copy(),
+                  pos[:, 1].copy(), pos[:, 2].copy(), q, eps, sig, mass, bonds, angles,
+                  meta={"molecules": m, "seed": seed, "cell": cell})
+
+
 def water_box_for_atoms(n_atoms: int, seed: int = 1, density: float = WATER_DENSITY,
                         **kw) -> System:
     """Water box holding n_atoms (a multiple of 3) at the given density."""

@@ -37,7 +37,7 @@ def _mdbas_pairs(r):
 
 def _engine_pairs(eng, n):
     p = eng.export_pairs(BIG).astype(np.int64)
-    keys = p[:, 0] * n + p[:, 1]
+    keys = np.minimum(p[:, 0], p[:, 1]) * n + np.maximum(p[:, 0], p[:, 1])
     return np.sort(keys)
 
 
@@ -45,6 +45,32 @@ def _same(a, b):
     assert len(a) == len(b), (len(a), len(b))
     assert np.array_equal(a, b)
     assert len(np.unique(a)) == len(a), "a pair listed twice"
+
+
+def _images_of_thin_box(keys, n, x, y, z, lengths, rlist=14.0):
+    """The cluster list keeps a pair once per periodic image within the list
+    radius, with the image's shift in the entry; in a box thinner than twice
+    the list radius (but thicker than twice the cut-off, so the pair kernel
+    still sees one image) a pair can have two.  MDBas's list holds the
+    minimum image only.  Checks that every pair listed twice has a second
+    image within the list radius, and returns the keys once each."""
+    u, cnt = np.unique(keys, return_counts=True)
+    assert cnt.max(initial=1) <= 2
+    dup = u[cnt == 2]
+    i, j = dup // n, dup % n
+    L = np.asarray(lengths, dtype=np.float64)
+    d = np.stack([x[j] - x[i], y[j] - y[i], z[j] - z[i]], 1)
+    d -= L * np.rint(d / L)
+    alt = np.full(len(dup), np.inf)
+    for sx in (-1, 0, 1):
+        for sy in (-1, 0, 1):
+            for sz in (-1, 0, 1):
+                if sx == sy == sz == 0:
+                    continue
+                e = d + L * np.array([sx, sy, sz])
+                alt = np.minimum(alt, (e * e).sum(1))
+    assert (alt <= (rlist + 1e-3) ** 2).all()
+    return u
 
 
 def _engine_on(r, s, **kw):
@@ -121,6 +147,61 @@ def test_cluster_list_96k(gpu):
     assert len(a) > 55_000_000
     eng.close()
     r.close()
+
+
+def test_cluster_list_tall_columns(gpu):
+    """A 25 x 25 x 700 A water box: 36 columns of ~1,200 atoms, so the
+    column sort ranks the columns over 1,024 atoms and sorts the others with
+    its 1,024-key network, and the search reads long z tables.  MDBas takes
+    its all-pairs builder (fewer than three link cells across x and y).  The
+    cluster list's pairs are MDBas's (the box is thinner than twice the list
+    radius: some pairs are listed in two images, MDBas's list has their
+    minimum image), and the forces and energies match its energy() within
+    the mixed tolerance."""
+    s = systems.water_box_ortho((25.0, 25.0, 700.0), seed=2)
+    cell = s.cell()
+    r = _reference(s, box_type=nb.ORBIC, cell=cell)
+    assert r.makelist() == 0
+    eng = _engine_on(r, s, box_type=nb.ORBIC, cell=cell)
+    eng.build()
+    x, y, z = r.positions()
+    got = _images_of_thin_box(_engine_pairs(eng, s.n), s.n, x, y, z, (25.0, 25.0, 700.0))
+    _same(got, _mdbas_pairs(r))
+    eng.compute()
+    f, e = eng.forces(), eng.energies()
+    rfx, rfy, rfz, re = r.energy()
+    assert force_rel_rms(f, (rfx, rfy, rfz)) < 1e-5
+    elec = e["elec_direct"] + e["elec_corr"]
+    assert abs(elec - re["elec"]) <= 1e-5 * abs(re["elec"])
+    assert abs(e["vdw"] - re["vdw"]) <= 1e-5 * abs(re["vdw"])
+    eng.close()
+    r.close()
+
+
+def test_cluster_list_very_tall_columns(gpu):
+    """A 25 x 25 x 2,600 A water box: columns of ~4,500 atoms (over 512
+    clusters each, more than the z-table kernel stages in shared memory).
+    Too large for MDBas's all-pairs builder on one core, so the cluster list
+    is compared with the FP64 form's list (MDBas's own order and pair set,
+    pinned to MDBas by the list tests) and the forces with the FP64 form's."""
+    s = systems.water_box_ortho((25.0, 25.0, 2600.0), seed=3)
+    cell = s.cell()
+    eng = nb.Engine(s, precision=1, box_type=nb.ORBIC, cell=cell)
+    ref = nb.Engine(s, precision=0, box_type=nb.ORBIC, cell=cell)
+    eng.build()
+    ref.build()
+    got = _images_of_thin_box(_engine_pairs(eng, s.n), s.n, s.x, s.y, s.z, (25.0, 25.0, 2600.0))
+    _same(got, _engine_pairs(ref, s.n))
+    eng.compute()
+    ref.compute()
+    assert force_rel_rms(eng.forces(), ref.forces()) < 1e-5
+    e, e0 = eng.energies(), ref.energies()
+    # the mixed form counts the pairs within its FP32 rc^2: a few at 12 A
+    # fall on the other side of the FP64 test
+    assert abs(e["n_pairs"] - e0["n_pairs"]) <= 1e-6 * e0["n_pairs"]
+    assert abs(e["vdw"] - e0["vdw"]) <= 1e-5 * abs(e0["vdw"])
+    eng.close()
+    ref.close()
 
 
 def test_mixed_dropin_all_pairs_half_rows(gpu):
