@@ -997,11 +997,9 @@ def run_ours(args, rank, world):
     hx[:], hy[:], hz[:] = s.x, s.y, s.z
 
     def step_e2e():
-        eng.set_positions(hx, hy, hz)
-        eng.build()
-        eng.compute()
-        eng.forces_into(fx, fy, fz)
-        eng.energies()
+        # one C-ABI call: positions H2D, list build, forces, forces D2H and
+        # the energy words, one wait
+        eng.evaluate(hx, hy, hz, fx, fy, fz, rebuild=True)
 
     for _ in range(2):
         step_e2e()
@@ -1166,7 +1164,9 @@ def run_ours(args, rank, world):
             "e2e_dropin": dropin,
             "e2e": {"value": e2e_value, "unit": "pairs/s", "ms_per_step": t_e2e,
                     "h2d_bytes_per_step": 3 * 8 * n,
-                    "d2h_bytes_per_step": 3 * 8 * n + 8 * 8},
+                    # forces, the eight energy/flag words, the build's error word
+                    "d2h_bytes_per_step": 3 * 8 * n + 8 * 8 + 8,
+                    "call": "mdbas_nb_engine_evaluate (host arrays, one call per step)"},
             "gpu_launches": int(launches),
             "clocks": clk,
             "cpu_baseline": cpu,

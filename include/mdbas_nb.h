@@ -396,6 +396,14 @@ int mdbas_nb_engine_compute(mdbas_nb_engine *e);
 int mdbas_nb_engine_get_forces(mdbas_nb_engine *e, double *fx, double *fy, double *fz,
                                int device_ptrs);
 int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out);
+/* One evaluation on host arrays in a single call: set_positions (host), then
+ * build (rebuild != 0) or refresh (rebuild == 0: the atoms are within half
+ * the skin of the last build), compute, get_forces into fx/fy/fz and, when
+ * out is not NULL, energies; one wait.  The same results as those calls made
+ * one by one. */
+int mdbas_nb_engine_evaluate(mdbas_nb_engine *e, const double *x, const double *y,
+                             const double *z, int rebuild, double *fx, double *fy, double *fz,
+                             mdbas_nb_energies *out);
 /* Statistics of the current list: out[0] = clusters (or atoms), out[1] =
  * list entries (cluster pairs or atom pairs), out[2] = candidate atom pairs
  * evaluated per compute, out[3] = list capacity. */

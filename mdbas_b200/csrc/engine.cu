@@ -624,6 +624,21 @@ int mdbas_nb_engine_energies(mdbas_nb_engine *e, mdbas_nb_energies *out) {
   return acc_status(e);
 }
 
+int mdbas_nb_engine_evaluate(mdbas_nb_engine *e, const double *x, const double *y,
+                             const double *z, int rebuild, double *fx, double *fy, double *fz,
+                             mdbas_nb_energies *out) {
+  if (!e || !x || !y || !z || !fx || !fy || !fz) return MDBAS_NB_ERR_ARG;
+  int st = mdbas_nb_engine_set_positions(e, x, y, z, 0);
+  if (st != MDBAS_NB_OK) return st;
+  st = (rebuild || !e->built) ? mdbas_nb_engine_build(e) : mdbas_nb_engine_refresh(e);
+  if (st != MDBAS_NB_OK) return st;
+  st = mdbas_nb_engine_compute(e);
+  if (st != MDBAS_NB_OK) return st;
+  st = mdbas_nb_engine_get_forces(e, fx, fy, fz, 0);
+  if (st != MDBAS_NB_OK || !out) return st;
+  return mdbas_nb_engine_energies(e, out);
+}
+
 int mdbas_nb_engine_list_stats(mdbas_nb_engine *e, long long out[4]) {
   if (!e || !out) return MDBAS_NB_ERR_ARG;
   if (!e->built) return MDBAS_NB_ERR_STATE;

@@ -205,6 +205,9 @@ def lib():
     L.mdbas_nb_engine_get_forces.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_int]
     L.mdbas_nb_engine_energies.argtypes = [C.c_void_p, C.POINTER(Energies)]
+    L.mdbas_nb_engine_evaluate.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.POINTER(Energies)]
     L.mdbas_nb_engine_list_stats.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
     L.mdbas_nb_engine_export_pairs.argtypes = [C.c_void_p, C.c_double, C.c_void_p, C.c_longlong,
                                                C.POINTER(C.c_longlong)]
@@ -446,6 +449,20 @@ class Engine:
     def energies(self) -> dict:
         e = Energies()
         check(lib().mdbas_nb_engine_energies(self.h, C.byref(e)), "engine_energies")
+        return {k: getattr(e, k) for k, _ in Energies._fields_}
+
+    def evaluate(self, x, y, z, fx, fy, fz, rebuild: bool = True) -> dict:
+        """One evaluation on host arrays in one C-ABI call (positions in,
+        forces into the caller's FP64 arrays fx/fy/fz, energies returned):
+        set_positions, build (or refresh), compute, get_forces, energies."""
+        self._pos = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z)]
+        for a in (fx, fy, fz):
+            if a.dtype != np.float64 or not a.flags.c_contiguous or a.shape[0] != self.n:
+                raise ValueError("forces need contiguous float64 arrays of n entries")
+        e = Energies()
+        check(lib().mdbas_nb_engine_evaluate(self.h, *(_ptr(a) for a in self._pos), int(rebuild),
+                                             _ptr(fx), _ptr(fy), _ptr(fz), C.byref(e)),
+              "engine_evaluate")
         return {k: getattr(e, k) for k, _ in Energies._fields_}
 
     def list_stats(self):

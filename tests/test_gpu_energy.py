@@ -245,6 +245,38 @@ def test_quad_kernel_in_pruned_dynamics(gpu):
     assert np.allclose(rows[4][:, 1:], rows[6][:, 1:], rtol=1e-6, atol=0.0)
 
 
+def test_evaluate_equals_separate_calls(gpu):
+    """mdbas_nb_engine_evaluate (positions in, forces and energies out, one
+    call) gives the results of set_positions + build/refresh + compute +
+    get_forces + energies made one by one, bit for bit, with a rebuild and
+    with a refresh after motion within the skin."""
+    s = systems.water_box_for_atoms(18558, seed=6)
+    a = nb.Engine(s, precision=1)
+    b = nb.Engine(s, precision=1)
+    rng = np.random.default_rng(11)
+    x, y, z = s.x.copy(), s.y.copy(), s.z.copy()
+    for rebuild in (True, False, True):
+        fx, fy, fz = (np.zeros(s.n) for _ in range(3))
+        ea = a.evaluate(x, y, z, fx, fy, fz, rebuild=rebuild)
+        b.set_positions(x, y, z)
+        if rebuild:
+            b.build()
+        else:
+            b.refresh()
+        b.compute()
+        gx, gy, gz = b.forces()
+        eb = b.energies()
+        for u, v in ((fx, gx), (fy, gy), (fz, gz)):
+            assert np.array_equal(u, v)
+        assert ea == eb
+        # move every atom by at most 0.3 A (within half the 2 A skin)
+        x, y, z = (v + rng.uniform(-0.3, 0.3, s.n) for v in (x, y, z))
+    with pytest.raises(ValueError):
+        a.evaluate(x, y, z, np.zeros(s.n, np.float32), fy, fz)
+    a.close()
+    b.close()
+
+
 def test_lean_half_kernel_matches_half(gpu):
     """The lean form of the half-cluster kernel (variant 7: masked pairs at
     r^2 = 1e30 instead of zeroed products, items from a counter) gives the
