@@ -1052,86 +1052,117 @@ __global__ void k_refresh(const int *__restrict__ nSlotsDev,
   p[6] = v.w;
 }
 
-// One warp per item of the list: recompute each entry's pairs within the
-// inner radius from the current layout (lane = (i atom, j atoms h and h + 4),
-// as in the search's bit order) and append the entry halves that keep a pair
-// to the inner list.
-__global__ void __launch_bounds__(128)
+// Per warp of the prune: the item's j atoms and its i atoms (negated and
+// paired, as the search stages them).
+struct PruneBuf {
+  float4 sj[kClusterSize * kItemMax];  // sj[a * kItemMax + entry]
+  float4 sn[kClusterSize];
+  float2 snz[kClusterSize];
+};
+constexpr int kPruneThreads = 128;
+
+// Rewrite the inner list at the current layout: one warp per item of the
+// list and one lane per entry, as in the search's flush.  The item's j atoms
+// are staged in shared memory, each lane forms its entry's 64 FP32 distances
+// (j atom plus the shift, minus the i atom, as the pair kernel does), shifts
+// the sign bits of (rin2 - r^2) into a word per half (bit i + 8 h) and keeps
+// the pairs the list mask holds.  The entry halves with a pair become the
+// item's inner entries, halves A first, at twice the entry index, and the
+// inner item takes the item's index: no room is taken and nothing can
+// overflow.  hcounters: [0] halves written, [1] items, [3] warp steps.
+__global__ void __launch_bounds__(kPruneThreads)
 k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
         const CPairEntry *__restrict__ entries, const uint2 *__restrict__ masks,
         const float4 *__restrict__ xq, float rin2, HalfEntry *__restrict__ hent,
         unsigned *__restrict__ hmask, int4 *__restrict__ hitems,
-        long long *__restrict__ hcounters, long long hEntryCap, long long hItemCap) {
+        long long *__restrict__ hcounters) {
+  __shared__ PruneBuf bufs[kPruneThreads / 32];
+  PruneBuf &B = bufs[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  const int il = lane & 7, jl = lane >> 3;
   const long long nItems = counters[1];
+  if (blockIdx.x == 0 && threadIdx.x == 0) hcounters[1] = nItems;
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const float2 rin = make_float2(rin2, rin2);
+  long long halves = 0, steps = 0;
   for (long long it = gw; it < nItems; it += nw) {
     const int4 item = items[it];
     const int ci = item.x, e0 = item.y, ne = item.z;
-    const float4 xi = xq[ci * kClusterSize + il];
-    uint2 mine = make_uint2(0u, 0u);
-    CPairEntry myEn{};
-    for (int k = 0; k < ne; ++k) {
-      const CPairEntry en = entries[e0 + k];
-      const uint2 mk = masks[e0 + k];
-      const float4 xa = xq[en.j * kClusterSize + jl], xb = xq[en.j * kClusterSize + jl + 4];
-      const float ax = xa.x + en.sx - xi.x, ay = xa.y + en.sy - xi.y, az = xa.z + en.sz - xi.z;
-      const float bx = xb.x + en.sx - xi.x, by = xb.y + en.sy - xi.y, bz = xb.z + en.sz - xi.z;
-      const bool ina = ((mk.x >> lane) & 1u) && (ax * ax + ay * ay + az * az <= rin2);
-      const bool inb = ((mk.y >> lane) & 1u) && (bx * bx + by * by + bz * bz <= rin2);
-      const unsigned lo = __ballot_sync(0xffffffffu, ina);
-      const unsigned hi = __ballot_sync(0xffffffffu, inb);
-      if (lane == k) {
-        mine = make_uint2(lo, hi);
-        myEn = en;
+    CPairEntry en{};
+    uint2 mk = make_uint2(0u, 0u);
+    if (lane < ne) {
+      en = entries[e0 + lane];
+      mk = masks[e0 + lane];
+    }
+    if (lane < kClusterSize) {
+      const float4 xi = xq[ci * kClusterSize + lane];
+      B.sn[lane] = make_float4(-xi.x, -xi.x, -xi.y, -xi.y);
+      B.snz[lane] = make_float2(-xi.z, -xi.z);
+    }
+#pragma unroll
+    for (int r = 0; r < kClusterSize; ++r) {
+      const int idx = lane + 32 * r, k = idx >> 3, a = idx & 7;
+      const int jk = __shfl_sync(0xffffffffu, en.j, k);
+      if (k < ne) B.sj[a * kItemMax + k] = xq[jk * kClusterSize + a];
+    }
+    __syncwarp();
+    unsigned in0 = 0u, in1 = 0u;  // set bits: beyond the inner radius
+    if (lane < ne) {
+#pragma unroll 1
+      for (int h = 3; h >= 0; --h) {
+        const float4 pa = B.sj[h * kItemMax + lane], pb = B.sj[(h + 4) * kItemMax + lane];
+        const float2 jx = make_float2(pa.x + en.sx, pb.x + en.sx);
+        const float2 jy = make_float2(pa.y + en.sy, pb.y + en.sy);
+        const float2 jz = make_float2(pa.z + en.sz, pb.z + en.sz);
+#pragma unroll
+        for (int i = kClusterSize - 1; i >= 0; --i) {
+          const float4 nxy = lds_keep(&B.sn[i]);
+          const float2 dx = __fadd2_rn(jx, make_float2(nxy.x, nxy.y));
+          const float2 dy = __fadd2_rn(jy, make_float2(nxy.z, nxy.w));
+          const float2 dz = __fadd2_rn(jz, lds_keep(&B.snz[i]));
+          const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+          const float2 d = __ffma2_rn(r2, make_float2(-1.f, -1.f), rin);
+          in0 = __funnelshift_l(__float_as_uint(d.x), in0, 1);
+          in1 = __funnelshift_l(__float_as_uint(d.y), in1, 1);
+        }
       }
+      in0 = ~in0 & mk.x;
+      in1 = ~in1 & mk.y;
     }
-    const unsigned hA = __ballot_sync(0xffffffffu, lane < ne && mine.x != 0u);
-    const unsigned hB = __ballot_sync(0xffffffffu, lane < ne && mine.y != 0u);
+    __syncwarp();  // every lane is done with B before the next item's staging
+    const unsigned hA = __ballot_sync(0xffffffffu, in0 != 0u);
+    const unsigned hB = __ballot_sync(0xffffffffu, in1 != 0u);
     const int nA = __popc(hA), nin = nA + __popc(hB);
-    if (nin == 0) continue;
-    long long h0 = 0, io = 0;
-    if (lane == 0) {
-      h0 = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 0),
-                                (unsigned long long)nin);
-      io = (long long)atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 1), 1ull);
-    }
-    h0 = __shfl_sync(0xffffffffu, h0, 0);
-    io = __shfl_sync(0xffffffffu, io, 0);
-    if (h0 + nin > hEntryCap || io >= hItemCap) {
-      if (lane == 0)
-        atomicOr(reinterpret_cast<unsigned long long *>(hcounters + 2),
-                 (unsigned long long)CL_OVERFLOW);
-      continue;
-    }
     const unsigned lt = (1u << lane) - 1u;
-    if (lane < ne && mine.x != 0u) {
-      const long long q = h0 + __popc(hA & lt);
+    if (in0 != 0u) {
+      const long long q = 2 * (long long)e0 + __popc(hA & lt);
       HalfEntry he;
-      he.jh = 2 * myEn.j;
-      he.sx = myEn.sx;
-      he.sy = myEn.sy;
-      he.sz = myEn.sz;
+      he.jh = 2 * en.j;
+      he.sx = en.sx;
+      he.sy = en.sy;
+      he.sz = en.sz;
       hent[q] = he;
-      hmask[q] = mine.x;
+      hmask[q] = in0;
     }
-    if (lane < ne && mine.y != 0u) {
-      const long long q = h0 + nA + __popc(hB & lt);
+    if (in1 != 0u) {
+      const long long q = 2 * (long long)e0 + nA + __popc(hB & lt);
       HalfEntry he;
-      he.jh = 2 * myEn.j + 1;
-      he.sx = myEn.sx;
-      he.sy = myEn.sy;
-      he.sz = myEn.sz;
+      he.jh = 2 * en.j + 1;
+      he.sx = en.sx;
+      he.sy = en.sy;
+      he.sz = en.sz;
       hent[q] = he;
-      hmask[q] = mine.y;
+      hmask[q] = in1;
     }
     if (lane == 0) {
-      hitems[io] = make_int4(ci, (int)h0, nin, 0);
-      atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 3),
-                (unsigned long long)((nin + 1) >> 1));
+      hitems[it] = make_int4(ci, 2 * e0, nin, 0);
+      halves += nin;
+      steps += (nin + 1) >> 1;
     }
+  }
+  if (lane == 0 && halves > 0) {
+    atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 0), (unsigned long long)halves);
+    atomicAdd(reinterpret_cast<unsigned long long *>(hcounters + 3), (unsigned long long)steps);
   }
 }
 
@@ -1469,10 +1500,10 @@ int cluster_prune(ClusterWork &w, float rin2, cudaStream_t s) {
   MDB_CUDA(cudaGetDevice(&dev));
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
-  MDB_LAUNCH(k_prune, sms * 16, 128, 0, s, w.counters.as<long long>(), w.items.as<int4>(),
-             w.entries.as<CPairEntry>(), w.masks.as<uint2>(), w.xq.as<float4>(), rin2,
-             w.entriesIn.as<HalfEntry>(), w.masksIn.as<unsigned>(), w.itemsIn.as<int4>(),
-             w.countersIn.as<long long>(), w.inEntryCap, w.inItemCap);
+  MDB_LAUNCH(k_prune, sms * 16, kPruneThreads, 0, s, w.counters.as<long long>(),
+             w.items.as<int4>(), w.entries.as<CPairEntry>(), w.masks.as<uint2>(),
+             w.xq.as<float4>(), rin2, w.entriesIn.as<HalfEntry>(), w.masksIn.as<unsigned>(),
+             w.itemsIn.as<int4>(), w.countersIn.as<long long>());
   MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.countersIn.as<long long>(),
              w.sticky.as<long long>());
   w.innerRin2 = rin2;
