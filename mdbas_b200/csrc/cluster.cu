@@ -932,21 +932,25 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
     }
     const int total = __shfl_sync(0xffffffffu, incl, 31);
     __syncwarp();
+    int k0 = 0;  // the listed range holding flat index b0
     for (int b0 = 0; b0 < total; b0 += 32) {
       const int t = b0 + lane;
       const bool valid = t < total;
       int cj = 0, sx = 0, sy = 0, sz = 0;
       float4 oj = make_float4(0.f, 0.f, 1e30f, 0.f);
       float4 hj = make_float4(0.f, 0.f, 0.f, 0.f);
+      // The range holding flat index t: lane j reads where range k0 + j ends,
+      // relative to b0 (at least 1: range k0 holds b0), and marks that bit;
+      // t's range is k0 plus the ranges that end at or before t.  At most 32
+      // ranges end within a round (ranges are not empty).
+      const int kj = k0 + lane + 1;
+      const int ej = kj <= ncol ? B.rpre[kj] - b0 : 64;
+      const unsigned ends = __reduce_or_sync(0xffffffffu, (ej > 0 && ej < 32) ? 1u << ej : 0u);
+      const int rk = k0 + __popc(ends & ((2u << lane) - 1u));
+      k0 += __popc(__ballot_sync(0xffffffffu, ej <= 32));
       if (valid) {
-        // the listed range holding flat index t
-        int lo = 0, hi2 = ncol - 1;
-        while (lo < hi2) {
-          const int mid = (lo + hi2 + 1) >> 1;
-          if (B.rpre[mid] <= t) lo = mid; else hi2 = mid - 1;
-        }
-        cj = B.rstart[lo] + (t - B.rpre[lo]);
-        const int rc = B.rcode[lo];
+        cj = B.rstart[rk] + (t - B.rpre[rk]);
+        const int rc = B.rcode[rk];
         sx = (rc & 3) - 1;
         sy = ((rc >> 2) & 3) - 1;
         sz = ((rc >> 4) & 3) - 1;
