@@ -546,19 +546,28 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
   const double4 oi = origin[ci];
   double4 oj = make_double4(0., 0., 0., 0.);
   if (lane < cnt) oj = origin[B.j[lane]];
+  // the j atoms straight into shared memory (asynchronous 16-byte copies:
+  // no registers hold them in flight)
 #pragma unroll
   for (int r = 0; r < kClusterSize; ++r) {
     const int idx = lane + 32 * r, k = idx >> 3, j = idx & 7;
-    if (k < cnt) B.sj[j * kItemMax + k] = xq[B.j[k] * kClusterSize + j];
+    if (k < cnt)
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(
+                       (unsigned)__cvta_generic_to_shared(&B.sj[j * kItemMax + k])),
+                   "l"(xq + (size_t)B.j[k] * kClusterSize + j)
+                   : "memory");
   }
-  __syncwarp();
+  // while the copies land: the entry's shift and its masks of padding slots,
+  // the cluster's own triangle, exclusions and frozen pairs
   uint2 inner = make_uint2(0u, 0u);
   CPairEntry en{};
-  int npin = 0;
+  int npin = 0, cj = 0, sidx = 0;
+  unsigned m0 = 0u, m1 = 0u;
   if (lane < cnt) {
-    const int k = lane;
-    const int cj = B.j[k], code = B.code[k];
-    const int sidx = code & 31, nrj = code >> 8;
+    const int code = B.code[lane];
+    cj = B.j[lane];
+    sidx = code & 31;
+    const int nrj = code >> 8;
     // the entry's shift, formed in FP64 and rounded once: the value the pair
     // kernel adds to the j atoms
     const int sx = sidx % 3 - 1, sy = (sidx / 3) % 3 - 1, sz = sidx / 9 - 1;
@@ -566,6 +575,42 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
     en.sx = (float)(oj.x + sx * g.Lx - oi.x);
     en.sy = (float)(oj.y + sy * g.Ly - oi.y);
     en.sz = (float)(oj.z + sz * g.Lz - oi.z);
+    // padding slots of either cluster
+    const unsigned irow = (nreal_i >= 8 ? 0xffu : ((1u << nreal_i) - 1u)) * 0x01010101u;
+    m0 = irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
+    m1 = irow & (nrj >= 8 ? 0xffffffffu : (nrj <= 4 ? 0u : ((1u << (8 * (nrj - 4))) - 1u)));
+    if (cj == ci && sidx == 13) {  // the cluster with itself: j > i
+      m0 &= 0x07030100u;
+      m1 &= 0x7f3f1f0fu;
+    }
+    if (cj >= pcLo && cj <= pcHi) {
+      for (int i = 0; i < kClusterSize; ++i) {
+        const int e0 = B.es[i], n = B.ee[i] - e0;
+        for (int r = 0; r < n; ++r) {
+          const int p = r < kExclRegs ? B.ps[i][r] : slotOf[__ldg(exclFlat + e0 + r)];
+          if ((p >> 3) == cj) {
+            const int j = p & 7;
+            if (j < 4) m0 &= ~(1u << (i + 8 * j));
+            else m1 &= ~(1u << (i + 8 * (j - 4)));
+          }
+        }
+      }
+    }
+    if (frozen && fimask) {
+      for (int j = 0; j < kClusterSize; ++j) {
+        const int ja = slotAtom[cj * kClusterSize + j];
+        if (ja >= 0 && frozen[ja]) {
+          const unsigned m = fimask << (8 * (j & 3));
+          if (j < 4) m0 &= ~m;
+          else m1 &= ~m;
+        }
+      }
+    }
+  }
+  asm volatile("cp.async.wait_all;" ::: "memory");
+  __syncwarp();
+  if (lane < cnt) {
+    const int k = lane;
     // Per pair the sign of (radius^2 - r^2), exact for the FP32 distance the
     // pair kernel forms (j atom plus the shift, minus the i atom), is shifted
     // into a word per radius and half: h from 3 down to 0, i from 7 down to
@@ -607,37 +652,6 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
     ca1 = ~ca1;
     in0 = ~in0;
     in1 = ~in1;
-    // padding slots of either cluster
-    const unsigned irow = (nreal_i >= 8 ? 0xffu : ((1u << nreal_i) - 1u)) * 0x01010101u;
-    unsigned m0 = irow & (nrj >= 4 ? 0xffffffffu : ((1u << (8 * nrj)) - 1u));
-    unsigned m1 = irow & (nrj >= 8 ? 0xffffffffu : (nrj <= 4 ? 0u : ((1u << (8 * (nrj - 4))) - 1u)));
-    if (cj == ci && sidx == 13) {  // the cluster with itself: j > i
-      m0 &= 0x07030100u;
-      m1 &= 0x7f3f1f0fu;
-    }
-    if (cj >= pcLo && cj <= pcHi) {
-      for (int i = 0; i < kClusterSize; ++i) {
-        const int e0 = B.es[i], n = B.ee[i] - e0;
-        for (int r = 0; r < n; ++r) {
-          const int p = r < kExclRegs ? B.ps[i][r] : slotOf[__ldg(exclFlat + e0 + r)];
-          if ((p >> 3) == cj) {
-            const int j = p & 7;
-            if (j < 4) m0 &= ~(1u << (i + 8 * j));
-            else m1 &= ~(1u << (i + 8 * (j - 4)));
-          }
-        }
-      }
-    }
-    if (frozen && fimask) {
-      for (int j = 0; j < kClusterSize; ++j) {
-        const int ja = slotAtom[cj * kClusterSize + j];
-        if (ja >= 0 && frozen[ja]) {
-          const unsigned m = fimask << (8 * (j & 3));
-          if (j < 4) m0 &= ~m;
-          else m1 &= ~m;
-        }
-      }
-    }
     // pairs in the band: MDBas's own FP64 distance decides
     unsigned amb0 = ca0 & ~lo0 & m0, amb1 = ca1 & ~lo1 & m1;
     unsigned fin0 = lo0 & m0, fin1 = lo1 & m1;
