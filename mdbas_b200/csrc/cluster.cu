@@ -734,17 +734,20 @@ __device__ void flush_item(WarpBuf &B, int cnt, int ci, int lane,
 // search reads a z window's range from two entries of this table instead of
 // two binary searches over the column; a conservative bin on either side
 // keeps the range a superset, and the bounding-box test that follows drops
-// the extra clusters.  One block per column, one thread per bin, binary
-// searches over the column's origins staged in shared memory.
+// the extra clusters.  The table is indexed by grid cell (colOff[r] + cy *
+// ncx + cx, the index of colRank), so the search reads it without going
+// through the column numbering.  One block per cell, one thread per bin,
+// binary searches over the column's origins staged in shared memory.
 __global__ void __launch_bounds__((kZBins + 32) & ~31)
 k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restrict__ clusterRep,
-           const int *__restrict__ colClStart, const float4 *__restrict__ originF,
-           int *__restrict__ zTab) {
+           const int *__restrict__ colRank, const int *__restrict__ colClStart,
+           const float4 *__restrict__ originF, int *__restrict__ zTab) {
   // the column's origin z in shared memory (one load each) when they fit
   constexpr int kStaged = 512;
   __shared__ float oz[kStaged];
-  const int col = blockIdx.x, b = threadIdx.x;
-  if (col >= nCols) return;
+  const int cell = blockIdx.x, b = threadIdx.x;
+  if (cell >= nCols) return;
+  const int col = colRank[cell];
   const int cs = colClStart[col], ce = colClStart[col + 1];
   const bool staged = ce - cs <= kStaged;
   if (staged)
@@ -763,7 +766,7 @@ k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restri
       if ((staged ? oz[mid - cs] : originF[mid].z) < zb) a = mid + 1; else hi = mid;
     }
   }
-  zTab[(size_t)col * (kZBins + 1) + b] = a;
+  zTab[(size_t)cell * (kZBins + 1) + b] = a;
 }
 
 // Cluster-pair search ("cell sweep"): one warp per i cluster.  The columns
@@ -784,8 +787,8 @@ k_col_ztab(int nCols, const ClusterGeom *__restrict__ geoms, const int *__restri
 __global__ void __launch_bounds__(kSearchThreads, 5)
 k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geoms,
          const DevBox *__restrict__ boxes, const int *__restrict__ clusterRep,
-         const int *__restrict__ colOff, const int *__restrict__ colRank,
-         const int *__restrict__ zTab, const int *__restrict__ clusterXY,
+         const int *__restrict__ colOff, const int *__restrict__ zTab,
+         const int *__restrict__ clusterXY,
          const double4 *__restrict__ origin, const float4 *__restrict__ originF,
          const float4 *__restrict__ half, const int *__restrict__ slotAtom,
          const int *__restrict__ slotOf, const int *__restrict__ frozen,
@@ -856,7 +859,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   for (int c0 = 0; c0 < ncomb; c0 += 32) {
     const int cb = c0 + lane;
     bool pass = false, zm = false, zp = false;
-    int code = 0, tab = 0, zbl = 0, zbh = 0;  // tab: the column's row of zTab
+    int code = 0, tab = 0, zbl = 0, zbh = 0;  // tab: the cell's row of zTab
     if (cb < ncomb) {
       const int dy = cb / nx - g.Dy, dx = cb % nx - g.Dx;
       int jy = cy + dy, sy = 0;
@@ -869,7 +872,7 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       const float gx = fmaxf(fmaxf(xlo - (oif.x + hi.x), (oif.x - hi.x) - xhi), 0.f);
       const float gxy2 = gx * gx + gy * gy;
       if (gxy2 <= rlist2) {
-        tab = colRank[colBase + jy * g.ncx + jx] * (kZBins + 1);
+        tab = (colBase + jy * g.ncx + jx) * (kZBins + 1);
         code = (sx + 1) | ((sy + 1) << 2);
         pass = true;
         // the z reach left over the column's x-y gap (a cluster's x-y extent
@@ -1396,8 +1399,9 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
              y, z, q, eps, sig, sqrtC, w.origin.as<double4>(), w.originF.as<float4>(),
              w.half.as<float4>(), w.xq.as<float4>(), w.lj.as<float2>(), w.xp.as<float>(),
              w.ljp.as<float>(), w.slotOf.as<int>(), w.clusterXY.as<int>(), w.hmax.as<int>());
-  MDB_LAUNCH(k_col_ztab, nCols, (kZBins + 32) & ~31, 0, s, nCols, gd, w.clusterRepDev(), w.colClStart.as<int>(),
-             w.originF.as<float4>(), w.zTab.as<int>());
+  MDB_LAUNCH(k_col_ztab, nCols, (kZBins + 32) & ~31, 0, s, nCols, gd, w.clusterRepDev(),
+             w.colRank.as<int>(), w.colClStart.as<int>(), w.originF.as<float4>(),
+             w.zTab.as<int>());
 
   // Cluster-pair search; in the synchronising form grow the list and search
   // again if it overflowed.  The inner list holds at most two halves per
@@ -1439,7 +1443,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[5], s));
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
                w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
-               w.colRank.as<int>(), w.zTab.as<int>(), w.clusterXY.as<int>(),
+               w.zTab.as<int>(), w.clusterXY.as<int>(),
                w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
                w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
                w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
