@@ -430,6 +430,26 @@ __device__ __forceinline__ void tri_vectors(const DevBox &b, const double (&px)[
   }
 }
 
+// Orthorhombic (and cubic) boxes: the minimum-image term dist() subtracts
+// from each component of a constraint vector, a box edge times -1, 0 or 1
+// (exact), fixed for the SHAKE iterations of one step (the corrections move
+// atoms by far less than half an edge); the iterations then form the vectors
+// without the conversions of the image test, with the same bits.
+__device__ __forceinline__ void tri_image_terms(const DevBox &b, const double (&px)[3],
+                                                const double (&py)[3], const double (&pz)[3],
+                                                double (&cx)[3], double (&cy)[3],
+                                                double (&cz)[3]) {
+  constexpr int LA[3] = {0, 0, 1}, LB[3] = {1, 2, 2};
+  const double ex = b.a1, ey = b.type == CUBIC ? b.a1 : b.b2, ez = b.type == CUBIC ? b.a1 : b.c3;
+  const double ux = b.u1, uy = b.type == CUBIC ? b.u1 : b.v2, uz = b.type == CUBIC ? b.u1 : b.w3;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    cx[k] = dmul(ex, (double)nint_d(dmul(px[LB[k]] - px[LA[k]], ux)));
+    cy[k] = dmul(ey, (double)nint_d(dmul(py[LB[k]] - py[LA[k]], uy)));
+    cz[k] = dmul(ez, (double)nint_d(dmul(pz[LB[k]] - pz[LA[k]], uz)));
+  }
+}
+
 __global__ void __launch_bounds__(128)
 k_tri_stage1(int nTri, const DevBox *__restrict__ boxes, const int *__restrict__ atomRep,
              double dt, double tol, int maxCycle,
@@ -475,10 +495,23 @@ k_tri_stage1(int nTri, const DevBox *__restrict__ boxes, const int *__restrict__
       py[i] += dt * qy[i];
       pz[i] += dt * qz[i];
     }
+    const bool ortho = b.type == CUBIC || b.type == ORBIC;
+    double cx[3] = {0., 0., 0.}, cy[3] = {0., 0., 0.}, cz[3] = {0., 0., 0.};
+    if (ortho) tri_image_terms(b, px, py, pz, cx, cy, cz);
     bool converged = false;
     do {
       double tx[3], ty[3], tz[3], rt2[3];
-      tri_vectors(b, px, py, pz, tx, ty, tz, rt2);
+      if (ortho) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          tx[k] = dsub(px[LB[k]] - px[LA[k]], cx[k]);
+          ty[k] = dsub(py[LB[k]] - py[LA[k]], cy[k]);
+          tz[k] = dsub(pz[LB[k]] - pz[LA[k]], cz[k]);
+          rt2[k] = dadd(dadd(dmul(tx[k], tx[k]), dmul(ty[k], ty[k])), dmul(tz[k], tz[k]));
+        }
+      } else {
+        tri_vectors(b, px, py, pz, tx, ty, tz, rt2);
+      }
       double maxdist = 0.;
 #pragma unroll
       for (int k = 0; k < 3; ++k) maxdist = fmax(maxdist, fabs(rt2[k] - r2c[k]) * irc[k]);
