@@ -21,6 +21,26 @@ def test_water_generator_deterministic_and_neutral():
     assert np.allclose(np.sqrt((d * d).sum(1)), 0.9572, atol=1e-12)
 
 
+def test_orthorhombic_water_box():
+    L = np.array([25.0, 27.0, 70.0])
+    a = systems.water_box_ortho(L, seed=2)
+    b = systems.water_box_ortho(L, seed=2)
+    assert np.array_equal(a.z, b.z)
+    m = a.meta["molecules"]
+    # a full lattice at the water density, n_a = round(L_a * density^(1/3))
+    nl = np.rint(L * systems.WATER_DENSITY ** (1.0 / 3.0)).astype(int)
+    assert m == int(np.prod(nl)) and a.n == 3 * m and abs(a.q.sum()) < 1e-9
+    assert np.array_equal(a.cell(), [25.0, 0, 0, 0, 27.0, 0, 0, 0, 70.0])
+    for v, edge in ((a.x, L[0]), (a.y, L[1]), (a.z, L[2])):
+        assert np.all(np.abs(v) <= 0.5 * edge)
+    # rigid geometry under the minimum image of each axis
+    for h in (1, 2):
+        d = np.stack([a.x[h::3] - a.x[0::3], a.y[h::3] - a.y[0::3], a.z[h::3] - a.z[0::3]], 1)
+        d -= L * np.round(d / L)
+        assert np.allclose(np.sqrt((d * d).sum(1)), 0.9572, atol=1e-12)
+    assert len(a.bonds) == 2 * m and len(a.angles) == m
+
+
 def test_96k_box_density_and_velocities():
     s = systems.config_96k(seed=1)
     assert s.n == 96000 and s.box == 98.6
