@@ -493,6 +493,15 @@ __device__ __noinline__ double mdbas_pair_r2(const DevBox &b, int listMode,
   return dist_d(b, dx, dy, dz);
 }
 
+// An asynchronous 16-byte copy from global into shared memory (completed by
+// cp.async.wait_all).
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(smem)),
+               "l"(gmem)
+               : "memory");
+}
+
 // Shared-memory loads the compiler keeps where they are written (not hoisted
 // out of a loop into registers that the loop would then hold throughout).
 __device__ __forceinline__ float4 lds_keep(const float4 *p) {
@@ -1124,8 +1133,9 @@ k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
     for (int r = 0; r < kClusterSize; ++r) {
       const int idx = lane + 32 * r, k = idx >> 3, a = idx & 7;
       const int jk = __shfl_sync(0xffffffffu, en.j, k);
-      if (k < ne) B.sj[a * kItemMax + k] = xq[jk * kClusterSize + a];
+      if (k < ne) cp_async16(&B.sj[a * kItemMax + k], xq + (size_t)jk * kClusterSize + a);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     __syncwarp();
     unsigned in0 = 0u, in1 = 0u;  // set bits: beyond the inner radius
     if (lane < ne) {
