@@ -134,6 +134,24 @@ k_col_scan(int nCols, const int *__restrict__ colCount, int *__restrict__ colSta
   }
 }
 
+// The build's counters and per-column tallies cleared in one launch (instead
+// of a memset each): column atom counts and fill cursors, the search's
+// counters of both lists, the largest half extents per replica.
+__global__ void __launch_bounds__(256)
+k_build_reset(int nCols, int nRep, int *__restrict__ colCount, int *__restrict__ colFill,
+              long long *__restrict__ counters, long long *__restrict__ countersIn,
+              int *__restrict__ hmax) {
+  for (int i = threadIdx.x; i <= nCols; i += blockDim.x) {
+    colCount[i] = 0;
+    colFill[i] = 0;
+  }
+  if (threadIdx.x < 8) {
+    counters[threadIdx.x] = 0;
+    countersIn[threadIdx.x] = 0;
+  }
+  for (int i = threadIdx.x; i < 4 * nRep; i += blockDim.x) hmax[i] = 0;
+}
+
 __global__ void k_col_scatter(int n, const int *__restrict__ atomCol,
                               const int *__restrict__ colStart, int *__restrict__ colFill,
                               int *__restrict__ tmpIdx) {
@@ -1362,6 +1380,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     MDB_TRY(w.tmpIdx.ensure(sizeof(int) * n));
     MDB_TRY(w.slotOf.ensure(sizeof(int) * n));
     MDB_TRY(w.counters.ensure(sizeof(long long) * 8));
+    MDB_TRY(w.countersIn.ensure(sizeof(long long) * 8));
     MDB_TRY(w.acc.ensure(sizeof(long long) * ACC_COUNT));
     if (!w.sticky.p) {
       MDB_TRY(w.sticky.ensure(sizeof(long long)));
@@ -1386,10 +1405,9 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
   }
   const ClusterGeom *gd = w.geoms.as<ClusterGeom>();
 
-  MDB_CUDA(cudaMemsetAsync(w.colCount.p, 0, sizeof(int) * (nCols + 1), s));
-  MDB_CUDA(cudaMemsetAsync(w.colFill.p, 0, sizeof(int) * (nCols + 1), s));
-  MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 8, s));
-  MDB_CUDA(cudaMemsetAsync(w.hmax.p, 0, sizeof(int) * 4 * nRep, s));
+  MDB_LAUNCH(k_build_reset, 1, 256, 0, s, nCols, nRep, w.colCount.as<int>(),
+             w.colFill.as<int>(), w.counters.as<long long>(), w.countersIn.as<long long>(),
+             w.hmax.as<int>());
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[0], s));
   MDB_LAUNCH(k_col_bin, grid_for(n, 256), 256, 0, s, n, gd, w.atomRepDev(), w.colOff.as<int>(),
              w.colRank.as<int>(), x, y, z, w.atomCol.as<int>(), w.atomZ.as<double>(),
@@ -1433,11 +1451,12 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
       MDB_TRY(w.entriesIn.ensure(sizeof(HalfEntry) * (size_t)w.inEntryCap));
       MDB_TRY(w.masksIn.ensure(sizeof(unsigned) * (size_t)w.inEntryCap));
       MDB_TRY(w.itemsIn.ensure(sizeof(int4) * (size_t)w.inItemCap));
-      MDB_TRY(w.countersIn.ensure(sizeof(long long) * 8));
     }
-    MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
-    MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 3, s));
-    MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
+    if (attempt > 0) {  // the first attempt's counters were cleared by k_build_reset
+      MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
+      MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 3, s));
+      MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
+    }
     SearchOut o;
     o.entries = w.entries.as<CPairEntry>();
     o.masks = w.masks.as<uint2>();
