@@ -273,6 +273,30 @@ def test_evaluate_equals_separate_calls(gpu):
         x, y, z = (v + rng.uniform(-0.3, 0.3, s.n) for v in (x, y, z))
     with pytest.raises(ValueError):
         a.evaluate(x, y, z, np.zeros(s.n, np.float32), fy, fz)
+
+    def separate(px, py, pz):
+        b.set_positions(px, py, pz)
+        b.build()
+        b.compute()
+        return b.forces(), b.energies()
+
+    # the same array objects again with their contents changed in place (the
+    # kept pointer arguments read the new values), and float32 positions,
+    # converted on every call
+    fx, fy, fz = (np.zeros(s.n) for _ in range(3))
+    x, y, z = s.x.copy(), s.y.copy(), s.z.copy()
+    a.evaluate(x, y, z, fx, fy, fz)
+    for shift in (0.05, 0.1):
+        x += shift
+        ea = a.evaluate(x, y, z, fx, fy, fz)
+        g, eb = separate(x, y, z)
+        assert all(np.array_equal(u, v) for u, v in zip((fx, fy, fz), g)) and ea == eb
+    x32, y32, z32 = (v.astype(np.float32) for v in (s.x, s.y, s.z))
+    for shift in (0.0, 0.125):
+        x32 += np.float32(shift)
+        ea = a.evaluate(x32, y32, z32, fx, fy, fz)
+        g, eb = separate(*(v.astype(np.float64) for v in (x32, y32, z32)))
+        assert all(np.array_equal(u, v) for u, v in zip((fx, fy, fz), g)) and ea == eb
     a.close()
     b.close()
 
