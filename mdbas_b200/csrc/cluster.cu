@@ -464,8 +464,8 @@ struct WarpBuf {
 // pair within sqrt(rin2), 32-bit masks).
 // Both lists take their room with one 64-bit atomic per flush on a packed
 // counter (items << 40 | entries taken): counters[4]; the inner list uses the
-// same item index and twice the entry index.  A one-thread kernel writes the
-// readers' counts into counters[0..1] / hcounters[0..1].
+// same item index and twice the entry index.  The search's last warp writes
+// the readers' counts into counters[0..1] / hcounters[0..1].
 constexpr int kPackShift = 40;
 struct SearchOut {
   CPairEntry *entries;
@@ -478,6 +478,7 @@ struct SearchOut {
   int4 *hitems;
   long long *hcounters;
   float rin2;
+  long long *sticky;  // a build that does not wait: the word the error bits are latched into
 };
 
 // MDBas's FP64 squared distance of atoms a and c, the expression of the list
@@ -826,7 +827,8 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
   __shared__ WarpBuf bufs[kSearchThreads / 32];
   const int lane = threadIdx.x & 31;
   const int ci = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  if (ci >= (*nSlotsDev >> 3)) return;
+  const int nClusters = *nSlotsDev >> 3;
+  if (ci >= nClusters) return;
   WarpBuf &B = bufs[threadIdx.x >> 5];
   const int rep = clusterRep ? clusterRep[ci] : 0;
   const ClusterGeom &g = geoms[rep];
@@ -1057,19 +1059,36 @@ k_search(const int *__restrict__ nSlotsDev, const ClusterGeom *__restrict__ geom
       atomicAdd(reinterpret_cast<unsigned long long *>(o.hcounters + 4),
                 (unsigned long long)B.tally[3]);
     }
-  }
-}
-
-// The search's counts for the readers: entries kept (counters[5]) and inner
-// halves written (hcounters[6]); both lists have the packed counter's item
-// count (items << 40 | entries taken, counters[4]).
-__global__ void k_unpack_counts(long long *__restrict__ counters, long long *__restrict__ hcounters) {
-  if (threadIdx.x == 0) {
-    const unsigned long long a = (unsigned long long)counters[4];
-    counters[0] = counters[5];
-    counters[1] = (long long)(a >> kPackShift);
-    hcounters[0] = hcounters[6];
-    hcounters[1] = (long long)(a >> kPackShift);
+    // The warp that finishes last (counters[7] counts the finished ones)
+    // writes the readers' counts: entries kept (counters[5]) and inner halves
+    // written (hcounters[6]); both lists have the packed counter's item count
+    // (items << 40 | entries taken, counters[4]).  For a build that does not
+    // wait it also latches the error bits into the sticky word: a list that
+    // overflowed is unusable (its item count may point past the item buffer
+    // and some items were never written), so the counts of both lists are
+    // zeroed and the pair kernels that follow in the same stream (or graph)
+    // see an empty list until the host rebuilds with room.
+    __threadfence();
+    const unsigned long long done =
+        atomicAdd(reinterpret_cast<unsigned long long *>(o.counters + 7), 1ull);
+    if (done + 1ull == (unsigned long long)nClusters) {
+      __threadfence();
+      auto rd = [](long long *p) {  // the value in L2, after every warp's atomics
+        return (long long)atomicAdd(reinterpret_cast<unsigned long long *>(p), 0ull);
+      };
+      const unsigned long long a = (unsigned long long)rd(o.counters + 4);
+      long long nEnt = rd(o.counters + 5), nIt = (long long)(a >> kPackShift);
+      long long nHalf = rd(o.hcounters + 6);
+      if (o.sticky) {
+        const long long f = rd(o.counters + 2) | rd(o.hcounters + 2);
+        o.sticky[0] |= f;
+        if (f & CL_OVERFLOW) nEnt = nIt = nHalf = 0;
+      }
+      o.counters[0] = nEnt;
+      o.counters[1] = nIt;
+      o.hcounters[0] = nHalf;
+      o.hcounters[1] = nIt;
+    }
   }
 }
 
@@ -1215,7 +1234,8 @@ k_prune(const long long *__restrict__ counters, const int4 *__restrict__ items,
   }
 }
 
-// Latch a search's (or prune's) error bits into the sticky word.  A list
+// Latch a prune's error bits into the sticky word (the search latches its
+// own in its last warp).  A list
 // that overflowed is unusable: its item count may point past the item buffer
 // and some items were never written, so the counts of both lists are zeroed
 // and the pair kernels that follow in the same stream (or graph) see an
@@ -1454,7 +1474,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     }
     if (attempt > 0) {  // the first attempt's counters were cleared by k_build_reset
       MDB_CUDA(cudaMemsetAsync(w.counters.p, 0, sizeof(long long) * 2, s));
-      MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 3, s));
+      MDB_CUDA(cudaMemsetAsync(w.counters.as<long long>() + 3, 0, sizeof(long long) * 5, s));
       MDB_CUDA(cudaMemsetAsync(w.countersIn.p, 0, sizeof(long long) * 8, s));
     }
     SearchOut o;
@@ -1469,6 +1489,7 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
     o.hitems = w.itemsIn.as<int4>();
     o.hcounters = w.countersIn.as<long long>();
     o.rin2 = rin2;
+    o.sticky = sync ? nullptr : w.sticky.as<long long>();
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[5], s));
     MDB_LAUNCH(k_search, grid_for((long long)w.clCap * 32, kSearchThreads), kSearchThreads, 0, s,
                w.nSlotsDev(), gd, w.boxes.as<DevBox>(), w.clusterRepDev(), w.colOff.as<int>(),
@@ -1476,14 +1497,10 @@ int cluster_build(ClusterWork &w, int n, int nRep, const DevBox *boxes, const in
                w.origin.as<double4>(), w.originF.as<float4>(), w.half.as<float4>(),
                w.slotAtom.as<int>(), w.slotOf.as<int>(), frozen, exclStart, exclFlat,
                w.hmax.as<int>(), w.xq.as<float4>(), x, y, z, o);
-    MDB_LAUNCH(k_unpack_counts, 1, 32, 0, s, w.counters.as<long long>(),
-               w.countersIn.as<long long>());
   if (w.timeStages) MDB_CUDA(cudaEventRecord(w.stageEv[6], s));
     w.innerRin2 = rin2;
     if (!sync) {
       w.useInner = true;
-      MDB_LAUNCH(k_latch, 1, 32, 0, s, w.counters.as<long long>(), w.countersIn.as<long long>(),
-                 w.sticky.as<long long>());
       return MDBAS_NB_OK;
     }
     long long flags[8], hflags[4];

@@ -102,8 +102,9 @@ struct ClusterWork {
   DBuf entries;       // CPairEntry
   DBuf masks;         // uint2 (64 interaction bits)
   DBuf items;         // int4: i cluster, first entry, entry count, 0
-  DBuf counters;      // int64[8]: entries, items, overflow flag, candidates, and the
-                      // search's packed count (items << 40 | entries)
+  DBuf counters;      // int64[8]: entries, items, overflow flag, candidates, the search's
+                      // packed count (items << 40 | entries taken), entries kept, -,
+                      // search warps finished
   long long entryCap = 0, itemCap = 0;
   long long nEntries = 0, nItems = 0;
   // Inner list: the j-cluster halves of the list above that hold a pair
